@@ -1,0 +1,273 @@
+/*
+ * mobydiff_b200.h -- C ABI of libmobyb200.so, the sm_100a implementation of
+ * the mobydiff RK3 time step.
+ *
+ * The entry points replace the OpenMP-offload bodies of the reference's
+ * Fortran modules one for one.  Each declaration names the reference
+ * interface it stands in for (paths relative to the mobydiff project root).
+ * A Fortran caller binds them with iso_c_binding; the
+ * driver, the INI reader, I/O and IBM geometry set-up stay on the host.
+ *
+ * Conventions
+ *   - Every call returns an int status: MDX_OK (0) or one of MDX_ERR_*;
+ *     mdx_last_error() gives the message of the last failure on a context.
+ *   - Field arrays are the reference's host arrays, unchanged: padded
+ *     (0:nx+1,0:ny+1,0:nz+1) in Fortran order, element (i,j,k) at
+ *     i + (nx+2)*(j + (ny+2)*k); oldrhs* are (1:nx,1:ny,1:nz).
+ *     src/modules/init.f90:14-19, src/modules/field_hdf5.c:4-7.
+ *   - Device mirrors are owned by the context (allocated in
+ *     mdx_enter_field_data, freed in mdx_exit_field_data), like OpenMP
+ *     `target enter/exit data` in src/modules/gpu_runtime.f90:22-48.
+ *   - One CUDA stream per context; calls are stream-ordered and return without
+ *     a host synchronisation except where they hand results to the host
+ *     (updates to the host, CFL, projection statistics).
+ *   - Single host thread per context.
+ */
+#ifndef MOBYDIFF_B200_H
+#define MOBYDIFF_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define MDX_OK                0
+#define MDX_ERR_ARG           1   /* invalid argument / unsupported size      */
+#define MDX_ERR_CUDA          2   /* a CUDA runtime call failed               */
+#define MDX_ERR_NO_DEVICE     3   /* no usable CUDA device                    */
+#define MDX_ERR_STATE         4   /* call out of order (e.g. no field data)   */
+#define MDX_NOT_CONVERGED     5   /* SOR hit max_iter before the tolerance    */
+#define MDX_ERR_NONFINITE     6   /* NaN/Inf detected in a residual or field  */
+#define MDX_ERR_IO            7   /* file could not be read / parsed          */
+#define MDX_ERR_TIMEOUT       8   /* a bounded device wait gave up            */
+
+/* ---- pressure solvers / precisions ------------------------------------ */
+#define MDX_SOLVER_FFT        0   /* batched x-z real FFT + Thomas in y      */
+#define MDX_SOLVER_REDBLACK   1   /* red-black SOR                            */
+#define MDX_PREC_FP64         0
+#define MDX_PREC_MIXED        1   /* FP32 inner solve in FP64 defect correction */
+
+/* ---- field identifiers for mdx_copy_field ----------------------------- */
+enum {
+    MDX_UN = 0, MDX_US, MDX_VN, MDX_VS, MDX_WN, MDX_WS, MDX_PN,
+    MDX_OLDRHSU, MDX_OLDRHSV, MDX_OLDRHSW,
+    MDX_COEF_U, MDX_COEF_V, MDX_COEF_W,
+    MDX_PHI,          /* last pressure correction, rhs(nx,nz,ny) layout (FFT path) */
+    MDX_NUM_FIELDS
+};
+
+/* grid_type, src/modules/init.f90:5-12 (same components, same order). */
+typedef struct {
+    int nx, ny, nz;
+    int nsteps;
+    double lx, ly, lz;
+    double dx, dy, dz;
+    double re, dt, t_final, t_current, cfl, cflmax, dtmax;
+    double forcing_x, forcing_y, forcing_z;
+} mdx_grid_t;
+
+/* boundary_type, src/modules/boundary.f90:6-10.  bc_type / bc_value keep the
+ * Fortran memory order of bcType(1:3,0:1,0:3): index (dir-1)+3*(side+2*var),
+ * dir x/y/z = 1..3, side min/max = 0/1, var p/u/v/w = 0..3; 0 Dirichlet,
+ * 1 Neumann. */
+typedef struct {
+    int is_periodic[3];
+    int bc_type[24];
+    double bc_value[24];
+} mdx_bc_t;
+
+/* pressure_solver_type knobs (src/modules/pressure_workspace.f90:7-8) plus the
+ * [b200] input.ini section.  mdx_default_solver_opts() fills the reference
+ * defaults (FFT, nIter 3, sor 1.5, fixed iteration count). */
+typedef struct {
+    int solver;        /* MDX_SOLVER_*                                        */
+    int n_iter;        /* red-black: sweeps per projection when tol <= 0      */
+    double sor;        /* red-black over-relaxation factor                    */
+    double tol;        /* red-black: stop when ||div u||2 <= tol*||div u*||2; <= 0: fixed n_iter */
+    int max_iter;      /* red-black: iteration cap when tol > 0               */
+    int check_every;   /* red-black: iterations between residual checks       */
+    int precision;     /* MDX_PREC_*                                          */
+    int reserved_i[7];
+    double atol;       /* red-black: absolute floor of ||div u||2, also accepted as converged.
+                          < 0 (default): the FP64 round-off level of the divergence,
+                          eps*sqrt(nx*ny*nz)*max|u*|*(1/dx+1/dy+1/dz); 0: none */
+    double reserved_d[7];
+} mdx_solver_opts_t;
+
+/* Statistics of the last pressure projection. */
+typedef struct {
+    int iterations;     /* red-black iterations (red+black = 1); 0 for FFT   */
+    int status;         /* MDX_OK / MDX_NOT_CONVERGED / MDX_ERR_NONFINITE    */
+    double residual;    /* final ||div u||2 / ||div u*||2 (red-black)        */
+    double residual0;   /* ||div u*||2                                       */
+    double atol;        /* absolute floor used (red-black)                   */
+} mdx_solve_stats_t;
+
+/* Per-kernel-class device time, filled when timing is on (mdx_set_timing). */
+enum {
+    MDX_T_MOMENTUM = 0, MDX_T_BC, MDX_T_FFT_FWD, MDX_T_THOMAS, MDX_T_FFT_INV,
+    MDX_T_CORRECT, MDX_T_SOR_SWEEP, MDX_T_RESIDUAL, MDX_T_OTHER, MDX_T_NUM
+};
+typedef struct {
+    double ms[MDX_T_NUM];
+    long long launches[MDX_T_NUM];
+} mdx_timing_t;
+
+typedef struct mdx_ctx mdx_ctx_t;
+
+/* ---- library / device ------------------------------------------------- */
+
+/* Library version string. */
+const char* mdx_version(void);
+
+/* Replaces init_openmp_offload, src/modules/gpu_runtime.f90:11-20: reports
+ * the number of CUDA devices (0 when none; returns MDX_ERR_NO_DEVICE then). */
+int mdx_device_count(int* count);
+
+/* Message of the last failed call on ctx (or of the last failed
+ * context-less call when ctx is NULL). */
+const char* mdx_last_error(const mdx_ctx_t* ctx);
+
+/* Fill the reference defaults: mdx_grid_t from init_grid
+ * (src/modules/init.f90:23-44), mdx_bc_t from init_bc
+ * (src/modules/boundary.f90:14-20), solver options from
+ * pressure_workspace.f90:7-8 with the FFT solver. */
+void mdx_default_grid(mdx_grid_t* g);
+void mdx_default_bc(mdx_bc_t* bc);
+void mdx_default_solver_opts(mdx_solver_opts_t* o);
+
+/* finalize_grid, src/modules/init.f90:38-44: dx,dy,dz and t_final. */
+void mdx_finalize_grid(mdx_grid_t* g);
+
+/* ---- host-side helpers (no device needed) ------------------------------ */
+
+/* read_runtime_config, src/modules/config.f90:10-75, with the same
+ * sections, keys, aliases, comment rules and warnings; plus the [b200]
+ * section (solver, tol, omega, max_iter, check_every, precision, seed, ...).
+ * A missing file keeps the defaults (config.f90:33-45) and returns MDX_OK.
+ * Outputs may be NULL. */
+typedef struct {
+    int output_interval;
+    int field_interval;
+    char output_prefix[256];
+    char field_prefix[256];
+    /* [b200] section */
+    int ic;              /* 0 = zero fields (reference), 1 = seeded channel IC */
+    uint64_t seed;
+    int ibm;             /* -1 none, 0 reference bump (ibm.f90:45-50), 1 wavy channel */
+    double ibm_amp, ibm_lambda, ibm_y0, ibm_height;
+    int warnings;        /* number of warnings printed */
+} mdx_run_config_t;
+int mdx_read_runtime_config(const char* path, mdx_grid_t* g, mdx_bc_t* bc, mdx_solver_opts_t* opts,
+                            mdx_run_config_t* run);
+
+/* set_ibm_coeff with USE_IBM_SECONDORDER, src/modules/ibm.f90:133-187, on the
+ * host (the reference computes the coefficients on the host once).
+ * geometry 0: the reference's lower-wall sinusoid with amp (ibm.f90:84-99);
+ * geometry 1: wavy channel, fluid for y_lo(x) < y < y_lo(x)+height with
+ * y_lo(x) = y0 + amp*sin(2*pi*x/lambda + phase).
+ * coeff: padded array; dix/diy/diz select the u/v/w staggering. */
+typedef struct {
+    int geometry;
+    int n_wave_x;
+    double amp, phase, lambda, y0, height;
+} mdx_ibm_geom_t;
+int mdx_set_ibm_coeff(const mdx_grid_t* g, const mdx_ibm_geom_t* geom, double* coeff, int dix, int diy, int diz);
+
+/* ---- context ---------------------------------------------------------- */
+
+/* Create a context on `device` for grid g and boundary set bc. */
+int mdx_create(int device, const mdx_grid_t* g, const mdx_bc_t* bc, mdx_ctx_t** out);
+int mdx_destroy(mdx_ctx_t* ctx);
+
+/* Use an external CUDA stream (cudaStream_t) instead of the context's own;
+ * NULL restores the context stream. */
+int mdx_set_stream(mdx_ctx_t* ctx, void* stream);
+int mdx_get_stream(mdx_ctx_t* ctx, void** stream);
+
+/* enter_field_data / exit_field_data, src/modules/gpu_runtime.f90:22-48:
+ * allocate the 10 device mirrors and copy the host arrays in; free them.
+ * Any host pointer may be NULL, which zero-fills that mirror. */
+int mdx_enter_field_data(mdx_ctx_t* ctx,
+                         const double* un, const double* us, const double* oldrhsu,
+                         const double* vn, const double* vs, const double* oldrhsv,
+                         const double* wn, const double* ws, const double* oldrhsw,
+                         const double* pn);
+int mdx_exit_field_data(mdx_ctx_t* ctx);
+
+/* `!$omp target update from/to` of un,vn,wn,pn around output and restart,
+ * src/modules/io.f90:123-128 and :160-165.  update_host synchronises. */
+int mdx_update_host(mdx_ctx_t* ctx, double* un, double* vn, double* wn, double* pn);
+int mdx_update_device(mdx_ctx_t* ctx, const double* un, const double* vn, const double* wn, const double* pn);
+
+/* Copy any one array between host and device (direction 0: device->host,
+ * synchronising; 1: host->device).  MDX_PHI is device->host only. */
+int mdx_copy_field(mdx_ctx_t* ctx, int field, double* host, int direction);
+
+/* enter_ibm_data / exit_ibm_data, src/modules/ibm.f90:57-81.  NULL
+ * coefficients mean "no body" (all zero).  exit restores zero coefficients. */
+int mdx_enter_ibm_data(mdx_ctx_t* ctx, const double* coef_u, const double* coef_v, const double* coef_w);
+int mdx_exit_ibm_data(mdx_ctx_t* ctx);
+
+/* ---- time step ---------------------------------------------------------- */
+
+/* momentum, src/modules/step.f90:27-207 (predictor of u*,v*,w*, RHS store). */
+int mdx_momentum(mdx_ctx_t* ctx, double dt_alpha, double dt_beta, double dt_gamma);
+
+/* apply_bc, src/modules/boundary.f90:23-170 (FFT builds: y walls, periodic
+ * x/z on the n and * arrays), and apply_bc_redblack, :173-368. */
+int mdx_apply_bc(mdx_ctx_t* ctx);
+int mdx_apply_bc_redblack(mdx_ctx_t* ctx);
+
+/* init_pressure_solver / destroy_pressure_solver,
+ * src/modules/pressure_solver.f90:35-46,65-74 (plans, Thomas tables,
+ * workspace; the red-black even-size check of pressure_redblack.f90:16-18). */
+int mdx_init_pressure_solver(mdx_ctx_t* ctx, const mdx_solver_opts_t* opts);
+int mdx_destroy_pressure_solver(mdx_ctx_t* ctx);
+
+/* pressure_projection, src/modules/pressure_solver.f90:48-63.  stats may be
+ * NULL; with stats or a residual tolerance the call synchronises. */
+int mdx_pressure_projection(mdx_ctx_t* ctx, double dt_gamma, mdx_solve_stats_t* stats);
+
+/* get_cfl, src/modules/step.f90:210-258 (synchronises). */
+int mdx_get_cfl(mdx_ctx_t* ctx, double* cfl);
+
+/* center_vel, src/modules/io.f90:184-222: cell-centred velocities
+ * (1:nx,1:ny,1:nz) copied to the host (synchronises). */
+int mdx_center_vel(mdx_ctx_t* ctx, double* uc, double* vc, double* wc);
+
+/* `nsteps` whole RK3 steps with fixed dt, src/main.f90:66-90 (substage
+ * order momentum -> apply_bc -> pressure_projection -> apply_bc, or the
+ * red-black variant).  Adds nsteps*dt to g.t_current.  The FFT path is
+ * replayed from a CUDA graph.  total_iters (may be NULL) returns the summed
+ * red-black iterations. */
+int mdx_step(mdx_ctx_t* ctx, int nsteps, long long* total_iters);
+
+/* Seeded channel initial condition + projection at t=0 (new; the reference
+ * zero-initialises, src/modules/init.f90:67-70): u = max(0,1-(y-yc(x))^2) +
+ * U(-amp_u,amp_u), v,w = U(-amp_vw,amp_vw) (counter-based SplitMix64 on
+ * seed, field and padded index), yc(x) = y0 + 1 + wave_amp*sin(2*pi*x/
+ * wave_lambda); then apply_bc, pressure_projection with dt_gamma = 1 and p=0.
+ * Requires field data and an initialised pressure solver. */
+int mdx_channel_ic(mdx_ctx_t* ctx, uint64_t seed, double amp_u, double amp_vw, double y0,
+                   double wave_amp, double wave_lambda, mdx_solve_stats_t* stats);
+
+/* Device divergence norms of (un,vn,wn) with the red-black neighbour rule
+ * (synchronises). */
+int mdx_divergence_norms(mdx_ctx_t* ctx, double* l2, double* linf);
+
+/* Per-kernel-class device timing with CUDA events on the context stream. */
+int mdx_set_timing(mdx_ctx_t* ctx, int on);
+int mdx_get_timing(mdx_ctx_t* ctx, mdx_timing_t* out);   /* synchronises; accumulated since set_timing(1) */
+
+/* Number of kernel launches issued by the library on this context so far. */
+long long mdx_launch_count(const mdx_ctx_t* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MOBYDIFF_B200_H */

@@ -1,0 +1,414 @@
+"""mobydiff_b200 -- sm_100a implementation of the mobydiff RK3 time step.
+
+The compute lives in ``libmobyb200.so`` (CUDA, built in-tree by
+``mobydiff_b200.build``) behind the C ABI of ``include/mobydiff_b200.h``.
+This package is the Python-side mirror of the reference's Fortran modules
+for that path, calling the C ABI through ctypes:
+
+=======================  ==============================================
+reference (Fortran)      here
+=======================  ==============================================
+init_openmp_offload      device_count()
+enter/exit_field_data    Solver.enter_field_data / exit_field_data
+enter/exit_ibm_data      Solver.enter_ibm_data / exit_ibm_data
+momentum                 Solver.momentum
+apply_bc(_redblack)      Solver.apply_bc / apply_bc_redblack
+init_pressure_solver     Solver.init_pressure_solver
+pressure_projection      Solver.pressure_projection
+get_cfl                  Solver.get_cfl
+center_vel               Solver.center_vel
+read_runtime_config      read_runtime_config
+set_ibm_coeff            set_ibm_coeff
+=======================  ==============================================
+
+There is no CPU fallback: every compute call goes to the CUDA library and
+raises ``MdxError`` when the library or a device is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libmobyb200.so")
+
+MDX_OK = 0
+MDX_ERR_ARG = 1
+MDX_ERR_CUDA = 2
+MDX_ERR_NO_DEVICE = 3
+MDX_ERR_STATE = 4
+MDX_NOT_CONVERGED = 5
+MDX_ERR_NONFINITE = 6
+MDX_ERR_IO = 7
+MDX_ERR_TIMEOUT = 8
+
+SOLVER_FFT = 0
+SOLVER_REDBLACK = 1
+PREC_FP64 = 0
+PREC_MIXED = 1
+
+FIELDS = ["un", "us", "vn", "vs", "wn", "ws", "pn", "oldrhsu", "oldrhsv", "oldrhsw",
+          "coef_u", "coef_v", "coef_w", "phi"]
+FIELD_ID = {n: t for t, n in enumerate(FIELDS)}
+TIMER_CLASSES = ["momentum", "bc", "fft_fwd", "thomas", "fft_inv", "correct", "sor_sweep", "residual", "other"]
+
+
+class MdxError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"mdx error {code}: {msg}")
+        self.code = code
+
+
+class GridT(C.Structure):
+    """grid_type, src/modules/init.f90:5-12."""
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("nsteps", C.c_int),
+                ("lx", C.c_double), ("ly", C.c_double), ("lz", C.c_double),
+                ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double),
+                ("re", C.c_double), ("dt", C.c_double), ("t_final", C.c_double), ("t_current", C.c_double),
+                ("cfl", C.c_double), ("cflmax", C.c_double), ("dtmax", C.c_double),
+                ("forcing_x", C.c_double), ("forcing_y", C.c_double), ("forcing_z", C.c_double)]
+
+
+class BcT(C.Structure):
+    """boundary_type, src/modules/boundary.f90:6-10 (bcType in Fortran memory order)."""
+    _fields_ = [("is_periodic", C.c_int * 3), ("bc_type", C.c_int * 24), ("bc_value", C.c_double * 24)]
+
+
+class SolverOptsT(C.Structure):
+    _fields_ = [("solver", C.c_int), ("n_iter", C.c_int), ("sor", C.c_double), ("tol", C.c_double),
+                ("max_iter", C.c_int), ("check_every", C.c_int), ("precision", C.c_int),
+                ("reserved_i", C.c_int * 7), ("atol", C.c_double), ("reserved_d", C.c_double * 7)]
+
+
+class SolveStatsT(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("status", C.c_int), ("residual", C.c_double), ("residual0", C.c_double),
+                ("atol", C.c_double)]
+
+
+class TimingT(C.Structure):
+    _fields_ = [("ms", C.c_double * 9), ("launches", C.c_longlong * 9)]
+
+
+class RunConfigT(C.Structure):
+    _fields_ = [("output_interval", C.c_int), ("field_interval", C.c_int),
+                ("output_prefix", C.c_char * 256), ("field_prefix", C.c_char * 256),
+                ("ic", C.c_int), ("seed", C.c_uint64), ("ibm", C.c_int),
+                ("ibm_amp", C.c_double), ("ibm_lambda", C.c_double), ("ibm_y0", C.c_double),
+                ("ibm_height", C.c_double), ("warnings", C.c_int)]
+
+
+class IbmGeomT(C.Structure):
+    _fields_ = [("geometry", C.c_int), ("n_wave_x", C.c_int), ("amp", C.c_double), ("phase", C.c_double),
+                ("lambda_", C.c_double), ("y0", C.c_double), ("height", C.c_double)]
+
+
+_lib = None
+
+
+def lib():
+    """Load libmobyb200.so (built by ``python -m mobydiff_b200.build``)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise MdxError(MDX_ERR_STATE, f"{LIB_PATH} is missing: run `python -m mobydiff_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    P = C.POINTER
+    d = C.c_double
+    vp = C.c_void_p
+    i = C.c_int
+    sig = {
+        "mdx_version": (C.c_char_p, []),
+        "mdx_device_count": (i, [P(i)]),
+        "mdx_last_error": (C.c_char_p, [vp]),
+        "mdx_default_grid": (None, [P(GridT)]),
+        "mdx_default_bc": (None, [P(BcT)]),
+        "mdx_default_solver_opts": (None, [P(SolverOptsT)]),
+        "mdx_finalize_grid": (None, [P(GridT)]),
+        "mdx_read_runtime_config": (i, [C.c_char_p, P(GridT), P(BcT), P(SolverOptsT), P(RunConfigT)]),
+        "mdx_set_ibm_coeff": (i, [P(GridT), P(IbmGeomT), vp, i, i, i]),
+        "mdx_create": (i, [i, P(GridT), P(BcT), P(vp)]),
+        "mdx_destroy": (i, [vp]),
+        "mdx_set_stream": (i, [vp, vp]),
+        "mdx_get_stream": (i, [vp, P(vp)]),
+        "mdx_enter_field_data": (i, [vp] + [vp] * 10),
+        "mdx_exit_field_data": (i, [vp]),
+        "mdx_update_host": (i, [vp, vp, vp, vp, vp]),
+        "mdx_update_device": (i, [vp, vp, vp, vp, vp]),
+        "mdx_copy_field": (i, [vp, i, vp, i]),
+        "mdx_enter_ibm_data": (i, [vp, vp, vp, vp]),
+        "mdx_exit_ibm_data": (i, [vp]),
+        "mdx_momentum": (i, [vp, d, d, d]),
+        "mdx_apply_bc": (i, [vp]),
+        "mdx_apply_bc_redblack": (i, [vp]),
+        "mdx_init_pressure_solver": (i, [vp, P(SolverOptsT)]),
+        "mdx_destroy_pressure_solver": (i, [vp]),
+        "mdx_pressure_projection": (i, [vp, d, P(SolveStatsT)]),
+        "mdx_get_cfl": (i, [vp, P(d)]),
+        "mdx_center_vel": (i, [vp, vp, vp, vp]),
+        "mdx_step": (i, [vp, i, P(C.c_longlong)]),
+        "mdx_channel_ic": (i, [vp, C.c_uint64, d, d, d, d, d, P(SolveStatsT)]),
+        "mdx_divergence_norms": (i, [vp, P(d), P(d)]),
+        "mdx_set_timing": (i, [vp, i]),
+        "mdx_get_timing": (i, [vp, P(TimingT)]),
+        "mdx_launch_count": (C.c_longlong, [vp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def version() -> str:
+    return lib().mdx_version().decode()
+
+
+def device_count() -> int:
+    n = C.c_int(0)
+    lib().mdx_device_count(C.byref(n))
+    return n.value
+
+
+def _check(rc: int, ctx=None):
+    if rc != MDX_OK:
+        msg = lib().mdx_last_error(ctx).decode(errors="replace")
+        raise MdxError(rc, msg)
+
+
+def _p(a):
+    if a is None:
+        return None
+    assert isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous, "need C-contiguous float64"
+    return a.ctypes.data
+
+
+# ---- reference-default structures -------------------------------------------
+def make_grid(nx, ny, nz, lx=1.0, ly=1.0, lz=1.0, re=100.0, dt=1e-4, forcing=(1.0, 0.0, 0.0), nsteps=1) -> GridT:
+    g = GridT()
+    lib().mdx_default_grid(C.byref(g))
+    g.nx, g.ny, g.nz, g.nsteps = int(nx), int(ny), int(nz), int(nsteps)
+    g.lx, g.ly, g.lz, g.re, g.dt = float(lx), float(ly), float(lz), float(re), float(dt)
+    g.forcing_x, g.forcing_y, g.forcing_z = (float(v) for v in forcing)
+    lib().mdx_finalize_grid(C.byref(g))
+    return g
+
+
+def make_bc(periodic=(True, True, True), types=None, values=None) -> BcT:
+    """types/values: dict {(dir, side, var): int/float}, dir 1..3, side 0/1, var p,u,v,w = 0..3."""
+    b = BcT()
+    lib().mdx_default_bc(C.byref(b))
+    for t in range(3):
+        b.is_periodic[t] = 1 if periodic[t] else 0
+    for (dd, s, v), val in (types or {}).items():
+        b.bc_type[(dd - 1) + 3 * (s + 2 * v)] = int(val)
+    for (dd, s, v), val in (values or {}).items():
+        b.bc_value[(dd - 1) + 3 * (s + 2 * v)] = float(val)
+    return b
+
+
+def channel_bc() -> BcT:
+    """Periodic x/z, walls in y, Neumann pressure (tutorials/wavychannel/input.ini:24-30)."""
+    return make_bc((True, False, True), types={(2, 0, 0): 1, (2, 1, 0): 1})
+
+
+def make_solver_opts(solver=SOLVER_FFT, n_iter=3, sor=1.5, tol=0.0, max_iter=100000, check_every=10,
+                     precision=PREC_FP64, atol=-1.0) -> SolverOptsT:
+    o = SolverOptsT()
+    lib().mdx_default_solver_opts(C.byref(o))
+    o.solver, o.n_iter, o.sor, o.tol = int(solver), int(n_iter), float(sor), float(tol)
+    o.max_iter, o.check_every, o.precision = int(max_iter), int(check_every), int(precision)
+    o.atol = float(atol)
+    return o
+
+
+def read_runtime_config(path: str):
+    """read_runtime_config (src/modules/config.f90:10-75) -> (grid, bc, opts, run)."""
+    g = GridT()
+    b = BcT()
+    o = SolverOptsT()
+    r = RunConfigT()
+    lib().mdx_default_grid(C.byref(g))
+    lib().mdx_default_bc(C.byref(b))
+    lib().mdx_default_solver_opts(C.byref(o))
+    _check(lib().mdx_read_runtime_config(path.encode(), C.byref(g), C.byref(b), C.byref(o), C.byref(r)))
+    return g, b, o, r
+
+
+def ibm_reference(g: GridT) -> IbmGeomT:
+    """The reference's hard-coded lower-wall sinusoid, src/modules/ibm.f90:45-50."""
+    return IbmGeomT(0, 1, 5 * g.dy, 0.0, 0.0, 0.0, 0.0)
+
+
+def ibm_wavy(amp, lam, y0, height=2.0, phase=0.0) -> IbmGeomT:
+    return IbmGeomT(1, 1, float(amp), float(phase), float(lam), float(y0), float(height))
+
+
+def set_ibm_coeff(g: GridT, geom: IbmGeomT):
+    """set_ibm_coeff for u, v, w (src/main.f90:57-60) -> (coef_u, coef_v, coef_w)."""
+    out = []
+    for dd in ((1, 0, 0), (0, 1, 0), (0, 0, 1)):
+        a = np.zeros((g.nz + 2, g.ny + 2, g.nx + 2))
+        _check(lib().mdx_set_ibm_coeff(C.byref(g), C.byref(geom), a.ctypes.data, *dd))
+        out.append(a)
+    return tuple(out)
+
+
+def rk_coeffs():
+    """src/modules/step.f90:21-23."""
+    return ([64.0 / 120.0, 50.0 / 120.0, 90.0 / 120.0],
+            [0.0, -34.0 / 120.0, -50.0 / 120.0],
+            [64.0 / 120.0, 16.0 / 120.0, 40.0 / 120.0])
+
+
+class Solver:
+    """One device context: the field mirrors, IBM coefficients and pressure solver."""
+
+    def __init__(self, grid: GridT, bc: BcT, device: int = 0):
+        self.grid = grid
+        self.bc = bc
+        h = C.c_void_p()
+        _check(lib().mdx_create(int(device), C.byref(grid), C.byref(bc), C.byref(h)))
+        self.h = h
+
+    # -- lifecycle
+    def close(self):
+        if getattr(self, "h", None):
+            lib().mdx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _c(self, rc):
+        _check(rc, self.h)
+
+    @property
+    def padded(self):
+        g = self.grid
+        return (g.nz + 2, g.ny + 2, g.nx + 2)
+
+    @property
+    def interior(self):
+        g = self.grid
+        return (g.nz, g.ny, g.nx)
+
+    # -- data residency (gpu_runtime.f90, ibm.f90, io.f90)
+    def enter_field_data(self, un=None, us=None, oldrhsu=None, vn=None, vs=None, oldrhsv=None, wn=None, ws=None,
+                         oldrhsw=None, pn=None):
+        self._c(lib().mdx_enter_field_data(self.h, _p(un), _p(us), _p(oldrhsu), _p(vn), _p(vs), _p(oldrhsv),
+                                           _p(wn), _p(ws), _p(oldrhsw), _p(pn)))
+
+    def exit_field_data(self):
+        self._c(lib().mdx_exit_field_data(self.h))
+
+    def enter_ibm_data(self, coef_u=None, coef_v=None, coef_w=None):
+        self._c(lib().mdx_enter_ibm_data(self.h, _p(coef_u), _p(coef_v), _p(coef_w)))
+
+    def exit_ibm_data(self):
+        self._c(lib().mdx_exit_ibm_data(self.h))
+
+    def update_host(self, un=None, vn=None, wn=None, pn=None):
+        self._c(lib().mdx_update_host(self.h, _p(un), _p(vn), _p(wn), _p(pn)))
+
+    def update_device(self, un=None, vn=None, wn=None, pn=None):
+        self._c(lib().mdx_update_device(self.h, _p(un), _p(vn), _p(wn), _p(pn)))
+
+    def get(self, name: str) -> np.ndarray:
+        g = self.grid
+        if name in ("oldrhsu", "oldrhsv", "oldrhsw"):
+            a = np.empty(self.interior)
+        elif name == "phi":
+            a = np.empty((g.ny, g.nz, g.nx))
+        else:
+            a = np.empty(self.padded)
+        self._c(lib().mdx_copy_field(self.h, FIELD_ID[name], a.ctypes.data, 0))
+        return a
+
+    def set(self, name: str, a: np.ndarray):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        self._c(lib().mdx_copy_field(self.h, FIELD_ID[name], a.ctypes.data, 1))
+
+    # -- time step
+    def momentum(self, dt_alpha, dt_beta, dt_gamma):
+        self._c(lib().mdx_momentum(self.h, dt_alpha, dt_beta, dt_gamma))
+
+    def apply_bc(self):
+        self._c(lib().mdx_apply_bc(self.h))
+
+    def apply_bc_redblack(self):
+        self._c(lib().mdx_apply_bc_redblack(self.h))
+
+    def init_pressure_solver(self, opts: SolverOptsT | None = None):
+        self.opts = opts if opts is not None else make_solver_opts()
+        self._c(lib().mdx_init_pressure_solver(self.h, C.byref(self.opts)))
+
+    def destroy_pressure_solver(self):
+        self._c(lib().mdx_destroy_pressure_solver(self.h))
+
+    def pressure_projection(self, dt_gamma, check=True) -> SolveStatsT:
+        st = SolveStatsT()
+        rc = lib().mdx_pressure_projection(self.h, dt_gamma, C.byref(st))
+        if check:
+            self._c(rc)
+        st.rc = rc
+        return st
+
+    def get_cfl(self) -> float:
+        c = C.c_double(0.0)
+        self._c(lib().mdx_get_cfl(self.h, C.byref(c)))
+        return c.value
+
+    def center_vel(self):
+        uc = np.empty(self.interior)
+        vc = np.empty(self.interior)
+        wc = np.empty(self.interior)
+        self._c(lib().mdx_center_vel(self.h, uc.ctypes.data, vc.ctypes.data, wc.ctypes.data))
+        return uc, vc, wc
+
+    def step(self, nsteps: int) -> int:
+        it = C.c_longlong(0)
+        self._c(lib().mdx_step(self.h, int(nsteps), C.byref(it)))
+        return it.value
+
+    def channel_ic(self, seed, amp_u=0.1, amp_vw=0.01, y0=0.0, wave_amp=0.0, wave_lambda=1.0) -> SolveStatsT:
+        st = SolveStatsT()
+        self._c(lib().mdx_channel_ic(self.h, seed, amp_u, amp_vw, y0, wave_amp, wave_lambda, C.byref(st)))
+        return st
+
+    def divergence_norms(self):
+        a = C.c_double(0.0)
+        b = C.c_double(0.0)
+        self._c(lib().mdx_divergence_norms(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def set_timing(self, on: bool):
+        self._c(lib().mdx_set_timing(self.h, 1 if on else 0))
+
+    def get_timing(self) -> dict:
+        t = TimingT()
+        self._c(lib().mdx_get_timing(self.h, C.byref(t)))
+        return {n: (t.ms[k], t.launches[k]) for k, n in enumerate(TIMER_CLASSES)}
+
+    def launch_count(self) -> int:
+        return lib().mdx_launch_count(self.h)
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        self._c(lib().mdx_get_stream(self.h, C.byref(s)))
+        return s.value or 0
+
+    def set_stream(self, stream_ptr: int | None):
+        self._c(lib().mdx_set_stream(self.h, C.c_void_p(stream_ptr) if stream_ptr else None))

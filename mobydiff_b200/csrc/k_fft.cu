@@ -1,0 +1,498 @@
+// k_fft.cu -- FFT pressure path: divergence, batched 2-D real FFT over the
+// periodic x-z planes, Thomas solve in y, inverse FFT and the projection.
+// Reference: src/modules/pressure_solver.f90:77-173,
+// src/modules/pressure/pressure_fft.f90:20-148 and the FFTW/cuFFT backends
+// (pressure_backend_fftw.f90:22-93, pressure_backend_cufft.f90:29-122).
+//
+// Data flow per projection (HBM passes):
+//   k_div_fftx   us,vs,ws -> spec        divergence/dt_gamma of one x row
+//                                        (build_fft_rhs) and its real FFT in
+//                                        shared memory
+//   k_fftz<fwd>  spec -> spec            complex FFT along z per (kx, y)
+//   k_thomas     spec -> spec            tridiagonal solve along y per mode
+//   k_fftz<inv>  spec -> spec
+//   k_ifftx      spec -> phi             inverse real FFT of one row, *1/(nx nz)
+//   k_correct    us,vs,ws,phi,pn -> un,vn,wn,pn
+//
+// The FFTs are shared-memory Stockham transforms (the formulation of
+// Govindaraju et al., "High performance discrete Fourier transforms on
+// graphics processors", SC 2008) with radices 4, 2, 3, 5, 7; the real
+// transform of length nx is a complex transform of length nx/2 on packed
+// even/odd samples plus the standard split step.  Twiddles are tables built
+// on the host with long-double cosl/sinl.
+//
+// Parity: the divergence, Thomas and correction arithmetic follow the
+// reference order with -fmad=false; the FFT differs from FFTW in operation
+// order only, so FFT-path fields agree to rounding.
+#include "mdx_internal.cuh"
+
+#include <cmath>
+
+// ---------------------------------------------------------------------------
+// Plans and twiddles (host)
+// ---------------------------------------------------------------------------
+void mdx_fft_make_plan(int n, mdx_fft_plan* p, bool* ok) {
+    p->n = n;
+    p->nstages = 0;
+    int m = n;
+    *ok = true;
+    for (int r : {4, 2, 3, 5, 7}) {
+        while (m % r == 0) {
+            if (p->nstages >= MDX_MAX_STAGES) { *ok = false; return; }
+            p->radix[p->nstages++] = r;
+            m /= r;
+        }
+    }
+    if (m != 1) *ok = false;
+    // one radix-2 stage is cheaper at the end than between radix-4 stages
+    // only in bank terms; keep the order 4..4,2,3,5,7.
+}
+
+void mdx_fft_twiddles(int n, std::vector<double2>& tw) {
+    tw.resize(n);
+    const long double two_pi = 6.283185307179586476925286766559005768L;
+    for (int t = 0; t < n; ++t) {
+        const long double a = two_pi * (long double)t / (long double)n;
+        tw[t] = make_double2((double)cosl(a), (double)(-sinl(a)));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Device complex helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+// a * (-i) and a * (+i)
+__device__ __forceinline__ double2 cmul_mi(double2 a) { return make_double2(a.y, -a.x); }
+__device__ __forceinline__ double2 cmul_pi(double2 a) { return make_double2(-a.y, a.x); }
+
+// Twiddle exp(-+2 pi i t / n) from the forward table (conjugated for INV).
+template <bool INV>
+__device__ __forceinline__ double2 twid(const double2* __restrict__ tw, int t) {
+    double2 w = __ldg(tw + t);
+    if (INV) w.y = -w.y;
+    return w;
+}
+
+// Radix-r DFT in registers.  For r = 3, 5, 7 the roots come from the table:
+// W_r^m = tw[m * (n/r) * tws].
+template <bool INV>
+__device__ __forceinline__ void dft_r(double2* a, int r, const double2* __restrict__ tw, int root_step) {
+    if (r == 2) {
+        const double2 x0 = a[0], x1 = a[1];
+        a[0] = cadd(x0, x1);
+        a[1] = csub(x0, x1);
+    } else if (r == 4) {
+        const double2 x0 = a[0], x1 = a[1], x2 = a[2], x3 = a[3];
+        const double2 s02 = cadd(x0, x2), d02 = csub(x0, x2);
+        const double2 s13 = cadd(x1, x3), d13 = csub(x1, x3);
+        const double2 rd13 = INV ? cmul_pi(d13) : cmul_mi(d13);
+        a[0] = cadd(s02, s13);
+        a[1] = cadd(d02, rd13);
+        a[2] = csub(s02, s13);
+        a[3] = csub(d02, rd13);
+    } else {
+        double2 b[7];
+        for (int p = 0; p < r; ++p) {
+            double2 acc = a[0];
+            for (int q = 1; q < r; ++q) acc = cadd(acc, cmul(a[q], twid<INV>(tw, ((p * q) % r) * root_step)));
+            b[p] = acc;
+        }
+        for (int p = 0; p < r; ++p) a[p] = b[p];
+    }
+}
+
+// In-place (ping-pong) Stockham FFT of `nlines` lines of length n held in
+// shared memory at A[line*ls + t]; all threads of the block participate.
+// `tw` is a table of exp(-2 pi i t / N) with N = n * tws.  Returns the
+// buffer holding the result (A or B).
+template <bool INV>
+__device__ double2* smem_fft(double2* A, double2* B, int n, int nlines, int ls, const mdx_fft_plan& pl,
+                             const double2* __restrict__ tw, int tws) {
+    int Ns = 1;
+    for (int s = 0; s < pl.nstages; ++s) {
+        const int r = pl.radix[s];
+        const int nr = n / r;
+        const int total = nlines * nr;
+        const int tstep = (n / (Ns * r)) * tws;
+        const int root_step = nr * tws;
+        for (int t = threadIdx.x; t < total; t += blockDim.x) {
+            const int line = t / nr;
+            const int jb = t - line * nr;
+            const int k = jb % Ns;
+            const double2* src = A + line * ls;
+            double2 a[7];
+            for (int q = 0; q < r; ++q) a[q] = src[jb + q * nr];
+            if (Ns > 1)
+                for (int q = 1; q < r; ++q) a[q] = cmul(a[q], twid<INV>(tw, q * k * tstep));
+            dft_r<INV>(a, r, tw, root_step);
+            double2* dst = B + line * ls;
+            const int base = (jb / Ns) * Ns * r + k;
+            for (int p = 0; p < r; ++p) dst[base + p * Ns] = a[p];
+        }
+        __syncthreads();
+        double2* t = A; A = B; B = t;
+        Ns *= r;
+    }
+    return A;
+}
+
+// ---------------------------------------------------------------------------
+// Divergence (build_fft_rhs, pressure_solver.f90:102-111) + forward real FFT
+// along x of each (k, j) row.  Rows are numbered r = (k-1) + nz*(j-1), the
+// order of plane_hat(nxh, nz, ny).  R rows per block, M = nx/2.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+k_div_fftx(mdx_dims d, int R, double dx, double dy, double dz, double dt_gamma, const double* __restrict__ us,
+           const double* __restrict__ vs, const double* __restrict__ ws, double2* __restrict__ spec,
+           mdx_fft_plan pl, const double2* __restrict__ twx) {
+    extern __shared__ double2 sm[];
+    const int M = d.nx / 2;
+    double2* A = sm;
+    double2* B = sm + R * M;
+    const int nrows = d.nz * d.ny;
+    const int row0 = blockIdx.x * R;
+    for (int t = threadIdx.x; t < R * M; t += blockDim.x) {
+        const int rl = t / M, n = t - rl * M;
+        const int row = row0 + rl;
+        double2 z = make_double2(0.0, 0.0);
+        if (row < nrows) {
+            const int k = row % d.nz + 1, j = row / d.nz + 1;
+            double x[2];
+            for (int e = 0; e < 2; ++e) {
+                const int i = 2 * n + 1 + e;
+                const long long c = pidx(d, i, j, k);
+                x[e] = ((__ldg(us + c + 1) - __ldg(us + c)) / dx + (__ldg(vs + c + d.nxp) - __ldg(vs + c)) / dy +
+                        (__ldg(ws + c + (long long)d.nxp * d.nyp) - __ldg(ws + c)) / dz) / dt_gamma;
+            }
+            z = make_double2(x[0], x[1]);
+        }
+        A[rl * M + n] = z;
+    }
+    __syncthreads();
+    double2* Z = smem_fft<false>(A, B, M, R, M, pl, twx, 2);
+    // split step: X_k = E_k + W^k O_k, E = (Z_k + conj Z_{M-k})/2, O = -i/2 (Z_k - conj Z_{M-k})
+    const int nxh = M + 1;
+    for (int t = threadIdx.x; t < R * nxh; t += blockDim.x) {
+        const int rl = t / nxh, kx = t - rl * nxh;
+        const int row = row0 + rl;
+        if (row >= nrows) continue;
+        const double2 zk = Z[rl * M + (kx == M ? 0 : kx)];
+        const double2 zc = cconj(Z[rl * M + (kx == 0 ? 0 : M - kx)]);
+        const double2 e = make_double2(0.5 * (zk.x + zc.x), 0.5 * (zk.y + zc.y));
+        const double2 o = cmul_mi(make_double2(0.5 * (zk.x - zc.x), 0.5 * (zk.y - zc.y)));
+        const double2 X = cadd(e, cmul(__ldg(twx + kx), o));
+        spec[(long long)row * nxh + kx] = X;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Complex FFT along z of spec(kx, :, j) for a tile of TX kx values per block.
+// ---------------------------------------------------------------------------
+template <bool INV>
+__global__ void __launch_bounds__(256)
+k_fftz(mdx_dims d, int TX, double2* __restrict__ spec, mdx_fft_plan pl, const double2* __restrict__ twz) {
+    extern __shared__ double2 sm[];
+    const int nz = d.nz, nxh = d.nxh, ls = nz + 1;
+    double2* A = sm;
+    double2* B = sm + TX * ls;
+    const int ntiles = (nxh + TX - 1) / TX;
+    const int j = blockIdx.x / ntiles;
+    const int kx0 = (blockIdx.x - j * ntiles) * TX;
+    double2* base = spec + (long long)j * nz * nxh;
+    for (int t = threadIdx.x; t < TX * nz; t += blockDim.x) {
+        const int c = t % TX, kz = t / TX;
+        const int kx = kx0 + c;
+        A[c * ls + kz] = (kx < nxh) ? base[(long long)kz * nxh + kx] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    double2* Z = smem_fft<INV>(A, B, nz, TX, ls, pl, twz, 1);
+    for (int t = threadIdx.x; t < TX * nz; t += blockDim.x) {
+        const int c = t % TX, kz = t / TX;
+        const int kx = kx0 + c;
+        if (kx < nxh) base[(long long)kz * nxh + kx] = Z[c * ls + kz];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Thomas tables, init_tridiag_coefficients (pressure_fft.f90:46-94): for each
+// (kx, kz <= nz/2) the reciprocal pivots dinv_j and c'_j.  kz and nz-kz have
+// bitwise-equal modified wavenumbers (sin is odd), so one table serves both.
+// ---------------------------------------------------------------------------
+__global__ void k_thomas_tables(int nxh, int nzh, int ny, double dyi2, const double* __restrict__ kxp,
+                                const double* __restrict__ kzp, double* __restrict__ dinv, double* __restrict__ cp) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= nxh * nzh) return;
+    const int kx = m % nxh, kz = m / nxh;
+    const long long plane = (long long)nxh * nzh;
+    const double k_tot = kxp[kx] + kzp[kz];
+    double cprev;
+    if (kx == 0 && kz == 0) {
+        dinv[m] = 1.0;
+        cp[m] = 0.0;
+        cprev = 0.0;
+    } else {
+        const double b = -dyi2 - k_tot, c = dyi2;
+        const double di = 1.0 / b;
+        dinv[m] = di;
+        cprev = c * di;
+        cp[m] = cprev;
+    }
+    const double a = dyi2;
+    for (int jj = 2; jj <= ny; ++jj) {
+        double b, c;
+        if (jj < ny) { b = -2.0 * dyi2 - k_tot; c = dyi2; }
+        else { b = -dyi2 - k_tot; c = 0.0; }
+        const double denom = b - a * cprev;
+        const double di = 1.0 / denom;
+        const double cc = (jj < ny) ? c * di : 0.0;
+        dinv[(jj - 1) * plane + m] = di;
+        cp[(jj - 1) * plane + m] = cc;
+        cprev = cc;
+    }
+}
+
+// solve_tridiagonal_y, pressure_fft.f90:102-148: one thread per (kx, kz);
+// the forward sweep stores dp in place, the back substitution overwrites it
+// with the solution.
+__global__ void __launch_bounds__(128)
+k_thomas(mdx_dims d, double dyi2, double2* __restrict__ spec, const double* __restrict__ dinv,
+         const double* __restrict__ cp) {
+    const int nxh = d.nxh, nz = d.nz, ny = d.ny, nzh = d.nz / 2 + 1;
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= nxh * nz) return;
+    const int kx = m % nxh, kz = m / nxh;
+    const int kzt = (kz <= nz / 2) ? kz : nz - kz;
+    const int mt = kx + nxh * kzt;
+    const long long tplane = (long long)nxh * nzh;
+    const long long splane = (long long)nxh * nz;
+    double2* col = spec + m;
+    const double a = dyi2;
+    double2 dp;
+    if (kx == 0 && kz == 0) {
+        dp = make_double2(0.0, 0.0);
+    } else {
+        const double2 r = col[0];
+        const double di = __ldg(dinv + mt);
+        dp = make_double2(r.x * di, r.y * di);
+    }
+    col[0] = dp;
+    for (int jj = 2; jj <= ny; ++jj) {
+        const double2 r = col[(jj - 1) * splane];
+        const double di = __ldg(dinv + (jj - 1) * tplane + mt);
+        dp = make_double2((r.x - a * dp.x) * di, (r.y - a * dp.y) * di);
+        col[(jj - 1) * splane] = dp;
+    }
+    double2 nxt = dp;  // plane_hat(ny) = dp(ny)
+    for (int jj = ny - 1; jj >= 1; --jj) {
+        const double2 dj = col[(jj - 1) * splane];
+        const double c = __ldg(cp + (jj - 1) * tplane + mt);
+        nxt = make_double2(dj.x - c * nxt.x, dj.y - c * nxt.y);
+        col[(jj - 1) * splane] = nxt;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Inverse real FFT along x of each row (c2r contract: imaginary parts of the
+// kx = 0 and kx = nx/2 bins are ignored), scaled by 1/(nx*nz) as
+// scale_pressure_correction_* (pressure_backend_fftw.f90:80-93).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+k_ifftx(mdx_dims d, int R, double scale, const double2* __restrict__ spec, double* __restrict__ phi,
+        mdx_fft_plan pl, const double2* __restrict__ twx) {
+    extern __shared__ double2 sm[];
+    const int M = d.nx / 2, nxh = M + 1;
+    double2* A = sm;
+    double2* B = sm + R * M;
+    const int nrows = d.nz * d.ny;
+    const int row0 = blockIdx.x * R;
+    // Z'_k = (X_k + conj X_{M-k}) + i W^{-k} (X_k - conj X_{M-k}),  k < M
+    for (int t = threadIdx.x; t < R * M; t += blockDim.x) {
+        const int rl = t / M, k = t - rl * M;
+        const int row = row0 + rl;
+        double2 z = make_double2(0.0, 0.0);
+        if (row < nrows) {
+            const double2* X = spec + (long long)row * nxh;
+            double2 xk = X[k], xm = X[M - k];
+            if (k == 0) { xk.y = 0.0; xm.y = 0.0; }   // kx = 0 and kx = M bins are real
+            const double2 xc = cconj(xm);
+            const double2 e = cadd(xk, xc);
+            const double2 o = cmul(csub(xk, xc), cconj(__ldg(twx + k)));
+            z = cadd(e, cmul_pi(o));
+        }
+        A[rl * M + k] = z;
+    }
+    __syncthreads();
+    double2* Z = smem_fft<true>(A, B, M, R, M, pl, twx, 2);
+    for (int t = threadIdx.x; t < R * M; t += blockDim.x) {
+        const int rl = t / M, n = t - rl * M;
+        const int row = row0 + rl;
+        if (row >= nrows) continue;
+        const double2 z = Z[rl * M + n];
+        double* out = phi + (long long)row * d.nx;
+        out[2 * n] = z.x * scale;
+        out[2 * n + 1] = z.y * scale;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// apply_fft_pressure_correction, pressure_solver.f90:150-169.
+// ---------------------------------------------------------------------------
+template <bool IBM>
+__global__ void __launch_bounds__(256)
+k_correct(mdx_dims d, double dx, double dy, double dz, double dt_gamma, const double* __restrict__ phi,
+          const double* __restrict__ us, const double* __restrict__ vs, const double* __restrict__ ws,
+          double* __restrict__ un, double* __restrict__ vn, double* __restrict__ wn, double* __restrict__ pn,
+          const double* __restrict__ cu, const double* __restrict__ cv, const double* __restrict__ cw) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
+    if (i > d.nx || j > d.ny || k > d.nz) return;
+    int im = i - 1, km = k - 1;
+    if (im < 1) im = d.nx;
+    if (km < 1) km = d.nz;
+    const long long c = pidx(d, i, j, k);
+    const double r = __ldg(phi + ridx(d, i, k, j));
+    double u = (__ldg(us + c) - dt_gamma * (r - __ldg(phi + ridx(d, im, k, j))) / dx);
+    double w = (__ldg(ws + c) - dt_gamma * (r - __ldg(phi + ridx(d, i, km, j))) / dz);
+    if (IBM) {
+        u = u / (1.0 + dt_gamma * __ldg(cu + c));
+        w = w / (1.0 + dt_gamma * __ldg(cw + c));
+    } else {
+        u = u / 1.0;
+        w = w / 1.0;
+    }
+    un[c] = u;
+    wn[c] = w;
+    pn[c] = pn[c] + r;
+    if (j >= 2) {
+        double v = (__ldg(vs + c) - dt_gamma * (r - __ldg(phi + ridx(d, i, k, j - 1))) / dy);
+        if (IBM) v = v / (1.0 + dt_gamma * __ldg(cv + c));
+        vn[c] = v;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+static int rows_per_block(int M) { return M >= 1024 ? 1 : 1024 / M; }
+static int ztile(int nz) {
+    int tx = 2048 / (nz + 1);
+    if (tx > 32) tx = 32;
+    if (tx < 1) tx = 1;
+    return tx;
+}
+
+int mdx_fft_init(mdx_ctx_t* ctx) {
+    const mdx_dims& d = ctx->d;
+    if (d.nx % 2 != 0)
+        return mdx_fail(ctx, MDX_ERR_ARG, "FFT solver: nx must be even (nx=%d)", d.nx);
+    bool ok1 = false, ok2 = false;
+    mdx_fft_make_plan(d.nx / 2, &ctx->plan_xh, &ok1);
+    mdx_fft_make_plan(d.nz, &ctx->plan_z, &ok2);
+    if (!ok1 || !ok2)
+        return mdx_fail(ctx, MDX_ERR_ARG, "FFT solver: nx/2=%d and nz=%d must factor into 2,3,5,7", d.nx / 2, d.nz);
+    if (d.nx / 2 > 4096 || d.nz > 4096)
+        return mdx_fail(ctx, MDX_ERR_ARG, "FFT solver: nx/2 and nz must be <= 4096");
+    std::vector<double2> tx, tz;
+    mdx_fft_twiddles(d.nx, tx);
+    mdx_fft_twiddles(d.nz, tz);
+    MDX_CUDA(ctx, cudaMalloc(&ctx->tw_x, sizeof(double2) * d.nx));
+    MDX_CUDA(ctx, cudaMalloc(&ctx->tw_z, sizeof(double2) * d.nz));
+    MDX_CUDA(ctx, cudaMemcpy(ctx->tw_x, tx.data(), sizeof(double2) * d.nx, cudaMemcpyHostToDevice));
+    MDX_CUDA(ctx, cudaMemcpy(ctx->tw_z, tz.data(), sizeof(double2) * d.nz, cudaMemcpyHostToDevice));
+    MDX_CUDA(ctx, cudaMalloc(&ctx->spec, sizeof(double2) * d.nspec));
+    if (!ctx->f[MDX_PHI]) {
+        MDX_CUDA(ctx, cudaMalloc(&ctx->f[MDX_PHI], sizeof(double) * d.nint));
+        MDX_CUDA(ctx, cudaMemset(ctx->f[MDX_PHI], 0, sizeof(double) * d.nint));
+    }
+
+    // Modified wavenumbers on the host with libm sin, pressure_fft.f90:53,61.
+    const double pi = 3.141592653589793;
+    const int nzh = d.nz / 2 + 1;
+    std::vector<double> kxp(d.nxh), kzp(d.nz);
+    for (int ikx = 1; ikx <= d.nxh; ++ikx) {
+        const int kx = ikx - 1;
+        const double s = std::sin(pi * (double)kx / (double)d.nx);
+        kxp[ikx - 1] = (4.0 / (ctx->g.dx * ctx->g.dx)) * (s * s);
+    }
+    for (int ikz = 1; ikz <= d.nz; ++ikz) {
+        const int kz = (ikz <= d.nz / 2 + 1) ? ikz - 1 : ikz - d.nz - 1;
+        const double s = std::sin(pi * (double)kz / (double)d.nz);
+        kzp[ikz - 1] = (4.0 / (ctx->g.dz * ctx->g.dz)) * (s * s);
+    }
+    double *dkx = nullptr, *dkz = nullptr;
+    MDX_CUDA(ctx, cudaMalloc(&dkx, sizeof(double) * d.nxh));
+    MDX_CUDA(ctx, cudaMalloc(&dkz, sizeof(double) * d.nz));
+    MDX_CUDA(ctx, cudaMemcpy(dkx, kxp.data(), sizeof(double) * d.nxh, cudaMemcpyHostToDevice));
+    MDX_CUDA(ctx, cudaMemcpy(dkz, kzp.data(), sizeof(double) * d.nz, cudaMemcpyHostToDevice));
+    const long long tsize = (long long)d.ny * d.nxh * nzh;
+    MDX_CUDA(ctx, cudaMalloc(&ctx->thomas_dinv, sizeof(double) * tsize));
+    MDX_CUDA(ctx, cudaMalloc(&ctx->thomas_cp, sizeof(double) * tsize));
+    const double dyi2 = 1.0 / (ctx->g.dy * ctx->g.dy);
+    const int nm = d.nxh * nzh;
+    k_thomas_tables<<<(nm + 127) / 128, 128, 0, ctx->stream>>>(d.nxh, nzh, d.ny, dyi2, dkx, dkz, ctx->thomas_dinv,
+                                                              ctx->thomas_cp);
+    int rc = mdx_check_launch(ctx, "thomas tables");
+    MDX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    cudaFree(dkx);
+    cudaFree(dkz);
+    if (rc != MDX_OK) return rc;
+
+    const int M = d.nx / 2;
+    const size_t smx = sizeof(double2) * 2 * rows_per_block(M) * M;
+    const size_t smz = sizeof(double2) * 2 * ztile(d.nz) * (d.nz + 1);
+    MDX_CUDA(ctx, cudaFuncSetAttribute(k_div_fftx, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx));
+    MDX_CUDA(ctx, cudaFuncSetAttribute(k_ifftx, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx));
+    MDX_CUDA(ctx, cudaFuncSetAttribute(k_fftz<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz));
+    MDX_CUDA(ctx, cudaFuncSetAttribute(k_fftz<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz));
+    return MDX_OK;
+}
+
+void mdx_fft_free(mdx_ctx_t* ctx) {
+    cudaFree(ctx->spec); ctx->spec = nullptr;
+    cudaFree(ctx->tw_x); ctx->tw_x = nullptr;
+    cudaFree(ctx->tw_z); ctx->tw_z = nullptr;
+    cudaFree(ctx->thomas_dinv); ctx->thomas_dinv = nullptr;
+    cudaFree(ctx->thomas_cp); ctx->thomas_cp = nullptr;
+}
+
+// pressure_projection of the FFT builds, pressure_solver.f90:58-61.
+int mdx_k_projection_fft(mdx_ctx_t* ctx, double dg) {
+    const mdx_dims& d = ctx->d;
+    const mdx_grid_t& g = ctx->g;
+    double** f = ctx->f;
+    const int M = d.nx / 2;
+    const int R = rows_per_block(M);
+    const int nrows = d.nz * d.ny;
+    const size_t smx = sizeof(double2) * 2 * R * M;
+    const int xblocks = (nrows + R - 1) / R;
+    MDX_LAUNCH(ctx, MDX_T_FFT_FWD, "div+fft x", k_div_fftx, xblocks, 256, smx, d, R, g.dx, g.dy, g.dz, dg, f[MDX_US],
+               f[MDX_VS], f[MDX_WS], ctx->spec, ctx->plan_xh, ctx->tw_x);
+    const int TX = ztile(d.nz);
+    const size_t smz = sizeof(double2) * 2 * TX * (d.nz + 1);
+    const int zblocks = ((d.nxh + TX - 1) / TX) * d.ny;
+    MDX_LAUNCH(ctx, MDX_T_FFT_FWD, "fft z", k_fftz<false>, zblocks, 256, smz, d, TX, ctx->spec, ctx->plan_z, ctx->tw_z);
+    const int nm = d.nxh * d.nz;
+    MDX_LAUNCH(ctx, MDX_T_THOMAS, "thomas", k_thomas, (nm + 127) / 128, 128, 0, d, 1.0 / (g.dy * g.dy), ctx->spec,
+               ctx->thomas_dinv, ctx->thomas_cp);
+    MDX_LAUNCH(ctx, MDX_T_FFT_INV, "ifft z", k_fftz<true>, zblocks, 256, smz, d, TX, ctx->spec, ctx->plan_z, ctx->tw_z);
+    const double scale = 1.0 / (double)(d.nx * d.nz);
+    MDX_LAUNCH(ctx, MDX_T_FFT_INV, "ifft x", k_ifftx, xblocks, 256, smx, d, R, scale, ctx->spec, f[MDX_PHI],
+               ctx->plan_xh, ctx->tw_x);
+    dim3 block(32, 4, 2);
+    dim3 grid((d.nx + 31) / 32, (d.ny + 3) / 4, (d.nz + 1) / 2);
+    if (ctx->ibm_zero)
+        MDX_LAUNCH(ctx, MDX_T_CORRECT, "correction", k_correct<false>, grid, block, 0, d, g.dx, g.dy, g.dz, dg,
+                   f[MDX_PHI], f[MDX_US], f[MDX_VS], f[MDX_WS], f[MDX_UN], f[MDX_VN], f[MDX_WN], f[MDX_PN],
+                   f[MDX_COEF_U], f[MDX_COEF_V], f[MDX_COEF_W]);
+    else
+        MDX_LAUNCH(ctx, MDX_T_CORRECT, "correction", k_correct<true>, grid, block, 0, d, g.dx, g.dy, g.dz, dg,
+                   f[MDX_PHI], f[MDX_US], f[MDX_VS], f[MDX_WS], f[MDX_UN], f[MDX_VN], f[MDX_WN], f[MDX_PN],
+                   f[MDX_COEF_U], f[MDX_COEF_V], f[MDX_COEF_W]);
+    return MDX_OK;
+}

@@ -1,0 +1,598 @@
+// k_step.cu -- predictor (momentum), ghost-cell boundary conditions, CFL,
+// cell-centre velocities and the seeded initial condition.
+//
+// Parity: this file is compiled with -fmad=false and every expression keeps
+// the reference's Fortran evaluation order, so the predictor and the
+// boundary conditions are bit-for-bit the reference arithmetic (x86-64
+// gfortran -O2 has no FMA contraction).  Skipping the IBM factor when all
+// coefficients are zero is exact: 1/(1+dt_gamma*0) == 1.
+#include "mdx_internal.cuh"
+
+// ---------------------------------------------------------------------------
+// Predictor, src/modules/step.f90:76-204.  One thread per cell, x fastest so
+// each warp reads 32 consecutive doubles of every array; the stencil
+// neighbours come from L1/L2.
+// ---------------------------------------------------------------------------
+template <bool IBM>
+__global__ void __launch_bounds__(256)
+k_momentum(mdx_dims d, mdx_step_params p, double dt_alpha, double dt_beta, double dt_gamma,
+           const double* __restrict__ un, const double* __restrict__ vn, const double* __restrict__ wn,
+           const double* __restrict__ pn, double* __restrict__ us, double* __restrict__ vs,
+           double* __restrict__ ws, double* __restrict__ ou, double* __restrict__ ov, double* __restrict__ ow,
+           const double* __restrict__ cu, const double* __restrict__ cv, const double* __restrict__ cw) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
+    if (i > d.nx || j > d.ny || k > d.nz) return;
+    const long long SX = 1, SY = d.nxp, SZ = (long long)d.nxp * d.nyp;
+    const long long c = pidx(d, i, j, k);
+    const long long q = qidx(d, i, j, k);
+    const double idx = p.idx, idy = p.idy, idz = p.idz, idx2 = p.idx2, idy2 = p.idy2, idz2 = p.idz2, ire = p.ire;
+
+    const double u_c = __ldg(un + c), v_c = __ldg(vn + c), w_c = __ldg(wn + c), p_c = __ldg(pn + c);
+
+    if (i >= p.nx0) {  // step.f90:106-136
+        const double u_ip = __ldg(un + c + SX), u_im = __ldg(un + c - SX);
+        const double u_jp = __ldg(un + c + SY), u_jm = __ldg(un + c - SY);
+        const double u_kp = __ldg(un + c + SZ), u_km = __ldg(un + c - SZ);
+        double s;
+        s = u_ip + u_c;
+        const double uu_p = 0.25 * (s * s);
+        s = u_c + u_im;
+        const double uu_m = 0.25 * (s * s);
+        const double uv_p = 0.25 * (u_jp + u_c) * (__ldg(vn + c + SY) + __ldg(vn + c - SX + SY));
+        const double uv_m = 0.25 * (u_c + u_jm) * (v_c + __ldg(vn + c - SX));
+        const double uw_p = 0.25 * (u_c + u_kp) * (__ldg(wn + c + SZ) + __ldg(wn + c - SX + SZ));
+        const double uw_m = 0.25 * (u_c + u_km) * (w_c + __ldg(wn + c - SX));
+        const double diff_ux = (u_im - 2.0 * u_c + u_ip) * idx2;
+        const double diff_uy = (u_jm - 2.0 * u_c + u_jp) * idy2;
+        const double diff_uz = (u_km - 2.0 * u_c + u_kp) * idz2;
+        const double dpx = (p_c - __ldg(pn + c - SX)) * idx;
+        const double rhsu = -((uu_p - uu_m) * idx) - (uv_p - uv_m) * idy - (uw_p - uw_m) * idz + p.fx +
+                            ire * (diff_ux + diff_uy + diff_uz);
+        double val = u_c + dt_alpha * rhsu + dt_beta * ou[q] - dt_gamma * dpx;
+        if (IBM) val = val * (1.0 / (1.0 + dt_gamma * __ldg(cu + c)));
+        us[c] = val;
+        ou[q] = rhsu;
+    }
+    if (j >= p.ny0) {  // step.f90:138-168
+        const double v_ip = __ldg(vn + c + SX), v_im = __ldg(vn + c - SX);
+        const double v_jp = __ldg(vn + c + SY), v_jm = __ldg(vn + c - SY);
+        const double v_kp = __ldg(vn + c + SZ), v_km = __ldg(vn + c - SZ);
+        double s;
+        const double vu_p = 0.25 * (v_c + v_ip) * (__ldg(un + c + SX) + __ldg(un + c + SX - SY));
+        const double vu_m = 0.25 * (v_c + v_im) * (u_c + __ldg(un + c - SY));
+        s = v_c + v_jp;
+        const double vv_p = 0.25 * (s * s);
+        s = v_c + v_jm;
+        const double vv_m = 0.25 * (s * s);
+        const double vw_p = 0.25 * (v_kp + v_c) * (__ldg(wn + c + SZ) + __ldg(wn + c - SY + SZ));
+        const double vw_m = 0.25 * (v_km + v_c) * (w_c + __ldg(wn + c - SY));
+        const double diff_vx = (v_im - 2.0 * v_c + v_ip) * idx2;
+        const double diff_vy = (v_jm - 2.0 * v_c + v_jp) * idy2;
+        const double diff_vz = (v_km - 2.0 * v_c + v_kp) * idz2;
+        const double dpy = (p_c - __ldg(pn + c - SY)) * idy;
+        const double rhsv = -((vu_p - vu_m) * idx) - (vv_p - vv_m) * idy - (vw_p - vw_m) * idz + p.fy +
+                            ire * (diff_vx + diff_vy + diff_vz);
+        double val = v_c + dt_alpha * rhsv + dt_beta * ov[q] - dt_gamma * dpy;
+        if (IBM) val = val * (1.0 / (1.0 + dt_gamma * __ldg(cv + c)));
+        vs[c] = val;
+        ov[q] = rhsv;
+    }
+    if (k >= p.nz0) {  // step.f90:170-200
+        const double w_ip = __ldg(wn + c + SX), w_im = __ldg(wn + c - SX);
+        const double w_jp = __ldg(wn + c + SY), w_jm = __ldg(wn + c - SY);
+        const double w_kp = __ldg(wn + c + SZ), w_km = __ldg(wn + c - SZ);
+        double s;
+        const double wu_p = 0.25 * (w_c + w_ip) * (__ldg(un + c + SX) + __ldg(un + c + SX - SZ));
+        const double wu_m = 0.25 * (w_c + w_im) * (u_c + __ldg(un + c - SZ));
+        s = w_c + w_kp;
+        const double ww_p = 0.25 * (s * s);
+        s = w_c + w_km;
+        const double ww_m = 0.25 * (s * s);
+        const double wv_p = 0.25 * (w_c + w_jp) * (__ldg(vn + c + SY) + __ldg(vn + c + SY - SZ));
+        const double wv_m = 0.25 * (w_c + w_jm) * (v_c + __ldg(vn + c - SZ));
+        const double diff_wx = (w_im - 2.0 * w_c + w_ip) * idx2;
+        const double diff_wy = (w_jm - 2.0 * w_c + w_jp) * idy2;
+        const double diff_wz = (w_km - 2.0 * w_c + w_kp) * idz2;
+        const double dpz = (p_c - __ldg(pn + c - SZ)) * idz;
+        const double rhsw = -((wu_p - wu_m) * idx) - (wv_p - wv_m) * idy - (ww_p - ww_m) * idz + p.fz +
+                            ire * (diff_wx + diff_wy + diff_wz);
+        double val = w_c + dt_alpha * rhsw + dt_beta * ow[q] - dt_gamma * dpz;
+        if (IBM) val = val * (1.0 / (1.0 + dt_gamma * __ldg(cw + c)));
+        ws[c] = val;
+        ow[q] = rhsw;
+    }
+}
+
+mdx_step_params mdx_make_params(const mdx_ctx_t* ctx) {
+    const mdx_grid_t& g = ctx->g;
+    mdx_step_params p;
+    p.dx = g.dx; p.dy = g.dy; p.dz = g.dz;
+    const double dx2 = g.dx * g.dx, dy2 = g.dy * g.dy, dz2 = g.dz * g.dz;  // step.f90:57-67
+    p.idx = 1.0 / g.dx; p.idy = 1.0 / g.dy; p.idz = 1.0 / g.dz;
+    p.idx2 = 1.0 / dx2; p.idy2 = 1.0 / dy2; p.idz2 = 1.0 / dz2;
+    p.ire = 1.0 / g.re;
+    p.fx = g.forcing_x; p.fy = g.forcing_y; p.fz = g.forcing_z;
+    p.nx0 = ctx->bc.is_periodic[0] ? 1 : 2;   // step.f90:71-73
+    p.ny0 = ctx->bc.is_periodic[1] ? 1 : 2;
+    p.nz0 = ctx->bc.is_periodic[2] ? 1 : 2;
+    return p;
+}
+
+int mdx_k_momentum(mdx_ctx_t* ctx, double da, double db, double dg) {
+    const mdx_dims& d = ctx->d;
+    dim3 block(32, 4, 2);
+    dim3 grid((d.nx + 31) / 32, (d.ny + 3) / 4, (d.nz + 1) / 2);
+    mdx_step_params p = mdx_make_params(ctx);
+    double** f = ctx->f;
+    if (ctx->ibm_zero)
+        MDX_LAUNCH(ctx, MDX_T_MOMENTUM, "momentum", k_momentum<false>, grid, block, 0, d, p, da, db, dg,
+                   f[MDX_UN], f[MDX_VN], f[MDX_WN], f[MDX_PN], f[MDX_US], f[MDX_VS], f[MDX_WS], f[MDX_OLDRHSU],
+                   f[MDX_OLDRHSV], f[MDX_OLDRHSW], f[MDX_COEF_U], f[MDX_COEF_V], f[MDX_COEF_W]);
+    else
+        MDX_LAUNCH(ctx, MDX_T_MOMENTUM, "momentum", k_momentum<true>, grid, block, 0, d, p, da, db, dg,
+                   f[MDX_UN], f[MDX_VN], f[MDX_WN], f[MDX_PN], f[MDX_US], f[MDX_VS], f[MDX_WS], f[MDX_OLDRHSU],
+                   f[MDX_OLDRHSV], f[MDX_OLDRHSW], f[MDX_COEF_U], f[MDX_COEF_V], f[MDX_COEF_W]);
+    return MDX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// apply_bc of the FFT builds, src/modules/boundary.f90:23-170, as the
+// reference's three sequential phases (y walls, x periodic, z periodic).
+// Each phase writes only ghost planes (plus the v wall row) and reads
+// interior or already-final values, so threads within a phase never race.
+// ---------------------------------------------------------------------------
+struct mdx_six { double *un, *vn, *wn, *us, *vs, *ws, *pn; };
+
+__global__ void k_bc_walls_y(mdx_dims d, mdx_six f) {   // boundary.f90:48-67
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i > d.nx + 1 || k > d.nz + 1) return;
+    const int ny = d.ny;
+    f.un[pidx(d, i, ny + 1, k)] = -f.un[pidx(d, i, ny, k)];
+    f.vn[pidx(d, i, ny + 1, k)] = 0.0;
+    f.wn[pidx(d, i, ny + 1, k)] = -f.wn[pidx(d, i, ny, k)];
+    f.un[pidx(d, i, 0, k)] = -f.un[pidx(d, i, 1, k)];
+    f.vn[pidx(d, i, 1, k)] = 0.0;
+    f.wn[pidx(d, i, 0, k)] = -f.wn[pidx(d, i, 1, k)];
+    f.us[pidx(d, i, ny + 1, k)] = -f.us[pidx(d, i, ny, k)];
+    f.vs[pidx(d, i, ny + 1, k)] = 0.0;
+    f.ws[pidx(d, i, ny + 1, k)] = -f.ws[pidx(d, i, ny, k)];
+    f.us[pidx(d, i, 0, k)] = -f.us[pidx(d, i, 1, k)];
+    f.vs[pidx(d, i, 1, k)] = 0.0;
+    f.ws[pidx(d, i, 0, k)] = -f.ws[pidx(d, i, 1, k)];
+}
+
+__global__ void k_bc_periodic_x(mdx_dims d, mdx_six f) {   // boundary.f90:87-117
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = blockIdx.y * blockDim.y + threadIdx.y;
+    if (j > d.ny + 1 || k > d.nz + 1) return;
+    const int nx = d.nx;
+    f.un[pidx(d, 0, j, k)] = f.un[pidx(d, nx, j, k)];
+    f.wn[pidx(d, 0, j, k)] = f.wn[pidx(d, nx, j, k)];
+    f.un[pidx(d, nx + 1, j, k)] = f.un[pidx(d, 1, j, k)];
+    f.wn[pidx(d, nx + 1, j, k)] = f.wn[pidx(d, 1, j, k)];
+    f.us[pidx(d, 0, j, k)] = f.us[pidx(d, nx, j, k)];
+    f.ws[pidx(d, 0, j, k)] = f.ws[pidx(d, nx, j, k)];
+    f.us[pidx(d, nx + 1, j, k)] = f.us[pidx(d, 1, j, k)];
+    f.ws[pidx(d, nx + 1, j, k)] = f.ws[pidx(d, 1, j, k)];
+    if (j >= 1) {
+        f.vn[pidx(d, 0, j, k)] = f.vn[pidx(d, nx, j, k)];
+        f.vn[pidx(d, nx + 1, j, k)] = f.vn[pidx(d, 1, j, k)];
+        f.vs[pidx(d, 0, j, k)] = f.vs[pidx(d, nx, j, k)];
+        f.vs[pidx(d, nx + 1, j, k)] = f.vs[pidx(d, 1, j, k)];
+    }
+    if (j >= 1 && j <= d.ny) {
+        f.pn[pidx(d, 0, j, k)] = f.pn[pidx(d, nx, j, k)];
+        f.pn[pidx(d, nx + 1, j, k)] = f.pn[pidx(d, 1, j, k)];
+    }
+}
+
+__global__ void k_bc_periodic_z(mdx_dims d, mdx_six f) {   // boundary.f90:137-168
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i > d.nx + 1 || j > d.ny + 1) return;
+    const int nz = d.nz;
+    f.un[pidx(d, i, j, 0)] = f.un[pidx(d, i, j, nz)];
+    f.wn[pidx(d, i, j, 0)] = f.wn[pidx(d, i, j, nz)];
+    f.un[pidx(d, i, j, nz + 1)] = f.un[pidx(d, i, j, 1)];
+    f.wn[pidx(d, i, j, nz + 1)] = f.wn[pidx(d, i, j, 1)];
+    f.us[pidx(d, i, j, 0)] = f.us[pidx(d, i, j, nz)];
+    f.ws[pidx(d, i, j, 0)] = f.ws[pidx(d, i, j, nz)];
+    f.us[pidx(d, i, j, nz + 1)] = f.us[pidx(d, i, j, 1)];
+    f.ws[pidx(d, i, j, nz + 1)] = f.ws[pidx(d, i, j, 1)];
+    if (j >= 1) {
+        f.vn[pidx(d, i, j, 0)] = f.vn[pidx(d, i, j, nz)];
+        f.vn[pidx(d, i, j, nz + 1)] = f.vn[pidx(d, i, j, 1)];
+        f.vs[pidx(d, i, j, 0)] = f.vs[pidx(d, i, j, nz)];
+        f.vs[pidx(d, i, j, nz + 1)] = f.vs[pidx(d, i, j, 1)];
+    }
+    if (j >= 1 && j <= d.ny) {
+        f.pn[pidx(d, i, j, 0)] = f.pn[pidx(d, i, j, nz)];
+        f.pn[pidx(d, i, j, nz + 1)] = f.pn[pidx(d, i, j, 1)];
+    }
+}
+
+int mdx_k_apply_bc(mdx_ctx_t* ctx) {
+    const mdx_dims& d = ctx->d;
+    double** a = ctx->f;
+    mdx_six f{a[MDX_UN], a[MDX_VN], a[MDX_WN], a[MDX_US], a[MDX_VS], a[MDX_WS], a[MDX_PN]};
+    dim3 b(32, 8);
+    MDX_LAUNCH(ctx, MDX_T_BC, "apply_bc y", k_bc_walls_y, dim3((d.nxp + 31) / 32, (d.nzp + 7) / 8), b, 0, d, f);
+    MDX_LAUNCH(ctx, MDX_T_BC, "apply_bc x", k_bc_periodic_x, dim3((d.nyp + 31) / 32, (d.nzp + 7) / 8), b, 0, d, f);
+    MDX_LAUNCH(ctx, MDX_T_BC, "apply_bc z", k_bc_periodic_z, dim3((d.nxp + 31) / 32, (d.nyp + 7) / 8), b, 0, d, f);
+    return MDX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// apply_bc_redblack, src/modules/boundary.f90:173-368.  The reference loops
+// over the faces sequentially in the order bottom, top, left, right, front,
+// back; faces of different directions read each other's values (e.g. the
+// x-periodic copy reads the v wall row set by the y faces), so the three
+// directions run as three ordered launches.  Within one direction the
+// min and max faces of a column touch disjoint cells (ny, nx, nz >= 2).
+// ---------------------------------------------------------------------------
+struct mdx_four { double *un, *vn, *wn, *pn; };
+
+__global__ void k_bcrb_y(mdx_dims d, mdx_bc_dev bc, double dy, mdx_four f) {   // :207-258
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int k = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    if (i > d.nx || k > d.nz) return;
+    const int ny = d.ny;
+    const int* T = bc.type;
+    const double* V = bc.value;
+    double *un = f.un, *vn = f.vn, *wn = f.wn, *pn = f.pn;
+    if (bc.per[1]) {
+        un[pidx(d, i, 0, k)] = un[pidx(d, i, ny, k)];
+        vn[pidx(d, i, 0, k)] = vn[pidx(d, i, ny, k)];
+        wn[pidx(d, i, 0, k)] = wn[pidx(d, i, ny, k)];
+        pn[pidx(d, i, 0, k)] = pn[pidx(d, i, ny, k)];
+    } else {
+        if (T[bci(2, 0, 1)] == 0) un[pidx(d, i, 0, k)] = 2 * V[bci(2, 0, 1)] - un[pidx(d, i, 1, k)];
+        else un[pidx(d, i, 0, k)] = un[pidx(d, i, 1, k)] - V[bci(2, 0, 1)] * dy;
+        if (T[bci(2, 0, 2)] == 0) vn[pidx(d, i, 1, k)] = V[bci(2, 0, 2)];
+        else vn[pidx(d, i, 1, k)] = vn[pidx(d, i, 2, k)] - V[bci(2, 0, 2)] * dy;
+        if (T[bci(2, 0, 3)] == 0) wn[pidx(d, i, 0, k)] = 2 * V[bci(2, 0, 3)] - wn[pidx(d, i, 1, k)];
+        else wn[pidx(d, i, 0, k)] = wn[pidx(d, i, 1, k)] - V[bci(2, 0, 3)] * dy;
+    }
+    if (bc.per[1]) {
+        un[pidx(d, i, ny + 1, k)] = un[pidx(d, i, 1, k)];
+        vn[pidx(d, i, ny + 1, k)] = vn[pidx(d, i, 1, k)];
+        wn[pidx(d, i, ny + 1, k)] = wn[pidx(d, i, 1, k)];
+        pn[pidx(d, i, ny + 1, k)] = pn[pidx(d, i, 1, k)];
+    } else {
+        if (T[bci(2, 1, 1)] == 0) un[pidx(d, i, ny + 1, k)] = 2 * V[bci(2, 1, 1)] - un[pidx(d, i, ny, k)];
+        else un[pidx(d, i, ny + 1, k)] = un[pidx(d, i, ny, k)] + V[bci(2, 1, 1)] * dy;
+        if (T[bci(2, 1, 2)] == 0) vn[pidx(d, i, ny + 1, k)] = V[bci(2, 1, 2)];
+        else vn[pidx(d, i, ny + 1, k)] = vn[pidx(d, i, ny, k)] + V[bci(2, 1, 2)] * dy;
+        if (T[bci(2, 1, 3)] == 0) wn[pidx(d, i, ny + 1, k)] = 2 * V[bci(2, 1, 3)] - wn[pidx(d, i, ny, k)];
+        else wn[pidx(d, i, ny + 1, k)] = wn[pidx(d, i, ny, k)] + V[bci(2, 1, 3)] * dy;
+    }
+}
+
+__global__ void k_bcrb_x(mdx_dims d, mdx_bc_dev bc, double dx, mdx_four f) {   // :259-310
+    const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int k = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    if (j > d.ny || k > d.nz) return;
+    const int nx = d.nx;
+    const int* T = bc.type;
+    const double* V = bc.value;
+    double *un = f.un, *vn = f.vn, *wn = f.wn, *pn = f.pn;
+    if (bc.per[0]) {
+        un[pidx(d, 0, j, k)] = un[pidx(d, nx, j, k)];
+        vn[pidx(d, 0, j, k)] = vn[pidx(d, nx, j, k)];
+        wn[pidx(d, 0, j, k)] = wn[pidx(d, nx, j, k)];
+        pn[pidx(d, 0, j, k)] = pn[pidx(d, nx, j, k)];
+    } else {
+        if (T[bci(1, 0, 1)] == 0) un[pidx(d, 1, j, k)] = V[bci(1, 0, 1)];
+        else un[pidx(d, 1, j, k)] = un[pidx(d, 2, j, k)] - V[bci(1, 0, 1)] * dx;
+        if (T[bci(1, 0, 2)] == 0) vn[pidx(d, 0, j, k)] = 2 * V[bci(1, 0, 2)] - vn[pidx(d, 1, j, k)];
+        else vn[pidx(d, 0, j, k)] = vn[pidx(d, 1, j, k)] - V[bci(1, 0, 2)] * dx;
+        if (T[bci(1, 0, 3)] == 0) wn[pidx(d, 0, j, k)] = 2 * V[bci(1, 0, 3)] - wn[pidx(d, 1, j, k)];
+        else wn[pidx(d, 0, j, k)] = wn[pidx(d, 1, j, k)] - V[bci(1, 0, 3)] * dx;
+    }
+    if (bc.per[0]) {
+        un[pidx(d, nx + 1, j, k)] = un[pidx(d, 1, j, k)];
+        vn[pidx(d, nx + 1, j, k)] = vn[pidx(d, 1, j, k)];
+        wn[pidx(d, nx + 1, j, k)] = wn[pidx(d, 1, j, k)];
+        pn[pidx(d, nx + 1, j, k)] = pn[pidx(d, 1, j, k)];
+    } else {
+        if (T[bci(1, 1, 1)] == 0) un[pidx(d, nx + 1, j, k)] = V[bci(1, 1, 1)];
+        else un[pidx(d, nx + 1, j, k)] = un[pidx(d, nx, j, k)] + V[bci(1, 1, 1)] * dx;
+        if (T[bci(1, 1, 2)] == 0) vn[pidx(d, nx + 1, j, k)] = 2 * V[bci(1, 1, 2)] - vn[pidx(d, nx, j, k)];
+        else vn[pidx(d, nx + 1, j, k)] = vn[pidx(d, nx, j, k)] + V[bci(1, 1, 2)] * dx;
+        if (T[bci(1, 1, 3)] == 0) wn[pidx(d, nx + 1, j, k)] = 2 * V[bci(1, 1, 3)] - wn[pidx(d, nx, j, k)];
+        else wn[pidx(d, nx + 1, j, k)] = wn[pidx(d, nx, j, k)] + V[bci(1, 1, 3)] * dx;
+    }
+}
+
+__global__ void k_bcrb_z(mdx_dims d, mdx_bc_dev bc, double dz, mdx_four f) {   // :311-364
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    if (i > d.nx || j > d.ny) return;
+    const int nz = d.nz;
+    const int* T = bc.type;
+    const double* V = bc.value;
+    double *un = f.un, *vn = f.vn, *wn = f.wn, *pn = f.pn;
+    if (bc.per[2]) {
+        un[pidx(d, i, j, 0)] = un[pidx(d, i, j, nz)];
+        vn[pidx(d, i, j, 0)] = vn[pidx(d, i, j, nz)];
+        wn[pidx(d, i, j, 0)] = wn[pidx(d, i, j, nz)];
+        pn[pidx(d, i, j, 0)] = pn[pidx(d, i, j, nz)];
+    } else {
+        if (T[bci(3, 0, 1)] == 0) un[pidx(d, i, j, 0)] = 2 * V[bci(3, 0, 1)] - un[pidx(d, i, j, 1)];
+        else un[pidx(d, i, j, 0)] = un[pidx(d, i, j, 1)] - V[bci(3, 0, 1)] * dz;
+        if (T[bci(3, 0, 2)] == 0) vn[pidx(d, i, j, 0)] = 2 * V[bci(3, 0, 2)] - vn[pidx(d, i, j, 1)];
+        else vn[pidx(d, i, j, 0)] = vn[pidx(d, i, j, 1)] - V[bci(3, 0, 2)] * dz;
+        if (T[bci(3, 0, 3)] == 0) wn[pidx(d, i, j, 1)] = V[bci(3, 0, 3)];
+        else wn[pidx(d, i, j, 1)] = wn[pidx(d, i, j, 2)] - V[bci(3, 0, 3)] * dz;
+    }
+    if (bc.per[2]) {
+        un[pidx(d, i, j, nz + 1)] = un[pidx(d, i, j, 1)];
+        vn[pidx(d, i, j, nz + 1)] = vn[pidx(d, i, j, 1)];
+        wn[pidx(d, i, j, nz + 1)] = wn[pidx(d, i, j, 1)];
+        pn[pidx(d, i, j, nz + 1)] = pn[pidx(d, i, j, 1)];
+    } else {
+        if (T[bci(3, 1, 1)] == 0) un[pidx(d, i, j, nz + 1)] = 2 * V[bci(3, 1, 1)] - un[pidx(d, i, j, nz)];
+        else un[pidx(d, i, j, nz + 1)] = un[pidx(d, i, j, nz)] + V[bci(3, 1, 1)] * dz;
+        if (T[bci(3, 1, 2)] == 0) vn[pidx(d, i, j, nz + 1)] = 2 * V[bci(3, 1, 2)] - vn[pidx(d, i, j, nz)];
+        else vn[pidx(d, i, j, nz + 1)] = vn[pidx(d, i, j, nz)] + V[bci(3, 1, 2)] * dz;
+        if (T[bci(3, 1, 3)] == 0) wn[pidx(d, i, j, nz + 1)] = V[bci(3, 1, 3)];
+        else wn[pidx(d, i, j, nz + 1)] = wn[pidx(d, i, j, nz)] + V[bci(3, 1, 3)] * dz;
+    }
+}
+
+int mdx_k_apply_bc_redblack(mdx_ctx_t* ctx) {
+    const mdx_dims& d = ctx->d;
+    double** a = ctx->f;
+    mdx_four f{a[MDX_UN], a[MDX_VN], a[MDX_WN], a[MDX_PN]};
+    dim3 b(32, 8);
+    MDX_LAUNCH(ctx, MDX_T_BC, "apply_bc_redblack y", k_bcrb_y, dim3((d.nx + 31) / 32, (d.nz + 7) / 8), b, 0, d,
+               ctx->bcd, ctx->g.dy, f);
+    MDX_LAUNCH(ctx, MDX_T_BC, "apply_bc_redblack x", k_bcrb_x, dim3((d.ny + 31) / 32, (d.nz + 7) / 8), b, 0, d,
+               ctx->bcd, ctx->g.dx, f);
+    MDX_LAUNCH(ctx, MDX_T_BC, "apply_bc_redblack z", k_bcrb_z, dim3((d.nx + 31) / 32, (d.ny + 7) / 8), b, 0, d,
+               ctx->bcd, ctx->g.dz, f);
+    return MDX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Deterministic reductions: fixed grid, per-block partials in a fixed order,
+// one final block.  Used by the CFL (max) and the divergence norms (sum of
+// squares and max-abs).
+// ---------------------------------------------------------------------------
+#define MDX_RED_THREADS 256
+
+// Block reduction of (sum, max, max) in a fixed order; NaN in a max slot wins.
+__device__ inline double nanmax(double a, double b) { return (a != a || b != b) ? (a + b) : fmax(a, b); }
+
+__device__ inline void block_reduce3(double& s, double& m, double& u) {
+    __shared__ double ss[MDX_RED_THREADS / 32], sm[MDX_RED_THREADS / 32], su[MDX_RED_THREADS / 32];
+    for (int o = 16; o > 0; o >>= 1) {
+        s += __shfl_down_sync(0xffffffffu, s, o);
+        m = nanmax(m, __shfl_down_sync(0xffffffffu, m, o));
+        u = nanmax(u, __shfl_down_sync(0xffffffffu, u, o));
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) { ss[w] = s; sm[w] = m; su[w] = u; }
+    __syncthreads();
+    if (w == 0) {
+        s = (l < MDX_RED_THREADS / 32) ? ss[l] : 0.0;
+        m = (l < MDX_RED_THREADS / 32) ? sm[l] : 0.0;
+        u = (l < MDX_RED_THREADS / 32) ? su[l] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) {
+            s += __shfl_down_sync(0xffffffffu, s, o);
+            m = nanmax(m, __shfl_down_sync(0xffffffffu, m, o));
+            u = nanmax(u, __shfl_down_sync(0xffffffffu, u, o));
+        }
+    }
+}
+
+// Divergence with the red-black neighbour rule (periodic wrap to 1):
+// partials of sum(div^2), max|div| and max(|u|,|v|,|w|) over the cells.
+__global__ void __launch_bounds__(MDX_RED_THREADS)
+k_div_partials(mdx_dims d, int perx, int pery, int perz, double idx, double idy, double idz,
+               const double* __restrict__ u, const double* __restrict__ v, const double* __restrict__ w,
+               double* __restrict__ part) {
+    double s = 0.0, m = 0.0, um = 0.0;
+    const long long n = d.nint;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % d.nx) + 1;
+        const long long r = t / d.nx;
+        const int j = (int)(r % d.ny) + 1;
+        const int k = (int)(r / d.ny) + 1;
+        const int ip = (perx && i + 1 > d.nx) ? 1 : i + 1;
+        const int jp = (pery && j + 1 > d.ny) ? 1 : j + 1;
+        const int kp = (perz && k + 1 > d.nz) ? 1 : k + 1;
+        const long long c = pidx(d, i, j, k);
+        const double uc = __ldg(u + c), vc = __ldg(v + c), wc = __ldg(w + c);
+        const double dv = (__ldg(u + pidx(d, ip, j, k)) - uc) * idx + (__ldg(v + pidx(d, i, jp, k)) - vc) * idy +
+                          (__ldg(w + pidx(d, i, j, kp)) - wc) * idz;
+        s += dv * dv;
+        m = nanmax(m, fabs(dv));
+        um = nanmax(um, nanmax(fabs(uc), nanmax(fabs(vc), fabs(wc))));
+    }
+    block_reduce3(s, m, um);
+    if (threadIdx.x == 0) {
+        part[3 * blockIdx.x] = s;
+        part[3 * blockIdx.x + 1] = m;
+        part[3 * blockIdx.x + 2] = um;
+    }
+}
+
+__global__ void __launch_bounds__(MDX_RED_THREADS)
+k_cfl_partials(long long n, double dx, double dy, double dz, const double* __restrict__ u,
+               const double* __restrict__ v, const double* __restrict__ w, double* __restrict__ part) {
+    double m = 0.0, s = 0.0, um = 0.0;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        m = fmax(m, fabs(__ldg(u + t) / dx));
+        m = fmax(m, fabs(__ldg(v + t) / dy));
+        m = fmax(m, fabs(__ldg(w + t) / dz));
+    }
+    block_reduce3(s, m, um);
+    if (threadIdx.x == 0) { part[3 * blockIdx.x] = 0.0; part[3 * blockIdx.x + 1] = m; part[3 * blockIdx.x + 2] = 0.0; }
+}
+
+__global__ void __launch_bounds__(MDX_RED_THREADS)
+k_reduce_final(int nb, const double* __restrict__ part, double* __restrict__ out) {
+    double s = 0.0, m = 0.0, um = 0.0;
+    for (int t = threadIdx.x; t < nb; t += blockDim.x) {
+        s += part[3 * t];
+        m = nanmax(m, part[3 * t + 1]);
+        um = nanmax(um, part[3 * t + 2]);
+    }
+    block_reduce3(s, m, um);
+    if (threadIdx.x == 0) { out[0] = s; out[1] = m; out[2] = um; }
+}
+
+int mdx_reduce_init(mdx_ctx_t* ctx) {
+    if (ctx->red_part) return MDX_OK;
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+    ctx->red_blocks = sms * 4;
+    MDX_CUDA(ctx, cudaMalloc(&ctx->red_part, sizeof(double) * 3 * ctx->red_blocks));
+    MDX_CUDA(ctx, cudaMalloc(&ctx->red_out, sizeof(double) * 3));
+    MDX_CUDA(ctx, cudaMallocHost(&ctx->red_host, sizeof(double) * 3));
+    return MDX_OK;
+}
+
+// Enqueue the divergence-norm reduction; the result lands in red_host after
+// the stream reaches it (caller synchronises).
+int mdx_k_div_norms_async(mdx_ctx_t* ctx, const double* u, const double* v, const double* w) {
+    MDX_TRY(mdx_reduce_init(ctx));
+    const mdx_dims& d = ctx->d;
+    const int* per = ctx->bc.is_periodic;
+    MDX_LAUNCH(ctx, MDX_T_RESIDUAL, "divergence partials", k_div_partials, ctx->red_blocks, MDX_RED_THREADS, 0, d,
+               per[0], per[1], per[2], 1.0 / ctx->g.dx, 1.0 / ctx->g.dy, 1.0 / ctx->g.dz, u, v, w, ctx->red_part);
+    MDX_LAUNCH(ctx, MDX_T_RESIDUAL, "reduce final", k_reduce_final, 1, MDX_RED_THREADS, 0, ctx->red_blocks,
+               ctx->red_part, ctx->red_out);
+    MDX_CUDA(ctx, cudaMemcpyAsync(ctx->red_host, ctx->red_out, 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    return MDX_OK;
+}
+
+int mdx_k_div_norms(mdx_ctx_t* ctx, const double* u, const double* v, const double* w, double* l2, double* linf,
+                    double* umax) {
+    MDX_TRY(mdx_k_div_norms_async(ctx, u, v, w));
+    MDX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    *l2 = sqrt(ctx->red_host[0]);
+    *linf = ctx->red_host[1];
+    if (umax) *umax = ctx->red_host[2];
+    return MDX_OK;
+}
+
+// get_cfl, src/modules/step.f90:210-258: max over the padded arrays of
+// |u/dx|, |v/dy|, |w/dz| (max is exact, so the result is order-independent).
+int mdx_k_cfl(mdx_ctx_t* ctx, double* cfl) {
+    MDX_TRY(mdx_reduce_init(ctx));
+    const mdx_dims& d = ctx->d;
+    MDX_LAUNCH(ctx, MDX_T_OTHER, "cfl partials", k_cfl_partials, ctx->red_blocks, MDX_RED_THREADS, 0, d.npad,
+               ctx->g.dx, ctx->g.dy, ctx->g.dz, ctx->f[MDX_UN], ctx->f[MDX_VN], ctx->f[MDX_WN],
+               ctx->red_part);
+    MDX_LAUNCH(ctx, MDX_T_OTHER, "reduce final", k_reduce_final, 1, MDX_RED_THREADS, 0, ctx->red_blocks,
+               ctx->red_part, ctx->red_out);
+    MDX_CUDA(ctx, cudaMemcpyAsync(ctx->red_host, ctx->red_out, 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    MDX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    *cfl = ctx->red_host[1];
+    return MDX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// center_vel, src/modules/io.f90:196-216.
+// ---------------------------------------------------------------------------
+__global__ void k_center_vel(mdx_dims d, const double* __restrict__ u, const double* __restrict__ v,
+                             const double* __restrict__ w, double* __restrict__ uc, double* __restrict__ vc,
+                             double* __restrict__ wc) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= d.nint) return;
+    const int i = (int)(t % d.nx) + 1;
+    const long long r = t / d.nx;
+    const int j = (int)(r % d.ny) + 1;
+    const int k = (int)(r / d.ny) + 1;
+    const long long c = pidx(d, i, j, k);
+    uc[t] = 0.5 * (u[c] + u[pidx(d, i + 1, j, k)]);
+    vc[t] = 0.5 * (v[c] + v[pidx(d, i, j + 1, k)]);
+    wc[t] = 0.5 * (w[c] + w[pidx(d, i, j, k + 1)]);
+}
+
+int mdx_k_center_vel(mdx_ctx_t* ctx, double* uc, double* vc, double* wc) {
+    const mdx_dims& d = ctx->d;
+    double* buf = nullptr;
+    MDX_CUDA(ctx, cudaMallocAsync(&buf, sizeof(double) * 3 * d.nint, ctx->stream));
+    const int nb = (int)((d.nint + 255) / 256);
+    mdx_event_pair p{};
+    mdx_timer_begin(ctx, MDX_T_OTHER, &p);
+    k_center_vel<<<nb, 256, 0, ctx->stream>>>(d, ctx->f[MDX_UN], ctx->f[MDX_VN], ctx->f[MDX_WN], buf, buf + d.nint,
+                                              buf + 2 * d.nint);
+    mdx_timer_end(ctx, &p);
+    int rc = mdx_check_launch(ctx, "center_vel");
+    if (rc == MDX_OK) {
+        cudaError_t e = cudaSuccess;
+        if (uc && e == cudaSuccess) e = cudaMemcpyAsync(uc, buf, sizeof(double) * d.nint, cudaMemcpyDeviceToHost, ctx->stream);
+        if (vc && e == cudaSuccess) e = cudaMemcpyAsync(vc, buf + d.nint, sizeof(double) * d.nint, cudaMemcpyDeviceToHost, ctx->stream);
+        if (wc && e == cudaSuccess) e = cudaMemcpyAsync(wc, buf + 2 * d.nint, sizeof(double) * d.nint, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) rc = mdx_fail(ctx, MDX_ERR_CUDA, "center_vel copy: %s", cudaGetErrorString(e));
+    }
+    cudaFreeAsync(buf, ctx->stream);
+    return rc;
+}
+
+// ---------------------------------------------------------------------------
+// Seeded channel initial condition (counter-based SplitMix64 finaliser of
+// Steele, Lea & Flood 2014 on seed + golden*(field<<40 | padded index)).
+// yc(x) per x index comes from the host so the profile is the host's libm.
+// ---------------------------------------------------------------------------
+__device__ inline uint64_t ic_hash(uint64_t seed, uint64_t field, uint64_t lin) {
+    uint64_t z = seed + 0x9E3779B97F4A7C15ull * ((field << 40) | lin);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+__device__ inline double ic_uniform(uint64_t seed, uint64_t field, uint64_t lin, double amp) {
+    const double u01 = (double)(ic_hash(seed, field, lin) >> 11) * (1.0 / 9007199254740992.0);
+    return amp * (2.0 * u01 - 1.0);
+}
+
+__global__ void k_channel_ic(mdx_dims d, double dy, uint64_t seed, double amp_u, double amp_vw,
+                             const double* __restrict__ yc, double* __restrict__ un, double* __restrict__ vn,
+                             double* __restrict__ wn) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= d.nint) return;
+    const int i = (int)(t % d.nx) + 1;
+    const long long r = t / d.nx;
+    const int j = (int)(r % d.ny) + 1;
+    const int k = (int)(r / d.ny) + 1;
+    const long long c = pidx(d, i, j, k);
+    const double y = ((double)j - 0.5) * dy;
+    const double e = y - yc[i - 1];
+    double base = 1.0 - e * e;
+    if (base < 0.0) base = 0.0;
+    un[c] = base + ic_uniform(seed, 0, (uint64_t)c, amp_u);
+    vn[c] = (j == 1) ? 0.0 : ic_uniform(seed, 1, (uint64_t)c, amp_vw);
+    wn[c] = ic_uniform(seed, 2, (uint64_t)c, amp_vw);
+}
+
+int mdx_k_channel_ic(mdx_ctx_t* ctx, uint64_t seed, double amp_u, double amp_vw, const double* yc_host) {
+    const mdx_dims& d = ctx->d;
+    double* yc = nullptr;
+    MDX_CUDA(ctx, cudaMallocAsync(&yc, sizeof(double) * d.nx, ctx->stream));
+    MDX_CUDA(ctx, cudaMemcpyAsync(yc, yc_host, sizeof(double) * d.nx, cudaMemcpyHostToDevice, ctx->stream));
+    const int nb = (int)((d.nint + 255) / 256);
+    k_channel_ic<<<nb, 256, 0, ctx->stream>>>(d, ctx->g.dy, seed, amp_u, amp_vw, yc, ctx->f[MDX_UN], ctx->f[MDX_VN],
+                                              ctx->f[MDX_WN]);
+    int rc = mdx_check_launch(ctx, "channel_ic");
+    MDX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));   // host yc buffer must outlive the copy
+    cudaFreeAsync(yc, ctx->stream);
+    return rc;
+}
+
+__global__ void k_fill(double* p, long long n, double v) {
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+        p[t] = v;
+}
+
+int mdx_k_fill(mdx_ctx_t* ctx, double* p, long long n, double v) {
+    MDX_LAUNCH(ctx, MDX_T_OTHER, "fill", k_fill, 1024, 256, 0, p, n, v);
+    return MDX_OK;
+}

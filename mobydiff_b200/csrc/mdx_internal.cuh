@@ -1,0 +1,162 @@
+// mdx_internal.cuh -- context, device layout and shared helpers of libmobyb200.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/mobydiff_b200.h"
+
+// Device layout.  Every field keeps the reference's host layout so that the
+// drop-in copies are flat memcpys: padded (0:nx+1,0:ny+1,0:nz+1) Fortran
+// order, x fastest.  The FFT workspace keeps the reference's orders too:
+// phi / rhs (nx,nz,ny) real and the spectrum (nxh,nz,ny) complex
+// (src/modules/pressure_workspace.f90:10-22).
+struct mdx_dims {
+    int nx, ny, nz;
+    int nxp, nyp, nzp;   // nx+2, ny+2, nz+2
+    int nxh;             // nx/2+1
+    long long npad;      // (nx+2)(ny+2)(nz+2)
+    long long nint;      // nx*ny*nz
+    long long nspec;     // nxh*nz*ny
+};
+
+__host__ __device__ inline long long pidx(const mdx_dims& d, int i, int j, int k) {
+    return (long long)i + (long long)d.nxp * ((long long)j + (long long)d.nyp * (long long)k);
+}
+__host__ __device__ inline long long qidx(const mdx_dims& d, int i, int j, int k) {  // (1:nx,1:ny,1:nz)
+    return (long long)(i - 1) + (long long)d.nx * ((long long)(j - 1) + (long long)d.ny * (long long)(k - 1));
+}
+__host__ __device__ inline long long ridx(const mdx_dims& d, int i, int k, int j) {  // rhs(i,k,j), 1-based
+    return (long long)(i - 1) + (long long)d.nx * ((long long)(k - 1) + (long long)d.nz * (long long)(j - 1));
+}
+
+// Scalars of one time step, passed by value to kernels.
+struct mdx_step_params {
+    double dx, dy, dz;
+    double idx, idy, idz, idx2, idy2, idz2, ire;
+    double fx, fy, fz;
+    int nx0, ny0, nz0;
+};
+
+struct mdx_bc_dev {
+    int per[3];
+    int type[24];
+    double value[24];
+};
+__host__ __device__ inline int bci(int dir, int side, int var) { return (dir - 1) + 3 * (side + 2 * var); }
+
+// FFT plan for one length: radix list and twiddle table exp(-2 pi i t/n).
+#define MDX_MAX_STAGES 16
+struct mdx_fft_plan {
+    int n;
+    int nstages;
+    int radix[MDX_MAX_STAGES];
+};
+
+struct mdx_event_pair { cudaEvent_t a, b; int cls; };
+
+struct mdx_ctx {
+    int device = 0;
+    mdx_grid_t g{};
+    mdx_bc_t bc{};
+    mdx_bc_dev bcd{};
+    mdx_solver_opts_t opts{};
+    mdx_dims d{};
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    std::string err;
+
+    bool fields = false;
+    bool solver = false;
+    double* f[MDX_NUM_FIELDS] = {nullptr};   // device mirrors (MDX_PHI -> phi)
+    bool ibm_zero = true;                    // all IBM coefficients zero
+
+    // FFT workspace
+    double2* spec = nullptr;                 // (nxh, nz, ny)
+    double* thomas_dinv = nullptr;           // (ny, nxh, nz/2+1)
+    double* thomas_cp = nullptr;             // (ny, nxh, nz/2+1)
+    double2* tw_x = nullptr;                 // exp(-2 pi i t/nx), t < nx
+    double2* tw_z = nullptr;                 // exp(-2 pi i t/nz), t < nz
+    mdx_fft_plan plan_xh{};                  // complex length nx/2 (packed real transform)
+    mdx_fft_plan plan_z{};                   // complex length nz
+
+    // reductions
+    double* red_part = nullptr;              // per-block partials (2 per block)
+    int red_blocks = 0;
+    double* red_out = nullptr;               // device result [2]
+    double* red_host = nullptr;              // pinned host result [2]
+
+    mdx_solve_stats_t last{};
+
+    // CUDA graph of one FFT-path RK3 step
+    cudaGraphExec_t step_graph = nullptr;
+    double graph_dt = 0.0;
+    long long graph_launches = 0;
+
+    // timing
+    bool timing = false;
+    std::vector<mdx_event_pair> ev_pending;
+    std::vector<cudaEvent_t> ev_free;
+    mdx_timing_t tim{};
+    long long launches = 0;
+    bool capturing = false;
+};
+
+// ---- error helpers -------------------------------------------------------
+int mdx_fail(mdx_ctx_t* ctx, int code, const char* fmt, ...);
+#define MDX_CUDA(ctx, call)                                                                   \
+    do {                                                                                      \
+        cudaError_t e__ = (call);                                                             \
+        if (e__ != cudaSuccess)                                                               \
+            return mdx_fail((ctx), MDX_ERR_CUDA, "%s failed: %s (%s:%d)", #call,             \
+                            cudaGetErrorString(e__), __FILE__, __LINE__);                     \
+    } while (0)
+#define MDX_TRY(expr)                         \
+    do {                                      \
+        int r__ = (expr);                     \
+        if (r__ != MDX_OK) return r__;        \
+    } while (0)
+
+// ---- launch bookkeeping ----------------------------------------------------
+void mdx_timer_begin(mdx_ctx_t* ctx, int cls, mdx_event_pair* p);
+void mdx_timer_end(mdx_ctx_t* ctx, mdx_event_pair* p);
+int mdx_check_launch(mdx_ctx_t* ctx, const char* what);
+
+// Launch wrapper: times the launch when timing is on and checks the launch.
+#define MDX_LAUNCH(ctx, cls, what, kernel, grid, block, smem, ...)                     \
+    do {                                                                               \
+        mdx_event_pair p__{};                                                          \
+        mdx_timer_begin((ctx), (cls), &p__);                                           \
+        kernel<<<(grid), (block), (smem), (ctx)->stream>>>(__VA_ARGS__);               \
+        mdx_timer_end((ctx), &p__);                                                    \
+        MDX_TRY(mdx_check_launch((ctx), (what)));                                      \
+    } while (0)
+
+// ---- per-module entry points (internal) --------------------------------------
+mdx_step_params mdx_make_params(const mdx_ctx_t* ctx);
+int mdx_k_momentum(mdx_ctx_t* ctx, double da, double db, double dg);
+int mdx_k_apply_bc(mdx_ctx_t* ctx);
+int mdx_k_apply_bc_redblack(mdx_ctx_t* ctx);
+int mdx_fft_init(mdx_ctx_t* ctx);
+void mdx_fft_free(mdx_ctx_t* ctx);
+int mdx_k_projection_fft(mdx_ctx_t* ctx, double dg);
+int mdx_k_projection_redblack(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t* st);
+int mdx_k_div_norms(mdx_ctx_t* ctx, const double* u, const double* v, const double* w, double* l2, double* linf,
+                    double* umax = nullptr);
+// Round-off floor of ||div u||_2: eps*sqrt(ncells)*umax*(1/dx+1/dy+1/dz).
+double mdx_div_floor(const mdx_ctx_t* ctx, double umax);
+int mdx_k_div_norms_async(mdx_ctx_t* ctx, const double* u, const double* v, const double* w);
+int mdx_k_cfl(mdx_ctx_t* ctx, double* cfl);
+int mdx_k_center_vel(mdx_ctx_t* ctx, double* uc, double* vc, double* wc);
+int mdx_k_channel_ic(mdx_ctx_t* ctx, uint64_t seed, double amp_u, double amp_vw, const double* yc_host);
+int mdx_k_fill(mdx_ctx_t* ctx, double* p, long long n, double v);
+int mdx_reduce_init(mdx_ctx_t* ctx);
+
+// Host-side modules.
+void mdx_rk_coeffs(double* a, double* b, double* c);
+void mdx_fft_make_plan(int n, mdx_fft_plan* p, bool* ok);
+void mdx_fft_twiddles(int n, std::vector<double2>& tw);
