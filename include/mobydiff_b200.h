@@ -183,6 +183,13 @@ int mdx_set_ibm_coeff(const mdx_grid_t* g, const mdx_ibm_geom_t* geom, double* c
 int mdx_create(int device, const mdx_grid_t* g, const mdx_bc_t* bc, mdx_ctx_t** out);
 int mdx_destroy(mdx_ctx_t* ctx);
 
+/* Replace the boundary set of a context.  The reference passes bc to
+ * momentum / pressure_projection / apply_bc_redblack on every call
+ * (src/modules/step.f90:27, pressure_solver.f90:48, boundary.f90:173) while
+ * enter_field_data gets none (gpu_runtime.f90:22), so a Fortran shim creates
+ * the context with init_bc defaults and updates it here when bc changes. */
+int mdx_set_bc(mdx_ctx_t* ctx, const mdx_bc_t* bc);
+
 /* Use an external CUDA stream (cudaStream_t) instead of the context's own;
  * NULL restores the context stream. */
 int mdx_set_stream(mdx_ctx_t* ctx, void* stream);

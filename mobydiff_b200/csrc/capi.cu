@@ -201,6 +201,9 @@ int mdx_destroy_pressure_solver(mdx_ctx_t* ctx) {
     mdx_fft_free(ctx);
     cudaFree(ctx->f[MDX_PHI]);
     ctx->f[MDX_PHI] = nullptr;
+    cudaFree(ctx->mu);
+    ctx->mu = nullptr;
+    ctx->mu_elems = 0;
     ctx->solver = false;
     return MDX_OK;
 }
@@ -230,6 +233,19 @@ int mdx_destroy(mdx_ctx_t* ctx) {
     for (auto e : ctx->ev_free) cudaEventDestroy(e);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
+    return MDX_OK;
+}
+
+int mdx_set_bc(mdx_ctx_t* ctx, const mdx_bc_t* bc) {
+    if (!ctx || !bc) return mdx_fail(ctx, MDX_ERR_ARG, "mdx_set_bc: null argument");
+    if (ctx->solver && ctx->opts.solver == MDX_SOLVER_REDBLACK && bc->is_periodic[1] && ctx->d.ny % 2 != 0)
+        return mdx_fail(ctx, MDX_ERR_ARG, "red-black pressure solver with periodic y requires even ny");
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    release_graph(ctx);
+    ctx->bc = *bc;
+    for (int t = 0; t < 3; ++t) ctx->bcd.per[t] = bc->is_periodic[t] ? 1 : 0;
+    for (int t = 0; t < 24; ++t) { ctx->bcd.type[t] = bc->bc_type[t]; ctx->bcd.value[t] = bc->bc_value[t]; }
     return MDX_OK;
 }
 
@@ -307,7 +323,10 @@ int mdx_copy_field(mdx_ctx_t* ctx, int field, double* host, int direction) {
     } else {
         MDX_CUDA(ctx, cudaMemcpyAsync(ctx->f[field], host, bytes, cudaMemcpyHostToDevice, ctx->stream));
         MDX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-        if (field >= MDX_COEF_U && field <= MDX_COEF_W) ctx->ibm_zero = false;
+        if (field >= MDX_COEF_U && field <= MDX_COEF_W) {
+            ctx->ibm_zero = false;
+            ctx->coef_zinv = false;
+        }
     }
     return MDX_OK;
 }
@@ -316,12 +335,15 @@ int mdx_enter_ibm_data(mdx_ctx_t* ctx, const double* cu, const double* cv, const
     MDX_TRY(need_fields(ctx));
     release_graph(ctx);
     const double* src[3] = {cu, cv, cw};
-    bool any = false;
+    bool any = false, zinv = true;
     const size_t n = (size_t)ctx->d.npad;
+    const size_t plane = (size_t)ctx->d.nxp * ctx->d.nyp;
     for (int t = 0; t < 3; ++t) {
         double* dst = ctx->f[MDX_COEF_U + t];
         if (src[t]) {
             for (size_t q = 0; q < n && !any; ++q) any = (src[t][q] != 0.0);
+            // geometry that depends on x and y only gives equal z planes
+            for (size_t q = plane; q < n && zinv; ++q) zinv = (src[t][q] == src[t][q % plane]);
             MDX_CUDA(ctx, cudaMemcpyAsync(dst, src[t], sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
         } else {
             MDX_CUDA(ctx, cudaMemsetAsync(dst, 0, sizeof(double) * n, ctx->stream));
@@ -329,6 +351,7 @@ int mdx_enter_ibm_data(mdx_ctx_t* ctx, const double* cu, const double* cv, const
     }
     MDX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     ctx->ibm_zero = !any;
+    ctx->coef_zinv = zinv;
     return MDX_OK;
 }
 

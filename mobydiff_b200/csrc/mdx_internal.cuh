@@ -74,6 +74,10 @@ struct mdx_ctx {
     bool solver = false;
     double* f[MDX_NUM_FIELDS] = {nullptr};   // device mirrors (MDX_PHI -> phi)
     bool ibm_zero = true;                    // all IBM coefficients zero
+    bool coef_zinv = false;                  // coefficients equal on every z plane
+    double* mu = nullptr;                    // red-black IBM factors 1/(1+dt_gamma*coef)
+    long long mu_elems = 0;
+    int mu_mode = 0;
 
     // FFT workspace
     double2* spec = nullptr;                 // (nxh, nz, ny)
