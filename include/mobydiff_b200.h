@@ -266,9 +266,12 @@ int mdx_channel_ic(mdx_ctx_t* ctx, uint64_t seed, double amp_u, double amp_vw, d
  * (synchronises). */
 int mdx_divergence_norms(mdx_ctx_t* ctx, double* l2, double* linf);
 
-/* Per-kernel-class device timing with CUDA events on the context stream. */
+/* Per-kernel-class device timing with CUDA events on the context stream:
+ * every 8th launch of a class is bracketed by an event pair; get_timing
+ * reports the launches of each class since set_timing(1) and their total
+ * time estimated as launches x the sampled mean (synchronises). */
 int mdx_set_timing(mdx_ctx_t* ctx, int on);
-int mdx_get_timing(mdx_ctx_t* ctx, mdx_timing_t* out);   /* synchronises; accumulated since set_timing(1) */
+int mdx_get_timing(mdx_ctx_t* ctx, mdx_timing_t* out);
 
 /* Number of kernel launches issued by the library on this context so far. */
 long long mdx_launch_count(const mdx_ctx_t* ctx);

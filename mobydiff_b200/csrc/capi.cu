@@ -40,10 +40,18 @@ static cudaEvent_t ev_get(mdx_ctx_t* ctx) {
     return e;
 }
 
-static void timing_resolve(mdx_ctx_t* ctx) {
+// Fold completed event pairs into the per-class sums; with `wait` the stream
+// is drained first so that every pending pair completes.
+static void timing_resolve(mdx_ctx_t* ctx, bool wait) {
     if (ctx->ev_pending.empty()) return;
-    cudaStreamSynchronize(ctx->stream);
-    for (auto& p : ctx->ev_pending) {
+    if (wait) cudaStreamSynchronize(ctx->stream);
+    size_t keep = 0;
+    for (size_t q = 0; q < ctx->ev_pending.size(); ++q) {
+        mdx_event_pair& p = ctx->ev_pending[q];
+        if (!wait && cudaEventQuery(p.b) != cudaSuccess) {
+            ctx->ev_pending[keep++] = p;
+            continue;
+        }
         float ms = 0.f;
         if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
             ctx->tim.ms[p.cls] += ms;
@@ -52,14 +60,21 @@ static void timing_resolve(mdx_ctx_t* ctx) {
         ctx->ev_free.push_back(p.a);
         ctx->ev_free.push_back(p.b);
     }
-    ctx->ev_pending.clear();
+    ctx->ev_pending.resize(keep);
 }
+
+// Every MDX_TIMING_STRIDE-th launch of a class is bracketed by events, so
+// that timing a long run costs little host time; get_timing scales the
+// sampled mean to all launches of the class.
+#define MDX_TIMING_STRIDE 8
 
 void mdx_timer_begin(mdx_ctx_t* ctx, int cls, mdx_event_pair* p) {
     p->a = p->b = nullptr;
     p->cls = cls;
     if (!ctx->timing || ctx->capturing) return;
-    if (ctx->ev_pending.size() >= 8192) timing_resolve(ctx);
+    if ((ctx->tim_issued[cls]++) % MDX_TIMING_STRIDE != 0) return;
+    if (ctx->ev_pending.size() >= 4096) timing_resolve(ctx, false);
+    if (ctx->ev_pending.size() >= 16384) timing_resolve(ctx, true);
     p->a = ev_get(ctx);
     p->b = ev_get(ctx);
     cudaEventRecord(p->a, ctx->stream);
@@ -562,16 +577,22 @@ int mdx_channel_ic(mdx_ctx_t* ctx, uint64_t seed, double amp_u, double amp_vw, d
 
 int mdx_set_timing(mdx_ctx_t* ctx, int on) {
     if (!ctx) return mdx_fail(nullptr, MDX_ERR_ARG, "null context");
-    timing_resolve(ctx);
+    timing_resolve(ctx, true);
     std::memset(&ctx->tim, 0, sizeof(ctx->tim));
+    std::memset(ctx->tim_issued, 0, sizeof(ctx->tim_issued));
     ctx->timing = on != 0;
     return MDX_OK;
 }
 
 int mdx_get_timing(mdx_ctx_t* ctx, mdx_timing_t* out) {
     if (!ctx || !out) return mdx_fail(ctx, MDX_ERR_ARG, "null argument");
-    timing_resolve(ctx);
-    *out = ctx->tim;
+    timing_resolve(ctx, true);
+    // scale the sampled launches' mean to every launch of the class
+    for (int c = 0; c < MDX_T_NUM; ++c) {
+        const long long timed = ctx->tim.launches[c];
+        out->launches[c] = ctx->tim_issued[c];
+        out->ms[c] = timed > 0 ? ctx->tim.ms[c] * (double)ctx->tim_issued[c] / (double)timed : 0.0;
+    }
     return MDX_OK;
 }
 

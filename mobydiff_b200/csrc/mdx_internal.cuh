@@ -105,7 +105,8 @@ struct mdx_ctx {
     bool timing = false;
     std::vector<mdx_event_pair> ev_pending;
     std::vector<cudaEvent_t> ev_free;
-    mdx_timing_t tim{};
+    mdx_timing_t tim{};                      // sums over the sampled launches
+    long long tim_issued[MDX_T_NUM] = {0};   // launches per class since set_timing(1)
     long long launches = 0;
     bool capturing = false;
 };
