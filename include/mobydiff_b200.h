@@ -90,7 +90,10 @@ typedef struct {
     int max_iter;      /* red-black: iteration cap when tol > 0               */
     int check_every;   /* red-black: iterations between residual checks       */
     int precision;     /* MDX_PREC_*                                          */
-    int reserved_i[7];
+    int sor_variant;   /* red-black kernels: 0 auto (one fused pass per red+black
+                          iteration when x and z are periodic), 1 one launch per colour */
+    int sor_kz;        /* z planes per block of the fused pass (0: default 16) */
+    int reserved_i[5];
     double atol;       /* red-black: absolute floor of ||div u||2, also accepted as converged.
                           < 0 (default): the FP64 round-off level of the divergence,
                           eps*sqrt(nx*ny*nz)*max|u*|*(1/dx+1/dy+1/dz); 0: none */

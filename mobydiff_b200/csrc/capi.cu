@@ -232,6 +232,10 @@ int mdx_exit_field_data(mdx_ctx_t* ctx) {
         cudaFree(ctx->f[f]);
         ctx->f[f] = nullptr;
     }
+    for (int t = 0; t < 4; ++t) {   // the fused red-black pass swaps these with the field mirrors
+        cudaFree(ctx->sor_alt[t]);
+        ctx->sor_alt[t] = nullptr;
+    }
     ctx->fields = false;
     return MDX_OK;
 }

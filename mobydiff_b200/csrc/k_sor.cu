@@ -38,6 +38,85 @@ __global__ void k_mu_tables(long long n, long long stride_in, double dg, const d
     (void)stride_in;
 }
 
+// The update of one cell, pressure_redblack.f90:117-241, on register copies
+// of its six faces and p.  In the reference's one-sided boundary formulas
+// un(nx,j,k), vn(i,j,k) and wn(i,j,nz) are the cell's own u_i, v_j, w_k
+// (those branches run only for i = nx, j = ny, k = nz).
+__device__ __forceinline__ void sor_cell(double& u_i, double& u_ip, double& v_j, double& v_jp, double& w_k,
+                                         double& w_kp, double& pc, double mu_u_i, double mu_u_ip, double mu_v_j,
+                                         double mu_v_jp, double mu_w_k, double mu_w_kp, const mdx_sor_params& p,
+                                         const mdx_bc_dev& bc, int i, int j, int k, int nx, int ny, int nz) {
+    const int* T = bc.type;
+    const double* V = bc.value;
+    const bool perx = bc.per[0] != 0, pery = bc.per[1] != 0, perz = bc.per[2] != 0;
+    const double denom = (mu_u_i + mu_u_ip) * p.idx2 + (mu_w_k + mu_w_kp) * p.idz2 + (mu_v_j + mu_v_jp) * p.idy2;
+    if (!perx) {  // :128-144
+        if (i < 2) {
+            if (T[bci(1, 0, 1)] == 0) u_i = V[bci(1, 0, 1)];
+            else u_i = u_ip - V[bci(1, 0, 1)] * p.dx;
+        }
+        if (i >= nx) {
+            if (T[bci(1, 1, 1)] == 0) u_ip = V[bci(1, 1, 1)];
+            else u_ip = u_i + V[bci(1, 1, 1)] * p.dx;
+        }
+    }
+    if (!pery) {  // :146-162
+        if (j < 2) {
+            if (T[bci(2, 0, 2)] == 0) v_j = V[bci(2, 0, 2)];
+            else v_j = v_jp - V[bci(2, 0, 2)] * p.dy;
+        }
+        if (j >= ny) {
+            if (T[bci(2, 1, 2)] == 0) v_jp = V[bci(2, 1, 2)];
+            else v_jp = v_j + V[bci(2, 1, 2)] * p.dy;
+        }
+    }
+    if (!perz) {  // :164-180
+        if (k < 2) {
+            if (T[bci(3, 0, 3)] == 0) w_k = V[bci(3, 0, 3)];
+            else w_k = w_kp - V[bci(3, 0, 3)] * p.dz;
+        }
+        if (k >= nz) {
+            if (T[bci(3, 1, 3)] == 0) w_kp = V[bci(3, 1, 3)];
+            else w_kp = w_k + V[bci(3, 1, 3)] * p.dz;
+        }
+    }
+    // :183-188
+    const double phi = ((u_ip - u_i) * p.idx + (v_jp - v_j) * p.idy + (w_kp - w_k) * p.idz) * (-p.sor / denom);
+    pc = pc + phi * p.idt;
+    // :190-241
+    u_i = u_i - phi * p.idx * mu_u_i;
+    if (!perx && i == 1) {
+        if (T[bci(1, 0, 0)] == 0) u_i = u_i + V[bci(1, 0, 0)] * p.idx * mu_u_i;
+        else u_i = u_i + (phi * p.idx - V[bci(1, 0, 0)]) * mu_u_i;
+    }
+    u_ip = u_ip + phi * p.idx * mu_u_ip;
+    if (!perx && i == nx) {
+        if (T[bci(1, 1, 0)] == 0) u_ip = u_ip - V[bci(1, 1, 0)] * p.idx * mu_u_ip;
+        else u_ip = u_ip + (V[bci(1, 1, 0)] - phi * p.idx) * mu_u_ip;
+    }
+    v_j = v_j - phi * p.idy * mu_v_j;
+    if (!pery && j == 1) {
+        if (T[bci(2, 0, 0)] == 0) v_j = v_j + V[bci(2, 0, 0)] * p.idy * mu_v_j;
+        else v_j = v_j + (phi * p.idy - V[bci(2, 0, 0)]) * mu_v_j;
+    }
+    v_jp = v_jp + phi * p.idy * mu_v_jp;
+    if (!pery && j == ny) {
+        if (T[bci(2, 1, 0)] == 0) v_jp = v_jp - V[bci(2, 1, 0)] * p.idy * mu_v_jp;
+        else v_jp = v_jp + (V[bci(2, 1, 0)] - phi * p.idy) * mu_v_jp;
+    }
+    w_k = w_k - phi * p.idz * mu_w_k;
+    if (!perz && k == 1) {
+        if (T[bci(3, 0, 0)] == 0) w_k = w_k + V[bci(3, 0, 0)] * p.idz * mu_w_k;
+        else w_k = w_k + (phi * p.idz - V[bci(3, 0, 0)]) * mu_w_k;
+    }
+    w_kp = w_kp + phi * p.idz * mu_w_kp;
+    if (!perz && k == nz) {
+        // :237 -- the Dirichlet branch of the reference has no mu factor
+        if (T[bci(3, 1, 0)] == 0) w_kp = w_kp - V[bci(3, 1, 0)] * p.idz;
+        else w_kp = w_kp + (V[bci(3, 1, 0)] - phi * p.idz) * mu_w_kp;
+    }
+}
+
 template <int MU>
 __global__ void __launch_bounds__(256)
 k_sor_sweep(mdx_dims d, mdx_bc_dev bc, mdx_sor_params p, int parity, int reverse, double* __restrict__ un,
@@ -84,80 +163,165 @@ k_sor_sweep(mdx_dims d, mdx_bc_dev bc, mdx_sor_params p, int parity, int reverse
         mu_w_k = __ldg(mu + 2 * np + c);
         mu_w_kp = __ldg(mu + 2 * np + ckp);
     }
-    const double denom = (mu_u_i + mu_u_ip) * p.idx2 + (mu_w_k + mu_w_kp) * p.idz2 + (mu_v_j + mu_v_jp) * p.idy2;
-
-    if (!perx) {  // :128-144
-        if (i < 2) {
-            if (T[bci(1, 0, 1)] == 0) un[c] = V[bci(1, 0, 1)];
-            else un[c] = un[cip] - V[bci(1, 0, 1)] * p.dx;
-        }
-        if (i >= nx) {
-            if (T[bci(1, 1, 1)] == 0) un[cip] = V[bci(1, 1, 1)];
-            else un[cip] = un[pidx(d, nx, j, k)] + V[bci(1, 1, 1)] * p.dx;
-        }
-    }
-    if (!pery) {  // :146-162
-        if (j < 2) {
-            if (T[bci(2, 0, 2)] == 0) vn[c] = V[bci(2, 0, 2)];
-            else vn[c] = vn[cjp] - V[bci(2, 0, 2)] * p.dy;
-        }
-        if (j >= ny) {
-            if (T[bci(2, 1, 2)] == 0) vn[cjp] = V[bci(2, 1, 2)];
-            else vn[cjp] = vn[c] + V[bci(2, 1, 2)] * p.dy;
-        }
-    }
-    if (!perz) {  // :164-180
-        if (k < 2) {
-            if (T[bci(3, 0, 3)] == 0) wn[c] = V[bci(3, 0, 3)];
-            else wn[c] = wn[ckp] - V[bci(3, 0, 3)] * p.dz;
-        }
-        if (k >= nz) {
-            if (T[bci(3, 1, 3)] == 0) wn[ckp] = V[bci(3, 1, 3)];
-            else wn[ckp] = wn[c] + V[bci(3, 1, 3)] * p.dz;
-        }
-    }
-    double u_i = un[c], u_ip = un[cip], v_j = vn[c], v_jp = vn[cjp], w_k = wn[c], w_kp = wn[ckp];
-    // :183-188
-    const double phi = ((u_ip - u_i) * p.idx + (v_jp - v_j) * p.idy + (w_kp - w_k) * p.idz) * (-p.sor / denom);
-    pn[c] = pn[c] + phi * p.idt;
-    // :190-241
-    u_i = u_i - phi * p.idx * mu_u_i;
-    if (!perx && i == 1) {
-        if (T[bci(1, 0, 0)] == 0) u_i = u_i + V[bci(1, 0, 0)] * p.idx * mu_u_i;
-        else u_i = u_i + (phi * p.idx - V[bci(1, 0, 0)]) * mu_u_i;
-    }
+    double u_i = un[c], u_ip = un[cip], v_j = vn[c], v_jp = vn[cjp], w_k = wn[c], w_kp = wn[ckp], pc = pn[c];
+    sor_cell(u_i, u_ip, v_j, v_jp, w_k, w_kp, pc, mu_u_i, mu_u_ip, mu_v_j, mu_v_jp, mu_w_k, mu_w_kp, p, bc, i, j, k,
+             nx, ny, nz);
     un[c] = u_i;
-    u_ip = u_ip + phi * p.idx * mu_u_ip;
-    if (!perx && i == nx) {
-        if (T[bci(1, 1, 0)] == 0) u_ip = u_ip - V[bci(1, 1, 0)] * p.idx * mu_u_ip;
-        else u_ip = u_ip + (V[bci(1, 1, 0)] - phi * p.idx) * mu_u_ip;
-    }
     un[cip] = u_ip;
-    v_j = v_j - phi * p.idy * mu_v_j;
-    if (!pery && j == 1) {
-        if (T[bci(2, 0, 0)] == 0) v_j = v_j + V[bci(2, 0, 0)] * p.idy * mu_v_j;
-        else v_j = v_j + (phi * p.idy - V[bci(2, 0, 0)]) * mu_v_j;
-    }
     vn[c] = v_j;
-    v_jp = v_jp + phi * p.idy * mu_v_jp;
-    if (!pery && j == ny) {
-        if (T[bci(2, 1, 0)] == 0) v_jp = v_jp - V[bci(2, 1, 0)] * p.idy * mu_v_jp;
-        else v_jp = v_jp + (V[bci(2, 1, 0)] - phi * p.idy) * mu_v_jp;
-    }
     vn[cjp] = v_jp;
-    w_k = w_k - phi * p.idz * mu_w_k;
-    if (!perz && k == 1) {
-        if (T[bci(3, 0, 0)] == 0) w_k = w_k + V[bci(3, 0, 0)] * p.idz * mu_w_k;
-        else w_k = w_k + (phi * p.idz - V[bci(3, 0, 0)]) * mu_w_k;
-    }
     wn[c] = w_k;
-    w_kp = w_kp + phi * p.idz * mu_w_kp;
-    if (!perz && k == nz) {
-        // :237 -- the Dirichlet branch of the reference has no mu factor
-        if (T[bci(3, 1, 0)] == 0) w_kp = w_kp - V[bci(3, 1, 0)] * p.idz;
-        else w_kp = w_kp + (V[bci(3, 1, 0)] - phi * p.idz) * mu_w_kp;
-    }
     wn[ckp] = w_kp;
+    pn[c] = pc;
+    (void)T;
+    (void)V;
+}
+
+// ---------------------------------------------------------------------------
+// One full red+black iteration in one pass (periodic x and z).
+//
+// Each block owns the cells of a TX x TY tile in x-y and a chunk of KZ z
+// planes.  It walks its z range with a ring of three planes in shared
+// memory holding u, v, w, p of the tile plus a two-cell halo ring in x and
+// y.  On plane q it runs the red update on every red cell of the halo
+// region, then the black update of plane q-1 on the tile plus a one-cell
+// ring, then writes the owned faces of plane q-1 (u(i), v(j), w(k) and p of
+// the tile cells; v(ny+1) for a y wall).  All reads come from the old state
+// (u0..p0) and all writes go to the new state (u1..p1), so blocks never
+// see each other's updates; red cells of the halo are recomputed from the
+// same old values their owners use, so every face ends with exactly the
+// value of a red sweep followed by a black sweep.  The state crosses HBM
+// once per iteration instead of twice.
+// ---------------------------------------------------------------------------
+template <int MU, int TX, int TY>
+__global__ void __launch_bounds__(256)
+k_sor_fused(mdx_dims d, mdx_bc_dev bc, mdx_sor_params P, int KZ, const double* __restrict__ u0,
+            const double* __restrict__ v0, const double* __restrict__ w0, const double* __restrict__ p0,
+            double* __restrict__ u1, double* __restrict__ v1, double* __restrict__ w1, double* __restrict__ p1,
+            const double* __restrict__ mu) {
+    constexpr int WX = TX + 3, WY = TY + 3;   // halo: x in [x0-2, x0+TX], y in [y0-2, y0+TY]
+    constexpr int UX = WX + 1;                // u rows also hold the right face of the last cell
+    constexpr int NU = WY * UX, NV = (WY + 1) * WX, NC = WY * WX;
+    constexpr int SLOT = NU + NV + 2 * NC;
+    constexpr int HX = (WX + 1) / 2;
+    extern __shared__ double sm[];
+    double* smu = sm + 3 * SLOT;              // mu_u (NU), mu_v (NV), mu_w (NC)
+    int* gxt = (int*)(smu + (MU == MU_PLANE ? NU + NV + NC : 0));   // global x of local column (UX)
+    int* gyt = gxt + UX;                                             // global y of local row (WY+1), -1 outside
+
+    const int nx = d.nx, ny = d.ny, nz = d.nz;
+    const bool pery = bc.per[1] != 0;
+    const int x0 = blockIdx.x * TX + 1, y0 = blockIdx.y * TY + 1;
+    const int k0 = blockIdx.z * KZ + 1;
+    const int k1 = min(k0 + KZ, nz + 1);
+    const int tid = threadIdx.x;
+
+    for (int t = tid; t < UX; t += blockDim.x) gxt[t] = ((x0 - 2 + t - 1) % nx + nx) % nx + 1;
+    for (int t = tid; t <= WY; t += blockDim.x) {
+        int g = y0 - 2 + t;
+        if (pery) g = ((g - 1) % ny + ny) % ny + 1;
+        else if (g < 0 || g > ny + 1) g = -1;
+        gyt[t] = g;
+    }
+    __syncthreads();
+    const long long np = (long long)d.nxp * d.nyp;
+    if (MU == MU_PLANE) {
+        for (int t = tid; t < NU; t += blockDim.x) {
+            const int ly = t / UX, lx = t - ly * UX, gy = gyt[ly];
+            smu[t] = gy >= 0 ? __ldg(mu + gxt[lx] + (long long)d.nxp * gy) : 1.0;
+        }
+        for (int t = tid; t < NV; t += blockDim.x) {
+            const int ly = t / WX, lx = t - ly * WX, gy = gyt[ly];
+            smu[NU + t] = gy >= 0 ? __ldg(mu + np + gxt[lx] + (long long)d.nxp * gy) : 1.0;
+        }
+        for (int t = tid; t < NC; t += blockDim.x) {
+            const int ly = t / WX, lx = t - ly * WX, gy = gyt[ly];
+            smu[NU + NV + t] = gy >= 0 ? __ldg(mu + 2 * np + gxt[lx] + (long long)d.nxp * gy) : 1.0;
+        }
+    }
+
+    auto wrapz = [&](int q) { return ((q - 1) % nz + nz) % nz + 1; };
+    auto slot = [&](int q) { return sm + ((q - k0 + 2) % 3) * SLOT; };
+    auto load = [&](int q) {
+        double* s = slot(q);
+        const int gk = wrapz(q);
+        for (int t = tid; t < NU; t += blockDim.x) {
+            const int ly = t / UX, lx = t - ly * UX, gy = gyt[ly];
+            s[t] = gy >= 0 ? __ldg(u0 + pidx(d, gxt[lx], gy, gk)) : 0.0;
+        }
+        for (int t = tid; t < NV; t += blockDim.x) {
+            const int ly = t / WX, lx = t - ly * WX, gy = gyt[ly];
+            s[NU + t] = gy >= 0 ? __ldg(v0 + pidx(d, gxt[lx], gy, gk)) : 0.0;
+        }
+        for (int t = tid; t < NC; t += blockDim.x) {
+            const int ly = t / WX, lx = t - ly * WX, gy = gyt[ly];
+            const long long c = gy >= 0 ? pidx(d, gxt[lx], gy, gk) : 0;
+            s[NU + NV + t] = gy >= 0 ? __ldg(w0 + c) : 0.0;
+            s[NU + NV + NC + t] = gy >= 0 ? __ldg(p0 + c) : 0.0;
+        }
+    };
+    // Update the cells of colour `odd` ((i+j+k) odd: red) on plane q within
+    // local rows [ly0, ly1) and columns [lx0, lx1).
+    auto update = [&](int q, int odd, int lx0, int lx1, int ly0, int ly1) {
+        double* s = slot(q);
+        double* sn = slot(q + 1);
+        double* su = s;
+        double* sv = s + NU;
+        double* sw = s + NU + NV;
+        double* sp = s + NU + NV + NC;
+        double* swn = sn + NU + NV;
+        const int gk = wrapz(q);
+        const int rows = ly1 - ly0;
+        for (int t = tid; t < rows * HX; t += blockDim.x) {
+            const int ly = ly0 + t / HX;
+            const int gy = gyt[ly];
+            if (gy < 1 || gy > ny) continue;
+            // first column of the wanted colour: (x0-2+lx) + gy + gk must have
+            // the parity `odd`, i.e. lx = odd + x0 + gy + gk (mod 2)
+            const int off = ((x0 + lx0 + gy + gk + odd) & 1);
+            const int lx = lx0 + off + 2 * (t % HX);
+            if (lx >= lx1) continue;
+            const int gx = gxt[lx];
+            double mu_u_i = 1.0, mu_u_ip = 1.0, mu_v_j = 1.0, mu_v_jp = 1.0, mu_w = 1.0;
+            if (MU == MU_PLANE) {
+                mu_u_i = smu[ly * UX + lx];
+                mu_u_ip = smu[ly * UX + lx + 1];
+                mu_v_j = smu[NU + ly * WX + lx];
+                mu_v_jp = smu[NU + (ly + 1) * WX + lx];
+                mu_w = smu[NU + NV + ly * WX + lx];
+            }
+            sor_cell(su[ly * UX + lx], su[ly * UX + lx + 1], sv[ly * WX + lx], sv[(ly + 1) * WX + lx],
+                     sw[ly * WX + lx], swn[ly * WX + lx], sp[ly * WX + lx], mu_u_i, mu_u_ip, mu_v_j, mu_v_jp, mu_w,
+                     mu_w, P, bc, gx, gy, gk, nx, ny, nz);
+        }
+    };
+    auto store = [&](int q) {
+        double* s = slot(q);
+        const int gk = wrapz(q);
+        for (int t = tid; t < TX * TY; t += blockDim.x) {
+            const int ly = 2 + t / TX, lx = 2 + t % TX;
+            const int gxu = x0 + lx - 2, gyu = y0 + ly - 2;   // owned cells: no wrap
+            if (gxu > nx || gyu > ny) continue;
+            const long long c = pidx(d, gxu, gyu, gk);
+            u1[c] = s[ly * UX + lx];
+            v1[c] = s[NU + ly * WX + lx];
+            w1[c] = s[NU + NV + ly * WX + lx];
+            p1[c] = s[NU + NV + NC + ly * WX + lx];
+            if (!pery && gyu == ny) v1[pidx(d, gxu, ny + 1, gk)] = s[NU + (ly + 1) * WX + lx];
+        }
+    };
+
+    load(k0 - 2);
+    for (int q = k0 - 2; q <= k1; ++q) {
+        load(q + 1);
+        __syncthreads();
+        update(q, 1, 0, WX, 0, WY);                    // red on the halo region of plane q
+        __syncthreads();
+        if (q - 1 >= k0 - 1) update(q - 1, 0, 1, WX - 1, 1, WY - 1);   // black on the tile + 1 ring
+        __syncthreads();
+        if (q - 1 >= k0) store(q - 1);
+        __syncthreads();
+    }
 }
 
 double mdx_div_floor(const mdx_ctx_t* ctx, double umax) {
@@ -199,6 +363,65 @@ static int sor_iteration(mdx_ctx_t* ctx, const mdx_sor_params& p) {
     return MDX_OK;
 }
 
+// ---- fused red+black iterations ---------------------------------------------
+#define MDX_FUSED_TX 32
+#define MDX_FUSED_TY 8
+
+template <int MU>
+static size_t fused_smem() {
+    constexpr int WX = MDX_FUSED_TX + 3, WY = MDX_FUSED_TY + 3, UX = WX + 1;
+    constexpr int NU = WY * UX, NV = (WY + 1) * WX, NC = WY * WX;
+    constexpr int SLOT = NU + NV + 2 * NC;
+    return sizeof(double) * (3 * SLOT + (MU == MU_PLANE ? NU + NV + NC : 0)) + sizeof(int) * (UX + WY + 1);
+}
+
+static bool use_fused(const mdx_ctx_t* ctx) {
+    if (ctx->opts.sor_variant == 1) return false;
+    return ctx->bc.is_periodic[0] && ctx->bc.is_periodic[2] && ctx->mu_mode != MU_FULL;
+}
+
+static int fused_prepare(mdx_ctx_t* ctx) {
+    const size_t bytes = sizeof(double) * ctx->d.npad;
+    for (int t = 0; t < 4; ++t)
+        if (!ctx->sor_alt[t]) MDX_CUDA(ctx, cudaMalloc(&ctx->sor_alt[t], bytes));
+    // the second state starts as a copy, so faces the sweeps never touch
+    // (ghosts) are equal in both
+    const int ids[4] = {MDX_UN, MDX_VN, MDX_WN, MDX_PN};
+    for (int t = 0; t < 4; ++t)
+        MDX_CUDA(ctx, cudaMemcpyAsync(ctx->sor_alt[t], ctx->f[ids[t]], bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    if (!ctx->fused_attr) {
+        MDX_CUDA(ctx, cudaFuncSetAttribute(k_sor_fused<MU_ONE, MDX_FUSED_TX, MDX_FUSED_TY>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fused_smem<MU_ONE>()));
+        MDX_CUDA(ctx, cudaFuncSetAttribute(k_sor_fused<MU_PLANE, MDX_FUSED_TX, MDX_FUSED_TY>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fused_smem<MU_PLANE>()));
+        ctx->fused_attr = true;
+    }
+    return MDX_OK;
+}
+
+static int sor_fused_iteration(mdx_ctx_t* ctx, const mdx_sor_params& p) {
+    const mdx_dims& d = ctx->d;
+    double** f = ctx->f;
+    const int KZ = ctx->opts.sor_kz > 0 ? ctx->opts.sor_kz : 16;
+    dim3 grid((d.nx + MDX_FUSED_TX - 1) / MDX_FUSED_TX, (d.ny + MDX_FUSED_TY - 1) / MDX_FUSED_TY, (d.nz + KZ - 1) / KZ);
+    double** a = ctx->sor_alt;
+    if (ctx->mu_mode == MU_PLANE) {
+        auto kfn = k_sor_fused<MU_PLANE, MDX_FUSED_TX, MDX_FUSED_TY>;
+        MDX_LAUNCH(ctx, MDX_T_SOR_SWEEP, "sor fused", kfn, grid, 256, fused_smem<MU_PLANE>(), d, ctx->bcd, p, KZ,
+                   f[MDX_UN], f[MDX_VN], f[MDX_WN], f[MDX_PN], a[0], a[1], a[2], a[3], ctx->mu);
+    } else {
+        auto kfn = k_sor_fused<MU_ONE, MDX_FUSED_TX, MDX_FUSED_TY>;
+        MDX_LAUNCH(ctx, MDX_T_SOR_SWEEP, "sor fused", kfn, grid, 256, fused_smem<MU_ONE>(), d, ctx->bcd, p, KZ,
+                   f[MDX_UN], f[MDX_VN], f[MDX_WN], f[MDX_PN], a[0], a[1], a[2], a[3], ctx->mu);
+    }
+    // the new state becomes the current one
+    std::swap(f[MDX_UN], a[0]);
+    std::swap(f[MDX_VN], a[1]);
+    std::swap(f[MDX_WN], a[2]);
+    std::swap(f[MDX_PN], a[3]);
+    return MDX_OK;
+}
+
 // The IBM factors of this projection's dt_gamma.
 static int mu_tables(mdx_ctx_t* ctx, double dg) {
     const mdx_dims& d = ctx->d;
@@ -230,11 +453,13 @@ int mdx_k_projection_redblack(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t* st) 
     MDX_CUDA(ctx, cudaMemcpyAsync(f[MDX_VN], f[MDX_VS], bytes, cudaMemcpyDeviceToDevice, ctx->stream));
     MDX_CUDA(ctx, cudaMemcpyAsync(f[MDX_WN], f[MDX_WS], bytes, cudaMemcpyDeviceToDevice, ctx->stream));
     MDX_TRY(mu_tables(ctx, dg));
+    const bool fused = use_fused(ctx);
+    if (fused) MDX_TRY(fused_prepare(ctx));
     const mdx_sor_params p = sor_params(ctx, dg);
     mdx_solve_stats_t s{};
     const mdx_solver_opts_t& o = ctx->opts;
     if (o.tol <= 0.0) {
-        for (int it = 0; it < o.n_iter; ++it) MDX_TRY(sor_iteration(ctx, p));
+        for (int it = 0; it < o.n_iter; ++it) MDX_TRY(fused ? sor_fused_iteration(ctx, p) : sor_iteration(ctx, p));
         s.iterations = o.n_iter;
         s.status = MDX_OK;
     } else {
@@ -258,7 +483,7 @@ int mdx_k_projection_redblack(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t* st) 
             r = r0;
             while (it < o.max_iter) {
                 const int m = std::min(o.check_every, o.max_iter - it);
-                for (int q = 0; q < m; ++q) MDX_TRY(sor_iteration(ctx, p));
+                for (int q = 0; q < m; ++q) MDX_TRY(fused ? sor_fused_iteration(ctx, p) : sor_iteration(ctx, p));
                 it += m;
                 MDX_TRY(mdx_k_div_norms(ctx, f[MDX_UN], f[MDX_VN], f[MDX_WN], &r, &linf));
                 if (!std::isfinite(r)) { s.status = MDX_ERR_NONFINITE; break; }

@@ -75,6 +75,8 @@ struct mdx_ctx {
     double* f[MDX_NUM_FIELDS] = {nullptr};   // device mirrors (MDX_PHI -> phi)
     bool ibm_zero = true;                    // all IBM coefficients zero
     bool coef_zinv = false;                  // coefficients equal on every z plane
+    double* sor_alt[4] = {nullptr};          // second u,v,w,p state of the fused red-black pass
+    bool fused_attr = false;
     double* mu = nullptr;                    // red-black IBM factors 1/(1+dt_gamma*coef)
     long long mu_elems = 0;
     int mu_mode = 0;

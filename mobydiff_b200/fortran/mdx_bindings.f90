@@ -28,7 +28,8 @@ module mdx_bindings
         integer(C_INT) :: solver, n_iter
         real(C_DOUBLE) :: sor, tol
         integer(C_INT) :: max_iter, check_every, precision
-        integer(C_INT) :: reserved_i(7)
+        integer(C_INT) :: sor_variant, sor_kz
+        integer(C_INT) :: reserved_i(5)
         real(C_DOUBLE) :: atol
         real(C_DOUBLE) :: reserved_d(7)
     end type mdx_solver_opts_t

@@ -21,11 +21,13 @@ def random_fields(g: O.Grid, seed: int, ibm: str = "none", scale=1.0) -> O.Field
         getattr(f, n)[...] = scale * rng.uniform(-1.0, 1.0, g.padded)
     for n in O.RHS_NAMES:
         getattr(f, n)[...] = scale * rng.uniform(-1.0, 1.0, g.interior)
-    if ibm == "random":
+    if ibm in ("random", "zinv"):
         for n in O.COEF_NAMES:
             c = rng.uniform(0.0, 50.0, g.padded)
             c[rng.uniform(size=g.padded) < 0.6] = 0.0
             c[rng.uniform(size=g.padded) < 0.05] = 1e30 / g.re
+            if ibm == "zinv":           # geometry depending on x and y only
+                c[...] = c[0:1]
             getattr(f, n)[...] = c
     elif ibm == "reference":
         O.set_ibm_coeff(g, O.ibm_reference(g), f)
