@@ -351,6 +351,10 @@ def run_ours(args, cfg):
                 "avg_launch_ms": avg_s * 1e3, "launches": kn, "share_of_step_time": share}
 
     iters_per_substage = iters / (3 * args.steps) if cfg["solver"] == "redblack" else 0
+    sor_kernel = None
+    if cfg["solver"] == "redblack":
+        names = {1: "one launch per colour sweep", 2: "fused red+black pass 32x8", 3: "fused red+black pass 32x16"}
+        sor_kernel = names.get(s.last_solve_stats().variant, "?")
 
     # ---- CPU baseline (rank 0, one GPU only) -------------------------------
     cpu = None
@@ -376,6 +380,7 @@ def run_ours(args, cfg):
                            "parallelism": f"replicas x{ws}",
                            "l2": "inputs larger than L2 (state + IBM coefficients > 126 MB)"},
                 "poisson_iters_per_substage": iters_per_substage,
+                "sor_kernel": sor_kernel,
                 "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
                 "e2e": e2e_line, "gpu_launches": launches}
         print(json.dumps(line), flush=True)

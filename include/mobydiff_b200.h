@@ -90,8 +90,11 @@ typedef struct {
     int max_iter;      /* red-black: iteration cap when tol > 0               */
     int check_every;   /* red-black: iterations between residual checks       */
     int precision;     /* MDX_PREC_*                                          */
-    int sor_variant;   /* red-black kernels: 0 auto (one fused pass per red+black
-                          iteration when x and z are periodic), 1 one launch per colour */
+    int sor_variant;   /* red-black kernels (bit-identical results): 0 auto -- the
+                          first projection times each variant on one residual-check
+                          block of its own iterations and keeps the fastest; 1 one
+                          launch per colour; 2 fused red+black pass, 32x8 tiles;
+                          3 fused pass, 32x16 tiles (fused: periodic x and z only) */
     int sor_kz;        /* z planes per block of the fused pass (0: default 16) */
     int reserved_i[5];
     double atol;       /* red-black: absolute floor of ||div u||2, also accepted as converged.
@@ -107,6 +110,8 @@ typedef struct {
     double residual;    /* final ||div u||2 / ||div u*||2 (red-black)        */
     double residual0;   /* ||div u*||2                                       */
     double atol;        /* absolute floor used (red-black)                   */
+    int variant;        /* red-black kernel variant of the last iterations   */
+    int reserved;
 } mdx_solve_stats_t;
 
 /* Per-kernel-class device time, filled when timing is on (mdx_set_timing). */
@@ -241,6 +246,10 @@ int mdx_destroy_pressure_solver(mdx_ctx_t* ctx);
 /* pressure_projection, src/modules/pressure_solver.f90:48-63.  stats may be
  * NULL; with stats or a residual tolerance the call synchronises. */
 int mdx_pressure_projection(mdx_ctx_t* ctx, double dt_gamma, mdx_solve_stats_t* stats);
+
+/* Statistics of the last pressure projection (including those run inside
+ * mdx_step). */
+int mdx_last_solve_stats(const mdx_ctx_t* ctx, mdx_solve_stats_t* stats);
 
 /* get_cfl, src/modules/step.f90:210-258 (synchronises). */
 int mdx_get_cfl(mdx_ctx_t* ctx, double* cfl);

@@ -85,7 +85,7 @@ class SolverOptsT(C.Structure):
 
 class SolveStatsT(C.Structure):
     _fields_ = [("iterations", C.c_int), ("status", C.c_int), ("residual", C.c_double), ("residual0", C.c_double),
-                ("atol", C.c_double)]
+                ("atol", C.c_double), ("variant", C.c_int), ("reserved", C.c_int)]
 
 
 class TimingT(C.Structure):
@@ -155,6 +155,7 @@ def lib():
         "mdx_set_timing": (i, [vp, i]),
         "mdx_get_timing": (i, [vp, P(TimingT)]),
         "mdx_launch_count": (C.c_longlong, [vp]),
+        "mdx_last_solve_stats": (i, [vp, P(SolveStatsT)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -406,6 +407,11 @@ class Solver:
 
     def launch_count(self) -> int:
         return lib().mdx_launch_count(self.h)
+
+    def last_solve_stats(self) -> SolveStatsT:
+        st = SolveStatsT()
+        self._c(lib().mdx_last_solve_stats(self.h, C.byref(st)))
+        return st
 
     def stream(self) -> int:
         s = C.c_void_p()

@@ -248,6 +248,8 @@ int mdx_destroy(mdx_ctx_t* ctx) {
     cudaFree(ctx->red_part);
     cudaFree(ctx->red_out);
     cudaFreeHost(ctx->red_host);
+    for (int t = 0; t < 2; ++t)
+        if (ctx->tune_ev[t]) cudaEventDestroy(ctx->tune_ev[t]);
     for (auto& p : ctx->ev_pending) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
     for (auto e : ctx->ev_free) cudaEventDestroy(e);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
@@ -265,6 +267,8 @@ int mdx_set_bc(mdx_ctx_t* ctx, const mdx_bc_t* bc) {
     ctx->bc = *bc;
     for (int t = 0; t < 3; ++t) ctx->bcd.per[t] = bc->is_periodic[t] ? 1 : 0;
     for (int t = 0; t < 24; ++t) { ctx->bcd.type[t] = bc->bc_type[t]; ctx->bcd.value[t] = bc->bc_value[t]; }
+    ctx->sor_tuned = 0;
+    for (int t = 0; t < 4; ++t) ctx->sor_tune_ms[t] = 0.0;
     return MDX_OK;
 }
 
@@ -414,6 +418,8 @@ int mdx_init_pressure_solver(mdx_ctx_t* ctx, const mdx_solver_opts_t* opts) {
     if (o.max_iter < 1) o.max_iter = 1;
     if (o.n_iter < 0) return mdx_fail(ctx, MDX_ERR_ARG, "n_iter must be >= 0");
     ctx->opts = o;
+    ctx->sor_tuned = 0;
+    for (int t = 0; t < 4; ++t) ctx->sor_tune_ms[t] = 0.0;
     MDX_TRY(mdx_reduce_init(ctx));
     if (o.solver == MDX_SOLVER_REDBLACK) {
         // src/modules/pressure/pressure_redblack.f90:16-18
@@ -450,6 +456,12 @@ int mdx_pressure_projection(mdx_ctx_t* ctx, double dt_gamma, mdx_solve_stats_t* 
     if (s.status == MDX_NOT_CONVERGED)
         return mdx_fail(ctx, MDX_NOT_CONVERGED, "red-black solve not converged after %d iterations (residual %.3e)",
                         s.iterations, s.residual);
+    return MDX_OK;
+}
+
+int mdx_last_solve_stats(const mdx_ctx_t* ctx, mdx_solve_stats_t* stats) {
+    if (!ctx || !stats) return mdx_fail(nullptr, MDX_ERR_ARG, "mdx_last_solve_stats: null argument");
+    *stats = ctx->last;
     return MDX_OK;
 }
 

@@ -38,18 +38,29 @@ __global__ void k_mu_tables(long long n, long long stride_in, double dg, const d
     (void)stride_in;
 }
 
-// The update of one cell, pressure_redblack.f90:117-241, on register copies
-// of its six faces and p.  In the reference's one-sided boundary formulas
-// un(nx,j,k), vn(i,j,k) and wn(i,j,nz) are the cell's own u_i, v_j, w_k
-// (those branches run only for i = nx, j = ny, k = nz).
-__device__ __forceinline__ void sor_cell(double& u_i, double& u_ip, double& v_j, double& v_jp, double& w_k,
-                                         double& w_kp, double& pc, double mu_u_i, double mu_u_ip, double mu_v_j,
-                                         double mu_v_jp, double mu_w_k, double mu_w_kp, const mdx_sor_params& p,
-                                         const mdx_bc_dev& bc, int i, int j, int k, int nx, int ny, int nz) {
+// -omega/denom of one cell, pressure_redblack.f90:124-126,186.
+__device__ __forceinline__ double sor_factor(double mu_u_i, double mu_u_ip, double mu_v_j, double mu_v_jp,
+                                             double mu_w_k, double mu_w_kp, const mdx_sor_params& p) {
+    const double denom = (mu_u_i + mu_u_ip) * p.idx2 + (mu_w_k + mu_w_kp) * p.idz2 + (mu_v_j + mu_v_jp) * p.idy2;
+    return -p.sor / denom;
+}
+
+// The update of one cell, pressure_redblack.f90:128-241, on register copies
+// of its six faces and p, given its factor -omega/denom.  In the reference's
+// one-sided boundary formulas un(nx,j,k), vn(i,j,k) and wn(i,j,nz) are the
+// cell's own u_i, v_j, w_k (those branches run only for i = nx, j = ny,
+// k = nz).  PX/PY/PZ: 1 periodic, 0 not, -1 read from bc at run time.
+template <int PX = -1, int PY = -1, int PZ = -1>
+__device__ __forceinline__ void sor_cell_fac(double& u_i, double& u_ip, double& v_j, double& v_jp, double& w_k,
+                                             double& w_kp, double& pc, double mu_u_i, double mu_u_ip, double mu_v_j,
+                                             double mu_v_jp, double mu_w_k, double mu_w_kp, double fac,
+                                             const mdx_sor_params& p, const mdx_bc_dev& bc, int i, int j, int k,
+                                             int nx, int ny, int nz) {
     const int* T = bc.type;
     const double* V = bc.value;
-    const bool perx = bc.per[0] != 0, pery = bc.per[1] != 0, perz = bc.per[2] != 0;
-    const double denom = (mu_u_i + mu_u_ip) * p.idx2 + (mu_w_k + mu_w_kp) * p.idz2 + (mu_v_j + mu_v_jp) * p.idy2;
+    const bool perx = PX >= 0 ? PX != 0 : bc.per[0] != 0;
+    const bool pery = PY >= 0 ? PY != 0 : bc.per[1] != 0;
+    const bool perz = PZ >= 0 ? PZ != 0 : bc.per[2] != 0;
     if (!perx) {  // :128-144
         if (i < 2) {
             if (T[bci(1, 0, 1)] == 0) u_i = V[bci(1, 0, 1)];
@@ -81,7 +92,7 @@ __device__ __forceinline__ void sor_cell(double& u_i, double& u_ip, double& v_j,
         }
     }
     // :183-188
-    const double phi = ((u_ip - u_i) * p.idx + (v_jp - v_j) * p.idy + (w_kp - w_k) * p.idz) * (-p.sor / denom);
+    const double phi = ((u_ip - u_i) * p.idx + (v_jp - v_j) * p.idy + (w_kp - w_k) * p.idz) * fac;
     pc = pc + phi * p.idt;
     // :190-241
     u_i = u_i - phi * p.idx * mu_u_i;
@@ -115,6 +126,16 @@ __device__ __forceinline__ void sor_cell(double& u_i, double& u_ip, double& v_j,
         if (T[bci(3, 1, 0)] == 0) w_kp = w_kp - V[bci(3, 1, 0)] * p.idz;
         else w_kp = w_kp + (V[bci(3, 1, 0)] - phi * p.idz) * mu_w_kp;
     }
+}
+
+// The whole update of one cell, pressure_redblack.f90:117-241.
+__device__ __forceinline__ void sor_cell(double& u_i, double& u_ip, double& v_j, double& v_jp, double& w_k,
+                                         double& w_kp, double& pc, double mu_u_i, double mu_u_ip, double mu_v_j,
+                                         double mu_v_jp, double mu_w_k, double mu_w_kp, const mdx_sor_params& p,
+                                         const mdx_bc_dev& bc, int i, int j, int k, int nx, int ny, int nz) {
+    const double fac = sor_factor(mu_u_i, mu_u_ip, mu_v_j, mu_v_jp, mu_w_k, mu_w_kp, p);
+    sor_cell_fac(u_i, u_ip, v_j, v_jp, w_k, w_kp, pc, mu_u_i, mu_u_ip, mu_v_j, mu_v_jp, mu_w_k, mu_w_kp, fac, p, bc,
+                 i, j, k, nx, ny, nz);
 }
 
 template <int MU>
@@ -181,146 +202,236 @@ k_sor_sweep(mdx_dims d, mdx_bc_dev bc, mdx_sor_params p, int parity, int reverse
 // One full red+black iteration in one pass (periodic x and z).
 //
 // Each block owns the cells of a TX x TY tile in x-y and a chunk of KZ z
-// planes.  It walks its z range with a ring of three planes in shared
-// memory holding u, v, w, p of the tile plus a two-cell halo ring in x and
-// y.  On plane q it runs the red update on every red cell of the halo
-// region, then the black update of plane q-1 on the tile plus a one-cell
-// ring, then writes the owned faces of plane q-1 (u(i), v(j), w(k) and p of
-// the tile cells; v(ny+1) for a y wall).  All reads come from the old state
-// (u0..p0) and all writes go to the new state (u1..p1), so blocks never
-// see each other's updates; red cells of the halo are recomputed from the
-// same old values their owners use, so every face ends with exactly the
-// value of a red sweep followed by a black sweep.  The state crosses HBM
-// once per iteration instead of twice.
+// planes.  It walks its z range with a ring of four planes in shared memory
+// holding u, v, w, p of the tile plus a two-cell halo ring in x and y; the
+// plane two ahead is fetched with cp.async while the current ones compute.
+// On plane q it runs the red update on every red cell of the halo region,
+// then the black update of plane q-1 on the tile plus a one-cell ring, then
+// writes the owned faces of plane q-1 (u(i), v(j), w(k) and p of the tile
+// cells; v(ny+1) for a y wall).  All reads come from the old state (u0..p0)
+// and all writes go to the new state (u1..p1), so blocks never see each
+// other's updates; red cells of the halo are recomputed from the same old
+// values their owners use, so every face ends with exactly the value of a
+// red sweep followed by a black sweep.  The state crosses HBM once per
+// iteration instead of twice.
+//
+// Shared-memory rows store even columns then odd columns, so the cells of
+// one colour in a row (every other column) are contiguous: a warp's accesses
+// fall in distinct banks.
 // ---------------------------------------------------------------------------
-template <int MU, int TX, int TY>
-__global__ void __launch_bounds__(256)
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool valid) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    const int n = valid ? 8 : 0;   // 0 source bytes: the 8 destination bytes are zero-filled
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+template <int TX, int TY, int NTH>
+struct fused_geom {
+    static constexpr int NT = NTH;
+    static constexpr int WX = TX + 3, WY = TY + 3;   // halo: x in [x0-2, x0+TX], y in [y0-2, y0+TY]
+    static constexpr int UX = WX + 1;                // u rows also hold the right face of the last cell
+    static constexpr int H = (UX + 1) / 2;           // even columns, then odd columns
+    static constexpr int R = 2 * H;                  // row stride
+    static constexpr int NU = WY * R, NV = (WY + 1) * R, NC = WY * R;
+    static constexpr int SLOT = NU + NV + 2 * NC;
+    static constexpr int LU = WY * UX, LV = (WY + 1) * WX, LC = WY * WX;   // elements fetched per plane
+    static constexpr int LTOT = LU + LV + 2 * LC;
+    static constexpr int NLD = (LTOT + NT - 1) / NT;
+    static constexpr int HR = (WX + 1) / 2;          // red candidates per row
+    static constexpr int HB = (WX - 1) / 2;          // black candidates per row (columns 1..WX-2)
+    __device__ static __forceinline__ int col(int lx) { return (lx & 1) * H + (lx >> 1); }
+};
+
+template <int MU, int PY, int TX, int TY, int NTH>
+__global__ void __launch_bounds__(NTH)
 k_sor_fused(mdx_dims d, mdx_bc_dev bc, mdx_sor_params P, int KZ, const double* __restrict__ u0,
             const double* __restrict__ v0, const double* __restrict__ w0, const double* __restrict__ p0,
             double* __restrict__ u1, double* __restrict__ v1, double* __restrict__ w1, double* __restrict__ p1,
             const double* __restrict__ mu) {
-    constexpr int WX = TX + 3, WY = TY + 3;   // halo: x in [x0-2, x0+TX], y in [y0-2, y0+TY]
-    constexpr int UX = WX + 1;                // u rows also hold the right face of the last cell
-    constexpr int NU = WY * UX, NV = (WY + 1) * WX, NC = WY * WX;
-    constexpr int SLOT = NU + NV + 2 * NC;
-    constexpr int HX = (WX + 1) / 2;
+    using G = fused_geom<TX, TY, NTH>;
+    constexpr int NT = G::NT, WX = G::WX, WY = G::WY, UX = G::UX, R = G::R;
+    constexpr int NU = G::NU, NV = G::NV, NC = G::NC, SLOT = G::SLOT;
+    constexpr int LU = G::LU, LV = G::LV, LC = G::LC, LTOT = G::LTOT, NLD = G::NLD;
+    constexpr int HR = G::HR, HB = G::HB;
+    static_assert(WY * HR <= NT && (WY - 2) * HB <= NT && TX * TY <= NT, "one cell per thread per phase");
     extern __shared__ double sm[];
-    double* smu = sm + 3 * SLOT;              // mu_u (NU), mu_v (NV), mu_w (NC)
-    int* gxt = (int*)(smu + (MU == MU_PLANE ? NU + NV + NC : 0));   // global x of local column (UX)
-    int* gyt = gxt + UX;                                             // global y of local row (WY+1), -1 outside
+    double* smu = sm + 4 * SLOT;              // mu_u (NU), mu_v (NV), mu_w (NC)  [MU_PLANE]
+    double* sfac = smu + (MU == MU_PLANE ? NU + NV + NC : 0);   // -omega/denom per column (NC)
+    int* gxt = (int*)(sfac + NC);             // global x of local column (UX)
+    int* gyt = gxt + UX;                      // global y of local row (WY+1), -1 outside
 
     const int nx = d.nx, ny = d.ny, nz = d.nz;
-    const bool pery = bc.per[1] != 0;
     const int x0 = blockIdx.x * TX + 1, y0 = blockIdx.y * TY + 1;
     const int k0 = blockIdx.z * KZ + 1;
     const int k1 = min(k0 + KZ, nz + 1);
     const int tid = threadIdx.x;
+    const long long plane = (long long)d.nxp * d.nyp;
 
-    for (int t = tid; t < UX; t += blockDim.x) gxt[t] = ((x0 - 2 + t - 1) % nx + nx) % nx + 1;
-    for (int t = tid; t <= WY; t += blockDim.x) {
+    for (int t = tid; t < UX; t += NT) gxt[t] = ((x0 - 2 + t - 1) % nx + nx) % nx + 1;
+    for (int t = tid; t <= WY; t += NT) {
         int g = y0 - 2 + t;
-        if (pery) g = ((g - 1) % ny + ny) % ny + 1;
+        if (PY) g = ((g - 1) % ny + ny) % ny + 1;
         else if (g < 0 || g > ny + 1) g = -1;
         gyt[t] = g;
     }
     __syncthreads();
-    const long long np = (long long)d.nxp * d.nyp;
     if (MU == MU_PLANE) {
-        for (int t = tid; t < NU; t += blockDim.x) {
+        for (int t = tid; t < LU; t += NT) {
             const int ly = t / UX, lx = t - ly * UX, gy = gyt[ly];
-            smu[t] = gy >= 0 ? __ldg(mu + gxt[lx] + (long long)d.nxp * gy) : 1.0;
+            smu[ly * R + G::col(lx)] = gy >= 0 ? __ldg(mu + gxt[lx] + (long long)d.nxp * gy) : 1.0;
         }
-        for (int t = tid; t < NV; t += blockDim.x) {
+        for (int t = tid; t < LV; t += NT) {
             const int ly = t / WX, lx = t - ly * WX, gy = gyt[ly];
-            smu[NU + t] = gy >= 0 ? __ldg(mu + np + gxt[lx] + (long long)d.nxp * gy) : 1.0;
+            smu[NU + ly * R + G::col(lx)] = gy >= 0 ? __ldg(mu + plane + gxt[lx] + (long long)d.nxp * gy) : 1.0;
         }
-        for (int t = tid; t < NC; t += blockDim.x) {
+        for (int t = tid; t < LC; t += NT) {
             const int ly = t / WX, lx = t - ly * WX, gy = gyt[ly];
-            smu[NU + NV + t] = gy >= 0 ? __ldg(mu + 2 * np + gxt[lx] + (long long)d.nxp * gy) : 1.0;
+            smu[NU + NV + ly * R + G::col(lx)] =
+                gy >= 0 ? __ldg(mu + 2 * plane + gxt[lx] + (long long)d.nxp * gy) : 1.0;
         }
+        __syncthreads();
+    }
+    // -omega/denom of every column (:124-126,186); z-invariant in both modes
+    for (int t = tid; t < LC; t += NT) {
+        const int ly = t / WX, lx = t - ly * WX;
+        double mu_u_i = 1.0, mu_u_ip = 1.0, mu_v_j = 1.0, mu_v_jp = 1.0, mu_w = 1.0;
+        if (MU == MU_PLANE) {
+            mu_u_i = smu[ly * R + G::col(lx)];
+            mu_u_ip = smu[ly * R + G::col(lx + 1)];
+            mu_v_j = smu[NU + ly * R + G::col(lx)];
+            mu_v_jp = smu[NU + (ly + 1) * R + G::col(lx)];
+            mu_w = smu[NU + NV + ly * R + G::col(lx)];
+        }
+        sfac[ly * R + G::col(lx)] = sor_factor(mu_u_i, mu_u_ip, mu_v_j, mu_v_jp, mu_w, mu_w, P);
     }
 
-    auto wrapz = [&](int q) { return ((q - 1) % nz + nz) % nz + 1; };
-    auto slot = [&](int q) { return sm + ((q - k0 + 2) % 3) * SLOT; };
-    auto load = [&](int q) {
+    // Per-thread fetch descriptors: plane-relative global offset (-1 outside
+    // the domain: zero-filled) and the shared-memory index in a slot.
+    int ldoff[NLD], lddst[NLD];
+#pragma unroll
+    for (int m = 0; m < NLD; ++m) {
+        const int e = tid + m * NT;
+        int off = -1, dst = -1;
+        if (e < LTOT) {
+            int lx, ly, base;
+            if (e < LU) {
+                ly = e / UX;
+                lx = e - ly * UX;
+                base = 0;
+            } else if (e < LU + LV) {
+                const int t = e - LU;
+                ly = t / WX;
+                lx = t - ly * WX;
+                base = NU;
+            } else {
+                const int t = e - LU - LV;
+                const int t2 = t < LC ? t : t - LC;
+                ly = t2 / WX;
+                lx = t2 - ly * WX;
+                base = t < LC ? NU + NV : NU + NV + NC;
+            }
+            dst = base + ly * R + G::col(lx);
+            const int gy = gyt[ly];
+            if (gy >= 0) off = gxt[lx] + d.nxp * gy;
+        }
+        ldoff[m] = off;
+        lddst[m] = dst;
+    }
+    auto slot = [&](int q) { return sm + ((q - k0 + 2) & 3) * SLOT; };
+    auto issue = [&](int q, int gk) {
         double* s = slot(q);
-        const int gk = wrapz(q);
-        for (int t = tid; t < NU; t += blockDim.x) {
-            const int ly = t / UX, lx = t - ly * UX, gy = gyt[ly];
-            s[t] = gy >= 0 ? __ldg(u0 + pidx(d, gxt[lx], gy, gk)) : 0.0;
+        const long long pk = (long long)gk * plane;
+#pragma unroll
+        for (int m = 0; m < NLD; ++m) {
+            const int e = tid + m * NT;
+            if (e < LTOT) {
+                const double* src = e < LU ? u0 : (e < LU + LV ? v0 : (e < LU + LV + LC ? w0 : p0));
+                const int off = ldoff[m];
+                cp_async8(s + lddst[m], off >= 0 ? src + pk + off : u0, off >= 0);
+            }
         }
-        for (int t = tid; t < NV; t += blockDim.x) {
-            const int ly = t / WX, lx = t - ly * WX, gy = gyt[ly];
-            s[NU + t] = gy >= 0 ? __ldg(v0 + pidx(d, gxt[lx], gy, gk)) : 0.0;
-        }
-        for (int t = tid; t < NC; t += blockDim.x) {
-            const int ly = t / WX, lx = t - ly * WX, gy = gyt[ly];
-            const long long c = gy >= 0 ? pidx(d, gxt[lx], gy, gk) : 0;
-            s[NU + NV + t] = gy >= 0 ? __ldg(w0 + c) : 0.0;
-            s[NU + NV + NC + t] = gy >= 0 ? __ldg(p0 + c) : 0.0;
-        }
+        cp_async_commit();
     };
-    // Update the cells of colour `odd` ((i+j+k) odd: red) on plane q within
-    // local rows [ly0, ly1) and columns [lx0, lx1).
-    auto update = [&](int q, int odd, int lx0, int lx1, int ly0, int ly1) {
+    const int r_ly = tid / HR, r_m = tid % HR;
+    const int b_ly = 1 + tid / HB, b_m = tid % HB;
+    const bool r_ok = tid < WY * HR, b_ok = tid < (WY - 2) * HB;
+    auto cell = [&](int q, int ly, int lx, int gy, int gk) {
         double* s = slot(q);
-        double* sn = slot(q + 1);
         double* su = s;
         double* sv = s + NU;
         double* sw = s + NU + NV;
         double* sp = s + NU + NV + NC;
-        double* swn = sn + NU + NV;
-        const int gk = wrapz(q);
-        const int rows = ly1 - ly0;
-        for (int t = tid; t < rows * HX; t += blockDim.x) {
-            const int ly = ly0 + t / HX;
-            const int gy = gyt[ly];
-            if (gy < 1 || gy > ny) continue;
-            // first column of the wanted colour: (x0-2+lx) + gy + gk must have
-            // the parity `odd`, i.e. lx = odd + x0 + gy + gk (mod 2)
-            const int off = ((x0 + lx0 + gy + gk + odd) & 1);
-            const int lx = lx0 + off + 2 * (t % HX);
-            if (lx >= lx1) continue;
-            const int gx = gxt[lx];
-            double mu_u_i = 1.0, mu_u_ip = 1.0, mu_v_j = 1.0, mu_v_jp = 1.0, mu_w = 1.0;
-            if (MU == MU_PLANE) {
-                mu_u_i = smu[ly * UX + lx];
-                mu_u_ip = smu[ly * UX + lx + 1];
-                mu_v_j = smu[NU + ly * WX + lx];
-                mu_v_jp = smu[NU + (ly + 1) * WX + lx];
-                mu_w = smu[NU + NV + ly * WX + lx];
-            }
-            sor_cell(su[ly * UX + lx], su[ly * UX + lx + 1], sv[ly * WX + lx], sv[(ly + 1) * WX + lx],
-                     sw[ly * WX + lx], swn[ly * WX + lx], sp[ly * WX + lx], mu_u_i, mu_u_ip, mu_v_j, mu_v_jp, mu_w,
-                     mu_w, P, bc, gx, gy, gk, nx, ny, nz);
+        double* swn = slot(q + 1) + NU + NV;
+        const int c0 = ly * R + G::col(lx), c1 = ly * R + G::col(lx + 1), cn = c0 + R;
+        double mu_u_i = 1.0, mu_u_ip = 1.0, mu_v_j = 1.0, mu_v_jp = 1.0, mu_w = 1.0;
+        if (MU == MU_PLANE) {
+            mu_u_i = smu[c0];
+            mu_u_ip = smu[c1];
+            mu_v_j = smu[NU + c0];
+            mu_v_jp = smu[NU + cn];
+            mu_w = smu[NU + NV + c0];
         }
+        double ui = su[c0], uip = su[c1], vj = sv[c0], vjp = sv[cn], wk = sw[c0], wkp = swn[c0], pc = sp[c0];
+        sor_cell_fac<1, PY, 1>(ui, uip, vj, vjp, wk, wkp, pc, mu_u_i, mu_u_ip, mu_v_j, mu_v_jp, mu_w, mu_w, sfac[c0],
+                               P, bc, 0, gy, gk, nx, ny, nz);
+        su[c0] = ui;
+        su[c1] = uip;
+        sv[c0] = vj;
+        sv[cn] = vjp;
+        sw[c0] = wk;
+        swn[c0] = wkp;
+        sp[c0] = pc;
     };
-    auto store = [&](int q) {
-        double* s = slot(q);
-        const int gk = wrapz(q);
-        for (int t = tid; t < TX * TY; t += blockDim.x) {
-            const int ly = 2 + t / TX, lx = 2 + t % TX;
-            const int gxu = x0 + lx - 2, gyu = y0 + ly - 2;   // owned cells: no wrap
-            if (gxu > nx || gyu > ny) continue;
-            const long long c = pidx(d, gxu, gyu, gk);
-            u1[c] = s[ly * UX + lx];
-            v1[c] = s[NU + ly * WX + lx];
-            w1[c] = s[NU + NV + ly * WX + lx];
-            p1[c] = s[NU + NV + NC + ly * WX + lx];
-            if (!pery && gyu == ny) v1[pidx(d, gxu, ny + 1, gk)] = s[NU + (ly + 1) * WX + lx];
-        }
+    auto red = [&](int q, int gk) {   // red: (i+j+k) odd, whole halo region
+        if (!r_ok) return;
+        const int gy = gyt[r_ly];
+        if (gy < 1 || gy > ny) return;
+        const int lx = ((x0 + gy + gk + 1) & 1) + 2 * r_m;
+        if (lx < WX) cell(q, r_ly, lx, gy, gk);
     };
+    auto black = [&](int q, int gk) {   // black: (i+j+k) even, tile plus one ring
+        if (!b_ok) return;
+        const int gy = gyt[b_ly];
+        if (gy < 1 || gy > ny) return;
+        const int lx = 1 + ((x0 + 1 + gy + gk) & 1) + 2 * b_m;
+        if (lx < WX - 1) cell(q, b_ly, lx, gy, gk);
+    };
+    // owned cell of this thread
+    const int o_gx = x0 + tid % TX, o_gy = y0 + tid / TX;
+    const bool o_ok = o_gx <= nx && o_gy <= ny;
+    const int o_s = (2 + tid / TX) * R + G::col(2 + tid % TX);
+    const int o_off = o_gx + d.nxp * o_gy;
+    auto store = [&](int q, int gk) {
+        if (!o_ok) return;
+        const double* s = slot(q);
+        const long long c = (long long)gk * plane + o_off;
+        u1[c] = s[o_s];
+        v1[c] = s[NU + o_s];
+        w1[c] = s[NU + NV + o_s];
+        p1[c] = s[NU + NV + NC + o_s];
+        if (!PY && o_gy == ny) v1[c + d.nxp] = s[NU + o_s + R];
+    };
+    auto wrapz = [&](int q) { return ((q - 1) % nz + nz) % nz + 1; };
 
-    load(k0 - 2);
+    issue(k0 - 2, wrapz(k0 - 2));
+    issue(k0 - 1, wrapz(k0 - 1));
+    int gkm = wrapz(k0 - 3);   // plane q-1
+    int gk = wrapz(k0 - 2);    // plane q
     for (int q = k0 - 2; q <= k1; ++q) {
-        load(q + 1);
+        if (q + 2 <= k1 + 1) issue(q + 2, wrapz(q + 2));
+        else cp_async_commit();           // empty group keeps the wait count uniform
+        cp_async_wait1();                 // planes up to q+1 have landed
         __syncthreads();
-        update(q, 1, 0, WX, 0, WY);                    // red on the halo region of plane q
+        red(q, gk);                       // halo region of plane q
         __syncthreads();
-        if (q - 1 >= k0 - 1) update(q - 1, 0, 1, WX - 1, 1, WY - 1);   // black on the tile + 1 ring
+        if (q - 1 >= k0 - 1) black(q - 1, gkm);   // tile + one ring of plane q-1
         __syncthreads();
-        if (q - 1 >= k0) store(q - 1);
-        __syncthreads();
+        if (q - 1 >= k0) store(q - 1, gkm);
+        __syncthreads();                  // slot of q-1 is refilled by the next issue
+        gkm = gk;
+        gk = gk == nz ? 1 : gk + 1;
     }
 }
 
@@ -328,6 +439,52 @@ double mdx_div_floor(const mdx_ctx_t* ctx, double umax) {
     const double eps = 2.220446049250313e-16;
     const mdx_grid_t& g = ctx->g;
     return eps * std::sqrt((double)ctx->d.nint) * umax * (1.0 / g.dx + 1.0 / g.dy + 1.0 / g.dz);
+}
+
+// One colour sweep for periodic x and z (the configurations of every run
+// here): boundary flags are compile-time constants, in-plane offsets are
+// 32-bit, and registers are bounded for occupancy.
+template <int MU, int PY>
+__global__ void __launch_bounds__(256, 4)
+k_sor_sweep_pxz(mdx_dims d, mdx_bc_dev bc, mdx_sor_params p, int parity, int reverse, double* __restrict__ un,
+                double* __restrict__ vn, double* __restrict__ wn, double* __restrict__ pn,
+                const double* __restrict__ mu) {
+    const int ni = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int kk = blockIdx.z * blockDim.z + threadIdx.z + 1;
+    const int nx = d.nx, ny = d.ny, nz = d.nz;
+    if (ni > nx / 2 || j > ny || kk > nz) return;
+    const int k = reverse ? nz + 1 - kk : kk;
+    const int jp = (PY && j == ny) ? 1 : j + 1;
+    const int kp = (k == nz) ? 1 : k + 1;
+    const int i = 1 + ((j + k + parity) & 1) + 2 * (ni - 1);
+    const int ip = (i == nx) ? 1 : i + 1;
+    const long long plane = (long long)d.nxp * d.nyp;
+    const int q = i + d.nxp * j, qip = ip + d.nxp * j, qjp = i + d.nxp * jp;
+    double* U = un + k * plane;
+    double* Vv = vn + k * plane;
+    double* W = wn + k * plane;
+    double* Wn = wn + kp * plane;
+    double* Pp = pn + k * plane;
+    double mu_u_i = 1.0, mu_u_ip = 1.0, mu_v_j = 1.0, mu_v_jp = 1.0, mu_w = 1.0;
+    if (MU == MU_PLANE) {
+        mu_u_i = __ldg(mu + q);
+        mu_u_ip = __ldg(mu + qip);
+        mu_v_j = __ldg(mu + plane + q);
+        mu_v_jp = __ldg(mu + plane + qjp);
+        mu_w = __ldg(mu + 2 * plane + q);
+    }
+    double u_i = U[q], u_ip = U[qip], v_j = Vv[q], v_jp = Vv[qjp], w_k = W[q], w_kp = Wn[q], pc = Pp[q];
+    const double fac = sor_factor(mu_u_i, mu_u_ip, mu_v_j, mu_v_jp, mu_w, mu_w, p);
+    sor_cell_fac<1, PY, 1>(u_i, u_ip, v_j, v_jp, w_k, w_kp, pc, mu_u_i, mu_u_ip, mu_v_j, mu_v_jp, mu_w, mu_w, fac, p,
+                           bc, i, j, k, nx, ny, nz);
+    U[q] = u_i;
+    U[qip] = u_ip;
+    Vv[q] = v_j;
+    Vv[qjp] = v_jp;
+    W[q] = w_k;
+    Wn[q] = w_kp;
+    Pp[q] = pc;
 }
 
 static mdx_sor_params sor_params(const mdx_ctx_t* ctx, double dg) {
@@ -348,9 +505,16 @@ static int sor_iteration(mdx_ctx_t* ctx, const mdx_sor_params& p) {
     const int na = d.nx / 2;
     dim3 block(32, 4, 2);
     dim3 grid((na + 31) / 32, (d.ny + 3) / 4, (d.nz + 1) / 2);
+    const bool pxz = ctx->bc.is_periodic[0] && ctx->bc.is_periodic[2] && ctx->mu_mode != MU_FULL;
+    const bool py = ctx->bc.is_periodic[1] != 0;
     for (int parity = 0; parity < 2; ++parity) {
         const int rev = parity;   // red sweeps walk k up, black sweeps walk k down
-        if (ctx->mu_mode == MU_ONE)
+        if (pxz) {
+            auto kfn = ctx->mu_mode == MU_PLANE ? (py ? k_sor_sweep_pxz<MU_PLANE, 1> : k_sor_sweep_pxz<MU_PLANE, 0>)
+                                                : (py ? k_sor_sweep_pxz<MU_ONE, 1> : k_sor_sweep_pxz<MU_ONE, 0>);
+            MDX_LAUNCH(ctx, MDX_T_SOR_SWEEP, "sor sweep", kfn, grid, block, 0, d, ctx->bcd, p, parity, rev,
+                       f[MDX_UN], f[MDX_VN], f[MDX_WN], f[MDX_PN], ctx->mu);
+        } else if (ctx->mu_mode == MU_ONE)
             MDX_LAUNCH(ctx, MDX_T_SOR_SWEEP, "sor sweep", k_sor_sweep<MU_ONE>, grid, block, 0, d, ctx->bcd, p, parity,
                        rev, f[MDX_UN], f[MDX_VN], f[MDX_WN], f[MDX_PN], ctx->mu);
         else if (ctx->mu_mode == MU_PLANE)
@@ -363,21 +527,33 @@ static int sor_iteration(mdx_ctx_t* ctx, const mdx_sor_params& p) {
     return MDX_OK;
 }
 
-// ---- fused red+black iterations ---------------------------------------------
-#define MDX_FUSED_TX 32
-#define MDX_FUSED_TY 8
+// ---- red-black kernel variants and their autotuner ---------------------------
+// Variants (all bit-identical per iteration):
+//   MDX_SORV_SWEEPS    one launch per colour sweep
+//   MDX_SORV_FUSED8    fused red+black pass, 32x8 tiles, 256 threads
+//   MDX_SORV_FUSED16   fused red+black pass, 32x16 tiles, 512 threads
+// The fused passes need periodic x and z and mu = 1 or z-invariant.
+enum { MDX_SORV_AUTO = 0, MDX_SORV_SWEEPS = 1, MDX_SORV_FUSED8 = 2, MDX_SORV_FUSED16 = 3, MDX_SORV_NUM = 4 };
 
-template <int MU>
+template <int MU, int TY, int NT>
 static size_t fused_smem() {
-    constexpr int WX = MDX_FUSED_TX + 3, WY = MDX_FUSED_TY + 3, UX = WX + 1;
-    constexpr int NU = WY * UX, NV = (WY + 1) * WX, NC = WY * WX;
-    constexpr int SLOT = NU + NV + 2 * NC;
-    return sizeof(double) * (3 * SLOT + (MU == MU_PLANE ? NU + NV + NC : 0)) + sizeof(int) * (UX + WY + 1);
+    using G = fused_geom<32, TY, NT>;
+    return sizeof(double) * (4 * G::SLOT + (MU == MU_PLANE ? G::NU + G::NV + G::NC : 0) + G::NC) +
+           sizeof(int) * (G::UX + G::WY + 1);
 }
 
-static bool use_fused(const mdx_ctx_t* ctx) {
-    if (ctx->opts.sor_variant == 1) return false;
+static bool fused_ok(const mdx_ctx_t* ctx) {
     return ctx->bc.is_periodic[0] && ctx->bc.is_periodic[2] && ctx->mu_mode != MU_FULL;
+}
+
+template <int TY, int NT>
+static int fused_attrs(mdx_ctx_t* ctx) {
+    const int s_one = (int)fused_smem<MU_ONE, TY, NT>(), s_plane = (int)fused_smem<MU_PLANE, TY, NT>();
+    MDX_CUDA(ctx, cudaFuncSetAttribute(k_sor_fused<MU_ONE, 0, 32, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, s_one));
+    MDX_CUDA(ctx, cudaFuncSetAttribute(k_sor_fused<MU_ONE, 1, 32, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, s_one));
+    MDX_CUDA(ctx, cudaFuncSetAttribute(k_sor_fused<MU_PLANE, 0, 32, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, s_plane));
+    MDX_CUDA(ctx, cudaFuncSetAttribute(k_sor_fused<MU_PLANE, 1, 32, TY, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, s_plane));
+    return MDX_OK;
 }
 
 static int fused_prepare(mdx_ctx_t* ctx) {
@@ -390,36 +566,39 @@ static int fused_prepare(mdx_ctx_t* ctx) {
     for (int t = 0; t < 4; ++t)
         MDX_CUDA(ctx, cudaMemcpyAsync(ctx->sor_alt[t], ctx->f[ids[t]], bytes, cudaMemcpyDeviceToDevice, ctx->stream));
     if (!ctx->fused_attr) {
-        MDX_CUDA(ctx, cudaFuncSetAttribute(k_sor_fused<MU_ONE, MDX_FUSED_TX, MDX_FUSED_TY>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fused_smem<MU_ONE>()));
-        MDX_CUDA(ctx, cudaFuncSetAttribute(k_sor_fused<MU_PLANE, MDX_FUSED_TX, MDX_FUSED_TY>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fused_smem<MU_PLANE>()));
+        MDX_TRY((fused_attrs<8, 256>(ctx)));
+        MDX_TRY((fused_attrs<16, 512>(ctx)));
         ctx->fused_attr = true;
     }
     return MDX_OK;
 }
 
+template <int TY, int NT>
 static int sor_fused_iteration(mdx_ctx_t* ctx, const mdx_sor_params& p) {
     const mdx_dims& d = ctx->d;
     double** f = ctx->f;
     const int KZ = ctx->opts.sor_kz > 0 ? ctx->opts.sor_kz : 16;
-    dim3 grid((d.nx + MDX_FUSED_TX - 1) / MDX_FUSED_TX, (d.ny + MDX_FUSED_TY - 1) / MDX_FUSED_TY, (d.nz + KZ - 1) / KZ);
+    dim3 grid((d.nx + 31) / 32, (d.ny + TY - 1) / TY, (d.nz + KZ - 1) / KZ);
     double** a = ctx->sor_alt;
-    if (ctx->mu_mode == MU_PLANE) {
-        auto kfn = k_sor_fused<MU_PLANE, MDX_FUSED_TX, MDX_FUSED_TY>;
-        MDX_LAUNCH(ctx, MDX_T_SOR_SWEEP, "sor fused", kfn, grid, 256, fused_smem<MU_PLANE>(), d, ctx->bcd, p, KZ,
-                   f[MDX_UN], f[MDX_VN], f[MDX_WN], f[MDX_PN], a[0], a[1], a[2], a[3], ctx->mu);
-    } else {
-        auto kfn = k_sor_fused<MU_ONE, MDX_FUSED_TX, MDX_FUSED_TY>;
-        MDX_LAUNCH(ctx, MDX_T_SOR_SWEEP, "sor fused", kfn, grid, 256, fused_smem<MU_ONE>(), d, ctx->bcd, p, KZ,
-                   f[MDX_UN], f[MDX_VN], f[MDX_WN], f[MDX_PN], a[0], a[1], a[2], a[3], ctx->mu);
-    }
+    const bool py = ctx->bc.is_periodic[1] != 0;
+    const bool plane = ctx->mu_mode == MU_PLANE;
+    auto kfn = plane ? (py ? k_sor_fused<MU_PLANE, 1, 32, TY, NT> : k_sor_fused<MU_PLANE, 0, 32, TY, NT>)
+                     : (py ? k_sor_fused<MU_ONE, 1, 32, TY, NT> : k_sor_fused<MU_ONE, 0, 32, TY, NT>);
+    const size_t smem = plane ? fused_smem<MU_PLANE, TY, NT>() : fused_smem<MU_ONE, TY, NT>();
+    MDX_LAUNCH(ctx, MDX_T_SOR_SWEEP, "sor fused", kfn, grid, NT, smem, d, ctx->bcd, p, KZ, f[MDX_UN], f[MDX_VN],
+               f[MDX_WN], f[MDX_PN], a[0], a[1], a[2], a[3], ctx->mu);
     // the new state becomes the current one
     std::swap(f[MDX_UN], a[0]);
     std::swap(f[MDX_VN], a[1]);
     std::swap(f[MDX_WN], a[2]);
     std::swap(f[MDX_PN], a[3]);
     return MDX_OK;
+}
+
+static int sor_iterate(mdx_ctx_t* ctx, const mdx_sor_params& p, int variant) {
+    if (variant == MDX_SORV_FUSED8) return sor_fused_iteration<8, 256>(ctx, p);
+    if (variant == MDX_SORV_FUSED16) return sor_fused_iteration<16, 512>(ctx, p);
+    return sor_iteration(ctx, p);
 }
 
 // The IBM factors of this projection's dt_gamma.
@@ -453,13 +632,31 @@ int mdx_k_projection_redblack(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t* st) 
     MDX_CUDA(ctx, cudaMemcpyAsync(f[MDX_VN], f[MDX_VS], bytes, cudaMemcpyDeviceToDevice, ctx->stream));
     MDX_CUDA(ctx, cudaMemcpyAsync(f[MDX_WN], f[MDX_WS], bytes, cudaMemcpyDeviceToDevice, ctx->stream));
     MDX_TRY(mu_tables(ctx, dg));
-    const bool fused = use_fused(ctx);
-    if (fused) MDX_TRY(fused_prepare(ctx));
+    // kernel variant: the requested one, the tuned one, or -- while tuning --
+    // the next untried candidate for each residual-check block
+    const bool fok = fused_ok(ctx);
+    int want = ctx->opts.sor_variant;
+    if ((want == MDX_SORV_FUSED8 || want == MDX_SORV_FUSED16) && !fok) want = MDX_SORV_SWEEPS;
+    if (want == MDX_SORV_AUTO && !fok) want = MDX_SORV_SWEEPS;
+    if (want != MDX_SORV_SWEEPS) MDX_TRY(fused_prepare(ctx));
     const mdx_sor_params p = sor_params(ctx, dg);
+    auto pick = [&]() -> int {
+        if (want != MDX_SORV_AUTO) return want;
+        if (ctx->sor_tuned > 0) return ctx->sor_tuned;
+        for (int v = MDX_SORV_SWEEPS; v < MDX_SORV_NUM; ++v)
+            if (ctx->sor_tune_ms[v] <= 0.0) return v;
+        int best = MDX_SORV_SWEEPS;
+        for (int v = MDX_SORV_SWEEPS; v < MDX_SORV_NUM; ++v)
+            if (ctx->sor_tune_ms[v] < ctx->sor_tune_ms[best]) best = v;
+        ctx->sor_tuned = best;
+        return best;
+    };
     mdx_solve_stats_t s{};
     const mdx_solver_opts_t& o = ctx->opts;
     if (o.tol <= 0.0) {
-        for (int it = 0; it < o.n_iter; ++it) MDX_TRY(fused ? sor_fused_iteration(ctx, p) : sor_iteration(ctx, p));
+        const int v = (want == MDX_SORV_AUTO) ? (ctx->sor_tuned > 0 ? ctx->sor_tuned : MDX_SORV_SWEEPS) : want;
+        for (int it = 0; it < o.n_iter; ++it) MDX_TRY(sor_iterate(ctx, p, v));
+        s.variant = v;
         s.iterations = o.n_iter;
         s.status = MDX_OK;
     } else {
@@ -483,9 +680,19 @@ int mdx_k_projection_redblack(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t* st) 
             r = r0;
             while (it < o.max_iter) {
                 const int m = std::min(o.check_every, o.max_iter - it);
-                for (int q = 0; q < m; ++q) MDX_TRY(fused ? sor_fused_iteration(ctx, p) : sor_iteration(ctx, p));
+                const int v = pick();
+                const bool timing_block = want == MDX_SORV_AUTO && ctx->sor_tuned == 0 && m == o.check_every;
+                if (timing_block) MDX_CUDA(ctx, cudaEventRecord(ctx->tune_ev[0], ctx->stream));
+                for (int q = 0; q < m; ++q) MDX_TRY(sor_iterate(ctx, p, v));
+                if (timing_block) MDX_CUDA(ctx, cudaEventRecord(ctx->tune_ev[1], ctx->stream));
                 it += m;
+                s.variant = v;
                 MDX_TRY(mdx_k_div_norms(ctx, f[MDX_UN], f[MDX_VN], f[MDX_WN], &r, &linf));
+                if (timing_block) {   // the norms synchronised the stream
+                    float ms = 0.f;
+                    if (cudaEventElapsedTime(&ms, ctx->tune_ev[0], ctx->tune_ev[1]) == cudaSuccess)
+                        ctx->sor_tune_ms[v] = ms > 0.f ? ms : 1e-6;
+                }
                 if (!std::isfinite(r)) { s.status = MDX_ERR_NONFINITE; break; }
                 if (r <= target) { s.status = MDX_OK; break; }
             }

@@ -454,6 +454,8 @@ int mdx_reduce_init(mdx_ctx_t* ctx) {
     MDX_CUDA(ctx, cudaMalloc(&ctx->red_part, sizeof(double) * 3 * ctx->red_blocks));
     MDX_CUDA(ctx, cudaMalloc(&ctx->red_out, sizeof(double) * 3));
     MDX_CUDA(ctx, cudaMallocHost(&ctx->red_host, sizeof(double) * 3));
+    MDX_CUDA(ctx, cudaEventCreate(&ctx->tune_ev[0]));
+    MDX_CUDA(ctx, cudaEventCreate(&ctx->tune_ev[1]));
     return MDX_OK;
 }
 

@@ -77,6 +77,9 @@ struct mdx_ctx {
     bool coef_zinv = false;                  // coefficients equal on every z plane
     double* sor_alt[4] = {nullptr};          // second u,v,w,p state of the fused red-black pass
     bool fused_attr = false;
+    int sor_tuned = 0;                       // red-black kernel variant chosen by the autotuner (0: not yet)
+    double sor_tune_ms[4] = {0.0};           // time of one residual-check block per variant
+    cudaEvent_t tune_ev[2] = {nullptr, nullptr};
     double* mu = nullptr;                    // red-black IBM factors 1/(1+dt_gamma*coef)
     long long mu_elems = 0;
     int mu_mode = 0;

@@ -69,7 +69,7 @@ def test_apply_bc_redblack_bitwise(bcname):
 
 @pytest.mark.parametrize("bcname", list(BC_CASES))
 @pytest.mark.parametrize("ibm", ["none", "random", "zinv"])
-@pytest.mark.parametrize("variant", [0, 1])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
 def test_redblack_fixed_iterations_bitwise(bcname, ibm, variant):
     """pressure_projection_redblack with the reference's fixed nIter: bit-exact, both with
     one launch per colour sweep (variant 1) and with the fused red+black pass (variant 0,
@@ -87,13 +87,15 @@ def test_redblack_fixed_iterations_bitwise(bcname, ibm, variant):
 
 @pytest.mark.parametrize("shape,kz", [((36, 10, 6), 4), ((64, 24, 20), 16), ((40, 12, 10), 3), ((96, 48, 34), 8)])
 @pytest.mark.parametrize("bcname", ["periodic", "channel"])
-def test_redblack_fused_partial_tiles_bitwise(shape, kz, bcname):
-    """Fused pass on grids that are not multiples of its 32x8 tile or z chunk."""
+@pytest.mark.parametrize("variant", [2, 3])
+def test_redblack_fused_partial_tiles_bitwise(shape, kz, bcname, variant):
+    """Fused passes on grids that are not multiples of their 32x8 / 32x16 tiles or z chunk."""
     g = O.Grid(*shape, lx=1.1, ly=0.8, lz=1.7, re=800.0)
     bc = BC_CASES[bcname]()
     f = random_fields(g, 13, "zinv")
     with to_device(M, g, bc, f) as s:
-        s.init_pressure_solver(M.make_solver_opts(M.SOLVER_REDBLACK, n_iter=5, sor=1.7, sor_kz=kz))
+        s.init_pressure_solver(M.make_solver_opts(M.SOLVER_REDBLACK, n_iter=5, sor=1.7, sor_kz=kz,
+                                                  sor_variant=variant))
         O.pressure_projection_redblack(g, bc, f, 0.5e-3, niter=5, sor=1.7, tol=0.0)
         s.pressure_projection(0.5e-3)
         diff = compare_all(s, f, ["un", "vn", "wn", "pn"])
