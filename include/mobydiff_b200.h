@@ -288,6 +288,31 @@ int mdx_get_timing(mdx_ctx_t* ctx, mdx_timing_t* out);
 /* Number of kernel launches issued by the library on this context so far. */
 long long mdx_launch_count(const mdx_ctx_t* ctx);
 
+/* ---- allocation-free pressure solve --------------------------------------- */
+
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory through the CUDA runtime -- e.g. an OpenMP-offload Fortran program
+ * whose device arrays belong to the OpenMP runtime and are handed over with
+ * use_device_addr -- this solves the FFT-path pressure equation on device
+ * arrays the caller owns, without a context and without allocating.
+ *
+ * rhs, phi: device arrays in the rhs(nx,nz,ny) order (x fastest, then z,
+ * then y); phi = the FFT + Thomas solution scaled by 1/(nx*nz), the result
+ * of the context path (pressure_backend_*.f90 solve_pressure_*).  phi may
+ * equal rhs.  The call is enqueued on `stream` (cudaStream_t, NULL = legacy
+ * default stream) and returns without synchronising.
+ *
+ * Every intermediate (spectrum, Thomas tables, twiddles, wavenumbers) lives in
+ * one static device array of 8 MiB per device, which the library holds until
+ * the process exits; grids needing more (e.g. above about 64 x 64 x 128) are
+ * rejected with MDX_ERR_ARG before any device work.  The array's address is
+ * looked up on the first call on each device, so make that first call before
+ * any stream capture.  All calls share the array and it keeps the last call's
+ * contents; calls that overlap on the GPU (different streams or threads) race
+ * on it.  Requires even nx; nx/2 and nz must factor into 2, 3, 5, 7. */
+int mdx_solve_pressure_fft_noalloc(const double* rhs, double* phi, int nx, int ny, int nz, double dx, double dy,
+                                   double dz, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

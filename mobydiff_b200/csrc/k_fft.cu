@@ -496,3 +496,191 @@ int mdx_k_projection_fft(mdx_ctx_t* ctx, double dg) {
                    f[MDX_COEF_U], f[MDX_COEF_V], f[MDX_COEF_W]);
     return MDX_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free FFT pressure solve.
+//
+// mdx_solve_pressure_fft_noalloc runs the same kernels as the context path
+// (x real FFT, z FFT, Thomas solve in y, inverse FFTs, 1/(nx*nz) scale) on
+// device arrays the caller owns, with every intermediate array (spectrum,
+// Thomas tables, twiddles, modified wavenumbers) placed in the file-scope
+// array below instead of memory from cudaMalloc.  It exists for callers that
+// cannot allocate device memory through the CUDA runtime themselves, such as
+// an OpenMP-offload Fortran program whose device arrays belong to the OpenMP
+// runtime (the reference hands cuFFT such arrays through use_device_addr).
+//
+// The array is MDX_NOALLOC_SCRATCH_BYTES per device and lives as long as the
+// library is loaded.  Its device address is looked up once per device, on
+// that device's first call (cudaGetSymbolAddress), so the first call on a
+// device should come before any stream capture.  All calls share the array
+// and it keeps the last call's contents; every call rewrites all of it that
+// it reads, so nothing needs clearing.  Calls that overlap on the GPU (two
+// streams, or two host threads) race on the array.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+#define MDX_NOALLOC_SCRATCH_BYTES (8u << 20)
+#define MDX_NOALLOC_MAX_DEVICES 64
+
+static __device__ __align__(256) unsigned char mdx_noalloc_scratch[MDX_NOALLOC_SCRATCH_BYTES];
+
+static std::mutex g_noalloc_mu;
+static void* g_noalloc_addr[MDX_NOALLOC_MAX_DEVICES] = {nullptr};
+
+// Forward real FFT along x of each row of rhs(nx, nz, ny): rows r =
+// (k-1) + nz*(j-1) of nx reals -> nx/2+1 complex in plane_hat order.
+__global__ void __launch_bounds__(256)
+k_fftx_r2c(mdx_dims d, int R, const double* __restrict__ rhs, double2* __restrict__ spec, mdx_fft_plan pl,
+           const double2* __restrict__ twx) {
+    extern __shared__ double2 sm[];
+    const int M = d.nx / 2;
+    double2* A = sm;
+    double2* B = sm + R * M;
+    const int nrows = d.nz * d.ny;
+    const int row0 = blockIdx.x * R;
+    for (int t = threadIdx.x; t < R * M; t += blockDim.x) {
+        const int rl = t / M, n = t - rl * M;
+        const int row = row0 + rl;
+        A[rl * M + n] = (row < nrows) ? make_double2(__ldg(rhs + (long long)row * d.nx + 2 * n),
+                                                     __ldg(rhs + (long long)row * d.nx + 2 * n + 1))
+                                      : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    double2* Z = smem_fft<false>(A, B, M, R, M, pl, twx, 2);
+    const int nxh = M + 1;
+    for (int t = threadIdx.x; t < R * nxh; t += blockDim.x) {
+        const int rl = t / nxh, kx = t - rl * nxh;
+        const int row = row0 + rl;
+        if (row >= nrows) continue;
+        const double2 zk = Z[rl * M + (kx == M ? 0 : kx)];
+        const double2 zc = cconj(Z[rl * M + (kx == 0 ? 0 : M - kx)]);
+        const double2 e = make_double2(0.5 * (zk.x + zc.x), 0.5 * (zk.y + zc.y));
+        const double2 o = cmul_mi(make_double2(0.5 * (zk.x - zc.x), 0.5 * (zk.y - zc.y)));
+        spec[(long long)row * nxh + kx] = cadd(e, cmul(__ldg(twx + kx), o));
+    }
+}
+
+static size_t noalloc_align(size_t b) { return (b + 255) & ~(size_t)255; }
+
+extern "C" int mdx_solve_pressure_fft_noalloc(const double* rhs, double* phi, int nx, int ny, int nz, double dx,
+                                              double dy, double dz, void* stream) {
+    if (!rhs || !phi) return mdx_fail(nullptr, MDX_ERR_ARG, "noalloc solve: null rhs or phi");
+    if (nx < 2 || ny < 2 || nz < 2 || nx % 2 != 0)
+        return mdx_fail(nullptr, MDX_ERR_ARG, "noalloc solve: need even nx >= 2, ny >= 2, nz >= 2 (got %d %d %d)", nx,
+                        ny, nz);
+    if (!(dx > 0.0 && dy > 0.0 && dz > 0.0)) return mdx_fail(nullptr, MDX_ERR_ARG, "noalloc solve: dx, dy, dz must be > 0");
+    mdx_fft_plan plx, plz;
+    bool ok1 = false, ok2 = false;
+    mdx_fft_make_plan(nx / 2, &plx, &ok1);
+    mdx_fft_make_plan(nz, &plz, &ok2);
+    if (!ok1 || !ok2 || nx / 2 > 4096 || nz > 4096)
+        return mdx_fail(nullptr, MDX_ERR_ARG, "noalloc solve: nx/2=%d and nz=%d must factor into 2,3,5,7 (<= 4096)",
+                        nx / 2, nz);
+    mdx_dims d{};
+    d.nx = nx; d.ny = ny; d.nz = nz;
+    d.nxp = nx + 2; d.nyp = ny + 2; d.nzp = nz + 2;
+    d.nxh = nx / 2 + 1;
+    d.nint = (long long)nx * ny * nz;
+    d.nspec = (long long)d.nxh * nz * ny;
+    const int nzh = nz / 2 + 1;
+    // scratch layout: spectrum | dinv | c' | twiddles x | twiddles z | kx^2 | kz^2
+    const size_t b_spec = noalloc_align(sizeof(double2) * (size_t)d.nspec);
+    const size_t b_tab = noalloc_align(sizeof(double) * (size_t)ny * d.nxh * nzh);
+    const size_t b_twx = noalloc_align(sizeof(double2) * (size_t)nx);
+    const size_t b_twz = noalloc_align(sizeof(double2) * (size_t)nz);
+    const size_t b_kx = noalloc_align(sizeof(double) * (size_t)d.nxh);
+    const size_t b_kz = noalloc_align(sizeof(double) * (size_t)nz);
+    const size_t need = b_spec + 2 * b_tab + b_twx + b_twz + b_kx + b_kz;
+    if (need > MDX_NOALLOC_SCRATCH_BYTES)
+        return mdx_fail(nullptr, MDX_ERR_ARG,
+                        "noalloc solve: grid %dx%dx%d needs %zu bytes of scratch, the static array holds %u",
+                        nx, ny, nz, need, (unsigned)MDX_NOALLOC_SCRATCH_BYTES);
+
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return mdx_fail(nullptr, MDX_ERR_NO_DEVICE, "noalloc solve: %s", cudaGetErrorString(e));
+    if (dev < 0 || dev >= MDX_NOALLOC_MAX_DEVICES) return mdx_fail(nullptr, MDX_ERR_ARG, "noalloc solve: device %d", dev);
+    unsigned char* base = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_addr[dev]) {
+            void* p = nullptr;
+            e = cudaGetSymbolAddress(&p, mdx_noalloc_scratch);
+            if (e != cudaSuccess)
+                return mdx_fail(nullptr, MDX_ERR_CUDA, "noalloc solve: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+            g_noalloc_addr[dev] = p;
+        }
+        base = (unsigned char*)g_noalloc_addr[dev];
+    }
+    double2* spec = (double2*)base;
+    double* dinv = (double*)(base + b_spec);
+    double* cp = (double*)(base + b_spec + b_tab);
+    double2* twx = (double2*)(base + b_spec + 2 * b_tab);
+    double2* twz = (double2*)(base + b_spec + 2 * b_tab + b_twx);
+    double* kxp = (double*)(base + b_spec + 2 * b_tab + b_twx + b_twz);
+    double* kzp = (double*)(base + b_spec + 2 * b_tab + b_twx + b_twz + b_kx);
+    cudaStream_t st = (cudaStream_t)stream;
+
+    // Twiddles (long-double cosl/sinl) and modified wavenumbers (libm sin,
+    // pressure_fft.f90:53,61) on the host, staged through fixed static host
+    // arrays (under the lock) and copied into the scratch; a copy from
+    // pageable memory has read the host array when cudaMemcpyAsync returns.
+    {
+        static double2 host_tw[8192];
+        static double host_k[4097];
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        const long double two_pi = 6.283185307179586476925286766559005768L;
+        for (int t = 0; t < nx; ++t) {
+            const long double a = two_pi * (long double)t / (long double)nx;
+            host_tw[t] = make_double2((double)cosl(a), (double)(-sinl(a)));
+        }
+        e = cudaMemcpyAsync(twx, host_tw, sizeof(double2) * nx, cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) return mdx_fail(nullptr, MDX_ERR_CUDA, "noalloc solve: copy: %s", cudaGetErrorString(e));
+        for (int t = 0; t < nz; ++t) {
+            const long double a = two_pi * (long double)t / (long double)nz;
+            host_tw[t] = make_double2((double)cosl(a), (double)(-sinl(a)));
+        }
+        e = cudaMemcpyAsync(twz, host_tw, sizeof(double2) * nz, cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) return mdx_fail(nullptr, MDX_ERR_CUDA, "noalloc solve: copy: %s", cudaGetErrorString(e));
+        const double pi = 3.141592653589793;
+        for (int ikx = 1; ikx <= d.nxh; ++ikx) {
+            const double s = std::sin(pi * (double)(ikx - 1) / (double)nx);
+            host_k[ikx - 1] = (4.0 / (dx * dx)) * (s * s);
+        }
+        e = cudaMemcpyAsync(kxp, host_k, sizeof(double) * d.nxh, cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) return mdx_fail(nullptr, MDX_ERR_CUDA, "noalloc solve: copy: %s", cudaGetErrorString(e));
+        for (int ikz = 1; ikz <= nz; ++ikz) {
+            const int kz = (ikz <= nz / 2 + 1) ? ikz - 1 : ikz - nz - 1;
+            const double s = std::sin(pi * (double)kz / (double)nz);
+            host_k[ikz - 1] = (4.0 / (dz * dz)) * (s * s);
+        }
+        e = cudaMemcpyAsync(kzp, host_k, sizeof(double) * nz, cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) return mdx_fail(nullptr, MDX_ERR_CUDA, "noalloc solve: copy: %s", cudaGetErrorString(e));
+    }
+
+    const double dyi2 = 1.0 / (dy * dy);
+    const int nm = d.nxh * nzh;
+    k_thomas_tables<<<(nm + 127) / 128, 128, 0, st>>>(d.nxh, nzh, ny, dyi2, kxp, kzp, dinv, cp);
+    const int M = nx / 2;
+    const int R = rows_per_block(M);
+    const int nrows = nz * ny;
+    const size_t smx = sizeof(double2) * 2 * R * M;
+    const int xblocks = (nrows + R - 1) / R;
+    const int TX = ztile(nz);
+    const size_t smz = sizeof(double2) * 2 * TX * (nz + 1);
+    const int zblocks = ((d.nxh + TX - 1) / TX) * ny;
+    const cudaError_t a1 = cudaFuncSetAttribute(k_fftx_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx);
+    const cudaError_t a2 = cudaFuncSetAttribute(k_ifftx, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx);
+    const cudaError_t a3 = cudaFuncSetAttribute(k_fftz<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz);
+    const cudaError_t a4 = cudaFuncSetAttribute(k_fftz<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz);
+    if (a1 != cudaSuccess || a2 != cudaSuccess || a3 != cudaSuccess || a4 != cudaSuccess)
+        return mdx_fail(nullptr, MDX_ERR_CUDA, "noalloc solve: cudaFuncSetAttribute failed");
+    k_fftx_r2c<<<xblocks, 256, smx, st>>>(d, R, rhs, spec, plx, twx);
+    k_fftz<false><<<zblocks, 256, smz, st>>>(d, TX, spec, plz, twz);
+    k_thomas<<<(d.nxh * nz + 127) / 128, 128, 0, st>>>(d, dyi2, spec, dinv, cp);
+    k_fftz<true><<<zblocks, 256, smz, st>>>(d, TX, spec, plz, twz);
+    k_ifftx<<<xblocks, 256, smx, st>>>(d, R, 1.0 / (double)(nx * nz), spec, phi, plx, twx);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return mdx_fail(nullptr, MDX_ERR_CUDA, "noalloc solve: launch: %s", cudaGetErrorString(e));
+    return MDX_OK;
+}
