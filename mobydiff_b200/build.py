@@ -30,6 +30,7 @@ CUDA_SOURCES = {
     "k_step.cu": ["-fmad=false"],
     "k_fft.cu": ["-fmad=false"],
     "k_sor.cu": ["-fmad=false"],
+    "k_sor_mixed.cu": [],   # FP32 sweeps inside FP64 defect correction: FMA allowed
 }
 CXX_SOURCES = ["host_config.cpp"]
 

@@ -219,6 +219,7 @@ int mdx_destroy_pressure_solver(mdx_ctx_t* ctx) {
     cudaFree(ctx->mu);
     ctx->mu = nullptr;
     ctx->mu_elems = 0;
+    mdx_mixed_free(ctx);
     ctx->solver = false;
     return MDX_OK;
 }

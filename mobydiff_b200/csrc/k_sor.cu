@@ -632,6 +632,11 @@ int mdx_k_projection_redblack(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t* st) 
     MDX_CUDA(ctx, cudaMemcpyAsync(f[MDX_VN], f[MDX_VS], bytes, cudaMemcpyDeviceToDevice, ctx->stream));
     MDX_CUDA(ctx, cudaMemcpyAsync(f[MDX_WN], f[MDX_WS], bytes, cudaMemcpyDeviceToDevice, ctx->stream));
     MDX_TRY(mu_tables(ctx, dg));
+    if (ctx->opts.precision == MDX_PREC_MIXED) {   // FP32 sweeps in FP64 defect correction
+        bool handled = false;
+        MDX_TRY(mdx_k_projection_redblack_mixed(ctx, dg, st, &handled));
+        if (handled) return MDX_OK;
+    }
     // kernel variant: the requested one, the tuned one, or -- while tuning --
     // the next untried candidate for each residual-check block
     const bool fok = fused_ok(ctx);

@@ -473,6 +473,19 @@ int mdx_k_div_norms_async(mdx_ctx_t* ctx, const double* u, const double* v, cons
     return MDX_OK;
 }
 
+// Reduce the per-block partials (sum, max, max) left in red_part by a
+// kernel of another module and bring them to the host (synchronises).
+int mdx_reduce_partials(mdx_ctx_t* ctx, double* sum, double* max1, double* max2) {
+    MDX_LAUNCH(ctx, MDX_T_RESIDUAL, "reduce final", k_reduce_final, 1, MDX_RED_THREADS, 0, ctx->red_blocks,
+               ctx->red_part, ctx->red_out);
+    MDX_CUDA(ctx, cudaMemcpyAsync(ctx->red_host, ctx->red_out, 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    MDX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (sum) *sum = ctx->red_host[0];
+    if (max1) *max1 = ctx->red_host[1];
+    if (max2) *max2 = ctx->red_host[2];
+    return MDX_OK;
+}
+
 int mdx_k_div_norms(mdx_ctx_t* ctx, const double* u, const double* v, const double* w, double* l2, double* linf,
                     double* umax) {
     MDX_TRY(mdx_k_div_norms_async(ctx, u, v, w));

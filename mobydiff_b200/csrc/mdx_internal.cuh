@@ -77,6 +77,9 @@ struct mdx_ctx {
     bool coef_zinv = false;                  // coefficients equal on every z plane
     double* sor_alt[4] = {nullptr};          // second u,v,w,p state of the fused red-black pass
     bool fused_attr = false;
+    // mixed-precision red-black: FP32 corrections, FP32 residual, IBM tables
+    float *mx_du = nullptr, *mx_dv = nullptr, *mx_dw = nullptr, *mx_dp = nullptr, *mx_r = nullptr;
+    float *mx_mu = nullptr, *mx_fac = nullptr;
     int sor_tuned = 0;                       // red-black kernel variant chosen by the autotuner (0: not yet)
     double sor_tune_ms[4] = {0.0};           // time of one residual-check block per variant
     cudaEvent_t tune_ev[2] = {nullptr, nullptr};
@@ -159,6 +162,10 @@ int mdx_k_div_norms(mdx_ctx_t* ctx, const double* u, const double* v, const doub
                     double* umax = nullptr);
 // Round-off floor of ||div u||_2: eps*sqrt(ncells)*umax*(1/dx+1/dy+1/dz).
 double mdx_div_floor(const mdx_ctx_t* ctx, double umax);
+int mdx_reduce_partials(mdx_ctx_t* ctx, double* sum, double* max1, double* max2);
+#define MDX_RED_THREADS 256
+int mdx_k_projection_redblack_mixed(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t* st, bool* handled);
+void mdx_mixed_free(mdx_ctx_t* ctx);
 int mdx_k_div_norms_async(mdx_ctx_t* ctx, const double* u, const double* v, const double* w);
 int mdx_k_cfl(mdx_ctx_t* ctx, double* cfl);
 int mdx_k_center_vel(mdx_ctx_t* ctx, double* uc, double* vc, double* wc);

@@ -1,0 +1,95 @@
+"""Mixed precision red-black projection (FP32 sweeps inside FP64 defect
+correction) against the FP64 path and the FP64 oracle."""
+import numpy as np
+import pytest
+
+import mobydiff_b200 as M
+from oracle import oracle as O
+from tests.helpers import oracle_channel_ic, random_fields, rel_l2, to_device
+
+pytestmark = pytest.mark.gpu
+
+
+def _wavy_case(nx=64, ny=32, nz=32, re=3000.0):
+    ly = 2.25
+    y0 = (ly - 2.0) / 2.0
+    g = O.Grid(nx, ny, nz, lx=2 * np.pi, ly=ly, lz=np.pi, re=re, dt=1e-3, forcing=(2.0 / re, 0.0, 0.0))
+    bc = O.channel_bc()
+    f = O.Fields(g)
+    O.set_ibm_coeff(g, O.ibm_wavy(0.05, g.lx / 2, y0), f)
+    oracle_channel_ic(g, bc, f, 20261203, solver=1, sor=1.7, tol=1e-10, check_every=50, y0=y0,
+                      wave_amp=0.05, wave_lambda=g.lx / 2)
+    return g, bc, f
+
+
+def _pair(g, bc, f, tol):
+    sp = to_device(M, g, bc, f)
+    sm = to_device(M, g, bc, f)
+    sp.init_pressure_solver(M.make_solver_opts(M.SOLVER_REDBLACK, sor=1.7, tol=tol, check_every=50))
+    sm.init_pressure_solver(M.make_solver_opts(M.SOLVER_REDBLACK, sor=1.7, tol=tol, check_every=50,
+                                               precision=M.PREC_MIXED))
+    return sp, sm
+
+
+@pytest.mark.parametrize("tol", [1e-8, 1e-10])
+def test_mixed_projection_matches_fp64(tol):
+    g, bc, f = _wavy_case()
+    a, b, c = O.rk_coeffs()
+    O.momentum(g, bc, f, g.dt * a[0], g.dt * b[0], g.dt * c[0])
+    sp, sm = _pair(g, bc, f, tol)
+    with sp, sm:
+        stp = sp.pressure_projection(g.dt * c[0])
+        stm = sm.pressure_projection(g.dt * c[0])
+        assert stp.status == 0 and stm.status == 0
+        assert stm.variant > 100                      # the mixed path ran
+        assert stm.residual <= tol * 1.0000001 or stm.residual * stm.residual0 <= stm.atol
+        # FP32 sweeps: about as many iterations as FP64
+        assert stm.iterations <= 1.5 * stp.iterations + 200
+        l2, _ = sm.divergence_norms()
+        assert l2 <= max(tol * stm.residual0, stm.atol) * 1.0000001
+        # both solves stop within the tolerance of the same projection; the
+        # north-star bound for the mixed path is a velocity error <= 1e-6
+        errs = {n: rel_l2(sm.get(n), sp.get(n)) for n in ("un", "vn", "wn", "pn")}
+        print("mixed vs fp64 rel-L2", tol, errs, stp.iterations, stm.iterations)
+        for n in ("un", "vn", "wn"):
+            assert errs[n] <= 1e-6, (n, errs)
+        assert errs["pn"] <= 1e-4, errs
+
+
+def test_mixed_two_steps_velocity_error():
+    """Two RK3 steps: velocity error of the mixed path vs the FP64 oracle <= 1e-6."""
+    g, bc, f = _wavy_case()
+    sp, sm = _pair(g, bc, f, 1e-8)
+    with sp, sm:
+        st, _ = O.run(g, bc, f, g.dt, 2, solver=1, sor=1.7, tol=1e-8, check_every=50)
+        assert st == 0
+        sm.step(2)
+        for n in ("un", "vn", "wn"):
+            assert rel_l2(sm.get(n), getattr(f, n)) <= 1e-6, n
+
+
+def test_mixed_periodic_y():
+    g = O.Grid(32, 16, 16, lx=1.3, ly=0.9, lz=1.1, re=700.0, dt=1e-3)
+    bc = O.BC((True, True, True))
+    f = random_fields(g, 17, "zinv", scale=0.2)
+    sp, sm = _pair(g, bc, f, 1e-10)
+    with sp, sm:
+        stp = sp.pressure_projection(0.5e-3)
+        stm = sm.pressure_projection(0.5e-3)
+        assert stp.status == 0 and stm.status == 0 and stm.variant > 100
+        for n in ("un", "vn", "wn"):
+            assert rel_l2(sm.get(n), sp.get(n)) <= 1e-6, n
+
+
+def test_mixed_falls_back_to_fp64_for_other_boundaries():
+    """Walls with Dirichlet pressure (the mixed path needs Neumann): the FP64 path runs, bit for bit."""
+    g = O.Grid(32, 16, 16, lx=1.3, ly=0.9, lz=1.1, re=700.0, dt=1e-3)
+    bc = O.channel_bc().set(2, 0, 0, typ=0).set(2, 1, 0, typ=0)
+    f = random_fields(g, 18, scale=0.2)
+    sp, sm = _pair(g, bc, f, 1e-8)
+    with sp, sm:
+        stp = sp.pressure_projection(0.5e-3)
+        stm = sm.pressure_projection(0.5e-3)
+        assert stm.variant < 100 and stm.iterations == stp.iterations
+        for n in ("un", "vn", "wn", "pn"):
+            assert np.array_equal(sm.get(n), sp.get(n)), n
