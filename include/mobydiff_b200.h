@@ -110,9 +110,18 @@ typedef struct {
     double residual;    /* final ||div u||2 / ||div u*||2 (red-black)        */
     double residual0;   /* ||div u*||2                                       */
     double atol;        /* absolute floor used (red-black)                   */
-    int variant;        /* red-black kernel variant of the last iterations   */
-    int reserved;
+    int variant;        /* red-black kernel variant of the last iterations;
+                           100 + n: mixed precision with n FP64 corrections */
+    int guessed;        /* 1 when a warm-start guess was applied             */
 } mdx_solve_stats_t;
+
+/* Warm starts of the red-black projection (no counterpart in the reference,
+ * which starts every projection from phi = 0). */
+#define MDX_GUESS_ZERO        0   /* the reference's start                          */
+#define MDX_GUESS_PREVIOUS    1   /* increment of the same RK substage, previous step */
+#define MDX_GUESS_LEARNED     2   /* extrapolated increment plus the U-Net's correction
+                                     predicted from the divergence it leaves           */
+#define MDX_GUESS_EXTRAPOLATED 3  /* 2*dp(n-1) - dp(n-2) of the same RK substage      */
 
 /* Per-kernel-class device time, filled when timing is on (mdx_set_timing). */
 enum {
@@ -250,6 +259,21 @@ int mdx_pressure_projection(mdx_ctx_t* ctx, double dt_gamma, mdx_solve_stats_t* 
 /* Statistics of the last pressure projection (including those run inside
  * mdx_step). */
 int mdx_last_solve_stats(const mdx_ctx_t* ctx, mdx_solve_stats_t* stats);
+
+/* Warm start of the red-black projection: mode MDX_GUESS_*; record != 0
+ * keeps the pressure increment of every projection (p_after - p_before, per
+ * RK substage, projections numbered in call order, three per step) even
+ * without a guess.  The guess is applied as the sweeps apply phi and the
+ * projection still runs to its tolerance relative to ||div u*||; a guess
+ * that does not lower ||div u|| below ||div u*|| is undone (with tol > 0).
+ * Needs periodic x and z and y periodic or Neumann-pressure walls
+ * (otherwise no guess is applied).  The t=0 projection of mdx_channel_ic
+ * resets the history. */
+int mdx_set_pressure_guess(mdx_ctx_t* ctx, int mode, int record);
+
+/* Copy the recorded increment of RK substage s (0..2) to host (nx,ny,nz)
+ * cells, x fastest (synchronises); MDX_ERR_STATE if none was recorded. */
+int mdx_get_increment(mdx_ctx_t* ctx, int substage, double* host);
 
 /* get_cfl, src/modules/step.f90:210-258 (synchronises). */
 int mdx_get_cfl(mdx_ctx_t* ctx, double* cfl);

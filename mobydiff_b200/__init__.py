@@ -48,6 +48,10 @@ SOLVER_FFT = 0
 SOLVER_REDBLACK = 1
 PREC_FP64 = 0
 PREC_MIXED = 1
+GUESS_ZERO = 0
+GUESS_PREVIOUS = 1
+GUESS_LEARNED = 2
+GUESS_EXTRAPOLATED = 3
 
 FIELDS = ["un", "us", "vn", "vs", "wn", "ws", "pn", "oldrhsu", "oldrhsv", "oldrhsw",
           "coef_u", "coef_v", "coef_w", "phi"]
@@ -85,7 +89,7 @@ class SolverOptsT(C.Structure):
 
 class SolveStatsT(C.Structure):
     _fields_ = [("iterations", C.c_int), ("status", C.c_int), ("residual", C.c_double), ("residual0", C.c_double),
-                ("atol", C.c_double), ("variant", C.c_int), ("reserved", C.c_int)]
+                ("atol", C.c_double), ("variant", C.c_int), ("guessed", C.c_int)]
 
 
 class TimingT(C.Structure):
@@ -156,6 +160,8 @@ def lib():
         "mdx_get_timing": (i, [vp, P(TimingT)]),
         "mdx_launch_count": (C.c_longlong, [vp]),
         "mdx_last_solve_stats": (i, [vp, P(SolveStatsT)]),
+        "mdx_set_pressure_guess": (i, [vp, i, i]),
+        "mdx_get_increment": (i, [vp, i, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -412,6 +418,20 @@ class Solver:
         st = SolveStatsT()
         self._c(lib().mdx_last_solve_stats(self.h, C.byref(st)))
         return st
+
+    def set_pressure_guess(self, mode: int, record: bool = True) -> None:
+        """Warm start of the red-black projection: GUESS_ZERO, GUESS_PREVIOUS
+        (the same substage's increment of the previous step) or GUESS_LEARNED
+        (U-Net prediction); `record` keeps the increments of every projection."""
+        self._c(lib().mdx_set_pressure_guess(self.h, int(mode), 1 if record else 0))
+
+    def get_increment(self, substage: int) -> np.ndarray:
+        """Pressure increment of the last projection of RK substage 0..2 over
+        the interior cells, indexed [k, j, i] like the fields."""
+        g = self.grid
+        out = np.empty(g.nx * g.ny * g.nz, dtype=np.float64)
+        self._c(lib().mdx_get_increment(self.h, int(substage), out.ctypes.data_as(C.c_void_p)))
+        return out.reshape((g.nz, g.ny, g.nx))
 
     def stream(self) -> int:
         s = C.c_void_p()

@@ -31,6 +31,8 @@ CUDA_SOURCES = {
     "k_fft.cu": ["-fmad=false"],
     "k_sor.cu": ["-fmad=false"],
     "k_sor_mixed.cu": [],   # FP32 sweeps inside FP64 defect correction: FMA allowed
+    "k_warm.cu": ["-fmad=false"],
+    "k_unet.cu": [],        # BF16 network with FP32 accumulation: FMA allowed
 }
 CXX_SOURCES = ["host_config.cpp"]
 

@@ -220,6 +220,7 @@ int mdx_destroy_pressure_solver(mdx_ctx_t* ctx) {
     ctx->mu = nullptr;
     ctx->mu_elems = 0;
     mdx_mixed_free(ctx);
+    mdx_warm_free(ctx);
     ctx->solver = false;
     return MDX_OK;
 }
@@ -237,6 +238,7 @@ int mdx_exit_field_data(mdx_ctx_t* ctx) {
         cudaFree(ctx->sor_alt[t]);
         ctx->sor_alt[t] = nullptr;
     }
+    mdx_warm_free(ctx);
     ctx->fields = false;
     return MDX_OK;
 }
@@ -576,14 +578,25 @@ int mdx_channel_ic(mdx_ctx_t* ctx, uint64_t seed, double amp_u, double amp_vw, d
     MDX_CUDA(ctx, cudaMemcpyAsync(f[MDX_VS], f[MDX_VN], bytes, cudaMemcpyDeviceToDevice, ctx->stream));
     MDX_CUDA(ctx, cudaMemcpyAsync(f[MDX_WS], f[MDX_WN], bytes, cudaMemcpyDeviceToDevice, ctx->stream));
     mdx_solve_stats_t s{};
+    // the t=0 projection takes no guess and starts the increment history afresh
+    const int guess_mode = ctx->guess_mode;
+    const bool record = ctx->record_increments;
+    ctx->guess_mode = MDX_GUESS_ZERO;
+    ctx->record_increments = false;
+    int rc = MDX_OK;
     if (ctx->opts.solver == MDX_SOLVER_FFT) {
-        MDX_TRY(mdx_k_apply_bc(ctx));
-        MDX_TRY(mdx_k_projection_fft(ctx, 1.0));
-        MDX_TRY(mdx_k_apply_bc(ctx));
+        rc = mdx_k_apply_bc(ctx);
+        if (rc == MDX_OK) rc = mdx_k_projection_fft(ctx, 1.0);
+        if (rc == MDX_OK) rc = mdx_k_apply_bc(ctx);
     } else {
-        MDX_TRY(mdx_k_projection_redblack(ctx, 1.0, &s));
-        MDX_TRY(mdx_k_apply_bc_redblack(ctx));
+        rc = mdx_k_projection_redblack(ctx, 1.0, &s);
+        if (rc == MDX_OK) rc = mdx_k_apply_bc_redblack(ctx);
     }
+    ctx->guess_mode = guess_mode;
+    ctx->record_increments = record;
+    ctx->proj_count = 0;
+    ctx->hist_valid = 0;
+    MDX_TRY(rc);
     MDX_CUDA(ctx, cudaMemsetAsync(f[MDX_PN], 0, bytes, ctx->stream));
     MDX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     if (stats) *stats = s;

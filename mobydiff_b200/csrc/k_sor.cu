@@ -632,10 +632,45 @@ int mdx_k_projection_redblack(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t* st) 
     MDX_CUDA(ctx, cudaMemcpyAsync(f[MDX_VN], f[MDX_VS], bytes, cudaMemcpyDeviceToDevice, ctx->stream));
     MDX_CUDA(ctx, cudaMemcpyAsync(f[MDX_WN], f[MDX_WS], bytes, cudaMemcpyDeviceToDevice, ctx->stream));
     MDX_TRY(mu_tables(ctx, dg));
-    if (ctx->opts.precision == MDX_PREC_MIXED) {   // FP32 sweeps in FP64 defect correction
+    const mdx_solver_opts_t& o = ctx->opts;
+    // Residual scale of this projection, on u* before any guess: converged
+    // when ||div u|| <= max(tol*||div u*||, atol); the default atol is the
+    // round-off level of the divergence, below which a relative target
+    // cannot be met once u* is nearly solenoidal.
+    double r0 = 0.0, umax = 0.0, atol = 0.0, target = 0.0;
+    if (o.tol > 0.0) {
+        double linf = 0.0;
+        MDX_TRY(mdx_k_div_norms(ctx, f[MDX_UN], f[MDX_VN], f[MDX_WN], &r0, &linf, &umax));
+        atol = (o.atol < 0.0) ? mdx_div_floor(ctx, umax) : o.atol;
+        target = std::max(o.tol * r0, atol);
+    }
+    // warm start: record this projection's increment; apply a guess
+    const bool warm = mdx_guess_supported(ctx) && (ctx->guess_mode != MDX_GUESS_ZERO || ctx->record_increments);
+    if (warm) MDX_TRY(mdx_warm_begin(ctx));
+    bool guessed = false;
+    double rg = r0;   // ||div u|| after the guess
+    if (warm && ctx->guess_mode != MDX_GUESS_ZERO) MDX_TRY(mdx_make_guess(ctx, dg, &guessed));
+    if (guessed) {
+        MDX_TRY(mdx_apply_guess(ctx, dg, ctx->mu_mode));
+        if (o.tol > 0.0) {   // a guess that does not lower the divergence is undone
+            double linf = 0.0;
+            MDX_TRY(mdx_k_div_norms(ctx, f[MDX_UN], f[MDX_VN], f[MDX_WN], &rg, &linf));
+            if (!(rg < r0)) {
+                MDX_TRY(mdx_undo_guess(ctx));
+                rg = r0;
+                guessed = false;
+            }
+        }
+    }
+    if (o.precision == MDX_PREC_MIXED) {   // FP32 sweeps in FP64 defect correction
         bool handled = false;
-        MDX_TRY(mdx_k_projection_redblack_mixed(ctx, dg, st, &handled));
-        if (handled) return MDX_OK;
+        MDX_TRY(mdx_k_projection_redblack_mixed(ctx, dg, st, &handled, r0, umax, atol));
+        if (handled) {
+            ctx->last.guessed = guessed ? 1 : 0;
+            if (st) st->guessed = ctx->last.guessed;
+            if (warm) MDX_TRY(mdx_warm_end(ctx));
+            return MDX_OK;
+        }
     }
     // kernel variant: the requested one, the tuned one, or -- while tuning --
     // the next untried candidate for each residual-check block
@@ -657,7 +692,7 @@ int mdx_k_projection_redblack(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t* st) 
         return best;
     };
     mdx_solve_stats_t s{};
-    const mdx_solver_opts_t& o = ctx->opts;
+    s.guessed = guessed ? 1 : 0;
     if (o.tol <= 0.0) {
         const int v = (want == MDX_SORV_AUTO) ? (ctx->sor_tuned > 0 ? ctx->sor_tuned : MDX_SORV_SWEEPS) : want;
         for (int it = 0; it < o.n_iter; ++it) MDX_TRY(sor_iterate(ctx, p, v));
@@ -665,24 +700,17 @@ int mdx_k_projection_redblack(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t* st) 
         s.iterations = o.n_iter;
         s.status = MDX_OK;
     } else {
-        double r0 = 0.0, linf = 0.0, r = 0.0, umax = 0.0;
-        MDX_TRY(mdx_k_div_norms(ctx, f[MDX_UN], f[MDX_VN], f[MDX_WN], &r0, &linf, &umax));
+        double linf = 0.0, r = rg;
         s.residual0 = r0;
-        // converged when ||div u|| <= max(tol*||div u*||, atol); the default
-        // atol is the round-off level of the divergence, below which a
-        // relative target cannot be met once u* is nearly solenoidal
-        const double atol = (o.atol < 0.0) ? mdx_div_floor(ctx, umax) : o.atol;
         s.atol = atol;
-        const double target = std::max(o.tol * r0, atol);
-        if (!std::isfinite(r0) || !std::isfinite(umax)) {
+        if (!std::isfinite(r0) || !std::isfinite(umax) || !std::isfinite(r)) {
             s.status = MDX_ERR_NONFINITE;
-        } else if (r0 <= target) {
+        } else if (r <= target) {
             s.status = MDX_OK;
-            s.residual = (r0 > 0.0) ? 1.0 : 0.0;
+            s.residual = (r0 > 0.0) ? r / r0 : 0.0;
         } else {
             int it = 0;
             s.status = MDX_NOT_CONVERGED;
-            r = r0;
             while (it < o.max_iter) {
                 const int m = std::min(o.check_every, o.max_iter - it);
                 const int v = pick();
@@ -705,6 +733,7 @@ int mdx_k_projection_redblack(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t* st) 
             s.residual = r / r0;
         }
     }
+    if (warm) MDX_TRY(mdx_warm_end(ctx));
     ctx->last = s;
     if (st) *st = s;
     return MDX_OK;

@@ -236,8 +236,11 @@ void mdx_mixed_free(mdx_ctx_t* ctx) {
     }
 }
 
-// Called after u <- u* and the FP64 IBM factors of this projection.
-int mdx_k_projection_redblack_mixed(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t* st, bool* handled) {
+// Called after u <- u*, the FP64 IBM factors of this projection and any
+// warm-start guess; r0 and umax are ||div u*|| and max|u*| before the guess,
+// atol the absolute floor.
+int mdx_k_projection_redblack_mixed(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t* st, bool* handled, double r0,
+                                    double umax, double atol) {
     *handled = false;
     if (!mixed_supported(ctx) || ctx->opts.tol <= 0.0) return MDX_OK;
     *handled = true;
@@ -293,20 +296,18 @@ int mdx_k_projection_redblack_mixed(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t
     };
 
     mdx_solve_stats_t s{};
-    double r0 = 0.0, umax = 0.0;
-    MDX_TRY(residual(&r0, &umax));
+    double r = 0.0;
+    MDX_TRY(residual(&r, nullptr));   // r~ of the current (possibly warm-started) state
     s.residual0 = r0;
-    const double atol = (o.atol < 0.0) ? mdx_div_floor(ctx, umax) : o.atol;
     s.atol = atol;
     const double target = std::max(o.tol * r0, atol);
-    double r = r0;
     int it = 0, outer = 0;
     s.status = MDX_NOT_CONVERGED;
-    if (!std::isfinite(r0) || !std::isfinite(umax)) {
+    if (!std::isfinite(r0) || !std::isfinite(umax) || !std::isfinite(r)) {
         s.status = MDX_ERR_NONFINITE;
-    } else if (r0 <= target) {
+    } else if (r <= target) {
         s.status = MDX_OK;
-        s.residual = r0 > 0.0 ? 1.0 : 0.0;
+        s.residual = r0 > 0.0 ? r / r0 : 0.0;
     } else {
         // FP32 resolves a correction to about 1e-5 of its right-hand side
         const double inner_rel = 1e-5;

@@ -80,6 +80,16 @@ struct mdx_ctx {
     // mixed-precision red-black: FP32 corrections, FP32 residual, IBM tables
     float *mx_du = nullptr, *mx_dv = nullptr, *mx_dw = nullptr, *mx_dp = nullptr, *mx_r = nullptr;
     float *mx_mu = nullptr, *mx_fac = nullptr;
+    // warm starts: increments of the last projection of each RK substage
+    int guess_mode = 0;                      // MDX_GUESS_*
+    bool record_increments = false;
+    double* dp_hist[3] = {nullptr, nullptr, nullptr};   // (nx,ny,nz) cells, previous step
+    double* dp_hist2[3] = {nullptr, nullptr, nullptr};  // the step before
+    double* p_before = nullptr;              // padded p at the start of the projection
+    double* guess = nullptr;                 // increment guess of the current projection
+    int hist_valid = 0;                      // bit s: dp_hist[s] holds an increment; bit 3+s: dp_hist2[s]
+    long long proj_count = 0;                // projections since the t=0 projection
+    void* unet = nullptr;                    // learned warm start (k_unet.cu)
     int sor_tuned = 0;                       // red-black kernel variant chosen by the autotuner (0: not yet)
     double sor_tune_ms[4] = {0.0};           // time of one residual-check block per variant
     cudaEvent_t tune_ev[2] = {nullptr, nullptr};
@@ -164,8 +174,19 @@ int mdx_k_div_norms(mdx_ctx_t* ctx, const double* u, const double* v, const doub
 double mdx_div_floor(const mdx_ctx_t* ctx, double umax);
 int mdx_reduce_partials(mdx_ctx_t* ctx, double* sum, double* max1, double* max2);
 #define MDX_RED_THREADS 256
-int mdx_k_projection_redblack_mixed(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t* st, bool* handled);
+int mdx_k_projection_redblack_mixed(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t* st, bool* handled, double r0,
+                                    double umax, double atol);
 void mdx_mixed_free(mdx_ctx_t* ctx);
+// warm starts (k_warm.cu, k_unet.cu)
+bool mdx_guess_supported(const mdx_ctx_t* ctx);
+int mdx_warm_alloc(mdx_ctx_t* ctx);
+void mdx_warm_free(mdx_ctx_t* ctx);
+int mdx_warm_begin(mdx_ctx_t* ctx);
+int mdx_warm_end(mdx_ctx_t* ctx);
+int mdx_apply_guess(mdx_ctx_t* ctx, double dg, int mu_mode);
+int mdx_undo_guess(mdx_ctx_t* ctx);
+int mdx_make_guess(mdx_ctx_t* ctx, double dg, bool* made);
+int mdx_unet_guess(mdx_ctx_t* ctx, double dg, bool* made);
 int mdx_k_div_norms_async(mdx_ctx_t* ctx, const double* u, const double* v, const double* w);
 int mdx_k_cfl(mdx_ctx_t* ctx, double* cfl);
 int mdx_k_center_vel(mdx_ctx_t* ctx, double* uc, double* vc, double* wc);

@@ -37,7 +37,7 @@ module mdx_bindings
     type, bind(C) :: mdx_solve_stats_t
         integer(C_INT) :: iterations, status
         real(C_DOUBLE) :: residual, residual0, atol
-        integer(C_INT) :: variant, reserved
+        integer(C_INT) :: variant, guessed
     end type mdx_solve_stats_t
 
     interface
