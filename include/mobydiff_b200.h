@@ -275,6 +275,70 @@ int mdx_set_pressure_guess(mdx_ctx_t* ctx, int mode, int record);
  * cells, x fastest (synchronises); MDX_ERR_STATE if none was recorded. */
 int mdx_get_increment(mdx_ctx_t* ctx, int substage, double* host);
 
+/* ---- learned warm start (no counterpart in the reference) ----------------
+ * A 4-level 3-D U-Net on the cells of the grid (channels-last BF16
+ * activations and weights, FP32 accumulation on the tensor cores).  With
+ * mode MDX_GUESS_LEARNED, once the extrapolated increment has been applied,
+ * the net maps four per-cell inputs
+ *     div u left by the extrapolated guess / its RMS,
+ *     dp(n-1) / RMS(dp(n-1)),  dp(n-2) / RMS(dp(n-1)),  IBM factor mu of the cell
+ * to a correction of the increment, out * out_scale * RMS(div) * h2 / dt_gamma
+ * with h2 = 1/(1/dx^2+1/dy^2+1/dz^2).  A correction that does not lower
+ * ||div u|| is undone; the sweeps then run to the usual tolerance.
+ * The net is trained on the device (Adam, FP32 master weights) on
+ * snapshots the projection records: inputs as above and the target
+ * (dp_converged - dp_extrapolated) * dt_gamma / (RMS(div) * h2).
+ * Needs nx, ny, nz multiples of 8 and the warm-start boundary conditions. */
+typedef struct {
+    int channels0;          /* channels at full resolution: 16                  */
+    int channels;           /* channels of the three coarser levels: 16 or 32   */
+    int extra_bottleneck;   /* extra 3x3x3 convolutions at the coarsest level, 0..8 */
+    int capacity;           /* snapshots kept on the device for training        */
+    double slope;           /* leaky-ReLU slope, (0, 1]; 1 makes the net linear */
+    uint64_t seed;          /* weight initialisation                            */
+    int reserved_i[8];
+    double reserved_d[8];
+} mdx_unet_opts_t;
+
+typedef struct {
+    long long corrections;  /* learned corrections applied                      */
+    long long rejected;     /* corrections undone (did not lower ||div u||)     */
+    long long snapshots;    /* snapshots recorded since creation                */
+    int stored;             /* snapshots held now (<= capacity)                 */
+    int trained;            /* weights trained or set                           */
+    double out_scale;       /* output scale of the net                          */
+    double last_gain;       /* ||div|| after the extrapolated guess / after the correction */
+    double infer_ms;        /* device time of the last correction               */
+    double train_ms;        /* device time of the last mdx_unet_train call      */
+    double reserved_d[6];
+} mdx_unet_stats_t;
+
+void mdx_default_unet_opts(mdx_unet_opts_t* opts);
+int mdx_unet_create(mdx_ctx_t* ctx, const mdx_unet_opts_t* opts);
+int mdx_unet_destroy(mdx_ctx_t* ctx);
+/* Record a snapshot in every converged projection that had an extrapolated
+ * guess (guess mode MDX_GUESS_EXTRAPOLATED or MDX_GUESS_LEARNED); the oldest
+ * is overwritten once `capacity` are held. */
+int mdx_unet_record(mdx_ctx_t* ctx, int on);
+/* `iters` Adam steps (one snapshot each, in a seeded random order) at
+ * learning rate lr; the mean-square loss of the first and the last step. */
+int mdx_unet_train(mdx_ctx_t* ctx, int iters, double lr, double* loss_first, double* loss_last);
+/* Parameters, FP32, in this order per 3x3x3 convolution: W[tap][cout][cin]
+ * (tap = 9*(dz+1) + 3*(dy+1) + (dx+1)), bias[cout]; then the 1x1 head
+ * w[channels0], b.  Convolutions in the order enc0a, enc0b, enc1a, enc1b,
+ * enc2a, enc2b, enc3a, enc3b, the extra bottleneck ones, dec2, dec1, dec0. */
+long long mdx_unet_param_count(const mdx_ctx_t* ctx);
+int mdx_unet_get_params(mdx_ctx_t* ctx, float* host, long long n);
+int mdx_unet_set_params(mdx_ctx_t* ctx, const float* host, long long n);   /* marks the net trained */
+int mdx_unet_get_out_scale(mdx_ctx_t* ctx, double* scale);
+int mdx_unet_set_out_scale(mdx_ctx_t* ctx, double scale);
+/* One forward and backward pass on host inputs in4 [4][ncells] and target
+ * [ncells] (cells x fastest): loss = mean((out - target)^2), its gradient
+ * with respect to every parameter (param_count floats) and the output
+ * [ncells].  No update; used to check the kernels against a CPU network. */
+int mdx_unet_loss_grad(mdx_ctx_t* ctx, const float* in4, const float* target, double* loss, float* grad, float* out);
+int mdx_unet_stats(mdx_ctx_t* ctx, mdx_unet_stats_t* stats);
+
 /* get_cfl, src/modules/step.f90:210-258 (synchronises). */
 int mdx_get_cfl(mdx_ctx_t* ctx, double* cfl);
 

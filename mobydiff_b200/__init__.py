@@ -92,6 +92,17 @@ class SolveStatsT(C.Structure):
                 ("atol", C.c_double), ("variant", C.c_int), ("guessed", C.c_int)]
 
 
+class UnetOptsT(C.Structure):
+    _fields_ = [("channels0", C.c_int), ("channels", C.c_int), ("extra_bottleneck", C.c_int), ("capacity", C.c_int),
+                ("slope", C.c_double), ("seed", C.c_uint64), ("reserved_i", C.c_int * 8), ("reserved_d", C.c_double * 8)]
+
+
+class UnetStatsT(C.Structure):
+    _fields_ = [("corrections", C.c_longlong), ("rejected", C.c_longlong), ("snapshots", C.c_longlong),
+                ("stored", C.c_int), ("trained", C.c_int), ("out_scale", C.c_double), ("last_gain", C.c_double),
+                ("infer_ms", C.c_double), ("train_ms", C.c_double), ("reserved_d", C.c_double * 6)]
+
+
 class TimingT(C.Structure):
     _fields_ = [("ms", C.c_double * 9), ("launches", C.c_longlong * 9)]
 
@@ -162,6 +173,18 @@ def lib():
         "mdx_last_solve_stats": (i, [vp, P(SolveStatsT)]),
         "mdx_set_pressure_guess": (i, [vp, i, i]),
         "mdx_get_increment": (i, [vp, i, vp]),
+        "mdx_default_unet_opts": (None, [P(UnetOptsT)]),
+        "mdx_unet_create": (i, [vp, P(UnetOptsT)]),
+        "mdx_unet_destroy": (i, [vp]),
+        "mdx_unet_record": (i, [vp, i]),
+        "mdx_unet_train": (i, [vp, i, d, P(d), P(d)]),
+        "mdx_unet_param_count": (C.c_longlong, [vp]),
+        "mdx_unet_get_params": (i, [vp, vp, C.c_longlong]),
+        "mdx_unet_set_params": (i, [vp, vp, C.c_longlong]),
+        "mdx_unet_get_out_scale": (i, [vp, P(d)]),
+        "mdx_unet_set_out_scale": (i, [vp, d]),
+        "mdx_unet_loss_grad": (i, [vp, vp, vp, P(d), vp, vp]),
+        "mdx_unet_stats": (i, [vp, P(UnetStatsT)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -424,6 +447,67 @@ class Solver:
         (the same substage's increment of the previous step) or GUESS_LEARNED
         (U-Net prediction); `record` keeps the increments of every projection."""
         self._c(lib().mdx_set_pressure_guess(self.h, int(mode), 1 if record else 0))
+
+    # ---- learned warm start ----------------------------------------------
+    def unet_create(self, channels: int = 32, extra_bottleneck: int = 0, capacity: int = 64, slope: float = 0.1,
+                    seed: int = 20261203) -> None:
+        o = UnetOptsT()
+        lib().mdx_default_unet_opts(C.byref(o))
+        o.channels = channels
+        o.extra_bottleneck = extra_bottleneck
+        o.capacity = capacity
+        o.slope = slope
+        o.seed = seed
+        self._c(lib().mdx_unet_create(self.h, C.byref(o)))
+
+    def unet_destroy(self) -> None:
+        self._c(lib().mdx_unet_destroy(self.h))
+
+    def unet_record(self, on: bool = True) -> None:
+        self._c(lib().mdx_unet_record(self.h, 1 if on else 0))
+
+    def unet_train(self, iters: int, lr: float = 1e-3):
+        """Adam steps on the recorded snapshots; (first loss, last loss)."""
+        a, b = C.c_double(0.0), C.c_double(0.0)
+        self._c(lib().mdx_unet_train(self.h, int(iters), float(lr), C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def unet_param_count(self) -> int:
+        return int(lib().mdx_unet_param_count(self.h))
+
+    def unet_params(self) -> np.ndarray:
+        p = np.empty(self.unet_param_count(), dtype=np.float32)
+        self._c(lib().mdx_unet_get_params(self.h, p.ctypes.data_as(C.c_void_p), p.size))
+        return p
+
+    def unet_set_params(self, p) -> None:
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        self._c(lib().mdx_unet_set_params(self.h, p.ctypes.data_as(C.c_void_p), p.size))
+
+    def unet_out_scale(self, value: float | None = None) -> float:
+        if value is not None:
+            self._c(lib().mdx_unet_set_out_scale(self.h, float(value)))
+        v = C.c_double(0.0)
+        self._c(lib().mdx_unet_get_out_scale(self.h, C.byref(v)))
+        return v.value
+
+    def unet_loss_grad(self, in4, target):
+        """One forward/backward pass on host inputs [4][n] and target [n]:
+        (loss, gradient [param_count], output [n])."""
+        in4 = np.ascontiguousarray(in4, dtype=np.float32)
+        target = np.ascontiguousarray(target, dtype=np.float32)
+        grad = np.empty(self.unet_param_count(), dtype=np.float32)
+        out = np.empty(target.size, dtype=np.float32)
+        loss = C.c_double(0.0)
+        self._c(lib().mdx_unet_loss_grad(self.h, in4.ctypes.data_as(C.c_void_p), target.ctypes.data_as(C.c_void_p),
+                                         C.byref(loss), grad.ctypes.data_as(C.c_void_p),
+                                         out.ctypes.data_as(C.c_void_p)))
+        return loss.value, grad, out
+
+    def unet_stats(self) -> UnetStatsT:
+        st = UnetStatsT()
+        self._c(lib().mdx_unet_stats(self.h, C.byref(st)))
+        return st
 
     def get_increment(self, substage: int) -> np.ndarray:
         """Pressure increment of the last projection of RK substage 0..2 over

@@ -239,6 +239,7 @@ int mdx_exit_field_data(mdx_ctx_t* ctx) {
         ctx->sor_alt[t] = nullptr;
     }
     mdx_warm_free(ctx);
+    mdx_unet_free(ctx);
     ctx->fields = false;
     return MDX_OK;
 }

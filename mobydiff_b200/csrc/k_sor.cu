@@ -649,26 +649,14 @@ int mdx_k_projection_redblack(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t* st) 
     if (warm) MDX_TRY(mdx_warm_begin(ctx));
     bool guessed = false;
     double rg = r0;   // ||div u|| after the guess
-    if (warm && ctx->guess_mode != MDX_GUESS_ZERO) MDX_TRY(mdx_make_guess(ctx, dg, &guessed));
-    if (guessed) {
-        MDX_TRY(mdx_apply_guess(ctx, dg, ctx->mu_mode));
-        if (o.tol > 0.0) {   // a guess that does not lower the divergence is undone
-            double linf = 0.0;
-            MDX_TRY(mdx_k_div_norms(ctx, f[MDX_UN], f[MDX_VN], f[MDX_WN], &rg, &linf));
-            if (!(rg < r0)) {
-                MDX_TRY(mdx_undo_guess(ctx));
-                rg = r0;
-                guessed = false;
-            }
-        }
-    }
+    if (warm && ctx->guess_mode != MDX_GUESS_ZERO) MDX_TRY(mdx_guess_apply(ctx, dg, r0, &guessed, &rg));
     if (o.precision == MDX_PREC_MIXED) {   // FP32 sweeps in FP64 defect correction
         bool handled = false;
         MDX_TRY(mdx_k_projection_redblack_mixed(ctx, dg, st, &handled, r0, umax, atol));
         if (handled) {
             ctx->last.guessed = guessed ? 1 : 0;
             if (st) st->guessed = ctx->last.guessed;
-            if (warm) MDX_TRY(mdx_warm_end(ctx));
+            if (warm) MDX_TRY(mdx_warm_end(ctx, ctx->last.status == MDX_OK));
             return MDX_OK;
         }
     }
@@ -733,7 +721,7 @@ int mdx_k_projection_redblack(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t* st) 
             s.residual = r / r0;
         }
     }
-    if (warm) MDX_TRY(mdx_warm_end(ctx));
+    if (warm) MDX_TRY(mdx_warm_end(ctx, o.tol > 0.0 && s.status == MDX_OK));
     ctx->last = s;
     if (st) *st = s;
     return MDX_OK;

@@ -129,7 +129,7 @@ int mdx_warm_begin(mdx_ctx_t* ctx) {
     return MDX_OK;
 }
 
-int mdx_warm_end(mdx_ctx_t* ctx) {
+int mdx_warm_end(mdx_ctx_t* ctx, bool converged) {
     const int s = (int)(ctx->proj_count % 3);
     const mdx_dims& d = ctx->d;
     const int nb = (int)std::min<long long>((d.nint + 255) / 256, 8192);
@@ -139,6 +139,7 @@ int mdx_warm_end(mdx_ctx_t* ctx) {
     MDX_LAUNCH(ctx, MDX_T_OTHER, "record increment", k_record_increment, nb, 256, 0, d, ctx->f[MDX_PN], ctx->p_before,
                ctx->dp_hist[s]);
     ctx->hist_valid |= 1 << s;
+    if (ctx->unet) MDX_TRY(mdx_unet_finish(ctx, converged));
     ctx->proj_count++;
     return MDX_OK;
 }
@@ -154,9 +155,10 @@ int mdx_undo_guess(mdx_ctx_t* ctx) {
     return MDX_OK;
 }
 
-// Apply ctx->guess (the increment guess of this projection) with the IBM
-// factors of mode `mu_mode` (0 one, 1 planes, 2 padded) in ctx->mu.
-int mdx_apply_guess(mdx_ctx_t* ctx, double dg, int mu_mode) {
+// Apply the increment guess gs (cells) with the IBM factors of this
+// projection (ctx->mu in mode ctx->mu_mode: 0 one, 1 planes, 2 padded).
+int mdx_apply_guess(mdx_ctx_t* ctx, const double* gs, double dg) {
+    const int mu_mode = ctx->mu_mode;
     const mdx_dims& d = ctx->d;
     const mdx_grid_t& g = ctx->g;
     double** f = ctx->f;
@@ -165,14 +167,14 @@ int mdx_apply_guess(mdx_ctx_t* ctx, double dg, int mu_mode) {
     auto kfn = mu_mode == 1 ? (py ? k_apply_guess<1, 1> : k_apply_guess<1, 0>)
                             : (mu_mode == 2 ? (py ? k_apply_guess<2, 1> : k_apply_guess<2, 0>)
                                             : (py ? k_apply_guess<0, 1> : k_apply_guess<0, 0>));
-    MDX_LAUNCH(ctx, MDX_T_OTHER, "apply guess", kfn, nb, 256, 0, d, dg, 1.0 / g.dx, 1.0 / g.dy, 1.0 / g.dz, ctx->guess,
+    MDX_LAUNCH(ctx, MDX_T_OTHER, "apply guess", kfn, nb, 256, 0, d, dg, 1.0 / g.dx, 1.0 / g.dy, 1.0 / g.dz, gs,
                ctx->mu, f[MDX_UN], f[MDX_VN], f[MDX_WN], f[MDX_PN]);
     return MDX_OK;
 }
 
 // The guess of this projection into ctx->guess; *made = false when none is
 // available (no history yet, no trained network).
-int mdx_make_guess(mdx_ctx_t* ctx, double dg, bool* made) {
+int mdx_make_guess(mdx_ctx_t* ctx, bool* made) {
     *made = false;
     if (ctx->guess_mode == MDX_GUESS_ZERO) return MDX_OK;
     const int s = (int)(ctx->proj_count % 3);
@@ -187,7 +189,27 @@ int mdx_make_guess(mdx_ctx_t* ctx, double dg, bool* made) {
                                       ctx->stream));
     }
     *made = true;
-    if (ctx->guess_mode == MDX_GUESS_LEARNED) return mdx_unet_guess(ctx, dg, made);
+    return MDX_OK;
+}
+
+int mdx_guess_apply(mdx_ctx_t* ctx, double dg, double r0, bool* guessed, double* rg) {
+    *guessed = false;
+    *rg = r0;
+    bool made = false;
+    MDX_TRY(mdx_make_guess(ctx, &made));
+    if (!made) return MDX_OK;
+    MDX_TRY(mdx_apply_guess(ctx, ctx->guess, dg));
+    double r = r0;
+    if (ctx->opts.tol > 0.0) {   // a guess that does not lower the divergence is undone
+        double linf = 0.0;
+        MDX_TRY(mdx_k_div_norms(ctx, ctx->f[MDX_UN], ctx->f[MDX_VN], ctx->f[MDX_WN], &r, &linf));
+        if (!(r < r0)) return mdx_undo_guess(ctx);
+    }
+    *guessed = true;
+    *rg = r;
+    const int s = (int)(ctx->proj_count % 3);
+    if (ctx->unet && ctx->guess_mode != MDX_GUESS_PREVIOUS && (ctx->hist_valid & (8 << s)))
+        MDX_TRY(mdx_unet_correct(ctx, dg, rg));
     return MDX_OK;
 }
 

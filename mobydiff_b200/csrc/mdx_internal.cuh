@@ -182,11 +182,17 @@ bool mdx_guess_supported(const mdx_ctx_t* ctx);
 int mdx_warm_alloc(mdx_ctx_t* ctx);
 void mdx_warm_free(mdx_ctx_t* ctx);
 int mdx_warm_begin(mdx_ctx_t* ctx);
-int mdx_warm_end(mdx_ctx_t* ctx);
-int mdx_apply_guess(mdx_ctx_t* ctx, double dg, int mu_mode);
+int mdx_warm_end(mdx_ctx_t* ctx, bool converged);
+int mdx_apply_guess(mdx_ctx_t* ctx, const double* gs, double dg);
 int mdx_undo_guess(mdx_ctx_t* ctx);
-int mdx_make_guess(mdx_ctx_t* ctx, double dg, bool* made);
-int mdx_unet_guess(mdx_ctx_t* ctx, double dg, bool* made);
+int mdx_make_guess(mdx_ctx_t* ctx, bool* made);
+// Make and apply this projection's guess; *rg = ||div u|| after it (r0 when
+// none was kept or tol <= 0).
+int mdx_guess_apply(mdx_ctx_t* ctx, double dg, double r0, bool* guessed, double* rg);
+// learned correction of an applied extrapolated guess and snapshot capture (k_unet.cu)
+int mdx_unet_correct(mdx_ctx_t* ctx, double dg, double* rg);
+int mdx_unet_finish(mdx_ctx_t* ctx, bool converged);
+void mdx_unet_free(mdx_ctx_t* ctx);
 int mdx_k_div_norms_async(mdx_ctx_t* ctx, const double* u, const double* v, const double* w);
 int mdx_k_cfl(mdx_ctx_t* ctx, double* cfl);
 int mdx_k_center_vel(mdx_ctx_t* ctx, double* uc, double* vc, double* wc);

@@ -1,0 +1,128 @@
+"""Learned warm start: the tensor-core network kernels against the CPU FP64
+network (BF16 rounding emulated), training on recorded snapshots, and what
+the trained network gains over the extrapolated guess without it."""
+import math
+
+import numpy as np
+import pytest
+
+import mobydiff_b200 as M
+from oracle import unet_oracle as UO
+from tests.helpers import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _plain_solver(nx, ny, nz, pery):
+    g = M.make_grid(nx, ny, nz, 2 * math.pi, 2.0, math.pi, 1000.0, 1e-3, (0.0, 0.0, 0.0))
+    bc = M.make_bc((True, True, True)) if pery else M.channel_bc()
+    s = M.Solver(g, bc, 0)
+    s.enter_field_data()
+    return s
+
+
+@pytest.mark.parametrize("c1,pery,extra", [(16, False, 0), (32, False, 0), (32, True, 1), (16, True, 0)])
+def test_unet_loss_and_gradients_match_cpu_network(c1, pery, extra):
+    """One forward/backward pass (every conv, pool, up-add, head and
+    weight-gradient kernel) against the CPU network with the same BF16
+    rounding points.  FP32 accumulation on the GPU against FP64 on the CPU
+    flips a few BF16 roundings, and the network carries such flips forward:
+    the CPU network itself moves by ~4e-3 in its output under a 1e-7
+    relative perturbation of its parameters, so the bounds below are a few
+    times that spread; a wrong index or fragment gives O(1) errors."""
+    nx, ny, nz = 32, 16, 16
+    n = nx * ny * nz
+    slope = 0.1
+    s = _plain_solver(nx, ny, nz, pery)
+    with s:
+        s.unet_create(channels=c1, extra_bottleneck=extra, capacity=0, slope=slope)
+        net = UO.Net(c0=16, c1=c1, extra=extra, slope=slope, pery=pery)
+        assert s.unet_param_count() == net.nparam()
+        p = UO.init_params(net, 11).astype(np.float32)
+        s.unet_set_params(p)
+        assert np.array_equal(s.unet_params(), p)
+        rng = np.random.default_rng(5)
+        in4 = rng.standard_normal((4, n)).astype(np.float32)
+        t = rng.standard_normal(n).astype(np.float32)
+        lg, gg, og = s.unet_loss_grad(in4, t)
+        lc, gc, oc = UO.loss_grad(net, p.astype(np.float64), in4, t, (nx, ny, nz), bf16=True)
+        assert abs(lg - lc) <= 5e-3 * lc
+        assert rel_l2(og, oc) <= 1.5e-2
+        offs, ho = net.offsets()
+        for (a, b), (_, c, _) in zip(offs, net.layers()):
+            assert rel_l2(gg[a:b + c], gc[a:b + c]) <= 5e-2, (a, b)
+        assert rel_l2(gg[ho:], gc[ho:]) <= 2e-2
+        assert rel_l2(gg, gc) <= 3e-2
+
+
+def _wavy(seed, re, mode, nx=64, ny=32, nz=32, amp=0.05, tol=1e-8):
+    ly = 2.25
+    y0 = (ly - 2.0) / 2
+    lx = 2 * math.pi
+    g = M.make_grid(nx, ny, nz, lx, ly, math.pi, re, 1e-3, (2.0 / re, 0.0, 0.0))
+    s = M.Solver(g, M.channel_bc(), 0)
+    s.enter_field_data()
+    s.enter_ibm_data(*M.set_ibm_coeff(g, M.ibm_wavy(amp, lx / 2, y0)))
+    s.init_pressure_solver(M.make_solver_opts(M.SOLVER_REDBLACK, sor=1.7, tol=tol, check_every=10, max_iter=200000))
+    s.set_pressure_guess(mode, record=True)
+    s.channel_ic(seed, 0.1, 0.01, y0, amp, lx / 2)
+    return s
+
+
+def test_snapshots_train_and_learned_guess_gain():
+    """Snapshots recorded by one wavy-channel run (Re 2500) train the net;
+    on a held-out run (Re 3000, another seed) the learned correction lowers
+    the divergence the extrapolated guess leaves, the sweeps still run to
+    the same tolerance, and the result agrees with the run without it."""
+    tr = _wavy(101, 2500.0, M.GUESS_EXTRAPOLATED)
+    with tr:
+        tr.unet_create(channels=32, capacity=48, slope=0.1)
+        tr.step(3)
+        tr.unet_record(True)
+        tr.step(16)
+        st = tr.unet_stats()
+        assert st.snapshots == 48 and st.stored == 48 and st.trained == 0
+        l0, l1 = tr.unet_train(300, 1e-3)
+        st = tr.unet_stats()
+        assert st.trained == 1 and st.train_ms > 0.0 and st.out_scale > 0.0
+        print("training loss", l0, "->", l1)
+        assert l1 < 0.2 * l0
+        params, scale = tr.unet_params(), tr.unet_out_scale()
+    se = _wavy(202, 3000.0, M.GUESS_EXTRAPOLATED)
+    sl = _wavy(202, 3000.0, M.GUESS_LEARNED)
+    with se, sl:
+        sl.unet_create(channels=32, capacity=0, slope=0.1)
+        sl.unet_set_params(params)
+        sl.unet_out_scale(scale)
+        ie = se.step(3)
+        assert sl.step(3) == ie            # no two-step history yet: no correction
+        assert sl.unet_stats().corrections == 0
+        ie, il = se.step(4), sl.step(4)
+        st = sl.unet_stats()
+        print("iterations, 4 steps: extrapolated", ie, "learned", il, "divergence gain", st.last_gain,
+              "inference ms", st.infer_ms)
+        assert st.corrections == 12 and st.rejected == 0
+        assert st.last_gain >= 2.0          # ||div|| after extrapolation / after the correction
+        assert il <= 1.1 * ie
+        ls = sl.last_solve_stats()
+        assert ls.status == 0 and ls.guessed == 1
+        l2, _ = sl.divergence_norms()
+        assert l2 <= max(1e-8 * ls.residual0, ls.atol) * 1.0000001
+        for n in ("un", "vn", "wn"):
+            assert rel_l2(sl.get(n), se.get(n)) <= 1e-6, n
+
+
+def test_unet_argument_checks():
+    s = _plain_solver(36, 16, 16, False)   # nx not a multiple of 8
+    with s:
+        with pytest.raises(M.MdxError):
+            s.unet_create()
+        with pytest.raises(M.MdxError):
+            s.unet_train(10)
+    s = _plain_solver(32, 16, 16, False)
+    with s:
+        s.unet_create(capacity=4)
+        with pytest.raises(M.MdxError):   # nothing recorded yet
+            s.unet_train(10)
+        with pytest.raises(M.MdxError):
+            s.unet_set_params(np.zeros(3, dtype=np.float32))
