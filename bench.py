@@ -1,18 +1,27 @@
 #!/usr/bin/env python
 """Benchmark of the mobydiff RK3 time step on B200.
 
-Workload (default ``--config c1``): the wavy-wall channel with immersed
-boundary on a 256x128x128 staggered grid, FP64, Re 3000, dt 1e-3, red-black
-SOR (omega 1.7) to residual 1e-10, walls y = y0 + A sin(2 pi x / lambda)
-(and +2) with A = 0.05, lambda = Lx/2, seeded Poiseuille + noise initial
-condition projected at t = 0.  One step = one full RK3 step (3 predictor
-passes, 3 projections to tolerance, boundary conditions).
+Default workload (``--config c1``): the wavy-wall channel with immersed
+boundary on a 256x128x128 staggered grid (walls y = y0 + A sin(2 pi x /
+lambda) and +2, A = 0.05, lambda = Lx/2), Re 3000, dt 1e-3, red-black SOR
+(omega 1.7), seeded Poiseuille + noise initial condition projected at
+t = 0.  One step = one full RK3 step (3 predictor passes, 3 projections to
+tolerance, boundary conditions).  ``value`` is the learned + mixed step:
+each projection starts from the extrapolated pressure increment plus the
+trained network's correction and runs FP32 sweeps inside FP64 defect
+correction to residual 1e-8.  The same run measures the plain FP64 step
+(zero start, FP64 sweeps) at residual 1e-8 and at 1e-10, the velocity error
+of the learned + mixed state against the plain FP64 one after the same
+steps, and the network's training (snapshots recorded by two held-out runs
+of the geometry at other seeds and amplitudes).  ``--config c1-plain`` is
+the plain FP64 step to 1e-10 alone; ``c0`` and ``c2`` the FFT path.
 
 Prints ONE JSON line on rank 0.  ``value`` is Mcell-steps/s with fields
 resident in HBM; ``e2e`` is the same metric through the C ABI with the
 state copied host->device and device->host (pinned buffers) every step.
 ``--impl reference`` times the CPU restatement of the reference (the
-oracle) on the host cores instead.
+oracle: plain FP64 red-black SOR from phi = 0, the reference's method) on
+the host cores instead, at the tolerance of the chosen config.
 
 Multi-GPU (torchrun): every rank advances its own replica of the workload
 (the step has no exchange between independent channels); value = total
@@ -36,22 +45,30 @@ sys.path.insert(0, ROOT)
 METRIC = "Mcell-steps/s and Poisson iters to 1e-8: learned+mixed vs plain FP64, 1 B200"
 UNIT = "Mcell-steps/s"
 
+C1_GEOM = dict(nx=256, ny=128, nz=128, lx=2 * math.pi, ly=2.25, lz=math.pi, re=3000.0, dt=1e-3, solver="redblack",
+               sor=1.7, check_every=50, ibm="wavy", amp=0.05)
 CONFIGS = {
-    "c1": dict(workload="wavy-wall IBM channel 256x128x128, FP64 red-black SOR omega=1.7 to residual 1e-10",
-               nx=256, ny=128, nz=128, lx=2 * math.pi, ly=2.25, lz=math.pi, re=3000.0, dt=1e-3,
-               solver="redblack", sor=1.7, tol=1e-10, check_every=50, ibm="wavy", amp=0.05),
+    "c1": dict(C1_GEOM, workload="wavy-wall IBM channel 256x128x128 (Re 3000, A 0.05), red-black SOR omega=1.7 to "
+                                 "residual 1e-8: learned warm start + FP32 sweeps in FP64 defect correction",
+               tol=1e-8, method="learned-mixed"),
+    "c1-plain": dict(C1_GEOM, workload="wavy-wall IBM channel 256x128x128, FP64 red-black SOR omega=1.7 to residual "
+                                       "1e-10", tol=1e-10, method="plain"),
     "c0": dict(workload="periodic channel 64^3, FP64 FFT+Thomas", nx=64, ny=64, nz=64, lx=2 * math.pi, ly=2.0,
-               lz=math.pi, re=2000.0, dt=1e-3, solver="fft", ibm="none", amp=0.0),
+               lz=math.pi, re=2000.0, dt=1e-3, solver="fft", ibm="none", amp=0.0, method="plain"),
     "c2": dict(workload="periodic channel 512x256x256, FP64 FFT+Thomas", nx=512, ny=256, nz=256,
-               lx=4 * math.pi, ly=2.0, lz=2 * math.pi, re=5000.0, dt=1e-3, solver="fft", ibm="none", amp=0.0),
+               lx=4 * math.pi, ly=2.0, lz=2 * math.pi, re=5000.0, dt=1e-3, solver="fft", ibm="none", amp=0.0,
+               method="plain"),
 }
 
-# Red-black iterations per RK3 step of the c1 workload in the steps the
-# default run times (warm-up 3, steps 3), measured on B200; the oracle's
-# sweeps are bit-identical, so its iteration count is the same.  Used only
-# to scale the reference arm's bounded CPU sample to a full step.
-C1_ITERS_PER_STEP = 48000.0
+# Red-black iterations per RK3 step of the plain FP64 method (zero start) on
+# the 256x128x128 wavy channel in the steps the default run times (warm-up
+# 3, steps 3), measured on B200, per tolerance; the oracle's sweeps are
+# bit-identical, so its counts are the same.  Used only to scale the
+# reference arm's bounded CPU sample to a full step.
+PLAIN_ITERS_PER_STEP = {1e-10: 48000.0, 1e-8: 27500.0}
 
+# Held-out training runs of the learned warm start: (seed, wall amplitude).
+TRAIN_RUNS = ((20261204, 0.03), (20261205, 0.07))
 SEED = 20261203
 
 
@@ -127,7 +144,7 @@ def _dist():
     return ws, rank, local
 
 
-def _setup(cfg, M, device, profile=False):
+def _setup(cfg, M, device, profile=False, tol=None, precision=None, seed=None):
     g = M.make_grid(cfg["nx"], cfg["ny"], cfg["nz"], cfg["lx"], cfg["ly"], cfg["lz"], cfg["re"], cfg["dt"],
                     (2.0 / cfg["re"], 0.0, 0.0))
     bc = M.channel_bc()
@@ -142,12 +159,13 @@ def _setup(cfg, M, device, profile=False):
         # projection, so that an ncu capture of a few launches ends quickly
         opts = M.make_solver_opts(M.SOLVER_REDBLACK, sor=cfg["sor"], n_iter=20, tol=0.0)
     elif cfg["solver"] == "redblack":
-        opts = M.make_solver_opts(M.SOLVER_REDBLACK, sor=cfg["sor"], tol=cfg["tol"], check_every=cfg["check_every"],
-                                  max_iter=200000)
+        opts = M.make_solver_opts(M.SOLVER_REDBLACK, sor=cfg["sor"], tol=cfg["tol"] if tol is None else tol,
+                                  check_every=cfg["check_every"], max_iter=400000,
+                                  precision=M.PREC_FP64 if precision is None else precision)
     else:
         opts = M.make_solver_opts(M.SOLVER_FFT)
     s.init_pressure_solver(opts)
-    s.channel_ic(SEED, 0.1, 0.01, y0, cfg["amp"], lam)
+    s.channel_ic(SEED if seed is None else seed, 0.1, 0.01, y0, cfg["amp"], lam)
     return s, g
 
 
@@ -208,12 +226,25 @@ def _cpu_step_seconds(cfg, ph, iters_per_step):
     return 3 * (ph["momentum"] + ph["projection"])
 
 
+def _cpu_baseline(cfg, iters_per_step):
+    threads = os.cpu_count() or 1
+    ph, cells = _oracle_sample(cfg, threads)
+    per_step = _cpu_step_seconds(cfg, ph, iters_per_step)
+    if cfg["solver"] == "redblack":
+        sample = (f"3 predictor passes + {ph['sor_iters_sampled']} red-black iterations on the full grid; "
+                  f"step time extrapolated to the {iters_per_step:.0f} iterations per step of the plain FP64 "
+                  f"method at residual {cfg['tol']:g} (the sweeps are bit-identical, so are the counts)")
+    else:
+        sample = "one predictor + one FFT projection on the full grid, x3 substages"
+    return {"value": cells / per_step / 1e6, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
+
+
 def run_reference(args, cfg):
     ws, rank, _ = _dist()
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
-    iters = C1_ITERS_PER_STEP if cfg["solver"] == "redblack" else 0.0
+    iters = PLAIN_ITERS_PER_STEP[cfg["tol"]] if cfg["solver"] == "redblack" else 0.0
     vals = []
     for step in range(args.warmup + args.steps):
         ph, cells = _oracle_sample(cfg, threads, target_s=6.0)
@@ -222,35 +253,114 @@ def run_reference(args, cfg):
     value = float(np.median(vals))
     if cfg["solver"] == "redblack":
         sample = (f"per step: 3 predictor passes + ~{ph['sor_iters_sampled']} red-black iterations of the "
-                  f"{int(iters)} a full step needs, on the full {cfg['nx']}x{cfg['ny']}x{cfg['nz']} grid; "
-                  "step time extrapolated by iteration count")
+                  f"{int(iters)} a full step of the reference's method (FP64 sweeps from phi = 0) needs at "
+                  f"residual {cfg['tol']:g}, on the full {cfg['nx']}x{cfg['ny']}x{cfg['nz']} grid; step time "
+                  "extrapolated by iteration count")
     else:
         sample = "one full RK3 step on the full grid"
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": cfg["workload"], "arm": "CPU restatement of the reference (oracle), OpenMP"},
+            "config": {"workload": cfg["workload"], "arm": "CPU restatement of the reference (oracle), OpenMP, "
+                                                           "plain FP64 method"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
 
 
-def run_ours(args, cfg):
+def _timed_steps(s, stream, steps, pg=None, timing=False):
+    """K steps between events on the solver's stream (barrier + synchronize
+    on both sides); returns (ms over ranks, ms of this rank, iterations,
+    launches, per-class timing).  With `timing` every 8th launch of each
+    kernel class is bracketed by events as well (for the roofline; it costs
+    a few per cent, so the headline runs without it)."""
     import torch
-    import mobydiff_b200 as M
+    s.set_timing(timing)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    launches0 = s.launch_count()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    iters = 0
+    for _ in range(steps):
+        iters += s.step(1)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    launches = s.launch_count() - launches0
+    ms = ev0.elapsed_time(ev1)
+    tim = s.get_timing()
+    s.set_timing(False)
+    ms_all = ms
+    if pg:
+        t = torch.tensor([ms], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms_all = float(t.item())
+    return ms_all, ms, iters, launches, tim
 
+
+def _e2e_steps(s, stream, host, steps, pg=None):
+    """K steps through the C ABI with the state (u, v, w, p) copied from and
+    to pinned host buffers every step."""
+    import torch
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    iters = 0
+    for _ in range(steps):
+        s.update_device(*[h.numpy() for h in host])
+        iters += s.step(1)
+        s.update_host(*[h.numpy() for h in host])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ems = e0.elapsed_time(e1)
+    if pg:
+        t = torch.tensor([ems], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ems = float(t.item())
+    return ems, iters
+
+
+def _roofline(tim, kname, alg_per_cell, cells, ms, traffic_key=None):
+    peak, peak_kind = _peaks()
+    kms, kn = tim[kname]
+    avg_s = (kms / 1e3) / max(kn, 1)
+    alg_bytes = alg_per_cell * cells
+    achieved = alg_bytes / avg_s / 1e9 if kn else None
+    tpc = _traffic_per_cell(traffic_key or kname)
+    return {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind,
+            "traffic": (tpc * cells) if tpc else None, "algorithmic_bytes": alg_bytes,
+            "avg_launch_ms": avg_s * 1e3, "launches": kn, "share_of_step_time": kms / ms if ms > 0 else None}
+
+
+def _init_dist(device):
+    import torch
     ws, rank, local = _dist()
-    device = local
     torch.cuda.set_device(device)
-    pg = None
     if ws > 1:
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900),
                                 device_id=torch.device("cuda", device))
-        pg = dist
+        return dist
+    return None
 
+
+def run_plain(args, cfg):
+    import torch
+    import mobydiff_b200 as M
+
+    ws, rank, local = _dist()
+    device = local
+    pg = _init_dist(device)
     s, g = _setup(cfg, M, device, profile=args.profile)
     cells = cfg["nx"] * cfg["ny"] * cfg["nz"]
     stream = torch.cuda.ExternalStream(s.stream(), device=device)
@@ -266,110 +376,43 @@ def run_ours(args, cfg):
     for _ in range(args.warmup):
         s.step(1)
     torch.cuda.synchronize()
-    # The state at the start of the timed steps, kept on the host so that the
-    # end-to-end leg below replays exactly the same steps (same iteration
-    # counts).  At a step boundary u, v, w, p are the whole state: beta_1 = 0
-    # (step.f90:22), so oldrhs is not read before it is rewritten.
+    # the state at the start of the timed steps, kept on the host so that the
+    # end-to-end leg replays exactly the same steps (same iteration counts);
+    # at a step boundary u, v, w, p are the whole state (beta_1 = 0,
+    # step.f90:22, so oldrhs is not read before it is rewritten)
     host = None
     if not args.no_e2e:
         host = [torch.empty(s.padded, dtype=torch.float64, pin_memory=True) for _ in range(4)]
         s.update_host(*[h.numpy() for h in host])
-
-    # ---- timed region: device-resident state --------------------------------
-    s.set_timing(True)
     clocks = ClockSampler(device)
-    if pg:
-        pg.barrier()
-    torch.cuda.synchronize()
     clocks.start()
-    launches0 = s.launch_count()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    iters = 0
-    for _ in range(args.steps):
-        iters += s.step(1)
-    ev1.record(stream)
-    torch.cuda.synchronize()
+    ms_all, ms, iters, launches, _ = _timed_steps(s, stream, args.steps, pg)
     clk = clocks.stop()
-    if pg:
-        pg.barrier()
-    launches = s.launch_count() - launches0
-    ms = ev0.elapsed_time(ev1)
-    tim = s.get_timing()
-    s.set_timing(False)
-    ms_all = ms
-    if pg:
-        t = torch.tensor([ms], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms_all = float(t.item())
     value = ws * cells * args.steps / (ms_all / 1e3) / 1e6
-
-    # ---- end to end through the C ABI with host buffers -------------------
-    # every step: the state (u, v, w, p) host->device from pinned memory,
-    # one RK3 step, the state device->host
     e2e_line = None
     if not args.no_e2e:
+        ems, e2e_iters = _e2e_steps(s, stream, host, args.steps, pg)
         nbytes = 4 * host[0].numel() * 8
-        torch.cuda.synchronize()
-        if pg:
-            pg.barrier()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        e2e_iters = 0
-        for _ in range(args.steps):
-            s.update_device(*[h.numpy() for h in host])
-            e2e_iters += s.step(1)
-            s.update_host(*[h.numpy() for h in host])
-        e1.record(stream)
-        torch.cuda.synchronize()
-        ems = e0.elapsed_time(e1)
-        if pg:
-            t = torch.tensor([ems], device="cuda")
-            pg.all_reduce(t, op=pg.ReduceOp.MAX)
-            ems = float(t.item())
-        e2e = ws * cells * args.steps / (ems / 1e3) / 1e6
-        e2e_line = {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+        e2e_line = {"value": ws * cells * args.steps / (ems / 1e3) / 1e6, "unit": UNIT,
+                    "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
                     "same_steps_as_value": e2e_iters == iters}
-
-    # ---- roofline of the dominant kernel ------------------------------------
-    peak, peak_kind = _peaks()
-    if cfg["solver"] == "redblack":
-        kname, alg_per_cell = "sor_sweep", 32.0          # 4 doubles per cell per colour sweep
+        # the same steps once more with per-kernel events, for the roofline
+        s.update_device(*[h.numpy() for h in host])
+        _, ms, _, _, tim = _timed_steps(s, stream, args.steps, pg, timing=True)
     else:
-        kname, alg_per_cell = "momentum", 112.0          # 14 doubles per cell
-    kms, kn = tim[kname]
-    avg_s = (kms / 1e3) / max(kn, 1)
-    alg_bytes = alg_per_cell * cells
-    achieved = alg_bytes / avg_s / 1e9 if kn else None
-    tpc = _traffic_per_cell(kname)
-    share = kms / ms if ms > 0 else None
-    roofline = {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind,
-                "traffic": (tpc * cells) if tpc else None, "algorithmic_bytes": alg_bytes,
-                "avg_launch_ms": avg_s * 1e3, "launches": kn, "share_of_step_time": share}
-
+        _, ms, _, _, tim = _timed_steps(s, stream, args.steps, pg, timing=True)
+    if cfg["solver"] == "redblack":
+        roofline = _roofline(tim, "sor_sweep", 32.0, cells, ms)   # 4 doubles per cell per colour sweep
+    else:
+        roofline = _roofline(tim, "momentum", 112.0, cells, ms)   # 14 doubles per cell
     iters_per_substage = iters / (3 * args.steps) if cfg["solver"] == "redblack" else 0
     sor_kernel = None
     if cfg["solver"] == "redblack":
         names = {1: "one launch per colour sweep", 2: "fused red+black pass 32x8", 3: "fused red+black pass 32x16"}
         sor_kernel = names.get(s.last_solve_stats().variant, "?")
-
-    # ---- CPU baseline (rank 0, one GPU only) -------------------------------
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
-        threads = os.cpu_count() or 1
-        ph, _ = _oracle_sample(cfg, threads)
-        per_step = _cpu_step_seconds(cfg, ph, iters / max(args.steps, 1))
-        if cfg["solver"] == "redblack":
-            sample = (f"3 predictor passes + {ph['sor_iters_sampled']} red-black iterations on the full grid; "
-                      f"step time extrapolated to the {iters / max(args.steps, 1):.0f} iterations per step of "
-                      "the timed GPU steps (the sweeps are bit-identical, so are the counts)")
-        else:
-            sample = "one predictor + one FFT projection on the full grid, x3 substages"
-        cpu = {"value": cells / per_step / 1e6, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
-
+        cpu = _cpu_baseline(cfg, iters / max(args.steps, 1))
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_all / args.steps, "higher_is_better": True,
@@ -379,10 +422,158 @@ def run_ours(args, cfg):
                            "re": cfg["re"], "dt": cfg["dt"], "method": "plain FP64",
                            "parallelism": f"replicas x{ws}",
                            "l2": "inputs larger than L2 (state + IBM coefficients > 126 MB)"},
-                "poisson_iters_per_substage": iters_per_substage,
-                "sor_kernel": sor_kernel,
-                "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
-                "e2e": e2e_line, "gpu_launches": launches}
+                "poisson_iters_per_substage": iters_per_substage, "sor_kernel": sor_kernel,
+                "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "e2e": e2e_line,
+                "gpu_launches": launches}
+        print(json.dumps(line), flush=True)
+    s.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
+def run_profile_mixed(args, cfg):
+    """Only the set-up: the t=0 projection of the full-size workload with
+    FP32 sweeps in FP64 defect correction (for an ncu capture of a few
+    FP32 sweep launches)."""
+    import torch
+    import mobydiff_b200 as M
+    _, rank, local = _dist()
+    torch.cuda.set_device(local)
+    s, _ = _setup(cfg, M, local, tol=1e-8, precision=M.PREC_MIXED)
+    torch.cuda.synchronize()
+    if rank == 0:
+        print(json.dumps({"profile_run": cfg["workload"] + "; t=0 projection, FP32 sweeps",
+                          "launches": s.launch_count()}), flush=True)
+    s.close()
+    return 0
+
+
+def run_learned_mixed(args, cfg):
+    import torch
+    import mobydiff_b200 as M
+    from mobydiff_b200 import learned
+
+    ws, rank, local = _dist()
+    device = local
+    pg = _init_dist(device)
+    cells = cfg["nx"] * cfg["ny"] * cfg["nz"]
+    tol = cfg["tol"]
+    W, K = args.warmup, args.steps
+
+    # ---- plain FP64 arm: zero start, FP64 sweeps, same tolerance ------------
+    sp, g = _setup(cfg, M, device, tol=tol, precision=M.PREC_FP64)
+    stream_p = torch.cuda.ExternalStream(sp.stream(), device=device)
+    for _ in range(W):
+        sp.step(1)
+    p_ms_all, p_ms, p_iters, _, _ = _timed_steps(sp, stream_p, K, pg)
+    plain_value = ws * cells * K / (p_ms_all / 1e3) / 1e6
+    plain_state = {n: sp.get(n) for n in ("un", "vn", "wn", "pn")}
+    # one more step with per-kernel events, for the FP64 sweep's roofline
+    _, r_ms, _, _, p_tim = _timed_steps(sp, stream_p, 1, pg, timing=True)
+    roof64 = _roofline(p_tim, "sor_sweep", 32.0, cells, r_ms)
+    plain_c1 = None
+    if not args.quick:   # the plain FP64 step at the C1 tolerance 1e-10
+        sp.init_pressure_solver(M.make_solver_opts(M.SOLVER_REDBLACK, sor=cfg["sor"], tol=1e-10,
+                                                   check_every=cfg["check_every"], max_iter=400000))
+        y0 = (cfg["ly"] - 2.0) / 2.0
+        sp.channel_ic(SEED, 0.1, 0.01, y0, cfg["amp"], cfg["lx"] / 2.0)
+        for _ in range(W):
+            sp.step(1)
+        c_ms_all, _, c_iters, _, _ = _timed_steps(sp, stream_p, K, pg)
+        plain_c1 = {"value": ws * cells * K / (c_ms_all / 1e3) / 1e6, "unit": UNIT, "tol": 1e-10,
+                    "poisson_iters_per_substage": c_iters / (3 * K), "ms_per_step": c_ms_all / K}
+    sp.close()
+
+    # ---- training: snapshots of two held-out runs, Adam on the device --------
+    t0 = time.time()
+    st_, gt = learned.wavy_solver(cfg["nx"], cfg["ny"], cfg["nz"], cfg["re"], cfg["amp"], tol,
+                                  check_every=cfg["check_every"], precision=M.PREC_MIXED, device=device,
+                                  ly=cfg["ly"], lx=cfg["lx"], lz=cfg["lz"], dt=cfg["dt"])
+    net = learned.record_and_train(st_, gt, TRAIN_RUNS, warm_steps=3, record_steps=8, iters=args.train_iters)
+    st_.close()
+    train_wall = time.time() - t0
+
+    # ---- learned + mixed arm ----------------------------------------------------
+    s, g = _setup(cfg, M, device, tol=tol, precision=M.PREC_MIXED)
+    learned.load_into(s, net)
+    s.set_pressure_guess(M.GUESS_LEARNED, record=True)
+    stream = torch.cuda.ExternalStream(s.stream(), device=device)
+    for _ in range(W):
+        s.step(1)
+    # the state at the start of the timed steps: u, v, w, p on the host, the
+    # warm-start history in a device checkpoint, so that the end-to-end leg
+    # and the arm without the network replay exactly the same steps
+    host = [torch.empty(s.padded, dtype=torch.float64, pin_memory=True) for _ in range(4)]
+    s.update_host(*[h.numpy() for h in host])
+    s.warm_checkpoint()
+    u0 = s.unet_stats()
+    clocks = ClockSampler(device)
+    clocks.start()
+    ms_all, ms, iters, launches, _ = _timed_steps(s, stream, K, pg)
+    clk = clocks.stop()
+    u1 = s.unet_stats()
+    value = ws * cells * K / (ms_all / 1e3) / 1e6
+    err = {n: float(np.linalg.norm(s.get(n) - plain_state[n]) / np.linalg.norm(plain_state[n]))
+           for n in ("un", "vn", "wn", "pn")}
+    vnum = sum(float(np.sum((s.get(n) - plain_state[n]) ** 2)) for n in ("un", "vn", "wn"))
+    vden = sum(float(np.sum(plain_state[n] ** 2)) for n in ("un", "vn", "wn"))
+    err["velocity"] = math.sqrt(vnum / vden)
+    ls = s.last_solve_stats()
+    l2, linf = s.divergence_norms()
+
+    # ---- end to end: the same K steps through the C ABI with host buffers ----
+    e2e_line = None
+    if not args.no_e2e:
+        s.warm_checkpoint(restore=True)
+        ems, e2e_iters = _e2e_steps(s, stream, host, K, pg)
+        nbytes = 4 * host[0].numel() * 8
+        e2e_line = {"value": ws * cells * K / (ems / 1e3) / 1e6, "unit": UNIT, "h2d_bytes_per_step": nbytes,
+                    "d2h_bytes_per_step": nbytes, "same_steps_as_value": e2e_iters == iters}
+
+    # ---- the same steps with per-kernel events, for the roofline ----------------
+    s.warm_checkpoint(restore=True)
+    s.update_device(*[h.numpy() for h in host])
+    _, r_ms, _, _, tim = _timed_steps(s, stream, K, pg, timing=True)
+    roofline = _roofline(tim, "sor_sweep", 16.0, cells, r_ms, traffic_key="sor_sweep32")   # 4 floats per cell per colour sweep
+
+    # ---- the same steps without the network: extrapolated increment only ----
+    s.warm_checkpoint(restore=True)
+    s.update_device(*[h.numpy() for h in host])
+    s.set_pressure_guess(M.GUESS_EXTRAPOLATED, record=True)
+    x_ms_all, _, x_iters, _, _ = _timed_steps(s, stream, K, pg)
+    no_net = {"value": ws * cells * K / (x_ms_all / 1e3) / 1e6, "unit": UNIT, "ms_per_step": x_ms_all / K,
+              "poisson_iters_per_substage": x_iters / (3 * K)}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        cpu = _cpu_baseline(cfg, p_iters / max(K, 1))
+    if rank == 0:
+        corr = u1.corrections - u0.corrections
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": W,
+                "ms_per_step": ms_all / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64+f32 (FP32 sweeps in FP64 defect correction; BF16/FP32 network)",
+                "data": "synthetic: seeded Poiseuille+noise IC (SplitMix64), projected at t=0; network trained on "
+                        "snapshots of two runs at other seeds and wall amplitudes",
+                "config": {"workload": cfg["workload"], "grid": [cfg["nx"], cfg["ny"], cfg["nz"]], "re": cfg["re"],
+                           "dt": cfg["dt"], "tol": tol, "method": "learned warm start + mixed precision",
+                           "parallelism": f"replicas x{ws}",
+                           "l2": "inputs larger than L2 (state + IBM coefficients > 126 MB)"},
+                "poisson_iters_per_substage": iters / (3 * K),
+                "plain_fp64": {"value": plain_value, "unit": UNIT, "tol": tol, "ms_per_step": p_ms_all / K,
+                               "poisson_iters_per_substage": p_iters / (3 * K), "roofline": roof64},
+                "plain_fp64_c1_tol": plain_c1,
+                "extrapolated_mixed_no_network": no_net,
+                "speedup_vs_plain_fp64": value / plain_value,
+                "error_vs_plain_fp64": {"rel_l2": err, "residual": ls.residual, "div_l2": l2, "div_linf": linf},
+                "learned": {"corrections": corr, "rejected": u1.rejected - u0.rejected,
+                            "divergence_gain_last": u1.last_gain, "inference_ms": u1.infer_ms,
+                            "snapshots": net.snapshots, "loss_first": net.loss_first, "loss_last": net.loss_last,
+                            "record_s": net.record_seconds, "train_ms": net.train_ms, "setup_wall_s": train_wall,
+                            "train_runs": [list(r) for r in TRAIN_RUNS]},
+                "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "e2e": e2e_line,
+                "gpu_launches": launches}
         print(json.dumps(line), flush=True)
     s.close()
     if pg:
@@ -402,11 +593,19 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     ap.add_argument("--profile", action="store_true",
                     help="profiling run for ncu: full-size state, fixed 20 red-black iterations per projection")
+    ap.add_argument("--profile-mixed", action="store_true",
+                    help="profiling run for ncu: the full-size t=0 projection with FP32 sweeps to residual 1e-8")
+    ap.add_argument("--quick", action="store_true", help="skip the plain FP64 leg at residual 1e-10")
+    ap.add_argument("--train-iters", type=int, default=600, help="Adam steps of the learned warm start")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
     if args.impl == "reference":
         return run_reference(args, cfg)
-    return run_ours(args, cfg)
+    if args.profile_mixed:
+        return run_profile_mixed(args, cfg)
+    if cfg["method"] == "learned-mixed" and not args.profile:
+        return run_learned_mixed(args, cfg)
+    return run_plain(args, cfg)
 
 
 if __name__ == "__main__":

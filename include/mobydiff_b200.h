@@ -275,6 +275,12 @@ int mdx_set_pressure_guess(mdx_ctx_t* ctx, int mode, int record);
  * cells, x fastest (synchronises); MDX_ERR_STATE if none was recorded. */
 int mdx_get_increment(mdx_ctx_t* ctx, int substage, double* host);
 
+/* Save (restore = 0) or restore (restore != 0) the warm-start history --
+ * the recorded increments and the projection count -- in a device-side copy,
+ * so that steps can be replayed from a saved u, v, w, p with the same
+ * guesses.  No counterpart in the reference. */
+int mdx_warm_checkpoint(mdx_ctx_t* ctx, int restore);
+
 /* ---- learned warm start (no counterpart in the reference) ----------------
  * A 4-level 3-D U-Net on the cells of the grid (channels-last BF16
  * activations and weights, FP32 accumulation on the tensor cores).  With

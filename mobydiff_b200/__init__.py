@@ -173,6 +173,7 @@ def lib():
         "mdx_last_solve_stats": (i, [vp, P(SolveStatsT)]),
         "mdx_set_pressure_guess": (i, [vp, i, i]),
         "mdx_get_increment": (i, [vp, i, vp]),
+        "mdx_warm_checkpoint": (i, [vp, i]),
         "mdx_default_unet_opts": (None, [P(UnetOptsT)]),
         "mdx_unet_create": (i, [vp, P(UnetOptsT)]),
         "mdx_unet_destroy": (i, [vp]),
@@ -447,6 +448,10 @@ class Solver:
         (the same substage's increment of the previous step) or GUESS_LEARNED
         (U-Net prediction); `record` keeps the increments of every projection."""
         self._c(lib().mdx_set_pressure_guess(self.h, int(mode), 1 if record else 0))
+
+    def warm_checkpoint(self, restore: bool = False) -> None:
+        """Save (or restore) the warm-start history on the device."""
+        self._c(lib().mdx_warm_checkpoint(self.h, 1 if restore else 0))
 
     # ---- learned warm start ----------------------------------------------
     def unet_create(self, channels: int = 32, extra_bottleneck: int = 0, capacity: int = 64, slope: float = 0.1,

@@ -119,6 +119,9 @@ void mdx_warm_free(mdx_ctx_t* ctx) {
     ctx->p_before = nullptr;
     cudaFree(ctx->guess);
     ctx->guess = nullptr;
+    cudaFree(ctx->ckpt);
+    ctx->ckpt = nullptr;
+    ctx->ckpt_valid = -1;
     ctx->hist_valid = 0;
 }
 
@@ -218,6 +221,37 @@ extern "C" int mdx_set_pressure_guess(mdx_ctx_t* ctx, int mode, int record) {
     if (mode < MDX_GUESS_ZERO || mode > MDX_GUESS_EXTRAPOLATED) return mdx_fail(ctx, MDX_ERR_ARG, "unknown guess mode %d", mode);
     ctx->guess_mode = mode;
     ctx->record_increments = record != 0;
+    return MDX_OK;
+}
+
+extern "C" int mdx_warm_checkpoint(mdx_ctx_t* ctx, int restore) {
+    if (!ctx) return mdx_fail(nullptr, MDX_ERR_ARG, "null context");
+    if (!ctx->fields) return mdx_fail(ctx, MDX_ERR_STATE, "field data not entered");
+    MDX_CUDA(ctx, cudaSetDevice(ctx->device));
+    const size_t n = (size_t)ctx->d.nint;
+    if (!restore) {
+        if (!ctx->dp_hist[0]) MDX_TRY(mdx_warm_alloc(ctx));
+        if (!ctx->ckpt) MDX_CUDA(ctx, cudaMalloc(&ctx->ckpt, sizeof(double) * 6 * n));
+        for (int t = 0; t < 3; ++t) {
+            MDX_CUDA(ctx, cudaMemcpyAsync(ctx->ckpt + t * n, ctx->dp_hist[t], sizeof(double) * n,
+                                          cudaMemcpyDeviceToDevice, ctx->stream));
+            MDX_CUDA(ctx, cudaMemcpyAsync(ctx->ckpt + (3 + t) * n, ctx->dp_hist2[t], sizeof(double) * n,
+                                          cudaMemcpyDeviceToDevice, ctx->stream));
+        }
+        ctx->ckpt_valid = ctx->hist_valid;
+        ctx->ckpt_count = ctx->proj_count;
+        return MDX_OK;
+    }
+    if (ctx->ckpt_valid < 0 || !ctx->ckpt || !ctx->dp_hist[0])
+        return mdx_fail(ctx, MDX_ERR_STATE, "no warm-start checkpoint saved");
+    for (int t = 0; t < 3; ++t) {
+        MDX_CUDA(ctx, cudaMemcpyAsync(ctx->dp_hist[t], ctx->ckpt + t * n, sizeof(double) * n, cudaMemcpyDeviceToDevice,
+                                      ctx->stream));
+        MDX_CUDA(ctx, cudaMemcpyAsync(ctx->dp_hist2[t], ctx->ckpt + (3 + t) * n, sizeof(double) * n,
+                                      cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+    ctx->hist_valid = ctx->ckpt_valid;
+    ctx->proj_count = ctx->ckpt_count;
     return MDX_OK;
 }
 

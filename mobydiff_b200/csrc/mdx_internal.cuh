@@ -88,6 +88,9 @@ struct mdx_ctx {
     double* p_before = nullptr;              // padded p at the start of the projection
     double* guess = nullptr;                 // increment guess of the current projection
     int hist_valid = 0;                      // bit s: dp_hist[s] holds an increment; bit 3+s: dp_hist2[s]
+    double* ckpt = nullptr;                  // saved dp_hist, dp_hist2 (mdx_warm_checkpoint)
+    int ckpt_valid = -1;                     // hist_valid at the save, -1: none
+    long long ckpt_count = 0;
     long long proj_count = 0;                // projections since the t=0 projection
     void* unet = nullptr;                    // learned warm start (k_unet.cu)
     int sor_tuned = 0;                       // red-black kernel variant chosen by the autotuner (0: not yet)

@@ -98,3 +98,23 @@ def test_guess_matches_oracle_trajectory():
         sp.step(5)
         for n in ("un", "vn", "wn"):
             assert rel_l2(sp.get(n), getattr(f, n)) <= 1e-6, n
+
+
+def test_checkpoint_replays_the_same_steps():
+    """u, v, w, p from the host plus the device checkpoint of the increment
+    history replay the same guessed steps bit for bit."""
+    g, bc, f = _wavy_case()
+    s = _solver(g, bc, f, 1e-8)
+    with s:
+        s.set_pressure_guess(M.GUESS_EXTRAPOLATED, record=True)
+        s.step(4)
+        state = [s.get(n).copy() for n in ("un", "vn", "wn", "pn")]
+        s.warm_checkpoint()
+        ia = s.step(2)
+        a = [s.get(n).copy() for n in ("un", "vn", "wn", "pn")]
+        s.warm_checkpoint(restore=True)
+        s.update_device(*state)
+        ib = s.step(2)
+        assert ia == ib
+        for x, n in zip(a, ("un", "vn", "wn", "pn")):
+            assert np.array_equal(x, s.get(n)), n
