@@ -281,6 +281,60 @@ int mdx_get_increment(mdx_ctx_t* ctx, int substage, double* host);
  * guesses.  No counterpart in the reference. */
 int mdx_warm_checkpoint(mdx_ctx_t* ctx, int restore);
 
+/* ---- batched ensemble (no counterpart in the reference) -----------------
+ * Many independent wavy-wall channels of different sizes advanced together:
+ * one persistent cooperative launch per RK3 substage for all members
+ * (momentum, red-black projection to each member's own tolerance, boundary
+ * conditions), the three launches of a step captured in a CUDA graph.
+ * Every member: periodic x and z, no-slip walls in y with Neumann
+ * pressure, walls y0 + A sin(2 pi x/(Lx/2)) and y0 + 2 + ... imposed by the
+ * IBM of mdx_set_ibm_coeff (geometry 1) when A > 0 (y0 = (Ly-2)/2), forcing
+ * 2/Re in x, FP64 red-black sweeps.  With a fixed iteration count (tol <= 0)
+ * each member's fields are bit-for-bit the single-context path's. */
+typedef struct {
+    int nx, ny, nz;        /* even nx and nz                                   */
+    double lx, ly, lz;     /* ly > 2                                           */
+    double re, dt;
+    double amp;            /* wall amplitude A (0: no IBM)                     */
+    uint64_t seed;         /* initial condition (mdx_channel_ic's)             */
+    int reserved_i[4];
+    double reserved_d[4];
+} mdx_member_t;
+
+typedef struct mdx_ensemble mdx_ensemble_t;
+
+void mdx_default_member(mdx_member_t* m);
+/* opts: MDX_SOLVER_REDBLACK, MDX_PREC_FP64; n_iter / tol / max_iter /
+ * check_every / atol / sor as for a context. */
+int mdx_ensemble_create(int device, int n, const mdx_member_t* members, const mdx_solver_opts_t* opts,
+                        mdx_ensemble_t** out);
+int mdx_ensemble_destroy(mdx_ensemble_t* ens);
+const char* mdx_ensemble_last_error(const mdx_ensemble_t* ens);
+/* MDX_GUESS_ZERO, MDX_GUESS_PREVIOUS or MDX_GUESS_EXTRAPOLATED. */
+int mdx_ensemble_set_guess(mdx_ensemble_t* ens, int mode);
+/* Seeded channel initial condition of every member, projected at t = 0
+ * (dt_gamma = 1), then p = 0 (mdx_channel_ic with y0 = (Ly-2)/2, the
+ * member's amplitude and lambda = Lx/2, noise amplitudes 0.1 and 0.01). */
+int mdx_ensemble_ic(mdx_ensemble_t* ens);
+/* nsteps RK3 steps of every member; *total_iters = red-black iterations of
+ * all members (synchronises).  MDX_NOT_CONVERGED / MDX_ERR_NONFINITE when a
+ * member's projection ended so. */
+int mdx_ensemble_step(mdx_ensemble_t* ens, int nsteps, long long* total_iters);
+int mdx_ensemble_member_stats(mdx_ensemble_t* ens, int member, mdx_solve_stats_t* last, long long* iters_total);
+/* Padded field MDX_UN, MDX_VN, MDX_WN or MDX_PN of a member. */
+int mdx_ensemble_get(mdx_ensemble_t* ens, int member, int field, double* host);
+int mdx_ensemble_set(mdx_ensemble_t* ens, int member, int field, const double* host);
+/* Threads per block (multiple of 32, <= 512) and blocks per SM (0: as many
+ * as fit) of the persistent grid. */
+int mdx_ensemble_config(mdx_ensemble_t* ens, int threads, int blocks_per_sm);
+/* Time one step of each candidate grid from the same saved state and keep
+ * the fastest; the choice is cached in the JSON file cache_path (may be
+ * NULL) under a key of the member sizes, the mode and the device name. */
+int mdx_ensemble_tune(mdx_ensemble_t* ens, const char* cache_path, int* threads, int* blocks_per_sm, double* ms);
+int mdx_ensemble_use_graph(mdx_ensemble_t* ens, int on);
+int mdx_ensemble_info(mdx_ensemble_t* ens, int* threads, int* grid, int* graph, double* last_step_ms,
+                      long long* launches);
+
 /* ---- learned warm start (no counterpart in the reference) ----------------
  * A 4-level 3-D U-Net on the cells of the grid (channels-last BF16
  * activations and weights, FP32 accumulation on the tensor cores).  With

@@ -103,6 +103,12 @@ class UnetStatsT(C.Structure):
                 ("infer_ms", C.c_double), ("train_ms", C.c_double), ("reserved_d", C.c_double * 6)]
 
 
+class MemberT(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("lx", C.c_double), ("ly", C.c_double),
+                ("lz", C.c_double), ("re", C.c_double), ("dt", C.c_double), ("amp", C.c_double), ("seed", C.c_uint64),
+                ("reserved_i", C.c_int * 4), ("reserved_d", C.c_double * 4)]
+
+
 class TimingT(C.Structure):
     _fields_ = [("ms", C.c_double * 9), ("launches", C.c_longlong * 9)]
 
@@ -174,6 +180,20 @@ def lib():
         "mdx_set_pressure_guess": (i, [vp, i, i]),
         "mdx_get_increment": (i, [vp, i, vp]),
         "mdx_warm_checkpoint": (i, [vp, i]),
+        "mdx_default_member": (None, [P(MemberT)]),
+        "mdx_ensemble_create": (i, [i, i, P(MemberT), P(SolverOptsT), P(vp)]),
+        "mdx_ensemble_destroy": (i, [vp]),
+        "mdx_ensemble_last_error": (C.c_char_p, [vp]),
+        "mdx_ensemble_set_guess": (i, [vp, i]),
+        "mdx_ensemble_ic": (i, [vp]),
+        "mdx_ensemble_step": (i, [vp, i, P(C.c_longlong)]),
+        "mdx_ensemble_member_stats": (i, [vp, i, P(SolveStatsT), P(C.c_longlong)]),
+        "mdx_ensemble_get": (i, [vp, i, i, vp]),
+        "mdx_ensemble_set": (i, [vp, i, i, vp]),
+        "mdx_ensemble_config": (i, [vp, i, i]),
+        "mdx_ensemble_tune": (i, [vp, C.c_char_p, P(i), P(i), P(d)]),
+        "mdx_ensemble_use_graph": (i, [vp, i]),
+        "mdx_ensemble_info": (i, [vp, P(i), P(i), P(i), P(d), P(C.c_longlong)]),
         "mdx_default_unet_opts": (None, [P(UnetOptsT)]),
         "mdx_unet_create": (i, [vp, P(UnetOptsT)]),
         "mdx_unet_destroy": (i, [vp]),
@@ -529,3 +549,92 @@ class Solver:
 
     def set_stream(self, stream_ptr: int | None):
         self._c(lib().mdx_set_stream(self.h, C.c_void_p(stream_ptr) if stream_ptr else None))
+
+
+def make_member(nx, ny, nz, lx=2 * np.pi, ly=2.25, lz=np.pi, re=3000.0, dt=1e-3, amp=0.05, seed=20261203) -> MemberT:
+    m = MemberT()
+    lib().mdx_default_member(C.byref(m))
+    m.nx, m.ny, m.nz = int(nx), int(ny), int(nz)
+    m.lx, m.ly, m.lz, m.re, m.dt, m.amp, m.seed = float(lx), float(ly), float(lz), float(re), float(dt), float(amp), int(seed)
+    return m
+
+
+class Ensemble:
+    """Independent wavy-wall channels of different sizes advanced together:
+    one persistent launch per RK3 substage for all members (C ABI
+    mdx_ensemble_*)."""
+
+    def __init__(self, members, opts: SolverOptsT, device: int = 0):
+        arr = (MemberT * len(members))(*members)
+        h = C.c_void_p()
+        rc = lib().mdx_ensemble_create(int(device), len(members), arr, C.byref(opts), C.byref(h))
+        if rc != MDX_OK:
+            raise MdxError(rc, lib().mdx_last_error(None).decode(errors="replace"))
+        self.h = h
+        self.members = list(members)
+
+    def _c(self, rc):
+        if rc != MDX_OK:
+            raise MdxError(rc, lib().mdx_ensemble_last_error(self.h).decode(errors="replace"))
+
+    def close(self):
+        if self.h:
+            lib().mdx_ensemble_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_guess(self, mode: int) -> None:
+        self._c(lib().mdx_ensemble_set_guess(self.h, int(mode)))
+
+    def ic(self) -> None:
+        self._c(lib().mdx_ensemble_ic(self.h))
+
+    def step(self, nsteps: int) -> int:
+        it = C.c_longlong(0)
+        self._c(lib().mdx_ensemble_step(self.h, int(nsteps), C.byref(it)))
+        return it.value
+
+    def member_stats(self, m: int):
+        st = SolveStatsT()
+        tot = C.c_longlong(0)
+        self._c(lib().mdx_ensemble_member_stats(self.h, int(m), C.byref(st), C.byref(tot)))
+        return st, tot.value
+
+    def get(self, m: int, name: str) -> np.ndarray:
+        q = self.members[m]
+        a = np.empty((q.nz + 2, q.ny + 2, q.nx + 2))
+        self._c(lib().mdx_ensemble_get(self.h, int(m), FIELD_ID[name], a.ctypes.data_as(C.c_void_p)))
+        return a
+
+    def set(self, m: int, name: str, a) -> None:
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        self._c(lib().mdx_ensemble_set(self.h, int(m), FIELD_ID[name], a.ctypes.data_as(C.c_void_p)))
+
+    def config(self, threads: int, blocks_per_sm: int = 0) -> None:
+        self._c(lib().mdx_ensemble_config(self.h, int(threads), int(blocks_per_sm)))
+
+    def tune(self, cache_path=None):
+        t, b, ms = C.c_int(0), C.c_int(0), C.c_double(0.0)
+        path = cache_path.encode() if cache_path else None
+        self._c(lib().mdx_ensemble_tune(self.h, path, C.byref(t), C.byref(b), C.byref(ms)))
+        return t.value, b.value, ms.value
+
+    def use_graph(self, on: bool) -> None:
+        self._c(lib().mdx_ensemble_use_graph(self.h, 1 if on else 0))
+
+    def info(self) -> dict:
+        t, g, gr, ms, ln = C.c_int(0), C.c_int(0), C.c_int(0), C.c_double(0.0), C.c_longlong(0)
+        self._c(lib().mdx_ensemble_info(self.h, C.byref(t), C.byref(g), C.byref(gr), C.byref(ms), C.byref(ln)))
+        return {"threads": t.value, "grid": g.value, "graph": bool(gr.value), "last_step_ms": ms.value,
+                "launches": ln.value}

@@ -33,6 +33,7 @@ CUDA_SOURCES = {
     "k_sor_mixed.cu": [],   # FP32 sweeps inside FP64 defect correction: FMA allowed
     "k_warm.cu": ["-fmad=false"],
     "k_unet.cu": [],        # BF16 network with FP32 accumulation: FMA allowed
+    "k_ensemble.cu": ["-fmad=false"],
 }
 CXX_SOURCES = ["host_config.cpp"]
 

@@ -16,16 +16,10 @@
 // formula gives the same bits.  Successive sweeps walk the z planes in
 // opposite directions, so each starts on the planes the previous one left
 // in the 126 MB L2.
-#include "mdx_internal.cuh"
+#include "mdx_cell.cuh"
 
 #include <algorithm>
 #include <cmath>
-
-struct mdx_sor_params {
-    double dx, dy, dz, idx, idy, idz, idx2, idy2, idz2, idt, sor, dt_gamma;
-};
-
-enum { MU_ONE = 0, MU_PLANE = 1, MU_FULL = 2 };
 
 // mu = 1/(1 + dt_gamma*coef) over n elements of each component.
 __global__ void k_mu_tables(long long n, long long stride_in, double dg, const double* __restrict__ cu,
@@ -38,105 +32,6 @@ __global__ void k_mu_tables(long long n, long long stride_in, double dg, const d
     (void)stride_in;
 }
 
-// -omega/denom of one cell, pressure_redblack.f90:124-126,186.
-__device__ __forceinline__ double sor_factor(double mu_u_i, double mu_u_ip, double mu_v_j, double mu_v_jp,
-                                             double mu_w_k, double mu_w_kp, const mdx_sor_params& p) {
-    const double denom = (mu_u_i + mu_u_ip) * p.idx2 + (mu_w_k + mu_w_kp) * p.idz2 + (mu_v_j + mu_v_jp) * p.idy2;
-    return -p.sor / denom;
-}
-
-// The update of one cell, pressure_redblack.f90:128-241, on register copies
-// of its six faces and p, given its factor -omega/denom.  In the reference's
-// one-sided boundary formulas un(nx,j,k), vn(i,j,k) and wn(i,j,nz) are the
-// cell's own u_i, v_j, w_k (those branches run only for i = nx, j = ny,
-// k = nz).  PX/PY/PZ: 1 periodic, 0 not, -1 read from bc at run time.
-template <int PX = -1, int PY = -1, int PZ = -1>
-__device__ __forceinline__ void sor_cell_fac(double& u_i, double& u_ip, double& v_j, double& v_jp, double& w_k,
-                                             double& w_kp, double& pc, double mu_u_i, double mu_u_ip, double mu_v_j,
-                                             double mu_v_jp, double mu_w_k, double mu_w_kp, double fac,
-                                             const mdx_sor_params& p, const mdx_bc_dev& bc, int i, int j, int k,
-                                             int nx, int ny, int nz) {
-    const int* T = bc.type;
-    const double* V = bc.value;
-    const bool perx = PX >= 0 ? PX != 0 : bc.per[0] != 0;
-    const bool pery = PY >= 0 ? PY != 0 : bc.per[1] != 0;
-    const bool perz = PZ >= 0 ? PZ != 0 : bc.per[2] != 0;
-    if (!perx) {  // :128-144
-        if (i < 2) {
-            if (T[bci(1, 0, 1)] == 0) u_i = V[bci(1, 0, 1)];
-            else u_i = u_ip - V[bci(1, 0, 1)] * p.dx;
-        }
-        if (i >= nx) {
-            if (T[bci(1, 1, 1)] == 0) u_ip = V[bci(1, 1, 1)];
-            else u_ip = u_i + V[bci(1, 1, 1)] * p.dx;
-        }
-    }
-    if (!pery) {  // :146-162
-        if (j < 2) {
-            if (T[bci(2, 0, 2)] == 0) v_j = V[bci(2, 0, 2)];
-            else v_j = v_jp - V[bci(2, 0, 2)] * p.dy;
-        }
-        if (j >= ny) {
-            if (T[bci(2, 1, 2)] == 0) v_jp = V[bci(2, 1, 2)];
-            else v_jp = v_j + V[bci(2, 1, 2)] * p.dy;
-        }
-    }
-    if (!perz) {  // :164-180
-        if (k < 2) {
-            if (T[bci(3, 0, 3)] == 0) w_k = V[bci(3, 0, 3)];
-            else w_k = w_kp - V[bci(3, 0, 3)] * p.dz;
-        }
-        if (k >= nz) {
-            if (T[bci(3, 1, 3)] == 0) w_kp = V[bci(3, 1, 3)];
-            else w_kp = w_k + V[bci(3, 1, 3)] * p.dz;
-        }
-    }
-    // :183-188
-    const double phi = ((u_ip - u_i) * p.idx + (v_jp - v_j) * p.idy + (w_kp - w_k) * p.idz) * fac;
-    pc = pc + phi * p.idt;
-    // :190-241
-    u_i = u_i - phi * p.idx * mu_u_i;
-    if (!perx && i == 1) {
-        if (T[bci(1, 0, 0)] == 0) u_i = u_i + V[bci(1, 0, 0)] * p.idx * mu_u_i;
-        else u_i = u_i + (phi * p.idx - V[bci(1, 0, 0)]) * mu_u_i;
-    }
-    u_ip = u_ip + phi * p.idx * mu_u_ip;
-    if (!perx && i == nx) {
-        if (T[bci(1, 1, 0)] == 0) u_ip = u_ip - V[bci(1, 1, 0)] * p.idx * mu_u_ip;
-        else u_ip = u_ip + (V[bci(1, 1, 0)] - phi * p.idx) * mu_u_ip;
-    }
-    v_j = v_j - phi * p.idy * mu_v_j;
-    if (!pery && j == 1) {
-        if (T[bci(2, 0, 0)] == 0) v_j = v_j + V[bci(2, 0, 0)] * p.idy * mu_v_j;
-        else v_j = v_j + (phi * p.idy - V[bci(2, 0, 0)]) * mu_v_j;
-    }
-    v_jp = v_jp + phi * p.idy * mu_v_jp;
-    if (!pery && j == ny) {
-        if (T[bci(2, 1, 0)] == 0) v_jp = v_jp - V[bci(2, 1, 0)] * p.idy * mu_v_jp;
-        else v_jp = v_jp + (V[bci(2, 1, 0)] - phi * p.idy) * mu_v_jp;
-    }
-    w_k = w_k - phi * p.idz * mu_w_k;
-    if (!perz && k == 1) {
-        if (T[bci(3, 0, 0)] == 0) w_k = w_k + V[bci(3, 0, 0)] * p.idz * mu_w_k;
-        else w_k = w_k + (phi * p.idz - V[bci(3, 0, 0)]) * mu_w_k;
-    }
-    w_kp = w_kp + phi * p.idz * mu_w_kp;
-    if (!perz && k == nz) {
-        // :237 -- the Dirichlet branch of the reference has no mu factor
-        if (T[bci(3, 1, 0)] == 0) w_kp = w_kp - V[bci(3, 1, 0)] * p.idz;
-        else w_kp = w_kp + (V[bci(3, 1, 0)] - phi * p.idz) * mu_w_kp;
-    }
-}
-
-// The whole update of one cell, pressure_redblack.f90:117-241.
-__device__ __forceinline__ void sor_cell(double& u_i, double& u_ip, double& v_j, double& v_jp, double& w_k,
-                                         double& w_kp, double& pc, double mu_u_i, double mu_u_ip, double mu_v_j,
-                                         double mu_v_jp, double mu_w_k, double mu_w_kp, const mdx_sor_params& p,
-                                         const mdx_bc_dev& bc, int i, int j, int k, int nx, int ny, int nz) {
-    const double fac = sor_factor(mu_u_i, mu_u_ip, mu_v_j, mu_v_jp, mu_w_k, mu_w_kp, p);
-    sor_cell_fac(u_i, u_ip, v_j, v_jp, w_k, w_kp, pc, mu_u_i, mu_u_ip, mu_v_j, mu_v_jp, mu_w_k, mu_w_kp, fac, p, bc,
-                 i, j, k, nx, ny, nz);
-}
 
 template <int MU>
 __global__ void __launch_bounds__(256)

@@ -6,7 +6,7 @@
 // boundary conditions are bit-for-bit the reference arithmetic (x86-64
 // gfortran -O2 has no FMA contraction).  Skipping the IBM factor when all
 // coefficients are zero is exact: 1/(1+dt_gamma*0) == 1.
-#include "mdx_internal.cuh"
+#include "mdx_cell.cuh"
 
 // ---------------------------------------------------------------------------
 // Predictor, src/modules/step.f90:76-204.  One thread per cell, x fastest so
@@ -24,85 +24,8 @@ k_momentum(mdx_dims d, mdx_step_params p, double dt_alpha, double dt_beta, doubl
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     const int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
     if (i > d.nx || j > d.ny || k > d.nz) return;
-    const long long SX = 1, SY = d.nxp, SZ = (long long)d.nxp * d.nyp;
-    const long long c = pidx(d, i, j, k);
-    const long long q = qidx(d, i, j, k);
-    const double idx = p.idx, idy = p.idy, idz = p.idz, idx2 = p.idx2, idy2 = p.idy2, idz2 = p.idz2, ire = p.ire;
-
-    const double u_c = __ldg(un + c), v_c = __ldg(vn + c), w_c = __ldg(wn + c), p_c = __ldg(pn + c);
-
-    if (i >= p.nx0) {  // step.f90:106-136
-        const double u_ip = __ldg(un + c + SX), u_im = __ldg(un + c - SX);
-        const double u_jp = __ldg(un + c + SY), u_jm = __ldg(un + c - SY);
-        const double u_kp = __ldg(un + c + SZ), u_km = __ldg(un + c - SZ);
-        double s;
-        s = u_ip + u_c;
-        const double uu_p = 0.25 * (s * s);
-        s = u_c + u_im;
-        const double uu_m = 0.25 * (s * s);
-        const double uv_p = 0.25 * (u_jp + u_c) * (__ldg(vn + c + SY) + __ldg(vn + c - SX + SY));
-        const double uv_m = 0.25 * (u_c + u_jm) * (v_c + __ldg(vn + c - SX));
-        const double uw_p = 0.25 * (u_c + u_kp) * (__ldg(wn + c + SZ) + __ldg(wn + c - SX + SZ));
-        const double uw_m = 0.25 * (u_c + u_km) * (w_c + __ldg(wn + c - SX));
-        const double diff_ux = (u_im - 2.0 * u_c + u_ip) * idx2;
-        const double diff_uy = (u_jm - 2.0 * u_c + u_jp) * idy2;
-        const double diff_uz = (u_km - 2.0 * u_c + u_kp) * idz2;
-        const double dpx = (p_c - __ldg(pn + c - SX)) * idx;
-        const double rhsu = -((uu_p - uu_m) * idx) - (uv_p - uv_m) * idy - (uw_p - uw_m) * idz + p.fx +
-                            ire * (diff_ux + diff_uy + diff_uz);
-        double val = u_c + dt_alpha * rhsu + dt_beta * ou[q] - dt_gamma * dpx;
-        if (IBM) val = val * (1.0 / (1.0 + dt_gamma * __ldg(cu + c)));
-        us[c] = val;
-        ou[q] = rhsu;
-    }
-    if (j >= p.ny0) {  // step.f90:138-168
-        const double v_ip = __ldg(vn + c + SX), v_im = __ldg(vn + c - SX);
-        const double v_jp = __ldg(vn + c + SY), v_jm = __ldg(vn + c - SY);
-        const double v_kp = __ldg(vn + c + SZ), v_km = __ldg(vn + c - SZ);
-        double s;
-        const double vu_p = 0.25 * (v_c + v_ip) * (__ldg(un + c + SX) + __ldg(un + c + SX - SY));
-        const double vu_m = 0.25 * (v_c + v_im) * (u_c + __ldg(un + c - SY));
-        s = v_c + v_jp;
-        const double vv_p = 0.25 * (s * s);
-        s = v_c + v_jm;
-        const double vv_m = 0.25 * (s * s);
-        const double vw_p = 0.25 * (v_kp + v_c) * (__ldg(wn + c + SZ) + __ldg(wn + c - SY + SZ));
-        const double vw_m = 0.25 * (v_km + v_c) * (w_c + __ldg(wn + c - SY));
-        const double diff_vx = (v_im - 2.0 * v_c + v_ip) * idx2;
-        const double diff_vy = (v_jm - 2.0 * v_c + v_jp) * idy2;
-        const double diff_vz = (v_km - 2.0 * v_c + v_kp) * idz2;
-        const double dpy = (p_c - __ldg(pn + c - SY)) * idy;
-        const double rhsv = -((vu_p - vu_m) * idx) - (vv_p - vv_m) * idy - (vw_p - vw_m) * idz + p.fy +
-                            ire * (diff_vx + diff_vy + diff_vz);
-        double val = v_c + dt_alpha * rhsv + dt_beta * ov[q] - dt_gamma * dpy;
-        if (IBM) val = val * (1.0 / (1.0 + dt_gamma * __ldg(cv + c)));
-        vs[c] = val;
-        ov[q] = rhsv;
-    }
-    if (k >= p.nz0) {  // step.f90:170-200
-        const double w_ip = __ldg(wn + c + SX), w_im = __ldg(wn + c - SX);
-        const double w_jp = __ldg(wn + c + SY), w_jm = __ldg(wn + c - SY);
-        const double w_kp = __ldg(wn + c + SZ), w_km = __ldg(wn + c - SZ);
-        double s;
-        const double wu_p = 0.25 * (w_c + w_ip) * (__ldg(un + c + SX) + __ldg(un + c + SX - SZ));
-        const double wu_m = 0.25 * (w_c + w_im) * (u_c + __ldg(un + c - SZ));
-        s = w_c + w_kp;
-        const double ww_p = 0.25 * (s * s);
-        s = w_c + w_km;
-        const double ww_m = 0.25 * (s * s);
-        const double wv_p = 0.25 * (w_c + w_jp) * (__ldg(vn + c + SY) + __ldg(vn + c + SY - SZ));
-        const double wv_m = 0.25 * (w_c + w_jm) * (v_c + __ldg(vn + c - SZ));
-        const double diff_wx = (w_im - 2.0 * w_c + w_ip) * idx2;
-        const double diff_wy = (w_jm - 2.0 * w_c + w_jp) * idy2;
-        const double diff_wz = (w_km - 2.0 * w_c + w_kp) * idz2;
-        const double dpz = (p_c - __ldg(pn + c - SZ)) * idz;
-        const double rhsw = -((wu_p - wu_m) * idx) - (wv_p - wv_m) * idy - (ww_p - ww_m) * idz + p.fz +
-                            ire * (diff_wx + diff_wy + diff_wz);
-        double val = w_c + dt_alpha * rhsw + dt_beta * ow[q] - dt_gamma * dpz;
-        if (IBM) val = val * (1.0 / (1.0 + dt_gamma * __ldg(cw + c)));
-        ws[c] = val;
-        ow[q] = rhsw;
-    }
+    momentum_cell<IBM>(d, p, dt_alpha, dt_beta, dt_gamma, un, vn, wn, pn, us, vs, ws, ou, ov, ow, cu, cv, cw,
+                       pidx(d, i, j, k), i, j, k);
 }
 
 mdx_step_params mdx_make_params(const mdx_ctx_t* ctx) {
@@ -233,114 +156,26 @@ int mdx_k_apply_bc(mdx_ctx_t* ctx) {
 // directions run as three ordered launches.  Within one direction the
 // min and max faces of a column touch disjoint cells (ny, nx, nz >= 2).
 // ---------------------------------------------------------------------------
-struct mdx_four { double *un, *vn, *wn, *pn; };
 
 __global__ void k_bcrb_y(mdx_dims d, mdx_bc_dev bc, double dy, mdx_four f) {   // :207-258
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int k = blockIdx.y * blockDim.y + threadIdx.y + 1;
     if (i > d.nx || k > d.nz) return;
-    const int ny = d.ny;
-    const int* T = bc.type;
-    const double* V = bc.value;
-    double *un = f.un, *vn = f.vn, *wn = f.wn, *pn = f.pn;
-    if (bc.per[1]) {
-        un[pidx(d, i, 0, k)] = un[pidx(d, i, ny, k)];
-        vn[pidx(d, i, 0, k)] = vn[pidx(d, i, ny, k)];
-        wn[pidx(d, i, 0, k)] = wn[pidx(d, i, ny, k)];
-        pn[pidx(d, i, 0, k)] = pn[pidx(d, i, ny, k)];
-    } else {
-        if (T[bci(2, 0, 1)] == 0) un[pidx(d, i, 0, k)] = 2 * V[bci(2, 0, 1)] - un[pidx(d, i, 1, k)];
-        else un[pidx(d, i, 0, k)] = un[pidx(d, i, 1, k)] - V[bci(2, 0, 1)] * dy;
-        if (T[bci(2, 0, 2)] == 0) vn[pidx(d, i, 1, k)] = V[bci(2, 0, 2)];
-        else vn[pidx(d, i, 1, k)] = vn[pidx(d, i, 2, k)] - V[bci(2, 0, 2)] * dy;
-        if (T[bci(2, 0, 3)] == 0) wn[pidx(d, i, 0, k)] = 2 * V[bci(2, 0, 3)] - wn[pidx(d, i, 1, k)];
-        else wn[pidx(d, i, 0, k)] = wn[pidx(d, i, 1, k)] - V[bci(2, 0, 3)] * dy;
-    }
-    if (bc.per[1]) {
-        un[pidx(d, i, ny + 1, k)] = un[pidx(d, i, 1, k)];
-        vn[pidx(d, i, ny + 1, k)] = vn[pidx(d, i, 1, k)];
-        wn[pidx(d, i, ny + 1, k)] = wn[pidx(d, i, 1, k)];
-        pn[pidx(d, i, ny + 1, k)] = pn[pidx(d, i, 1, k)];
-    } else {
-        if (T[bci(2, 1, 1)] == 0) un[pidx(d, i, ny + 1, k)] = 2 * V[bci(2, 1, 1)] - un[pidx(d, i, ny, k)];
-        else un[pidx(d, i, ny + 1, k)] = un[pidx(d, i, ny, k)] + V[bci(2, 1, 1)] * dy;
-        if (T[bci(2, 1, 2)] == 0) vn[pidx(d, i, ny + 1, k)] = V[bci(2, 1, 2)];
-        else vn[pidx(d, i, ny + 1, k)] = vn[pidx(d, i, ny, k)] + V[bci(2, 1, 2)] * dy;
-        if (T[bci(2, 1, 3)] == 0) wn[pidx(d, i, ny + 1, k)] = 2 * V[bci(2, 1, 3)] - wn[pidx(d, i, ny, k)];
-        else wn[pidx(d, i, ny + 1, k)] = wn[pidx(d, i, ny, k)] + V[bci(2, 1, 3)] * dy;
-    }
+    bcrb_y_col(d, bc, dy, f, i, k);
 }
 
 __global__ void k_bcrb_x(mdx_dims d, mdx_bc_dev bc, double dx, mdx_four f) {   // :259-310
     const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int k = blockIdx.y * blockDim.y + threadIdx.y + 1;
     if (j > d.ny || k > d.nz) return;
-    const int nx = d.nx;
-    const int* T = bc.type;
-    const double* V = bc.value;
-    double *un = f.un, *vn = f.vn, *wn = f.wn, *pn = f.pn;
-    if (bc.per[0]) {
-        un[pidx(d, 0, j, k)] = un[pidx(d, nx, j, k)];
-        vn[pidx(d, 0, j, k)] = vn[pidx(d, nx, j, k)];
-        wn[pidx(d, 0, j, k)] = wn[pidx(d, nx, j, k)];
-        pn[pidx(d, 0, j, k)] = pn[pidx(d, nx, j, k)];
-    } else {
-        if (T[bci(1, 0, 1)] == 0) un[pidx(d, 1, j, k)] = V[bci(1, 0, 1)];
-        else un[pidx(d, 1, j, k)] = un[pidx(d, 2, j, k)] - V[bci(1, 0, 1)] * dx;
-        if (T[bci(1, 0, 2)] == 0) vn[pidx(d, 0, j, k)] = 2 * V[bci(1, 0, 2)] - vn[pidx(d, 1, j, k)];
-        else vn[pidx(d, 0, j, k)] = vn[pidx(d, 1, j, k)] - V[bci(1, 0, 2)] * dx;
-        if (T[bci(1, 0, 3)] == 0) wn[pidx(d, 0, j, k)] = 2 * V[bci(1, 0, 3)] - wn[pidx(d, 1, j, k)];
-        else wn[pidx(d, 0, j, k)] = wn[pidx(d, 1, j, k)] - V[bci(1, 0, 3)] * dx;
-    }
-    if (bc.per[0]) {
-        un[pidx(d, nx + 1, j, k)] = un[pidx(d, 1, j, k)];
-        vn[pidx(d, nx + 1, j, k)] = vn[pidx(d, 1, j, k)];
-        wn[pidx(d, nx + 1, j, k)] = wn[pidx(d, 1, j, k)];
-        pn[pidx(d, nx + 1, j, k)] = pn[pidx(d, 1, j, k)];
-    } else {
-        if (T[bci(1, 1, 1)] == 0) un[pidx(d, nx + 1, j, k)] = V[bci(1, 1, 1)];
-        else un[pidx(d, nx + 1, j, k)] = un[pidx(d, nx, j, k)] + V[bci(1, 1, 1)] * dx;
-        if (T[bci(1, 1, 2)] == 0) vn[pidx(d, nx + 1, j, k)] = 2 * V[bci(1, 1, 2)] - vn[pidx(d, nx, j, k)];
-        else vn[pidx(d, nx + 1, j, k)] = vn[pidx(d, nx, j, k)] + V[bci(1, 1, 2)] * dx;
-        if (T[bci(1, 1, 3)] == 0) wn[pidx(d, nx + 1, j, k)] = 2 * V[bci(1, 1, 3)] - wn[pidx(d, nx, j, k)];
-        else wn[pidx(d, nx + 1, j, k)] = wn[pidx(d, nx, j, k)] + V[bci(1, 1, 3)] * dx;
-    }
+    bcrb_x_col(d, bc, dx, f, j, k);
 }
 
 __global__ void k_bcrb_z(mdx_dims d, mdx_bc_dev bc, double dz, mdx_four f) {   // :311-364
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     if (i > d.nx || j > d.ny) return;
-    const int nz = d.nz;
-    const int* T = bc.type;
-    const double* V = bc.value;
-    double *un = f.un, *vn = f.vn, *wn = f.wn, *pn = f.pn;
-    if (bc.per[2]) {
-        un[pidx(d, i, j, 0)] = un[pidx(d, i, j, nz)];
-        vn[pidx(d, i, j, 0)] = vn[pidx(d, i, j, nz)];
-        wn[pidx(d, i, j, 0)] = wn[pidx(d, i, j, nz)];
-        pn[pidx(d, i, j, 0)] = pn[pidx(d, i, j, nz)];
-    } else {
-        if (T[bci(3, 0, 1)] == 0) un[pidx(d, i, j, 0)] = 2 * V[bci(3, 0, 1)] - un[pidx(d, i, j, 1)];
-        else un[pidx(d, i, j, 0)] = un[pidx(d, i, j, 1)] - V[bci(3, 0, 1)] * dz;
-        if (T[bci(3, 0, 2)] == 0) vn[pidx(d, i, j, 0)] = 2 * V[bci(3, 0, 2)] - vn[pidx(d, i, j, 1)];
-        else vn[pidx(d, i, j, 0)] = vn[pidx(d, i, j, 1)] - V[bci(3, 0, 2)] * dz;
-        if (T[bci(3, 0, 3)] == 0) wn[pidx(d, i, j, 1)] = V[bci(3, 0, 3)];
-        else wn[pidx(d, i, j, 1)] = wn[pidx(d, i, j, 2)] - V[bci(3, 0, 3)] * dz;
-    }
-    if (bc.per[2]) {
-        un[pidx(d, i, j, nz + 1)] = un[pidx(d, i, j, 1)];
-        vn[pidx(d, i, j, nz + 1)] = vn[pidx(d, i, j, 1)];
-        wn[pidx(d, i, j, nz + 1)] = wn[pidx(d, i, j, 1)];
-        pn[pidx(d, i, j, nz + 1)] = pn[pidx(d, i, j, 1)];
-    } else {
-        if (T[bci(3, 1, 1)] == 0) un[pidx(d, i, j, nz + 1)] = 2 * V[bci(3, 1, 1)] - un[pidx(d, i, j, nz)];
-        else un[pidx(d, i, j, nz + 1)] = un[pidx(d, i, j, nz)] + V[bci(3, 1, 1)] * dz;
-        if (T[bci(3, 1, 2)] == 0) vn[pidx(d, i, j, nz + 1)] = 2 * V[bci(3, 1, 2)] - vn[pidx(d, i, j, nz)];
-        else vn[pidx(d, i, j, nz + 1)] = vn[pidx(d, i, j, nz)] + V[bci(3, 1, 2)] * dz;
-        if (T[bci(3, 1, 3)] == 0) wn[pidx(d, i, j, nz + 1)] = V[bci(3, 1, 3)];
-        else wn[pidx(d, i, j, nz + 1)] = wn[pidx(d, i, j, nz)] + V[bci(3, 1, 3)] * dz;
-    }
+    bcrb_z_col(d, bc, dz, f, i, j);
 }
 
 int mdx_k_apply_bc_redblack(mdx_ctx_t* ctx) {
@@ -558,17 +393,6 @@ int mdx_k_center_vel(mdx_ctx_t* ctx, double* uc, double* vc, double* wc) {
 // Steele, Lea & Flood 2014 on seed + golden*(field<<40 | padded index)).
 // yc(x) per x index comes from the host so the profile is the host's libm.
 // ---------------------------------------------------------------------------
-__device__ inline uint64_t ic_hash(uint64_t seed, uint64_t field, uint64_t lin) {
-    uint64_t z = seed + 0x9E3779B97F4A7C15ull * ((field << 40) | lin);
-    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-    return z ^ (z >> 31);
-}
-__device__ inline double ic_uniform(uint64_t seed, uint64_t field, uint64_t lin, double amp) {
-    const double u01 = (double)(ic_hash(seed, field, lin) >> 11) * (1.0 / 9007199254740992.0);
-    return amp * (2.0 * u01 - 1.0);
-}
-
 __global__ void k_channel_ic(mdx_dims d, double dy, uint64_t seed, double amp_u, double amp_vw,
                              const double* __restrict__ yc, double* __restrict__ un, double* __restrict__ vn,
                              double* __restrict__ wn) {

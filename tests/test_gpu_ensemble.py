@@ -1,0 +1,130 @@
+"""Batched ensemble: every member against the single-context path run
+alone (bit for bit with a fixed iteration count), CUDA-graph replay against
+eager launches, and the autotuner's cache."""
+import json
+
+import numpy as np
+import pytest
+
+import mobydiff_b200 as M
+from tests.helpers import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+MEMBERS = [
+    dict(nx=32, ny=32, nz=32, re=3000.0, amp=0.05, seed=11),
+    dict(nx=48, ny=32, nz=64, re=1500.0, amp=0.08, seed=12),
+    dict(nx=64, ny=48, nz=32, re=4200.0, amp=0.0, seed=13),
+]
+
+
+def _members():
+    return [M.make_member(**m) for m in MEMBERS]
+
+
+def _single(m, opts, mode):
+    g = M.make_grid(m.nx, m.ny, m.nz, m.lx, m.ly, m.lz, m.re, m.dt, (2.0 / m.re, 0.0, 0.0))
+    s = M.Solver(g, M.channel_bc(), 0)
+    s.enter_field_data()
+    y0 = (m.ly - 2.0) / 2.0
+    lam = m.lx / 2.0
+    if m.amp > 0.0:
+        s.enter_ibm_data(*M.set_ibm_coeff(g, M.ibm_wavy(m.amp, lam, y0)))
+    s.init_pressure_solver(opts)
+    s.set_pressure_guess(mode, record=mode != M.GUESS_ZERO)
+    s.channel_ic(m.seed, 0.1, 0.01, y0, m.amp, lam)
+    return s
+
+
+@pytest.mark.parametrize("mode", [M.GUESS_ZERO, M.GUESS_EXTRAPOLATED])
+def test_fixed_iterations_bitwise_equal_to_single_channels(mode):
+    opts = M.make_solver_opts(M.SOLVER_REDBLACK, sor=1.7, n_iter=30, tol=0.0)
+    mems = _members()
+    with M.Ensemble(mems, opts) as E:
+        E.set_guess(mode)
+        E.ic()
+        for q, m in enumerate(mems):   # the t=0 projection alone
+            with _single(m, opts, mode) as s:
+                for n in ("un", "vn", "wn", "pn"):
+                    assert np.array_equal(E.get(q, n), s.get(n)), (q, n)
+        E.step(3)
+        for q, m in enumerate(mems):
+            with _single(m, opts, mode) as s:
+                s.step(3)
+                for n in ("un", "vn", "wn", "pn"):
+                    assert np.array_equal(E.get(q, n), s.get(n)), (q, n)
+                st, tot = E.member_stats(q)
+                assert st.iterations == 30 and tot == 9 * 30
+
+
+def test_tolerance_mode_matches_single_channels():
+    opts = M.make_solver_opts(M.SOLVER_REDBLACK, sor=1.7, tol=1e-8, check_every=10, max_iter=200000)
+    mems = _members()
+    with M.Ensemble(mems, opts) as E:
+        E.set_guess(M.GUESS_EXTRAPOLATED)
+        E.ic()
+        it_e = E.step(4)
+        it_s = 0
+        for q, m in enumerate(mems):
+            with _single(m, opts, M.GUESS_EXTRAPOLATED) as s:
+                it_s += s.step(4)
+                st, _ = E.member_stats(q)
+                ss = s.last_solve_stats()
+                assert st.status == 0 and abs(st.iterations - ss.iterations) <= 10, (q, st.iterations, ss.iterations)
+                assert st.residual <= 1e-8 * 1.0000001 or st.residual * st.residual0 <= st.atol * 1.0000001
+                for n in ("un", "vn", "wn"):
+                    assert rel_l2(E.get(q, n), s.get(n)) <= 1e-6, (q, n)
+        print("iterations: ensemble", it_e, "single channels", it_s)
+        assert abs(it_e - it_s) <= 0.02 * it_s + 30 * len(mems)
+
+
+def test_graph_replay_equals_eager_launches():
+    opts = M.make_solver_opts(M.SOLVER_REDBLACK, sor=1.7, tol=1e-8, check_every=10, max_iter=200000)
+    mems = _members()
+    with M.Ensemble(mems, opts) as A, M.Ensemble(mems, opts) as B:
+        for E in (A, B):
+            E.set_guess(M.GUESS_EXTRAPOLATED)
+            E.ic()
+        B.use_graph(False)
+        ia, ib = A.step(3), B.step(3)
+        assert ia == ib
+        print("graph:", A.info())
+        assert not B.info()["graph"]
+        for q in range(len(mems)):
+            for n in ("un", "vn", "wn", "pn"):
+                assert np.array_equal(A.get(q, n), B.get(q, n)), (q, n)
+
+
+def test_autotuner_choice_is_cached_and_results_unchanged(tmp_path):
+    cache = str(tmp_path / "ensemble_tune.json")
+    opts = M.make_solver_opts(M.SOLVER_REDBLACK, sor=1.7, n_iter=20, tol=0.0)
+    mems = _members()
+    with M.Ensemble(mems, opts) as A, M.Ensemble(mems, opts) as B:
+        for E in (A, B):
+            E.set_guess(M.GUESS_EXTRAPOLATED)
+            E.ic()
+        t, b, ms = A.tune(cache)
+        assert t in (128, 256, 512) and b in (1, 2, 4) and ms > 0.0
+        data = json.load(open(cache))
+        assert len(data) == 1 and list(data.values())[0]["threads"] == t
+        t2, b2, ms2 = B.tune(cache)   # cache hit: no timing
+        assert (t2, b2, ms2) == (t, b, -1.0)
+        B.config(128, 1)
+        A.step(2)
+        B.step(2)
+        for q in range(len(mems)):
+            for n in ("un", "vn", "wn", "pn"):
+                assert np.array_equal(A.get(q, n), B.get(q, n)), (q, n)
+
+
+def test_ensemble_argument_checks():
+    opts = M.make_solver_opts(M.SOLVER_REDBLACK, sor=1.7, n_iter=5, tol=0.0)
+    with pytest.raises(M.MdxError):
+        M.Ensemble([M.make_member(33, 16, 16)], opts)   # odd nx
+    with pytest.raises(M.MdxError):
+        M.Ensemble([M.make_member(32, 16, 16)], M.make_solver_opts(M.SOLVER_FFT))
+    with M.Ensemble([M.make_member(32, 16, 16)], opts) as E:
+        with pytest.raises(M.MdxError):
+            E.config(100)
+        with pytest.raises(M.MdxError):
+            E.set_guess(M.GUESS_LEARNED)
