@@ -53,6 +53,10 @@ CONFIGS = {
                tol=1e-8, method="learned-mixed"),
     "c1-plain": dict(C1_GEOM, workload="wavy-wall IBM channel 256x128x128, FP64 red-black SOR omega=1.7 to residual "
                                        "1e-10", tol=1e-10, method="plain"),
+    "c4": dict(workload="ensemble of 64 wavy-wall IBM channels, nx,nz in 32..128 and ny in 32..96 (multiples of 16), "
+                         "Re U(1000,5000), A U(0,0.1), FP64 red-black SOR omega=1.7 to residual 1e-8 from the "
+                         "extrapolated increment; one persistent launch per RK3 substage, CUDA graph, autotuned grid",
+               solver="redblack", sor=1.7, tol=1e-8, check_every=10, members=64, method="ensemble"),
     "c0": dict(workload="periodic channel 64^3, FP64 FFT+Thomas", nx=64, ny=64, nz=64, lx=2 * math.pi, ly=2.0,
                lz=math.pi, re=2000.0, dt=1e-3, solver="fft", ibm="none", amp=0.0, method="plain"),
     "c2": dict(workload="periodic channel 512x256x256, FP64 FFT+Thomas", nx=512, ny=256, nz=256,
@@ -269,6 +273,24 @@ def run_reference(args, cfg):
     return 0
 
 
+def max_over_ranks(ms, pg):
+    """The slowest rank's time: every rank times its own replica, the job
+    took as long as the slowest one (NCCL on the GPU, gloo on the CPU)."""
+    import torch
+    if pg is None:
+        return ms
+    dev = "cuda" if pg.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=dev)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_value(cells_per_rank, steps, ms_max, world):
+    """Whole-job Mcell-steps/s: the cells of every replica times the steps,
+    over the slowest rank's time."""
+    return world * cells_per_rank * steps / (ms_max / 1e3) / 1e6
+
+
 def _timed_steps(s, stream, steps, pg=None, timing=False):
     """K steps between events on the solver's stream (barrier + synchronize
     on both sides); returns (ms over ranks, ms of this rank, iterations,
@@ -297,9 +319,7 @@ def _timed_steps(s, stream, steps, pg=None, timing=False):
     s.set_timing(False)
     ms_all = ms
     if pg:
-        t = torch.tensor([ms], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms_all = float(t.item())
+        ms_all = max_over_ranks(ms, pg)
     return ms_all, ms, iters, launches, tim
 
 
@@ -322,9 +342,7 @@ def _e2e_steps(s, stream, host, steps, pg=None):
     torch.cuda.synchronize()
     ems = e0.elapsed_time(e1)
     if pg:
-        t = torch.tensor([ems], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ems = float(t.item())
+        ems = max_over_ranks(ems, pg)
     return ems, iters
 
 
@@ -427,6 +445,137 @@ def run_plain(args, cfg):
                 "gpu_launches": launches}
         print(json.dumps(line), flush=True)
     s.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
+def _splitmix(state):
+    state[0] = (state[0] + 0x9E3779B97F4A7C15) & 0xFFFFFFFFFFFFFFFF
+    z = state[0]
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & 0xFFFFFFFFFFFFFFFF
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & 0xFFFFFFFFFFFFFFFF
+    return z ^ (z >> 31)
+
+
+def ensemble_members(M, n, seed=SEED):
+    """Seeded members: nx, nz in {32..128}, ny in {32..96} (multiples of 16),
+    Re ~ U(1000, 5000), A ~ U(0, 0.1)."""
+    st = [seed]
+    u01 = lambda: (_splitmix(st) >> 11) * (1.0 / 9007199254740992.0)
+    out = []
+    for q in range(n):
+        nx = 16 * (2 + _splitmix(st) % 7)
+        nz = 16 * (2 + _splitmix(st) % 7)
+        ny = 16 * (2 + _splitmix(st) % 5)
+        re = 1000.0 + 4000.0 * u01()
+        amp = 0.1 * u01()
+        out.append(M.make_member(nx, ny, nz, re=re, amp=amp, seed=seed + 1 + q))
+    return out
+
+
+def run_ensemble(args, cfg):
+    import torch
+    import mobydiff_b200 as M
+
+    ws, rank, local = _dist()
+    device = local
+    pg = _init_dist(device)
+    mems = ensemble_members(M, cfg["members"])
+    sizes = [m.nx * m.ny * m.nz for m in mems]
+    cells = sum(sizes)
+    opts = M.make_solver_opts(M.SOLVER_REDBLACK, sor=cfg["sor"], tol=cfg["tol"], check_every=cfg["check_every"],
+                              max_iter=400000)
+    W, K = args.warmup, args.steps
+    E = M.Ensemble(mems, opts, device)
+    E.set_guess(M.GUESS_EXTRAPOLATED)
+    E.ic()
+    cache = os.path.join(os.path.expanduser("~"), ".cache", "mobydiff_b200", "ensemble_tune.json")
+    os.makedirs(os.path.dirname(cache), exist_ok=True)
+    E.step(W)
+    tuned = E.tune(cache)   # times each candidate grid from a saved state, then restores it
+    host = {(q, n): E.get(q, n) for q in range(len(mems)) for n in ("un", "vn", "wn", "pn")}
+    it0 = [E.member_stats(q)[1] for q in range(len(mems))]
+    if pg:
+        pg.barrier()
+    clocks = ClockSampler(device)
+    clocks.start()
+    iters = E.step(K)   # device time between events around the K graph replays
+    clk = clocks.stop()
+    info = E.info()
+    it_m = [E.member_stats(q)[1] - it0[q] for q in range(len(mems))]
+    ms = info["last_step_ms"] * K
+    ms_all = ms
+    if pg:
+        ms_all = max_over_ranks(ms, pg)
+    value = ws * cells * K / (ms_all / 1e3) / 1e6
+    # red-black path algorithmic bytes (FP64): 3 x 104 B per cell per step for
+    # the predictor and projection set-up, 64 B per cell per red+black iteration
+    alg = sum(n * (3.0 * 104.0 * K + 64.0 * it) for n, it in zip(sizes, it_m))
+    peak, peak_kind = _peaks()
+    achieved = alg / (ms / 1e3) / 1e9
+    roofline = {"kernel": "k_ens_substage (whole substage)", "bound": "hbm", "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                "algorithmic_bytes": alg / K, "avg_launch_ms": ms / (3 * K), "launches": 3 * K}
+    # e2e: the timed steps replayed from the same u, v, w, p, copied from host
+    # memory every step through the C ABI (the warm-start history has moved on)
+    e2e_line = None
+    if not args.no_e2e:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2e_iters = 0
+        for _ in range(K):
+            for (q, n), a in host.items():
+                E.set(q, n, a)
+            e2e_iters += E.step(1)
+            for (q, n) in host:
+                E.get(q, n)
+        e2e_s = time.perf_counter() - t0
+        nbytes = sum(a.nbytes for a in host.values())
+        e2e_line = {"value": ws * cells * K / e2e_s / 1e6, "unit": UNIT, "h2d_bytes_per_step": nbytes,
+                    "d2h_bytes_per_step": nbytes, "timer": "host wall clock around the C-ABI calls",
+                    "same_steps_as_value": False, "iterations": e2e_iters}
+    # the same members one after another through single contexts
+    seq = None
+    if not args.quick:
+        seq_ms, seq_iters = 0.0, 0
+        for m in mems:
+            g = M.make_grid(m.nx, m.ny, m.nz, m.lx, m.ly, m.lz, m.re, m.dt, (2.0 / m.re, 0.0, 0.0))
+            s = M.Solver(g, M.channel_bc(), device)
+            s.enter_field_data()
+            y0, lam = (m.ly - 2.0) / 2.0, m.lx / 2.0
+            if m.amp > 0.0:
+                s.enter_ibm_data(*M.set_ibm_coeff(g, M.ibm_wavy(m.amp, lam, y0)))
+            s.init_pressure_solver(opts)
+            s.set_pressure_guess(M.GUESS_EXTRAPOLATED, record=True)
+            s.channel_ic(m.seed, 0.1, 0.01, y0, m.amp, lam)
+            s.step(W)
+            stream = torch.cuda.ExternalStream(s.stream(), device=device)
+            ms1, _, it1, _, _ = _timed_steps(s, stream, K)
+            seq_ms += ms1
+            seq_iters += it1
+            s.close()
+        seq = {"value": ws * cells * K / (seq_ms / 1e3) / 1e6, "unit": UNIT, "ms_per_step": seq_ms / K,
+               "iterations": seq_iters, "ensemble_iterations": iters}
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": W,
+                "ms_per_step": ms_all / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64", "data": "synthetic: 64 seeded members (SplitMix64 sizes, Re, A, IC seeds)",
+                "config": {"workload": cfg["workload"], "members": len(mems), "cells": cells, "tol": cfg["tol"],
+                           "parallelism": f"replicas x{ws}",
+                           "l2": "inputs larger than L2 (64 members' state > 126 MB)"},
+                "poisson_iters_per_member_substage": iters / (3 * K * len(mems)),
+                "ensemble": {"threads": info["threads"], "grid": info["grid"], "cuda_graph": info["graph"],
+                             "low_regs": info["low_regs"],
+                             "autotuned": {"threads": tuned[0], "blocks_per_sm": tuned[1], "low_regs": tuned[2],
+                                           "step_ms": tuned[3] if tuned[3] >= 0 else "from cache"},
+                             "launches_per_step": 3},
+                "sequential_single_contexts": seq,
+                "roofline": roofline, "cpu_baseline": None, "clocks": clk, "e2e": e2e_line,
+                "gpu_launches": 3 * K}
+        print(json.dumps(line), flush=True)
+    E.close()
     if pg:
         pg.barrier()
         pg.destroy_process_group()
@@ -603,6 +752,8 @@ def main():
         return run_reference(args, cfg)
     if args.profile_mixed:
         return run_profile_mixed(args, cfg)
+    if cfg["method"] == "ensemble":
+        return run_ensemble(args, cfg)
     if cfg["method"] == "learned-mixed" and not args.profile:
         return run_learned_mixed(args, cfg)
     return run_plain(args, cfg)

@@ -103,13 +103,13 @@ def test_autotuner_choice_is_cached_and_results_unchanged(tmp_path):
         for E in (A, B):
             E.set_guess(M.GUESS_EXTRAPOLATED)
             E.ic()
-        t, b, ms = A.tune(cache)
-        assert t in (128, 256, 512) and b in (1, 2, 4) and ms > 0.0
+        t, b, lr, ms = A.tune(cache)
+        assert t in (128, 256, 512) and b in (1, 2, 4, 8) and ms > 0.0
         data = json.load(open(cache))
-        assert len(data) == 1 and list(data.values())[0]["threads"] == t
-        t2, b2, ms2 = B.tune(cache)   # cache hit: no timing
-        assert (t2, b2, ms2) == (t, b, -1.0)
-        B.config(128, 1)
+        entry = list(data.values())[0]
+        assert len(data) == 1 and entry["threads"] == t and entry["low_regs"] == int(lr)
+        assert B.tune(cache) == (t, b, lr, -1.0)   # cache hit: no timing
+        B.config(128, 1, low_regs=not lr)
         A.step(2)
         B.step(2)
         for q in range(len(mems)):
