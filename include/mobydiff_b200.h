@@ -324,15 +324,18 @@ int mdx_ensemble_member_stats(mdx_ensemble_t* ens, int member, mdx_solve_stats_t
 /* Padded field MDX_UN, MDX_VN, MDX_WN or MDX_PN of a member. */
 int mdx_ensemble_get(mdx_ensemble_t* ens, int member, int field, double* host);
 int mdx_ensemble_set(mdx_ensemble_t* ens, int member, int field, const double* host);
-/* Threads per block (multiple of 32, <= 512) and blocks per SM (0: as many
- * as fit) of the persistent grid. */
-int mdx_ensemble_config(mdx_ensemble_t* ens, int threads, int blocks_per_sm);
-/* Time one step of each candidate grid from the same saved state and keep
- * the fastest; the choice is cached in the JSON file cache_path (may be
- * NULL) under a key of the member sizes, the mode and the device name. */
-int mdx_ensemble_tune(mdx_ensemble_t* ens, const char* cache_path, int* threads, int* blocks_per_sm, double* ms);
+/* Launch shape of the persistent kernel: threads per block (multiple of
+ * 32, <= 512), blocks per SM (0: as many as fit) and the register variant
+ * (low_regs != 0: 64 registers per thread, twice the resident warps). */
+int mdx_ensemble_config(mdx_ensemble_t* ens, int threads, int blocks_per_sm, int low_regs);
+/* Time one step of each candidate launch shape from the same saved state and
+ * keep the fastest; the choice is cached in the JSON file cache_path (may be
+ * NULL) under a key of the member sizes, the mode and the device name
+ * (*ms = -1 when it came from the cache). */
+int mdx_ensemble_tune(mdx_ensemble_t* ens, const char* cache_path, int* threads, int* blocks_per_sm, int* low_regs,
+                      double* ms);
 int mdx_ensemble_use_graph(mdx_ensemble_t* ens, int on);
-int mdx_ensemble_info(mdx_ensemble_t* ens, int* threads, int* grid, int* graph, double* last_step_ms,
+int mdx_ensemble_info(mdx_ensemble_t* ens, int* threads, int* grid, int* low_regs, int* graph, double* last_step_ms,
                       long long* launches);
 
 /* ---- learned warm start (no counterpart in the reference) ----------------

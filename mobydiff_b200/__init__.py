@@ -190,10 +190,10 @@ def lib():
         "mdx_ensemble_member_stats": (i, [vp, i, P(SolveStatsT), P(C.c_longlong)]),
         "mdx_ensemble_get": (i, [vp, i, i, vp]),
         "mdx_ensemble_set": (i, [vp, i, i, vp]),
-        "mdx_ensemble_config": (i, [vp, i, i]),
-        "mdx_ensemble_tune": (i, [vp, C.c_char_p, P(i), P(i), P(d)]),
+        "mdx_ensemble_config": (i, [vp, i, i, i]),
+        "mdx_ensemble_tune": (i, [vp, C.c_char_p, P(i), P(i), P(i), P(d)]),
         "mdx_ensemble_use_graph": (i, [vp, i]),
-        "mdx_ensemble_info": (i, [vp, P(i), P(i), P(i), P(d), P(C.c_longlong)]),
+        "mdx_ensemble_info": (i, [vp, P(i), P(i), P(i), P(i), P(d), P(C.c_longlong)]),
         "mdx_default_unet_opts": (None, [P(UnetOptsT)]),
         "mdx_unet_create": (i, [vp, P(UnetOptsT)]),
         "mdx_unet_destroy": (i, [vp]),
@@ -621,20 +621,23 @@ class Ensemble:
         a = np.ascontiguousarray(a, dtype=np.float64)
         self._c(lib().mdx_ensemble_set(self.h, int(m), FIELD_ID[name], a.ctypes.data_as(C.c_void_p)))
 
-    def config(self, threads: int, blocks_per_sm: int = 0) -> None:
-        self._c(lib().mdx_ensemble_config(self.h, int(threads), int(blocks_per_sm)))
+    def config(self, threads: int, blocks_per_sm: int = 0, low_regs: bool = False) -> None:
+        self._c(lib().mdx_ensemble_config(self.h, int(threads), int(blocks_per_sm), 1 if low_regs else 0))
 
     def tune(self, cache_path=None):
-        t, b, ms = C.c_int(0), C.c_int(0), C.c_double(0.0)
+        """(threads, blocks per SM, low-register variant, ms of the chosen
+        shape's step; -1 when it came from the cache)."""
+        t, b, r, ms = C.c_int(0), C.c_int(0), C.c_int(0), C.c_double(0.0)
         path = cache_path.encode() if cache_path else None
-        self._c(lib().mdx_ensemble_tune(self.h, path, C.byref(t), C.byref(b), C.byref(ms)))
-        return t.value, b.value, ms.value
+        self._c(lib().mdx_ensemble_tune(self.h, path, C.byref(t), C.byref(b), C.byref(r), C.byref(ms)))
+        return t.value, b.value, bool(r.value), ms.value
 
     def use_graph(self, on: bool) -> None:
         self._c(lib().mdx_ensemble_use_graph(self.h, 1 if on else 0))
 
     def info(self) -> dict:
-        t, g, gr, ms, ln = C.c_int(0), C.c_int(0), C.c_int(0), C.c_double(0.0), C.c_longlong(0)
-        self._c(lib().mdx_ensemble_info(self.h, C.byref(t), C.byref(g), C.byref(gr), C.byref(ms), C.byref(ln)))
-        return {"threads": t.value, "grid": g.value, "graph": bool(gr.value), "last_step_ms": ms.value,
-                "launches": ln.value}
+        t, g, lr, gr, ms, ln = C.c_int(0), C.c_int(0), C.c_int(0), C.c_int(0), C.c_double(0.0), C.c_longlong(0)
+        self._c(lib().mdx_ensemble_info(self.h, C.byref(t), C.byref(g), C.byref(lr), C.byref(gr), C.byref(ms),
+                                        C.byref(ln)))
+        return {"threads": t.value, "grid": g.value, "low_regs": bool(lr.value), "graph": bool(gr.value),
+                "last_step_ms": ms.value, "launches": ln.value}

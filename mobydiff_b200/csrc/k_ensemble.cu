@@ -45,6 +45,17 @@ namespace {
 constexpr int ETILE = 256;           // elements per work tile
 constexpr int MAX_THREADS = 512;
 
+// n / d for 32-bit n by one multiply-high with c = ceil(2^64 / d) (Lemire,
+// Kaser & Kurz, "Faster remainder by direct computation", 2019); d >= 2.
+struct fdiv32 {
+    unsigned long long c;
+    unsigned d;
+};
+fdiv32 make_fdiv(unsigned d) { return fdiv32{~0ull / d + 1ull, d}; }
+__device__ __forceinline__ unsigned fq(unsigned n, const fdiv32& f) {
+    return (unsigned)__umul64hi(f.c, (unsigned long long)n);
+}
+
 struct ens_member {                  // per member, read-only in the kernel
     mdx_dims d;
     mdx_step_params p;
@@ -53,6 +64,7 @@ struct ens_member {                  // per member, read-only in the kernel
     double dt;
     double idx, idy, idz;            // 1/dx, 1/dy, 1/dz
     int ibm;                         // coefficient planes present (MU_PLANE)
+    fdiv32 fx, fy, fh;               // division by nx, ny, nx/2
     double *un, *vn, *wn, *pn, *us, *vs, *ws, *ou, *ov, *ow;
     double *cu, *cv, *cw;            // (nx+2)(ny+2) planes
     double *mu;                      // 3 planes of this projection
@@ -117,11 +129,12 @@ __device__ void block_reduce3(double& s, double& m, double& u) {
     }
 }
 
-__device__ __forceinline__ void cell_ijk(const mdx_dims& d, long long t, int& i, int& j, int& k) {
-    i = (int)(t % d.nx) + 1;
-    const long long r = t / d.nx;
-    j = (int)(r % d.ny) + 1;
-    k = (int)(r / d.ny) + 1;
+__device__ __forceinline__ void cell_ijk(const ens_member& M, unsigned t, int& i, int& j, int& k) {
+    const unsigned r = fq(t, M.fx);
+    i = (int)(t - r * M.fx.d) + 1;
+    const unsigned kk = fq(r, M.fy);
+    j = (int)(r - kk * M.fy.d) + 1;
+    k = (int)kk + 1;
 }
 
 __device__ __forceinline__ double dg_of(const ens_args& A, const ens_member& M) {
@@ -139,10 +152,10 @@ __device__ void residual_tiles(const ens_args& A, Want want) {
         const mdx_dims& d = M.d;
         double s = 0.0, m = 0.0, um = 0.0;
         for (int e = threadIdx.x; e < ETILE; e += blockDim.x) {
-            const long long t = (long long)T.y + e;
-            if (t >= d.nint) break;
+            const unsigned t = (unsigned)T.y + e;
+            if (t >= (unsigned)d.nint) break;
             int i, j, k;
-            cell_ijk(d, t, i, j, k);
+            cell_ijk(M, t, i, j, k);
             const int ip = i + 1 > d.nx ? 1 : i + 1;
             const int jp = (M.bc.per[1] && j + 1 > d.ny) ? 1 : j + 1;
             const int kp = k + 1 > d.nz ? 1 : k + 1;
@@ -180,13 +193,13 @@ __device__ void member_sums(const ens_args& A, int m, double& s, double& um) {
 
 // One colour sweep of member M's cell at sweep element t (the generic
 // k_sor_sweep of k_sor.cu).
-__device__ __forceinline__ void sweep_cell(const ens_member& M, const mdx_sor_params& p, int parity, long long t) {
+__device__ __forceinline__ void sweep_cell(const ens_member& M, const mdx_sor_params& p, int parity, unsigned t) {
     const mdx_dims& d = M.d;
-    const int na = d.nx / 2;
-    const int ni = (int)(t % na) + 1;
-    const long long r = t / na;
-    const int j = (int)(r % d.ny) + 1;
-    const int kk = (int)(r / d.ny) + 1;
+    const unsigned r = fq(t, M.fh);
+    const int ni = (int)(t - r * M.fh.d) + 1;
+    const unsigned q = fq(r, M.fy);
+    const int j = (int)(r - q * M.fy.d) + 1;
+    const int kk = (int)q + 1;
     const int nx = d.nx, ny = d.ny, nz = d.nz;
     const int k = parity ? nz + 1 - kk : kk;
     const mdx_bc_dev& bc = M.bc;
@@ -240,10 +253,10 @@ __device__ void sweep_tiles(const ens_args& A, int parity, Want want) {
         const int2 T = A.half.t[ti];
         if (!want(T.x)) continue;
         const ens_member& M = A.mem[T.x];
-        const long long nh = (long long)(M.d.nx / 2) * M.d.ny * M.d.nz;
+        const unsigned nh = (unsigned)((M.d.nx / 2) * M.d.ny * M.d.nz);
         const mdx_sor_params p = proj_params(M, dg_of(A, M));
         for (int e = threadIdx.x; e < ETILE; e += blockDim.x) {
-            const long long t = (long long)T.y + e;
+            const unsigned t = (unsigned)T.y + e;
             if (t >= nh) break;
             sweep_cell(M, p, parity, t);
         }
@@ -269,18 +282,18 @@ __device__ void cell_tiles(const ens_args& A, F f) {
         const int2 T = A.cell.t[ti];
         const ens_member& M = A.mem[T.x];
         for (int e = threadIdx.x; e < ETILE; e += blockDim.x) {
-            const long long t = (long long)T.y + e;
-            if (t >= M.d.nint) break;
+            const unsigned t = (unsigned)T.y + e;
+            if (t >= (unsigned)M.d.nint) break;
             f(T.x, M, t);
         }
     }
 }
 
 // Apply member M's increment guess at cell t (k_apply_guess of k_warm.cu).
-__device__ __forceinline__ void guess_cell(const ens_member& M, double dg, long long t) {
+__device__ __forceinline__ void guess_cell(const ens_member& M, double dg, unsigned t) {
     const mdx_dims& d = M.d;
     int i, j, k;
-    cell_ijk(d, t, i, j, k);
+    cell_ijk(M, t, i, j, k);
     const int im = i == 1 ? d.nx : i - 1;
     const int km = k == 1 ? d.nz : k - 1;
     const long long c = pidx(d, i, j, k);
@@ -305,7 +318,11 @@ __device__ __forceinline__ void guess_cell(const ens_member& M, double dg, long 
     M.pn[c] += gs[t];
 }
 
-__global__ void __launch_bounds__(MAX_THREADS) k_ens_substage(ens_args A) {
+// MINB 1: registers for the predictor (one block of 512 per SM); MINB 2:
+// 64 registers (spills in the predictor), twice the resident warps for
+// the latency-bound sweeps.  The autotuner picks one.
+template <int MINB>
+__global__ void __launch_bounds__(MAX_THREADS, MINB) k_ens_substage(ens_args A) {
     cg::grid_group grid = cg::this_grid();
     const int s = A.substage;
     const bool warm = A.momentum && A.guess_mode != MDX_GUESS_ZERO;
@@ -314,9 +331,9 @@ __global__ void __launch_bounds__(MAX_THREADS) k_ens_substage(ens_args A) {
 
     // ---- predictor (or u* = u for the t=0 projection) ----
     if (A.momentum) {
-        cell_tiles(A, [&](int, const ens_member& M, long long t) {
+        cell_tiles(A, [&](int, const ens_member& M, unsigned t) {
             int i, j, k;
-            cell_ijk(M.d, t, i, j, k);
+            cell_ijk(M, t, i, j, k);
             const double dg = M.dt * A.c, da = M.dt * A.a, db = M.dt * A.b;
             if (M.ibm)
                 momentum_cell<true>(M.d, M.p, da, db, dg, M.un, M.vn, M.wn, M.pn, M.us, M.vs, M.ws, M.ou, M.ov, M.ow,
@@ -396,7 +413,7 @@ __global__ void __launch_bounds__(MAX_THREADS) k_ens_substage(ens_args A) {
 
     // ---- warm start: the previous or extrapolated increment ----
     if (warm) {
-        cell_tiles(A, [&](int m, const ens_member& M, long long t) {
+        cell_tiles(A, [&](int m, const ens_member& M, unsigned t) {
             const ens_state& S = A.st[m];
             if (!S.has_guess) return;
             const int cur = (S.flip >> s) & 1;
@@ -404,7 +421,7 @@ __global__ void __launch_bounds__(MAX_THREADS) k_ens_substage(ens_args A) {
             M.guess[t] = S.extrap ? 2.0 * h1 - M.h[s][cur ^ 1][t] : h1;
         });
         grid.sync();
-        cell_tiles(A, [&](int m, const ens_member& M, long long t) {
+        cell_tiles(A, [&](int m, const ens_member& M, unsigned t) {
             if (A.st[m].has_guess) guess_cell(M, dg_of(A, M), t);
         });
         grid.sync();
@@ -515,10 +532,10 @@ __global__ void __launch_bounds__(MAX_THREADS) k_ens_substage(ens_args A) {
         }
     grid.sync();
     if (warm) {
-        cell_tiles(A, [&](int m, const ens_member& M, long long t) {
+        cell_tiles(A, [&](int m, const ens_member& M, unsigned t) {
             const int cur = (A.st[m].flip >> s) & 1;
             int i, j, k;
-            cell_ijk(M.d, t, i, j, k);
+            cell_ijk(M, t, i, j, k);
             const long long c = pidx(M.d, i, j, k);
             M.h[s][cur][t] = M.pn[c] - M.p0[c];
         });
@@ -531,9 +548,10 @@ __global__ void __launch_bounds__(MAX_THREADS) k_ens_substage(ens_args A) {
         const ens_member& M = A.mem[T.x];
         const mdx_four f{M.un, M.vn, M.wn, M.pn};
         for (int e = threadIdx.x; e < ETILE; e += blockDim.x) {
-            const long long t = (long long)T.y + e;
-            if (t >= (long long)M.d.nx * M.d.nz) break;
-            bcrb_y_col(M.d, M.bc, M.p.dy, f, (int)(t % M.d.nx) + 1, (int)(t / M.d.nx) + 1);
+            const unsigned t = (unsigned)T.y + e;
+            if (t >= (unsigned)(M.d.nx * M.d.nz)) break;
+            const unsigned q = fq(t, M.fx);
+            bcrb_y_col(M.d, M.bc, M.p.dy, f, (int)(t - q * M.fx.d) + 1, (int)q + 1);
         }
     }
     grid.sync();
@@ -542,9 +560,10 @@ __global__ void __launch_bounds__(MAX_THREADS) k_ens_substage(ens_args A) {
         const ens_member& M = A.mem[T.x];
         const mdx_four f{M.un, M.vn, M.wn, M.pn};
         for (int e = threadIdx.x; e < ETILE; e += blockDim.x) {
-            const long long t = (long long)T.y + e;
-            if (t >= (long long)M.d.ny * M.d.nz) break;
-            bcrb_x_col(M.d, M.bc, M.p.dx, f, (int)(t % M.d.ny) + 1, (int)(t / M.d.ny) + 1);
+            const unsigned t = (unsigned)T.y + e;
+            if (t >= (unsigned)(M.d.ny * M.d.nz)) break;
+            const unsigned q = fq(t, M.fy);
+            bcrb_x_col(M.d, M.bc, M.p.dx, f, (int)(t - q * M.fy.d) + 1, (int)q + 1);
         }
     }
     grid.sync();
@@ -553,9 +572,10 @@ __global__ void __launch_bounds__(MAX_THREADS) k_ens_substage(ens_args A) {
         const ens_member& M = A.mem[T.x];
         const mdx_four f{M.un, M.vn, M.wn, M.pn};
         for (int e = threadIdx.x; e < ETILE; e += blockDim.x) {
-            const long long t = (long long)T.y + e;
-            if (t >= (long long)M.d.nx * M.d.ny) break;
-            bcrb_z_col(M.d, M.bc, M.p.dz, f, (int)(t % M.d.nx) + 1, (int)(t / M.d.nx) + 1);
+            const unsigned t = (unsigned)T.y + e;
+            if (t >= (unsigned)(M.d.nx * M.d.ny)) break;
+            const unsigned q = fq(t, M.fx);
+            bcrb_z_col(M.d, M.bc, M.p.dz, f, (int)(t - q * M.fx.d) + 1, (int)q + 1);
         }
     }
 }
@@ -566,8 +586,10 @@ __global__ void k_ens_ic(mdx_dims d, double dy, uint64_t seed, double amp_u, dou
                          double* __restrict__ wn) {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= d.nint) return;
-    int i, j, k;
-    cell_ijk(d, t, i, j, k);
+    const int i = (int)(t % d.nx) + 1;
+    const long long r = t / d.nx;
+    const int j = (int)(r % d.ny) + 1;
+    const int k = (int)(r / d.ny) + 1;
     const long long c = pidx(d, i, j, k);
     const double y = ((double)j - 0.5) * dy;
     const double e = y - yc[i - 1];
@@ -602,7 +624,7 @@ struct mdx_ensemble {
     std::vector<int> cell_begin;
     int* dcell_begin = nullptr;
     double* part = nullptr;
-    int threads = 256, blocks_per_sm = 0, grid = 0;
+    int threads = 256, blocks_per_sm = 0, grid = 0, variant = 0;
     bool use_graph = true, graph_ok = true;
     cudaGraphExec_t graph = nullptr;
     cudaEvent_t ev[2] = {nullptr, nullptr};
@@ -646,9 +668,13 @@ void free_graph(mdx_ensemble_t* E) {
     E->graph = nullptr;
 }
 
-int grid_for(mdx_ensemble_t* E, int threads, int bps, int* grid) {
+const void* kernel_of(int variant) {
+    return variant ? (const void*)k_ens_substage<2> : (const void*)k_ens_substage<1>;
+}
+
+int grid_for(mdx_ensemble_t* E, int variant, int threads, int bps, int* grid) {
     int occ = 0;
-    ENS_CUDA(E, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_ens_substage, threads, 0));
+    ENS_CUDA(E, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel_of(variant), threads, 0));
     int sms = 0;
     ENS_CUDA(E, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, E->device));
     if (occ < 1) return efail(E, MDX_ERR_ARG, "ensemble kernel does not fit %d threads per block", threads);
@@ -682,22 +708,22 @@ ens_args make_args(mdx_ensemble_t* E, int s, int momentum) {
     return A;
 }
 
-int launch_substage(mdx_ensemble_t* E, int s, int momentum, int threads, int grid) {
+int launch_substage(mdx_ensemble_t* E, int s, int momentum, int variant, int threads, int grid) {
     ens_args A = make_args(E, s, momentum);
     void* args[] = {&A};
-    ENS_CUDA(E, cudaLaunchCooperativeKernel((const void*)k_ens_substage, dim3(grid), dim3(threads), args, 0, E->stream));
+    ENS_CUDA(E, cudaLaunchCooperativeKernel(kernel_of(variant), dim3(grid), dim3(threads), args, 0, E->stream));
     E->launches++;
     return MDX_OK;
 }
 
-int step_eager(mdx_ensemble_t* E, int threads, int grid) {
-    for (int s = 0; s < 3; ++s) MDX_TRY(launch_substage(E, s, 1, threads, grid));
+int step_eager(mdx_ensemble_t* E, int variant, int threads, int grid) {
+    for (int s = 0; s < 3; ++s) MDX_TRY(launch_substage(E, s, 1, variant, threads, grid));
     return MDX_OK;
 }
 
 int ensure_grid(mdx_ensemble_t* E) {
     if (E->grid > 0) return MDX_OK;
-    return grid_for(E, E->threads, E->blocks_per_sm, &E->grid);
+    return grid_for(E, E->variant, E->threads, E->blocks_per_sm, &E->grid);
 }
 
 int read_stats(mdx_ensemble_t* E, std::vector<ens_state>& h) {
@@ -744,8 +770,8 @@ std::string tune_key(const mdx_ensemble_t* E) {
     return buf;
 }
 
-// The cache is a JSON object {"<key>": {"threads": T, "blocks_per_sm": B, "ms": M}, ...}.
-bool cache_lookup(const char* path, const std::string& key, int* threads, int* bps) {
+// The cache is a JSON object {"<key>": {"threads": T, "blocks_per_sm": B, "low_regs": R, "ms": M}, ...}.
+bool cache_lookup(const char* path, const std::string& key, int* threads, int* bps, int* low_regs) {
     if (!path) return false;
     FILE* f = fopen(path, "rb");
     if (!f) return false;
@@ -757,14 +783,16 @@ bool cache_lookup(const char* path, const std::string& key, int* threads, int* b
     const std::string q = "\"" + key + "\"";
     const size_t at = s.find(q);
     if (at == std::string::npos) return false;
-    const size_t t = s.find("\"threads\":", at), b = s.find("\"blocks_per_sm\":", at);
-    if (t == std::string::npos || b == std::string::npos) return false;
+    const size_t t = s.find("\"threads\":", at), b = s.find("\"blocks_per_sm\":", at),
+                 lr = s.find("\"low_regs\":", at);
+    if (t == std::string::npos || b == std::string::npos || lr == std::string::npos) return false;
     *threads = atoi(s.c_str() + t + 10);
     *bps = atoi(s.c_str() + b + 16);
+    *low_regs = atoi(s.c_str() + lr + 11);
     return *threads > 0 && *threads <= MAX_THREADS && *threads % 32 == 0 && *bps > 0;
 }
 
-void cache_store(const char* path, const std::string& key, int threads, int bps, double ms) {
+void cache_store(const char* path, const std::string& key, int threads, int bps, int low_regs, double ms) {
     if (!path) return;
     std::string s;
     if (FILE* f = fopen(path, "rb")) {
@@ -774,8 +802,8 @@ void cache_store(const char* path, const std::string& key, int threads, int bps,
         fclose(f);
     }
     char entry[512];
-    snprintf(entry, sizeof(entry), "\"%s\": {\"threads\": %d, \"blocks_per_sm\": %d, \"ms\": %.6f}", key.c_str(),
-             threads, bps, ms);
+    snprintf(entry, sizeof(entry), "\"%s\": {\"threads\": %d, \"blocks_per_sm\": %d, \"low_regs\": %d, \"ms\": %.6f}",
+             key.c_str(), threads, bps, low_regs, ms);
     const size_t close = s.rfind('}');
     if (s.empty() || close == std::string::npos || s.find('{') == std::string::npos) {
         s = std::string("{\n  ") + entry + "\n}\n";
@@ -915,6 +943,9 @@ int mdx_ensemble_create(int device, int n, const mdx_member_t* members, const md
         for (int t = 0; t < 3; ++t) M.bc.per[t] = bc.is_periodic[t] ? 1 : 0;
         for (int t = 0; t < 24; ++t) { M.bc.type[t] = bc.bc_type[t]; M.bc.value[t] = bc.bc_value[t]; }
         M.dt = q.dt;
+        M.fx = make_fdiv((unsigned)q.nx);
+        M.fy = make_fdiv((unsigned)q.ny);
+        M.fh = make_fdiv((unsigned)(q.nx / 2));
         const size_t np = (size_t)d.npad, ni = (size_t)d.nint, pl = (size_t)d.nxp * d.nyp;
         double** pads[7] = {&M.un, &M.vn, &M.wn, &M.pn, &M.us, &M.vs, &M.ws};
         for (int t = 0; t < 7 && rc == MDX_OK; ++t) rc = ealloc(E, pads[t], np, true, t < 4);
@@ -1033,7 +1064,7 @@ int mdx_ensemble_ic(mdx_ensemble_t* E) {
     std::vector<ens_state> hs(E->n);
     std::memset(hs.data(), 0, sizeof(ens_state) * E->n);
     ENS_CUDA(E, cudaMemcpyAsync(E->dst, hs.data(), sizeof(ens_state) * E->n, cudaMemcpyHostToDevice, E->stream));
-    MDX_TRY(launch_substage(E, 0, 0, E->threads, E->grid));   // the t=0 projection, dt_gamma = 1
+    MDX_TRY(launch_substage(E, 0, 0, E->variant, E->threads, E->grid));   // the t=0 projection, dt_gamma = 1
     for (int m = 0; m < E->n; ++m)
         ENS_CUDA(E, cudaMemsetAsync(E->hm[m].pn, 0, sizeof(double) * E->hm[m].d.npad, E->stream));
     std::vector<ens_state> after;
@@ -1050,12 +1081,14 @@ int mdx_ensemble_ic(mdx_ensemble_t* E) {
     return MDX_OK;
 }
 
-int mdx_ensemble_config(mdx_ensemble_t* E, int threads, int blocks_per_sm) {
+int mdx_ensemble_config(mdx_ensemble_t* E, int threads, int blocks_per_sm, int low_regs) {
     if (!E) return MDX_ERR_ARG;
+    const int variant = low_regs ? 1 : 0;
     if (threads < 32 || threads > MAX_THREADS || threads % 32)
         return efail(E, MDX_ERR_ARG, "threads per block must be a multiple of 32 up to %d", MAX_THREADS);
     int grid = 0;
-    MDX_TRY(grid_for(E, threads, blocks_per_sm, &grid));
+    MDX_TRY(grid_for(E, variant, threads, blocks_per_sm, &grid));
+    E->variant = variant;
     E->threads = threads;
     E->blocks_per_sm = blocks_per_sm;
     E->grid = grid;
@@ -1083,7 +1116,7 @@ int mdx_ensemble_step(mdx_ensemble_t* E, int nsteps, long long* total_iters) {
             cudaGraph_t g = nullptr;
             ENS_CUDA(E, cudaStreamBeginCapture(E->stream, cudaStreamCaptureModeThreadLocal));
             const long long l0 = E->launches;
-            int rc = step_eager(E, E->threads, E->grid);
+            int rc = step_eager(E, E->variant, E->threads, E->grid);
             E->launches = l0;
             cudaError_t e = cudaStreamEndCapture(E->stream, &g);
             if (rc != MDX_OK || e != cudaSuccess || !g || cudaGraphInstantiate(&E->graph, g, 0) != cudaSuccess) {
@@ -1097,7 +1130,7 @@ int mdx_ensemble_step(mdx_ensemble_t* E, int nsteps, long long* total_iters) {
             ENS_CUDA(E, cudaGraphLaunch(E->graph, E->stream));
             E->launches += 3;
         } else {
-            MDX_TRY(step_eager(E, E->threads, E->grid));
+            MDX_TRY(step_eager(E, E->variant, E->threads, E->grid));
         }
     }
     ENS_CUDA(E, cudaEventRecord(E->ev[1], E->stream));
@@ -1159,58 +1192,64 @@ int mdx_ensemble_set(mdx_ensemble_t* E, int m, int field, const double* host) {
     return MDX_OK;
 }
 
-int mdx_ensemble_tune(mdx_ensemble_t* E, const char* cache_path, int* threads_out, int* bps_out, double* ms_out) {
+int mdx_ensemble_tune(mdx_ensemble_t* E, const char* cache_path, int* threads_out, int* bps_out, int* low_regs_out,
+                      double* ms_out) {
     if (!E) return MDX_ERR_ARG;
     ENS_CUDA(E, cudaSetDevice(E->device));
     const std::string key = tune_key(E);
-    int t = 0, b = 0;
-    if (cache_lookup(cache_path, key, &t, &b) && mdx_ensemble_config(E, t, b) == MDX_OK) {
+    int t = 0, b = 0, lr = 0;
+    if (cache_lookup(cache_path, key, &t, &b, &lr) && mdx_ensemble_config(E, t, b, lr) == MDX_OK) {
         if (threads_out) *threads_out = t;
         if (bps_out) *bps_out = b;
+        if (low_regs_out) *low_regs_out = lr;
         if (ms_out) *ms_out = -1.0;
         return MDX_OK;
     }
     // time one step of each candidate from the same saved state
     MDX_TRY(snapshot(E, false));
     const int cand_t[3] = {128, 256, 512};
-    const int cand_b[3] = {1, 2, 4};
+    const int cand_b[4] = {1, 2, 4, 8};
     double best = 1e300;
-    int bt = E->threads, bb = E->blocks_per_sm;
-    for (int ti = 0; ti < 3; ++ti) {
-        int occ = 0;
-        ENS_CUDA(E, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_ens_substage, cand_t[ti], 0));
-        for (int bi = 0; bi < 3; ++bi) {
-            if (cand_b[bi] > occ) continue;
-            int grid = 0;
-            MDX_TRY(grid_for(E, cand_t[ti], cand_b[bi], &grid));
-            MDX_TRY(snapshot(E, true));
-            ENS_CUDA(E, cudaEventRecord(E->ev[0], E->stream));
-            MDX_TRY(step_eager(E, cand_t[ti], grid));
-            ENS_CUDA(E, cudaEventRecord(E->ev[1], E->stream));
-            ENS_CUDA(E, cudaEventSynchronize(E->ev[1]));
-            float ms = 0.f;
-            ENS_CUDA(E, cudaEventElapsedTime(&ms, E->ev[0], E->ev[1]));
-            if (ms < best) {
-                best = ms;
-                bt = cand_t[ti];
-                bb = cand_b[bi];
+    int bt = E->threads, bb = E->blocks_per_sm, bv = E->variant;
+    for (int v = 0; v < 2; ++v)
+        for (int ti = 0; ti < 3; ++ti) {
+            int occ = 0;
+            ENS_CUDA(E, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel_of(v), cand_t[ti], 0));
+            for (int bi = 0; bi < 4; ++bi) {
+                if (cand_b[bi] > occ) continue;
+                int grid = 0;
+                MDX_TRY(grid_for(E, v, cand_t[ti], cand_b[bi], &grid));
+                MDX_TRY(snapshot(E, true));
+                ENS_CUDA(E, cudaEventRecord(E->ev[0], E->stream));
+                MDX_TRY(step_eager(E, v, cand_t[ti], grid));
+                ENS_CUDA(E, cudaEventRecord(E->ev[1], E->stream));
+                ENS_CUDA(E, cudaEventSynchronize(E->ev[1]));
+                float ms = 0.f;
+                ENS_CUDA(E, cudaEventElapsedTime(&ms, E->ev[0], E->ev[1]));
+                if (ms < best) {
+                    best = ms;
+                    bt = cand_t[ti];
+                    bb = cand_b[bi];
+                    bv = v;
+                }
             }
         }
-    }
     MDX_TRY(snapshot(E, true));
     ENS_CUDA(E, cudaStreamSynchronize(E->stream));
-    MDX_TRY(mdx_ensemble_config(E, bt, bb));
-    cache_store(cache_path, key, bt, bb, best);
+    MDX_TRY(mdx_ensemble_config(E, bt, bb, bv));
+    cache_store(cache_path, key, bt, bb, bv, best);
     if (threads_out) *threads_out = bt;
     if (bps_out) *bps_out = bb;
+    if (low_regs_out) *low_regs_out = bv;
     if (ms_out) *ms_out = best;
     return MDX_OK;
 }
 
-int mdx_ensemble_info(mdx_ensemble_t* E, int* threads, int* grid, int* graph, double* last_step_ms,
+int mdx_ensemble_info(mdx_ensemble_t* E, int* threads, int* grid, int* low_regs, int* graph, double* last_step_ms,
                       long long* launches) {
     if (!E) return MDX_ERR_ARG;
     MDX_TRY(ensure_grid(E));
+    if (low_regs) *low_regs = E->variant;
     if (threads) *threads = E->threads;
     if (grid) *grid = E->grid;
     if (graph) *graph = E->graph ? 1 : 0;
