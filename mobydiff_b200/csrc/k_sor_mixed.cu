@@ -30,6 +30,22 @@ struct mixed_params {
     float idx, idy, idz, idt;
 };
 
+// Colour-split layout of the FP32 arrays (du, dv, dw, dp, r): element
+// (i, j, k) of the padded grid lives in half (i + j + k) & 1 at
+// (k (ny+2) + j) (nx+2)/2 + i/2, so the cells of one colour in a row -- and
+// the faces they own or share -- are consecutive: every access of a colour
+// sweep is unit-stride.  A face belongs to the cell on its high side
+// (u(i) to cell i).  nx is even, so (nx+2)/2 is whole.
+__device__ __forceinline__ long long cidx(const mdx_dims& d, int i, int j, int k) {
+    const int hx = d.nxp >> 1;
+    return ((i + j + k) & 1) * ((long long)hx * d.nyp * d.nzp) + ((long long)k * d.nyp + j) * hx + (i >> 1);
+}
+// (i, j) planes of the IBM factors and sweep factors split by the parity of i.
+__device__ __forceinline__ int pidx2(const mdx_dims& d, int i, int j) {
+    const int hx = d.nxp >> 1;
+    return (i & 1) * (hx * d.nyp) + j * hx + (i >> 1);
+}
+
 __device__ inline double nanmax2(double a, double b) { return (a != a || b != b) ? (a + b) : fmax(a, b); }
 
 __device__ inline void block_reduce3(double& s, double& m, double& u) {
@@ -74,7 +90,7 @@ k_mixed_residual(mdx_dims d, double idx, double idy, double idz, const double* _
         const double uc = __ldg(u + c), vc = __ldg(v + c), wc = __ldg(w + c);
         const double dv = (__ldg(u + pidx(d, ip, j, k)) - uc) * idx + (__ldg(v + pidx(d, i, jp, k)) - vc) * idy +
                           (__ldg(w + pidx(d, i, j, kp)) - wc) * idz;
-        r[c] = (float)dv;
+        r[cidx(d, i, j, k)] = (float)dv;
         s += dv * dv;
         m = nanmax2(m, fabs(dv));
         um = nanmax2(um, nanmax2(fabs(uc), nanmax2(fabs(vc), fabs(wc))));
@@ -101,10 +117,10 @@ k_mixed_corr_residual(mdx_dims d, mixed_params P, const float* __restrict__ du, 
         const int ip = i == d.nx ? 1 : i + 1;
         const int jp = (PY && j == d.ny) ? 1 : j + 1;
         const int kp = k == d.nz ? 1 : k + 1;
-        const long long c = pidx(d, i, j, k);
-        const float e = __ldg(r + c) + (__ldg(du + pidx(d, ip, j, k)) - __ldg(du + c)) * P.idx +
-                        (__ldg(dv + pidx(d, i, jp, k)) - __ldg(dv + c)) * P.idy +
-                        (__ldg(dw + pidx(d, i, j, kp)) - __ldg(dw + c)) * P.idz;
+        const long long c = cidx(d, i, j, k);
+        const float e = __ldg(r + c) + (__ldg(du + cidx(d, ip, j, k)) - __ldg(du + c)) * P.idx +
+                        (__ldg(dv + cidx(d, i, jp, k)) - __ldg(dv + c)) * P.idy +
+                        (__ldg(dw + cidx(d, i, j, kp)) - __ldg(dw + c)) * P.idz;
         s += (double)e * (double)e;
         m = nanmax2(m, fabs((double)e));
     }
@@ -130,9 +146,10 @@ __global__ void k_mixed_tables(mdx_dims d, int py, double idx2, double idy2, dou
             mu_v = mu[np + t];
             mu_w = mu[2 * np + t];
         }
-        mu32[t] = (float)mu_u;
-        mu32[np + t] = (float)mu_v;
-        mu32[2 * np + t] = (float)mu_w;
+        const int o = pidx2(d, i, j);
+        mu32[o] = (float)mu_u;
+        mu32[np + o] = (float)mu_v;
+        mu32[2 * np + o] = (float)mu_w;
         double f = 0.0;
         if (i >= 1 && i <= d.nx && j >= 1 && j <= d.ny) {
             const int ip = i == d.nx ? 1 : i + 1;
@@ -145,11 +162,12 @@ __global__ void k_mixed_tables(mdx_dims d, int py, double idx2, double idy2, dou
             const double denom = (mu_u + mu_uip) * idx2 + (mu_w + mu_w) * idz2 + (mu_v + mu_vjp) * idy2;
             f = -sor / denom;
         }
-        fac32[t] = (float)f;
+        fac32[o] = (float)f;
     }
 }
 
-// One FP32 colour sweep of the correction (periodic x and z).
+// One FP32 colour sweep of the correction (periodic x and z), on the
+// colour-split arrays.
 template <int PY>
 __global__ void __launch_bounds__(256)
 k_sor_sweep32(mdx_dims d, mixed_params P, int parity, int reverse, float* __restrict__ du, float* __restrict__ dv,
@@ -165,40 +183,42 @@ k_sor_sweep32(mdx_dims d, mixed_params P, int parity, int reverse, float* __rest
     const int kp = (k == nz) ? 1 : k + 1;
     const int i = 1 + ((j + k + parity) & 1) + 2 * (ni - 1);
     const int ip = (i == nx) ? 1 : i + 1;
-    const long long plane = (long long)d.nxp * d.nyp;
-    const int q = i + d.nxp * j, qip = ip + d.nxp * j, qjp = i + d.nxp * jp;
-    float* U = du + k * plane;
-    float* V = dv + k * plane;
-    float* W = dw + k * plane;
-    float* Wn = dw + kp * plane;
-    const float mu_u_i = __ldg(mu32 + q), mu_u_ip = __ldg(mu32 + qip);
-    const float mu_v_j = __ldg(mu32 + plane + q), mu_v_jp = __ldg(mu32 + plane + qjp);
-    const float mu_w = __ldg(mu32 + 2 * plane + q);
-    const float u_i = U[q], u_ip = U[qip], v_j = V[q], v_jp = V[qjp], w_k = W[q], w_kp = Wn[q];
-    const float div = __ldg(r + k * plane + q) + (u_ip - u_i) * P.idx + (v_jp - v_j) * P.idy + (w_kp - w_k) * P.idz;
+    const int np = d.nxp * d.nyp;
+    const int q = pidx2(d, i, j);
+    const long long c = cidx(d, i, j, k), cip = cidx(d, ip, j, k), cjp = cidx(d, i, jp, k), ckp = cidx(d, i, j, kp);
+    const float mu_u_i = __ldg(mu32 + q), mu_u_ip = __ldg(mu32 + pidx2(d, ip, j));
+    const float mu_v_j = __ldg(mu32 + np + q), mu_v_jp = __ldg(mu32 + np + pidx2(d, i, jp));
+    const float mu_w = __ldg(mu32 + 2 * np + q);
+    const float u_i = du[c], u_ip = du[cip], v_j = dv[c], v_jp = dv[cjp], w_k = dw[c], w_kp = dw[ckp];
+    const float div = __ldg(r + c) + (u_ip - u_i) * P.idx + (v_jp - v_j) * P.idy + (w_kp - w_k) * P.idz;
     const float phi = div * __ldg(fac32 + q);
-    dp[k * plane + q] += phi * P.idt;
-    U[q] = u_i - phi * P.idx * mu_u_i;
-    U[qip] = u_ip + phi * P.idx * mu_u_ip;
-    if (PY || j > 1) V[q] = v_j - phi * P.idy * mu_v_j;         // wall face v(1) stays 0
-    if (PY || j < ny) V[qjp] = v_jp + phi * P.idy * mu_v_jp;    // wall face v(ny+1) stays 0
-    W[q] = w_k - phi * P.idz * mu_w;
-    Wn[q] = w_kp + phi * P.idz * mu_w;
+    dp[c] += phi * P.idt;
+    du[c] = u_i - phi * P.idx * mu_u_i;
+    du[cip] = u_ip + phi * P.idx * mu_u_ip;
+    if (PY || j > 1) dv[c] = v_j - phi * P.idy * mu_v_j;         // wall face v(1) stays 0
+    if (PY || j < ny) dv[cjp] = v_jp + phi * P.idy * mu_v_jp;    // wall face v(ny+1) stays 0
+    dw[c] = w_k - phi * P.idz * mu_w;
+    dw[ckp] = w_kp + phi * P.idz * mu_w;
 }
 
 // u += du, v += dv, w += dw, p += dp over the padded arrays; corrections reset.
-__global__ void k_mixed_apply(long long n, double* __restrict__ u, double* __restrict__ v, double* __restrict__ w,
+__global__ void k_mixed_apply(mdx_dims d, double* __restrict__ u, double* __restrict__ v, double* __restrict__ w,
                               double* __restrict__ p, float* __restrict__ du, float* __restrict__ dv,
                               float* __restrict__ dw, float* __restrict__ dp) {
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-        u[t] += (double)du[t];
-        v[t] += (double)dv[t];
-        w[t] += (double)dw[t];
-        p[t] += (double)dp[t];
-        du[t] = 0.f;
-        dv[t] = 0.f;
-        dw[t] = 0.f;
-        dp[t] = 0.f;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < d.npad; t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % d.nxp);
+        const long long rr = t / d.nxp;
+        const int j = (int)(rr % d.nyp);
+        const int k = (int)(rr / d.nyp);
+        const long long c = cidx(d, i, j, k);
+        u[t] += (double)du[c];
+        v[t] += (double)dv[c];
+        w[t] += (double)dw[c];
+        p[t] += (double)dp[c];
+        du[c] = 0.f;
+        dv[c] = 0.f;
+        dw[c] = 0.f;
+        dp[c] = 0.f;
     }
 }
 
@@ -328,7 +348,7 @@ int mdx_k_projection_redblack_mixed(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t
             }
             const long long n = d.npad;
             MDX_LAUNCH(ctx, MDX_T_OTHER, "mixed apply", k_mixed_apply, (int)std::min<long long>((n + 255) / 256, 8192),
-                       256, 0, n, f[MDX_UN], f[MDX_VN], f[MDX_WN], f[MDX_PN], ctx->mx_du, ctx->mx_dv, ctx->mx_dw,
+                       256, 0, d, f[MDX_UN], f[MDX_VN], f[MDX_WN], f[MDX_PN], ctx->mx_du, ctx->mx_dv, ctx->mx_dw,
                        ctx->mx_dp);
             MDX_TRY(residual(&r, nullptr));
             if (!std::isfinite(r)) { s.status = MDX_ERR_NONFINITE; break; }

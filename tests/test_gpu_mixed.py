@@ -93,3 +93,4 @@ def test_mixed_falls_back_to_fp64_for_other_boundaries():
         assert stm.variant < 100 and stm.iterations == stp.iterations
         for n in ("un", "vn", "wn", "pn"):
             assert np.array_equal(sm.get(n), sp.get(n)), n
+
