@@ -177,6 +177,7 @@ typedef struct {
     int ibm;             /* -1 none, 0 reference bump (ibm.f90:45-50), 1 wavy channel */
     double ibm_amp, ibm_lambda, ibm_y0, ibm_height;
     int warnings;        /* number of warnings printed */
+    int guess;           /* red-black warm start: MDX_GUESS_ZERO / _PREVIOUS / _EXTRAPOLATED */
 } mdx_run_config_t;
 int mdx_read_runtime_config(const char* path, mdx_grid_t* g, mdx_bc_t* bc, mdx_solver_opts_t* opts,
                             mdx_run_config_t* run);

@@ -118,7 +118,7 @@ class RunConfigT(C.Structure):
                 ("output_prefix", C.c_char * 256), ("field_prefix", C.c_char * 256),
                 ("ic", C.c_int), ("seed", C.c_uint64), ("ibm", C.c_int),
                 ("ibm_amp", C.c_double), ("ibm_lambda", C.c_double), ("ibm_y0", C.c_double),
-                ("ibm_height", C.c_double), ("warnings", C.c_int)]
+                ("ibm_height", C.c_double), ("warnings", C.c_int), ("guess", C.c_int)]
 
 
 class IbmGeomT(C.Structure):

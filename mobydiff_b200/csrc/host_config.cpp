@@ -192,6 +192,11 @@ struct Reader {
             if (v == "fp64" || v == "double" || v == "0") o->precision = MDX_PREC_FP64;
             else if (v == "mixed" || v == "1") o->precision = MDX_PREC_MIXED;
             else warn("b200 precision must be fp64 or mixed", line);
+        } else if (run && (key == "guess" || key == "warm_start")) {
+            if (v == "zero" || v == "0") run->guess = MDX_GUESS_ZERO;
+            else if (v == "previous" || v == "1") run->guess = MDX_GUESS_PREVIOUS;
+            else if (v == "extrapolated" || v == "3") run->guess = MDX_GUESS_EXTRAPOLATED;
+            else warn("b200 guess must be zero, previous or extrapolated", line);
         } else if (run && key == "ic") {
             if (v == "zero" || v == "0") run->ic = 0;
             else if (v == "channel" || v == "1") run->ic = 1;

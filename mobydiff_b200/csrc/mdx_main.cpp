@@ -81,6 +81,7 @@ int main(int argc, char** argv) {
 
     std::printf(" initialising pressure solver...\n");
     CHECK(ctx, mdx_init_pressure_solver(ctx, &opts));
+    if (run.guess != MDX_GUESS_ZERO) CHECK(ctx, mdx_set_pressure_guess(ctx, run.guess, 1));
 
     std::printf(" initialising IBM...\n");
     const size_t npad = (size_t)(g.nx + 2) * (g.ny + 2) * (g.nz + 2);

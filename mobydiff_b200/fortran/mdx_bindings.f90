@@ -150,6 +150,61 @@ module mdx_bindings
             type(C_PTR), value :: ctx, uc, vc, wc
             integer(C_INT) :: rc
         end function
+        ! warm starts and the learned warm start (no counterpart in the reference)
+        function mdx_set_pressure_guess(ctx, mode, record) bind(C, name="mdx_set_pressure_guess") result(rc)
+            import :: C_INT, C_PTR
+            type(C_PTR), value :: ctx
+            integer(C_INT), value :: mode, record
+            integer(C_INT) :: rc
+        end function
+        function mdx_unet_create(ctx, opts) bind(C, name="mdx_unet_create") result(rc)
+            import :: C_INT, C_PTR
+            type(C_PTR), value :: ctx, opts     ! NULL: default options
+            integer(C_INT) :: rc
+        end function
+        function mdx_unet_record(ctx, on) bind(C, name="mdx_unet_record") result(rc)
+            import :: C_INT, C_PTR
+            type(C_PTR), value :: ctx
+            integer(C_INT), value :: on
+            integer(C_INT) :: rc
+        end function
+        function mdx_unet_train(ctx, iters, lr, loss_first, loss_last) bind(C, name="mdx_unet_train") result(rc)
+            import :: C_INT, C_PTR, C_DOUBLE
+            type(C_PTR), value :: ctx
+            integer(C_INT), value :: iters
+            real(C_DOUBLE), value :: lr
+            real(C_DOUBLE), intent(out) :: loss_first, loss_last
+            integer(C_INT) :: rc
+        end function
+        function mdx_unet_param_count(ctx) bind(C, name="mdx_unet_param_count") result(n)
+            import :: C_PTR, C_LONG_LONG
+            type(C_PTR), value :: ctx
+            integer(C_LONG_LONG) :: n
+        end function
+        function mdx_unet_get_params(ctx, host, n) bind(C, name="mdx_unet_get_params") result(rc)
+            import :: C_INT, C_PTR, C_LONG_LONG
+            type(C_PTR), value :: ctx, host
+            integer(C_LONG_LONG), value :: n
+            integer(C_INT) :: rc
+        end function
+        function mdx_unet_set_params(ctx, host, n) bind(C, name="mdx_unet_set_params") result(rc)
+            import :: C_INT, C_PTR, C_LONG_LONG
+            type(C_PTR), value :: ctx, host
+            integer(C_LONG_LONG), value :: n
+            integer(C_INT) :: rc
+        end function
+        function mdx_unet_get_out_scale(ctx, scale) bind(C, name="mdx_unet_get_out_scale") result(rc)
+            import :: C_INT, C_PTR, C_DOUBLE
+            type(C_PTR), value :: ctx
+            real(C_DOUBLE), intent(out) :: scale
+            integer(C_INT) :: rc
+        end function
+        function mdx_unet_set_out_scale(ctx, scale) bind(C, name="mdx_unet_set_out_scale") result(rc)
+            import :: C_INT, C_PTR, C_DOUBLE
+            type(C_PTR), value :: ctx
+            real(C_DOUBLE), value :: scale
+            integer(C_INT) :: rc
+        end function
     end interface
 
 contains
