@@ -93,6 +93,8 @@ struct ens_args {
     int nmem;
     ens_list cell, half, pad, plane, bcy, bcx, bcz;
     const int* cell_begin;           // [nmem + 1]: each member's range of cell tiles
+    const int* half_begin;           // [nmem + 1]: each member's range of sweep tiles
+    int* act;                        // [2 (nmem + 1)]: prefix sums of the active members' sweep, then cell tiles
     double* part;                    // 3 doubles per cell tile
     double a, b, c;                  // RK3 coefficients of this substage
     int substage;
@@ -141,40 +143,90 @@ __device__ __forceinline__ double dg_of(const ens_args& A, const ens_member& M) 
     return A.momentum ? M.dt * A.c : 1.0;
 }
 
-// Per-tile partials of sum div^2, max|div|, max(|u|,|v|,|w|) for the members
-// selected by `want` (the divergence of k_div_partials).
+// Prefix sums of the sweep and cell tiles of the members still active (one
+// thread); a converged member's range is empty, so the sweeps and residual
+// checks visit only live tiles however many members have finished.
+__device__ void compact_active(const ens_args& A) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    int h = 0, c = 0;
+    int* ah = A.act;
+    int* ac = A.act + A.nmem + 1;
+    for (int m = 0; m < A.nmem; ++m) {
+        ah[m] = h;
+        ac[m] = c;
+        if (A.st[m].active) {
+            h += A.half_begin[m + 1] - A.half_begin[m];
+            c += A.cell_begin[m + 1] - A.cell_begin[m];
+        }
+    }
+    ah[A.nmem] = h;
+    ac[A.nmem] = c;
+}
+
+// Virtual tile vt of a compacted prefix -> (member, tile of that member's range).
+__device__ __forceinline__ int2 active_tile(const int* pref, const int* begin, int nmem, int vt) {
+    int lo = 0, hi = nmem;   // pref[lo] <= vt < pref[hi]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (pref[mid] <= vt) lo = mid;
+        else hi = mid;
+    }
+    return make_int2(lo, begin[lo] + (vt - pref[lo]));
+}
+
+// Partials of sum div^2, max|div|, max(|u|,|v|,|w|) of cell tile ti (the
+// divergence of k_div_partials) into part[3 ti ..].
+__device__ void residual_tile(const ens_args& A, int ti) {
+    const int2 T = A.cell.t[ti];
+    const ens_member& M = A.mem[T.x];
+    const mdx_dims d = M.d;
+    const double* __restrict__ un = M.un;
+    const double* __restrict__ vn = M.vn;
+    const double* __restrict__ wn = M.wn;
+    const double idx = M.idx, idy = M.idy, idz = M.idz;
+    const fdiv32 fx = M.fx, fy = M.fy;
+    double s = 0.0, m = 0.0, um = 0.0;
+    for (int e = threadIdx.x; e < ETILE; e += blockDim.x) {
+        const unsigned t = (unsigned)T.y + e;
+        if (t >= (unsigned)d.nint) break;
+        const unsigned r = fq(t, fx);
+        const int i = (int)(t - r * fx.d) + 1;
+        const unsigned kq = fq(r, fy);
+        const int j = (int)(r - kq * fy.d) + 1;
+        const int k = (int)kq + 1;
+        const int ip = i + 1 > d.nx ? 1 : i + 1;
+        const int jp = j + 1;   // walls in y: v(ny+1) is the wall face
+        const int kp = k + 1 > d.nz ? 1 : k + 1;
+        const long long c = pidx(d, i, j, k);
+        const double uc = un[c], vc = vn[c], wc = wn[c];
+        const double dv = (un[pidx(d, ip, j, k)] - uc) * idx + (vn[pidx(d, i, jp, k)] - vc) * idy +
+                          (wn[pidx(d, i, j, kp)] - wc) * idz;
+        s += dv * dv;
+        m = nanmax(m, fabs(dv));
+        um = nanmax(um, nanmax(fabs(uc), nanmax(fabs(vc), fabs(wc))));
+    }
+    block_reduce3(s, m, um);
+    if (threadIdx.x == 0) {
+        A.part[3 * ti] = s;
+        A.part[3 * ti + 1] = m;
+        A.part[3 * ti + 2] = um;
+    }
+    __syncthreads();
+}
+
+// Residual partials of the members selected by `want`.
 template <typename Want>
 __device__ void residual_tiles(const ens_args& A, Want want) {
-    for (int ti = blockIdx.x; ti < A.cell.n; ti += gridDim.x) {
-        const int2 T = A.cell.t[ti];
-        if (!want(T.x)) continue;   // uniform per block
-        const ens_member& M = A.mem[T.x];
-        const mdx_dims& d = M.d;
-        double s = 0.0, m = 0.0, um = 0.0;
-        for (int e = threadIdx.x; e < ETILE; e += blockDim.x) {
-            const unsigned t = (unsigned)T.y + e;
-            if (t >= (unsigned)d.nint) break;
-            int i, j, k;
-            cell_ijk(M, t, i, j, k);
-            const int ip = i + 1 > d.nx ? 1 : i + 1;
-            const int jp = (M.bc.per[1] && j + 1 > d.ny) ? 1 : j + 1;
-            const int kp = k + 1 > d.nz ? 1 : k + 1;
-            const long long c = pidx(d, i, j, k);
-            const double uc = M.un[c], vc = M.vn[c], wc = M.wn[c];
-            const double dv = (M.un[pidx(d, ip, j, k)] - uc) * M.idx + (M.vn[pidx(d, i, jp, k)] - vc) * M.idy +
-                              (M.wn[pidx(d, i, j, kp)] - wc) * M.idz;
-            s += dv * dv;
-            m = nanmax(m, fabs(dv));
-            um = nanmax(um, nanmax(fabs(uc), nanmax(fabs(vc), fabs(wc))));
-        }
-        block_reduce3(s, m, um);
-        if (threadIdx.x == 0) {
-            A.part[3 * ti] = s;
-            A.part[3 * ti + 1] = m;
-            A.part[3 * ti + 2] = um;
-        }
-        __syncthreads();
-    }
+    for (int ti = blockIdx.x; ti < A.cell.n; ti += gridDim.x)
+        if (want(A.cell.t[ti].x)) residual_tile(A, ti);   // uniform per block
+}
+
+// Residual partials of the active members (compacted ranges).
+__device__ void residual_active(const ens_args& A) {
+    const int* pref = A.act + A.nmem + 1;
+    const int total = pref[A.nmem];
+    for (int vt = blockIdx.x; vt < total; vt += gridDim.x)
+        residual_tile(A, active_tile(pref, A.cell_begin, A.nmem, vt).y);
 }
 
 // Sum the tile partials of member m (block-wide, fixed order for a fixed
@@ -191,20 +243,44 @@ __device__ void member_sums(const ens_args& A, int m, double& s, double& um) {
     um = uu;
 }
 
-// One colour sweep of member M's cell at sweep element t (the generic
-// k_sor_sweep of k_sor.cu).
-__device__ __forceinline__ void sweep_cell(const ens_member& M, const mdx_sor_params& p, int parity, unsigned t) {
-    const mdx_dims& d = M.d;
-    const unsigned r = fq(t, M.fh);
-    const int ni = (int)(t - r * M.fh.d) + 1;
-    const unsigned q = fq(r, M.fy);
-    const int j = (int)(r - q * M.fy.d) + 1;
+// What a colour sweep of one member reads, copied to registers per tile so
+// that stores through the field pointers do not force reloads.
+struct sweep_view {
+    mdx_dims d;
+    double *un, *vn, *wn, *pn;
+    const double* mu;
+    int ibm;
+    fdiv32 fy, fh;
+};
+
+__device__ __forceinline__ sweep_view make_view(const ens_member& M) {
+    sweep_view v;
+    v.d = M.d;
+    v.un = M.un;
+    v.vn = M.vn;
+    v.wn = M.wn;
+    v.pn = M.pn;
+    v.mu = M.mu;
+    v.ibm = M.ibm;
+    v.fy = M.fy;
+    v.fh = M.fh;
+    return v;
+}
+
+// One colour sweep of a member's cell at sweep element t: the arithmetic of
+// k_sor_sweep_pxz (periodic x and z, walls in y; the wall rows read the
+// boundary values from bc).
+__device__ __forceinline__ void sweep_cell(const sweep_view& v, const mdx_bc_dev& bc, const mdx_sor_params& p,
+                                           int parity, unsigned t) {
+    const mdx_dims& d = v.d;
+    const unsigned r = fq(t, v.fh);
+    const int ni = (int)(t - r * v.fh.d) + 1;
+    const unsigned q = fq(r, v.fy);
+    const int j = (int)(r - q * v.fy.d) + 1;
     const int kk = (int)q + 1;
     const int nx = d.nx, ny = d.ny, nz = d.nz;
     const int k = parity ? nz + 1 - kk : kk;
-    const mdx_bc_dev& bc = M.bc;
-    int jp = j + 1;
-    if (bc.per[1] && jp > ny) jp = 1;
+    const int jp = j + 1;
     int kp = k + 1;
     if (kp > nz) kp = 1;
     const int i = 1 + ((j + k + parity) & 1) + 2 * (ni - 1);
@@ -212,25 +288,25 @@ __device__ __forceinline__ void sweep_cell(const ens_member& M, const mdx_sor_pa
     if (ip > nx) ip = 1;
     const long long c = pidx(d, i, j, k);
     const long long cip = pidx(d, ip, j, k), cjp = pidx(d, i, jp, k), ckp = pidx(d, i, j, kp);
-    double mu_u_i = 1.0, mu_u_ip = 1.0, mu_v_j = 1.0, mu_v_jp = 1.0, mu_w_k = 1.0, mu_w_kp = 1.0;
-    if (M.ibm) {
-        const double* mu = M.mu;
+    double mu_u_i = 1.0, mu_u_ip = 1.0, mu_v_j = 1.0, mu_v_jp = 1.0, mu_w = 1.0;
+    if (v.ibm) {
+        const double* mu = v.mu;
         const long long np = (long long)d.nxp * d.nyp;
-        const long long q = i + (long long)d.nxp * j;
-        mu_u_i = mu[q];
+        const long long qq = i + (long long)d.nxp * j;
+        mu_u_i = mu[qq];
         mu_u_ip = mu[ip + (long long)d.nxp * j];
-        mu_v_j = mu[np + q];
+        mu_v_j = mu[np + qq];
         mu_v_jp = mu[np + i + (long long)d.nxp * jp];
-        mu_w_k = mu[2 * np + q];
-        mu_w_kp = mu_w_k;
+        mu_w = mu[2 * np + qq];
     }
-    double* un = M.un;
-    double* vn = M.vn;
-    double* wn = M.wn;
-    double* pn = M.pn;
+    double* __restrict__ un = v.un;
+    double* __restrict__ vn = v.vn;
+    double* __restrict__ wn = v.wn;
+    double* __restrict__ pn = v.pn;
     double u_i = un[c], u_ip = un[cip], v_j = vn[c], v_jp = vn[cjp], w_k = wn[c], w_kp = wn[ckp], pc = pn[c];
-    sor_cell(u_i, u_ip, v_j, v_jp, w_k, w_kp, pc, mu_u_i, mu_u_ip, mu_v_j, mu_v_jp, mu_w_k, mu_w_kp, p, bc, i, j, k,
-             nx, ny, nz);
+    const double fac = sor_factor(mu_u_i, mu_u_ip, mu_v_j, mu_v_jp, mu_w, mu_w, p);
+    sor_cell_fac<1, 0, 1>(u_i, u_ip, v_j, v_jp, w_k, w_kp, pc, mu_u_i, mu_u_ip, mu_v_j, mu_v_jp, mu_w, mu_w, fac, p, bc,
+                          i, j, k, nx, ny, nz);
     un[c] = u_i;
     un[cip] = u_ip;
     vn[c] = v_j;
@@ -247,20 +323,30 @@ __device__ __forceinline__ mdx_sor_params proj_params(const ens_member& M, doubl
     return p;
 }
 
-template <typename Want>
-__device__ void sweep_tiles(const ens_args& A, int parity, Want want) {
-    for (int ti = blockIdx.x; ti < A.half.n; ti += gridDim.x) {
-        const int2 T = A.half.t[ti];
-        if (!want(T.x)) continue;
-        const ens_member& M = A.mem[T.x];
-        const unsigned nh = (unsigned)((M.d.nx / 2) * M.d.ny * M.d.nz);
-        const mdx_sor_params p = proj_params(M, dg_of(A, M));
-        for (int e = threadIdx.x; e < ETILE; e += blockDim.x) {
-            const unsigned t = (unsigned)T.y + e;
-            if (t >= nh) break;
-            sweep_cell(M, p, parity, t);
-        }
+__device__ __forceinline__ void sweep_tile(const ens_args& A, int parity, int ti) {
+    const int2 T = A.half.t[ti];
+    const ens_member& M = A.mem[T.x];
+    const sweep_view v = make_view(M);
+    const unsigned nh = (unsigned)((v.d.nx / 2) * v.d.ny * v.d.nz);
+    const mdx_sor_params p = proj_params(M, dg_of(A, M));
+    for (int e = threadIdx.x; e < ETILE; e += blockDim.x) {
+        const unsigned t = (unsigned)T.y + e;
+        if (t >= nh) break;
+        sweep_cell(v, M.bc, p, parity, t);
     }
+}
+
+// One colour sweep of every member.
+__device__ void sweep_all(const ens_args& A, int parity) {
+    for (int ti = blockIdx.x; ti < A.half.n; ti += gridDim.x) sweep_tile(A, parity, ti);
+}
+
+// One colour sweep of the active members (compacted ranges).
+__device__ void sweep_active(const ens_args& A, int parity) {
+    const int* pref = A.act;
+    const int total = pref[A.nmem];
+    for (int vt = blockIdx.x; vt < total; vt += gridDim.x)
+        sweep_tile(A, parity, active_tile(pref, A.half_begin, A.nmem, vt).y);
 }
 
 template <typename F>
@@ -327,21 +413,36 @@ __global__ void __launch_bounds__(MAX_THREADS, MINB) k_ens_substage(ens_args A) 
     const int s = A.substage;
     const bool warm = A.momentum && A.guess_mode != MDX_GUESS_ZERO;
     const bool meas = A.tol > 0.0;
-    __shared__ int any_sh;
 
     // ---- predictor (or u* = u for the t=0 projection) ----
     if (A.momentum) {
-        cell_tiles(A, [&](int, const ens_member& M, unsigned t) {
-            int i, j, k;
-            cell_ijk(M, t, i, j, k);
+        for (int ti = blockIdx.x; ti < A.cell.n; ti += gridDim.x) {
+            const int2 T = A.cell.t[ti];
+            const ens_member& M = A.mem[T.x];
+            const mdx_dims d = M.d;
+            const mdx_step_params p = M.p;
             const double dg = M.dt * A.c, da = M.dt * A.a, db = M.dt * A.b;
-            if (M.ibm)
-                momentum_cell<true>(M.d, M.p, da, db, dg, M.un, M.vn, M.wn, M.pn, M.us, M.vs, M.ws, M.ou, M.ov, M.ow,
-                                    M.cu, M.cv, M.cw, i + (long long)M.d.nxp * j, i, j, k);
-            else
-                momentum_cell<false>(M.d, M.p, da, db, dg, M.un, M.vn, M.wn, M.pn, M.us, M.vs, M.ws, M.ou, M.ov,
-                                     M.ow, M.cu, M.cv, M.cw, 0, i, j, k);
-        });
+            const fdiv32 fx = M.fx, fy = M.fy;
+            const double *un = M.un, *vn = M.vn, *wn = M.wn, *pn = M.pn;
+            double *us = M.us, *vs = M.vs, *ws = M.ws, *ou = M.ou, *ov = M.ov, *ow = M.ow;
+            const double *cu = M.cu, *cv = M.cv, *cw = M.cw;
+            const int ibm = M.ibm;
+            for (int e = threadIdx.x; e < ETILE; e += blockDim.x) {
+                const unsigned t = (unsigned)T.y + e;
+                if (t >= (unsigned)d.nint) break;
+                const unsigned r = fq(t, fx);
+                const int i = (int)(t - r * fx.d) + 1;
+                const unsigned kq = fq(r, fy);
+                const int j = (int)(r - kq * fy.d) + 1;
+                const int k = (int)kq + 1;
+                if (ibm)
+                    momentum_cell<true>(d, p, da, db, dg, un, vn, wn, pn, us, vs, ws, ou, ov, ow, cu, cv, cw,
+                                        i + (long long)d.nxp * j, i, j, k);
+                else
+                    momentum_cell<false>(d, p, da, db, dg, un, vn, wn, pn, us, vs, ws, ou, ov, ow, cu, cv, cw, 0, i,
+                                         j, k);
+            }
+        }
     } else {
         pad_tiles(A, [&](int, const ens_member& M, long long t) {
             M.us[t] = M.un[t];
@@ -467,29 +568,24 @@ __global__ void __launch_bounds__(MAX_THREADS, MINB) k_ens_substage(ens_args A) 
     if (!meas) {
         for (int it = 0; it < A.n_iter; ++it) {
             for (int parity = 0; parity < 2; ++parity) {
-                sweep_tiles(A, parity, [](int) { return true; });
+                sweep_all(A, parity);
                 grid.sync();
             }
         }
     } else {
+        compact_active(A);
+        grid.sync();
         int it = 0;
-        while (it < A.max_iter) {
-            // every block reads the same flags after the barrier
-            if (threadIdx.x == 0) {
-                int any = 0;
-                for (int m = 0; m < A.nmem; ++m) any |= A.st[m].active;
-                any_sh = any;
-            }
-            __syncthreads();
-            if (!any_sh) break;
+        // every block reads the same compacted prefix after the barrier
+        while (it < A.max_iter && A.act[A.nmem] > 0) {
             const int mm = min(A.check_every, A.max_iter - it);
             for (int q = 0; q < mm; ++q)
                 for (int parity = 0; parity < 2; ++parity) {
-                    sweep_tiles(A, parity, [&](int m) { return A.st[m].active != 0; });
+                    sweep_active(A, parity);
                     grid.sync();
                 }
             it += mm;
-            residual_tiles(A, [&](int m) { return A.st[m].active != 0; });
+            residual_active(A);
             grid.sync();
             for (int m = blockIdx.x; m < A.nmem; m += gridDim.x) {
                 if (!A.st[m].active) continue;
@@ -511,6 +607,8 @@ __global__ void __launch_bounds__(MAX_THREADS, MINB) k_ens_substage(ens_args A) 
                 }
                 __syncthreads();
             }
+            grid.sync();
+            compact_active(A);
             grid.sync();
         }
     }
@@ -621,8 +719,10 @@ struct mdx_ensemble {
     ens_state* dst = nullptr;
     std::vector<int2> tiles[7];
     int2* dtiles[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
-    std::vector<int> cell_begin;
+    std::vector<int> cell_begin, half_begin;
     int* dcell_begin = nullptr;
+    int* dhalf_begin = nullptr;
+    int* dact = nullptr;
     double* part = nullptr;
     int threads = 256, blocks_per_sm = 0, grid = 0, variant = 0;
     bool use_graph = true, graph_ok = true;
@@ -693,6 +793,8 @@ ens_args make_args(mdx_ensemble_t* E, int s, int momentum) {
     ens_list* L[7] = {&A.cell, &A.half, &A.pad, &A.plane, &A.bcy, &A.bcx, &A.bcz};
     for (int q = 0; q < 7; ++q) *L[q] = ens_list{E->dtiles[q], (int)E->tiles[q].size()};
     A.cell_begin = E->dcell_begin;
+    A.half_begin = E->dhalf_begin;
+    A.act = E->dact;
     A.part = E->part;
     A.a = a[s];
     A.b = b[s];
@@ -851,6 +953,8 @@ int mdx_ensemble_destroy(mdx_ensemble_t* E) {
     cudaFree(E->dm);
     cudaFree(E->dst);
     cudaFree(E->dcell_begin);
+    cudaFree(E->dhalf_begin);
+    cudaFree(E->dact);
     cudaFree(E->part);
     for (auto& e : E->ev)
         if (e) cudaEventDestroy(e);
@@ -989,15 +1093,18 @@ int mdx_ensemble_create(int device, int n, const mdx_member_t* members, const md
     if (rc != MDX_OK) return fail(rc);
     // tile lists, members back to back
     E->cell_begin.assign(n + 1, 0);
+    E->half_begin.assign(n + 1, 0);
     for (int m = 0; m < n; ++m) {
         const mdx_dims& d = E->hm[m].d;
         const long long cnt[7] = {d.nint, (long long)(d.nx / 2) * d.ny * d.nz, d.npad, (long long)d.nxp * d.nyp,
                                   (long long)d.nx * d.nz, (long long)d.ny * d.nz, (long long)d.nx * d.ny};
         E->cell_begin[m] = (int)E->tiles[0].size();
+        E->half_begin[m] = (int)E->tiles[1].size();
         for (int q = 0; q < 7; ++q)
             for (long long s0 = 0; s0 < cnt[q]; s0 += ETILE) E->tiles[q].push_back(make_int2(m, (int)s0));
     }
     E->cell_begin[n] = (int)E->tiles[0].size();
+    E->half_begin[n] = (int)E->tiles[1].size();
     for (int q = 0; q < 7 && rc == MDX_OK; ++q) {
         if (cudaMalloc(&E->dtiles[q], sizeof(int2) * std::max<size_t>(E->tiles[q].size(), 1)) != cudaSuccess ||
             cudaMemcpy(E->dtiles[q], E->tiles[q].data(), sizeof(int2) * E->tiles[q].size(), cudaMemcpyHostToDevice) !=
@@ -1007,6 +1114,10 @@ int mdx_ensemble_create(int device, int n, const mdx_member_t* members, const md
     if (rc == MDX_OK &&
         (cudaMalloc(&E->dcell_begin, sizeof(int) * (n + 1)) != cudaSuccess ||
          cudaMemcpy(E->dcell_begin, E->cell_begin.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice) != cudaSuccess ||
+         cudaMalloc(&E->dhalf_begin, sizeof(int) * (n + 1)) != cudaSuccess ||
+         cudaMemcpy(E->dhalf_begin, E->half_begin.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice) != cudaSuccess ||
+         cudaMalloc(&E->dact, sizeof(int) * 2 * (n + 1)) != cudaSuccess ||
+         cudaMemset(E->dact, 0, sizeof(int) * 2 * (n + 1)) != cudaSuccess ||
          cudaMalloc(&E->part, sizeof(double) * 3 * std::max<size_t>(E->tiles[0].size(), 1)) != cudaSuccess ||
          cudaMalloc(&E->dm, sizeof(ens_member) * n) != cudaSuccess ||
          cudaMemcpy(E->dm, E->hm.data(), sizeof(ens_member) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
