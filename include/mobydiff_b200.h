@@ -111,7 +111,9 @@ typedef struct {
     double residual0;   /* ||div u*||2                                       */
     double atol;        /* absolute floor used (red-black)                   */
     int variant;        /* red-black kernel variant of the last iterations;
-                           100 + n: mixed precision with n FP64 corrections */
+                           100 + n: mixed precision with n FP64 corrections;
+                           200 + n: FFT path in mixed precision, n FP64 passes
+                           (iterations = n as well) */
     int guessed;        /* 1 when a warm-start guess was applied             */
 } mdx_solve_stats_t;
 

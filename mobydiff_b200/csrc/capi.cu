@@ -445,12 +445,19 @@ int mdx_pressure_projection(mdx_ctx_t* ctx, double dt_gamma, mdx_solve_stats_t* 
     if (!(dt_gamma != 0.0)) return mdx_fail(ctx, MDX_ERR_ARG, "dt_gamma must be non-zero");
     if (ctx->opts.solver == MDX_SOLVER_FFT) {
         MDX_TRY(mdx_k_projection_fft(ctx, dt_gamma));
-        mdx_solve_stats_t s{};
-        ctx->last = s;
+        if (ctx->opts.precision != MDX_PREC_MIXED) {
+            mdx_solve_stats_t s{};
+            ctx->last = s;
+        }
         if (stats) {
             MDX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-            *stats = s;
+            *stats = ctx->last;
         }
+        if (ctx->last.status == MDX_ERR_NONFINITE)
+            return mdx_fail(ctx, MDX_ERR_NONFINITE, "non-finite divergence in the FFT defect correction");
+        if (ctx->last.status == MDX_NOT_CONVERGED)
+            return mdx_fail(ctx, MDX_NOT_CONVERGED, "FFT defect correction not converged after %d passes",
+                            ctx->last.iterations);
         return MDX_OK;
     }
     mdx_solve_stats_t s{};
@@ -501,6 +508,12 @@ static int rk_step_eager(mdx_ctx_t* ctx, double dt, long long* iters) {
         if (ctx->opts.solver == MDX_SOLVER_FFT) {
             MDX_TRY(mdx_k_apply_bc(ctx));
             MDX_TRY(mdx_k_projection_fft(ctx, dg));
+            if (ctx->opts.precision == MDX_PREC_MIXED) {
+                if (iters) *iters += ctx->last.iterations;
+                if (ctx->last.status != MDX_OK)
+                    return mdx_fail(ctx, ctx->last.status, "FFT defect correction ended with status %d",
+                                    ctx->last.status);
+            }
             MDX_TRY(mdx_k_apply_bc(ctx));
         } else {
             mdx_solve_stats_t st{};
@@ -541,7 +554,8 @@ int mdx_step(mdx_ctx_t* ctx, int nsteps, long long* total_iters) {
     if (nsteps < 0) return mdx_fail(ctx, MDX_ERR_ARG, "nsteps < 0");
     long long iters = 0;
     const double dt = ctx->g.dt;
-    const bool use_graph = ctx->opts.solver == MDX_SOLVER_FFT && !ctx->timing;
+    // the mixed FFT path decides its passes on the host: no graph
+    const bool use_graph = ctx->opts.solver == MDX_SOLVER_FFT && ctx->opts.precision == MDX_PREC_FP64 && !ctx->timing;
     if (use_graph && (!ctx->step_graph || ctx->graph_dt != dt)) MDX_TRY(capture_fft_step(ctx, dt));
     for (int n = 0; n < nsteps; ++n) {
         ctx->g.t_current = ctx->g.t_current + dt;   // src/main.f90:67

@@ -26,6 +26,7 @@
 // order only, so FFT-path fields agree to rounding.
 #include "mdx_internal.cuh"
 
+#include <algorithm>
 #include <cmath>
 
 // ---------------------------------------------------------------------------
@@ -60,45 +61,56 @@ void mdx_fft_twiddles(int n, std::vector<double2>& tw) {
 // ---------------------------------------------------------------------------
 // Device complex helpers
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
-    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+// Complex types of the FP64 path (double2) and of the FP32 inner solve of
+// the mixed-precision path (float2); one code for both.
+template <typename C2> struct cx;
+template <> struct cx<double2> {
+    typedef double R;
+    __device__ __forceinline__ static double2 mk(double a, double b) { return make_double2(a, b); }
+};
+template <> struct cx<float2> {
+    typedef float R;
+    __device__ __forceinline__ static float2 mk(float a, float b) { return make_float2(a, b); }
+};
+template <typename C2> __device__ __forceinline__ C2 cadd(C2 a, C2 b) { return cx<C2>::mk(a.x + b.x, a.y + b.y); }
+template <typename C2> __device__ __forceinline__ C2 csub(C2 a, C2 b) { return cx<C2>::mk(a.x - b.x, a.y - b.y); }
+template <typename C2> __device__ __forceinline__ C2 cmul(C2 a, C2 b) {
+    return cx<C2>::mk(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
-__device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+template <typename C2> __device__ __forceinline__ C2 cconj(C2 a) { return cx<C2>::mk(a.x, -a.y); }
 // a * (-i) and a * (+i)
-__device__ __forceinline__ double2 cmul_mi(double2 a) { return make_double2(a.y, -a.x); }
-__device__ __forceinline__ double2 cmul_pi(double2 a) { return make_double2(-a.y, a.x); }
+template <typename C2> __device__ __forceinline__ C2 cmul_mi(C2 a) { return cx<C2>::mk(a.y, -a.x); }
+template <typename C2> __device__ __forceinline__ C2 cmul_pi(C2 a) { return cx<C2>::mk(-a.y, a.x); }
 
 // Twiddle exp(-+2 pi i t / n) from the forward table (conjugated for INV).
-template <bool INV>
-__device__ __forceinline__ double2 twid(const double2* __restrict__ tw, int t) {
-    double2 w = __ldg(tw + t);
+template <bool INV, typename C2>
+__device__ __forceinline__ C2 twid(const C2* __restrict__ tw, int t) {
+    C2 w = __ldg(tw + t);
     if (INV) w.y = -w.y;
     return w;
 }
 
 // Radix-r DFT in registers.  For r = 3, 5, 7 the roots come from the table:
 // W_r^m = tw[m * (n/r) * tws].
-template <bool INV>
-__device__ __forceinline__ void dft_r(double2* a, int r, const double2* __restrict__ tw, int root_step) {
+template <bool INV, typename C2>
+__device__ __forceinline__ void dft_r(C2* a, int r, const C2* __restrict__ tw, int root_step) {
     if (r == 2) {
-        const double2 x0 = a[0], x1 = a[1];
+        const C2 x0 = a[0], x1 = a[1];
         a[0] = cadd(x0, x1);
         a[1] = csub(x0, x1);
     } else if (r == 4) {
-        const double2 x0 = a[0], x1 = a[1], x2 = a[2], x3 = a[3];
-        const double2 s02 = cadd(x0, x2), d02 = csub(x0, x2);
-        const double2 s13 = cadd(x1, x3), d13 = csub(x1, x3);
-        const double2 rd13 = INV ? cmul_pi(d13) : cmul_mi(d13);
+        const C2 x0 = a[0], x1 = a[1], x2 = a[2], x3 = a[3];
+        const C2 s02 = cadd(x0, x2), d02 = csub(x0, x2);
+        const C2 s13 = cadd(x1, x3), d13 = csub(x1, x3);
+        const C2 rd13 = INV ? cmul_pi(d13) : cmul_mi(d13);
         a[0] = cadd(s02, s13);
         a[1] = cadd(d02, rd13);
         a[2] = csub(s02, s13);
         a[3] = csub(d02, rd13);
     } else {
-        double2 b[7];
+        C2 b[7];
         for (int p = 0; p < r; ++p) {
-            double2 acc = a[0];
+            C2 acc = a[0];
             for (int q = 1; q < r; ++q) acc = cadd(acc, cmul(a[q], twid<INV>(tw, ((p * q) % r) * root_step)));
             b[p] = acc;
         }
@@ -110,9 +122,9 @@ __device__ __forceinline__ void dft_r(double2* a, int r, const double2* __restri
 // shared memory at A[line*ls + t]; all threads of the block participate.
 // `tw` is a table of exp(-2 pi i t / N) with N = n * tws.  Returns the
 // buffer holding the result (A or B).
-template <bool INV>
-__device__ double2* smem_fft(double2* A, double2* B, int n, int nlines, int ls, const mdx_fft_plan& pl,
-                             const double2* __restrict__ tw, int tws) {
+template <bool INV, typename C2>
+__device__ C2* smem_fft(C2* A, C2* B, int n, int nlines, int ls, const mdx_fft_plan& pl, const C2* __restrict__ tw,
+                        int tws) {
     int Ns = 1;
     for (int s = 0; s < pl.nstages; ++s) {
         const int r = pl.radix[s];
@@ -124,18 +136,18 @@ __device__ double2* smem_fft(double2* A, double2* B, int n, int nlines, int ls, 
             const int line = t / nr;
             const int jb = t - line * nr;
             const int k = jb % Ns;
-            const double2* src = A + line * ls;
-            double2 a[7];
+            const C2* src = A + line * ls;
+            C2 a[7];
             for (int q = 0; q < r; ++q) a[q] = src[jb + q * nr];
             if (Ns > 1)
                 for (int q = 1; q < r; ++q) a[q] = cmul(a[q], twid<INV>(tw, q * k * tstep));
             dft_r<INV>(a, r, tw, root_step);
-            double2* dst = B + line * ls;
+            C2* dst = B + line * ls;
             const int base = (jb / Ns) * Ns * r + k;
             for (int p = 0; p < r; ++p) dst[base + p * Ns] = a[p];
         }
         __syncthreads();
-        double2* t = A; A = B; B = t;
+        C2* t = A; A = B; B = t;
         Ns *= r;
     }
     return A;
@@ -146,20 +158,23 @@ __device__ double2* smem_fft(double2* A, double2* B, int n, int nlines, int ls, 
 // along x of each (k, j) row.  Rows are numbered r = (k-1) + nz*(j-1), the
 // order of plane_hat(nxh, nz, ny).  R rows per block, M = nx/2.
 // ---------------------------------------------------------------------------
+template <typename C2>
 __global__ void __launch_bounds__(256)
 k_div_fftx(mdx_dims d, int R, double dx, double dy, double dz, double dt_gamma, const double* __restrict__ us,
-           const double* __restrict__ vs, const double* __restrict__ ws, double2* __restrict__ spec,
-           mdx_fft_plan pl, const double2* __restrict__ twx) {
-    extern __shared__ double2 sm[];
+           const double* __restrict__ vs, const double* __restrict__ ws, C2* __restrict__ spec,
+           mdx_fft_plan pl, const C2* __restrict__ twx) {
+    typedef typename cx<C2>::R RT;
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    C2* sm = reinterpret_cast<C2*>(sm_raw);
     const int M = d.nx / 2;
-    double2* A = sm;
-    double2* B = sm + R * M;
+    C2* A = sm;
+    C2* B = sm + R * M;
     const int nrows = d.nz * d.ny;
     const int row0 = blockIdx.x * R;
     for (int t = threadIdx.x; t < R * M; t += blockDim.x) {
         const int rl = t / M, n = t - rl * M;
         const int row = row0 + rl;
-        double2 z = make_double2(0.0, 0.0);
+        C2 z = cx<C2>::mk(0, 0);
         if (row < nrows) {
             const int k = row % d.nz + 1, j = row / d.nz + 1;
             double x[2];
@@ -169,23 +184,24 @@ k_div_fftx(mdx_dims d, int R, double dx, double dy, double dz, double dt_gamma, 
                 x[e] = ((__ldg(us + c + 1) - __ldg(us + c)) / dx + (__ldg(vs + c + d.nxp) - __ldg(vs + c)) / dy +
                         (__ldg(ws + c + (long long)d.nxp * d.nyp) - __ldg(ws + c)) / dz) / dt_gamma;
             }
-            z = make_double2(x[0], x[1]);
+            z = cx<C2>::mk((RT)x[0], (RT)x[1]);
         }
         A[rl * M + n] = z;
     }
     __syncthreads();
-    double2* Z = smem_fft<false>(A, B, M, R, M, pl, twx, 2);
+    C2* Z = smem_fft<false>(A, B, M, R, M, pl, twx, 2);
     // split step: X_k = E_k + W^k O_k, E = (Z_k + conj Z_{M-k})/2, O = -i/2 (Z_k - conj Z_{M-k})
     const int nxh = M + 1;
     for (int t = threadIdx.x; t < R * nxh; t += blockDim.x) {
         const int rl = t / nxh, kx = t - rl * nxh;
         const int row = row0 + rl;
         if (row >= nrows) continue;
-        const double2 zk = Z[rl * M + (kx == M ? 0 : kx)];
-        const double2 zc = cconj(Z[rl * M + (kx == 0 ? 0 : M - kx)]);
-        const double2 e = make_double2(0.5 * (zk.x + zc.x), 0.5 * (zk.y + zc.y));
-        const double2 o = cmul_mi(make_double2(0.5 * (zk.x - zc.x), 0.5 * (zk.y - zc.y)));
-        const double2 X = cadd(e, cmul(__ldg(twx + kx), o));
+        const C2 zk = Z[rl * M + (kx == M ? 0 : kx)];
+        const C2 zc = cconj(Z[rl * M + (kx == 0 ? 0 : M - kx)]);
+        const RT h = (RT)0.5;
+        const C2 e = cx<C2>::mk(h * (zk.x + zc.x), h * (zk.y + zc.y));
+        const C2 o = cmul_mi(cx<C2>::mk(h * (zk.x - zc.x), h * (zk.y - zc.y)));
+        const C2 X = cadd(e, cmul(__ldg(twx + kx), o));
         spec[(long long)row * nxh + kx] = X;
     }
 }
@@ -193,24 +209,25 @@ k_div_fftx(mdx_dims d, int R, double dx, double dy, double dz, double dt_gamma, 
 // ---------------------------------------------------------------------------
 // Complex FFT along z of spec(kx, :, j) for a tile of TX kx values per block.
 // ---------------------------------------------------------------------------
-template <bool INV>
+template <bool INV, typename C2>
 __global__ void __launch_bounds__(256)
-k_fftz(mdx_dims d, int TX, double2* __restrict__ spec, mdx_fft_plan pl, const double2* __restrict__ twz) {
-    extern __shared__ double2 sm[];
+k_fftz(mdx_dims d, int TX, C2* __restrict__ spec, mdx_fft_plan pl, const C2* __restrict__ twz) {
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    C2* sm = reinterpret_cast<C2*>(sm_raw);
     const int nz = d.nz, nxh = d.nxh, ls = nz + 1;
-    double2* A = sm;
-    double2* B = sm + TX * ls;
+    C2* A = sm;
+    C2* B = sm + TX * ls;
     const int ntiles = (nxh + TX - 1) / TX;
     const int j = blockIdx.x / ntiles;
     const int kx0 = (blockIdx.x - j * ntiles) * TX;
-    double2* base = spec + (long long)j * nz * nxh;
+    C2* base = spec + (long long)j * nz * nxh;
     for (int t = threadIdx.x; t < TX * nz; t += blockDim.x) {
         const int c = t % TX, kz = t / TX;
         const int kx = kx0 + c;
-        A[c * ls + kz] = (kx < nxh) ? base[(long long)kz * nxh + kx] : make_double2(0.0, 0.0);
+        A[c * ls + kz] = (kx < nxh) ? base[(long long)kz * nxh + kx] : cx<C2>::mk(0, 0);
     }
     __syncthreads();
-    double2* Z = smem_fft<INV>(A, B, nz, TX, ls, pl, twz, 1);
+    C2* Z = smem_fft<INV>(A, B, nz, TX, ls, pl, twz, 1);
     for (int t = threadIdx.x; t < TX * nz; t += blockDim.x) {
         const int c = t % TX, kz = t / TX;
         const int kx = kx0 + c;
@@ -258,10 +275,13 @@ __global__ void k_thomas_tables(int nxh, int nzh, int ny, double dyi2, const dou
 
 // solve_tridiagonal_y, pressure_fft.f90:102-148: one thread per (kx, kz);
 // the forward sweep stores dp in place, the back substitution overwrites it
-// with the solution.
+// with the solution.  SKIP0: the (0, 0) mode is left to an FP64 solve and
+// zeroed here (the mixed-precision path).
+template <typename C2, bool SKIP0>
 __global__ void __launch_bounds__(128)
-k_thomas(mdx_dims d, double dyi2, double2* __restrict__ spec, const double* __restrict__ dinv,
-         const double* __restrict__ cp) {
+k_thomas(mdx_dims d, typename cx<C2>::R dyi2, C2* __restrict__ spec, const typename cx<C2>::R* __restrict__ dinv,
+         const typename cx<C2>::R* __restrict__ cp) {
+    typedef typename cx<C2>::R RT;
     const int nxh = d.nxh, nz = d.nz, ny = d.ny, nzh = d.nz / 2 + 1;
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= nxh * nz) return;
@@ -270,28 +290,32 @@ k_thomas(mdx_dims d, double dyi2, double2* __restrict__ spec, const double* __re
     const int mt = kx + nxh * kzt;
     const long long tplane = (long long)nxh * nzh;
     const long long splane = (long long)nxh * nz;
-    double2* col = spec + m;
-    const double a = dyi2;
-    double2 dp;
+    C2* col = spec + m;
+    if (SKIP0 && kx == 0 && kz == 0) {
+        for (int jj = 1; jj <= ny; ++jj) col[(jj - 1) * splane] = cx<C2>::mk(0, 0);
+        return;
+    }
+    const RT a = dyi2;
+    C2 dp;
     if (kx == 0 && kz == 0) {
-        dp = make_double2(0.0, 0.0);
+        dp = cx<C2>::mk(0, 0);
     } else {
-        const double2 r = col[0];
-        const double di = __ldg(dinv + mt);
-        dp = make_double2(r.x * di, r.y * di);
+        const C2 r = col[0];
+        const RT di = __ldg(dinv + mt);
+        dp = cx<C2>::mk(r.x * di, r.y * di);
     }
     col[0] = dp;
     for (int jj = 2; jj <= ny; ++jj) {
-        const double2 r = col[(jj - 1) * splane];
-        const double di = __ldg(dinv + (jj - 1) * tplane + mt);
-        dp = make_double2((r.x - a * dp.x) * di, (r.y - a * dp.y) * di);
+        const C2 r = col[(jj - 1) * splane];
+        const RT di = __ldg(dinv + (jj - 1) * tplane + mt);
+        dp = cx<C2>::mk((r.x - a * dp.x) * di, (r.y - a * dp.y) * di);
         col[(jj - 1) * splane] = dp;
     }
-    double2 nxt = dp;  // plane_hat(ny) = dp(ny)
+    C2 nxt = dp;  // plane_hat(ny) = dp(ny)
     for (int jj = ny - 1; jj >= 1; --jj) {
-        const double2 dj = col[(jj - 1) * splane];
-        const double c = __ldg(cp + (jj - 1) * tplane + mt);
-        nxt = make_double2(dj.x - c * nxt.x, dj.y - c * nxt.y);
+        const C2 dj = col[(jj - 1) * splane];
+        const RT c = __ldg(cp + (jj - 1) * tplane + mt);
+        nxt = cx<C2>::mk(dj.x - c * nxt.x, dj.y - c * nxt.y);
         col[(jj - 1) * splane] = nxt;
     }
 }
@@ -301,39 +325,42 @@ k_thomas(mdx_dims d, double dyi2, double2* __restrict__ spec, const double* __re
 // kx = 0 and kx = nx/2 bins are ignored), scaled by 1/(nx*nz) as
 // scale_pressure_correction_* (pressure_backend_fftw.f90:80-93).
 // ---------------------------------------------------------------------------
+template <typename C2>
 __global__ void __launch_bounds__(256)
-k_ifftx(mdx_dims d, int R, double scale, const double2* __restrict__ spec, double* __restrict__ phi,
-        mdx_fft_plan pl, const double2* __restrict__ twx) {
-    extern __shared__ double2 sm[];
+k_ifftx(mdx_dims d, int R, typename cx<C2>::R scale, const C2* __restrict__ spec, typename cx<C2>::R* __restrict__ phi,
+        mdx_fft_plan pl, const C2* __restrict__ twx) {
+    typedef typename cx<C2>::R RT;
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    C2* sm = reinterpret_cast<C2*>(sm_raw);
     const int M = d.nx / 2, nxh = M + 1;
-    double2* A = sm;
-    double2* B = sm + R * M;
+    C2* A = sm;
+    C2* B = sm + R * M;
     const int nrows = d.nz * d.ny;
     const int row0 = blockIdx.x * R;
     // Z'_k = (X_k + conj X_{M-k}) + i W^{-k} (X_k - conj X_{M-k}),  k < M
     for (int t = threadIdx.x; t < R * M; t += blockDim.x) {
         const int rl = t / M, k = t - rl * M;
         const int row = row0 + rl;
-        double2 z = make_double2(0.0, 0.0);
+        C2 z = cx<C2>::mk(0, 0);
         if (row < nrows) {
-            const double2* X = spec + (long long)row * nxh;
-            double2 xk = X[k], xm = X[M - k];
-            if (k == 0) { xk.y = 0.0; xm.y = 0.0; }   // kx = 0 and kx = M bins are real
-            const double2 xc = cconj(xm);
-            const double2 e = cadd(xk, xc);
-            const double2 o = cmul(csub(xk, xc), cconj(__ldg(twx + k)));
+            const C2* X = spec + (long long)row * nxh;
+            C2 xk = X[k], xm = X[M - k];
+            if (k == 0) { xk.y = 0; xm.y = 0; }   // kx = 0 and kx = M bins are real
+            const C2 xc = cconj(xm);
+            const C2 e = cadd(xk, xc);
+            const C2 o = cmul(csub(xk, xc), cconj(__ldg(twx + k)));
             z = cadd(e, cmul_pi(o));
         }
         A[rl * M + k] = z;
     }
     __syncthreads();
-    double2* Z = smem_fft<true>(A, B, M, R, M, pl, twx, 2);
+    C2* Z = smem_fft<true>(A, B, M, R, M, pl, twx, 2);
     for (int t = threadIdx.x; t < R * M; t += blockDim.x) {
         const int rl = t / M, n = t - rl * M;
         const int row = row0 + rl;
         if (row >= nrows) continue;
-        const double2 z = Z[rl * M + n];
-        double* out = phi + (long long)row * d.nx;
+        const C2 z = Z[rl * M + n];
+        RT* out = phi + (long long)row * d.nx;
         out[2 * n] = z.x * scale;
         out[2 * n + 1] = z.y * scale;
     }
@@ -446,14 +473,22 @@ int mdx_fft_init(mdx_ctx_t* ctx) {
     const int M = d.nx / 2;
     const size_t smx = sizeof(double2) * 2 * rows_per_block(M) * M;
     const size_t smz = sizeof(double2) * 2 * ztile(d.nz) * (d.nz + 1);
-    MDX_CUDA(ctx, cudaFuncSetAttribute(k_div_fftx, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx));
-    MDX_CUDA(ctx, cudaFuncSetAttribute(k_ifftx, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx));
-    MDX_CUDA(ctx, cudaFuncSetAttribute(k_fftz<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz));
-    MDX_CUDA(ctx, cudaFuncSetAttribute(k_fftz<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz));
+    MDX_CUDA(ctx, cudaFuncSetAttribute(k_div_fftx<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx));
+    MDX_CUDA(ctx, cudaFuncSetAttribute(k_ifftx<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx));
+    MDX_CUDA(ctx, cudaFuncSetAttribute(k_fftz<false, double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz));
+    MDX_CUDA(ctx, cudaFuncSetAttribute(k_fftz<true, double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz));
     return MDX_OK;
 }
 
 void mdx_fft_free(mdx_ctx_t* ctx) {
+    cudaFree(ctx->spec32); ctx->spec32 = nullptr;
+    cudaFree(ctx->tw_x32); ctx->tw_x32 = nullptr;
+    cudaFree(ctx->tw_z32); ctx->tw_z32 = nullptr;
+    cudaFree(ctx->phi32); ctx->phi32 = nullptr;
+    cudaFree(ctx->dinv32); ctx->dinv32 = nullptr;
+    cudaFree(ctx->cp32); ctx->cp32 = nullptr;
+    cudaFree(ctx->rhs0); ctx->rhs0 = nullptr;
+    cudaFree(ctx->phi0); ctx->phi0 = nullptr;
     cudaFree(ctx->spec); ctx->spec = nullptr;
     cudaFree(ctx->tw_x); ctx->tw_x = nullptr;
     cudaFree(ctx->tw_z); ctx->tw_z = nullptr;
@@ -463,6 +498,7 @@ void mdx_fft_free(mdx_ctx_t* ctx) {
 
 // pressure_projection of the FFT builds, pressure_solver.f90:58-61.
 int mdx_k_projection_fft(mdx_ctx_t* ctx, double dg) {
+    if (ctx->opts.precision == MDX_PREC_MIXED) return mdx_k_projection_fft_mixed(ctx, dg);
     const mdx_dims& d = ctx->d;
     const mdx_grid_t& g = ctx->g;
     double** f = ctx->f;
@@ -471,18 +507,21 @@ int mdx_k_projection_fft(mdx_ctx_t* ctx, double dg) {
     const int nrows = d.nz * d.ny;
     const size_t smx = sizeof(double2) * 2 * R * M;
     const int xblocks = (nrows + R - 1) / R;
-    MDX_LAUNCH(ctx, MDX_T_FFT_FWD, "div+fft x", k_div_fftx, xblocks, 256, smx, d, R, g.dx, g.dy, g.dz, dg, f[MDX_US],
-               f[MDX_VS], f[MDX_WS], ctx->spec, ctx->plan_xh, ctx->tw_x);
+    MDX_LAUNCH(ctx, MDX_T_FFT_FWD, "div+fft x", k_div_fftx<double2>, xblocks, 256, smx, d, R, g.dx, g.dy, g.dz, dg,
+               f[MDX_US], f[MDX_VS], f[MDX_WS], ctx->spec, ctx->plan_xh, ctx->tw_x);
     const int TX = ztile(d.nz);
     const size_t smz = sizeof(double2) * 2 * TX * (d.nz + 1);
     const int zblocks = ((d.nxh + TX - 1) / TX) * d.ny;
-    MDX_LAUNCH(ctx, MDX_T_FFT_FWD, "fft z", k_fftz<false>, zblocks, 256, smz, d, TX, ctx->spec, ctx->plan_z, ctx->tw_z);
+    auto kz_f = k_fftz<false, double2>;
+    auto kz_i = k_fftz<true, double2>;
+    auto kth = k_thomas<double2, false>;
+    MDX_LAUNCH(ctx, MDX_T_FFT_FWD, "fft z", kz_f, zblocks, 256, smz, d, TX, ctx->spec, ctx->plan_z, ctx->tw_z);
     const int nm = d.nxh * d.nz;
-    MDX_LAUNCH(ctx, MDX_T_THOMAS, "thomas", k_thomas, (nm + 127) / 128, 128, 0, d, 1.0 / (g.dy * g.dy), ctx->spec,
+    MDX_LAUNCH(ctx, MDX_T_THOMAS, "thomas", kth, (nm + 127) / 128, 128, 0, d, 1.0 / (g.dy * g.dy), ctx->spec,
                ctx->thomas_dinv, ctx->thomas_cp);
-    MDX_LAUNCH(ctx, MDX_T_FFT_INV, "ifft z", k_fftz<true>, zblocks, 256, smz, d, TX, ctx->spec, ctx->plan_z, ctx->tw_z);
+    MDX_LAUNCH(ctx, MDX_T_FFT_INV, "ifft z", kz_i, zblocks, 256, smz, d, TX, ctx->spec, ctx->plan_z, ctx->tw_z);
     const double scale = 1.0 / (double)(d.nx * d.nz);
-    MDX_LAUNCH(ctx, MDX_T_FFT_INV, "ifft x", k_ifftx, xblocks, 256, smx, d, R, scale, ctx->spec, f[MDX_PHI],
+    MDX_LAUNCH(ctx, MDX_T_FFT_INV, "ifft x", k_ifftx<double2>, xblocks, 256, smx, d, R, scale, ctx->spec, f[MDX_PHI],
                ctx->plan_xh, ctx->tw_x);
     dim3 block(32, 4, 2);
     dim3 grid((d.nx + 31) / 32, (d.ny + 3) / 4, (d.nz + 1) / 2);
@@ -494,6 +533,212 @@ int mdx_k_projection_fft(mdx_ctx_t* ctx, double dg) {
         MDX_LAUNCH(ctx, MDX_T_CORRECT, "correction", k_correct<true>, grid, block, 0, d, g.dx, g.dy, g.dz, dg,
                    f[MDX_PHI], f[MDX_US], f[MDX_VS], f[MDX_WS], f[MDX_UN], f[MDX_VN], f[MDX_WN], f[MDX_PN],
                    f[MDX_COEF_U], f[MDX_COEF_V], f[MDX_COEF_W]);
+    return MDX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Mixed precision on the FFT path: the x-z FFTs and the Thomas solves run in
+// FP32 inside FP64 defect correction.  Each pass takes the FP64 divergence of
+// the current velocity (k_div_fftx computes it in FP64 and hands FP32 to the
+// transform), solves for the FP32 correction phi, and corrects u, v, w and p
+// in FP64.  The zero-wavenumber mode -- the near-singular Neumann problem in y
+// pinned at j = 1 -- stays FP64: its right-hand side is the FP64 plane sum of
+// the divergence, its Thomas solve uses the FP64 tables, and its solution is
+// added to phi in FP64.  Without IBM the FFT-path correction makes the
+// discrete divergence exactly L(phi_exact - phi) / dt_gamma, so the next pass
+// solves the defect; passes repeat until ||div u|| <= max(tol ||div u*||,
+// atol), the red-black path's stop rule.
+// ---------------------------------------------------------------------------
+
+// FP64 plane sums of the divergence/dt_gamma (the (0,0) Fourier coefficient of
+// each y plane), one block per plane, fixed order.
+__global__ void __launch_bounds__(256)
+k_zero_rhs(mdx_dims d, double dx, double dy, double dz, double dt_gamma, const double* __restrict__ us,
+           const double* __restrict__ vs, const double* __restrict__ ws, double* __restrict__ rhs0) {
+    const int j = blockIdx.x + 1;
+    double s = 0.0;
+    for (int t = threadIdx.x; t < d.nx * d.nz; t += blockDim.x) {
+        const int i = t % d.nx + 1, k = t / d.nx + 1;
+        const long long c = pidx(d, i, j, k);
+        s += ((__ldg(us + c + 1) - __ldg(us + c)) / dx + (__ldg(vs + c + d.nxp) - __ldg(vs + c)) / dy +
+              (__ldg(ws + c + (long long)d.nxp * d.nyp) - __ldg(ws + c)) / dz) / dt_gamma;
+    }
+    __shared__ double sh[256];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) sh[threadIdx.x] += sh[threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) rhs0[j - 1] = sh[0];
+}
+
+// The (0, 0) column of k_thomas in FP64, scaled by 1/(nx nz) like the inverse
+// transform: phi0[j] is that mode's contribution to phi on plane j.
+__global__ void k_zero_solve(int ny, long long tplane, double dyi2, double scale, const double* __restrict__ dinv,
+                             const double* __restrict__ cp, const double* __restrict__ rhs0, double* __restrict__ phi0) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    const double a = dyi2;
+    double dp = 0.0;   // the pinned row j = 1
+    phi0[0] = dp;
+    for (int jj = 2; jj <= ny; ++jj) {
+        dp = (rhs0[jj - 1] - a * dp) * dinv[(jj - 1) * tplane];
+        phi0[jj - 1] = dp;
+    }
+    double nxt = dp;
+    phi0[ny - 1] = nxt * scale;
+    for (int jj = ny - 1; jj >= 1; --jj) {
+        nxt = phi0[jj - 1] - cp[(jj - 1) * tplane] * nxt;
+        phi0[jj - 1] = nxt;
+    }
+    for (int jj = 1; jj < ny; ++jj) phi0[jj - 1] *= scale;
+}
+
+__global__ void k_to_float(long long n, const double* __restrict__ a, float* __restrict__ b) {
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+        b[t] = (float)a[t];
+}
+
+// apply_fft_pressure_correction with phi = FP32 correction + FP64 zero mode.
+template <bool IBM>
+__global__ void __launch_bounds__(256)
+k_correct_mixed(mdx_dims d, double dx, double dy, double dz, double dt_gamma, const float* __restrict__ phi,
+                const double* __restrict__ phi0, const double* __restrict__ us, const double* __restrict__ vs,
+                const double* __restrict__ ws, double* __restrict__ un, double* __restrict__ vn,
+                double* __restrict__ wn, double* __restrict__ pn, const double* __restrict__ cu,
+                const double* __restrict__ cv, const double* __restrict__ cw) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
+    if (i > d.nx || j > d.ny || k > d.nz) return;
+    int im = i - 1, km = k - 1;
+    if (im < 1) im = d.nx;
+    if (km < 1) km = d.nz;
+    const long long c = pidx(d, i, j, k);
+    const double p0 = __ldg(phi0 + j - 1);
+    const double r = (double)__ldg(phi + ridx(d, i, k, j)) + p0;
+    double u = __ldg(us + c) - dt_gamma * (r - ((double)__ldg(phi + ridx(d, im, k, j)) + p0)) / dx;
+    double w = __ldg(ws + c) - dt_gamma * (r - ((double)__ldg(phi + ridx(d, i, km, j)) + p0)) / dz;
+    if (IBM) {
+        u = u / (1.0 + dt_gamma * __ldg(cu + c));
+        w = w / (1.0 + dt_gamma * __ldg(cw + c));
+    }
+    un[c] = u;
+    wn[c] = w;
+    pn[c] = pn[c] + r;
+    if (j >= 2) {
+        const double rm = (double)__ldg(phi + ridx(d, i, k, j - 1)) + __ldg(phi0 + j - 2);
+        double v = __ldg(vs + c) - dt_gamma * (r - rm) / dy;
+        if (IBM) v = v / (1.0 + dt_gamma * __ldg(cv + c));
+        vn[c] = v;
+    }
+}
+
+static int fft_mixed_alloc(mdx_ctx_t* ctx) {
+    if (ctx->spec32) return MDX_OK;
+    const mdx_dims& d = ctx->d;
+    const int nzh = d.nz / 2 + 1;
+    const long long tsize = (long long)d.ny * d.nxh * nzh;
+    MDX_CUDA(ctx, cudaMalloc(&ctx->spec32, sizeof(float2) * d.nspec));
+    MDX_CUDA(ctx, cudaMalloc(&ctx->phi32, sizeof(float) * d.nint));
+    MDX_CUDA(ctx, cudaMalloc(&ctx->dinv32, sizeof(float) * tsize));
+    MDX_CUDA(ctx, cudaMalloc(&ctx->cp32, sizeof(float) * tsize));
+    MDX_CUDA(ctx, cudaMalloc(&ctx->rhs0, sizeof(double) * d.ny));
+    MDX_CUDA(ctx, cudaMalloc(&ctx->phi0, sizeof(double) * d.ny));
+    std::vector<double2> tx, tz;
+    mdx_fft_twiddles(d.nx, tx);
+    mdx_fft_twiddles(d.nz, tz);
+    std::vector<float2> fx(d.nx), fz(d.nz);
+    for (int t = 0; t < d.nx; ++t) fx[t] = make_float2((float)tx[t].x, (float)tx[t].y);
+    for (int t = 0; t < d.nz; ++t) fz[t] = make_float2((float)tz[t].x, (float)tz[t].y);
+    MDX_CUDA(ctx, cudaMalloc(&ctx->tw_x32, sizeof(float2) * d.nx));
+    MDX_CUDA(ctx, cudaMalloc(&ctx->tw_z32, sizeof(float2) * d.nz));
+    MDX_CUDA(ctx, cudaMemcpy(ctx->tw_x32, fx.data(), sizeof(float2) * d.nx, cudaMemcpyHostToDevice));
+    MDX_CUDA(ctx, cudaMemcpy(ctx->tw_z32, fz.data(), sizeof(float2) * d.nz, cudaMemcpyHostToDevice));
+    const int nb = (int)std::min<long long>((tsize + 255) / 256, 4096);
+    MDX_LAUNCH(ctx, MDX_T_OTHER, "thomas tables fp32", k_to_float, nb, 256, 0, tsize, ctx->thomas_dinv, ctx->dinv32);
+    MDX_LAUNCH(ctx, MDX_T_OTHER, "thomas tables fp32", k_to_float, nb, 256, 0, tsize, ctx->thomas_cp, ctx->cp32);
+    const int M = d.nx / 2;
+    const size_t smx = sizeof(float2) * 2 * rows_per_block(M) * M;
+    const size_t smz = sizeof(float2) * 2 * ztile(d.nz) * (d.nz + 1);
+    MDX_CUDA(ctx, cudaFuncSetAttribute(k_div_fftx<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx));
+    MDX_CUDA(ctx, cudaFuncSetAttribute(k_ifftx<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx));
+    MDX_CUDA(ctx, cudaFuncSetAttribute(k_fftz<false, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz));
+    MDX_CUDA(ctx, cudaFuncSetAttribute(k_fftz<true, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz));
+    return MDX_OK;
+}
+
+int mdx_k_projection_fft_mixed(mdx_ctx_t* ctx, double dg) {
+    MDX_TRY(fft_mixed_alloc(ctx));
+    const mdx_dims& d = ctx->d;
+    const mdx_grid_t& g = ctx->g;
+    const mdx_solver_opts_t& o = ctx->opts;
+    double** f = ctx->f;
+    const int M = d.nx / 2;
+    const int R = rows_per_block(M);
+    const int nrows = d.nz * d.ny;
+    const size_t smx = sizeof(float2) * 2 * R * M;
+    const int xblocks = (nrows + R - 1) / R;
+    const int TX = ztile(d.nz);
+    const size_t smz = sizeof(float2) * 2 * TX * (d.nz + 1);
+    const int zblocks = ((d.nxh + TX - 1) / TX) * d.ny;
+    const int nm = d.nxh * d.nz;
+    const double dyi2 = 1.0 / (g.dy * g.dy);
+    const double scale = 1.0 / (double)(d.nx * d.nz);
+    const long long tplane = (long long)d.nxh * (d.nz / 2 + 1);
+    const size_t pad = sizeof(double) * d.npad;
+    auto kz_f = k_fftz<false, float2>;
+    auto kz_i = k_fftz<true, float2>;
+    auto kth = k_thomas<float2, true>;
+    auto kcor = ctx->ibm_zero ? k_correct_mixed<false> : k_correct_mixed<true>;
+    dim3 block(32, 4, 2);
+    dim3 grid((d.nx + 31) / 32, (d.ny + 3) / 4, (d.nz + 1) / 2);
+    // the stop rule of the red-black path, on ||div u*|| before the first pass
+    double r0 = 0.0, linf = 0.0, umax = 0.0;
+    MDX_TRY(mdx_k_div_norms(ctx, f[MDX_US], f[MDX_VS], f[MDX_WS], &r0, &linf, &umax));
+    const double tol = o.tol > 0.0 ? o.tol : 1e-10;
+    const double atol = (o.atol < 0.0) ? mdx_div_floor(ctx, umax) : o.atol;
+    const double target = std::max(tol * r0, atol);
+    mdx_solve_stats_t st{};
+    st.residual0 = r0;
+    st.atol = atol;
+    st.status = MDX_NOT_CONVERGED;
+    double r = r0;
+    int pass = 0;
+    const int max_pass = 8;
+    while (pass < max_pass) {
+        if (pass > 0) {   // the corrected state becomes the next pass's u*
+            MDX_TRY(mdx_k_apply_bc(ctx));
+            MDX_CUDA(ctx, cudaMemcpyAsync(f[MDX_US], f[MDX_UN], pad, cudaMemcpyDeviceToDevice, ctx->stream));
+            MDX_CUDA(ctx, cudaMemcpyAsync(f[MDX_VS], f[MDX_VN], pad, cudaMemcpyDeviceToDevice, ctx->stream));
+            MDX_CUDA(ctx, cudaMemcpyAsync(f[MDX_WS], f[MDX_WN], pad, cudaMemcpyDeviceToDevice, ctx->stream));
+        }
+        MDX_LAUNCH(ctx, MDX_T_FFT_FWD, "div+fft x fp32", k_div_fftx<float2>, xblocks, 256, smx, d, R, g.dx, g.dy,
+                   g.dz, dg, f[MDX_US], f[MDX_VS], f[MDX_WS], ctx->spec32, ctx->plan_xh, ctx->tw_x32);
+        MDX_LAUNCH(ctx, MDX_T_FFT_FWD, "zero mode rhs", k_zero_rhs, d.ny, 256, 0, d, g.dx, g.dy, g.dz, dg, f[MDX_US],
+                   f[MDX_VS], f[MDX_WS], ctx->rhs0);
+        MDX_LAUNCH(ctx, MDX_T_FFT_FWD, "fft z fp32", kz_f, zblocks, 256, smz, d, TX, ctx->spec32, ctx->plan_z,
+                   ctx->tw_z32);
+        MDX_LAUNCH(ctx, MDX_T_THOMAS, "thomas fp32", kth, (nm + 127) / 128, 128, 0, d, (float)dyi2, ctx->spec32,
+                   ctx->dinv32, ctx->cp32);
+        MDX_LAUNCH(ctx, MDX_T_THOMAS, "zero mode fp64", k_zero_solve, 1, 32, 0, d.ny, tplane, dyi2, scale,
+                   ctx->thomas_dinv, ctx->thomas_cp, ctx->rhs0, ctx->phi0);
+        MDX_LAUNCH(ctx, MDX_T_FFT_INV, "ifft z fp32", kz_i, zblocks, 256, smz, d, TX, ctx->spec32, ctx->plan_z,
+                   ctx->tw_z32);
+        MDX_LAUNCH(ctx, MDX_T_FFT_INV, "ifft x fp32", k_ifftx<float2>, xblocks, 256, smx, d, R, (float)scale,
+                   ctx->spec32, ctx->phi32, ctx->plan_xh, ctx->tw_x32);
+        MDX_LAUNCH(ctx, MDX_T_CORRECT, "correction mixed", kcor, grid, block, 0, d, g.dx, g.dy, g.dz, dg, ctx->phi32,
+                   ctx->phi0, f[MDX_US], f[MDX_VS], f[MDX_WS], f[MDX_UN], f[MDX_VN], f[MDX_WN], f[MDX_PN],
+                   f[MDX_COEF_U], f[MDX_COEF_V], f[MDX_COEF_W]);
+        ++pass;
+        MDX_TRY(mdx_k_div_norms(ctx, f[MDX_UN], f[MDX_VN], f[MDX_WN], &r, &linf));
+        if (!std::isfinite(r)) { st.status = MDX_ERR_NONFINITE; break; }
+        if (r <= target) { st.status = MDX_OK; break; }
+    }
+    st.iterations = pass;
+    st.residual = r0 > 0.0 ? r / r0 : 0.0;
+    st.variant = 200 + pass;   // FFT mixed path: 200 + FP64 passes
+    ctx->last = st;
     return MDX_OK;
 }
 
@@ -532,7 +777,8 @@ static void* g_noalloc_addr[MDX_NOALLOC_MAX_DEVICES] = {nullptr};
 __global__ void __launch_bounds__(256)
 k_fftx_r2c(mdx_dims d, int R, const double* __restrict__ rhs, double2* __restrict__ spec, mdx_fft_plan pl,
            const double2* __restrict__ twx) {
-    extern __shared__ double2 sm[];
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    double2* sm = reinterpret_cast<double2*>(sm_raw);
     const int M = d.nx / 2;
     double2* A = sm;
     double2* B = sm + R * M;
@@ -670,16 +916,18 @@ extern "C" int mdx_solve_pressure_fft_noalloc(const double* rhs, double* phi, in
     const size_t smz = sizeof(double2) * 2 * TX * (nz + 1);
     const int zblocks = ((d.nxh + TX - 1) / TX) * ny;
     const cudaError_t a1 = cudaFuncSetAttribute(k_fftx_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx);
-    const cudaError_t a2 = cudaFuncSetAttribute(k_ifftx, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx);
-    const cudaError_t a3 = cudaFuncSetAttribute(k_fftz<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz);
-    const cudaError_t a4 = cudaFuncSetAttribute(k_fftz<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz);
+    const cudaError_t a2 = cudaFuncSetAttribute(k_ifftx<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx);
+    const cudaError_t a3 =
+        cudaFuncSetAttribute(k_fftz<false, double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz);
+    const cudaError_t a4 =
+        cudaFuncSetAttribute(k_fftz<true, double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz);
     if (a1 != cudaSuccess || a2 != cudaSuccess || a3 != cudaSuccess || a4 != cudaSuccess)
         return mdx_fail(nullptr, MDX_ERR_CUDA, "noalloc solve: cudaFuncSetAttribute failed");
     k_fftx_r2c<<<xblocks, 256, smx, st>>>(d, R, rhs, spec, plx, twx);
-    k_fftz<false><<<zblocks, 256, smz, st>>>(d, TX, spec, plz, twz);
-    k_thomas<<<(d.nxh * nz + 127) / 128, 128, 0, st>>>(d, dyi2, spec, dinv, cp);
-    k_fftz<true><<<zblocks, 256, smz, st>>>(d, TX, spec, plz, twz);
-    k_ifftx<<<xblocks, 256, smx, st>>>(d, R, 1.0 / (double)(nx * nz), spec, phi, plx, twx);
+    k_fftz<false, double2><<<zblocks, 256, smz, st>>>(d, TX, spec, plz, twz);
+    k_thomas<double2, false><<<(d.nxh * nz + 127) / 128, 128, 0, st>>>(d, dyi2, spec, dinv, cp);
+    k_fftz<true, double2><<<zblocks, 256, smz, st>>>(d, TX, spec, plz, twz);
+    k_ifftx<double2><<<xblocks, 256, smx, st>>>(d, R, 1.0 / (double)(nx * nz), spec, phi, plx, twx);
     e = cudaGetLastError();
     if (e != cudaSuccess) return mdx_fail(nullptr, MDX_ERR_CUDA, "noalloc solve: launch: %s", cudaGetErrorString(e));
     return MDX_OK;

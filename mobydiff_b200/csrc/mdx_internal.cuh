@@ -108,6 +108,11 @@ struct mdx_ctx {
     double2* tw_z = nullptr;                 // exp(-2 pi i t/nz), t < nz
     mdx_fft_plan plan_xh{};                  // complex length nx/2 (packed real transform)
     mdx_fft_plan plan_z{};                   // complex length nz
+    // mixed-precision FFT path: FP32 spectrum, correction, twiddles, Thomas
+    // tables; FP64 zero-wavenumber right-hand side and solution per y
+    float2 *spec32 = nullptr, *tw_x32 = nullptr, *tw_z32 = nullptr;
+    float *phi32 = nullptr, *dinv32 = nullptr, *cp32 = nullptr;
+    double *rhs0 = nullptr, *phi0 = nullptr;
 
     // reductions
     double* red_part = nullptr;              // per-block partials (2 per block)
@@ -170,6 +175,7 @@ int mdx_k_apply_bc_redblack(mdx_ctx_t* ctx);
 int mdx_fft_init(mdx_ctx_t* ctx);
 void mdx_fft_free(mdx_ctx_t* ctx);
 int mdx_k_projection_fft(mdx_ctx_t* ctx, double dg);
+int mdx_k_projection_fft_mixed(mdx_ctx_t* ctx, double dg);
 int mdx_k_projection_redblack(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t* st);
 int mdx_k_div_norms(mdx_ctx_t* ctx, const double* u, const double* v, const double* w, double* l2, double* linf,
                     double* umax = nullptr);
