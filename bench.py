@@ -59,9 +59,13 @@ CONFIGS = {
                solver="redblack", sor=1.7, tol=1e-8, check_every=10, members=64, method="ensemble"),
     "c0": dict(workload="periodic channel 64^3, FP64 FFT+Thomas", nx=64, ny=64, nz=64, lx=2 * math.pi, ly=2.0,
                lz=math.pi, re=2000.0, dt=1e-3, solver="fft", ibm="none", amp=0.0, method="plain"),
-    "c2": dict(workload="periodic channel 512x256x256, FP64 FFT+Thomas", nx=512, ny=256, nz=256,
-               lx=4 * math.pi, ly=2.0, lz=2 * math.pi, re=5000.0, dt=1e-3, solver="fft", ibm="none", amp=0.0,
-               method="plain"),
+    "c2": dict(workload="channel 512x256x256 (Lx 4pi, Lz 2pi, Re 5000): FP32 FFT + Thomas inside FP64 defect "
+                         "correction to residual 1e-10, zero-wavenumber mode in FP64",
+               nx=512, ny=256, nz=256, lx=4 * math.pi, ly=2.0, lz=2 * math.pi, re=5000.0, dt=1e-3, solver="fft",
+               ibm="none", amp=0.0, tol=1e-10, method="fft-mixed"),
+    "c2-plain": dict(workload="channel 512x256x256 (Lx 4pi, Lz 2pi, Re 5000), FP64 FFT+Thomas", nx=512, ny=256,
+                     nz=256, lx=4 * math.pi, ly=2.0, lz=2 * math.pi, re=5000.0, dt=1e-3, solver="fft", ibm="none",
+                     amp=0.0, method="plain"),
 }
 
 # Red-black iterations per RK3 step of the plain FP64 method (zero start) on
@@ -167,7 +171,8 @@ def _setup(cfg, M, device, profile=False, tol=None, precision=None, seed=None):
                                   check_every=cfg["check_every"], max_iter=400000,
                                   precision=M.PREC_FP64 if precision is None else precision)
     else:
-        opts = M.make_solver_opts(M.SOLVER_FFT)
+        opts = M.make_solver_opts(M.SOLVER_FFT, tol=cfg.get("tol", 0.0) if precision == M.PREC_MIXED else 0.0,
+                                  precision=M.PREC_FP64 if precision is None else precision)
     s.init_pressure_solver(opts)
     s.channel_ic(SEED if seed is None else seed, 0.1, 0.01, y0, cfg["amp"], lam)
     return s, g
@@ -584,6 +589,80 @@ def run_ensemble(args, cfg):
     return 0
 
 
+def run_fft_mixed(args, cfg):
+    """The FFT path in mixed precision beside the plain FP64 FFT path, on the
+    same seeded start and the same steps."""
+    import torch
+    import mobydiff_b200 as M
+
+    ws, rank, local = _dist()
+    device = local
+    pg = _init_dist(device)
+    cells = cfg["nx"] * cfg["ny"] * cfg["nz"]
+    W, K = args.warmup, args.steps
+    # plain FP64 FFT arm (CUDA-graph steps)
+    sp, _ = _setup(cfg, M, device, precision=M.PREC_FP64)
+    stream_p = torch.cuda.ExternalStream(sp.stream(), device=device)
+    for _ in range(W):
+        sp.step(1)
+    p_ms_all, _, _, _, _ = _timed_steps(sp, stream_p, K, pg)
+    plain_value = ws * cells * K / (p_ms_all / 1e3) / 1e6
+    plain_state = {n: sp.get(n) for n in ("un", "vn", "wn", "pn")}
+    sp.close()
+    # mixed arm
+    s, _ = _setup(cfg, M, device, precision=M.PREC_MIXED)
+    stream = torch.cuda.ExternalStream(s.stream(), device=device)
+    for _ in range(W):
+        s.step(1)
+    host = [torch.empty(s.padded, dtype=torch.float64, pin_memory=True) for _ in range(4)]
+    s.update_host(*[h.numpy() for h in host])
+    clocks = ClockSampler(device)
+    clocks.start()
+    torch.cuda.nvtx.range_push("value")
+    ms_all, ms, passes, launches, _ = _timed_steps(s, stream, K, pg)
+    torch.cuda.nvtx.range_pop()
+    clk = clocks.stop()
+    value = ws * cells * K / (ms_all / 1e3) / 1e6
+    interior = (slice(1, -1), slice(1, -1), slice(1, -1))
+    err = {n: float(np.linalg.norm((s.get(n) - plain_state[n])[interior]) / np.linalg.norm(plain_state[n][interior]))
+           for n in ("un", "vn", "wn", "pn")}
+    l2, linf = s.divergence_norms()
+    e2e_line = None
+    if not args.no_e2e:
+        ems, e2e_passes = _e2e_steps(s, stream, host, K, pg)
+        nbytes = 4 * host[0].numel() * 8
+        e2e_line = {"value": ws * cells * K / (ems / 1e3) / 1e6, "unit": UNIT, "h2d_bytes_per_step": nbytes,
+                    "d2h_bytes_per_step": nbytes, "same_steps_as_value": e2e_passes == passes}
+    s.update_device(*[h.numpy() for h in host])
+    _, r_ms, _, _, tim = _timed_steps(s, stream, K, pg, timing=True)
+    roofline = _roofline(tim, "momentum", 112.0, cells, r_ms)   # 14 doubles per cell
+    shares = {k: v[0] / r_ms for k, v in tim.items() if v[1]}
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        cpu = _cpu_baseline(cfg, 0.0)
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": W,
+                "ms_per_step": ms_all / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64+f32 (FP32 FFT and Thomas in FP64 defect correction)",
+                "data": "synthetic: seeded Poiseuille+noise IC (SplitMix64), projected at t=0",
+                "config": {"workload": cfg["workload"], "grid": [cfg["nx"], cfg["ny"], cfg["nz"]], "re": cfg["re"],
+                           "dt": cfg["dt"], "tol": cfg["tol"], "parallelism": f"replicas x{ws}",
+                           "l2": "inputs larger than L2 (state > 126 MB)"},
+                "defect_correction_passes_per_substage": passes / (3 * K),
+                "plain_fp64": {"value": plain_value, "unit": UNIT, "ms_per_step": p_ms_all / K,
+                               "note": "direct FP64 solve, CUDA-graph steps"},
+                "speedup_vs_plain_fp64": value / plain_value,
+                "error_vs_plain_fp64": {"rel_l2_interior": err, "div_l2": l2, "div_linf": linf},
+                "kernel_class_shares": shares,
+                "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "e2e": e2e_line, "gpu_launches": launches}
+        print(json.dumps(line), flush=True)
+    s.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
 def run_profile_mixed(args, cfg):
     """Only the set-up: the t=0 projection of the full-size workload with
     FP32 sweeps in FP64 defect correction (for an ncu capture of a few
@@ -758,6 +837,8 @@ def main():
         return run_profile_mixed(args, cfg)
     if cfg["method"] == "ensemble":
         return run_ensemble(args, cfg)
+    if cfg["method"] == "fft-mixed" and not args.profile:
+        return run_fft_mixed(args, cfg)
     if cfg["method"] == "learned-mixed" and not args.profile:
         return run_learned_mixed(args, cfg)
     return run_plain(args, cfg)
