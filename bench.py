@@ -721,7 +721,7 @@ def run_learned_mixed(args, cfg):
     st_, gt = learned.wavy_solver(cfg["nx"], cfg["ny"], cfg["nz"], cfg["re"], cfg["amp"], tol,
                                   check_every=cfg["check_every"], precision=M.PREC_MIXED, device=device,
                                   ly=cfg["ly"], lx=cfg["lx"], lz=cfg["lz"], dt=cfg["dt"])
-    net = learned.record_and_train(st_, gt, TRAIN_RUNS, warm_steps=3, record_steps=8, iters=args.train_iters)
+    net = learned.record_and_train(st_, gt, TRAIN_RUNS, warm_steps=3, record_steps=16, iters=args.train_iters)
     st_.close()
     train_wall = time.time() - t0
 
@@ -828,7 +828,7 @@ def main():
     ap.add_argument("--profile-mixed", action="store_true",
                     help="profiling run for ncu: the full-size t=0 projection with FP32 sweeps to residual 1e-8")
     ap.add_argument("--quick", action="store_true", help="skip the plain FP64 leg at residual 1e-10")
-    ap.add_argument("--train-iters", type=int, default=600, help="Adam steps of the learned warm start")
+    ap.add_argument("--train-iters", type=int, default=1200, help="Adam steps of the learned warm start")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
     if args.impl == "reference":
