@@ -777,6 +777,36 @@ def run_learned_mixed(args, cfg):
     x_ms_all, _, x_iters, _, _ = _timed_steps(s, stream, K, pg)
     no_net = {"value": ws * cells * K / (x_ms_all / 1e3) / 1e6, "unit": UNIT, "ms_per_step": x_ms_all / K,
               "poisson_iters_per_substage": x_iters / (3 * K)}
+    s.close()
+
+    # ---- the relaxation factor's share, measured apart: learned + mixed with
+    # the FP32 correction sweeps at omega 1.95 (the FP64 test unchanged), and
+    # the plain FP64 method with omega 1.95 as its input, same start and steps
+    tuned = None
+    if not args.quick:
+        om = 1.95
+        st2, _ = _setup(cfg, M, device, tol=tol, precision=M.PREC_MIXED)
+        st2.init_pressure_solver(M.make_solver_opts(M.SOLVER_REDBLACK, sor=cfg["sor"], tol=tol,
+                                                    check_every=cfg["check_every"], max_iter=400000,
+                                                    precision=M.PREC_MIXED, inner_sor=om))
+        st2.channel_ic(SEED, 0.1, 0.01, (cfg["ly"] - 2.0) / 2.0, cfg["amp"], cfg["lx"] / 2.0)
+        learned.load_into(st2, net)
+        st2.set_pressure_guess(M.GUESS_LEARNED, record=True)
+        for _ in range(W):
+            st2.step(1)
+        t_ms_all, _, t_iters, _, _ = _timed_steps(st2, torch.cuda.ExternalStream(st2.stream(), device=device), K, pg)
+        st2.close()
+        cfg_om = dict(cfg, sor=om)
+        sp2, _ = _setup(cfg_om, M, device, tol=tol, precision=M.PREC_FP64)
+        for _ in range(W):
+            sp2.step(1)
+        q_ms_all, _, q_iters, _, _ = _timed_steps(sp2, torch.cuda.ExternalStream(sp2.stream(), device=device), K, pg)
+        sp2.close()
+        tuned = {"omega": om,
+                 "learned_mixed_inner_omega": {"value": ws * cells * K / (t_ms_all / 1e3) / 1e6, "unit": UNIT,
+                                               "poisson_iters_per_substage": t_iters / (3 * K)},
+                 "plain_fp64_omega": {"value": ws * cells * K / (q_ms_all / 1e3) / 1e6, "unit": UNIT,
+                                      "poisson_iters_per_substage": q_iters / (3 * K)}}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
@@ -797,6 +827,7 @@ def run_learned_mixed(args, cfg):
                                "poisson_iters_per_substage": p_iters / (3 * K), "roofline": roof64},
                 "plain_fp64_c1_tol": plain_c1,
                 "extrapolated_mixed_no_network": no_net,
+                "relaxation_tuned": tuned,
                 "speedup_vs_plain_fp64": value / plain_value,
                 "error_vs_plain_fp64": {"rel_l2": err, "residual": ls.residual, "div_l2": l2, "div_linf": linf},
                 "learned": {"corrections": corr, "rejected": u1.rejected - u0.rejected,
@@ -807,7 +838,6 @@ def run_learned_mixed(args, cfg):
                 "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "e2e": e2e_line,
                 "gpu_launches": launches}
         print(json.dumps(line), flush=True)
-    s.close()
     if pg:
         pg.barrier()
         pg.destroy_process_group()

@@ -100,7 +100,9 @@ typedef struct {
     double atol;       /* red-black: absolute floor of ||div u||2, also accepted as converged.
                           < 0 (default): the FP64 round-off level of the divergence,
                           eps*sqrt(nx*ny*nz)*max|u*|*(1/dx+1/dy+1/dz); 0: none */
-    double reserved_d[7];
+    double inner_sor;  /* mixed precision: over-relaxation of the FP32 correction sweeps
+                          (the outer FP64 test is unchanged); <= 0 (default): sor */
+    double reserved_d[6];
 } mdx_solver_opts_t;
 
 /* Statistics of the last pressure projection. */

@@ -168,6 +168,7 @@ void mdx_default_solver_opts(mdx_solver_opts_t* o) {   // src/modules/pressure_w
     o->check_every = 10;
     o->precision = MDX_PREC_FP64;
     o->atol = -1.0;
+    o->inner_sor = 0.0;
 }
 
 int mdx_create(int device, const mdx_grid_t* g, const mdx_bc_t* bc, mdx_ctx_t** out) {

@@ -184,6 +184,8 @@ struct Reader {
             rd_real(value, &o->tol, line);
         } else if (key == "omega" || key == "sor") {
             rd_real(value, &o->sor, line);
+        } else if (key == "inner_omega" || key == "inner_sor") {
+            rd_real(value, &o->inner_sor, line);
         } else if (key == "max_iter") {
             rd_int(value, &o->max_iter, line);
         } else if (key == "check_every") {

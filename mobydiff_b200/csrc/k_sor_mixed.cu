@@ -274,7 +274,8 @@ int mdx_k_projection_redblack_mixed(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t
     mixed_params P{(float)idx, (float)idy, (float)idz, (float)(1.0 / dg)};
     const int nbt = (int)std::min<long long>(((long long)d.nxp * d.nyp + 255) / 256, 1024);
     MDX_LAUNCH(ctx, MDX_T_OTHER, "mixed tables", k_mixed_tables, nbt, 256, 0, d, py, idx * idx, idy * idy, idz * idz,
-               o.sor, ctx->mu, ctx->mu_mode == MU_PLANE ? 1 : 0, ctx->mx_mu, ctx->mx_fac);
+               o.inner_sor > 0.0 ? o.inner_sor : o.sor, ctx->mu, ctx->mu_mode == MU_PLANE ? 1 : 0, ctx->mx_mu,
+               ctx->mx_fac);
     MDX_TRY(mdx_reduce_init(ctx));
 
     auto residual = [&](double* l2, double* umax) -> int {

@@ -31,7 +31,8 @@ module mdx_bindings
         integer(C_INT) :: sor_variant, sor_kz
         integer(C_INT) :: reserved_i(5)
         real(C_DOUBLE) :: atol
-        real(C_DOUBLE) :: reserved_d(7)
+        real(C_DOUBLE) :: inner_sor
+        real(C_DOUBLE) :: reserved_d(6)
     end type mdx_solver_opts_t
 
     type, bind(C) :: mdx_solve_stats_t
