@@ -54,9 +54,10 @@ CONFIGS = {
     "c1-plain": dict(C1_GEOM, workload="wavy-wall IBM channel 256x128x128, FP64 red-black SOR omega=1.7 to residual "
                                        "1e-10", tol=1e-10, method="plain"),
     "c4": dict(workload="ensemble of 64 wavy-wall IBM channels, nx,nz in 32..128 and ny in 32..96 (multiples of 16), "
-                         "Re U(1000,5000), A U(0,0.1), FP64 red-black SOR omega=1.7 to residual 1e-8 from the "
-                         "extrapolated increment; one persistent launch per RK3 substage, CUDA graph, autotuned grid",
-               solver="redblack", sor=1.7, tol=1e-8, check_every=10, members=64, method="ensemble"),
+                         "Re U(1000,5000), A U(0,0.1), red-black SOR omega=1.7 to residual 1e-8 from the extrapolated "
+                         "increment, FP32 sweeps in FP64 defect correction; one persistent launch per RK3 substage, "
+                         "CUDA graph, autotuned launch shape",
+               solver="redblack", sor=1.7, tol=1e-8, check_every=10, members=64, method="ensemble", mixed=True),
     "c0": dict(workload="periodic channel 64^3, FP64 FFT+Thomas", nx=64, ny=64, nz=64, lx=2 * math.pi, ly=2.0,
                lz=math.pi, re=2000.0, dt=1e-3, solver="fft", ibm="none", amp=0.0, method="plain"),
     "c2": dict(workload="channel 512x256x256 (Lx 4pi, Lz 2pi, Re 5000): FP32 FFT + Thomas inside FP64 defect "
@@ -492,8 +493,9 @@ def run_ensemble(args, cfg):
     mems = ensemble_members(M, cfg["members"])
     sizes = [m.nx * m.ny * m.nz for m in mems]
     cells = sum(sizes)
+    prec = M.PREC_MIXED if cfg.get("mixed") else M.PREC_FP64
     opts = M.make_solver_opts(M.SOLVER_REDBLACK, sor=cfg["sor"], tol=cfg["tol"], check_every=cfg["check_every"],
-                              max_iter=400000)
+                              max_iter=400000, precision=prec)
     W, K = args.warmup, args.steps
     E = M.Ensemble(mems, opts, device)
     E.set_guess(M.GUESS_EXTRAPOLATED)
@@ -517,9 +519,11 @@ def run_ensemble(args, cfg):
     if pg:
         ms_all = max_over_ranks(ms, pg)
     value = ws * cells * K / (ms_all / 1e3) / 1e6
-    # red-black path algorithmic bytes (FP64): 3 x 104 B per cell per step for
-    # the predictor and projection set-up, 64 B per cell per red+black iteration
-    alg = sum(n * (3.0 * 104.0 * K + 64.0 * it) for n, it in zip(sizes, it_m))
+    # red-black path algorithmic bytes: 3 x 104 B per cell per step for the
+    # predictor and projection set-up, 64 B (FP64) or 32 B (FP32 sweeps) per
+    # cell per red+black iteration
+    per_it = 32.0 if cfg.get("mixed") else 64.0
+    alg = sum(n * (3.0 * 104.0 * K + per_it * it) for n, it in zip(sizes, it_m))
     peak, peak_kind = _peaks()
     achieved = alg / (ms / 1e3) / 1e9
     roofline = {"kernel": "k_ens_substage (whole substage)", "bound": "hbm", "achieved": achieved, "peak": peak,
@@ -564,11 +568,12 @@ def run_ensemble(args, cfg):
             seq_iters += it1
             s.close()
         seq = {"value": ws * cells * K / (seq_ms / 1e3) / 1e6, "unit": UNIT, "ms_per_step": seq_ms / K,
-               "iterations": seq_iters, "ensemble_iterations": iters}
+               "iterations": seq_iters, "ensemble_iterations": iters, "precision": "same as the ensemble"}
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": W,
                 "ms_per_step": ms_all / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f64", "data": "synthetic: 64 seeded members (SplitMix64 sizes, Re, A, IC seeds)",
+                "dtype": "f64+f32 (FP32 sweeps in FP64 defect correction)" if cfg.get("mixed") else "f64",
+                "data": "synthetic: 64 seeded members (SplitMix64 sizes, Re, A, IC seeds)",
                 "config": {"workload": cfg["workload"], "members": len(mems), "cells": cells, "tol": cfg["tol"],
                            "parallelism": f"replicas x{ws}",
                            "l2": "inputs larger than L2 (64 members' state > 126 MB)"},

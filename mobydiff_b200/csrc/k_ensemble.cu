@@ -26,6 +26,7 @@
 // max_iter.  The grid (threads per block, blocks per SM) comes from a timed
 // autotuner whose choice is cached in a JSON file.
 #include "mdx_cell.cuh"
+#include "mdx_cell32.cuh"
 
 #include <cooperative_groups.h>
 
@@ -70,6 +71,8 @@ struct ens_member {                  // per member, read-only in the kernel
     double *mu;                      // 3 planes of this projection
     double *p0, *guess;
     double* h[3][2];                 // increment history per substage
+    // mixed precision: FP32 corrections and residual (colour-split), FP32 factor planes
+    float *du, *dv, *dw, *dp, *r32, *mu32, *fac32;
 };
 
 struct ens_state {                   // per member, updated in the kernel
@@ -80,6 +83,10 @@ struct ens_state {                   // per member, updated in the kernel
     int last_iters;
     long long iters_total;
     double last_residual;
+    // mixed precision: 0 FP64 residual (after applying the corrections), 1 FP32
+    // sweeps, 2 done; outer FP64 corrections; inner stop state
+    int phase, outer, stale;
+    double e_best, inner_target;
 };
 
 struct ens_list {
@@ -102,6 +109,8 @@ struct ens_args {
     int guess_mode;
     int n_iter, max_iter, check_every;
     double tol, atol;
+    int mixed;                       // FP32 sweeps in FP64 defect correction
+    double inner_sor;                // their over-relaxation
 };
 
 __device__ __forceinline__ double nanmax(double a, double b) { return (a != a || b != b) ? (a + b) : fmax(a, b); }
@@ -316,6 +325,104 @@ __device__ __forceinline__ void sweep_cell(const sweep_view& v, const mdx_bc_dev
     pn[c] = pc;
 }
 
+// ---- mixed precision -------------------------------------------------------
+__device__ __forceinline__ mixed_params mixed_of(const ens_member& M, double dg) {
+    return mixed_params{(float)M.idx, (float)M.idy, (float)M.idz, (float)(1.0 / dg)};
+}
+
+// FP64 residual of cell tile ti into r~ and partials (sum div^2, max|div|, max|u|).
+__device__ void mixed_residual_tile(const ens_args& A, int ti) {
+    const int2 T = A.cell.t[ti];
+    const ens_member& M = A.mem[T.x];
+    const mdx_dims d = M.d;
+    const double *un = M.un, *vn = M.vn, *wn = M.wn;
+    float* r = M.r32;
+    const double idx = M.idx, idy = M.idy, idz = M.idz;
+    const fdiv32 fx = M.fx, fy = M.fy;
+    double s = 0.0, m = 0.0, um = 0.0;
+    for (int e = threadIdx.x; e < ETILE; e += blockDim.x) {
+        const unsigned t = (unsigned)T.y + e;
+        if (t >= (unsigned)d.nint) break;
+        const unsigned q = fq(t, fx);
+        const int i = (int)(t - q * fx.d) + 1;
+        const unsigned kq = fq(q, fy);
+        const int j = (int)(q - kq * fy.d) + 1;
+        const int k = (int)kq + 1;
+        const double dv = mixed_residual_cell<0>(d, idx, idy, idz, i, j, k, un, vn, wn, r);
+        const long long c = pidx(d, i, j, k);
+        s += dv * dv;
+        m = nanmax(m, fabs(dv));
+        um = nanmax(um, nanmax(fabs(un[c]), nanmax(fabs(vn[c]), fabs(wn[c]))));
+    }
+    block_reduce3(s, m, um);
+    if (threadIdx.x == 0) {
+        A.part[3 * ti] = s;
+        A.part[3 * ti + 1] = m;
+        A.part[3 * ti + 2] = um;
+    }
+    __syncthreads();
+}
+
+// FP32 correction residual of cell tile ti: partials of sum e^2 and max|e|.
+__device__ void corr_residual_tile(const ens_args& A, int ti) {
+    const int2 T = A.cell.t[ti];
+    const ens_member& M = A.mem[T.x];
+    const mdx_dims d = M.d;
+    const mixed_params P = mixed_of(M, dg_of(A, M));
+    const fdiv32 fx = M.fx, fy = M.fy;
+    double s = 0.0, m = 0.0, z = 0.0;
+    for (int e = threadIdx.x; e < ETILE; e += blockDim.x) {
+        const unsigned t = (unsigned)T.y + e;
+        if (t >= (unsigned)d.nint) break;
+        const unsigned q = fq(t, fx);
+        const int i = (int)(t - q * fx.d) + 1;
+        const unsigned kq = fq(q, fy);
+        const int j = (int)(q - kq * fy.d) + 1;
+        const int k = (int)kq + 1;
+        const float ev = corr_residual_cell<0>(d, P, i, j, k, M.du, M.dv, M.dw, M.r32);
+        s += (double)ev * (double)ev;
+        m = nanmax(m, fabs((double)ev));
+    }
+    block_reduce3(s, m, z);
+    if (threadIdx.x == 0) {
+        A.part[3 * ti] = s;
+        A.part[3 * ti + 1] = m;
+        A.part[3 * ti + 2] = 0.0;
+    }
+    __syncthreads();
+}
+
+// One FP32 colour sweep of sweep tile ti.
+__device__ __forceinline__ void sweep32_tile(const ens_args& A, int parity, int ti) {
+    const int2 T = A.half.t[ti];
+    const ens_member& M = A.mem[T.x];
+    const mdx_dims d = M.d;
+    const mixed_params P = mixed_of(M, dg_of(A, M));
+    const fdiv32 fy = M.fy, fh = M.fh;
+    float *du = M.du, *dv = M.dv, *dw = M.dw, *dp = M.dp;
+    const float *r = M.r32, *mu32 = M.mu32, *fac32 = M.fac32;
+    const unsigned nh = (unsigned)((d.nx / 2) * d.ny * d.nz);
+    for (int e = threadIdx.x; e < ETILE; e += blockDim.x) {
+        const unsigned t = (unsigned)T.y + e;
+        if (t >= nh) break;
+        const unsigned q = fq(t, fh);
+        const int ni = (int)(t - q * fh.d) + 1;
+        const unsigned kq = fq(q, fy);
+        const int j = (int)(q - kq * fy.d) + 1;
+        const int kk = (int)kq + 1;
+        const int k = parity ? d.nz + 1 - kk : kk;
+        const int i = 1 + ((j + k + parity) & 1) + 2 * (ni - 1);
+        sweep32_cell<0>(d, P, i, j, k, du, dv, dw, dp, r, mu32, fac32);
+    }
+}
+
+__device__ void sweep32_active(const ens_args& A, int parity) {
+    const int* pref = A.act;
+    const int total = pref[A.nmem];
+    for (int vt = blockIdx.x; vt < total; vt += gridDim.x)
+        sweep32_tile(A, parity, active_tile(pref, A.half_begin, A.nmem, vt).y);
+}
+
 __device__ __forceinline__ mdx_sor_params proj_params(const ens_member& M, double dg) {
     mdx_sor_params p = M.sp;
     p.idt = 1.0 / dg;
@@ -487,8 +594,21 @@ __global__ void __launch_bounds__(MAX_THREADS, MINB) k_ens_substage(ens_args A) 
         }
     grid.sync();
 
-    // ---- ||div u*||, max|u*|, target ----
+    // ---- ||div u*||, max|u*|, target (and the FP32 factor planes) ----
     if (meas) {
+        if (A.mixed)
+            for (int ti = blockIdx.x; ti < A.plane.n; ti += gridDim.x) {
+                const int2 T = A.plane.t[ti];
+                const ens_member& M = A.mem[T.x];
+                const long long np = (long long)M.d.nxp * M.d.nyp;
+                const double om = A.inner_sor > 0.0 ? A.inner_sor : M.sp.sor;
+                for (int e = threadIdx.x; e < ETILE; e += blockDim.x) {
+                    const long long t = (long long)T.y + e;
+                    if (t >= np) break;
+                    mixed_tables_elem(M.d, 0, M.sp.idx2, M.sp.idy2, M.sp.idz2, om, M.ibm ? M.mu : nullptr, t, M.mu32,
+                                      M.fac32);
+                }
+            }
         residual_tiles(A, [](int) { return true; });
         grid.sync();
         for (int m = blockIdx.x; m < A.nmem; m += gridDim.x) {
@@ -572,6 +692,95 @@ __global__ void __launch_bounds__(MAX_THREADS, MINB) k_ens_substage(ens_args A) 
                 grid.sync();
             }
         }
+    } else if (A.mixed) {
+        // FP32 sweeps in FP64 defect correction (k_sor_mixed.cu's loop), each
+        // member on its own: phase 0 applies its corrections (none on the first
+        // round) and takes the FP64 residual r~, phase 1 sweeps until the FP32
+        // correction residual meets max(target, 1e-5 r) or stagnates
+        if (blockIdx.x == 0)
+            for (int m = threadIdx.x; m < A.nmem; m += blockDim.x) {
+                ens_state& S = A.st[m];
+                S.phase = S.active ? 0 : 2;
+                S.outer = 0;
+                S.it = 0;
+                S.active = 0;   // sweeping members
+            }
+        grid.sync();
+        const int max_rounds = A.max_iter / max(A.check_every, 1) + 64;
+        for (int round = 0; round < max_rounds; ++round) {
+            pad_tiles(A, [&](int m, const ens_member& M, long long t) {
+                const ens_state& S = A.st[m];
+                if (S.phase == 0 && S.outer > 0) mixed_apply_elem(M.d, t, M.un, M.vn, M.wn, M.pn, M.du, M.dv, M.dw, M.dp);
+            });
+            grid.sync();
+            for (int ti = blockIdx.x; ti < A.cell.n; ti += gridDim.x)
+                if (A.st[A.cell.t[ti].x].phase == 0) mixed_residual_tile(A, ti);
+            grid.sync();
+            for (int m = blockIdx.x; m < A.nmem; m += gridDim.x) {
+                if (A.st[m].phase != 0) continue;
+                double s2, um;
+                member_sums(A, m, s2, um);
+                if (threadIdx.x == 0) {
+                    ens_state& S = A.st[m];
+                    S.r = sqrt(s2);
+                    if (!isfinite(S.r)) {
+                        S.status = MDX_ERR_NONFINITE;
+                        S.phase = 2;
+                    } else if (S.r <= S.target) {
+                        S.status = MDX_OK;
+                        S.phase = 2;
+                    } else if (S.outer >= 16 || S.it >= A.max_iter) {
+                        S.phase = 2;   // NOT_CONVERGED
+                    } else {
+                        S.outer++;
+                        S.inner_target = fmax(S.target, 1e-5 * S.r);
+                        S.e_best = S.r;
+                        S.stale = 0;
+                        S.phase = 1;
+                    }
+                    S.active = S.phase == 1;
+                }
+                __syncthreads();
+            }
+            grid.sync();
+            compact_active(A);
+            grid.sync();
+            if (A.act[A.nmem] == 0) break;   // every member done
+            const int mm = A.check_every;
+            for (int q = 0; q < mm; ++q)
+                for (int parity = 0; parity < 2; ++parity) {
+                    sweep32_active(A, parity);
+                    grid.sync();
+                }
+            for (int ti = blockIdx.x; ti < A.cell.n; ti += gridDim.x)
+                if (A.st[A.cell.t[ti].x].phase == 1) corr_residual_tile(A, ti);
+            grid.sync();
+            for (int m = blockIdx.x; m < A.nmem; m += gridDim.x) {
+                if (A.st[m].phase != 1) continue;
+                double s2, um;
+                member_sums(A, m, s2, um);
+                if (threadIdx.x == 0) {
+                    ens_state& S = A.st[m];
+                    const double e = sqrt(s2);
+                    S.it += mm;
+                    bool stop = !isfinite(e) || e <= S.inner_target || S.it >= A.max_iter;
+                    if (!stop) {
+                        if (e < 0.999 * S.e_best) {
+                            S.e_best = e;
+                            S.stale = 0;
+                        } else if (++S.stale >= 20) {
+                            stop = true;   // FP32 stagnation
+                        }
+                    }
+                    if (stop) S.phase = 0;
+                }
+                __syncthreads();
+            }
+            grid.sync();
+        }
+        if (blockIdx.x == 0)
+            for (int m = threadIdx.x; m < A.nmem; m += blockDim.x) A.st[m].active = 0;
+        grid.sync();
     } else {
         compact_active(A);
         grid.sync();
@@ -617,7 +826,7 @@ __global__ void __launch_bounds__(MAX_THREADS, MINB) k_ens_substage(ens_args A) 
     if (blockIdx.x == 0)
         for (int m = threadIdx.x; m < A.nmem; m += blockDim.x) {
             ens_state& S = A.st[m];
-            const int iters = meas ? S.it : A.n_iter;
+            const int iters = meas ? S.it : A.n_iter;   // mixed: FP32 iterations
             S.last_iters = iters;
             S.iters_total += iters;
             S.last_residual = meas ? (S.r0 > 0.0 ? S.r / S.r0 : 0.0) : 0.0;
@@ -807,6 +1016,8 @@ ens_args make_args(mdx_ensemble_t* E, int s, int momentum) {
     A.check_every = E->opts.check_every;
     A.tol = E->opts.tol;
     A.atol = E->opts.atol;
+    A.mixed = E->opts.precision == MDX_PREC_MIXED && E->opts.tol > 0.0;
+    A.inner_sor = E->opts.inner_sor;
     return A;
 }
 
@@ -974,7 +1185,8 @@ int mdx_ensemble_create(int device, int n, const mdx_member_t* members, const md
     if (opts) o = *opts;
     else mdx_default_solver_opts(&o);
     if (o.solver != MDX_SOLVER_REDBLACK) return mdx_fail(nullptr, MDX_ERR_ARG, "the ensemble runs the red-black solver");
-    if (o.precision != MDX_PREC_FP64) return mdx_fail(nullptr, MDX_ERR_ARG, "the ensemble runs FP64 sweeps");
+    if (o.precision != MDX_PREC_FP64 && o.precision != MDX_PREC_MIXED)
+        return mdx_fail(nullptr, MDX_ERR_ARG, "unknown precision %d", o.precision);
     if (o.check_every < 1) o.check_every = 1;
     if (o.max_iter < 1) o.max_iter = 1;
     if (o.n_iter < 0) return mdx_fail(nullptr, MDX_ERR_ARG, "n_iter must be >= 0");
@@ -1059,6 +1271,12 @@ int mdx_ensemble_create(int device, int n, const mdx_member_t* members, const md
         if (rc == MDX_OK) rc = ealloc(E, &M.guess, ni);
         for (int s = 0; s < 3 && rc == MDX_OK; ++s)
             for (int b = 0; b < 2 && rc == MDX_OK; ++b) rc = ealloc(E, &M.h[s][b], ni, true, true);
+        if (o.precision == MDX_PREC_MIXED) {   // colour-split FP32 arrays (npad elements), factor planes
+            float** f32[5] = {&M.du, &M.dv, &M.dw, &M.dp, &M.r32};
+            for (int t = 0; t < 5 && rc == MDX_OK; ++t) rc = ealloc(E, f32[t], np, true, t < 4);
+            if (rc == MDX_OK) rc = ealloc(E, &M.mu32, 3 * pl);
+            if (rc == MDX_OK) rc = ealloc(E, &M.fac32, pl);
+        }
         if (rc == MDX_OK && q.amp > 0.0) {
             // wavy walls y0 + A sin(2 pi x / (Lx/2)) and y0 + 2 + ..., y0 = (Ly - 2)/2
             std::vector<double> cu(np), cv(np), cw(np);
@@ -1274,7 +1492,7 @@ int mdx_ensemble_member_stats(mdx_ensemble_t* E, int m, mdx_solve_stats_t* st, l
         st->residual = S.last_residual;
         st->residual0 = S.r0;
         st->atol = S.atol;
-        st->variant = 1;
+        st->variant = E->opts.precision == MDX_PREC_MIXED && E->opts.tol > 0.0 ? 100 + S.outer : 1;
         st->guessed = S.guessed;
     }
     if (iters_total) *iters_total = S.iters_total;

@@ -17,7 +17,7 @@
 // Neumann 0 (the channel), where the correction equations are exactly the
 // homogeneous ones (the wall faces v(1), v(ny+1) stay 0); IBM factors 1 or
 // z-invariant.  Other boundary sets run the FP64 path.
-#include "mdx_internal.cuh"
+#include "mdx_cell32.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -25,26 +25,6 @@
 namespace {
 
 enum { MU_ONE = 0, MU_PLANE = 1, MU_FULL = 2 };   // the IBM-factor modes of k_sor.cu
-
-struct mixed_params {
-    float idx, idy, idz, idt;
-};
-
-// Colour-split layout of the FP32 arrays (du, dv, dw, dp, r): element
-// (i, j, k) of the padded grid lives in half (i + j + k) & 1 at
-// (k (ny+2) + j) (nx+2)/2 + i/2, so the cells of one colour in a row -- and
-// the faces they own or share -- are consecutive: every access of a colour
-// sweep is unit-stride.  A face belongs to the cell on its high side
-// (u(i) to cell i).  nx is even, so (nx+2)/2 is whole.
-__device__ __forceinline__ long long cidx(const mdx_dims& d, int i, int j, int k) {
-    const int hx = d.nxp >> 1;
-    return ((i + j + k) & 1) * ((long long)hx * d.nyp * d.nzp) + ((long long)k * d.nyp + j) * hx + (i >> 1);
-}
-// (i, j) planes of the IBM factors and sweep factors split by the parity of i.
-__device__ __forceinline__ int pidx2(const mdx_dims& d, int i, int j) {
-    const int hx = d.nxp >> 1;
-    return (i & 1) * (hx * d.nyp) + j * hx + (i >> 1);
-}
 
 __device__ inline double nanmax2(double a, double b) { return (a != a || b != b) ? (a + b) : fmax(a, b); }
 
@@ -83,17 +63,11 @@ k_mixed_residual(mdx_dims d, double idx, double idy, double idz, const double* _
         const long long rr = t / d.nx;
         const int j = (int)(rr % d.ny) + 1;
         const int k = (int)(rr / d.ny) + 1;
-        const int ip = i == d.nx ? 1 : i + 1;
-        const int jp = (PY && j == d.ny) ? 1 : j + 1;
-        const int kp = k == d.nz ? 1 : k + 1;
         const long long c = pidx(d, i, j, k);
-        const double uc = __ldg(u + c), vc = __ldg(v + c), wc = __ldg(w + c);
-        const double dv = (__ldg(u + pidx(d, ip, j, k)) - uc) * idx + (__ldg(v + pidx(d, i, jp, k)) - vc) * idy +
-                          (__ldg(w + pidx(d, i, j, kp)) - wc) * idz;
-        r[cidx(d, i, j, k)] = (float)dv;
+        const double dv = mixed_residual_cell<PY>(d, idx, idy, idz, i, j, k, u, v, w, r);
         s += dv * dv;
         m = nanmax2(m, fabs(dv));
-        um = nanmax2(um, nanmax2(fabs(uc), nanmax2(fabs(vc), fabs(wc))));
+        um = nanmax2(um, nanmax2(fabs(__ldg(u + c)), nanmax2(fabs(__ldg(v + c)), fabs(__ldg(w + c)))));
     }
     block_reduce3(s, m, um);
     if (threadIdx.x == 0) {
@@ -114,13 +88,7 @@ k_mixed_corr_residual(mdx_dims d, mixed_params P, const float* __restrict__ du, 
         const long long rr = t / d.nx;
         const int j = (int)(rr % d.ny) + 1;
         const int k = (int)(rr / d.ny) + 1;
-        const int ip = i == d.nx ? 1 : i + 1;
-        const int jp = (PY && j == d.ny) ? 1 : j + 1;
-        const int kp = k == d.nz ? 1 : k + 1;
-        const long long c = cidx(d, i, j, k);
-        const float e = __ldg(r + c) + (__ldg(du + cidx(d, ip, j, k)) - __ldg(du + c)) * P.idx +
-                        (__ldg(dv + cidx(d, i, jp, k)) - __ldg(dv + c)) * P.idy +
-                        (__ldg(dw + cidx(d, i, j, kp)) - __ldg(dw + c)) * P.idz;
+        const float e = corr_residual_cell<PY>(d, P, i, j, k, du, dv, dw, r);
         s += (double)e * (double)e;
         m = nanmax2(m, fabs((double)e));
     }
@@ -138,32 +106,8 @@ __global__ void k_mixed_tables(mdx_dims d, int py, double idx2, double idy2, dou
                                const double* __restrict__ mu, int plane_mu, float* __restrict__ mu32,
                                float* __restrict__ fac32) {
     const long long np = (long long)d.nxp * d.nyp;
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < np; t += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(t % d.nxp), j = (int)(t / d.nxp);
-        double mu_u = 1.0, mu_v = 1.0, mu_w = 1.0;
-        if (plane_mu) {
-            mu_u = mu[t];
-            mu_v = mu[np + t];
-            mu_w = mu[2 * np + t];
-        }
-        const int o = pidx2(d, i, j);
-        mu32[o] = (float)mu_u;
-        mu32[np + o] = (float)mu_v;
-        mu32[2 * np + o] = (float)mu_w;
-        double f = 0.0;
-        if (i >= 1 && i <= d.nx && j >= 1 && j <= d.ny) {
-            const int ip = i == d.nx ? 1 : i + 1;
-            const int jp = (py && j == d.ny) ? 1 : j + 1;
-            double mu_uip = 1.0, mu_vjp = 1.0;
-            if (plane_mu) {
-                mu_uip = mu[ip + (long long)d.nxp * j];
-                mu_vjp = mu[np + i + (long long)d.nxp * jp];
-            }
-            const double denom = (mu_u + mu_uip) * idx2 + (mu_w + mu_w) * idz2 + (mu_v + mu_vjp) * idy2;
-            f = -sor / denom;
-        }
-        fac32[o] = (float)f;
-    }
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < np; t += (long long)gridDim.x * blockDim.x)
+        mixed_tables_elem(d, py, idx2, idy2, idz2, sor, plane_mu ? mu : nullptr, t, mu32, fac32);
 }
 
 // One FP32 colour sweep of the correction (periodic x and z), on the
@@ -176,50 +120,18 @@ k_sor_sweep32(mdx_dims d, mixed_params P, int parity, int reverse, float* __rest
     const int ni = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     const int kk = blockIdx.z * blockDim.z + threadIdx.z + 1;
-    const int nx = d.nx, ny = d.ny, nz = d.nz;
-    if (ni > nx / 2 || j > ny || kk > nz) return;
-    const int k = reverse ? nz + 1 - kk : kk;
-    const int jp = (PY && j == ny) ? 1 : j + 1;
-    const int kp = (k == nz) ? 1 : k + 1;
+    if (ni > d.nx / 2 || j > d.ny || kk > d.nz) return;
+    const int k = reverse ? d.nz + 1 - kk : kk;
     const int i = 1 + ((j + k + parity) & 1) + 2 * (ni - 1);
-    const int ip = (i == nx) ? 1 : i + 1;
-    const int np = d.nxp * d.nyp;
-    const int q = pidx2(d, i, j);
-    const long long c = cidx(d, i, j, k), cip = cidx(d, ip, j, k), cjp = cidx(d, i, jp, k), ckp = cidx(d, i, j, kp);
-    const float mu_u_i = __ldg(mu32 + q), mu_u_ip = __ldg(mu32 + pidx2(d, ip, j));
-    const float mu_v_j = __ldg(mu32 + np + q), mu_v_jp = __ldg(mu32 + np + pidx2(d, i, jp));
-    const float mu_w = __ldg(mu32 + 2 * np + q);
-    const float u_i = du[c], u_ip = du[cip], v_j = dv[c], v_jp = dv[cjp], w_k = dw[c], w_kp = dw[ckp];
-    const float div = __ldg(r + c) + (u_ip - u_i) * P.idx + (v_jp - v_j) * P.idy + (w_kp - w_k) * P.idz;
-    const float phi = div * __ldg(fac32 + q);
-    dp[c] += phi * P.idt;
-    du[c] = u_i - phi * P.idx * mu_u_i;
-    du[cip] = u_ip + phi * P.idx * mu_u_ip;
-    if (PY || j > 1) dv[c] = v_j - phi * P.idy * mu_v_j;         // wall face v(1) stays 0
-    if (PY || j < ny) dv[cjp] = v_jp + phi * P.idy * mu_v_jp;    // wall face v(ny+1) stays 0
-    dw[c] = w_k - phi * P.idz * mu_w;
-    dw[ckp] = w_kp + phi * P.idz * mu_w;
+    sweep32_cell<PY>(d, P, i, j, k, du, dv, dw, dp, r, mu32, fac32);
 }
 
 // u += du, v += dv, w += dw, p += dp over the padded arrays; corrections reset.
 __global__ void k_mixed_apply(mdx_dims d, double* __restrict__ u, double* __restrict__ v, double* __restrict__ w,
                               double* __restrict__ p, float* __restrict__ du, float* __restrict__ dv,
                               float* __restrict__ dw, float* __restrict__ dp) {
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < d.npad; t += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(t % d.nxp);
-        const long long rr = t / d.nxp;
-        const int j = (int)(rr % d.nyp);
-        const int k = (int)(rr / d.nyp);
-        const long long c = cidx(d, i, j, k);
-        u[t] += (double)du[c];
-        v[t] += (double)dv[c];
-        w[t] += (double)dw[c];
-        p[t] += (double)dp[c];
-        du[c] = 0.f;
-        dv[c] = 0.f;
-        dw[c] = 0.f;
-        dp[c] = 0.f;
-    }
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < d.npad; t += (long long)gridDim.x * blockDim.x)
+        mixed_apply_elem(d, t, u, v, w, p, du, dv, dw, dp);
 }
 
 bool mixed_supported(const mdx_ctx_t* ctx) {

@@ -128,3 +128,32 @@ def test_ensemble_argument_checks():
             E.config(100)
         with pytest.raises(M.MdxError):
             E.set_guess(M.GUESS_LEARNED)
+
+
+def test_mixed_precision_members_match_single_channels():
+    """FP32 sweeps in FP64 defect correction inside the persistent kernel:
+    each member lands within the solve tolerance of the single-context mixed
+    path and of the FP64 ensemble (the FP32 arithmetic is not bit-equal: the
+    ensemble file is built without FMA contraction)."""
+    mix = M.make_solver_opts(M.SOLVER_REDBLACK, sor=1.7, tol=1e-8, check_every=10, max_iter=200000,
+                             precision=M.PREC_MIXED)
+    f64 = M.make_solver_opts(M.SOLVER_REDBLACK, sor=1.7, tol=1e-8, check_every=10, max_iter=200000)
+    mems = _members()
+    with M.Ensemble(mems, mix) as E, M.Ensemble(mems, f64) as F:
+        for X in (E, F):
+            X.set_guess(M.GUESS_EXTRAPOLATED)
+            X.ic()
+        ie, i_f = E.step(4), F.step(4)
+        print("iterations: ensemble mixed", ie, "ensemble fp64", i_f)
+        for q, m in enumerate(mems):
+            st, _ = E.member_stats(q)
+            assert st.status == 0 and st.variant > 100
+            assert st.residual <= 1e-8 * 1.0000001 or st.residual * st.residual0 <= st.atol * 1.0000001
+            with _single(m, mix, M.GUESS_EXTRAPOLATED) as s:
+                s.step(4)
+                for other in (s.get, lambda n: F.get(q, n)):
+                    num = sum(float(np.sum((E.get(q, n) - other(n)) ** 2)) for n in ("un", "vn", "wn"))
+                    den = sum(float(np.sum(other(n) ** 2)) for n in ("un", "vn", "wn"))
+                    assert (num / den) ** 0.5 <= 1e-6, q          # the velocity vector
+                    for n in ("un", "vn", "wn"):                  # each component, v and w of small norm
+                        assert rel_l2(E.get(q, n), other(n)) <= 1e-5, (q, n)
