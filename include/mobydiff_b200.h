@@ -96,7 +96,12 @@ typedef struct {
                           launch per colour; 2 fused red+black pass, 32x8 tiles;
                           3 fused pass, 32x16 tiles (fused: periodic x and z only) */
     int sor_kz;        /* z planes per block of the fused pass (0: default 16) */
-    int reserved_i[5];
+    int check_mode;    /* red-black, tol > 0: 0 (default) residual checks at multiples of check_every,
+                          up to 8 blocks apart while the residual falls at a steady rate that
+                          puts the target more than twice as far; 1: every check_every
+                          iterations (the stop is then the first multiple of check_every that
+                          meets the target) */
+    int reserved_i[4];
     double atol;       /* red-black: absolute floor of ||div u||2, also accepted as converged.
                           < 0 (default): the FP64 round-off level of the divergence,
                           eps*sqrt(nx*ny*nz)*max|u*|*(1/dx+1/dy+1/dz); 0: none */

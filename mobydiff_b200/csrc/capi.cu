@@ -196,6 +196,7 @@ int mdx_create(int device, const mdx_grid_t* g, const mdx_bc_t* bc, mdx_ctx_t** 
     d.nx = g->nx; d.ny = g->ny; d.nz = g->nz;
     d.nxp = g->nx + 2; d.nyp = g->ny + 2; d.nzp = g->nz + 2;
     d.nxh = g->nx / 2 + 1;
+    d.hs = split_stride(g->nx);
     d.npad = npad;
     d.nint = (long long)g->nx * g->ny * g->nz;
     d.nspec = (long long)d.nxh * g->nz * g->ny;

@@ -186,6 +186,10 @@ struct Reader {
             rd_real(value, &o->sor, line);
         } else if (key == "inner_omega" || key == "inner_sor") {
             rd_real(value, &o->inner_sor, line);
+        } else if (key == "check_mode" || key == "residual_checks") {
+            if (v == "adaptive" || v == "0") o->check_mode = 0;
+            else if (v == "fixed" || v == "every" || v == "1") o->check_mode = 1;
+            else warn("b200 residual_checks must be adaptive or fixed", line);
         } else if (key == "max_iter") {
             rd_int(value, &o->max_iter, line);
         } else if (key == "check_every") {

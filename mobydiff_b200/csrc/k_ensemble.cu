@@ -1238,6 +1238,7 @@ int mdx_ensemble_create(int device, int n, const mdx_member_t* members, const md
         d.nx = q.nx; d.ny = q.ny; d.nz = q.nz;
         d.nxp = q.nx + 2; d.nyp = q.ny + 2; d.nzp = q.nz + 2;
         d.nxh = q.nx / 2 + 1;
+        d.hs = split_stride(q.nx);
         d.npad = (long long)d.nxp * d.nyp * d.nzp;
         d.nint = (long long)q.nx * q.ny * q.nz;
         d.nspec = 0;
@@ -1271,11 +1272,12 @@ int mdx_ensemble_create(int device, int n, const mdx_member_t* members, const md
         if (rc == MDX_OK) rc = ealloc(E, &M.guess, ni);
         for (int s = 0; s < 3 && rc == MDX_OK; ++s)
             for (int b = 0; b < 2 && rc == MDX_OK; ++b) rc = ealloc(E, &M.h[s][b], ni, true, true);
-        if (o.precision == MDX_PREC_MIXED) {   // colour-split FP32 arrays (npad elements), factor planes
+        if (o.precision == MDX_PREC_MIXED) {   // colour-split FP32 arrays, factor planes
+            const size_t ns = (size_t)split_elems(d), ps = (size_t)split_plane_elems(d);
             float** f32[5] = {&M.du, &M.dv, &M.dw, &M.dp, &M.r32};
-            for (int t = 0; t < 5 && rc == MDX_OK; ++t) rc = ealloc(E, f32[t], np, true, t < 4);
-            if (rc == MDX_OK) rc = ealloc(E, &M.mu32, 3 * pl);
-            if (rc == MDX_OK) rc = ealloc(E, &M.fac32, pl);
+            for (int t = 0; t < 5 && rc == MDX_OK; ++t) rc = ealloc(E, f32[t], ns, true, t < 4);
+            if (rc == MDX_OK) rc = ealloc(E, &M.mu32, 3 * ps, true);
+            if (rc == MDX_OK) rc = ealloc(E, &M.fac32, ps, true);
         }
         if (rc == MDX_OK && q.amp > 0.0) {
             // wavy walls y0 + A sin(2 pi x / (Lx/2)) and y0 + 2 + ..., y0 = (Ly - 2)/2

@@ -594,23 +594,27 @@ int mdx_k_projection_redblack(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t* st) 
         } else {
             int it = 0;
             s.status = MDX_NOT_CONVERGED;
+            mdx_check_schedule cs;
+            cs.start(o.check_every, o.check_mode, r);
+            int block = cs.every;
             while (it < o.max_iter) {
-                const int m = std::min(o.check_every, o.max_iter - it);
+                const int m = std::min(block, o.max_iter - it);
                 const int v = pick();
-                const bool timing_block = want == MDX_SORV_AUTO && ctx->sor_tuned == 0 && m == o.check_every;
+                const bool timing_block = want == MDX_SORV_AUTO && ctx->sor_tuned == 0;
                 if (timing_block) MDX_CUDA(ctx, cudaEventRecord(ctx->tune_ev[0], ctx->stream));
                 for (int q = 0; q < m; ++q) MDX_TRY(sor_iterate(ctx, p, v));
                 if (timing_block) MDX_CUDA(ctx, cudaEventRecord(ctx->tune_ev[1], ctx->stream));
                 it += m;
                 s.variant = v;
                 MDX_TRY(mdx_k_div_norms(ctx, f[MDX_UN], f[MDX_VN], f[MDX_WN], &r, &linf));
-                if (timing_block) {   // the norms synchronised the stream
+                if (timing_block) {   // the norms synchronised the stream; time per iteration
                     float ms = 0.f;
                     if (cudaEventElapsedTime(&ms, ctx->tune_ev[0], ctx->tune_ev[1]) == cudaSuccess)
-                        ctx->sor_tune_ms[v] = ms > 0.f ? ms : 1e-6;
+                        ctx->sor_tune_ms[v] = ms > 0.f ? ms / m : 1e-9;
                 }
                 if (!std::isfinite(r)) { s.status = MDX_ERR_NONFINITE; break; }
                 if (r <= target) { s.status = MDX_OK; break; }
+                block = cs.next(it, r, target);
             }
             s.iterations = it;
             s.residual = r / r0;

@@ -145,27 +145,33 @@ bool mixed_supported(const mdx_ctx_t* ctx) {
            T[bci(2, 0, 0)] == 1 && V[bci(2, 0, 0)] == 0.0 && T[bci(2, 1, 0)] == 1 && V[bci(2, 1, 0)] == 0.0;
 }
 
+// One allocation for the five colour-split FP32 arrays and the tables, each
+// part starting on a 256-byte boundary.
 int mixed_alloc(mdx_ctx_t* ctx) {
     if (ctx->mx_du) return MDX_OK;
-    const size_t n = (size_t)ctx->d.npad, np = (size_t)ctx->d.nxp * ctx->d.nyp;
+    const size_t n = (size_t)split_elems(ctx->d), np = (size_t)split_plane_elems(ctx->d);
+    auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    const size_t arr = up(sizeof(float) * n), mu = up(sizeof(float) * 3 * np), fac = up(sizeof(float) * np);
+    const size_t total = 5 * arr + mu + fac;
+    char* base = nullptr;
+    MDX_CUDA(ctx, cudaMalloc(&base, total));
+    MDX_CUDA(ctx, cudaMemsetAsync(base, 0, total, ctx->stream));
     float** arrs[5] = {&ctx->mx_du, &ctx->mx_dv, &ctx->mx_dw, &ctx->mx_dp, &ctx->mx_r};
-    for (auto a : arrs) {
-        MDX_CUDA(ctx, cudaMalloc(a, sizeof(float) * n));
-        MDX_CUDA(ctx, cudaMemsetAsync(*a, 0, sizeof(float) * n, ctx->stream));
-    }
-    MDX_CUDA(ctx, cudaMalloc(&ctx->mx_mu, sizeof(float) * 3 * np));
-    MDX_CUDA(ctx, cudaMalloc(&ctx->mx_fac, sizeof(float) * np));
+    for (int a = 0; a < 5; ++a) *arrs[a] = reinterpret_cast<float*>(base + a * arr);
+    ctx->mx_mu = reinterpret_cast<float*>(base + 5 * arr);
+    ctx->mx_fac = reinterpret_cast<float*>(base + 5 * arr + mu);
+    ctx->mx_bytes = total;
     return MDX_OK;
 }
+
 
 }  // namespace
 
 void mdx_mixed_free(mdx_ctx_t* ctx) {
+    cudaFree(ctx->mx_du);   // the base of the one allocation
     float** arrs[7] = {&ctx->mx_du, &ctx->mx_dv, &ctx->mx_dw, &ctx->mx_dp, &ctx->mx_r, &ctx->mx_mu, &ctx->mx_fac};
-    for (auto a : arrs) {
-        cudaFree(*a);
-        *a = nullptr;
-    }
+    for (auto a : arrs) *a = nullptr;
+    ctx->mx_bytes = 0;
 }
 
 // Called after u <- u*, the FP64 IBM factors of this projection and any
@@ -249,15 +255,20 @@ int mdx_k_projection_redblack_mixed(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t
             const double inner_target = std::max(target, inner_rel * r);
             double e = r, best = r;
             int stale = 0;
+            mdx_check_schedule cs;
+            cs.start(o.check_every, o.check_mode, r);
+            int block = cs.every;
             while (it < o.max_iter) {
-                const int m = std::min(o.check_every, o.max_iter - it);
+                const int m = std::min(block, o.max_iter - it);
                 MDX_TRY(sweeps(m));
                 it += m;
                 MDX_TRY(corr_residual(&e));
                 if (!std::isfinite(e)) break;
                 if (e <= inner_target) break;
-                if (e < 0.999 * best) { best = e; stale = 0; }
-                else if (++stale >= 20) break;   // FP32 stagnation
+                // FP32 stagnation: less than 0.1 % per check_every iterations for 20 x check_every
+                if (e < std::pow(0.999, (double)m / cs.every) * best) { best = e; stale = 0; }
+                else if ((stale += m) >= 20 * cs.every) break;
+                block = cs.next(it, e, inner_target);
             }
             const long long n = d.npad;
             MDX_LAUNCH(ctx, MDX_T_OTHER, "mixed apply", k_mixed_apply, (int)std::min<long long>((n + 255) / 256, 8192),

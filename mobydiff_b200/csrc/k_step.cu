@@ -226,6 +226,14 @@ __device__ inline void block_reduce3(double& s, double& m, double& u) {
 
 // Divergence with the red-black neighbour rule (periodic wrap to 1):
 // partials of sum(div^2), max|div| and max(|u|,|v|,|w|) over the cells.
+// SPLIT: u, v, w in the colour-split layout (the FP64 sweeps' working copies);
+// the same cells in the same order, so the same sums.
+template <bool SPLIT>
+__device__ __forceinline__ long long lay(const mdx_dims& d, int i, int j, int k) {
+    return SPLIT ? cidx(d, i, j, k) : pidx(d, i, j, k);
+}
+
+template <bool SPLIT>
 __global__ void __launch_bounds__(MDX_RED_THREADS)
 k_div_partials(mdx_dims d, int perx, int pery, int perz, double idx, double idy, double idz,
                const double* __restrict__ u, const double* __restrict__ v, const double* __restrict__ w,
@@ -240,10 +248,11 @@ k_div_partials(mdx_dims d, int perx, int pery, int perz, double idx, double idy,
         const int ip = (perx && i + 1 > d.nx) ? 1 : i + 1;
         const int jp = (pery && j + 1 > d.ny) ? 1 : j + 1;
         const int kp = (perz && k + 1 > d.nz) ? 1 : k + 1;
-        const long long c = pidx(d, i, j, k);
+        const long long c = lay<SPLIT>(d, i, j, k);
         const double uc = __ldg(u + c), vc = __ldg(v + c), wc = __ldg(w + c);
-        const double dv = (__ldg(u + pidx(d, ip, j, k)) - uc) * idx + (__ldg(v + pidx(d, i, jp, k)) - vc) * idy +
-                          (__ldg(w + pidx(d, i, j, kp)) - wc) * idz;
+        const double dv = (__ldg(u + lay<SPLIT>(d, ip, j, k)) - uc) * idx +
+                          (__ldg(v + lay<SPLIT>(d, i, jp, k)) - vc) * idy +
+                          (__ldg(w + lay<SPLIT>(d, i, j, kp)) - wc) * idz;
         s += dv * dv;
         m = nanmax(m, fabs(dv));
         um = nanmax(um, nanmax(fabs(uc), nanmax(fabs(vc), fabs(wc))));
@@ -300,8 +309,9 @@ int mdx_k_div_norms_async(mdx_ctx_t* ctx, const double* u, const double* v, cons
     MDX_TRY(mdx_reduce_init(ctx));
     const mdx_dims& d = ctx->d;
     const int* per = ctx->bc.is_periodic;
-    MDX_LAUNCH(ctx, MDX_T_RESIDUAL, "divergence partials", k_div_partials, ctx->red_blocks, MDX_RED_THREADS, 0, d,
-               per[0], per[1], per[2], 1.0 / ctx->g.dx, 1.0 / ctx->g.dy, 1.0 / ctx->g.dz, u, v, w, ctx->red_part);
+    auto kfn = ctx->split_norms ? k_div_partials<true> : k_div_partials<false>;
+    MDX_LAUNCH(ctx, MDX_T_RESIDUAL, "divergence partials", kfn, ctx->red_blocks, MDX_RED_THREADS, 0, d, per[0],
+               per[1], per[2], 1.0 / ctx->g.dx, 1.0 / ctx->g.dy, 1.0 / ctx->g.dz, u, v, w, ctx->red_part);
     MDX_LAUNCH(ctx, MDX_T_RESIDUAL, "reduce final", k_reduce_final, 1, MDX_RED_THREADS, 0, ctx->red_blocks,
                ctx->red_part, ctx->red_out);
     MDX_CUDA(ctx, cudaMemcpyAsync(ctx->red_host, ctx->red_out, 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));

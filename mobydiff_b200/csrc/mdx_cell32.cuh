@@ -9,22 +9,25 @@ struct mixed_params {
     float idx, idy, idz, idt;
 };
 
-// Colour-split layout of the FP32 arrays (du, dv, dw, dp, r): element
-// (i, j, k) of the padded grid lives in half (i + j + k) & 1 at
-// (k (ny+2) + j) (nx+2)/2 + i/2, so the cells of one colour in a row -- and
-// the faces they own or share -- are consecutive: every access of a colour
-// sweep is unit-stride.  A face belongs to the cell on its high side
-// (u(i) to cell i).  nx is even, so (nx+2)/2 is whole.
-__device__ __forceinline__ long long cidx(const mdx_dims& d, int i, int j, int k) {
-    const int hx = d.nxp >> 1;
-    return ((i + j + k) & 1) * ((long long)hx * d.nyp * d.nzp) + ((long long)k * d.nyp + j) * hx + (i >> 1);
+// The update of one cell from its six faces, its correction dp and its
+// residual r~ (pressure_redblack.f90:117-241 with homogeneous boundary
+// values): phi = fac * (r~ + div), dp += phi/dt_gamma, faces -+ phi/h mu.
+// v_lo / v_hi false keep a wall face v(1) / v(ny+1) at its value (0).
+__device__ __forceinline__ void sweep32_update(const mixed_params& P, float r, float& u_i, float& u_ip, float& v_j,
+                                               float& v_jp, float& w_k, float& w_kp, float& dp, float mu_u_i,
+                                               float mu_u_ip, float mu_v_j, float mu_v_jp, float mu_w, float fac,
+                                               bool v_lo, bool v_hi) {
+    const float ui = u_i, uip = u_ip, vj = v_j, vjp = v_jp, wk = w_k, wkp = w_kp;
+    const float div = r + (uip - ui) * P.idx + (vjp - vj) * P.idy + (wkp - wk) * P.idz;
+    const float phi = div * fac;
+    dp += phi * P.idt;
+    u_i = ui - phi * P.idx * mu_u_i;
+    u_ip = uip + phi * P.idx * mu_u_ip;
+    if (v_lo) v_j = vj - phi * P.idy * mu_v_j;
+    if (v_hi) v_jp = vjp + phi * P.idy * mu_v_jp;
+    w_k = wk - phi * P.idz * mu_w;
+    w_kp = wkp + phi * P.idz * mu_w;
 }
-// (i, j) planes of the IBM factors and sweep factors split by the parity of i.
-__device__ __forceinline__ int pidx2(const mdx_dims& d, int i, int j) {
-    const int hx = d.nxp >> 1;
-    return (i & 1) * (hx * d.nyp) + j * hx + (i >> 1);
-}
-
 
 // One FP32 colour-sweep update of cell (i, j, k) of the correction problem
 // (periodic x and z; y periodic when PY, else walls whose faces v(1),
@@ -38,22 +41,23 @@ __device__ __forceinline__ void sweep32_cell(const mdx_dims& d, const mixed_para
     const int jp = (PY && j == ny) ? 1 : j + 1;
     const int kp = (k == nz) ? 1 : k + 1;
     const int ip = (i == nx) ? 1 : i + 1;
-    const int np = d.nxp * d.nyp;
+    const int np = split_plane_elems(d);
     const int q = pidx2(d, i, j);
     const long long c = cidx(d, i, j, k), cip = cidx(d, ip, j, k), cjp = cidx(d, i, jp, k), ckp = cidx(d, i, j, kp);
     const float mu_u_i = __ldg(mu32 + q), mu_u_ip = __ldg(mu32 + pidx2(d, ip, j));
     const float mu_v_j = __ldg(mu32 + np + q), mu_v_jp = __ldg(mu32 + np + pidx2(d, i, jp));
     const float mu_w = __ldg(mu32 + 2 * np + q);
-    const float u_i = du[c], u_ip = du[cip], v_j = dv[c], v_jp = dv[cjp], w_k = dw[c], w_kp = dw[ckp];
-    const float div = __ldg(r + c) + (u_ip - u_i) * P.idx + (v_jp - v_j) * P.idy + (w_kp - w_k) * P.idz;
-    const float phi = div * __ldg(fac32 + q);
-    dp[c] += phi * P.idt;
-    du[c] = u_i - phi * P.idx * mu_u_i;
-    du[cip] = u_ip + phi * P.idx * mu_u_ip;
-    if (PY || j > 1) dv[c] = v_j - phi * P.idy * mu_v_j;         // wall face v(1) stays 0
-    if (PY || j < ny) dv[cjp] = v_jp + phi * P.idy * mu_v_jp;    // wall face v(ny+1) stays 0
-    dw[c] = w_k - phi * P.idz * mu_w;
-    dw[ckp] = w_kp + phi * P.idz * mu_w;
+    float u_i = du[c], u_ip = du[cip], v_j = dv[c], v_jp = dv[cjp], w_k = dw[c], w_kp = dw[ckp], p = dp[c];
+    const bool v_lo = PY || j > 1, v_hi = PY || j < ny;   // wall faces v(1), v(ny+1) stay 0
+    sweep32_update(P, __ldg(r + c), u_i, u_ip, v_j, v_jp, w_k, w_kp, p, mu_u_i, mu_u_ip, mu_v_j, mu_v_jp, mu_w,
+                   __ldg(fac32 + q), v_lo, v_hi);
+    dp[c] = p;
+    du[c] = u_i;
+    du[cip] = u_ip;
+    if (v_lo) dv[c] = v_j;
+    if (v_hi) dv[cjp] = v_jp;
+    dw[c] = w_k;
+    dw[ckp] = w_kp;
 }
 
 // Residual of the correction problem at cell (i, j, k): r~ + div(du).
@@ -115,6 +119,7 @@ __device__ __forceinline__ void mixed_tables_elem(const mdx_dims& d, int py, dou
                                                   double sor, const double* __restrict__ mu, long long t,
                                                   float* __restrict__ mu32, float* __restrict__ fac32) {
     const long long np = (long long)d.nxp * d.nyp;
+    const int ps = split_plane_elems(d);
     const int i = (int)(t % d.nxp), j = (int)(t / d.nxp);
     double mu_u = 1.0, mu_v = 1.0, mu_w = 1.0;
     if (mu) {
@@ -124,8 +129,8 @@ __device__ __forceinline__ void mixed_tables_elem(const mdx_dims& d, int py, dou
     }
     const int o = pidx2(d, i, j);
     mu32[o] = (float)mu_u;
-    mu32[np + o] = (float)mu_v;
-    mu32[2 * np + o] = (float)mu_w;
+    mu32[ps + o] = (float)mu_v;
+    mu32[2 * ps + o] = (float)mu_w;
     double f = 0.0;
     if (i >= 1 && i <= d.nx && j >= 1 && j <= d.ny) {
         const int ip = i == d.nx ? 1 : i + 1;

@@ -2,6 +2,8 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdint>
@@ -22,7 +24,10 @@ struct mdx_dims {
     long long npad;      // (nx+2)(ny+2)(nz+2)
     long long nint;      // nx*ny*nz
     long long nspec;     // nxh*nz*ny
+    int hs;              // row length of the colour-split layout, (nx+2)/2
 };
+
+__host__ __device__ inline int split_stride(int nx) { return (nx + 2) / 2; }
 
 __host__ __device__ inline long long pidx(const mdx_dims& d, int i, int j, int k) {
     return (long long)i + (long long)d.nxp * ((long long)j + (long long)d.nyp * (long long)k);
@@ -33,6 +38,26 @@ __host__ __device__ inline long long qidx(const mdx_dims& d, int i, int j, int k
 __host__ __device__ inline long long ridx(const mdx_dims& d, int i, int k, int j) {  // rhs(i,k,j), 1-based
     return (long long)(i - 1) + (long long)d.nx * ((long long)(k - 1) + (long long)d.nz * (long long)(j - 1));
 }
+
+// Colour-split layout (the mixed path's FP32 arrays, the FP64 sweeps' working
+// copies, the ensemble's FP32 arrays): element (i, j, k) of the padded grid
+// lives in half (i + j + k) & 1 at (k (ny+2) + j) hs + i/2, hs = (nx+2)/2,
+// so the cells of one colour in a row -- and the faces they own or share --
+// are consecutive: every access of a colour sweep is unit-stride.  A face
+// belongs to the cell on its high side (u(i) to cell i).  nx is even, so
+// (nx+2)/2 is whole.
+__host__ __device__ __forceinline__ long long cidx(const mdx_dims& d, int i, int j, int k) {
+    return ((i + j + k) & 1) * ((long long)d.hs * d.nyp * d.nzp) + ((long long)k * d.nyp + j) * d.hs + (i >> 1);
+}
+__host__ __device__ inline long long split_elems(const mdx_dims& d) { return 2LL * d.hs * d.nyp * d.nzp; }
+// (i, j) planes of the IBM factors and sweep factors, split the same way by
+// (i + j) & 1: for one colour and one z plane all rows of the cells' factors
+// lie in one half.  A plane of one component holds split_plane_elems values.
+__host__ __device__ __forceinline__ int pidx2(const mdx_dims& d, int i, int j) {
+    return ((i + j) & 1) * (d.hs * d.nyp) + j * d.hs + (i >> 1);
+}
+__host__ __device__ inline int split_plane_elems(const mdx_dims& d) { return 2 * d.hs * d.nyp; }
+
 
 // Scalars of one time step, passed by value to kernels.
 struct mdx_step_params {
@@ -75,11 +100,15 @@ struct mdx_ctx {
     double* f[MDX_NUM_FIELDS] = {nullptr};   // device mirrors (MDX_PHI -> phi)
     bool ibm_zero = true;                    // all IBM coefficients zero
     bool coef_zinv = false;                  // coefficients equal on every z plane
-    double* sor_alt[4] = {nullptr};          // second u,v,w,p state of the fused red-black pass
+    double* sor_alt[4] = {nullptr};          // second u,v,w,p state of the fused red-black pass, or the
+                                             // colour-split working copies of the split sweeps
+    bool split_norms = false;                // divergence norms read colour-split arrays
     bool fused_attr = false;
-    // mixed-precision red-black: FP32 corrections, FP32 residual, IBM tables
+    // mixed-precision red-black: FP32 corrections, FP32 residual, IBM tables,
+    // carved from one allocation (mx_du is its base) of mx_bytes
     float *mx_du = nullptr, *mx_dv = nullptr, *mx_dw = nullptr, *mx_dp = nullptr, *mx_r = nullptr;
     float *mx_mu = nullptr, *mx_fac = nullptr;
+    size_t mx_bytes = 0;
     // warm starts: increments of the last projection of each RK substage
     int guess_mode = 0;                      // MDX_GUESS_*
     bool record_increments = false;
@@ -94,7 +123,7 @@ struct mdx_ctx {
     long long proj_count = 0;                // projections since the t=0 projection
     void* unet = nullptr;                    // learned warm start (k_unet.cu)
     int sor_tuned = 0;                       // red-black kernel variant chosen by the autotuner (0: not yet)
-    double sor_tune_ms[4] = {0.0};           // time of one residual-check block per variant
+    double sor_tune_ms[4] = {0.0};           // time per iteration of a timed residual-check block, per variant
     cudaEvent_t tune_ev[2] = {nullptr, nullptr};
     double* mu = nullptr;                    // red-black IBM factors 1/(1+dt_gamma*coef)
     long long mu_elems = 0;
@@ -135,6 +164,38 @@ struct mdx_ctx {
     long long tim_issued[MDX_T_NUM] = {0};   // launches per class since set_timing(1)
     long long launches = 0;
     bool capturing = false;
+};
+
+// Iterations until the next residual check of a red-black solve.  Once the
+// residual falls at a steady geometric rate -- the rates of the last two
+// check intervals agree within 25 % -- that rate predicts the iterations left
+// to the target, and the next check comes after half of them, in whole
+// check_every blocks (1 to 8).  Checks far from the target are sparse, the
+// last ones check_every apart, and every check lands on a multiple of
+// check_every.  While the rate changes (the first sweeps, or a plateau of the
+// over-relaxed iteration) and in mode 1, every block is checked.
+struct mdx_check_schedule {
+    int every = 1, mode = 0;
+    int last_it = 0;
+    double last_r = 0.0, rate = 0.0;   // natural-log decrease per iteration of the last interval
+    void start(int check_every, int check_mode, double r) {
+        every = check_every > 0 ? check_every : 1;
+        mode = check_mode;
+        last_it = 0;
+        last_r = r;
+        rate = 0.0;
+    }
+    int next(int it, double r, double target) {
+        const double rt = (it > last_it && r > 0.0 && last_r > r) ? std::log(last_r / r) / (double)(it - last_it) : 0.0;
+        const bool steady = rt > 0.0 && rate > 0.0 && std::fabs(rt - rate) <= 0.25 * rt;
+        rate = rt;
+        last_it = it;
+        last_r = r;
+        if (mode == 1 || !steady || !(r > target) || !(target > 0.0)) return every;
+        const double left = std::log(r / target) / rt;
+        const double blocks = std::floor(0.5 * left / (double)every);
+        return every * (int)std::min(8.0, std::max(1.0, blocks));
+    }
 };
 
 // ---- error helpers -------------------------------------------------------

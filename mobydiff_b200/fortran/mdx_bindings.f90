@@ -29,7 +29,8 @@ module mdx_bindings
         real(C_DOUBLE) :: sor, tol
         integer(C_INT) :: max_iter, check_every, precision
         integer(C_INT) :: sor_variant, sor_kz
-        integer(C_INT) :: reserved_i(5)
+        integer(C_INT) :: check_mode
+        integer(C_INT) :: reserved_i(4)
         real(C_DOUBLE) :: atol
         real(C_DOUBLE) :: inner_sor
         real(C_DOUBLE) :: reserved_d(6)

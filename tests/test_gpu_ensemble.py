@@ -58,7 +58,9 @@ def test_fixed_iterations_bitwise_equal_to_single_channels(mode):
 
 
 def test_tolerance_mode_matches_single_channels():
-    opts = M.make_solver_opts(M.SOLVER_REDBLACK, sor=1.7, tol=1e-8, check_every=10, max_iter=200000)
+    # the ensemble checks every check_every iterations: the single channels too
+    opts = M.make_solver_opts(M.SOLVER_REDBLACK, sor=1.7, tol=1e-8, check_every=10, max_iter=200000,
+                              adaptive_checks=False)
     mems = _members()
     with M.Ensemble(mems, opts) as E:
         E.set_guess(M.GUESS_EXTRAPOLATED)

@@ -111,7 +111,8 @@ def test_redblack_residual_driven_matches_oracle():
     f.vs[...] = f.vn
     f.ws[...] = f.wn
     with to_device(M, g, bc, f) as s:
-        s.init_pressure_solver(M.make_solver_opts(M.SOLVER_REDBLACK, sor=1.7, tol=1e-10, check_every=10))
+        s.init_pressure_solver(M.make_solver_opts(M.SOLVER_REDBLACK, sor=1.7, tol=1e-10, check_every=10,
+                                                  adaptive_checks=False))
         st_o, it_o, res_o = O.pressure_projection_redblack(g, bc, f, 1e-3 * 64 / 120, sor=1.7, tol=1e-10,
                                                            check_every=10)
         st = s.pressure_projection(1e-3 * 64 / 120)
@@ -198,7 +199,8 @@ def test_c1_wavy_redblack_truncated():
     s = to_device(M, g, bc, O.Fields(g))
     with s:
         s.enter_ibm_data(f.coef_u, f.coef_v, f.coef_w)
-        s.init_pressure_solver(M.make_solver_opts(M.SOLVER_REDBLACK, sor=1.7, tol=1e-10, check_every=50))
+        s.init_pressure_solver(M.make_solver_opts(M.SOLVER_REDBLACK, sor=1.7, tol=1e-10, check_every=50,
+                                                  adaptive_checks=False))
         s.channel_ic(20261203, y0=y0, wave_amp=0.05, wave_lambda=g.lx / 2)
         for n in ("un", "vn", "wn"):
             assert np.array_equal(s.get(n), getattr(f, n)), n
