@@ -203,6 +203,15 @@ typedef struct {
     double amp, phase, lambda, y0, height;
 } mdx_ibm_geom_t;
 int mdx_set_ibm_coeff(const mdx_grid_t* g, const mdx_ibm_geom_t* geom, double* coeff, int dix, int diy, int diz);
+/* The same coefficients computed on the device into d_coeff (a padded
+ * (nx+2)(ny+2)(nz+2) device array), stream-ordered on `stream` (a
+ * cudaStream_t, NULL for the default stream).  Same arithmetic as the host
+ * routine; the device sin may round differently from the host's in the last
+ * bit, which can move a bisected wall distance only for a point within one
+ * rounding of the wall.  No counterpart in the reference (its
+ * set_ibm_coeff is a host loop, src/modules/ibm.f90:133-187). */
+int mdx_set_ibm_coeff_device(const mdx_grid_t* g, const mdx_ibm_geom_t* geom, double* d_coeff, int dix, int diy,
+                             int diz, void* stream);
 
 /* ---- context ---------------------------------------------------------- */
 
@@ -244,6 +253,11 @@ int mdx_copy_field(mdx_ctx_t* ctx, int field, double* host, int direction);
 /* enter_ibm_data / exit_ibm_data, src/modules/ibm.f90:57-81.  NULL
  * coefficients mean "no body" (all zero).  exit restores zero coefficients. */
 int mdx_enter_ibm_data(mdx_ctx_t* ctx, const double* coef_u, const double* coef_v, const double* coef_w);
+/* The reference's IBM setup, src/main.f90:58-61 -- set_ibm_coeff for u, v, w
+ * (ibm.f90:133-187) then enter_ibm_data -- in one call, the coefficients
+ * generated on the device (mdx_set_ibm_coeff_device) straight into the
+ * context's mirrors: no host arrays, no copies. */
+int mdx_enter_ibm_geometry(mdx_ctx_t* ctx, const mdx_ibm_geom_t* geom);
 int mdx_exit_ibm_data(mdx_ctx_t* ctx);
 
 /* ---- time step ---------------------------------------------------------- */

@@ -162,6 +162,8 @@ def lib():
         "mdx_update_device": (i, [vp, vp, vp, vp, vp]),
         "mdx_copy_field": (i, [vp, i, vp, i]),
         "mdx_enter_ibm_data": (i, [vp, vp, vp, vp]),
+        "mdx_enter_ibm_geometry": (i, [vp, P(IbmGeomT)]),
+        "mdx_set_ibm_coeff_device": (i, [P(GridT), P(IbmGeomT), vp, i, i, i, vp]),
         "mdx_exit_ibm_data": (i, [vp]),
         "mdx_momentum": (i, [vp, d, d, d]),
         "mdx_apply_bc": (i, [vp]),
@@ -373,6 +375,10 @@ class Solver:
 
     def enter_ibm_data(self, coef_u=None, coef_v=None, coef_w=None):
         self._c(lib().mdx_enter_ibm_data(self.h, _p(coef_u), _p(coef_v), _p(coef_w)))
+
+    def enter_ibm_geometry(self, geom: IbmGeomT):
+        """set_ibm_coeff for u, v, w generated on the device, then enter_ibm_data."""
+        self._c(lib().mdx_enter_ibm_geometry(self.h, C.byref(geom)))
 
     def exit_ibm_data(self):
         self._c(lib().mdx_exit_ibm_data(self.h))

@@ -34,6 +34,7 @@ CUDA_SOURCES = {
     "k_warm.cu": ["-fmad=false"],
     "k_unet.cu": [],        # BF16 network with FP32 accumulation: FMA allowed
     "k_ensemble.cu": ["-fmad=false"],
+    "k_ibm.cu": ["-fmad=false"],   # IBM coefficients: the host routine's arithmetic
 }
 CXX_SOURCES = ["host_config.cpp"]
 

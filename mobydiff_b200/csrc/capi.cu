@@ -384,6 +384,25 @@ int mdx_enter_ibm_data(mdx_ctx_t* ctx, const double* cu, const double* cv, const
     return MDX_OK;
 }
 
+// set_ibm_coeff for u, v, w then enter_ibm_data (src/main.f90:58-61), with
+// the coefficients generated on the device straight into the mirrors.
+int mdx_enter_ibm_geometry(mdx_ctx_t* ctx, const mdx_ibm_geom_t* geom) {
+    MDX_TRY(need_fields(ctx));
+    if (!geom) return mdx_fail(ctx, MDX_ERR_ARG, "mdx_enter_ibm_geometry: null geometry");
+    release_graph(ctx);
+    MDX_CUDA(ctx, cudaSetDevice(ctx->device));
+    for (int t = 0; t < 3; ++t) {
+        const int rc = mdx_ibm_coeff_launch(&ctx->g, geom, ctx->f[MDX_COEF_U + t], t == 0, t == 1, t == 2,
+                                            ctx->d.nzp, ctx->stream);
+        if (rc != MDX_OK) return mdx_fail(ctx, rc, "mdx_enter_ibm_geometry: bad geometry or launch failure");
+        ctx->launches++;
+    }
+    MDX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    ctx->ibm_zero = false;   // a body is present (SOLID cells at least)
+    ctx->coef_zinv = true;   // the walls depend on x and y only
+    return MDX_OK;
+}
+
 int mdx_exit_ibm_data(mdx_ctx_t* ctx) {
     MDX_TRY(need_fields(ctx));
     release_graph(ctx);

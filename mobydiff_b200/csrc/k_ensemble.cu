@@ -1280,8 +1280,9 @@ int mdx_ensemble_create(int device, int n, const mdx_member_t* members, const md
             if (rc == MDX_OK) rc = ealloc(E, &M.fac32, ps, true);
         }
         if (rc == MDX_OK && q.amp > 0.0) {
-            // wavy walls y0 + A sin(2 pi x / (Lx/2)) and y0 + 2 + ..., y0 = (Ly - 2)/2
-            std::vector<double> cu(np), cv(np), cw(np);
+            // wavy walls y0 + A sin(2 pi x / (Lx/2)) and y0 + 2 + ..., y0 = (Ly - 2)/2;
+            // one z plane of each component, generated on the device (the walls
+            // depend on x and y only)
             mdx_ibm_geom_t geo{};
             geo.geometry = 1;
             geo.n_wave_x = 1;
@@ -1290,21 +1291,11 @@ int mdx_ensemble_create(int device, int n, const mdx_member_t* members, const md
             geo.lambda = q.lx / 2.0;
             geo.y0 = (q.ly - 2.0) / 2.0;
             geo.height = 2.0;
-            double* arrs[3] = {cu.data(), cv.data(), cw.data()};
-            for (int t = 0; t < 3 && rc == MDX_OK; ++t) {
-                rc = mdx_set_ibm_coeff(&g, &geo, arrs[t], t == 0, t == 1, t == 2);
-                if (rc != MDX_OK) efail(E, rc, "member %d: IBM coefficients: %s", m, mdx_last_error(nullptr));
-            }
-            for (size_t c = pl; c < np && rc == MDX_OK; ++c)
-                if (cu[c] != cu[c % pl] || cv[c] != cv[c % pl] || cw[c] != cw[c % pl])
-                    rc = efail(E, MDX_ERR_ARG, "member %d: IBM coefficients vary along z", m);
             double** planes[3] = {&M.cu, &M.cv, &M.cw};
             for (int t = 0; t < 3 && rc == MDX_OK; ++t) {
                 rc = ealloc(E, planes[t], pl, false);
-                if (rc == MDX_OK)
-                    rc = cudaMemcpy(*planes[t], arrs[t], sizeof(double) * pl, cudaMemcpyHostToDevice) == cudaSuccess
-                             ? MDX_OK
-                             : efail(E, MDX_ERR_CUDA, "coefficient copy failed");
+                if (rc == MDX_OK && mdx_ibm_coeff_launch(&g, &geo, *planes[t], t == 0, t == 1, t == 2, 1, E->stream) != MDX_OK)
+                    rc = efail(E, MDX_ERR_CUDA, "member %d: IBM coefficient generation failed", m);
             }
             if (rc == MDX_OK) rc = ealloc(E, &M.mu, 3 * pl);
             M.ibm = 1;

@@ -247,6 +247,8 @@ int mdx_reduce_partials(mdx_ctx_t* ctx, double* sum, double* max1, double* max2)
 int mdx_k_projection_redblack_mixed(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t* st, bool* handled, double r0,
                                     double umax, double atol);
 void mdx_mixed_free(mdx_ctx_t* ctx);
+int mdx_ibm_coeff_launch(const mdx_grid_t* g, const mdx_ibm_geom_t* geom, double* d_coeff, int dix, int diy, int diz,
+                         int planes, cudaStream_t stream);
 // warm starts (k_warm.cu, k_unet.cu)
 bool mdx_guess_supported(const mdx_ctx_t* ctx);
 int mdx_warm_alloc(mdx_ctx_t* ctx);

@@ -42,6 +42,12 @@ module mdx_bindings
         integer(C_INT) :: variant, guessed
     end type mdx_solve_stats_t
 
+    ! ibm_type geometry parameters (mdx_ibm_geom_t)
+    type, bind(C) :: mdx_ibm_geom_t
+        integer(C_INT) :: geometry, n_wave_x
+        real(C_DOUBLE) :: amp, phase, lambda, y0, height
+    end type mdx_ibm_geom_t
+
     interface
         function mdx_device_count(count) bind(C, name="mdx_device_count") result(rc)
             import :: C_INT
@@ -100,6 +106,12 @@ module mdx_bindings
         function mdx_enter_ibm_data(ctx, cu, cv, cw) bind(C, name="mdx_enter_ibm_data") result(rc)
             import :: C_INT, C_PTR
             type(C_PTR), value :: ctx, cu, cv, cw
+            integer(C_INT) :: rc
+        end function
+        function mdx_enter_ibm_geometry(ctx, geom) bind(C, name="mdx_enter_ibm_geometry") result(rc)
+            import :: C_INT, C_PTR, mdx_ibm_geom_t
+            type(C_PTR), value :: ctx
+            type(mdx_ibm_geom_t), intent(in) :: geom
             integer(C_INT) :: rc
         end function
         function mdx_exit_ibm_data(ctx) bind(C, name="mdx_exit_ibm_data") result(rc)

@@ -28,8 +28,8 @@ def _single(m, opts, mode):
     s.enter_field_data()
     y0 = (m.ly - 2.0) / 2.0
     lam = m.lx / 2.0
-    if m.amp > 0.0:
-        s.enter_ibm_data(*M.set_ibm_coeff(g, M.ibm_wavy(m.amp, lam, y0)))
+    if m.amp > 0.0:   # the ensemble generates its members' coefficients on the device too
+        s.enter_ibm_geometry(M.ibm_wavy(m.amp, lam, y0))
     s.init_pressure_solver(opts)
     s.set_pressure_guess(mode, record=mode != M.GUESS_ZERO)
     s.channel_ic(m.seed, 0.1, 0.01, y0, m.amp, lam)
