@@ -202,6 +202,24 @@ typedef struct {
     int n_wave_x;
     double amp, phase, lambda, y0, height;
 } mdx_ibm_geom_t;
+/* ---- field files (HDF5), src/modules/field_hdf5.c ------------------------
+ * The reference's two C entry points under their own names and signatures
+ * (field_hdf5.c:149-204, bound by io.f90:7-24), written without libhdf5:
+ * root attributes nx, ny, nz (int32) and lx, ly, lz, dx, dy, dz, re, dt,
+ * t_current (float64), datasets un, vn, wn, pn (float64, dims
+ * (nx+2, ny+2, nz+2), C order).  Host arrays in the padded Fortran layout.
+ * Return 0 on success, 1 on any failure, as the reference does. */
+int fdm_h5_write_field(const char* filename, int nx, int ny, int nz, double lx, double ly, double lz, double dx,
+                       double dy, double dz, double re, double dt, double t_current, const double* un,
+                       const double* vn, const double* wn, const double* pn);
+int fdm_h5_read_field(const char* filename, int nx, int ny, int nz, double* un, double* vn, double* wn, double* pn);
+/* The scalar root attributes of a field file (no counterpart in the
+ * reference, whose read_field reads the datasets only): dims = nx, ny, nz;
+ * vals = lx, ly, lz, dx, dy, dz, re, dt, t_current.  MDX_ERR_IO on failure. */
+int mdx_h5_read_header(const char* filename, int* dims, double* vals);
+/* Why the last fdm_h5_read_field / mdx_h5_read_header call failed. */
+const char* mdx_h5_last_error(void);
+
 int mdx_set_ibm_coeff(const mdx_grid_t* g, const mdx_ibm_geom_t* geom, double* coeff, int dix, int diy, int diz);
 /* The same coefficients computed on the device into d_coeff (a padded
  * (nx+2)(ny+2)(nz+2) device array), stream-ordered on `stream` (a
@@ -253,6 +271,11 @@ int mdx_copy_field(mdx_ctx_t* ctx, int field, double* host, int direction);
 /* enter_ibm_data / exit_ibm_data, src/modules/ibm.f90:57-81.  NULL
  * coefficients mean "no body" (all zero).  exit restores zero coefficients. */
 int mdx_enter_ibm_data(mdx_ctx_t* ctx, const double* coef_u, const double* coef_v, const double* coef_w);
+/* write_field / read_field, src/modules/io.f90:105-166: the device mirrors
+ * of un, vn, wn, pn to the host and into a field file with the context's
+ * grid and t_current; or a field file into the mirrors (synchronising). */
+int mdx_write_field_h5(mdx_ctx_t* ctx, const char* filename);
+int mdx_read_field_h5(mdx_ctx_t* ctx, const char* filename);
 /* The reference's IBM setup, src/main.f90:58-61 -- set_ibm_coeff for u, v, w
  * (ibm.f90:133-187) then enter_ibm_data -- in one call, the coefficients
  * generated on the device (mdx_set_ibm_coeff_device) straight into the

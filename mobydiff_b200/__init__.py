@@ -163,6 +163,12 @@ def lib():
         "mdx_copy_field": (i, [vp, i, vp, i]),
         "mdx_enter_ibm_data": (i, [vp, vp, vp, vp]),
         "mdx_enter_ibm_geometry": (i, [vp, P(IbmGeomT)]),
+        "fdm_h5_write_field": (i, [C.c_char_p, i, i, i] + [d] * 9 + [vp] * 4),
+        "fdm_h5_read_field": (i, [C.c_char_p, i, i, i] + [vp] * 4),
+        "mdx_h5_read_header": (i, [C.c_char_p, P(i), P(d)]),
+        "mdx_h5_last_error": (C.c_char_p, []),
+        "mdx_write_field_h5": (i, [vp, C.c_char_p]),
+        "mdx_read_field_h5": (i, [vp, C.c_char_p]),
         "mdx_set_ibm_coeff_device": (i, [P(GridT), P(IbmGeomT), vp, i, i, i, vp]),
         "mdx_exit_ibm_data": (i, [vp]),
         "mdx_momentum": (i, [vp, d, d, d]),
@@ -316,6 +322,44 @@ def set_ibm_coeff(g: GridT, geom: IbmGeomT):
     return tuple(out)
 
 
+H5_ATTRS = ("lx", "ly", "lz", "dx", "dy", "dz", "re", "dt", "t_current")
+
+
+def h5_write_field(path: str, g: GridT, un, vn, wn, pn, t_current=None) -> None:
+    """fdm_h5_write_field (src/modules/field_hdf5.c:149-184): padded arrays
+    (any shape holding (nx+2)(ny+2)(nz+2) values in Fortran order)."""
+    arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (un, vn, wn, pn)]
+    n = (g.nx + 2) * (g.ny + 2) * (g.nz + 2)
+    if any(a.size != n for a in arrs):
+        raise MdxError(MDX_ERR_ARG, "h5_write_field: arrays must hold (nx+2)(ny+2)(nz+2) values")
+    t = g.t_current if t_current is None else t_current
+    rc = lib().fdm_h5_write_field(os.fsencode(path), g.nx, g.ny, g.nz, g.lx, g.ly, g.lz, g.dx, g.dy, g.dz, g.re,
+                                  g.dt, t, *[a.ctypes.data for a in arrs])
+    if rc != 0:
+        raise MdxError(MDX_ERR_IO, f"could not write HDF5 field file: {path}")
+
+
+def h5_read_field(path: str, nx: int, ny: int, nz: int):
+    """fdm_h5_read_field (src/modules/field_hdf5.c:186-204) -> (un, vn, wn, pn),
+    padded arrays indexed [k, j, i]."""
+    arrs = [np.empty((nz + 2, ny + 2, nx + 2)) for _ in range(4)]
+    if lib().fdm_h5_read_field(os.fsencode(path), nx, ny, nz, *[a.ctypes.data for a in arrs]) != 0:
+        raise MdxError(MDX_ERR_IO, lib().mdx_h5_last_error().decode())
+    return tuple(arrs)
+
+
+def h5_read_header(path: str) -> dict:
+    """Root attributes of a field file: nx, ny, nz and lx .. t_current."""
+    dims = (C.c_int * 3)()
+    vals = (C.c_double * 9)()
+    rc = lib().mdx_h5_read_header(os.fsencode(path), dims, vals)
+    if rc != MDX_OK:
+        raise MdxError(rc, lib().mdx_h5_last_error().decode())
+    out = {"nx": dims[0], "ny": dims[1], "nz": dims[2]}
+    out.update({k: vals[t] for t, k in enumerate(H5_ATTRS)})
+    return out
+
+
 def rk_coeffs():
     """src/modules/step.f90:21-23."""
     return ([64.0 / 120.0, 50.0 / 120.0, 90.0 / 120.0],
@@ -375,6 +419,14 @@ class Solver:
 
     def enter_ibm_data(self, coef_u=None, coef_v=None, coef_w=None):
         self._c(lib().mdx_enter_ibm_data(self.h, _p(coef_u), _p(coef_v), _p(coef_w)))
+
+    def write_field_h5(self, path: str) -> None:
+        """write_field (src/modules/io.f90:105-137) from the device mirrors."""
+        self._c(lib().mdx_write_field_h5(self.h, os.fsencode(path)))
+
+    def read_field_h5(self, path: str) -> None:
+        """read_field (src/modules/io.f90:139-166) into the device mirrors."""
+        self._c(lib().mdx_read_field_h5(self.h, os.fsencode(path)))
 
     def enter_ibm_geometry(self, geom: IbmGeomT):
         """set_ibm_coeff for u, v, w generated on the device, then enter_ibm_data."""

@@ -36,7 +36,7 @@ CUDA_SOURCES = {
     "k_ensemble.cu": ["-fmad=false"],
     "k_ibm.cu": ["-fmad=false"],   # IBM coefficients: the host routine's arithmetic
 }
-CXX_SOURCES = ["host_config.cpp"]
+CXX_SOURCES = ["host_config.cpp", "h5_field.cpp"]
 
 
 def _nvcc() -> str:

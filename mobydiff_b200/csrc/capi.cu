@@ -384,6 +384,41 @@ int mdx_enter_ibm_data(mdx_ctx_t* ctx, const double* cu, const double* cv, const
     return MDX_OK;
 }
 
+// write_field (io.f90:105-137): device mirrors -> host -> field file.
+int mdx_write_field_h5(mdx_ctx_t* ctx, const char* filename) {
+    MDX_TRY(need_fields(ctx));
+    if (!filename) return mdx_fail(ctx, MDX_ERR_ARG, "mdx_write_field_h5: null file name");
+    const size_t n = (size_t)ctx->d.npad;
+    std::vector<double> h(4 * n);
+    const int ids[4] = {MDX_UN, MDX_VN, MDX_WN, MDX_PN};
+    for (int t = 0; t < 4; ++t)
+        MDX_CUDA(ctx, cudaMemcpyAsync(h.data() + t * n, ctx->f[ids[t]], sizeof(double) * n, cudaMemcpyDeviceToHost,
+                                      ctx->stream));
+    MDX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    const mdx_grid_t& g = ctx->g;
+    if (fdm_h5_write_field(filename, g.nx, g.ny, g.nz, g.lx, g.ly, g.lz, g.dx, g.dy, g.dz, g.re, g.dt, g.t_current,
+                           h.data(), h.data() + n, h.data() + 2 * n, h.data() + 3 * n) != 0)
+        return mdx_fail(ctx, MDX_ERR_IO, "could not write HDF5 field file: %s", filename);
+    return MDX_OK;
+}
+
+// read_field (io.f90:139-166): field file -> host -> device mirrors.
+int mdx_read_field_h5(mdx_ctx_t* ctx, const char* filename) {
+    MDX_TRY(need_fields(ctx));
+    if (!filename) return mdx_fail(ctx, MDX_ERR_ARG, "mdx_read_field_h5: null file name");
+    const size_t n = (size_t)ctx->d.npad;
+    std::vector<double> h(4 * n);
+    const mdx_grid_t& g = ctx->g;
+    if (fdm_h5_read_field(filename, g.nx, g.ny, g.nz, h.data(), h.data() + n, h.data() + 2 * n, h.data() + 3 * n) != 0)
+        return mdx_fail(ctx, MDX_ERR_IO, "could not read HDF5 field file: %s", mdx_h5_last_error());
+    const int ids[4] = {MDX_UN, MDX_VN, MDX_WN, MDX_PN};
+    for (int t = 0; t < 4; ++t)
+        MDX_CUDA(ctx, cudaMemcpyAsync(ctx->f[ids[t]], h.data() + t * n, sizeof(double) * n, cudaMemcpyHostToDevice,
+                                      ctx->stream));
+    MDX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return MDX_OK;
+}
+
 // set_ibm_coeff for u, v, w then enter_ibm_data (src/main.f90:58-61), with
 // the coefficients generated on the device straight into the mirrors.
 int mdx_enter_ibm_geometry(mdx_ctx_t* ctx, const mdx_ibm_geom_t* geom) {

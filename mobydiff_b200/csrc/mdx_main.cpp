@@ -35,6 +35,24 @@ static bool output_is_due(int step, int interval) {   // io.f90:31-39
 
 // Legacy-ASCII VTK of cell-centred velocity, io.f90:168-259 (same header
 // lines and ES20.12 number format).
+// write_field, src/modules/io.f90:105-137: "<prefix>_<step>.h5" through the
+// reference's own entry point, with the driver's grid and time.
+static int write_field(mdx_ctx_t* ctx, const mdx_grid_t& g, int step, const char* prefix) {
+    char name[600];
+    std::snprintf(name, sizeof(name), "%s_%d.h5", prefix, step);
+    std::printf(" current time step: %12d   field filename: %s\n", step, name);
+    const size_t n = (size_t)(g.nx + 2) * (g.ny + 2) * (g.nz + 2);
+    std::vector<double> h(4 * n);
+    int rc = mdx_update_host(ctx, h.data(), h.data() + n, h.data() + 2 * n, h.data() + 3 * n);
+    if (rc != MDX_OK) return rc;
+    if (fdm_h5_write_field(name, g.nx, g.ny, g.nz, g.lx, g.ly, g.lz, g.dx, g.dy, g.dz, g.re, g.dt, g.t_current,
+                           h.data(), h.data() + n, h.data() + 2 * n, h.data() + 3 * n) != 0) {
+        std::printf(" error: could not write HDF5 field file: %s\n", name);
+        return MDX_ERR_IO;
+    }
+    return MDX_OK;
+}
+
 static int write_vtk(mdx_ctx_t* ctx, const mdx_grid_t& g, int step, const char* prefix) {
     char name[512];
     std::snprintf(name, sizeof(name), "%s_%d.vtk", prefix, step);
@@ -144,8 +162,8 @@ int main(int argc, char** argv) {
         if (g.cflmax > 0.0 && g.cfl > 0.0) g.dt = std::fmin(g.cflmax / g.cfl, g.dtmax);
         if (run.output_interval > 0 && output_is_due(i, run.output_interval))
             CHECK(ctx, write_vtk(ctx, g, i, run.output_prefix));
-        if (run.field_interval > 0 && output_is_due(i, run.field_interval))
-            std::printf(" warning: HDF5 field output (step %d) is not available in this build\n", i);
+        if (run.field_interval > 0 && output_is_due(i, run.field_interval))   // io.f90:95-137
+            CHECK(ctx, write_field(ctx, g, i, run.field_prefix));
     }
     double dummy = 0.0;
     CHECK(ctx, mdx_divergence_norms(ctx, &dummy, &dummy));   // drains the stream

@@ -48,3 +48,29 @@ def test_restart_from_host_state_is_bitwise(solver, amp):
         b.step(2)
         for x, n in zip(full, ("un", "vn", "wn", "pn")):
             assert np.array_equal(x, b.get(n)), n
+
+
+@pytest.mark.parametrize("solver,amp", [(M.SOLVER_FFT, 0.0), (M.SOLVER_REDBLACK, 0.05)])
+def test_restart_through_hdf5_field_file_is_bitwise(tmp_path, solver, amp):
+    """write_field / read_field (io.f90:105-166) through a field file: the
+    restarted run equals the uninterrupted one, and the file holds the
+    context's time and grid."""
+    g, opts, y0, coef = _case(solver, amp)
+    path = str(tmp_path / "field_3.h5")
+    with _solver(g, opts, coef) as a:
+        a.channel_ic(20261203, 0.1, 0.01, y0, amp, math.pi)
+        a.step(3)
+        a.write_field_h5(path)
+        on_file = M.h5_read_field(path, g.nx, g.ny, g.nz)
+        for x, n in zip(on_file, ("un", "vn", "wn", "pn")):
+            assert np.array_equal(x, a.get(n)), n
+        a.step(2)
+        full = [a.get(n) for n in ("un", "vn", "wn", "pn")]
+    h = M.h5_read_header(path)
+    assert (h["nx"], h["ny"], h["nz"]) == (g.nx, g.ny, g.nz) and h["dt"] == g.dt and h["re"] == g.re
+    assert abs(h["t_current"] - 3 * g.dt) <= 1e-15
+    with _solver(g, opts, coef) as b:
+        b.read_field_h5(path)
+        b.step(2)
+        for x, n in zip(full, ("un", "vn", "wn", "pn")):
+            assert np.array_equal(x, b.get(n)), n
