@@ -153,6 +153,16 @@ def _dist():
     return ws, rank, local
 
 
+SOR_VARIANT = 0   # --sor-variant: red-black kernel variant (0: the autotuner's choice)
+SOR_NAMES = {1: "one launch per colour sweep", 2: "fused red+black pass 32x8", 3: "fused red+black pass 32x16",
+             4: "one launch per colour sweep on colour-split copies"}
+
+
+def _sor64_traffic_key(variant):
+    """traffic.json entry of the FP64 sweep kernel a solve ran."""
+    return "sor_sweep_split" if variant == 4 else "sor_sweep"
+
+
 def _setup(cfg, M, device, profile=False, tol=None, precision=None, seed=None):
     g = M.make_grid(cfg["nx"], cfg["ny"], cfg["nz"], cfg["lx"], cfg["ly"], cfg["lz"], cfg["re"], cfg["dt"],
                     (2.0 / cfg["re"], 0.0, 0.0))
@@ -166,11 +176,12 @@ def _setup(cfg, M, device, profile=False, tol=None, precision=None, seed=None):
     if cfg["solver"] == "redblack" and profile:
         # profiling mode: the full-size state with a fixed 20 sweeps per
         # projection, so that an ncu capture of a few launches ends quickly
-        opts = M.make_solver_opts(M.SOLVER_REDBLACK, sor=cfg["sor"], n_iter=20, tol=0.0)
+        opts = M.make_solver_opts(M.SOLVER_REDBLACK, sor=cfg["sor"], n_iter=20, tol=0.0, sor_variant=SOR_VARIANT)
     elif cfg["solver"] == "redblack":
         opts = M.make_solver_opts(M.SOLVER_REDBLACK, sor=cfg["sor"], tol=cfg["tol"] if tol is None else tol,
                                   check_every=cfg["check_every"], max_iter=400000,
-                                  precision=M.PREC_FP64 if precision is None else precision)
+                                  precision=M.PREC_FP64 if precision is None else precision,
+                                  sor_variant=SOR_VARIANT)
     else:
         opts = M.make_solver_opts(M.SOLVER_FFT, tol=cfg.get("tol", 0.0) if precision == M.PREC_MIXED else 0.0,
                                   precision=M.PREC_FP64 if precision is None else precision)
@@ -427,15 +438,15 @@ def run_plain(args, cfg):
         _, ms, _, _, tim = _timed_steps(s, stream, args.steps, pg, timing=True)
     else:
         _, ms, _, _, tim = _timed_steps(s, stream, args.steps, pg, timing=True)
-    if cfg["solver"] == "redblack":
-        roofline = _roofline(tim, "sor_sweep", 32.0, cells, ms)   # 4 doubles per cell per colour sweep
+    if cfg["solver"] == "redblack":   # 4 doubles per cell per colour sweep
+        roofline = _roofline(tim, "sor_sweep", 32.0, cells, ms,
+                             traffic_key=_sor64_traffic_key(s.last_solve_stats().variant))
     else:
         roofline = _roofline(tim, "momentum", 112.0, cells, ms)   # 14 doubles per cell
     iters_per_substage = iters / (3 * args.steps) if cfg["solver"] == "redblack" else 0
     sor_kernel = None
     if cfg["solver"] == "redblack":
-        names = {1: "one launch per colour sweep", 2: "fused red+black pass 32x8", 3: "fused red+black pass 32x16"}
-        sor_kernel = names.get(s.last_solve_stats().variant, "?")
+        sor_kernel = SOR_NAMES.get(s.last_solve_stats().variant, "?")
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         cpu = _cpu_baseline(cfg, iters / max(args.steps, 1))
@@ -707,7 +718,9 @@ def run_learned_mixed(args, cfg):
     plain_state = {n: sp.get(n) for n in ("un", "vn", "wn", "pn")}
     # one more step with per-kernel events, for the FP64 sweep's roofline
     _, r_ms, _, _, p_tim = _timed_steps(sp, stream_p, 1, pg, timing=True)
-    roof64 = _roofline(p_tim, "sor_sweep", 32.0, cells, r_ms)
+    roof64 = _roofline(p_tim, "sor_sweep", 32.0, cells, r_ms,
+                       traffic_key=_sor64_traffic_key(sp.last_solve_stats().variant))
+    roof64["sor_kernel"] = SOR_NAMES.get(sp.last_solve_stats().variant, "?")
     plain_c1 = None
     if not args.quick:   # the plain FP64 step at the C1 tolerance 1e-10
         sp.init_pressure_solver(M.make_solver_opts(M.SOLVER_REDBLACK, sor=cfg["sor"], tol=1e-10,
@@ -863,8 +876,12 @@ def main():
     ap.add_argument("--profile-mixed", action="store_true",
                     help="profiling run for ncu: the full-size t=0 projection with FP32 sweeps to residual 1e-8")
     ap.add_argument("--quick", action="store_true", help="skip the plain FP64 leg at residual 1e-10")
+    ap.add_argument("--sor-variant", type=int, default=0, choices=[0, 1, 2, 3, 4],
+                    help="red-black kernel variant (0: autotuned; all give the same bits)")
     ap.add_argument("--train-iters", type=int, default=1200, help="Adam steps of the learned warm start")
     args = ap.parse_args()
+    global SOR_VARIANT
+    SOR_VARIANT = args.sor_variant
     cfg = CONFIGS[args.config]
     if args.impl == "reference":
         return run_reference(args, cfg)

@@ -94,7 +94,9 @@ typedef struct {
                           first projection times each variant on one residual-check
                           block of its own iterations and keeps the fastest; 1 one
                           launch per colour; 2 fused red+black pass, 32x8 tiles;
-                          3 fused pass, 32x16 tiles (fused: periodic x and z only) */
+                          3 fused pass, 32x16 tiles; 4 one launch per colour on
+                          colour-split copies of u, v, w, p made once per projection
+                          (2-4: periodic x and z, IBM factors 1 or z-invariant) */
     int sor_kz;        /* z planes per block of the fused pass (0: default 16) */
     int check_mode;    /* red-black, tol > 0: 0 (default) residual checks at multiples of check_every,
                           up to 8 blocks apart while the residual falls at a steady rate that

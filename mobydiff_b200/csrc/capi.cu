@@ -221,6 +221,11 @@ int mdx_destroy_pressure_solver(mdx_ctx_t* ctx) {
     cudaFree(ctx->mu);
     ctx->mu = nullptr;
     ctx->mu_elems = 0;
+    for (int t = 0; t < 4; ++t) {
+        cudaFree(ctx->split_f[t]);
+        ctx->split_f[t] = nullptr;
+    }
+    ctx->split_norms = false;
     mdx_mixed_free(ctx);
     mdx_warm_free(ctx);
     ctx->solver = false;
@@ -274,7 +279,7 @@ int mdx_set_bc(mdx_ctx_t* ctx, const mdx_bc_t* bc) {
     for (int t = 0; t < 3; ++t) ctx->bcd.per[t] = bc->is_periodic[t] ? 1 : 0;
     for (int t = 0; t < 24; ++t) { ctx->bcd.type[t] = bc->bc_type[t]; ctx->bcd.value[t] = bc->bc_value[t]; }
     ctx->sor_tuned = 0;
-    for (int t = 0; t < 4; ++t) ctx->sor_tune_ms[t] = 0.0;
+    for (int t = 0; t < 8; ++t) ctx->sor_tune_ms[t] = 0.0;
     return MDX_OK;
 }
 
@@ -479,7 +484,7 @@ int mdx_init_pressure_solver(mdx_ctx_t* ctx, const mdx_solver_opts_t* opts) {
     if (o.n_iter < 0) return mdx_fail(ctx, MDX_ERR_ARG, "n_iter must be >= 0");
     ctx->opts = o;
     ctx->sor_tuned = 0;
-    for (int t = 0; t < 4; ++t) ctx->sor_tune_ms[t] = 0.0;
+    for (int t = 0; t < 8; ++t) ctx->sor_tune_ms[t] = 0.0;
     MDX_TRY(mdx_reduce_init(ctx));
     if (o.solver == MDX_SOLVER_REDBLACK) {
         // src/modules/pressure/pressure_redblack.f90:16-18

@@ -382,6 +382,72 @@ k_sor_sweep_pxz(mdx_dims d, mdx_bc_dev bc, mdx_sor_params p, int parity, int rev
     Pp[q] = pc;
 }
 
+// ---------------------------------------------------------------------------
+// The same colour sweep on colour-split copies of u, v, w, p (cidx): the
+// cells of one colour in a row and every face they touch are consecutive, so
+// a warp's loads and stores fill whole 32-byte sectors instead of every other
+// element of them.  Same per-cell arithmetic as k_sor_sweep_pxz, so the
+// same bits; the copies are made once per projection (k_split_copy).
+// ---------------------------------------------------------------------------
+template <int MU, int PY>
+__global__ void __launch_bounds__(256, 4)
+k_sor_sweep_split(mdx_dims d, mdx_bc_dev bc, mdx_sor_params p, int parity, int reverse, double* __restrict__ un,
+                  double* __restrict__ vn, double* __restrict__ wn, double* __restrict__ pn,
+                  const double* __restrict__ mu) {
+    const int ni = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int kk = blockIdx.z * blockDim.z + threadIdx.z + 1;
+    const int nx = d.nx, ny = d.ny, nz = d.nz;
+    if (ni > nx / 2 || j > ny || kk > nz) return;
+    const int k = reverse ? nz + 1 - kk : kk;
+    const int jp = (PY && j == ny) ? 1 : j + 1;
+    const int kp = (k == nz) ? 1 : k + 1;
+    const int i = 1 + ((j + k + parity) & 1) + 2 * (ni - 1);
+    const int ip = (i == nx) ? 1 : i + 1;
+    const long long c = cidx(d, i, j, k), cip = cidx(d, ip, j, k), cjp = cidx(d, i, jp, k), ckp = cidx(d, i, j, kp);
+    double mu_u_i = 1.0, mu_u_ip = 1.0, mu_v_j = 1.0, mu_v_jp = 1.0, mu_w = 1.0;
+    if (MU == MU_PLANE) {
+        const long long plane = (long long)d.nxp * d.nyp;
+        const int q = i + d.nxp * j;
+        mu_u_i = __ldg(mu + q);
+        mu_u_ip = __ldg(mu + ip + d.nxp * j);
+        mu_v_j = __ldg(mu + plane + q);
+        mu_v_jp = __ldg(mu + plane + i + d.nxp * jp);
+        mu_w = __ldg(mu + 2 * plane + q);
+    }
+    double u_i = un[c], u_ip = un[cip], v_j = vn[c], v_jp = vn[cjp], w_k = wn[c], w_kp = wn[ckp], pc = pn[c];
+    const double fac = sor_factor(mu_u_i, mu_u_ip, mu_v_j, mu_v_jp, mu_w, mu_w, p);
+    sor_cell_fac<1, PY, 1>(u_i, u_ip, v_j, v_jp, w_k, w_kp, pc, mu_u_i, mu_u_ip, mu_v_j, mu_v_jp, mu_w, mu_w, fac, p,
+                           bc, i, j, k, nx, ny, nz);
+    un[c] = u_i;
+    un[cip] = u_ip;
+    vn[c] = v_j;
+    vn[cjp] = v_jp;
+    wn[c] = w_k;
+    wn[ckp] = w_kp;
+    pn[c] = pc;
+}
+
+// Every padded element of u, v, w, p between the reference layout and the
+// colour-split copies (TO_SPLIT) or back.
+template <bool TO_SPLIT>
+__global__ void k_split_copy(mdx_dims d, double* __restrict__ a0, double* __restrict__ a1, double* __restrict__ a2,
+                             double* __restrict__ a3, double* __restrict__ s0, double* __restrict__ s1,
+                             double* __restrict__ s2, double* __restrict__ s3) {
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < d.npad; t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % d.nxp);
+        const long long r = t / d.nxp;
+        const int j = (int)(r % d.nyp);
+        const int k = (int)(r / d.nyp);
+        const long long c = cidx(d, i, j, k);
+        if (TO_SPLIT) {
+            s0[c] = a0[t]; s1[c] = a1[t]; s2[c] = a2[t]; s3[c] = a3[t];
+        } else {
+            a0[t] = s0[c]; a1[t] = s1[c]; a2[t] = s2[c]; a3[t] = s3[c];
+        }
+    }
+}
+
 static mdx_sor_params sor_params(const mdx_ctx_t* ctx, double dg) {
     const mdx_grid_t& g = ctx->g;
     mdx_sor_params p;
@@ -427,8 +493,48 @@ static int sor_iteration(mdx_ctx_t* ctx, const mdx_sor_params& p) {
 //   MDX_SORV_SWEEPS    one launch per colour sweep
 //   MDX_SORV_FUSED8    fused red+black pass, 32x8 tiles, 256 threads
 //   MDX_SORV_FUSED16   fused red+black pass, 32x16 tiles, 512 threads
-// The fused passes need periodic x and z and mu = 1 or z-invariant.
-enum { MDX_SORV_AUTO = 0, MDX_SORV_SWEEPS = 1, MDX_SORV_FUSED8 = 2, MDX_SORV_FUSED16 = 3, MDX_SORV_NUM = 4 };
+//   MDX_SORV_SPLIT     one launch per colour sweep on colour-split copies
+//                      (tol > 0 only: the copies cost two passes over u, v,
+//                      w, p per projection)
+// All but the first need periodic x and z and mu = 1 or z-invariant.
+enum {
+    MDX_SORV_AUTO = 0, MDX_SORV_SWEEPS = 1, MDX_SORV_FUSED8 = 2, MDX_SORV_FUSED16 = 3, MDX_SORV_SPLIT = 4,
+    MDX_SORV_NUM = 5
+};
+
+static int split_alloc(mdx_ctx_t* ctx) {
+    const size_t bytes = sizeof(double) * (size_t)split_elems(ctx->d);
+    for (int t = 0; t < 4; ++t)
+        if (!ctx->split_f[t]) MDX_CUDA(ctx, cudaMalloc(&ctx->split_f[t], bytes));
+    return MDX_OK;
+}
+
+// u, v, w, p into (to_split) or out of the colour-split copies.
+static int split_copy(mdx_ctx_t* ctx, bool to_split) {
+    const mdx_dims& d = ctx->d;
+    double** f = ctx->f;
+    double** s = ctx->split_f;
+    const int nb = (int)std::min<long long>((d.npad + 255) / 256, 148 * 16);
+    auto kfn = to_split ? k_split_copy<true> : k_split_copy<false>;
+    MDX_LAUNCH(ctx, MDX_T_OTHER, "split copy", kfn, nb, 256, 0, d, f[MDX_UN], f[MDX_VN], f[MDX_WN], f[MDX_PN], s[0],
+               s[1], s[2], s[3]);
+    ctx->split_norms = to_split;
+    return MDX_OK;
+}
+
+static int sor_split_iteration(mdx_ctx_t* ctx, const mdx_sor_params& p) {
+    const mdx_dims& d = ctx->d;
+    double** s = ctx->split_f;
+    dim3 block(32, 4, 2);
+    dim3 grid((d.nx / 2 + 31) / 32, (d.ny + 3) / 4, (d.nz + 1) / 2);
+    const bool py = ctx->bc.is_periodic[1] != 0;
+    auto kfn = ctx->mu_mode == MU_PLANE ? (py ? k_sor_sweep_split<MU_PLANE, 1> : k_sor_sweep_split<MU_PLANE, 0>)
+                                        : (py ? k_sor_sweep_split<MU_ONE, 1> : k_sor_sweep_split<MU_ONE, 0>);
+    for (int parity = 0; parity < 2; ++parity)
+        MDX_LAUNCH(ctx, MDX_T_SOR_SWEEP, "sor sweep split", kfn, grid, block, 0, d, ctx->bcd, p, parity, parity, s[0],
+                   s[1], s[2], s[3], ctx->mu);
+    return MDX_OK;
+}
 
 template <int MU, int TY, int NT>
 static size_t fused_smem() {
@@ -491,6 +597,7 @@ static int sor_fused_iteration(mdx_ctx_t* ctx, const mdx_sor_params& p) {
 }
 
 static int sor_iterate(mdx_ctx_t* ctx, const mdx_sor_params& p, int variant) {
+    if (variant == MDX_SORV_SPLIT) return sor_split_iteration(ctx, p);
     if (variant == MDX_SORV_FUSED8) return sor_fused_iteration<8, 256>(ctx, p);
     if (variant == MDX_SORV_FUSED16) return sor_fused_iteration<16, 512>(ctx, p);
     return sor_iteration(ctx, p);
@@ -559,10 +666,21 @@ int mdx_k_projection_redblack(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t* st) 
     // the next untried candidate for each residual-check block
     const bool fok = fused_ok(ctx);
     int want = ctx->opts.sor_variant;
-    if ((want == MDX_SORV_FUSED8 || want == MDX_SORV_FUSED16) && !fok) want = MDX_SORV_SWEEPS;
-    if (want == MDX_SORV_AUTO && !fok) want = MDX_SORV_SWEEPS;
-    if (want != MDX_SORV_SWEEPS) MDX_TRY(fused_prepare(ctx));
+    if (want < MDX_SORV_AUTO || want >= MDX_SORV_NUM) want = MDX_SORV_AUTO;
+    if (want != MDX_SORV_SWEEPS && !fok) want = MDX_SORV_SWEEPS;
+    if (want == MDX_SORV_AUTO || want == MDX_SORV_FUSED8 || want == MDX_SORV_FUSED16) MDX_TRY(fused_prepare(ctx));
+    if (want == MDX_SORV_AUTO || want == MDX_SORV_SPLIT) MDX_TRY(split_alloc(ctx));
     const mdx_sor_params p = sor_params(ctx, dg);
+    // where u, v, w, p live while the sweeps run: the colour-split copies for
+    // MDX_SORV_SPLIT blocks, the reference arrays for the others
+    bool in_split = false;
+    auto layout_for = [&](int v) -> int {
+        if ((v == MDX_SORV_SPLIT) != in_split) {
+            in_split = !in_split;
+            MDX_TRY(split_copy(ctx, in_split));
+        }
+        return MDX_OK;
+    };
     auto pick = [&]() -> int {
         if (want != MDX_SORV_AUTO) return want;
         if (ctx->sor_tuned > 0) return ctx->sor_tuned;
@@ -578,7 +696,9 @@ int mdx_k_projection_redblack(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t* st) 
     s.guessed = guessed ? 1 : 0;
     if (o.tol <= 0.0) {
         const int v = (want == MDX_SORV_AUTO) ? (ctx->sor_tuned > 0 ? ctx->sor_tuned : MDX_SORV_SWEEPS) : want;
+        MDX_TRY(layout_for(v));
         for (int it = 0; it < o.n_iter; ++it) MDX_TRY(sor_iterate(ctx, p, v));
+        MDX_TRY(layout_for(MDX_SORV_SWEEPS));
         s.variant = v;
         s.iterations = o.n_iter;
         s.status = MDX_OK;
@@ -600,13 +720,16 @@ int mdx_k_projection_redblack(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t* st) 
             while (it < o.max_iter) {
                 const int m = std::min(block, o.max_iter - it);
                 const int v = pick();
+                MDX_TRY(layout_for(v));
                 const bool timing_block = want == MDX_SORV_AUTO && ctx->sor_tuned == 0;
                 if (timing_block) MDX_CUDA(ctx, cudaEventRecord(ctx->tune_ev[0], ctx->stream));
                 for (int q = 0; q < m; ++q) MDX_TRY(sor_iterate(ctx, p, v));
                 if (timing_block) MDX_CUDA(ctx, cudaEventRecord(ctx->tune_ev[1], ctx->stream));
                 it += m;
                 s.variant = v;
-                MDX_TRY(mdx_k_div_norms(ctx, f[MDX_UN], f[MDX_VN], f[MDX_WN], &r, &linf));
+                double** uvw = in_split ? ctx->split_f : nullptr;
+                MDX_TRY(mdx_k_div_norms(ctx, uvw ? uvw[0] : f[MDX_UN], uvw ? uvw[1] : f[MDX_VN],
+                                        uvw ? uvw[2] : f[MDX_WN], &r, &linf));
                 if (timing_block) {   // the norms synchronised the stream; time per iteration
                     float ms = 0.f;
                     if (cudaEventElapsedTime(&ms, ctx->tune_ev[0], ctx->tune_ev[1]) == cudaSuccess)
@@ -616,6 +739,7 @@ int mdx_k_projection_redblack(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t* st) 
                 if (r <= target) { s.status = MDX_OK; break; }
                 block = cs.next(it, r, target);
             }
+            MDX_TRY(layout_for(MDX_SORV_SWEEPS));
             s.iterations = it;
             s.residual = r / r0;
         }

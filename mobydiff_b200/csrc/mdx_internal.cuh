@@ -100,8 +100,8 @@ struct mdx_ctx {
     double* f[MDX_NUM_FIELDS] = {nullptr};   // device mirrors (MDX_PHI -> phi)
     bool ibm_zero = true;                    // all IBM coefficients zero
     bool coef_zinv = false;                  // coefficients equal on every z plane
-    double* sor_alt[4] = {nullptr};          // second u,v,w,p state of the fused red-black pass, or the
-                                             // colour-split working copies of the split sweeps
+    double* sor_alt[4] = {nullptr};          // second u,v,w,p state of the fused red-black pass
+    double* split_f[4] = {nullptr};          // colour-split copies of u,v,w,p (split sweeps)
     bool split_norms = false;                // divergence norms read colour-split arrays
     bool fused_attr = false;
     // mixed-precision red-black: FP32 corrections, FP32 residual, IBM tables,
@@ -123,7 +123,7 @@ struct mdx_ctx {
     long long proj_count = 0;                // projections since the t=0 projection
     void* unet = nullptr;                    // learned warm start (k_unet.cu)
     int sor_tuned = 0;                       // red-black kernel variant chosen by the autotuner (0: not yet)
-    double sor_tune_ms[4] = {0.0};           // time per iteration of a timed residual-check block, per variant
+    double sor_tune_ms[8] = {0.0};           // time per iteration of a timed residual-check block, per variant
     cudaEvent_t tune_ev[2] = {nullptr, nullptr};
     double* mu = nullptr;                    // red-black IBM factors 1/(1+dt_gamma*coef)
     long long mu_elems = 0;
