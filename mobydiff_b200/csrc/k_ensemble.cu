@@ -1078,9 +1078,9 @@ std::string tune_key(const mdx_ensemble_t* E) {
     mix((uint64_t)(E->opts.tol > 0.0));
     cudaDeviceProp prop{};
     cudaGetDeviceProperties(&prop, E->device);
-    char buf[256];
-    snprintf(buf, sizeof(buf), "%s/%016llx", prop.name, (unsigned long long)h);
-    return buf;
+    char hex[17];
+    snprintf(hex, sizeof(hex), "%016llx", (unsigned long long)h);
+    return std::string(prop.name) + "/" + hex;
 }
 
 // The cache is a JSON object {"<key>": {"threads": T, "blocks_per_sm": B, "low_regs": R, "ms": M}, ...}.

@@ -22,14 +22,13 @@
 #include <cmath>
 
 // mu = 1/(1 + dt_gamma*coef) over n elements of each component.
-__global__ void k_mu_tables(long long n, long long stride_in, double dg, const double* __restrict__ cu,
-                            const double* __restrict__ cv, const double* __restrict__ cw, double* __restrict__ mu) {
+__global__ void k_mu_tables(long long n, double dg, const double* __restrict__ cu, const double* __restrict__ cv,
+                            const double* __restrict__ cw, double* __restrict__ mu) {
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
         mu[t] = 1.0 / (1.0 + dg * __ldg(cu + t));
         mu[n + t] = 1.0 / (1.0 + dg * __ldg(cv + t));
         mu[2 * n + t] = 1.0 / (1.0 + dg * __ldg(cw + t));
     }
-    (void)stride_in;
 }
 
 
@@ -44,8 +43,6 @@ k_sor_sweep(mdx_dims d, mdx_bc_dev bc, mdx_sor_params p, int parity, int reverse
     const int nx = d.nx, ny = d.ny, nz = d.nz;
     if (ni > nx / 2 || j > ny || kk > nz) return;
     const int k = reverse ? nz + 1 - kk : kk;
-    const int* T = bc.type;
-    const double* V = bc.value;
     const bool perx = bc.per[0] != 0, pery = bc.per[1] != 0, perz = bc.per[2] != 0;
     int jp = j + 1;
     if (pery && jp > ny) jp = 1;
@@ -55,11 +52,8 @@ k_sor_sweep(mdx_dims d, mdx_bc_dev bc, mdx_sor_params p, int parity, int reverse
     const int i = iLo + 2 * (ni - 1);
     int ip = i + 1;
     if (perx && ip > nx) ip = 1;
-    const double dg = p.dt_gamma;
     const long long c = pidx(d, i, j, k);
     const long long cip = pidx(d, ip, j, k), cjp = pidx(d, i, jp, k), ckp = pidx(d, i, j, kp);
-
-    (void)dg;
     double mu_u_i = 1.0, mu_u_ip = 1.0, mu_v_j = 1.0, mu_v_jp = 1.0, mu_w_k = 1.0, mu_w_kp = 1.0;
     if (MU == MU_PLANE) {  // :117-122, z-invariant coefficients
         const long long np = (long long)d.nxp * d.nyp;
@@ -89,8 +83,6 @@ k_sor_sweep(mdx_dims d, mdx_bc_dev bc, mdx_sor_params p, int parity, int reverse
     wn[c] = w_k;
     wn[ckp] = w_kp;
     pn[c] = pc;
-    (void)T;
-    (void)V;
 }
 
 // ---------------------------------------------------------------------------
@@ -620,7 +612,7 @@ static int mu_tables(mdx_ctx_t* ctx, double dg) {
     }
     ctx->mu_mode = plane ? MU_PLANE : MU_FULL;
     const int nb = (int)std::min<long long>((n + 255) / 256, 4096);
-    MDX_LAUNCH(ctx, MDX_T_OTHER, "mu tables", k_mu_tables, nb, 256, 0, n, 0LL, dg, ctx->f[MDX_COEF_U],
+    MDX_LAUNCH(ctx, MDX_T_OTHER, "mu tables", k_mu_tables, nb, 256, 0, n, dg, ctx->f[MDX_COEF_U],
                ctx->f[MDX_COEF_V], ctx->f[MDX_COEF_W], ctx->mu);
     return MDX_OK;
 }
