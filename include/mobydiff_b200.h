@@ -408,7 +408,10 @@ typedef struct {
     int capacity;           /* snapshots kept on the device for training        */
     double slope;           /* leaky-ReLU slope, (0, 1]; 1 makes the net linear */
     uint64_t seed;          /* weight initialisation                            */
-    int reserved_i[8];
+    int conv_kernel;        /* 0 (default): forward convolutions and data gradients on levels whose
+                               nx is a multiple of 128 run on tcgen05 (tensor-memory accumulators),
+                               the rest on mma.sync; 1: mma.sync everywhere                  */
+    int reserved_i[7];
     double reserved_d[8];
 } mdx_unet_opts_t;
 
@@ -422,7 +425,8 @@ typedef struct {
     double last_gain;       /* ||div|| after the extrapolated guess / after the correction */
     double infer_ms;        /* device time of the last correction               */
     double train_ms;        /* device time of the last mdx_unet_train call      */
-    double reserved_d[6];
+    long long tc_convs;     /* convolution launches on tcgen05 since creation   */
+    double reserved_d[5];
 } mdx_unet_stats_t;
 
 void mdx_default_unet_opts(mdx_unet_opts_t* opts);

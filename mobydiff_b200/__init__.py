@@ -95,13 +95,15 @@ class SolveStatsT(C.Structure):
 
 class UnetOptsT(C.Structure):
     _fields_ = [("channels0", C.c_int), ("channels", C.c_int), ("extra_bottleneck", C.c_int), ("capacity", C.c_int),
-                ("slope", C.c_double), ("seed", C.c_uint64), ("reserved_i", C.c_int * 8), ("reserved_d", C.c_double * 8)]
+                ("slope", C.c_double), ("seed", C.c_uint64), ("conv_kernel", C.c_int), ("reserved_i", C.c_int * 7),
+                ("reserved_d", C.c_double * 8)]
 
 
 class UnetStatsT(C.Structure):
     _fields_ = [("corrections", C.c_longlong), ("rejected", C.c_longlong), ("snapshots", C.c_longlong),
                 ("stored", C.c_int), ("trained", C.c_int), ("out_scale", C.c_double), ("last_gain", C.c_double),
-                ("infer_ms", C.c_double), ("train_ms", C.c_double), ("reserved_d", C.c_double * 6)]
+                ("infer_ms", C.c_double), ("train_ms", C.c_double), ("tc_convs", C.c_longlong),
+                ("reserved_d", C.c_double * 5)]
 
 
 class MemberT(C.Structure):
@@ -537,7 +539,7 @@ class Solver:
 
     # ---- learned warm start ----------------------------------------------
     def unet_create(self, channels: int = 32, extra_bottleneck: int = 0, capacity: int = 64, slope: float = 0.1,
-                    seed: int = 20261203) -> None:
+                    seed: int = 20261203, tcgen05: bool = True) -> None:
         o = UnetOptsT()
         lib().mdx_default_unet_opts(C.byref(o))
         o.channels = channels
@@ -545,6 +547,7 @@ class Solver:
         o.capacity = capacity
         o.slope = slope
         o.seed = seed
+        o.conv_kernel = 0 if tcgen05 else 1
         self._c(lib().mdx_unet_create(self.h, C.byref(o)))
 
     def unet_destroy(self) -> None:

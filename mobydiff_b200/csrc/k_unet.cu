@@ -19,7 +19,10 @@
 // forward pass and [26-tap][cin][cout] for the data gradient; FP32 master
 // weights, gradients and Adam moments in one flat vector.
 //
-// Kernels: the 3x3x3 convolution is an implicit GEMM on mma.sync
+// Kernels: on levels whose nx is a multiple of 128 the forward convolution
+// and the data gradient run on the tcgen05 tensor cores with accumulators in
+// tensor memory (k_conv3_tc, mdx_conv_tc.cuh); elsewhere, and for the weight
+// gradient, the 3x3x3 convolution is an implicit GEMM on mma.sync
 // m16n8k16 (BF16 in, FP32 accumulate).  A CTA computes a 16x4x4 tile of
 // output cells times all output channels: its input halo (18x6x6 cells) and
 // all 27 taps of the weights are staged in shared memory by cp.async, and
@@ -34,6 +37,8 @@
 #include "mdx_internal.cuh"
 
 #include <cuda_bf16.h>
+
+#include "mdx_conv_tc.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -757,12 +762,26 @@ struct mdx_unet {
     uint64_t order_state = 0;
     mdx_unet_stats_t st{};
     cudaEvent_t ev[2] = {nullptr, nullptr};
+    int* tc_err = nullptr;      // set by a tcgen05 convolution whose bounded wait gave up
 };
 
 namespace {
 
+// Output rows per CTA of the tcgen05 convolution: 4 x 2 for 16 input
+// channels, 2 x 2 for 32 (the staged halo then fills most of shared memory).
+template <int CIN>
+struct tc_rows {
+    static constexpr int RY = CIN == 16 ? 4 : 2, RZ = 2;
+};
+
 template <int CIN, int COUT>
 int set_attrs(mdx_ctx_t* ctx) {
+    using R = tc_rows<CIN>;
+    constexpr int tsmem = tc::geom<CIN, COUT, R::RY, R::RZ>::SMEM;
+    MDX_CUDA(ctx, cudaFuncSetAttribute(k_conv3_tc<CIN, COUT, 0, R::RY, R::RZ, lvl>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, tsmem));
+    MDX_CUDA(ctx, cudaFuncSetAttribute(k_conv3_tc<CIN, COUT, 1, R::RY, R::RZ, lvl>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, tsmem));
     MDX_CUDA(ctx, cudaFuncSetAttribute(k_conv3<CIN, COUT, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        conv_smem<CIN, COUT>()));
     MDX_CUDA(ctx, cudaFuncSetAttribute(k_conv3<CIN, COUT, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -781,8 +800,18 @@ int ntiles_host(const lvl& L) {
 }
 
 template <int CIN, int COUT, int EPI>
-int conv_launch(mdx_ctx_t* ctx, const lvl& L, int pery, const bf16* X, const bf16* W, const float* b, float slope,
-                bf16* Yb, float* Yf) {
+int conv_launch(mdx_ctx_t* ctx, mdx_unet* U, const lvl& L, int pery, const bf16* X, const bf16* W, const float* b,
+                float slope, bf16* Yb, float* Yf) {
+    if (U->o.conv_kernel == 0 && L.nx % tc::XT == 0) {   // tcgen05, whole 128-voxel rows
+        using R = tc_rows<CIN>;
+        auto tfn = k_conv3_tc<CIN, COUT, EPI, R::RY, R::RZ, lvl>;
+        constexpr int tsmem = tc::geom<CIN, COUT, R::RY, R::RZ>::SMEM;
+        const dim3 grid(L.nx / tc::XT, (L.ny + R::RY - 1) / R::RY, (L.nz + R::RZ - 1) / R::RZ);
+        MDX_LAUNCH(ctx, MDX_T_OTHER, "unet conv tc", tfn, grid, tc::THREADS, tsmem, L, pery, X, W, b, slope, Yb, Yf,
+                   U->tc_err);
+        U->st.tc_convs++;
+        return MDX_OK;
+    }
     auto kfn = k_conv3<CIN, COUT, EPI>;
     constexpr int smem = conv_smem<CIN, COUT>();
     MDX_LAUNCH(ctx, MDX_T_OTHER, "unet conv", kfn, ntiles_host(L), 256, smem, L, pery, X, W, b, slope, Yb, Yf);
@@ -798,8 +827,8 @@ int conv_run(mdx_ctx_t* ctx, mdx_unet* U, const conv_layer& c, bool data_grad, c
     const bf16* W = data_grad ? c.wt : c.wf;
 #define MDX_CONV_CASE(A, B)                                                                               \
     if (ci == A && co == B)                                                                               \
-        return data_grad ? conv_launch<A, B, 1>(ctx, L, U->pery, X, W, b, slope, Yb, Yf)                  \
-                         : conv_launch<A, B, 0>(ctx, L, U->pery, X, W, b, slope, Yb, Yf);
+        return data_grad ? conv_launch<A, B, 1>(ctx, U, L, U->pery, X, W, b, slope, Yb, Yf)               \
+                         : conv_launch<A, B, 0>(ctx, U, L, U->pery, X, W, b, slope, Yb, Yf);
     MDX_CONV_CASE(16, 16)
     MDX_CONV_CASE(16, 32)
     MDX_CONV_CASE(32, 16)
@@ -1001,6 +1030,8 @@ int alloc_net(mdx_ctx_t* ctx, mdx_unet* U) {
     if (U->o.capacity > 0) MDX_TRY(dalloc(ctx, &U->snap, (long long)U->o.capacity * (NIN + 1) * n0));
     MDX_CUDA(ctx, cudaEventCreate(&U->ev[0]));
     MDX_CUDA(ctx, cudaEventCreate(&U->ev[1]));
+    MDX_CUDA(ctx, cudaMalloc(&U->tc_err, sizeof(int)));
+    MDX_CUDA(ctx, cudaMemsetAsync(U->tc_err, 0, sizeof(int), ctx->stream));
     MDX_TRY((set_attrs<16, 16>(ctx)));
     MDX_TRY((set_attrs<16, 32>(ctx)));
     MDX_TRY((set_attrs<32, 16>(ctx)));
@@ -1017,6 +1048,16 @@ int loss_grad(mdx_ctx_t* ctx, mdx_unet* U, const float* in4, const float* t, flo
     MDX_TRY(forward(ctx, U));
     MDX_TRY(head_train(ctx, U, t, tscale, out));
     MDX_TRY(backward(ctx, U));
+    return MDX_OK;
+}
+
+// A tcgen05 convolution whose bounded wait gave up leaves *tc_err set: read
+// it (synchronising) where the caller synchronises anyway.
+int check_tc(mdx_ctx_t* ctx, mdx_unet* U) {
+    int e = 0;
+    MDX_CUDA(ctx, cudaMemcpyAsync(&e, U->tc_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    MDX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (e) return mdx_fail(ctx, MDX_ERR_TIMEOUT, "unet: a tensor-core convolution timed out waiting for its MMAs");
     return MDX_OK;
 }
 
@@ -1058,6 +1099,7 @@ void mdx_unet_free(mdx_ctx_t* ctx) {
     cudaFree(U->snap);
     if (U->ev[0]) cudaEventDestroy(U->ev[0]);
     if (U->ev[1]) cudaEventDestroy(U->ev[1]);
+    cudaFree(U->tc_err);
     delete U;
     ctx->unet = nullptr;
 }
@@ -1101,6 +1143,7 @@ int mdx_unet_correct(mdx_ctx_t* ctx, double dg, double* rg) {
     MDX_CUDA(ctx, cudaEventRecord(U->ev[1], ctx->stream));
     double r = 0.0, linf = 0.0;
     MDX_TRY(mdx_k_div_norms(ctx, ctx->f[MDX_UN], ctx->f[MDX_VN], ctx->f[MDX_WN], &r, &linf));
+    MDX_TRY(check_tc(ctx, U));
     float ms = 0.f;
     if (cudaEventElapsedTime(&ms, U->ev[0], U->ev[1]) == cudaSuccess) U->st.infer_ms = ms;
     if (r < *rg) {
@@ -1307,6 +1350,7 @@ int mdx_unet_loss_grad(mdx_ctx_t* ctx, const float* in4, const float* target, do
     }
     if (dout) cudaFree(dout);
     if (loss) *loss = (double)sse / (double)n;
+    if (rc == MDX_OK) rc = check_tc(ctx, U);
     return rc;
 }
 
@@ -1365,6 +1409,7 @@ int mdx_unet_train(mdx_ctx_t* ctx, int iters, double lr, double* loss_first, dou
     MDX_CUDA(ctx, cudaEventSynchronize(U->ev[1]));
     float ms = 0.f;
     if (cudaEventElapsedTime(&ms, U->ev[0], U->ev[1]) == cudaSuccess) U->st.train_ms = ms;
+    MDX_TRY(check_tc(ctx, U));
     U->trained = true;
     if (loss_first) *loss_first = (double)sse_first / (double)n;
     if (loss_last) *loss_last = (double)sse_last / (double)n;

@@ -55,6 +55,42 @@ def test_unet_loss_and_gradients_match_cpu_network(c1, pery, extra):
         assert rel_l2(gg, gc) <= 3e-2
 
 
+@pytest.mark.parametrize("pery", [False, True])
+def test_tcgen05_convolutions_match_mma_and_cpu_network(pery):
+    """On a grid whose finest level is 128 cells wide the forward convolutions
+    and data gradients of level 0 run on tcgen05 with tensor-memory
+    accumulators: the pass agrees with the mma.sync kernels and with the CPU
+    network within the bounds of the test above, and the launch list shows
+    the tcgen05 kernel ran."""
+    nx, ny, nz = 128, 16, 16
+    n = nx * ny * nz
+    slope = 0.1
+    rng = np.random.default_rng(9)
+    in4 = rng.standard_normal((4, n)).astype(np.float32)
+    t = rng.standard_normal(n).astype(np.float32)
+    net = UO.Net(c0=16, c1=32, extra=0, slope=slope, pery=pery)
+    p = UO.init_params(net, 21).astype(np.float32)
+    res, launches = {}, {}
+    s = _plain_solver(nx, ny, nz, pery)
+    with s:
+        for tc in (True, False):
+            s.unet_create(channels=32, capacity=0, slope=slope, tcgen05=tc)
+            s.unet_set_params(p)
+            res[tc] = s.unet_loss_grad(in4, t)
+            launches[tc] = s.unet_stats().tc_convs
+            s.unet_destroy()
+    # level 0 (nx 128): three forward convolutions and two data gradients
+    assert launches[True] == 5 and launches[False] == 0, launches
+    lc, gc, oc = UO.loss_grad(net, p.astype(np.float64), in4, t, (nx, ny, nz), bf16=True)
+    (lt, gt, ot), (lm, gm, om) = res[True], res[False]
+    print("loss tc", lt, "mma", lm, "cpu", lc, "out tc-mma", rel_l2(ot, om), "grad tc-mma", rel_l2(gt, gm))
+    assert rel_l2(ot, om) <= 1e-2 and rel_l2(gt, gm) <= 3e-2
+    for lg, gg, og in ((lt, gt, ot), (lm, gm, om)):
+        assert abs(lg - lc) <= 5e-3 * lc
+        assert rel_l2(og, oc) <= 1.5e-2
+        assert rel_l2(gg, gc) <= 3e-2
+
+
 def _wavy(seed, re, mode, nx=64, ny=32, nz=32, amp=0.05, tol=1e-8):
     ly = 2.25
     y0 = (ly - 2.0) / 2
