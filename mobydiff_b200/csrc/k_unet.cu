@@ -21,7 +21,7 @@
 //
 // Kernels: on levels whose nx is a multiple of 128 the forward convolution
 // and the data gradient run on the tcgen05 tensor cores with accumulators in
-// tensor memory (k_conv3_tc, mdx_conv_tc.cuh); elsewhere, and for the weight
+// tensor memory (k_conv3_tcp, mdx_conv_tc.cuh); elsewhere, and for the weight
 // gradient, the 3x3x3 convolution is an implicit GEMM on mma.sync
 // m16n8k16 (BF16 in, FP32 accumulate).  A CTA computes a 16x4x4 tile of
 // output cells times all output channels: its input halo (18x6x6 cells) and
@@ -767,20 +767,23 @@ struct mdx_unet {
 
 namespace {
 
-// Output rows per CTA of the tcgen05 convolution: 4 x 2 for 16 input
-// channels, 2 x 2 for 32 (the staged halo then fills most of shared memory).
-template <int CIN>
-struct tc_rows {
-    static constexpr int RY = CIN == 16 ? 4 : 2, RZ = 2;
+// tcgen05 convolution: output rows per CTA (4 for 16 input channels, 2 for
+// 32: four staged planes then fill most of shared memory) and z planes per
+// CTA (4 for the 16->16 layers, 8 where the staged weights are larger),
+// measured on the C1 level sizes.
+template <int CIN, int COUT>
+struct tc_cfg {
+    static constexpr int RY = CIN == 16 ? 4 : 2;
+    static constexpr int ZC = CIN * COUT >= 512 ? 8 : 4;
 };
 
 template <int CIN, int COUT>
 int set_attrs(mdx_ctx_t* ctx) {
-    using R = tc_rows<CIN>;
-    constexpr int tsmem = tc::geom<CIN, COUT, R::RY, R::RZ>::SMEM;
-    MDX_CUDA(ctx, cudaFuncSetAttribute(k_conv3_tc<CIN, COUT, 0, R::RY, R::RZ, lvl>,
+    using R = tc_cfg<CIN, COUT>;
+    constexpr int tsmem = tc::pgeom<CIN, COUT, R::RY>::SMEM;
+    MDX_CUDA(ctx, cudaFuncSetAttribute(k_conv3_tcp<CIN, COUT, 0, R::RY, lvl>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, tsmem));
-    MDX_CUDA(ctx, cudaFuncSetAttribute(k_conv3_tc<CIN, COUT, 1, R::RY, R::RZ, lvl>,
+    MDX_CUDA(ctx, cudaFuncSetAttribute(k_conv3_tcp<CIN, COUT, 1, R::RY, lvl>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, tsmem));
     MDX_CUDA(ctx, cudaFuncSetAttribute(k_conv3<CIN, COUT, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        conv_smem<CIN, COUT>()));
@@ -803,12 +806,12 @@ template <int CIN, int COUT, int EPI>
 int conv_launch(mdx_ctx_t* ctx, mdx_unet* U, const lvl& L, int pery, const bf16* X, const bf16* W, const float* b,
                 float slope, bf16* Yb, float* Yf) {
     if (U->o.conv_kernel == 0 && L.nx % tc::XT == 0) {   // tcgen05, whole 128-voxel rows
-        using R = tc_rows<CIN>;
-        auto tfn = k_conv3_tc<CIN, COUT, EPI, R::RY, R::RZ, lvl>;
-        constexpr int tsmem = tc::geom<CIN, COUT, R::RY, R::RZ>::SMEM;
-        const dim3 grid(L.nx / tc::XT, (L.ny + R::RY - 1) / R::RY, (L.nz + R::RZ - 1) / R::RZ);
-        MDX_LAUNCH(ctx, MDX_T_OTHER, "unet conv tc", tfn, grid, tc::THREADS, tsmem, L, pery, X, W, b, slope, Yb, Yf,
-                   U->tc_err);
+        using R = tc_cfg<CIN, COUT>;
+        auto tfn = k_conv3_tcp<CIN, COUT, EPI, R::RY, lvl>;
+        constexpr int tsmem = tc::pgeom<CIN, COUT, R::RY>::SMEM;
+        const dim3 grid(L.nx / tc::XT, (L.ny + R::RY - 1) / R::RY, (L.nz + R::ZC - 1) / R::ZC);
+        MDX_LAUNCH(ctx, MDX_T_OTHER, "unet conv tc", tfn, grid, tc::THREADS, tsmem, L, pery, R::ZC, X, W, b, slope,
+                   Yb, Yf, U->tc_err);
         U->st.tc_convs++;
         return MDX_OK;
     }

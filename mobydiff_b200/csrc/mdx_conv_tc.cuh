@@ -1,13 +1,13 @@
 // mdx_conv_tc.cuh -- 3x3x3 convolution of the learned warm start on the
 // Blackwell tensor cores (tcgen05.mma, FP32 accumulators in tensor memory).
 //
-// Implicit GEMM per CTA: D[128 voxels x COUT] += A[128 x 16] B[16 x COUT] for
-// every tap (27) and 16-channel slice of the input, for R = RY x RZ output
-// rows of 128 consecutive x voxels each (one accumulator of COUT tensor-memory
-// columns per row).  Activations are channels-last BF16 [z][y][x][C]; the
-// CTA stages its input halo -- 130 x voxels (x0-1 .. x0+128), RY+2 rows, RZ+2
-// planes, wrapped in x and z (and y when periodic), zero beyond y walls --
-// in shared memory as [z][y][8-channel chunk][x][8 x bf16], so that the A
+// Implicit GEMM: D[128 voxels x COUT] += A[128 x 16] B[16 x COUT] for every
+// tap (27) and 16-channel slice of the input, for RY output rows of 128
+// consecutive x voxels (one accumulator of COUT tensor-memory columns per
+// row).  Activations are channels-last BF16 [z][y][x][C]; input planes --
+// 130 x voxels (x0-1 .. x0+128) by RY+2 rows, wrapped in x and z (and y when
+// periodic), zero beyond y walls -- are staged in shared memory as
+// [y][8-channel chunk][x][8 x bf16], so that the A
 // operand of a tap is the same canonical no-swizzle K-major layout shifted
 // by whole 16-byte voxels: core matrices of 8 voxels x 16 bytes, 128 bytes
 // apart along M, one halo row apart (130 x 16 bytes) along K.  The weights
@@ -30,16 +30,6 @@ constexpr int XT = 128;            // voxels per output row (the MMA's M)
 constexpr int HXT = XT + 2;        // halo voxels per row
 constexpr int THREADS = 128;       // one warpgroup: four warps own the 128 tensor-memory lanes
 constexpr unsigned long long WAIT_NS = 1000000000ull;
-
-template <int CIN, int COUT, int RY, int RZ>
-struct geom {
-    static constexpr int CH = CIN / 8;                          // 16-byte chunks per voxel
-    static constexpr int R = RY * RZ;                           // output rows per CTA
-    static constexpr int W_BYTES = 27 * CH * COUT * 16;
-    static constexpr int H_BYTES = (RZ + 2) * (RY + 2) * CH * HXT * 16;
-    static constexpr int COLS = R * COUT <= 32 ? 32 : (R * COUT <= 64 ? 64 : (R * COUT <= 128 ? 128 : 256));
-    static constexpr int SMEM = 128 + W_BYTES + H_BYTES;   // 128: mbarrier and tensor-memory address
-};
 
 __device__ __forceinline__ unsigned s32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
@@ -114,25 +104,45 @@ __device__ __forceinline__ void tmem_ld<32>(unsigned taddr, float* v) {
 
 }  // namespace tc
 
-// EPI 0: y = leaky(acc + bias) stored BF16; EPI 1: acc stored FP32.
-// The level's (nx, ny, nz) and n come in through the same `L` struct the
-// mma.sync kernel takes; grid = (nx/128) x ceil(ny/RY) x ceil(nz/RZ) CTAs.
-// *err is set when a bounded wait gives up.
-template <int CIN, int COUT, int EPI, int RY, int RZ, typename LVL>
+// ---------------------------------------------------------------------------
+// The staging is pipelined across z: a CTA walks a chunk of zc planes for one
+// (128-voxel x, RY-row y) column.  Its weights are staged once; input planes
+// sit in a ring of 4 slots (plane z in slot (z - z_first + 1) mod 4); each
+// step issues the MMAs of plane z into one of two accumulator sets, then --
+// while they run -- reads back the other set (plane z-1) for the epilogue
+// and, once plane z-1's MMAs are done, stages plane z+2 into the slot plane
+// z-2 used.  EPI 0: y = leaky(acc + bias) stored BF16; EPI 1: acc stored FP32.
+// Grid: (nx/128) x ceil(ny/RY) x ceil(nz/zc).  *err is set when a bounded
+// wait gives up.
+// ---------------------------------------------------------------------------
+namespace tc {
+template <int CIN, int COUT, int RY>
+struct pgeom {
+    static constexpr int CH = CIN / 8;
+    static constexpr int SLOTS = 4;
+    static constexpr int PLANE_BYTES = (RY + 2) * CH * HXT * 16;
+    static constexpr int W_BYTES = 27 * CH * COUT * 16;
+    static constexpr int NCOL = 2 * RY * COUT;   // two accumulator sets
+    static constexpr int COLS = NCOL <= 32 ? 32 : (NCOL <= 64 ? 64 : (NCOL <= 128 ? 128 : (NCOL <= 256 ? 256 : 512)));
+    static constexpr int SMEM = 128 + W_BYTES + SLOTS * PLANE_BYTES;
+};
+}  // namespace tc
+
+template <int CIN, int COUT, int EPI, int RY, typename LVL>
 __global__ void __launch_bounds__(tc::THREADS, 1)
-k_conv3_tc(LVL L, int pery, const __nv_bfloat16* __restrict__ X, const __nv_bfloat16* __restrict__ W,
-           const float* __restrict__ bias, float slope, __nv_bfloat16* __restrict__ Yb, float* __restrict__ Yf,
-           int* __restrict__ err) {
-    using G = tc::geom<CIN, COUT, RY, RZ>;
+k_conv3_tcp(LVL L, int pery, int zc, const __nv_bfloat16* __restrict__ X, const __nv_bfloat16* __restrict__ W,
+            const float* __restrict__ bias, float slope, __nv_bfloat16* __restrict__ Yb, float* __restrict__ Yf,
+            int* __restrict__ err) {
+    using G = tc::pgeom<CIN, COUT, RY>;
     extern __shared__ __align__(1024) unsigned char smem[];
-    unsigned long long* bar = reinterpret_cast<unsigned long long*>(smem);
+    unsigned long long* bars = reinterpret_cast<unsigned long long*>(smem);   // two mbarriers
     unsigned* taddr_slot = reinterpret_cast<unsigned*>(smem + 16);
     unsigned char* sw = smem + 128;
-    unsigned char* sx = sw + G::W_BYTES;
-    const int x0 = blockIdx.x * tc::XT, y0 = blockIdx.y * RY, z0 = blockIdx.z * RZ;
+    unsigned char* ring = sw + G::W_BYTES;
+    const int x0 = blockIdx.x * tc::XT, y0 = blockIdx.y * RY, zb = blockIdx.z * zc;
+    const int nsteps = min(zc, L.nz - zb);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
-    // tensor memory for the R accumulators (warp 0 allocates and frees)
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(tc::s32(taddr_slot)),
                      "r"((unsigned)G::COLS)
@@ -140,76 +150,51 @@ k_conv3_tc(LVL L, int pery, const __nv_bfloat16* __restrict__ X, const __nv_bflo
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
     }
     if (threadIdx.x == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(tc::s32(bar)) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(tc::s32(bars)) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(tc::s32(bars + 1)) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
-    // weights [tap][cout][cin] -> [tap][chunk][cout][16 B]
     for (int q = threadIdx.x; q < 27 * COUT * G::CH; q += tc::THREADS) {
-        const int ch = q % G::CH, row = q / G::CH;   // row = tap * COUT + cout
+        const int ch = q % G::CH, row = q / G::CH;
         const int tap = row / COUT, co = row - tap * COUT;
-        const unsigned dst = tc::s32(sw + ((tap * G::CH + ch) * COUT + co) * 16);
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(W + (long long)row * CIN + ch * 8));
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(tc::s32(sw + ((tap * G::CH + ch) * COUT + co) * 16)),
+                     "l"(W + (long long)row * CIN + ch * 8));
     }
-    // halo [hz][hy][chunk][hx][16 B]
-    for (int q = threadIdx.x; q < (RZ + 2) * (RY + 2) * G::CH * tc::HXT; q += tc::THREADS) {
-        const int hx = q % tc::HXT;
-        const int rest = q / tc::HXT;
-        const int ch = rest % G::CH;
-        const int hyz = rest / G::CH;
-        const int hy = hyz % (RY + 2), hz = hyz / (RY + 2);
-        int gx = x0 + hx - 1, gy = y0 + hy - 1, gz = z0 + hz - 1;
-        gx = gx < 0 ? gx + L.nx : (gx >= L.nx ? gx - L.nx : gx);
-        gz = gz < 0 ? gz + L.nz : (gz >= L.nz ? gz - L.nz : gz);
-        bool ok = true;
-        if (pery) gy = gy < 0 ? gy + L.ny : (gy >= L.ny ? gy - L.ny : gy);
-        else ok = gy >= 0 && gy < L.ny;
-        unsigned char* dst = sx + (((hz * (RY + 2) + hy) * G::CH + ch) * tc::HXT + hx) * 16;
-        if (ok)
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(tc::s32(dst)),
-                         "l"(X + ((((long long)gz * L.ny + gy) * L.nx + gx) * CIN + ch * 8)));
-        else
-            *reinterpret_cast<uint4*>(dst) = make_uint4(0u, 0u, 0u, 0u);
-    }
-    asm volatile("cp.async.commit_group;\n" ::);
-    asm volatile("cp.async.wait_all;\n" ::: "memory");
-    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");   // staged data visible to the tensor cores
-    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-    __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-    const unsigned tmem = *taddr_slot;
-
-    if (threadIdx.x == 0) {
-        constexpr unsigned idesc = tc::idesc_bf16(128, COUT);
-        const unsigned xbase = tc::s32(sx), wbase = tc::s32(sw);
-        for (int r = 0; r < G::R; ++r) {
-            const int ty = r % RY, tz = r / RY;
-            for (int tap = 0; tap < 27; ++tap) {
-                const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
-#pragma unroll
-                for (int kc = 0; kc < CIN / 16; ++kc) {
-                    const unsigned a = xbase + ((((tz + dz + 1) * (RY + 2) + (ty + dy + 1)) * G::CH + 2 * kc) *
-                                                    tc::HXT + (dx + 1)) * 16;
-                    const unsigned b = wbase + ((tap * G::CH + 2 * kc) * COUT) * 16;
-                    tc::mma_bf16(tmem + (unsigned)(r * COUT), tc::sdesc(a, tc::HXT * 16, 128),
-                                 tc::sdesc(b, COUT * 16, 128), idesc, (tap | kc) != 0);
-                }
-            }
+    auto slot_of = [&](int z) { return (z - zb + 1) & (G::SLOTS - 1); };
+    auto stage = [&](int z) {   // plane z (wrapped) into its slot
+        int gz = z < 0 ? z + L.nz : (z >= L.nz ? z - L.nz : z);
+        unsigned char* base = ring + slot_of(z) * G::PLANE_BYTES;
+        for (int q = threadIdx.x; q < (RY + 2) * G::CH * tc::HXT; q += tc::THREADS) {
+            const int hx = q % tc::HXT;
+            const int rest = q / tc::HXT;
+            const int ch = rest % G::CH, hy = rest / G::CH;
+            int gx = x0 + hx - 1, gy = y0 + hy - 1;
+            gx = gx < 0 ? gx + L.nx : (gx >= L.nx ? gx - L.nx : gx);
+            bool ok = true;
+            if (pery) gy = gy < 0 ? gy + L.ny : (gy >= L.ny ? gy - L.ny : gy);
+            else ok = gy >= 0 && gy < L.ny;
+            unsigned char* dst = base + ((hy * G::CH + ch) * tc::HXT + hx) * 16;
+            if (ok)
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(tc::s32(dst)),
+                             "l"(X + ((((long long)gz * L.ny + gy) * L.nx + gx) * CIN + ch * 8)));
+            else
+                *reinterpret_cast<uint4*>(dst) = make_uint4(0u, 0u, 0u, 0u);
         }
-        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
-                         tc::s32(bar))
-                     : "memory");
-    }
-    const bool done = tc::bar_wait(tc::s32(bar), 0);
-    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-    if (!done) {
-        if (threadIdx.x == 0) atomicExch(err, 1);
-    } else {
-        const int x = x0 + warp * 32 + lane;   // tensor-memory lane = voxel of the row
-        for (int r = 0; r < G::R; ++r) {
+    };
+    stage(zb - 1);
+    stage(zb);
+    if (nsteps > 0) stage(zb + 1);
+    asm volatile("cp.async.commit_group;\n" ::);
+
+    unsigned tmem = 0;
+    auto epilogue = [&](int q) {   // plane zb+q from accumulator set q & 1
+        const int z = zb + q;
+        const int x = x0 + warp * 32 + lane;
+        for (int r = 0; r < RY; ++r) {
             float v[COUT];
-            tc::tmem_ld<COUT>(tmem + ((unsigned)(warp * 32) << 16) + (unsigned)(r * COUT), v);
-            const int y = y0 + r % RY, z = z0 + r / RY;
-            if (y >= L.ny || z >= L.nz) continue;
+            tc::tmem_ld<COUT>(tmem + ((unsigned)(warp * 32) << 16) + (unsigned)(((q & 1) * RY + r) * COUT), v);
+            const int y = y0 + r;
+            if (y >= L.ny) continue;
             const long long vox = ((long long)z * L.ny + y) * L.nx + x;
             if (EPI == 0) {
                 __align__(16) __nv_bfloat16 o[COUT];
@@ -228,10 +213,74 @@ k_conv3_tc(LVL L, int pery, const __nv_bfloat16* __restrict__ X, const __nv_bflo
                     *reinterpret_cast<float4*>(Yf + vox * COUT + c) = make_float4(v[c], v[c + 1], v[c + 2], v[c + 3]);
             }
         }
+    };
+
+    bool ok = true;
+    for (int q = 0; q < nsteps; ++q) {
+        const int z = zb + q;
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");   // planes z-1 .. z+1 (and the weights) staged
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        tmem = *taddr_slot;
+        if (threadIdx.x == 0) {
+            // Descriptors differ only in their start address (bits 0-13, in 16-byte
+            // units, all addresses below 256 KB): build each once and add offsets
+            // that are compile-time constants but for the three plane slots.
+            constexpr unsigned idesc = tc::idesc_bf16(128, COUT);
+            const unsigned long long b0 = tc::sdesc(tc::s32(sw), COUT * 16, 128);
+            const unsigned long long a0 = tc::sdesc(tc::s32(ring), tc::HXT * 16, 128);
+            const unsigned long long as[3] = {a0 + (unsigned)(slot_of(z - 1) * G::PLANE_BYTES / 16),
+                                              a0 + (unsigned)(slot_of(z) * G::PLANE_BYTES / 16),
+                                              a0 + (unsigned)(slot_of(z + 1) * G::PLANE_BYTES / 16)};
+            const unsigned dset = tmem + (unsigned)((q & 1) * RY * COUT);
+#pragma unroll
+            for (int r = 0; r < RY; ++r)
+#pragma unroll
+                for (int tap = 0; tap < 27; ++tap) {
+                    const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+#pragma unroll
+                    for (int kc = 0; kc < CIN / 16; ++kc) {
+                        const unsigned aoff = ((r + dy + 1) * G::CH + 2 * kc) * tc::HXT + (dx + 1);
+                        const unsigned boff = (tap * G::CH + 2 * kc) * COUT;
+                        tc::mma_bf16(dset + (unsigned)(r * COUT), as[dz + 1] + aoff, b0 + boff, idesc,
+                                     (tap | kc) != 0);
+                    }
+                }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                             tc::s32(bars + (q & 1)))
+                         : "memory");
+        }
+        if (q > 0) {   // plane z-1: its MMAs done, then its epilogue; its slot z-2 is free afterwards
+            const bool done = tc::bar_wait(tc::s32(bars + ((q - 1) & 1)), (unsigned)(((q - 1) >> 1) & 1));
+            if (__syncthreads_or(!done)) { ok = false; break; }
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            epilogue(q - 1);
+        }
+        if (q + 1 < nsteps) stage(z + 2);
+        asm volatile("cp.async.commit_group;\n" ::);
+        asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     }
+    if (ok && nsteps > 0) {
+        const int q = nsteps - 1;
+        const bool done = tc::bar_wait(tc::s32(bars + (q & 1)), (unsigned)((q >> 1) & 1));
+        if (__syncthreads_or(!done)) ok = false;
+        else {
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            epilogue(q);
+        }
+    }
+    if (!ok) {   // a wait gave up: flag it and give the MMAs in flight one more bounded wait
+        if (threadIdx.x == 0) atomicExch(err, 1);
+        tc::bar_wait(tc::s32(bars), 0);
+        tc::bar_wait(tc::s32(bars + 1), 0);
+    }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     __syncthreads();
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"((unsigned)G::COLS)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem ? tmem : *taddr_slot),
+                     "r"((unsigned)G::COLS)
                      : "memory");
 }
