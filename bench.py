@@ -696,6 +696,31 @@ def run_profile_mixed(args, cfg):
     return 0
 
 
+def run_profile_unet(args, cfg):
+    """One forward + backward pass of the learned warm start's network on
+    random inputs of the workload's grid (for an ncu capture of a few
+    convolution launches; no solver steps)."""
+    import torch
+    import mobydiff_b200 as M
+    _, rank, local = _dist()
+    torch.cuda.set_device(local)
+    g = M.make_grid(cfg["nx"], cfg["ny"], cfg["nz"], cfg["lx"], cfg["ly"], cfg["lz"], cfg["re"], cfg["dt"],
+                    (2.0 / cfg["re"], 0.0, 0.0))
+    s = M.Solver(g, M.channel_bc(), local)
+    s.enter_field_data()
+    s.unet_create(channels=32, capacity=0, slope=0.1)
+    n = cfg["nx"] * cfg["ny"] * cfg["nz"]
+    rng = np.random.default_rng(SEED)
+    loss, _, _ = s.unet_loss_grad(rng.standard_normal((4, n)).astype(np.float32),
+                                  rng.standard_normal(n).astype(np.float32))
+    st = s.unet_stats()
+    if rank == 0:
+        print(json.dumps({"profile_run": cfg["workload"] + "; one network forward + backward", "loss": loss,
+                          "tcgen05_convolutions": int(st.tc_convs), "launches": s.launch_count()}), flush=True)
+    s.close()
+    return 0
+
+
 def run_learned_mixed(args, cfg):
     import torch
     import mobydiff_b200 as M
@@ -873,6 +898,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     ap.add_argument("--profile", action="store_true",
                     help="profiling run for ncu: full-size state, fixed 20 red-black iterations per projection")
+    ap.add_argument("--profile-unet", action="store_true",
+                    help="one network forward + backward on the workload's grid (for an ncu capture)")
     ap.add_argument("--profile-mixed", action="store_true",
                     help="profiling run for ncu: the full-size t=0 projection with FP32 sweeps to residual 1e-8")
     ap.add_argument("--quick", action="store_true", help="skip the plain FP64 leg at residual 1e-10")
@@ -887,6 +914,8 @@ def main():
         return run_reference(args, cfg)
     if args.profile_mixed:
         return run_profile_mixed(args, cfg)
+    if args.profile_unet:
+        return run_profile_unet(args, cfg)
     if cfg["method"] == "ensemble":
         return run_ensemble(args, cfg)
     if cfg["method"] == "fft-mixed" and not args.profile:
