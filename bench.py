@@ -53,6 +53,13 @@ CONFIGS = {
                tol=1e-8, method="learned-mixed"),
     "c1-plain": dict(C1_GEOM, workload="wavy-wall IBM channel 256x128x128, FP64 red-black SOR omega=1.7 to residual "
                                        "1e-10", tol=1e-10, method="plain"),
+    "c3": dict(C1_GEOM, workload="learned warm start on the 256x128x128 wavy-wall IBM channel: network trained on "
+                                 "snapshots of runs at Re in 1000..5000, A in 0..0.1 (stratified draws); "
+                                 "held-out runs at Re U(1000,5000), A U(0,0.1); SOR iterations to residual 1e-8 "
+                                 "on held-out runs against zero, previous-step and extrapolated guesses (FP32 sweeps "
+                                 "in FP64 defect correction, omega 1.7)",
+               tol=1e-8, method="learned-eval", check_every=10, train_runs=8, record_steps=8, heldout_runs=4,
+               heldout_steps=10),
     "c4": dict(workload="ensemble of 64 wavy-wall IBM channels, nx,nz in 32..128 and ny in 32..96 (multiples of 16), "
                          "Re U(1000,5000), A U(0,0.1), red-black SOR omega=1.7 to residual 1e-8 from the extrapolated "
                          "increment, FP32 sweeps in FP64 defect correction; one persistent launch per RK3 substage, "
@@ -721,6 +728,102 @@ def run_profile_unet(args, cfg):
     return 0
 
 
+def run_learned_eval(args, cfg):
+    """Config 3: the network trained on snapshots of runs over a range of Re
+    and wall amplitudes, judged by red-black iterations to the tolerance on
+    held-out runs against the guesses without it."""
+    import torch
+    import mobydiff_b200 as M
+    from mobydiff_b200 import learned
+
+    _, rank, local = _dist()
+    torch.cuda.set_device(local)
+    rng = np.random.default_rng(SEED + 3)
+    # training runs: Re and A each stratified over their range (one draw per
+    # stratum, Re strata in a seeded random order), so that a few runs cover
+    # both ranges; held-out runs: independent uniform draws
+    nt = cfg["train_runs"]
+    perm = rng.permutation(nt)
+    train = [(SEED + 100 + q, float(0.1 * (q + rng.uniform()) / nt),
+              float(1000.0 + 4000.0 * (perm[q] + rng.uniform()) / nt)) for q in range(nt)]   # (seed, A, Re)
+    held = [(SEED + 200 + q, float(rng.uniform(0.0, 0.1)), float(rng.uniform(1000.0, 5000.0)))
+            for q in range(cfg["heldout_runs"])]
+    steps = args.c3_steps or cfg["heldout_steps"]
+    cells = cfg["nx"] * cfg["ny"] * cfg["nz"]
+    y0 = (cfg["ly"] - 2.0) / 2.0
+    lam = cfg["lx"] / 2.0
+
+    def solver(re, amp):
+        g = M.make_grid(cfg["nx"], cfg["ny"], cfg["nz"], cfg["lx"], cfg["ly"], cfg["lz"], re, cfg["dt"],
+                        (2.0 / re, 0.0, 0.0))
+        s = M.Solver(g, M.channel_bc(), local)
+        s.enter_field_data()
+        if amp > 0.0:
+            s.enter_ibm_geometry(M.ibm_wavy(amp, lam, y0))
+        s.init_pressure_solver(M.make_solver_opts(M.SOLVER_REDBLACK, sor=cfg["sor"], tol=cfg["tol"],
+                                                  check_every=cfg["check_every"], max_iter=400000,
+                                                  precision=M.PREC_MIXED))
+        return s, g
+
+    t0 = time.time()
+    st_, gt = solver(train[0][2], train[0][1])
+    net = learned.record_and_train(st_, gt, train, warm_steps=3, record_steps=cfg["record_steps"],
+                                   iters=args.train_iters * 2)
+    st_.close()
+    train_wall = time.time() - t0
+
+    modes = [("zero", M.GUESS_ZERO), ("previous", M.GUESS_PREVIOUS), ("extrapolated", M.GUESS_EXTRAPOLATED),
+             ("learned", M.GUESS_LEARNED)]
+    per_run, totals = [], {m: [0, 0.0] for m, _ in modes}
+    for seed, amp, re in held:
+        row = {"seed": seed, "re": re, "amp": amp}
+        final = {}
+        for name, mode in modes:
+            s, g = solver(re, amp)
+            if mode == M.GUESS_LEARNED:
+                learned.load_into(s, net)
+            s.set_pressure_guess(mode, record=True)
+            s.channel_ic(seed, 0.1, 0.01, y0, amp, lam)
+            s.step(3)
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            it = s.step(steps)
+            dt = time.perf_counter() - t1
+            row[name] = {"iters_per_substage": it / (3 * steps), "mcell_steps_s": cells * steps / dt / 1e6}
+            totals[name][0] += it
+            totals[name][1] += dt
+            final[name] = [s.get(n) for n in ("un", "vn", "wn")]
+            s.close()
+        num = sum(float(np.sum((a - b) ** 2)) for a, b in zip(final["learned"], final["zero"]))
+        den = sum(float(np.sum(b ** 2)) for b in final["zero"])
+        row["velocity_rel_l2_learned_vs_zero"] = math.sqrt(num / den)
+        per_run.append(row)
+    nsub = 3 * steps * len(held)
+    summary = {m: {"iters_per_substage": totals[m][0] / nsub,
+                   "mcell_steps_s": cells * steps * len(held) / totals[m][1] / 1e6} for m, _ in modes}
+    if rank == 0:
+        print(json.dumps({
+            "metric": "red-black iterations per substage to residual 1e-8 on held-out runs, learned warm start vs "
+                      "zero / previous / extrapolated guesses, 1 B200",
+            "value": summary["learned"]["iters_per_substage"], "unit": "iterations per substage",
+            "higher_is_better": False, "n_gpus": 1, "steps": steps, "warmup": 3, "dtype": "f64+f32",
+            "data": "synthetic: seeded Poiseuille+noise ICs; training and held-out runs at seeded Re and A",
+            "config": {"workload": cfg["workload"], "grid": [cfg["nx"], cfg["ny"], cfg["nz"]], "tol": cfg["tol"],
+                       "train_runs": [{"seed": a, "amp": b, "re": c} for a, b, c in train],
+                       "record_steps_per_run": cfg["record_steps"], "heldout_steps": steps * len(held)},
+            "by_guess": summary,
+            "reduction_vs_zero": summary["zero"]["iters_per_substage"] / summary["learned"]["iters_per_substage"],
+            "reduction_vs_previous": summary["previous"]["iters_per_substage"] /
+                                     summary["learned"]["iters_per_substage"],
+            "reduction_vs_extrapolated": summary["extrapolated"]["iters_per_substage"] /
+                                         summary["learned"]["iters_per_substage"],
+            "heldout_runs": per_run,
+            "learned": {"snapshots": net.snapshots, "loss_first": net.loss_first, "loss_last": net.loss_last,
+                        "train_ms": net.train_ms, "record_s": net.record_seconds, "setup_wall_s": train_wall},
+        }), flush=True)
+    return 0
+
+
 def run_learned_mixed(args, cfg):
     import torch
     import mobydiff_b200 as M
@@ -905,6 +1008,8 @@ def main():
     ap.add_argument("--quick", action="store_true", help="skip the plain FP64 leg at residual 1e-10")
     ap.add_argument("--sor-variant", type=int, default=0, choices=[0, 1, 2, 3, 4],
                     help="red-black kernel variant (0: autotuned; all give the same bits)")
+    ap.add_argument("--c3-steps", type=int, default=0,
+                    help="config c3: measured steps per held-out run (0: the config's 10)")
     ap.add_argument("--train-iters", type=int, default=1200, help="Adam steps of the learned warm start")
     args = ap.parse_args()
     global SOR_VARIANT
@@ -922,6 +1027,8 @@ def main():
         return run_fft_mixed(args, cfg)
     if cfg["method"] == "learned-mixed" and not args.profile:
         return run_learned_mixed(args, cfg)
+    if cfg["method"] == "learned-eval":
+        return run_learned_eval(args, cfg)
     return run_plain(args, cfg)
 
 

@@ -246,6 +246,12 @@ int mdx_destroy(mdx_ctx_t* ctx);
  * the context with init_bc defaults and updates it here when bc changes. */
 int mdx_set_bc(mdx_ctx_t* ctx, const mdx_bc_t* bc);
 
+/* Re and body force (grid_type re, forcing_x/y/z, src/modules/init.f90:14-19)
+ * of an existing context, for running several flows on one context (the
+ * reference sets them once from input.ini).  IBM coefficients carry 1/Re:
+ * re-enter them after a change. */
+int mdx_set_flow(mdx_ctx_t* ctx, double re, double fx, double fy, double fz);
+
 /* Use an external CUDA stream (cudaStream_t) instead of the context's own;
  * NULL restores the context stream. */
 int mdx_set_stream(mdx_ctx_t* ctx, void* stream);

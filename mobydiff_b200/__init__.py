@@ -164,6 +164,7 @@ def lib():
         "mdx_update_device": (i, [vp, vp, vp, vp, vp]),
         "mdx_copy_field": (i, [vp, i, vp, i]),
         "mdx_enter_ibm_data": (i, [vp, vp, vp, vp]),
+        "mdx_set_flow": (i, [vp, d, d, d, d]),
         "mdx_enter_ibm_geometry": (i, [vp, P(IbmGeomT)]),
         "fdm_h5_write_field": (i, [C.c_char_p, i, i, i] + [d] * 9 + [vp] * 4),
         "fdm_h5_read_field": (i, [C.c_char_p, i, i, i] + [vp] * 4),
@@ -429,6 +430,14 @@ class Solver:
     def read_field_h5(self, path: str) -> None:
         """read_field (src/modules/io.f90:139-166) into the device mirrors."""
         self._c(lib().mdx_read_field_h5(self.h, os.fsencode(path)))
+
+    def set_flow(self, re: float, forcing=(None, 0.0, 0.0)):
+        """Re and body force of this context (default forcing_x = 2/Re, the
+        force that keeps the Poiseuille profile steady)."""
+        fx = 2.0 / re if forcing[0] is None else forcing[0]
+        self._c(lib().mdx_set_flow(self.h, float(re), float(fx), float(forcing[1]), float(forcing[2])))
+        self.grid.re = float(re)
+        self.grid.forcing_x, self.grid.forcing_y, self.grid.forcing_z = fx, float(forcing[1]), float(forcing[2])
 
     def enter_ibm_geometry(self, geom: IbmGeomT):
         """set_ibm_coeff for u, v, w generated on the device, then enter_ibm_data."""

@@ -268,6 +268,24 @@ int mdx_destroy(mdx_ctx_t* ctx) {
     return MDX_OK;
 }
 
+// Re and the body force of an existing context (the reference reads them
+// once from input.ini; a training pipeline recording several flows on one
+// context changes them between runs).  IBM coefficients, which carry 1/Re,
+// are the caller's to re-enter.
+int mdx_set_flow(mdx_ctx_t* ctx, double re, double fx, double fy, double fz) {
+    if (!ctx) return mdx_fail(nullptr, MDX_ERR_ARG, "null context");
+    if (!(re > 0.0) || !std::isfinite(re) || !std::isfinite(fx) || !std::isfinite(fy) || !std::isfinite(fz))
+        return mdx_fail(ctx, MDX_ERR_ARG, "mdx_set_flow: Re must be positive and the forces finite");
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    release_graph(ctx);
+    ctx->g.re = re;
+    ctx->g.forcing_x = fx;
+    ctx->g.forcing_y = fy;
+    ctx->g.forcing_z = fz;
+    return MDX_OK;
+}
+
 int mdx_set_bc(mdx_ctx_t* ctx, const mdx_bc_t* bc) {
     if (!ctx || !bc) return mdx_fail(ctx, MDX_ERR_ARG, "mdx_set_bc: null argument");
     if (ctx->solver && ctx->opts.solver == MDX_SOLVER_REDBLACK && bc->is_periodic[1] && ctx->d.ny % 2 != 0)

@@ -54,12 +54,15 @@ def wavy_solver(nx, ny, nz, re, amp, tol, check_every=50, precision=PREC_FP64, d
 def record_and_train(s: Solver, g, runs, warm_steps: int = 3, record_steps: int = 8, iters: int = 600,
                      lr: float = 3e-4, channels: int = 32, extra_bottleneck: int = 0, slope: float = 0.1,
                      seed: int = 20261203) -> TrainedNet:
-    """Record snapshots on `s` for each (seed, amplitude) in `runs` -- a fresh
-    channel IC each, `warm_steps` steps to build the increment history, then
-    `record_steps` recorded steps (three snapshots each) -- and train.
+    """Record snapshots on `s` for each (seed, amplitude) or (seed, amplitude,
+    Re) in `runs` -- a fresh channel IC each, `warm_steps` steps to build the
+    increment history, then `record_steps` recorded steps (three snapshots
+    each) -- and train.
 
-    The IBM coefficients of `s` are replaced per run; Re and the grid are the
-    solver's.  The first half of the Adam steps runs at lr, the second at lr/3.
+    The IBM coefficients of `s` are replaced per run (generated on the
+    device), and Re with its body force 2/Re when a run gives one; the grid is
+    the solver's.  The first half of the Adam steps runs at lr, the second at
+    lr/3.
     """
     ly = g.ly
     y0 = (ly - 2.0) / 2.0
@@ -68,9 +71,12 @@ def record_and_train(s: Solver, g, runs, warm_steps: int = 3, record_steps: int 
     s.unet_create(channels=channels, extra_bottleneck=extra_bottleneck, capacity=cap, slope=slope, seed=seed)
     s.set_pressure_guess(GUESS_EXTRAPOLATED, record=True)
     t0 = time.time()
-    for run_seed, amp in runs:
+    for run in runs:
+        run_seed, amp = run[0], run[1]
+        if len(run) > 2:
+            s.set_flow(run[2])
         if amp > 0.0:
-            s.enter_ibm_data(*set_ibm_coeff(g, ibm_wavy(amp, lam, y0)))
+            s.enter_ibm_geometry(ibm_wavy(amp, lam, y0))
         else:
             s.exit_ibm_data()
         s.unet_record(False)
