@@ -74,3 +74,26 @@ def test_restart_through_hdf5_field_file_is_bitwise(tmp_path, solver, amp):
         b.step(2)
         for x, n in zip(full, ("un", "vn", "wn", "pn")):
             assert np.array_equal(x, b.get(n)), n
+
+
+def test_set_flow_steps_like_a_context_created_at_that_re():
+    """Re and body force changed on an existing context (with its IBM
+    coefficients re-entered) give the steps of a context created with them."""
+    g_a, opts, y0, _ = _case(M.SOLVER_REDBLACK, 0.05)
+    g_b = M.make_grid(g_a.nx, g_a.ny, g_a.nz, g_a.lx, g_a.ly, g_a.lz, 3500.0, g_a.dt, (2.0 / 3500.0, 0.0, 0.0))
+    geom = M.ibm_wavy(0.05, math.pi, y0)
+    a = M.Solver(g_a, M.channel_bc(), 0)
+    b = M.Solver(g_b, M.channel_bc(), 0)
+    with a, b:
+        for s in (a, b):
+            s.enter_field_data()
+        a.set_flow(3500.0)
+        with pytest.raises(M.MdxError):
+            a.set_flow(-1.0)
+        for s in (a, b):
+            s.enter_ibm_geometry(geom)
+            s.init_pressure_solver(opts)
+            s.channel_ic(20261203, 0.1, 0.01, y0, 0.05, math.pi)
+            s.step(2)
+        for n in ("un", "vn", "wn", "pn"):
+            assert np.array_equal(a.get(n), b.get(n)), n
