@@ -161,6 +161,7 @@ def _dist():
 
 
 SOR_VARIANT = 0   # --sor-variant: red-black kernel variant (0: the autotuner's choice)
+FFT_KERNEL = 0    # --fft-kernel: 0 warp-shuffle transforms where the lengths allow, 1 Stockham
 SOR_NAMES = {1: "one launch per colour sweep", 2: "fused red+black pass 32x8", 3: "fused red+black pass 32x16",
              4: "one launch per colour sweep on colour-split copies"}
 
@@ -191,7 +192,7 @@ def _setup(cfg, M, device, profile=False, tol=None, precision=None, seed=None):
                                   sor_variant=SOR_VARIANT)
     else:
         opts = M.make_solver_opts(M.SOLVER_FFT, tol=cfg.get("tol", 0.0) if precision == M.PREC_MIXED else 0.0,
-                                  precision=M.PREC_FP64 if precision is None else precision)
+                                  precision=M.PREC_FP64 if precision is None else precision, fft_kernel=FFT_KERNEL)
     s.init_pressure_solver(opts)
     s.channel_ic(SEED if seed is None else seed, 0.1, 0.01, y0, cfg["amp"], lam)
     return s, g
@@ -383,6 +384,30 @@ def _roofline(tim, kname, alg_per_cell, cells, ms, traffic_key=None):
             "avg_launch_ms": avg_s * 1e3, "launches": kn, "share_of_step_time": kms / ms if ms > 0 else None}
 
 
+def _fft_passes(cfg, tim, cells, ms):
+    """Achieved HBM rate of each pass class of the FP64 FFT projection, from
+    its algorithmic bytes per cell: fft_fwd = divergence reads (3 doubles) +
+    spectrum write, z transform read+write; thomas = spectrum read+write + the
+    two tables; fft_inv = z transform read+write, spectrum read + phi write;
+    correct = phi, u*, v*, w*, p read, u, v, w, p write."""
+    nx, ny, nz = cfg["nx"], cfg["ny"], cfg["nz"]
+    spec = 16.0 * (nx // 2 + 1) / nx                      # bytes of spectrum per cell
+    tables = 16.0 * (nx // 2 + 1) * (nz // 2 + 1) * ny / cells
+    per_cell = {"fft_fwd": 24.0 + 3 * spec, "thomas": 2 * spec + tables, "fft_inv": 3 * spec + 8.0,
+                "correct": 72.0 + (24.0 if cfg["ibm"] != "none" else 0.0)}
+    peak, peak_kind = _peaks()
+    out = {"peak_gbs": peak, "peak_kind": peak_kind}
+    nproj = tim["correct"][1]          # one correction launch per projection
+    for k, b in per_cell.items():
+        kms, kn = tim[k]
+        if not kn or not nproj:
+            continue
+        gbs = b * cells * nproj / (kms / 1e3) / 1e9
+        out[k] = {"alg_bytes_per_cell": round(b, 3), "launches": kn, "projections": nproj, "ms": kms, "gbs": gbs,
+                  "frac": gbs / peak, "share_of_step_time": kms / ms if ms > 0 else None}
+    return out
+
+
 def _init_dist(device):
     import torch
     ws, rank, local = _dist()
@@ -450,6 +475,7 @@ def run_plain(args, cfg):
                              traffic_key=_sor64_traffic_key(s.last_solve_stats().variant))
     else:
         roofline = _roofline(tim, "momentum", 112.0, cells, ms)   # 14 doubles per cell
+    fft_passes = _fft_passes(cfg, tim, cells, ms) if cfg["solver"] != "redblack" else None
     iters_per_substage = iters / (3 * args.steps) if cfg["solver"] == "redblack" else 0
     sor_kernel = None
     if cfg["solver"] == "redblack":
@@ -467,7 +493,7 @@ def run_plain(args, cfg):
                            "parallelism": f"replicas x{ws}",
                            "l2": "inputs larger than L2 (state + IBM coefficients > 126 MB)"},
                 "poisson_iters_per_substage": iters_per_substage, "sor_kernel": sor_kernel,
-                "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "e2e": e2e_line,
+                "roofline": roofline, "fft_passes": fft_passes, "cpu_baseline": cpu, "clocks": clk, "e2e": e2e_line,
                 "gpu_launches": launches}
         print(json.dumps(line), flush=True)
     s.close()
@@ -1008,12 +1034,15 @@ def main():
     ap.add_argument("--quick", action="store_true", help="skip the plain FP64 leg at residual 1e-10")
     ap.add_argument("--sor-variant", type=int, default=0, choices=[0, 1, 2, 3, 4],
                     help="red-black kernel variant (0: autotuned; all give the same bits)")
+    ap.add_argument("--fft-kernel", type=int, default=0, choices=[0, 1],
+                    help="FFT path transforms: 0 warp-shuffle where nx/2 and nz allow, 1 shared-memory Stockham")
     ap.add_argument("--c3-steps", type=int, default=0,
                     help="config c3: measured steps per held-out run (0: the config's 10)")
     ap.add_argument("--train-iters", type=int, default=1200, help="Adam steps of the learned warm start")
     args = ap.parse_args()
-    global SOR_VARIANT
+    global SOR_VARIANT, FFT_KERNEL
     SOR_VARIANT = args.sor_variant
+    FFT_KERNEL = args.fft_kernel
     cfg = CONFIGS[args.config]
     if args.impl == "reference":
         return run_reference(args, cfg)

@@ -103,7 +103,10 @@ typedef struct {
                           puts the target more than twice as far; 1: every check_every
                           iterations (the stop is then the first multiple of check_every that
                           meets the target) */
-    int reserved_i[4];
+    int fft_kernel;    /* FFT path: 0 (default) warp-shuffle transforms where nx/2 and nz are
+                          32, 64, 128, 256 or 512 (shared-memory Stockham otherwise); 1 always
+                          the shared-memory Stockham transforms */
+    int reserved_i[3];
     double atol;       /* red-black: absolute floor of ||div u||2, also accepted as converged.
                           < 0 (default): the FP64 round-off level of the divergence,
                           eps*sqrt(nx*ny*nz)*max|u*|*(1/dx+1/dy+1/dz); 0: none */

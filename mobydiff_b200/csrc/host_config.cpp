@@ -190,6 +190,10 @@ struct Reader {
             if (v == "adaptive" || v == "0") o->check_mode = 0;
             else if (v == "fixed" || v == "every" || v == "1") o->check_mode = 1;
             else warn("b200 residual_checks must be adaptive or fixed", line);
+        } else if (key == "fft_kernel") {
+            if (v == "warp" || v == "0") o->fft_kernel = 0;
+            else if (v == "stockham" || v == "1") o->fft_kernel = 1;
+            else warn("b200 fft_kernel must be warp or stockham", line);
         } else if (key == "max_iter") {
             rd_int(value, &o->max_iter, line);
         } else if (key == "check_every") {

@@ -14,12 +14,15 @@
 //   k_ifftx      spec -> phi             inverse real FFT of one row, *1/(nx nz)
 //   k_correct    us,vs,ws,phi,pn -> un,vn,wn,pn
 //
-// The FFTs are shared-memory Stockham transforms (the formulation of
-// Govindaraju et al., "High performance discrete Fourier transforms on
-// graphics processors", SC 2008) with radices 4, 2, 3, 5, 7; the real
-// transform of length nx is a complex transform of length nx/2 on packed
-// even/odd samples plus the standard split step.  Twiddles are tables built
-// on the host with long-double cosl/sinl.
+// Where nx/2 and nz are 32 P (P = 1, 2, 4, 8, 16) each line is one warp's
+// four-step transform: a P-point DFT in registers and a 32-point DFT across
+// the lanes by shuffles (k_div_fftx_w, k_fftz_w, k_ifftx_w).  Other lengths
+// use shared-memory Stockham transforms (the formulation of Govindaraju et
+// al., "High performance discrete Fourier transforms on graphics
+// processors", SC 2008) with radices 4, 2, 3, 5, 7.  The real transform of
+// length nx is a complex transform of length nx/2 on packed even/odd samples
+// plus the standard split step.  Twiddles are tables built on the host with
+// long-double cosl/sinl.
 //
 // Parity: the divergence, Thomas and correction arithmetic follow the
 // reference order with -fmad=false; the FFT differs from FFTW in operation
@@ -28,6 +31,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 
 // ---------------------------------------------------------------------------
 // Plans and twiddles (host)
@@ -81,6 +85,13 @@ template <typename C2> __device__ __forceinline__ C2 cconj(C2 a) { return cx<C2>
 // a * (-i) and a * (+i)
 template <typename C2> __device__ __forceinline__ C2 cmul_mi(C2 a) { return cx<C2>::mk(a.y, -a.x); }
 template <typename C2> __device__ __forceinline__ C2 cmul_pi(C2 a) { return cx<C2>::mk(-a.y, a.x); }
+// complex product with fused multiply-adds (the transforms only; the
+// divergence, Thomas and correction arithmetic keep separate rounding)
+__device__ __forceinline__ double fma_r(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float fma_r(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+template <typename C2> __device__ __forceinline__ C2 cmul_f(C2 a, C2 b) {
+    return cx<C2>::mk(fma_r(a.x, b.x, -(a.y * b.y)), fma_r(a.x, b.y, a.y * b.x));
+}
 
 // Twiddle exp(-+2 pi i t / n) from the forward table (conjugated for INV).
 template <bool INV, typename C2>
@@ -367,6 +378,240 @@ k_ifftx(mdx_dims d, int R, typename cx<C2>::R scale, const C2* __restrict__ spec
 }
 
 // ---------------------------------------------------------------------------
+// Warp-shuffle transforms of length N = 32 P, P = 1, 2, 4, 8, 16: one warp
+// per line, no block barrier inside a transform.  The length splits as
+// N = P x 32: lane l holds x[l + 32 m] (m < P), takes the P-point DFT over m
+// in registers, multiplies by W_N^(l p), and the 32-point DFT across the
+// lanes runs for each p as five radix-2 decimation-in-frequency stages whose
+// partner values come from __shfl_xor_sync:
+//   X[p + P q] = sum_l W_32^(l q) W_N^(l p) sum_m x[l + 32 m] W_P^(m p).
+// Lane l ends holding X[p + P brev5(l)] in v[p].  Roots come from the same
+// long-double twiddle tables as the Stockham transforms: W_N^t = tw[t tws].
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr int wlog2(int p) { return p <= 1 ? 0 : 1 + wlog2(p / 2); }
+// reversal of the low `bits` (<= 4) bits of x
+__host__ __device__ __forceinline__ constexpr int wbrev(int x, int bits) {
+    return (((x & 1) << 3) | ((x & 2) << 1) | ((x & 4) >> 1) | ((x & 8) >> 3)) >> (4 - bits);
+}
+
+template <bool INV, int P, typename C2>
+__device__ __forceinline__ void warp_fft(C2 (&v)[P], int lane, const C2* __restrict__ tw, int tws) {
+    constexpr int N = 32 * P;
+    constexpr int LP = wlog2(P);
+    // P-point DIF in registers; v[i] then holds Y[brev(i)]
+#pragma unroll
+    for (int s = 0; s < LP; ++s) {
+        const int h = P >> (s + 1);
+#pragma unroll
+        for (int b = 0; b < P; b += 2 * h) {
+#pragma unroll
+            for (int r = 0; r < h; ++r) {
+                const C2 a0 = v[b + r], a1 = v[b + r + h];
+                const C2 dd = csub(a0, a1);
+                v[b + r] = cadd(a0, a1);
+                if (r == 0) v[b + r + h] = dd;
+                else if (2 * r == h) v[b + r + h] = INV ? cmul_pi(dd) : cmul_mi(dd);   // W_4^1 = -i
+                else v[b + r + h] = cmul_f(dd, twid<INV>(tw, r * (N / (2 * h)) * tws));
+            }
+        }
+    }
+    C2 y[P];
+#pragma unroll
+    for (int i = 0; i < P; ++i) y[wbrev(i, LP)] = v[i];
+#pragma unroll
+    for (int p = 1; p < P; ++p) y[p] = cmul_f(y[p], twid<INV>(tw, lane * p * tws));
+    // 32-point DIF across the lanes; the roots of the last two stages are
+    // 1 and W_4 = -i, applied without a multiply
+#pragma unroll
+    for (int s = 0; s < 5; ++s) {
+        const int h = 16 >> s;
+        const bool up = (lane & h) != 0;
+        C2 w = cx<C2>::mk(1, 0);
+        if (h > 2) w = twid<INV>(tw, (lane & (h - 1)) * (N / (2 * h)) * tws);   // W_2h^(l mod h)
+        const bool rot = (h == 2) && (lane & 1);
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+            C2 o;
+            o.x = __shfl_xor_sync(0xffffffffu, y[p].x, h);
+            o.y = __shfl_xor_sync(0xffffffffu, y[p].y, h);
+            if (!up) {
+                y[p] = cadd(y[p], o);
+            } else {
+                const C2 dd = csub(o, y[p]);
+                if (h > 2) y[p] = cmul_f(dd, w);
+                else if (rot) y[p] = INV ? cmul_pi(dd) : cmul_mi(dd);
+                else y[p] = dd;
+            }
+        }
+    }
+#pragma unroll
+    for (int p = 0; p < P; ++p) v[p] = y[p];
+}
+
+// Shared-memory swizzle of element k of a line: the natural-order reads
+// (k = l + 32 m) and the bit-reversed writes (k = p + P brev5(l)) of a warp
+// both spread over all bank groups of G = 128 / sizeof(C2) elements.
+template <int P, typename C2> __device__ __forceinline__ int wsw(int k) {
+    constexpr int G = 128 / (int)sizeof(C2);
+    return P == 1 ? 0 : (k / P) & (G - 1);
+}
+template <int P, typename C2> __device__ __forceinline__ int wline(int k) { return k ^ wsw<P, C2>(k); }
+// z tiles: G columns per z row; column c of row kz at kz*G + (c ^ wcol(kz))
+template <int P, typename C2> __device__ __forceinline__ int wcol(int kz) {
+    constexpr int G = 128 / (int)sizeof(C2);
+    return (kz ^ wsw<P, C2>(kz)) & (G - 1);
+}
+__device__ __forceinline__ int brev5(int l) { return (int)(__brev((unsigned)l) >> 27); }
+// one complex element global -> shared, asynchronous (cp.async; 16 bytes
+// bypass L1, 8 bytes through it)
+template <typename C2> __device__ __forceinline__ void cp_async_elem(C2* dst, const C2* src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    if (sizeof(C2) == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+
+// build_fft_rhs + forward real FFT along x, one warp per (k, j) row; M = nx/2 = 32 P.
+template <int P, typename C2>
+__global__ void __launch_bounds__(256)
+k_div_fftx_w(mdx_dims d, double dx, double dy, double dz, double dt_gamma, const double* __restrict__ us,
+             const double* __restrict__ vs, const double* __restrict__ ws, C2* __restrict__ spec,
+             const C2* __restrict__ twx) {
+    typedef typename cx<C2>::R RT;
+    constexpr int M = 32 * P;
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    C2* buf = reinterpret_cast<C2*>(sm_raw) + warp * M;
+    const int row = blockIdx.x * 8 + warp;
+    if (row >= d.nz * d.ny) return;
+    const int k = row % d.nz + 1, j = row / d.nz + 1;
+    const long long plane = (long long)d.nxp * d.nyp;
+    C2 v[P];
+#pragma unroll
+    for (int m = 0; m < P; ++m) {
+        const int n = lane + 32 * m;
+        double x[2];
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            const long long c = pidx(d, 2 * n + 1 + e, j, k);
+            x[e] = ((__ldg(us + c + 1) - __ldg(us + c)) / dx + (__ldg(vs + c + d.nxp) - __ldg(vs + c)) / dy +
+                    (__ldg(ws + c + plane) - __ldg(ws + c)) / dz) / dt_gamma;
+        }
+        v[m] = cx<C2>::mk((RT)x[0], (RT)x[1]);
+    }
+    warp_fft<false, P>(v, lane, twx, 2);
+    const int q = brev5(lane);
+#pragma unroll
+    for (int p = 0; p < P; ++p) buf[wline<P, C2>(p + P * q)] = v[p];
+    __syncwarp();
+    // split step: X_k = E_k + W^k O_k, E = (Z_k + conj Z_{M-k})/2, O = -i/2 (Z_k - conj Z_{M-k})
+    C2* X = spec + (long long)row * d.nxh;
+    const RT h = (RT)0.5;
+#pragma unroll
+    for (int m = 0; m <= P; ++m) {
+        const int kx = lane + 32 * m;
+        if (m == P && lane != 0) break;
+        const C2 zk = buf[wline<P, C2>(kx & (M - 1))];
+        const C2 zc = cconj(buf[wline<P, C2>((M - kx) & (M - 1))]);
+        const C2 e = cx<C2>::mk(h * (zk.x + zc.x), h * (zk.y + zc.y));
+        const C2 o = cmul_mi(cx<C2>::mk(h * (zk.x - zc.x), h * (zk.y - zc.y)));
+        X[kx] = cadd(e, cmul_f(__ldg(twx + kx), o));
+    }
+}
+
+// Complex FFT along z of spec(kx, :, j), nz = 32 P: a block stages TX = G
+// consecutive kx columns of one j (one 128-byte row segment per kz: 8 FP64
+// or 16 FP32 complex values) through shared memory; one warp per column.
+template <typename C2> __host__ __device__ constexpr int ztile_w() { return 128 / (int)sizeof(C2); }
+template <bool INV, int P, typename C2>
+__global__ void __launch_bounds__(32 * ztile_w<C2>(), P >= 16 ? 1 : (sizeof(C2) == 16 ? 3 : 2))
+k_fftz_w(mdx_dims d, C2* __restrict__ spec, const C2* __restrict__ twz) {
+    constexpr int NZ = 32 * P, TX = ztile_w<C2>();
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    C2* S = reinterpret_cast<C2*>(sm_raw);
+    const int nxh = d.nxh;
+    const int ntiles = (nxh + TX - 1) / TX;
+    const int j = blockIdx.x / ntiles;
+    const int kx0 = (blockIdx.x - j * ntiles) * TX;
+    C2* base = spec + (long long)j * NZ * nxh + kx0;
+    const int ncol = min(TX, nxh - kx0);
+    // the whole tile in flight at once: asynchronous copies into the
+    // swizzled layout (columns >= ncol are neither read nor transformed)
+#pragma unroll
+    for (int e = 0; e < P; ++e) {
+        const int t = threadIdx.x + e * 32 * TX;
+        const int c = t % TX, kz = t / TX;
+        if (c < ncol) cp_async_elem(&S[kz * TX + (c ^ wcol<P, C2>(kz))], base + (long long)kz * nxh + c);
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    __syncthreads();
+    const int lane = threadIdx.x & 31, c = threadIdx.x >> 5;
+    if (c < ncol) {
+        C2 v[P];
+#pragma unroll
+        for (int m = 0; m < P; ++m) {
+            const int kz = lane + 32 * m;
+            v[m] = S[kz * TX + (c ^ wcol<P, C2>(kz))];
+        }
+        warp_fft<INV, P>(v, lane, twz, 1);
+        __syncwarp();
+        const int q = brev5(lane);
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+            const int kz = p + P * q;
+            S[kz * TX + (c ^ wcol<P, C2>(kz))] = v[p];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int e = 0; e < P; ++e) {
+        const int t = threadIdx.x + e * 32 * TX;
+        const int c = t % TX, kz = t / TX;
+        if (c < ncol) base[(long long)kz * nxh + c] = S[kz * TX + (c ^ wcol<P, C2>(kz))];
+    }
+}
+
+// Inverse real FFT along x (c2r contract) scaled by 1/(nx nz), one warp per row.
+template <int P, typename C2>
+__global__ void __launch_bounds__(256)
+k_ifftx_w(mdx_dims d, typename cx<C2>::R scale, const C2* __restrict__ spec, typename cx<C2>::R* __restrict__ phi,
+          const C2* __restrict__ twx) {
+    constexpr int M = 32 * P;
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    C2* buf = reinterpret_cast<C2*>(sm_raw) + warp * M;
+    const int row = blockIdx.x * 8 + warp;
+    if (row >= d.nz * d.ny) return;
+    const C2* X = spec + (long long)row * d.nxh;
+    // Z'_k = (X_k + conj X_{M-k}) + i W^{-k} (X_k - conj X_{M-k}),  k < M
+    C2 v[P];
+#pragma unroll
+    for (int m = 0; m < P; ++m) {
+        const int kk = lane + 32 * m;
+        C2 xk = X[kk], xm = X[M - kk];
+        if (kk == 0) { xk.y = 0; xm.y = 0; }   // kx = 0 and kx = M bins are real
+        const C2 xc = cconj(xm);
+        const C2 e = cadd(xk, xc);
+        const C2 o = cmul_f(csub(xk, xc), cconj(__ldg(twx + kk)));
+        v[m] = cadd(e, cmul_pi(o));
+    }
+    warp_fft<true, P>(v, lane, twx, 2);
+    const int q = brev5(lane);
+#pragma unroll
+    for (int p = 0; p < P; ++p) buf[wline<P, C2>(p + P * q)] = v[p];
+    __syncwarp();
+    C2* out = reinterpret_cast<C2*>(phi + (long long)row * d.nx);
+#pragma unroll
+    for (int m = 0; m < P; ++m) {
+        const int n = lane + 32 * m;
+        const C2 z = buf[wline<P, C2>(n)];
+        out[n] = cx<C2>::mk(z.x * scale, z.y * scale);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // apply_fft_pressure_correction, pressure_solver.f90:150-169.
 // ---------------------------------------------------------------------------
 template <bool IBM>
@@ -412,6 +657,108 @@ static int ztile(int nz) {
     if (tx > 32) tx = 32;
     if (tx < 1) tx = 1;
     return tx;
+}
+
+// Warp-shuffle transform lengths: 32 P with P = 1, 2, 4, 8, 16 (0: none).
+static int warp_p(int n) {
+    if (n % 32 != 0) return 0;
+    const int p = n / 32;
+    return (p == 1 || p == 2 || p == 4 || p == 8 || p == 16) ? p : 0;
+}
+template <typename F> static int with_p(int p, F&& f) {
+    switch (p) {
+        case 1: return f(std::integral_constant<int, 1>());
+        case 2: return f(std::integral_constant<int, 2>());
+        case 4: return f(std::integral_constant<int, 4>());
+        case 8: return f(std::integral_constant<int, 8>());
+        case 16: return f(std::integral_constant<int, 16>());
+    }
+    return MDX_ERR_ARG;
+}
+static int fft_px(const mdx_ctx_t* ctx) { return ctx->opts.fft_kernel == 0 ? warp_p(ctx->d.nx / 2) : 0; }
+static int fft_pz(const mdx_ctx_t* ctx) { return ctx->opts.fft_kernel == 0 ? warp_p(ctx->d.nz) : 0; }
+
+template <typename C2> static int fft_warp_attrs(mdx_ctx_t* ctx) {
+    const int px = warp_p(ctx->d.nx / 2), pz = warp_p(ctx->d.nz);
+    if (px)
+        MDX_TRY(with_p(px, [&](auto pc) -> int {
+            constexpr int P = decltype(pc)::value;
+            const int sm = 8 * 32 * P * (int)sizeof(C2);
+            MDX_CUDA(ctx, cudaFuncSetAttribute(k_div_fftx_w<P, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+            MDX_CUDA(ctx, cudaFuncSetAttribute(k_ifftx_w<P, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+            return MDX_OK;
+        }));
+    if (pz)
+        MDX_TRY(with_p(pz, [&](auto pc) -> int {
+            constexpr int P = decltype(pc)::value;
+            const int sm = 32 * P * 128;
+            MDX_CUDA(ctx, cudaFuncSetAttribute(k_fftz_w<false, P, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+            MDX_CUDA(ctx, cudaFuncSetAttribute(k_fftz_w<true, P, C2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+            return MDX_OK;
+        }));
+    return MDX_OK;
+}
+
+// The three transform passes of a projection, warp-shuffle where the length
+// allows and opts.fft_kernel is 0, shared-memory Stockham otherwise.
+template <typename C2>
+static int launch_div_fftx(mdx_ctx_t* ctx, const char* what, double dg, C2* spec, const C2* twx) {
+    const mdx_dims& d = ctx->d;
+    const mdx_grid_t& g = ctx->g;
+    double** f = ctx->f;
+    const int nrows = d.nz * d.ny;
+    if (const int px = fft_px(ctx))
+        return with_p(px, [&](auto pc) -> int {
+            constexpr int P = decltype(pc)::value;
+            auto kern = k_div_fftx_w<P, C2>;
+            MDX_LAUNCH(ctx, MDX_T_FFT_FWD, what, kern, (nrows + 7) / 8, 256, 8 * 32 * P * sizeof(C2), d, g.dx, g.dy,
+                       g.dz, dg, f[MDX_US], f[MDX_VS], f[MDX_WS], spec, twx);
+            return MDX_OK;
+        });
+    const int M = d.nx / 2, R = rows_per_block(M);
+    auto kern = k_div_fftx<C2>;
+    MDX_LAUNCH(ctx, MDX_T_FFT_FWD, what, kern, (nrows + R - 1) / R, 256, sizeof(C2) * 2 * R * M, d, R, g.dx, g.dy,
+               g.dz, dg, f[MDX_US], f[MDX_VS], f[MDX_WS], spec, ctx->plan_xh, twx);
+    return MDX_OK;
+}
+
+template <bool INV, typename C2>
+static int launch_fftz(mdx_ctx_t* ctx, const char* what, C2* spec, const C2* twz) {
+    const mdx_dims& d = ctx->d;
+    const int cls = INV ? MDX_T_FFT_INV : MDX_T_FFT_FWD;
+    if (const int pz = fft_pz(ctx))
+        return with_p(pz, [&](auto pc) -> int {
+            constexpr int P = decltype(pc)::value;
+            auto kern = k_fftz_w<INV, P, C2>;
+            constexpr int TX = ztile_w<C2>();
+            MDX_LAUNCH(ctx, cls, what, kern, ((d.nxh + TX - 1) / TX) * d.ny, 32 * TX, 32 * P * 128, d, spec, twz);
+            return MDX_OK;
+        });
+    const int TX = ztile(d.nz);
+    auto kern = k_fftz<INV, C2>;
+    MDX_LAUNCH(ctx, cls, what, kern, ((d.nxh + TX - 1) / TX) * d.ny, 256, sizeof(C2) * 2 * TX * (d.nz + 1), d, TX,
+               spec, ctx->plan_z, twz);
+    return MDX_OK;
+}
+
+template <typename C2>
+static int launch_ifftx(mdx_ctx_t* ctx, const char* what, typename cx<C2>::R scale, const C2* spec,
+                        typename cx<C2>::R* phi, const C2* twx) {
+    const mdx_dims& d = ctx->d;
+    const int nrows = d.nz * d.ny;
+    if (const int px = fft_px(ctx))
+        return with_p(px, [&](auto pc) -> int {
+            constexpr int P = decltype(pc)::value;
+            auto kern = k_ifftx_w<P, C2>;
+            MDX_LAUNCH(ctx, MDX_T_FFT_INV, what, kern, (nrows + 7) / 8, 256, 8 * 32 * P * sizeof(C2), d, scale, spec,
+                       phi, twx);
+            return MDX_OK;
+        });
+    const int M = d.nx / 2, R = rows_per_block(M);
+    auto kern = k_ifftx<C2>;
+    MDX_LAUNCH(ctx, MDX_T_FFT_INV, what, kern, (nrows + R - 1) / R, 256, sizeof(C2) * 2 * R * M, d, R, scale, spec,
+               phi, ctx->plan_xh, twx);
+    return MDX_OK;
 }
 
 int mdx_fft_init(mdx_ctx_t* ctx) {
@@ -477,6 +824,7 @@ int mdx_fft_init(mdx_ctx_t* ctx) {
     MDX_CUDA(ctx, cudaFuncSetAttribute(k_ifftx<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx));
     MDX_CUDA(ctx, cudaFuncSetAttribute(k_fftz<false, double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz));
     MDX_CUDA(ctx, cudaFuncSetAttribute(k_fftz<true, double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz));
+    MDX_TRY(fft_warp_attrs<double2>(ctx));
     return MDX_OK;
 }
 
@@ -502,27 +850,15 @@ int mdx_k_projection_fft(mdx_ctx_t* ctx, double dg) {
     const mdx_dims& d = ctx->d;
     const mdx_grid_t& g = ctx->g;
     double** f = ctx->f;
-    const int M = d.nx / 2;
-    const int R = rows_per_block(M);
-    const int nrows = d.nz * d.ny;
-    const size_t smx = sizeof(double2) * 2 * R * M;
-    const int xblocks = (nrows + R - 1) / R;
-    MDX_LAUNCH(ctx, MDX_T_FFT_FWD, "div+fft x", k_div_fftx<double2>, xblocks, 256, smx, d, R, g.dx, g.dy, g.dz, dg,
-               f[MDX_US], f[MDX_VS], f[MDX_WS], ctx->spec, ctx->plan_xh, ctx->tw_x);
-    const int TX = ztile(d.nz);
-    const size_t smz = sizeof(double2) * 2 * TX * (d.nz + 1);
-    const int zblocks = ((d.nxh + TX - 1) / TX) * d.ny;
-    auto kz_f = k_fftz<false, double2>;
-    auto kz_i = k_fftz<true, double2>;
     auto kth = k_thomas<double2, false>;
-    MDX_LAUNCH(ctx, MDX_T_FFT_FWD, "fft z", kz_f, zblocks, 256, smz, d, TX, ctx->spec, ctx->plan_z, ctx->tw_z);
+    MDX_TRY(launch_div_fftx<double2>(ctx, "div+fft x", dg, ctx->spec, ctx->tw_x));
+    MDX_TRY((launch_fftz<false, double2>(ctx, "fft z", ctx->spec, ctx->tw_z)));
     const int nm = d.nxh * d.nz;
     MDX_LAUNCH(ctx, MDX_T_THOMAS, "thomas", kth, (nm + 127) / 128, 128, 0, d, 1.0 / (g.dy * g.dy), ctx->spec,
                ctx->thomas_dinv, ctx->thomas_cp);
-    MDX_LAUNCH(ctx, MDX_T_FFT_INV, "ifft z", kz_i, zblocks, 256, smz, d, TX, ctx->spec, ctx->plan_z, ctx->tw_z);
+    MDX_TRY((launch_fftz<true, double2>(ctx, "ifft z", ctx->spec, ctx->tw_z)));
     const double scale = 1.0 / (double)(d.nx * d.nz);
-    MDX_LAUNCH(ctx, MDX_T_FFT_INV, "ifft x", k_ifftx<double2>, xblocks, 256, smx, d, R, scale, ctx->spec, f[MDX_PHI],
-               ctx->plan_xh, ctx->tw_x);
+    MDX_TRY(launch_ifftx<double2>(ctx, "ifft x", scale, ctx->spec, f[MDX_PHI], ctx->tw_x));
     dim3 block(32, 4, 2);
     dim3 grid((d.nx + 31) / 32, (d.ny + 3) / 4, (d.nz + 1) / 2);
     if (ctx->ibm_zero)
@@ -665,6 +1001,7 @@ static int fft_mixed_alloc(mdx_ctx_t* ctx) {
     MDX_CUDA(ctx, cudaFuncSetAttribute(k_ifftx<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx));
     MDX_CUDA(ctx, cudaFuncSetAttribute(k_fftz<false, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz));
     MDX_CUDA(ctx, cudaFuncSetAttribute(k_fftz<true, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz));
+    MDX_TRY(fft_warp_attrs<float2>(ctx));
     return MDX_OK;
 }
 
@@ -674,21 +1011,11 @@ int mdx_k_projection_fft_mixed(mdx_ctx_t* ctx, double dg) {
     const mdx_grid_t& g = ctx->g;
     const mdx_solver_opts_t& o = ctx->opts;
     double** f = ctx->f;
-    const int M = d.nx / 2;
-    const int R = rows_per_block(M);
-    const int nrows = d.nz * d.ny;
-    const size_t smx = sizeof(float2) * 2 * R * M;
-    const int xblocks = (nrows + R - 1) / R;
-    const int TX = ztile(d.nz);
-    const size_t smz = sizeof(float2) * 2 * TX * (d.nz + 1);
-    const int zblocks = ((d.nxh + TX - 1) / TX) * d.ny;
     const int nm = d.nxh * d.nz;
     const double dyi2 = 1.0 / (g.dy * g.dy);
     const double scale = 1.0 / (double)(d.nx * d.nz);
     const long long tplane = (long long)d.nxh * (d.nz / 2 + 1);
     const size_t pad = sizeof(double) * d.npad;
-    auto kz_f = k_fftz<false, float2>;
-    auto kz_i = k_fftz<true, float2>;
     auto kth = k_thomas<float2, true>;
     auto kcor = ctx->ibm_zero ? k_correct_mixed<false> : k_correct_mixed<true>;
     dim3 block(32, 4, 2);
@@ -713,20 +1040,16 @@ int mdx_k_projection_fft_mixed(mdx_ctx_t* ctx, double dg) {
             MDX_CUDA(ctx, cudaMemcpyAsync(f[MDX_VS], f[MDX_VN], pad, cudaMemcpyDeviceToDevice, ctx->stream));
             MDX_CUDA(ctx, cudaMemcpyAsync(f[MDX_WS], f[MDX_WN], pad, cudaMemcpyDeviceToDevice, ctx->stream));
         }
-        MDX_LAUNCH(ctx, MDX_T_FFT_FWD, "div+fft x fp32", k_div_fftx<float2>, xblocks, 256, smx, d, R, g.dx, g.dy,
-                   g.dz, dg, f[MDX_US], f[MDX_VS], f[MDX_WS], ctx->spec32, ctx->plan_xh, ctx->tw_x32);
+        MDX_TRY(launch_div_fftx<float2>(ctx, "div+fft x fp32", dg, ctx->spec32, ctx->tw_x32));
         MDX_LAUNCH(ctx, MDX_T_FFT_FWD, "zero mode rhs", k_zero_rhs, d.ny, 256, 0, d, g.dx, g.dy, g.dz, dg, f[MDX_US],
                    f[MDX_VS], f[MDX_WS], ctx->rhs0);
-        MDX_LAUNCH(ctx, MDX_T_FFT_FWD, "fft z fp32", kz_f, zblocks, 256, smz, d, TX, ctx->spec32, ctx->plan_z,
-                   ctx->tw_z32);
+        MDX_TRY((launch_fftz<false, float2>(ctx, "fft z fp32", ctx->spec32, ctx->tw_z32)));
         MDX_LAUNCH(ctx, MDX_T_THOMAS, "thomas fp32", kth, (nm + 127) / 128, 128, 0, d, (float)dyi2, ctx->spec32,
                    ctx->dinv32, ctx->cp32);
         MDX_LAUNCH(ctx, MDX_T_THOMAS, "zero mode fp64", k_zero_solve, 1, 32, 0, d.ny, tplane, dyi2, scale,
                    ctx->thomas_dinv, ctx->thomas_cp, ctx->rhs0, ctx->phi0);
-        MDX_LAUNCH(ctx, MDX_T_FFT_INV, "ifft z fp32", kz_i, zblocks, 256, smz, d, TX, ctx->spec32, ctx->plan_z,
-                   ctx->tw_z32);
-        MDX_LAUNCH(ctx, MDX_T_FFT_INV, "ifft x fp32", k_ifftx<float2>, xblocks, 256, smx, d, R, (float)scale,
-                   ctx->spec32, ctx->phi32, ctx->plan_xh, ctx->tw_x32);
+        MDX_TRY((launch_fftz<true, float2>(ctx, "ifft z fp32", ctx->spec32, ctx->tw_z32)));
+        MDX_TRY(launch_ifftx<float2>(ctx, "ifft x fp32", (float)scale, ctx->spec32, ctx->phi32, ctx->tw_x32));
         MDX_LAUNCH(ctx, MDX_T_CORRECT, "correction mixed", kcor, grid, block, 0, d, g.dx, g.dy, g.dz, dg, ctx->phi32,
                    ctx->phi0, f[MDX_US], f[MDX_VS], f[MDX_WS], f[MDX_UN], f[MDX_VN], f[MDX_WN], f[MDX_PN],
                    f[MDX_COEF_U], f[MDX_COEF_V], f[MDX_COEF_W]);

@@ -30,7 +30,8 @@ module mdx_bindings
         integer(C_INT) :: max_iter, check_every, precision
         integer(C_INT) :: sor_variant, sor_kz
         integer(C_INT) :: check_mode
-        integer(C_INT) :: reserved_i(4)
+        integer(C_INT) :: fft_kernel
+        integer(C_INT) :: reserved_i(3)
         real(C_DOUBLE) :: atol
         real(C_DOUBLE) :: inner_sor
         real(C_DOUBLE) :: reserved_d(6)
