@@ -115,9 +115,146 @@ __device__ __forceinline__ void sor_cell(double& u_i, double& u_ip, double& v_j,
 }
 
 
-// The predictor of one cell (i,j,k), src/modules/step.f90:76-204; the IBM
+// The stencil of the predictor at one cell: u, v, w on the cell's faces and
+// their neighbours, p at the cell and its three lower neighbours.  Suffixes
+// name the offset: ip = (i+1), jm = (j-1), ip_km = (i+1, k-1), and so on.
+// momentum_vals reads it through accessors, so a caller can hand it values
+// held in registers (mdx_mom_nb) or read on demand from the padded arrays
+// (mdx_mom_ld, each value loaded in the branch that uses it).
+#define MDX_MOM_STENCIL(X)                                                            \
+    X(u_c) X(u_ip) X(u_im) X(u_jp) X(u_jm) X(u_kp) X(u_km) X(u_ip_jm) X(u_ip_km)   \
+    X(v_c) X(v_ip) X(v_im) X(v_jp) X(v_jm) X(v_kp) X(v_km) X(v_im_jp) X(v_jp_km)   \
+    X(w_c) X(w_ip) X(w_im) X(w_jp) X(w_jm) X(w_kp) X(w_km) X(w_im_kp) X(w_jm_kp)   \
+    X(p_c) X(p_im) X(p_jm) X(p_km)
+struct mdx_mom_nb {
+#define MDX_MOM_FIELD(n) double n##_v;
+#define MDX_MOM_GET(n) __device__ __forceinline__ double n() const { return n##_v; }
+    MDX_MOM_STENCIL(MDX_MOM_FIELD)
+    MDX_MOM_STENCIL(MDX_MOM_GET)
+#undef MDX_MOM_FIELD
+#undef MDX_MOM_GET
+};
+struct mdx_mom_ld {
+    const double *un, *vn, *wn, *pn;
+    long long c, SX, SY, SZ;
+    __device__ __forceinline__ double u_c() const { return __ldg(un + c); }
+    __device__ __forceinline__ double u_ip() const { return __ldg(un + c + SX); }
+    __device__ __forceinline__ double u_im() const { return __ldg(un + c - SX); }
+    __device__ __forceinline__ double u_jp() const { return __ldg(un + c + SY); }
+    __device__ __forceinline__ double u_jm() const { return __ldg(un + c - SY); }
+    __device__ __forceinline__ double u_kp() const { return __ldg(un + c + SZ); }
+    __device__ __forceinline__ double u_km() const { return __ldg(un + c - SZ); }
+    __device__ __forceinline__ double u_ip_jm() const { return __ldg(un + c + SX - SY); }
+    __device__ __forceinline__ double u_ip_km() const { return __ldg(un + c + SX - SZ); }
+    __device__ __forceinline__ double v_c() const { return __ldg(vn + c); }
+    __device__ __forceinline__ double v_ip() const { return __ldg(vn + c + SX); }
+    __device__ __forceinline__ double v_im() const { return __ldg(vn + c - SX); }
+    __device__ __forceinline__ double v_jp() const { return __ldg(vn + c + SY); }
+    __device__ __forceinline__ double v_jm() const { return __ldg(vn + c - SY); }
+    __device__ __forceinline__ double v_kp() const { return __ldg(vn + c + SZ); }
+    __device__ __forceinline__ double v_km() const { return __ldg(vn + c - SZ); }
+    __device__ __forceinline__ double v_im_jp() const { return __ldg(vn + c - SX + SY); }
+    __device__ __forceinline__ double v_jp_km() const { return __ldg(vn + c + SY - SZ); }
+    __device__ __forceinline__ double w_c() const { return __ldg(wn + c); }
+    __device__ __forceinline__ double w_ip() const { return __ldg(wn + c + SX); }
+    __device__ __forceinline__ double w_im() const { return __ldg(wn + c - SX); }
+    __device__ __forceinline__ double w_jp() const { return __ldg(wn + c + SY); }
+    __device__ __forceinline__ double w_jm() const { return __ldg(wn + c - SY); }
+    __device__ __forceinline__ double w_kp() const { return __ldg(wn + c + SZ); }
+    __device__ __forceinline__ double w_km() const { return __ldg(wn + c - SZ); }
+    __device__ __forceinline__ double w_im_kp() const { return __ldg(wn + c - SX + SZ); }
+    __device__ __forceinline__ double w_jm_kp() const { return __ldg(wn + c - SY + SZ); }
+    __device__ __forceinline__ double p_c() const { return __ldg(pn + c); }
+    __device__ __forceinline__ double p_im() const { return __ldg(pn + c - SX); }
+    __device__ __forceinline__ double p_jm() const { return __ldg(pn + c - SY); }
+    __device__ __forceinline__ double p_km() const { return __ldg(pn + c - SZ); }
+};
+
+// The predictor of one cell (i,j,k), src/modules/step.f90:76-204, from its
+// stencil values; writes us/vs/ws[c] and the new oldrhs at q.  The IBM
 // coefficients of the cell are cu/cv/cw[cc] (padded index, or the (i,j)
 // plane index when they do not vary along z).
+template <bool IBM, class NB>
+__device__ __forceinline__ void momentum_vals(const NB& n, const mdx_step_params& p, double dt_alpha,
+                                              double dt_beta, double dt_gamma, double* __restrict__ us,
+                                              double* __restrict__ vs, double* __restrict__ ws,
+                                              double* __restrict__ ou, double* __restrict__ ov,
+                                              double* __restrict__ ow, const double* __restrict__ cu,
+                                              const double* __restrict__ cv, const double* __restrict__ cw,
+                                              long long c, long long q, long long cc, int i, int j, int k) {
+    const double idx = p.idx, idy = p.idy, idz = p.idz, idx2 = p.idx2, idy2 = p.idy2, idz2 = p.idz2, ire = p.ire;
+    const double u_c = n.u_c(), v_c = n.v_c(), w_c = n.w_c(), p_c = n.p_c();
+    if (i >= p.nx0) {  // step.f90:106-136
+        const double u_ip = n.u_ip(), u_im = n.u_im(), u_jp = n.u_jp(), u_jm = n.u_jm(), u_kp = n.u_kp(), u_km = n.u_km();
+        double s;
+        s = u_ip + u_c;
+        const double uu_p = 0.25 * (s * s);
+        s = u_c + u_im;
+        const double uu_m = 0.25 * (s * s);
+        const double uv_p = 0.25 * (u_jp + u_c) * (n.v_jp() + n.v_im_jp());
+        const double uv_m = 0.25 * (u_c + u_jm) * (v_c + n.v_im());
+        const double uw_p = 0.25 * (u_c + u_kp) * (n.w_kp() + n.w_im_kp());
+        const double uw_m = 0.25 * (u_c + u_km) * (w_c + n.w_im());
+        const double diff_ux = (u_im - 2.0 * u_c + u_ip) * idx2;
+        const double diff_uy = (u_jm - 2.0 * u_c + u_jp) * idy2;
+        const double diff_uz = (u_km - 2.0 * u_c + u_kp) * idz2;
+        const double dpx = (p_c - n.p_im()) * idx;
+        const double rhsu = -((uu_p - uu_m) * idx) - (uv_p - uv_m) * idy - (uw_p - uw_m) * idz + p.fx +
+                            ire * (diff_ux + diff_uy + diff_uz);
+        double val = u_c + dt_alpha * rhsu + dt_beta * ou[q] - dt_gamma * dpx;
+        if (IBM) val = val * (1.0 / (1.0 + dt_gamma * __ldg(cu + cc)));
+        us[c] = val;
+        ou[q] = rhsu;
+    }
+    if (j >= p.ny0) {  // step.f90:138-168
+        const double v_ip = n.v_ip(), v_im = n.v_im(), v_jp = n.v_jp(), v_jm = n.v_jm(), v_kp = n.v_kp(), v_km = n.v_km();
+        double s;
+        const double vu_p = 0.25 * (v_c + v_ip) * (n.u_ip() + n.u_ip_jm());
+        const double vu_m = 0.25 * (v_c + v_im) * (u_c + n.u_jm());
+        s = v_c + v_jp;
+        const double vv_p = 0.25 * (s * s);
+        s = v_c + v_jm;
+        const double vv_m = 0.25 * (s * s);
+        const double vw_p = 0.25 * (v_kp + v_c) * (n.w_kp() + n.w_jm_kp());
+        const double vw_m = 0.25 * (v_km + v_c) * (w_c + n.w_jm());
+        const double diff_vx = (v_im - 2.0 * v_c + v_ip) * idx2;
+        const double diff_vy = (v_jm - 2.0 * v_c + v_jp) * idy2;
+        const double diff_vz = (v_km - 2.0 * v_c + v_kp) * idz2;
+        const double dpy = (p_c - n.p_jm()) * idy;
+        const double rhsv = -((vu_p - vu_m) * idx) - (vv_p - vv_m) * idy - (vw_p - vw_m) * idz + p.fy +
+                            ire * (diff_vx + diff_vy + diff_vz);
+        double val = v_c + dt_alpha * rhsv + dt_beta * ov[q] - dt_gamma * dpy;
+        if (IBM) val = val * (1.0 / (1.0 + dt_gamma * __ldg(cv + cc)));
+        vs[c] = val;
+        ov[q] = rhsv;
+    }
+    if (k >= p.nz0) {  // step.f90:170-200
+        const double w_ip = n.w_ip(), w_im = n.w_im(), w_jp = n.w_jp(), w_jm = n.w_jm(), w_kp = n.w_kp(), w_km = n.w_km();
+        double s;
+        const double wu_p = 0.25 * (w_c + w_ip) * (n.u_ip() + n.u_ip_km());
+        const double wu_m = 0.25 * (w_c + w_im) * (u_c + n.u_km());
+        s = w_c + w_kp;
+        const double ww_p = 0.25 * (s * s);
+        s = w_c + w_km;
+        const double ww_m = 0.25 * (s * s);
+        const double wv_p = 0.25 * (w_c + w_jp) * (n.v_jp() + n.v_jp_km());
+        const double wv_m = 0.25 * (w_c + w_jm) * (v_c + n.v_km());
+        const double diff_wx = (w_im - 2.0 * w_c + w_ip) * idx2;
+        const double diff_wy = (w_jm - 2.0 * w_c + w_jp) * idy2;
+        const double diff_wz = (w_km - 2.0 * w_c + w_kp) * idz2;
+        const double dpz = (p_c - n.p_km()) * idz;
+        const double rhsw = -((wu_p - wu_m) * idx) - (wv_p - wv_m) * idy - (ww_p - ww_m) * idz + p.fz +
+                            ire * (diff_wx + diff_wy + diff_wz);
+        double val = w_c + dt_alpha * rhsw + dt_beta * ow[q] - dt_gamma * dpz;
+        if (IBM) val = val * (1.0 / (1.0 + dt_gamma * __ldg(cw + cc)));
+        ws[c] = val;
+        ow[q] = rhsw;
+    }
+}
+
+// The predictor of one cell with its stencil read from the padded arrays in
+// the branches that use it (every offset stays inside the ghost layer for
+// 1 <= i,j,k <= n).
 template <bool IBM>
 __device__ __forceinline__ void momentum_cell(const mdx_dims& d, const mdx_step_params& p, double dt_alpha,
                                               double dt_beta, double dt_gamma, const double* __restrict__ un,
@@ -128,85 +265,10 @@ __device__ __forceinline__ void momentum_cell(const mdx_dims& d, const mdx_step_
                                               double* __restrict__ ow, const double* __restrict__ cu,
                                               const double* __restrict__ cv, const double* __restrict__ cw,
                                               long long cc, int i, int j, int k) {
-    const long long SX = 1, SY = d.nxp, SZ = (long long)d.nxp * d.nyp;
     const long long c = pidx(d, i, j, k);
-    const long long q = qidx(d, i, j, k);
-    const double idx = p.idx, idy = p.idy, idz = p.idz, idx2 = p.idx2, idy2 = p.idy2, idz2 = p.idz2, ire = p.ire;
-
-    const double u_c = __ldg(un + c), v_c = __ldg(vn + c), w_c = __ldg(wn + c), p_c = __ldg(pn + c);
-
-    if (i >= p.nx0) {  // step.f90:106-136
-        const double u_ip = __ldg(un + c + SX), u_im = __ldg(un + c - SX);
-        const double u_jp = __ldg(un + c + SY), u_jm = __ldg(un + c - SY);
-        const double u_kp = __ldg(un + c + SZ), u_km = __ldg(un + c - SZ);
-        double s;
-        s = u_ip + u_c;
-        const double uu_p = 0.25 * (s * s);
-        s = u_c + u_im;
-        const double uu_m = 0.25 * (s * s);
-        const double uv_p = 0.25 * (u_jp + u_c) * (__ldg(vn + c + SY) + __ldg(vn + c - SX + SY));
-        const double uv_m = 0.25 * (u_c + u_jm) * (v_c + __ldg(vn + c - SX));
-        const double uw_p = 0.25 * (u_c + u_kp) * (__ldg(wn + c + SZ) + __ldg(wn + c - SX + SZ));
-        const double uw_m = 0.25 * (u_c + u_km) * (w_c + __ldg(wn + c - SX));
-        const double diff_ux = (u_im - 2.0 * u_c + u_ip) * idx2;
-        const double diff_uy = (u_jm - 2.0 * u_c + u_jp) * idy2;
-        const double diff_uz = (u_km - 2.0 * u_c + u_kp) * idz2;
-        const double dpx = (p_c - __ldg(pn + c - SX)) * idx;
-        const double rhsu = -((uu_p - uu_m) * idx) - (uv_p - uv_m) * idy - (uw_p - uw_m) * idz + p.fx +
-                            ire * (diff_ux + diff_uy + diff_uz);
-        double val = u_c + dt_alpha * rhsu + dt_beta * ou[q] - dt_gamma * dpx;
-        if (IBM) val = val * (1.0 / (1.0 + dt_gamma * __ldg(cu + cc)));
-        us[c] = val;
-        ou[q] = rhsu;
-    }
-    if (j >= p.ny0) {  // step.f90:138-168
-        const double v_ip = __ldg(vn + c + SX), v_im = __ldg(vn + c - SX);
-        const double v_jp = __ldg(vn + c + SY), v_jm = __ldg(vn + c - SY);
-        const double v_kp = __ldg(vn + c + SZ), v_km = __ldg(vn + c - SZ);
-        double s;
-        const double vu_p = 0.25 * (v_c + v_ip) * (__ldg(un + c + SX) + __ldg(un + c + SX - SY));
-        const double vu_m = 0.25 * (v_c + v_im) * (u_c + __ldg(un + c - SY));
-        s = v_c + v_jp;
-        const double vv_p = 0.25 * (s * s);
-        s = v_c + v_jm;
-        const double vv_m = 0.25 * (s * s);
-        const double vw_p = 0.25 * (v_kp + v_c) * (__ldg(wn + c + SZ) + __ldg(wn + c - SY + SZ));
-        const double vw_m = 0.25 * (v_km + v_c) * (w_c + __ldg(wn + c - SY));
-        const double diff_vx = (v_im - 2.0 * v_c + v_ip) * idx2;
-        const double diff_vy = (v_jm - 2.0 * v_c + v_jp) * idy2;
-        const double diff_vz = (v_km - 2.0 * v_c + v_kp) * idz2;
-        const double dpy = (p_c - __ldg(pn + c - SY)) * idy;
-        const double rhsv = -((vu_p - vu_m) * idx) - (vv_p - vv_m) * idy - (vw_p - vw_m) * idz + p.fy +
-                            ire * (diff_vx + diff_vy + diff_vz);
-        double val = v_c + dt_alpha * rhsv + dt_beta * ov[q] - dt_gamma * dpy;
-        if (IBM) val = val * (1.0 / (1.0 + dt_gamma * __ldg(cv + cc)));
-        vs[c] = val;
-        ov[q] = rhsv;
-    }
-    if (k >= p.nz0) {  // step.f90:170-200
-        const double w_ip = __ldg(wn + c + SX), w_im = __ldg(wn + c - SX);
-        const double w_jp = __ldg(wn + c + SY), w_jm = __ldg(wn + c - SY);
-        const double w_kp = __ldg(wn + c + SZ), w_km = __ldg(wn + c - SZ);
-        double s;
-        const double wu_p = 0.25 * (w_c + w_ip) * (__ldg(un + c + SX) + __ldg(un + c + SX - SZ));
-        const double wu_m = 0.25 * (w_c + w_im) * (u_c + __ldg(un + c - SZ));
-        s = w_c + w_kp;
-        const double ww_p = 0.25 * (s * s);
-        s = w_c + w_km;
-        const double ww_m = 0.25 * (s * s);
-        const double wv_p = 0.25 * (w_c + w_jp) * (__ldg(vn + c + SY) + __ldg(vn + c + SY - SZ));
-        const double wv_m = 0.25 * (w_c + w_jm) * (v_c + __ldg(vn + c - SZ));
-        const double diff_wx = (w_im - 2.0 * w_c + w_ip) * idx2;
-        const double diff_wy = (w_jm - 2.0 * w_c + w_jp) * idy2;
-        const double diff_wz = (w_km - 2.0 * w_c + w_kp) * idz2;
-        const double dpz = (p_c - __ldg(pn + c - SZ)) * idz;
-        const double rhsw = -((wu_p - wu_m) * idx) - (wv_p - wv_m) * idy - (ww_p - ww_m) * idz + p.fz +
-                            ire * (diff_wx + diff_wy + diff_wz);
-        double val = w_c + dt_alpha * rhsw + dt_beta * ow[q] - dt_gamma * dpz;
-        if (IBM) val = val * (1.0 / (1.0 + dt_gamma * __ldg(cw + cc)));
-        ws[c] = val;
-        ow[q] = rhsw;
-    }
+    const mdx_mom_ld n{un, vn, wn, pn, c, 1, d.nxp, (long long)d.nxp * d.nyp};
+    momentum_vals<IBM>(n, p, dt_alpha, dt_beta, dt_gamma, us, vs, ws, ou, ov, ow, cu, cv, cw, c, qidx(d, i, j, k), cc,
+                       i, j, k);
 }
 
 // apply_bc_redblack, src/modules/boundary.f90:207-364, one (i,k), (j,k) or
