@@ -316,14 +316,48 @@ k_thomas(mdx_dims d, typename cx<C2>::R dyi2, C2* __restrict__ spec, const typen
         dp = cx<C2>::mk(r.x * di, r.y * di);
     }
     col[0] = dp;
-    for (int jj = 2; jj <= ny; ++jj) {
+    // The recurrences are serial in y, their operands are not: each block of
+    // TU rows is loaded before it is used, so one thread keeps TU row loads in
+    // flight (same arithmetic in the same order).
+    constexpr int TU = 8;
+    int jj = 2;
+    for (; jj + TU - 1 <= ny; jj += TU) {
+        C2 r[TU];
+        RT di[TU];
+#pragma unroll
+        for (int u = 0; u < TU; ++u) {
+            r[u] = col[(jj - 1 + u) * splane];
+            di[u] = __ldg(dinv + (jj - 1 + u) * tplane + mt);
+        }
+#pragma unroll
+        for (int u = 0; u < TU; ++u) {
+            dp = cx<C2>::mk((r[u].x - a * dp.x) * di[u], (r[u].y - a * dp.y) * di[u]);
+            col[(jj - 1 + u) * splane] = dp;
+        }
+    }
+    for (; jj <= ny; ++jj) {
         const C2 r = col[(jj - 1) * splane];
         const RT di = __ldg(dinv + (jj - 1) * tplane + mt);
         dp = cx<C2>::mk((r.x - a * dp.x) * di, (r.y - a * dp.y) * di);
         col[(jj - 1) * splane] = dp;
     }
     C2 nxt = dp;  // plane_hat(ny) = dp(ny)
-    for (int jj = ny - 1; jj >= 1; --jj) {
+    jj = ny - 1;
+    for (; jj - TU + 1 >= 1; jj -= TU) {
+        C2 dj[TU];
+        RT c[TU];
+#pragma unroll
+        for (int u = 0; u < TU; ++u) {
+            dj[u] = col[(jj - 1 - u) * splane];
+            c[u] = __ldg(cp + (jj - 1 - u) * tplane + mt);
+        }
+#pragma unroll
+        for (int u = 0; u < TU; ++u) {
+            nxt = cx<C2>::mk(dj[u].x - c[u] * nxt.x, dj[u].y - c[u] * nxt.y);
+            col[(jj - 1 - u) * splane] = nxt;
+        }
+    }
+    for (; jj >= 1; --jj) {
         const C2 dj = col[(jj - 1) * splane];
         const RT c = __ldg(cp + (jj - 1) * tplane + mt);
         nxt = cx<C2>::mk(dj.x - c * nxt.x, dj.y - c * nxt.y);
@@ -474,7 +508,7 @@ template <typename C2> __device__ __forceinline__ void cp_async_elem(C2* dst, co
 
 // build_fft_rhs + forward real FFT along x, one warp per (k, j) row; M = nx/2 = 32 P.
 template <int P, typename C2>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 4)
 k_div_fftx_w(mdx_dims d, double dx, double dy, double dz, double dt_gamma, const double* __restrict__ us,
              const double* __restrict__ vs, const double* __restrict__ ws, C2* __restrict__ spec,
              const C2* __restrict__ twx) {
