@@ -559,7 +559,7 @@ k_div_fftx_w(mdx_dims d, double dx, double dy, double dz, double dt_gamma, const
 // or 16 FP32 complex values) through shared memory; one warp per column.
 template <typename C2> __host__ __device__ constexpr int ztile_w() { return 128 / (int)sizeof(C2); }
 template <bool INV, int P, typename C2>
-__global__ void __launch_bounds__(32 * ztile_w<C2>(), P >= 16 ? 1 : (sizeof(C2) == 16 ? 3 : 2))
+__global__ void __launch_bounds__(32 * ztile_w<C2>(), P >= 16 ? 1 : (sizeof(C2) == 16 ? 4 : 2))
 k_fftz_w(mdx_dims d, C2* __restrict__ spec, const C2* __restrict__ twz) {
     constexpr int NZ = 32 * P, TX = ztile_w<C2>();
     extern __shared__ __align__(16) unsigned char sm_raw[];

@@ -21,7 +21,7 @@
 constexpr int MOM_KZ = 8;
 
 template <bool IBM>
-__global__ void __launch_bounds__(256, 3)
+__global__ void __launch_bounds__(256, 4)
 k_momentum(mdx_dims d, mdx_step_params p, double dt_alpha, double dt_beta, double dt_gamma,
            const double* __restrict__ un, const double* __restrict__ vn, const double* __restrict__ wn,
            const double* __restrict__ pn, double* __restrict__ us, double* __restrict__ vs,
