@@ -384,7 +384,7 @@ def _roofline(tim, kname, alg_per_cell, cells, ms, traffic_key=None):
             "avg_launch_ms": avg_s * 1e3, "launches": kn, "share_of_step_time": kms / ms if ms > 0 else None}
 
 
-def _fft_passes(cfg, tim, cells, ms):
+def _fft_passes(cfg, tim, cells, ms, ms_step):
     """Achieved HBM rate of each pass class of the FP64 FFT projection, from
     its algorithmic bytes per cell: fft_fwd = divergence reads (3 doubles) +
     spectrum write, z transform read+write; thomas = spectrum read+write + the
@@ -397,6 +397,11 @@ def _fft_passes(cfg, tim, cells, ms):
                 "correct": 72.0 + (24.0 if cfg["ibm"] != "none" else 0.0)}
     peak, peak_kind = _peaks()
     out = {"peak_gbs": peak, "peak_kind": peak_kind}
+    # the whole step against its algorithmic bytes: 29 doubles per cell and
+    # substage (predictor 14, x-z FFT 2, Thomas 2, inverse FFT 2, correction 9)
+    step_bytes = 3 * 29 * 8.0 * cells
+    step_gbs = step_bytes / (ms_step / 1e3) / 1e9
+    out["step"] = {"alg_bytes_per_cell_step": 696, "ms_per_step": ms_step, "gbs": step_gbs, "frac": step_gbs / peak}
     nproj = tim["correct"][1]          # one correction launch per projection
     for k, b in per_cell.items():
         kms, kn = tim[k]
@@ -475,7 +480,8 @@ def run_plain(args, cfg):
                              traffic_key=_sor64_traffic_key(s.last_solve_stats().variant))
     else:
         roofline = _roofline(tim, "momentum", 112.0, cells, ms)   # 14 doubles per cell
-    fft_passes = _fft_passes(cfg, tim, cells, ms) if cfg["solver"] != "redblack" else None
+    fft_passes = (_fft_passes(cfg, tim, cells, ms, ms_all / args.steps) if cfg["solver"] != "redblack"
+                  else None)
     iters_per_substage = iters / (3 * args.steps) if cfg["solver"] == "redblack" else 0
     sor_kernel = None
     if cfg["solver"] == "redblack":
