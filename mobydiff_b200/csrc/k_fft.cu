@@ -419,7 +419,7 @@ k_ifftx(mdx_dims d, int R, typename cx<C2>::R scale, const C2* __restrict__ spec
 // lanes runs for each p as five radix-2 decimation-in-frequency stages whose
 // partner values come from __shfl_xor_sync:
 //   X[p + P q] = sum_l W_32^(l q) W_N^(l p) sum_m x[l + 32 m] W_P^(m p).
-// Lane l ends holding X[p + P brev5(l)] in v[p].  Roots come from the same
+// Lane l ends holding X[wout(l, q)] in v[q].  Roots come from the same
 // long-double twiddle tables as the Stockham transforms: W_N^t = tw[t tws].
 // ---------------------------------------------------------------------------
 __host__ __device__ constexpr int wlog2(int p) { return p <= 1 ? 0 : 1 + wlog2(p / 2); }
@@ -455,7 +455,12 @@ __device__ __forceinline__ void warp_fft(C2 (&v)[P], int lane, const C2* __restr
 #pragma unroll
     for (int p = 1; p < P; ++p) y[p] = cmul_f(y[p], twid<INV>(tw, lane * p * tws));
     // 32-point DIF across the lanes; the roots of the last two stages are
-    // 1 and W_4 = -i, applied without a multiply
+    // 1 and W_4 = -i, applied without a multiply.  For P >= 2 each stage
+    // trades the lane bit h for register bit 0: a lane keeps the elements
+    // whose register bit 0 equals its lane bit h, sends the other half to its
+    // partner, and computes both outputs of the butterflies it holds, so a
+    // stage moves P/2 elements per lane instead of P (wout gives where each
+    // register ends up).
 #pragma unroll
     for (int s = 0; s < 5; ++s) {
         const int h = 16 >> s;
@@ -463,18 +468,33 @@ __device__ __forceinline__ void warp_fft(C2 (&v)[P], int lane, const C2* __restr
         C2 w = cx<C2>::mk(1, 0);
         if (h > 2) w = twid<INV>(tw, (lane & (h - 1)) * (N / (2 * h)) * tws);   // W_2h^(l mod h)
         const bool rot = (h == 2) && (lane & 1);
-#pragma unroll
-        for (int p = 0; p < P; ++p) {
+        if (P == 1) {
             C2 o;
-            o.x = __shfl_xor_sync(0xffffffffu, y[p].x, h);
-            o.y = __shfl_xor_sync(0xffffffffu, y[p].y, h);
+            o.x = __shfl_xor_sync(0xffffffffu, y[0].x, h);
+            o.y = __shfl_xor_sync(0xffffffffu, y[0].y, h);
             if (!up) {
-                y[p] = cadd(y[p], o);
+                y[0] = cadd(y[0], o);
             } else {
-                const C2 dd = csub(o, y[p]);
-                if (h > 2) y[p] = cmul_f(dd, w);
-                else if (rot) y[p] = INV ? cmul_pi(dd) : cmul_mi(dd);
-                else y[p] = dd;
+                const C2 dd = csub(o, y[0]);
+                if (h > 2) y[0] = cmul_f(dd, w);
+                else if (rot) y[0] = INV ? cmul_pi(dd) : cmul_mi(dd);
+                else y[0] = dd;
+            }
+        } else {
+#pragma unroll
+            for (int p0 = 0; p0 < P; p0 += 2) {
+                const C2 keep = up ? y[p0 + 1] : y[p0];
+                const C2 send = up ? y[p0] : y[p0 + 1];
+                C2 o;
+                o.x = __shfl_xor_sync(0xffffffffu, send.x, h);
+                o.y = __shfl_xor_sync(0xffffffffu, send.y, h);
+                const C2 lo = up ? o : keep;     // the element of the lower lane of the pair
+                const C2 hi = up ? keep : o;
+                y[p0] = cadd(lo, hi);
+                const C2 dd = csub(lo, hi);
+                if (h > 2) y[p0 + 1] = cmul_f(dd, w);
+                else if (rot) y[p0 + 1] = INV ? cmul_pi(dd) : cmul_mi(dd);
+                else y[p0 + 1] = dd;
             }
         }
     }
@@ -496,6 +516,16 @@ template <int P, typename C2> __device__ __forceinline__ int wcol(int kz) {
     return (kz ^ wsw<P, C2>(kz)) & (G - 1);
 }
 __device__ __forceinline__ int brev5(int l) { return (int)(__brev((unsigned)l) >> 27); }
+// Index of the transform output that warp_fft leaves in register q of lane
+// l.  With the bit trades of the lane stages, the conceptual lane is
+// (q bit 0, l bits 0..3) and the register index is (l bit 4, q bits 1..);
+// the output is X[p + P brev5(lane)].
+template <int P> __device__ __forceinline__ int wout(int lane, int q) {
+    if (P == 1) return brev5(lane);
+    const int p = (q & ~1) | (lane >> 4);
+    const int cl = (q & 1) | ((lane & 15) << 1);
+    return p + P * brev5(cl);
+}
 // one complex element global -> shared, asynchronous (cp.async; 16 bytes
 // bypass L1, 8 bytes through it)
 template <typename C2> __device__ __forceinline__ void cp_async_elem(C2* dst, const C2* src) {
@@ -508,7 +538,7 @@ template <typename C2> __device__ __forceinline__ void cp_async_elem(C2* dst, co
 
 // build_fft_rhs + forward real FFT along x, one warp per (k, j) row; M = nx/2 = 32 P.
 template <int P, typename C2>
-__global__ void __launch_bounds__(256, 4)
+__global__ void __launch_bounds__(256, P >= 16 ? 2 : 4)
 k_div_fftx_w(mdx_dims d, double dx, double dy, double dz, double dt_gamma, const double* __restrict__ us,
              const double* __restrict__ vs, const double* __restrict__ ws, C2* __restrict__ spec,
              const C2* __restrict__ twx) {
@@ -535,9 +565,8 @@ k_div_fftx_w(mdx_dims d, double dx, double dy, double dz, double dt_gamma, const
         v[m] = cx<C2>::mk((RT)x[0], (RT)x[1]);
     }
     warp_fft<false, P>(v, lane, twx, 2);
-    const int q = brev5(lane);
 #pragma unroll
-    for (int p = 0; p < P; ++p) buf[wline<P, C2>(p + P * q)] = v[p];
+    for (int p = 0; p < P; ++p) buf[wline<P, C2>(wout<P>(lane, p))] = v[p];
     __syncwarp();
     // split step: X_k = E_k + W^k O_k, E = (Z_k + conj Z_{M-k})/2, O = -i/2 (Z_k - conj Z_{M-k})
     C2* X = spec + (long long)row * d.nxh;
@@ -591,10 +620,9 @@ k_fftz_w(mdx_dims d, C2* __restrict__ spec, const C2* __restrict__ twz) {
         }
         warp_fft<INV, P>(v, lane, twz, 1);
         __syncwarp();
-        const int q = brev5(lane);
 #pragma unroll
         for (int p = 0; p < P; ++p) {
-            const int kz = p + P * q;
+            const int kz = wout<P>(lane, p);
             S[kz * TX + (c ^ wcol<P, C2>(kz))] = v[p];
         }
     }
@@ -632,9 +660,8 @@ k_ifftx_w(mdx_dims d, typename cx<C2>::R scale, const C2* __restrict__ spec, typ
         v[m] = cadd(e, cmul_pi(o));
     }
     warp_fft<true, P>(v, lane, twx, 2);
-    const int q = brev5(lane);
 #pragma unroll
-    for (int p = 0; p < P; ++p) buf[wline<P, C2>(p + P * q)] = v[p];
+    for (int p = 0; p < P; ++p) buf[wline<P, C2>(wout<P>(lane, p))] = v[p];
     __syncwarp();
     C2* out = reinterpret_cast<C2*>(phi + (long long)row * d.nx);
 #pragma unroll

@@ -1,7 +1,8 @@
 """CPU model of the warp-shuffle transforms of the FFT path (k_fft.cu,
-warp_fft / wline / wcol): the four-step split N = P x 32 with lane l holding
-x[l + 32 m], the radix-2 decimation-in-frequency stages in registers and
-across the lanes, and the shared-memory swizzles.  The model follows the
+warp_fft / wout / wline / wcol): the four-step split N = P x 32 with lane l
+holding x[l + 32 m], the radix-2 decimation-in-frequency stages in registers
+and across the lanes (half exchanges that trade a lane bit for a register
+bit), the output positions, and the shared-memory swizzles.  The model follows the
 kernel's index algebra step by step in numpy and is checked against
 numpy.fft; the swizzles are checked for being permutations that spread each
 warp access over all bank groups."""
@@ -18,8 +19,17 @@ def brev(x, bits):
     return r
 
 
+def wout(lane, q, P):
+    """Output index of register q of lane `lane` after warp_fft (k_fft.cu wout)."""
+    if P == 1:
+        return brev(lane, 5)
+    p = (q & ~1) | (lane >> 4)
+    cl = (q & 1) | ((lane & 15) << 1)
+    return p + P * brev(cl, 5)
+
+
 def warp_fft_model(x, inv=False):
-    """X[p + P brev5(l)] = v[l][p] after the kernel's steps; returns X."""
+    """X[wout(l, q)] = v[l][q] after the kernel's steps; returns X."""
     N = x.size
     P = N // 32
     sign = 1.0 if inv else -1.0
@@ -40,17 +50,31 @@ def warp_fft_model(x, inv=False):
         y[:, brev(i, LP)] = v[:, i]
     for p in range(1, P):
         y[:, p] *= W(lanes * p, N)
-    # 32-point DIF across the lanes, partner = lane ^ h
+    # 32-point DIF across the lanes, partner = lane ^ h.  P = 1 exchanges
+    # its one element; for P >= 2 a lane keeps the element of each register
+    # pair (p0, p0 + 1) whose bit 0 equals its lane bit h and sends the other.
     for s in range(5):
         h = 16 >> s
         up = (lanes & h) != 0
         w = W((lanes & (h - 1)) * (N // (2 * h)), N)
-        o = y[lanes ^ h]
-        y = np.where(up[:, None], (o - y) * w[:, None], y + o)
+        if P == 1:
+            o = y[lanes ^ h]
+            y = np.where(up[:, None], (o - y) * w[:, None], y + o)
+            continue
+        ny = y.copy()
+        for p0 in range(0, P, 2):
+            keep = np.where(up, y[:, p0 + 1], y[:, p0])
+            send = np.where(up, y[:, p0], y[:, p0 + 1])
+            o = send[lanes ^ h]
+            lo = np.where(up, o, keep)
+            hi = np.where(up, keep, o)
+            ny[:, p0] = lo + hi
+            ny[:, p0 + 1] = (lo - hi) * w
+        y = ny
     X = np.empty(N, dtype=np.complex128)
     for l in lanes:
-        for p in range(P):
-            X[p + P * brev(l, 5)] = y[l, p]
+        for q in range(P):
+            X[wout(l, q, P)] = y[l, q]
     return X
 
 
@@ -100,8 +124,8 @@ def test_line_swizzle_is_a_conflict_free_permutation(P, elem):
     lanes = range(32)
     for m in range(P):                            # natural-order reads k = l + 32 m
         assert _groups([wline(l + 32 * m, P, G) for l in lanes], elem) == best
-    for p in range(P):                            # bit-reversed writes k = p + P brev5(l)
-        assert _groups([wline(p + P * brev(l, 5), P, G) for l in lanes], elem) == best
+    for q in range(P):                            # the transform's writes k = wout(l, q)
+        assert _groups([wline(wout(l, q, P), P, G) for l in lanes], elem) == best
 
 
 @pytest.mark.parametrize("P", PS)
@@ -116,8 +140,8 @@ def test_z_tile_swizzle_is_a_conflict_free_permutation(P, elem):
     for c in range(TX):                           # a warp's column reads and writes
         for m in range(P):
             assert _groups([(l + 32 * m) * TX + (c ^ wcol(l + 32 * m, P, G)) for l in range(32)], elem) == best
-        for p in range(P):
-            kzs = [p + P * brev(l, 5) for l in range(32)]
+        for q in range(P):
+            kzs = [wout(l, q, P) for l in range(32)]
             assert _groups([kz * TX + (c ^ wcol(kz, P, G)) for kz in kzs], elem) == best
     # the cp.async staging: 32 consecutive threads cover 32 / TX whole rows
     for t0 in range(0, NZ * TX, 32):
