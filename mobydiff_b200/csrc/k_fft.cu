@@ -503,8 +503,9 @@ __device__ __forceinline__ void warp_fft(C2 (&v)[P], int lane, const C2* __restr
 }
 
 // Shared-memory swizzle of element k of a line: the natural-order reads
-// (k = l + 32 m) and the bit-reversed writes (k = p + P brev5(l)) of a warp
-// both spread over all bank groups of G = 128 / sizeof(C2) elements.
+// (k = l + 32 m) and the transform's writes (k = wout(l, q)) of a warp both
+// spread over all bank groups of G = 128 / sizeof(C2) elements (checked for
+// every P and both element sizes in tests/test_fft_warp_model.py).
 template <int P, typename C2> __device__ __forceinline__ int wsw(int k) {
     constexpr int G = 128 / (int)sizeof(C2);
     return P == 1 ? 0 : (k / P) & (G - 1);
@@ -517,9 +518,9 @@ template <int P, typename C2> __device__ __forceinline__ int wcol(int kz) {
 }
 __device__ __forceinline__ int brev5(int l) { return (int)(__brev((unsigned)l) >> 27); }
 // Index of the transform output that warp_fft leaves in register q of lane
-// l.  With the bit trades of the lane stages, the conceptual lane is
-// (q bit 0, l bits 0..3) and the register index is (l bit 4, q bits 1..);
-// the output is X[p + P brev5(lane)].
+// l.  With the bit trades of the lane stages, the conceptual lane c is
+// (q bit 0, l bits 0..3) and the conceptual register p is (l bit 4,
+// q bits 1..); the output is X[p + P brev5(c)].
 template <int P> __device__ __forceinline__ int wout(int lane, int q) {
     if (P == 1) return brev5(lane);
     const int p = (q & ~1) | (lane >> 4);
