@@ -76,13 +76,6 @@ CONFIGS = {
                      amp=0.0, method="plain"),
 }
 
-# Red-black iterations per RK3 step of the plain FP64 method (zero start) on
-# the 256x128x128 wavy channel in the steps the default run times (warm-up
-# 3, steps 3), measured on B200, per tolerance; the oracle's sweeps are
-# bit-identical, so its counts are the same.  Used only to scale the
-# reference arm's bounded CPU sample to a full step.
-PLAIN_ITERS_PER_STEP = {1e-10: 48000.0, 1e-8: 27500.0}
-
 # Held-out training runs of the learned warm start: (seed, wall amplitude).
 TRAIN_RUNS = ((20261204, 0.03), (20261205, 0.07))
 SEED = 20261203
@@ -268,30 +261,87 @@ def _cpu_baseline(cfg, iters_per_step):
     return {"value": cells / per_step / 1e6, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
 
 
+def _oracle_state(cfg, O):
+    """The seeded start of the workload on the host, made the way
+    mdx_channel_ic makes it on the device: Poiseuille + noise, projected at
+    t = 0 with dt_gamma = 1 by the config's own solver (red-black: residual
+    checked every `check_every` iterations), then p = 0."""
+    g = O.Grid(cfg["nx"], cfg["ny"], cfg["nz"], cfg["lx"], cfg["ly"], cfg["lz"], cfg["re"], cfg["dt"],
+               (2.0 / cfg["re"], 0.0, 0.0))
+    bc = O.channel_bc()
+    f = O.Fields(g)
+    y0 = (cfg["ly"] - 2.0) / 2.0
+    lam = cfg["lx"] / 2.0
+    if cfg["ibm"] == "wavy":
+        O.set_ibm_coeff(g, O.ibm_wavy(cfg["amp"], lam, y0), f)
+    O.channel_ic(g, f, SEED, 0.1, 0.01, y0, cfg["amp"], lam)
+    f.us[...] = f.un
+    f.vs[...] = f.vn
+    f.ws[...] = f.wn
+    ic_iters = 0
+    if cfg["solver"] == "redblack":
+        _, ic_iters, _ = O.pressure_projection_redblack(g, bc, f, 1.0, sor=cfg["sor"], tol=cfg["tol"],
+                                                        max_iter=400000, check_every=cfg["check_every"])
+        O.apply_bc_redblack(g, bc, f)
+    else:
+        O.apply_bc(g, f)
+        O.pressure_projection_fft(g, f, 1.0)
+        O.apply_bc(g, f)
+    f.pn[...] = 0.0
+    return g, bc, f, ic_iters
+
+
 def run_reference(args, cfg):
+    """The reference's method on the host cores: the oracle (the CPU
+    restatement of the reference's step) runs whole RK3 steps end to end
+    from the projected seeded start -- predictor, projection to the
+    config's residual with its own checks, boundary conditions -- and the
+    line reports the measured Mcell-steps/s.  Red-black: one full step
+    (minutes on the host; its iteration count is the GPU plain arm's
+    `first_step` count, the sweeps being bit-identical); FFT: up to K full
+    steps within about a minute."""
     ws, rank, _ = _dist()
     if rank != 0:
         return 0
+    from oracle import oracle as O
+    O.build()
     threads = os.cpu_count() or 1
-    iters = PLAIN_ITERS_PER_STEP[cfg["tol"]] if cfg["solver"] == "redblack" else 0.0
-    vals = []
-    for step in range(args.warmup + args.steps):
-        ph, cells = _oracle_sample(cfg, threads, target_s=6.0)
-        if step >= args.warmup:
-            vals.append(cells / _cpu_step_seconds(cfg, ph, iters) / 1e6)
-    value = float(np.median(vals))
+    O.set_threads(threads)
+    t0 = time.perf_counter()
+    g, bc, f, ic_iters = _oracle_state(cfg, O)
+    setup_s = time.perf_counter() - t0
+    cells = cfg["nx"] * cfg["ny"] * cfg["nz"]
+    a, _, _ = O.rk_coeffs()
+    extra = {}
     if cfg["solver"] == "redblack":
-        sample = (f"per step: 3 predictor passes + ~{ph['sor_iters_sampled']} red-black iterations of the "
-                  f"{int(iters)} a full step of the reference's method (FP64 sweeps from phi = 0) needs at "
-                  f"residual {cfg['tol']:g}, on the full {cfg['nx']}x{cfg['ny']}x{cfg['nz']} grid; step time "
-                  "extrapolated by iteration count")
+        t0 = time.perf_counter()
+        st, iters = O.run(g, bc, f, cfg["dt"], 1, solver=1, sor=cfg["sor"], tol=cfg["tol"], max_iter=400000,
+                          check_every=cfg["check_every"])
+        elapsed = time.perf_counter() - t0
+        nsteps = 1
+        extra = {"iterations_per_step": iters, "status": st, "t0_projection_iterations": ic_iters}
+        sample = (f"one full RK3 step of the reference's method (FP64 red-black SOR from phi = 0, omega "
+                  f"{cfg['sor']}, residual {cfg['tol']:g} checked every {cfg['check_every']} iterations) on the "
+                  f"full {cfg['nx']}x{cfg['ny']}x{cfg['nz']} grid from the projected seeded start: {iters} "
+                  f"iterations, timed end to end")
     else:
-        sample = "one full RK3 step on the full grid"
+        nsteps = 0
+        t0 = time.perf_counter()
+        while nsteps < max(args.steps, 1):
+            O.run(g, bc, f, cfg["dt"], 1, solver=0)
+            nsteps += 1
+            if time.perf_counter() - t0 > 60.0:
+                break
+        elapsed = time.perf_counter() - t0
+        sample = f"{nsteps} full RK3 steps (FP64 FFT + Thomas) on the full grid from the projected seeded start"
+    value = cells * nsteps / elapsed / 1e6
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "steps": nsteps, "steps_requested": args.steps, "warmup": 0, "ms_per_step": elapsed * 1e3 / nsteps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": cfg["workload"], "arm": "CPU restatement of the reference (oracle), OpenMP, "
-                                                           "plain FP64 method"},
+                                                           "plain FP64 method, whole steps timed",
+                       "setup_s": setup_s},
+            "reference_step": extra,
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -316,12 +366,13 @@ def aggregate_value(cells_per_rank, steps, ms_max, world):
     return world * cells_per_rank * steps / (ms_max / 1e3) / 1e6
 
 
-def _timed_steps(s, stream, steps, pg=None, timing=False):
+def _timed_steps(s, stream, steps, pg=None, timing=0):
     """K steps between events on the solver's stream (barrier + synchronize
     on both sides); returns (ms over ranks, ms of this rank, iterations,
-    launches, per-class timing).  With `timing` every 8th launch of each
-    kernel class is bracketed by events as well (for the roofline; it costs
-    a few per cent, so the headline runs without it)."""
+    launches, per-class timing).  timing 1: every 8th launch of each kernel
+    class is bracketed by events as well; timing 2: only each run of
+    back-to-back red-black sweeps between two residual checks (for the
+    roofline; the headline runs without events)."""
     import torch
     s.set_timing(timing)
     if pg:
@@ -372,16 +423,44 @@ def _e2e_steps(s, stream, host, steps, pg=None):
 
 
 def _roofline(tim, kname, alg_per_cell, cells, ms, traffic_key=None):
+    """Dominant kernel against measured HBM.  For the red-black sweeps
+    (kname "sor_run") the time is that of whole runs of back-to-back sweep
+    launches between residual checks, every run timed with one event pair,
+    so the average launch is the sweeps' throughput in the step and the
+    runs' share of the replay's time is at most 1."""
     peak, peak_kind = _peaks()
     kms, kn = tim[kname]
     avg_s = (kms / 1e3) / max(kn, 1)
     alg_bytes = alg_per_cell * cells
     achieved = alg_bytes / avg_s / 1e9 if kn else None
     tpc = _traffic_per_cell(traffic_key or kname)
-    return {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+    return {"kernel": traffic_key or kname, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind,
             "traffic": (tpc * cells) if tpc else None, "algorithmic_bytes": alg_bytes,
-            "avg_launch_ms": avg_s * 1e3, "launches": kn, "share_of_step_time": kms / ms if ms > 0 else None}
+            "avg_launch_ms": avg_s * 1e3, "launches": kn,
+            "timing": ("event pair around each run of back-to-back sweeps" if kname == "sor_run"
+                       else "every 8th launch bracketed by events"),
+            "share_of_step_time": kms / ms if ms > 0 else None}
+
+
+def _sor_alg_per_launch(variant, fp32=False):
+    """Algorithmic bytes per cell of one sweep launch: 4 arrays read and
+    written for the cells of one colour (FP64 32 B, FP32 16 B per cell of
+    the grid); a fused red+black launch does both colours."""
+    per_colour = 16.0 if fp32 else 32.0
+    return 2 * per_colour if variant in (2, 3) else per_colour
+
+
+def _step_hbm(cells, ms_per_step, iters_per_step, per_iter):
+    """The whole red-black step against its algorithmic bytes: 104 B per cell
+    per substage for the predictor and projection set-up (13 doubles) and
+    `per_iter` B per cell per red+black iteration (64 FP64, 32 FP32)."""
+    peak, peak_kind = _peaks()
+    b = cells * (3 * 104.0 + per_iter * iters_per_step)
+    gbs = b / (ms_per_step / 1e3) / 1e9
+    return {"alg_bytes_per_cell_step": 3 * 104.0 + per_iter * iters_per_step, "formula":
+            f"3*104 + {per_iter:g}*iterations per step", "gbs": gbs, "peak_gbs": peak, "frac": gbs / peak,
+            "peak_kind": peak_kind}
 
 
 def _fft_passes(cfg, tim, cells, ms, ms_step):
@@ -411,6 +490,24 @@ def _fft_passes(cfg, tim, cells, ms, ms_step):
         out[k] = {"alg_bytes_per_cell": round(b, 3), "launches": kn, "projections": nproj, "ms": kms, "gbs": gbs,
                   "frac": gbs / peak, "share_of_step_time": kms / ms if ms > 0 else None}
     return out
+
+
+def _first_step(cfg, M, device, tol):
+    """The plain FP64 method's first RK3 step from the projected seeded
+    start, residual checked after every `check_every` iterations (the
+    oracle's schedule): the same step, start and iteration count as the
+    reference arm's timed CPU step."""
+    import torch
+    s, _ = _setup(cfg, M, device, tol=tol, precision=M.PREC_FP64)
+    opts = M.make_solver_opts(M.SOLVER_REDBLACK, sor=cfg["sor"], tol=tol, check_every=cfg["check_every"],
+                              max_iter=400000, adaptive_checks=False)
+    s.init_pressure_solver(opts)
+    s.channel_ic(SEED, 0.1, 0.01, (cfg["ly"] - 2.0) / 2.0, cfg["amp"], cfg["lx"] / 2.0)   # t=0 projection, same checks
+    stream = torch.cuda.ExternalStream(s.stream(), device=device)
+    ms, _, it, _, _ = _timed_steps(s, stream, 1)
+    s.close()
+    return {"iterations": it, "ms": ms, "check": f"every {cfg['check_every']} iterations",
+            "value": cfg["nx"] * cfg["ny"] * cfg["nz"] / (ms / 1e3) / 1e6, "unit": UNIT}
 
 
 def _init_dist(device):
@@ -470,14 +567,16 @@ def run_plain(args, cfg):
         e2e_line = {"value": ws * cells * args.steps / (ems / 1e3) / 1e6, "unit": UNIT,
                     "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
                     "same_steps_as_value": e2e_iters == iters}
-        # the same steps once more with per-kernel events, for the roofline
+        # the same steps once more with events, for the roofline
         s.update_device(*[h.numpy() for h in host])
-        _, ms, _, _, tim = _timed_steps(s, stream, args.steps, pg, timing=True)
-    else:
-        _, ms, _, _, tim = _timed_steps(s, stream, args.steps, pg, timing=True)
+    mode = 2 if cfg["solver"] == "redblack" else 1
+    _, ms, _, _, tim = _timed_steps(s, stream, args.steps, pg, timing=mode)
+    step_hbm = None
     if cfg["solver"] == "redblack":   # 4 doubles per cell per colour sweep
-        roofline = _roofline(tim, "sor_sweep", 32.0, cells, ms,
-                             traffic_key=_sor64_traffic_key(s.last_solve_stats().variant))
+        var = s.last_solve_stats().variant
+        roofline = _roofline(tim, "sor_run", _sor_alg_per_launch(var), cells, ms,
+                             traffic_key=_sor64_traffic_key(var))
+        step_hbm = _step_hbm(cells, ms_all / args.steps, iters / args.steps, 64.0)
     else:
         roofline = _roofline(tim, "momentum", 112.0, cells, ms)   # 14 doubles per cell
     fft_passes = (_fft_passes(cfg, tim, cells, ms, ms_all / args.steps) if cfg["solver"] != "redblack"
@@ -499,8 +598,8 @@ def run_plain(args, cfg):
                            "parallelism": f"replicas x{ws}",
                            "l2": "inputs larger than L2 (state + IBM coefficients > 126 MB)"},
                 "poisson_iters_per_substage": iters_per_substage, "sor_kernel": sor_kernel,
-                "roofline": roofline, "fft_passes": fft_passes, "cpu_baseline": cpu, "clocks": clk, "e2e": e2e_line,
-                "gpu_launches": launches}
+                "roofline": roofline, "step_hbm": step_hbm, "fft_passes": fft_passes, "cpu_baseline": cpu,
+                "clocks": clk, "e2e": e2e_line, "gpu_launches": launches}
         print(json.dumps(line), flush=True)
     s.close()
     if pg:
@@ -869,6 +968,7 @@ def run_learned_mixed(args, cfg):
     W, K = args.warmup, args.steps
 
     # ---- plain FP64 arm: zero start, FP64 sweeps, same tolerance ------------
+    first_step = _first_step(cfg, M, device, tol)
     sp, g = _setup(cfg, M, device, tol=tol, precision=M.PREC_FP64)
     stream_p = torch.cuda.ExternalStream(sp.stream(), device=device)
     for _ in range(W):
@@ -876,11 +976,13 @@ def run_learned_mixed(args, cfg):
     p_ms_all, p_ms, p_iters, _, _ = _timed_steps(sp, stream_p, K, pg)
     plain_value = ws * cells * K / (p_ms_all / 1e3) / 1e6
     plain_state = {n: sp.get(n) for n in ("un", "vn", "wn", "pn")}
-    # one more step with per-kernel events, for the FP64 sweep's roofline
-    _, r_ms, _, _, p_tim = _timed_steps(sp, stream_p, 1, pg, timing=True)
-    roof64 = _roofline(p_tim, "sor_sweep", 32.0, cells, r_ms,
-                       traffic_key=_sor64_traffic_key(sp.last_solve_stats().variant))
-    roof64["sor_kernel"] = SOR_NAMES.get(sp.last_solve_stats().variant, "?")
+    # one more step with the sweep runs timed, for the FP64 sweep's roofline
+    _, r_ms, _, _, p_tim = _timed_steps(sp, stream_p, 1, pg, timing=2)
+    var64 = sp.last_solve_stats().variant
+    roof64 = _roofline(p_tim, "sor_run", _sor_alg_per_launch(var64), cells, r_ms,
+                       traffic_key=_sor64_traffic_key(var64))
+    roof64["sor_kernel"] = SOR_NAMES.get(var64, "?")
+    plain_step_hbm = _step_hbm(cells, p_ms_all / K, p_iters / K, 64.0)
     plain_c1 = None
     if not args.quick:   # the plain FP64 step at the C1 tolerance 1e-10
         sp.init_pressure_solver(M.make_solver_opts(M.SOLVER_REDBLACK, sor=cfg["sor"], tol=1e-10,
@@ -930,6 +1032,14 @@ def run_learned_mixed(args, cfg):
     vnum = sum(float(np.sum((s.get(n) - plain_state[n]) ** 2)) for n in ("un", "vn", "wn"))
     vden = sum(float(np.sum(plain_state[n] ** 2)) for n in ("un", "vn", "wn"))
     err["velocity"] = math.sqrt(vnum / vden)
+    # pressure is defined up to a constant (no projection fixes its mean):
+    # the error of p with each field's interior mean removed, and that mean's
+    # difference
+    inner = (slice(1, -1),) * 3
+    pa, pb = plain_state["pn"][inner], s.get("pn")[inner]
+    err["pn_zero_mean"] = float(np.linalg.norm((pb - pb.mean()) - (pa - pa.mean())) /
+                                np.linalg.norm(pa - pa.mean()))
+    err["pn_mean_difference"] = float(pb.mean() - pa.mean())
     ls = s.last_solve_stats()
     l2, linf = s.divergence_norms()
 
@@ -942,11 +1052,13 @@ def run_learned_mixed(args, cfg):
         e2e_line = {"value": ws * cells * K / (ems / 1e3) / 1e6, "unit": UNIT, "h2d_bytes_per_step": nbytes,
                     "d2h_bytes_per_step": nbytes, "same_steps_as_value": e2e_iters == iters}
 
-    # ---- the same steps with per-kernel events, for the roofline ----------------
+    # ---- the same steps with the sweep runs timed, for the roofline ------------
     s.warm_checkpoint(restore=True)
     s.update_device(*[h.numpy() for h in host])
-    _, r_ms, _, _, tim = _timed_steps(s, stream, K, pg, timing=True)
-    roofline = _roofline(tim, "sor_sweep", 16.0, cells, r_ms, traffic_key="sor_sweep32")   # 4 floats per cell per colour sweep
+    _, r_ms, _, _, tim = _timed_steps(s, stream, K, pg, timing=2)
+    # 4 floats per cell per colour sweep
+    roofline = _roofline(tim, "sor_run", _sor_alg_per_launch(1, fp32=True), cells, r_ms, traffic_key="sor_sweep32")
+    step_hbm = _step_hbm(cells, ms_all / K, iters / K, 32.0)
 
     # ---- the same steps without the network: extrapolated increment only ----
     s.warm_checkpoint(restore=True)
@@ -1002,7 +1114,8 @@ def run_learned_mixed(args, cfg):
                            "l2": "inputs larger than L2 (state + IBM coefficients > 126 MB)"},
                 "poisson_iters_per_substage": iters / (3 * K),
                 "plain_fp64": {"value": plain_value, "unit": UNIT, "tol": tol, "ms_per_step": p_ms_all / K,
-                               "poisson_iters_per_substage": p_iters / (3 * K), "roofline": roof64},
+                               "poisson_iters_per_substage": p_iters / (3 * K), "roofline": roof64,
+                               "step_hbm": plain_step_hbm, "first_step": first_step},
                 "plain_fp64_c1_tol": plain_c1,
                 "extrapolated_mixed_no_network": no_net,
                 "relaxation_tuned": tuned,
@@ -1013,7 +1126,7 @@ def run_learned_mixed(args, cfg):
                             "snapshots": net.snapshots, "loss_first": net.loss_first, "loss_last": net.loss_last,
                             "record_s": net.record_seconds, "train_ms": net.train_ms, "setup_wall_s": train_wall,
                             "train_runs": [list(r) for r in TRAIN_RUNS]},
-                "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "e2e": e2e_line,
+                "roofline": roofline, "step_hbm": step_hbm, "cpu_baseline": cpu, "clocks": clk, "e2e": e2e_line,
                 "gpu_launches": launches}
         print(json.dumps(line), flush=True)
     if pg:

@@ -5,8 +5,9 @@
  * The entry points replace the OpenMP-offload bodies of the reference's
  * Fortran modules one for one.  Each declaration names the reference
  * interface it stands in for (paths relative to the mobydiff project root).
- * A Fortran caller binds them with iso_c_binding; the
- * driver, the INI reader, I/O and IBM geometry set-up stay on the host.
+ * A Fortran caller binds them with iso_c_binding (the bind(C) interfaces are
+ * in mobydiff_b200/fortran/mdx_bindings.f90); the driver, the INI reader, I/O
+ * and IBM geometry set-up stay on the host.
  *
  * Conventions
  *   - Every call returns an int status: MDX_OK (0) or one of MDX_ERR_*;
@@ -137,10 +138,13 @@ typedef struct {
                                      predicted from the divergence it leaves           */
 #define MDX_GUESS_EXTRAPOLATED 3  /* 2*dp(n-1) - dp(n-2) of the same RK substage      */
 
-/* Per-kernel-class device time, filled when timing is on (mdx_set_timing). */
+/* Per-kernel-class device time, filled when timing is on (mdx_set_timing).
+ * MDX_T_SOR_BLOCK is not a kernel class: it is the device time of each run of
+ * back-to-back red-black sweep launches between two residual checks, every
+ * run timed, with `launches` the sweep launches inside the timed runs. */
 enum {
     MDX_T_MOMENTUM = 0, MDX_T_BC, MDX_T_FFT_FWD, MDX_T_THOMAS, MDX_T_FFT_INV,
-    MDX_T_CORRECT, MDX_T_SOR_SWEEP, MDX_T_RESIDUAL, MDX_T_OTHER, MDX_T_NUM
+    MDX_T_CORRECT, MDX_T_SOR_SWEEP, MDX_T_RESIDUAL, MDX_T_OTHER, MDX_T_SOR_BLOCK, MDX_T_NUM
 };
 typedef struct {
     double ms[MDX_T_NUM];
@@ -491,10 +495,13 @@ int mdx_channel_ic(mdx_ctx_t* ctx, uint64_t seed, double amp_u, double amp_vw, d
  * (synchronises). */
 int mdx_divergence_norms(mdx_ctx_t* ctx, double* l2, double* linf);
 
-/* Per-kernel-class device timing with CUDA events on the context stream:
- * every 8th launch of a class is bracketed by an event pair; get_timing
- * reports the launches of each class since set_timing(1) and their total
- * time estimated as launches x the sampled mean (synchronises). */
+/* Per-kernel-class device timing with CUDA events on the context stream.
+ * on = 1: every 8th launch of a class is bracketed by an event pair, and
+ * every run of back-to-back sweeps (MDX_T_SOR_BLOCK) as well; on = 2: only
+ * the sweep runs, so that no event sits between two sweeps.  get_timing
+ * reports the launches of each class since set_timing and their total time
+ * estimated as launches x the sampled mean; MDX_T_SOR_BLOCK is the measured
+ * total of the runs (synchronises). */
 int mdx_set_timing(mdx_ctx_t* ctx, int on);
 int mdx_get_timing(mdx_ctx_t* ctx, mdx_timing_t* out);
 
@@ -519,8 +526,11 @@ long long mdx_launch_count(const mdx_ctx_t* ctx);
  * one static device array of 8 MiB per device, which the library holds until
  * the process exits; grids needing more (e.g. above about 64 x 64 x 128) are
  * rejected with MDX_ERR_ARG before any device work.  The array's address is
- * looked up on the first call on each device, so make that first call before
- * any stream capture.  All calls share the array and it keeps the last call's
+ * looked up on the first call on each device (and again on later calls made
+ * outside a stream capture, so that a newly current context gets its own), so
+ * make that first call before any stream capture.  The tables, twiddles and
+ * wavenumbers are built on the device by every call; nothing is copied from
+ * host memory.  All calls share the array and it keeps the last call's
  * contents; calls that overlap on the GPU (different streams or threads) race
  * on it.  Requires even nx; nx/2 and nz must factor into 2, 3, 5, 7. */
 int mdx_solve_pressure_fft_noalloc(const double* rhs, double* phi, int nx, int ny, int nz, double dx, double dy,

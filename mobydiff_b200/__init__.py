@@ -56,7 +56,8 @@ GUESS_EXTRAPOLATED = 3
 FIELDS = ["un", "us", "vn", "vs", "wn", "ws", "pn", "oldrhsu", "oldrhsv", "oldrhsw",
           "coef_u", "coef_v", "coef_w", "phi"]
 FIELD_ID = {n: t for t, n in enumerate(FIELDS)}
-TIMER_CLASSES = ["momentum", "bc", "fft_fwd", "thomas", "fft_inv", "correct", "sor_sweep", "residual", "other"]
+TIMER_CLASSES = ["momentum", "bc", "fft_fwd", "thomas", "fft_inv", "correct", "sor_sweep", "residual", "other",
+                 "sor_run"]
 
 
 class MdxError(RuntimeError):
@@ -113,7 +114,7 @@ class MemberT(C.Structure):
 
 
 class TimingT(C.Structure):
-    _fields_ = [("ms", C.c_double * 9), ("launches", C.c_longlong * 9)]
+    _fields_ = [("ms", C.c_double * 10), ("launches", C.c_longlong * 10)]
 
 
 class RunConfigT(C.Structure):
@@ -521,8 +522,10 @@ class Solver:
         self._c(lib().mdx_divergence_norms(self.h, C.byref(a), C.byref(b)))
         return a.value, b.value
 
-    def set_timing(self, on: bool):
-        self._c(lib().mdx_set_timing(self.h, 1 if on else 0))
+    def set_timing(self, on):
+        """0/False off; 1/True sampled launches of every class plus whole
+        sweep runs; 2 whole sweep runs only (no event between two sweeps)."""
+        self._c(lib().mdx_set_timing(self.h, int(on)))
 
     def get_timing(self) -> dict:
         t = TimingT()

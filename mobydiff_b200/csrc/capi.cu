@@ -55,7 +55,7 @@ static void timing_resolve(mdx_ctx_t* ctx, bool wait) {
         float ms = 0.f;
         if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
             ctx->tim.ms[p.cls] += ms;
-            ctx->tim.launches[p.cls] += 1;
+            ctx->tim.launches[p.cls] += p.n;
         }
         ctx->ev_free.push_back(p.a);
         ctx->ev_free.push_back(p.b);
@@ -71,7 +71,8 @@ static void timing_resolve(mdx_ctx_t* ctx, bool wait) {
 void mdx_timer_begin(mdx_ctx_t* ctx, int cls, mdx_event_pair* p) {
     p->a = p->b = nullptr;
     p->cls = cls;
-    if (!ctx->timing || ctx->capturing) return;
+    p->n = 1;
+    if (ctx->timing != 1 || ctx->capturing) return;
     if ((ctx->tim_issued[cls]++) % MDX_TIMING_STRIDE != 0) return;
     if (ctx->ev_pending.size() >= 4096) timing_resolve(ctx, false);
     if (ctx->ev_pending.size() >= 16384) timing_resolve(ctx, true);
@@ -83,6 +84,25 @@ void mdx_timer_begin(mdx_ctx_t* ctx, int cls, mdx_event_pair* p) {
 void mdx_timer_end(mdx_ctx_t* ctx, mdx_event_pair* p) {
     if (!p->a) return;
     cudaEventRecord(p->b, ctx->stream);
+    ctx->ev_pending.push_back(*p);
+}
+
+void mdx_sweep_run_begin(mdx_ctx_t* ctx, mdx_event_pair* p) {
+    p->a = p->b = nullptr;
+    p->cls = MDX_T_SOR_BLOCK;
+    p->n = ctx->launches;
+    if (!ctx->timing || ctx->capturing) return;
+    if (ctx->ev_pending.size() >= 4096) timing_resolve(ctx, false);
+    if (ctx->ev_pending.size() >= 16384) timing_resolve(ctx, true);
+    p->a = ev_get(ctx);
+    p->b = ev_get(ctx);
+    cudaEventRecord(p->a, ctx->stream);
+}
+
+void mdx_sweep_run_end(mdx_ctx_t* ctx, mdx_event_pair* p) {
+    if (!p->a) return;
+    cudaEventRecord(p->b, ctx->stream);
+    p->n = ctx->launches - p->n;
     ctx->ev_pending.push_back(*p);
 }
 
@@ -704,7 +724,8 @@ int mdx_set_timing(mdx_ctx_t* ctx, int on) {
     timing_resolve(ctx, true);
     std::memset(&ctx->tim, 0, sizeof(ctx->tim));
     std::memset(ctx->tim_issued, 0, sizeof(ctx->tim_issued));
-    ctx->timing = on != 0;
+    if (on < 0 || on > 2) return mdx_fail(ctx, MDX_ERR_ARG, "timing mode %d (0 off, 1 sampled launches, 2 sweep runs)", on);
+    ctx->timing = on;
     return MDX_OK;
 }
 
@@ -713,6 +734,11 @@ int mdx_get_timing(mdx_ctx_t* ctx, mdx_timing_t* out) {
     timing_resolve(ctx, true);
     // scale the sampled launches' mean to every launch of the class
     for (int c = 0; c < MDX_T_NUM; ++c) {
+        if (c == MDX_T_SOR_BLOCK) {   // every run timed: the measured total
+            out->launches[c] = ctx->tim.launches[c];
+            out->ms[c] = ctx->tim.ms[c];
+            continue;
+        }
         const long long timed = ctx->tim.launches[c];
         out->launches[c] = ctx->tim_issued[c];
         out->ms[c] = timed > 0 ? ctx->tim.ms[c] * (double)ctx->tim_issued[c] / (double)timed : 0.0;

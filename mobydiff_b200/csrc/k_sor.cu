@@ -689,7 +689,10 @@ int mdx_k_projection_redblack(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t* st) 
     if (o.tol <= 0.0) {
         const int v = (want == MDX_SORV_AUTO) ? (ctx->sor_tuned > 0 ? ctx->sor_tuned : MDX_SORV_SWEEPS) : want;
         MDX_TRY(layout_for(v));
+        mdx_event_pair run{};
+        mdx_sweep_run_begin(ctx, &run);
         for (int it = 0; it < o.n_iter; ++it) MDX_TRY(sor_iterate(ctx, p, v));
+        mdx_sweep_run_end(ctx, &run);
         MDX_TRY(layout_for(MDX_SORV_SWEEPS));
         s.variant = v;
         s.iterations = o.n_iter;
@@ -715,7 +718,10 @@ int mdx_k_projection_redblack(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t* st) 
                 MDX_TRY(layout_for(v));
                 const bool timing_block = want == MDX_SORV_AUTO && ctx->sor_tuned == 0;
                 if (timing_block) MDX_CUDA(ctx, cudaEventRecord(ctx->tune_ev[0], ctx->stream));
+                mdx_event_pair run{};
+                mdx_sweep_run_begin(ctx, &run);
                 for (int q = 0; q < m; ++q) MDX_TRY(sor_iterate(ctx, p, v));
+                mdx_sweep_run_end(ctx, &run);
                 if (timing_block) MDX_CUDA(ctx, cudaEventRecord(ctx->tune_ev[1], ctx->stream));
                 it += m;
                 s.variant = v;

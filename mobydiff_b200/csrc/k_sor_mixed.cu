@@ -225,12 +225,15 @@ int mdx_k_projection_redblack_mixed(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t
         const int na = d.nx / 2;
         dim3 block(32, 4, 2);
         dim3 grid((na + 31) / 32, (d.ny + 3) / 4, (d.nz + 1) / 2);
+        mdx_event_pair run{};
+        mdx_sweep_run_begin(ctx, &run);
         for (int it = 0; it < iters; ++it)
             for (int parity = 0; parity < 2; ++parity) {
                 auto kfn = py ? k_sor_sweep32<1> : k_sor_sweep32<0>;
                 MDX_LAUNCH(ctx, MDX_T_SOR_SWEEP, "sor sweep fp32", kfn, grid, block, 0, d, P, parity, parity,
                            ctx->mx_du, ctx->mx_dv, ctx->mx_dw, ctx->mx_dp, ctx->mx_r, ctx->mx_mu, ctx->mx_fac);
             }
+        mdx_sweep_run_end(ctx, &run);
         return MDX_OK;
     };
 

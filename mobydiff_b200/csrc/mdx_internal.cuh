@@ -82,7 +82,7 @@ struct mdx_fft_plan {
     int radix[MDX_MAX_STAGES];
 };
 
-struct mdx_event_pair { cudaEvent_t a, b; int cls; };
+struct mdx_event_pair { cudaEvent_t a, b; int cls; long long n; };   // n: launches inside the pair
 
 struct mdx_ctx {
     int device = 0;
@@ -156,8 +156,8 @@ struct mdx_ctx {
     double graph_dt = 0.0;
     long long graph_launches = 0;
 
-    // timing
-    bool timing = false;
+    // timing: 0 off, 1 sampled launches + sweep runs, 2 sweep runs only
+    int timing = 0;
     std::vector<mdx_event_pair> ev_pending;
     std::vector<cudaEvent_t> ev_free;
     mdx_timing_t tim{};                      // sums over the sampled launches
@@ -216,6 +216,11 @@ int mdx_fail(mdx_ctx_t* ctx, int code, const char* fmt, ...);
 // ---- launch bookkeeping ----------------------------------------------------
 void mdx_timer_begin(mdx_ctx_t* ctx, int cls, mdx_event_pair* p);
 void mdx_timer_end(mdx_ctx_t* ctx, mdx_event_pair* p);
+// A run of back-to-back sweep launches between two residual checks, timed
+// whole (MDX_T_SOR_BLOCK) whenever timing is on; `end` counts the launches
+// issued since `begin`.
+void mdx_sweep_run_begin(mdx_ctx_t* ctx, mdx_event_pair* p);
+void mdx_sweep_run_end(mdx_ctx_t* ctx, mdx_event_pair* p);
 int mdx_check_launch(mdx_ctx_t* ctx, const char* what);
 
 // Launch wrapper: times the launch when timing is on and checks the launch.
