@@ -590,6 +590,30 @@ __global__ void __launch_bounds__(256) k_div_field(mdx_dims d, int pery, double 
     }
 }
 
+// Per-block partial sums of a double field (pairs: sum, 0), grid-stride so
+// that the block count, and with it the summation order, is fixed.
+__global__ void __launch_bounds__(256) k_sum_field(long long n, const double* __restrict__ a,
+                                                   double* __restrict__ part) {
+    double s0 = 0.0;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+        s0 += a[t];
+    __shared__ double sh[8];
+    for (int o = 16; o > 0; o >>= 1) s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s0;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int i = 0; i < 8; ++i) s += sh[i];
+        part[2 * blockIdx.x] = s;
+        part[2 * blockIdx.x + 1] = 0.0;
+    }
+}
+
+__global__ void k_add_const(long long n, double* __restrict__ a, double c) {
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+        a[t] += c;
+}
+
 // Sum of n-block pairs -> out[0..1] (one block).
 __global__ void k_sum_pairs(int nb, const double* __restrict__ part, double* __restrict__ out) {
     __shared__ double sh[2][256];
@@ -1142,6 +1166,18 @@ int mdx_unet_correct(mdx_ctx_t* ctx, double dg, double* rg) {
     MDX_TRY(forward(ctx, U));
     MDX_LAUNCH(ctx, MDX_T_OTHER, "unet head", k_head_infer<16>, nblocks(n), 256, 0, n, U->act.back(),
                U->param + U->head_off, U->out_scale * sr * h2 / dg, U->delta);
+    // A constant pressure increment moves no face (the red-black operator's
+    // null space with periodic or Neumann pressure), so the solve never
+    // removes one; a correction with a non-zero mean would shift p by a
+    // constant every projection and p would drift from the plain method's
+    // by a growing constant.  The correction is therefore made zero-mean.
+    {
+        MDX_LAUNCH(ctx, MDX_T_OTHER, "unet delta mean", k_sum_field, U->red_blocks, 256, 0, n, U->delta, U->red_part);
+        double sum = 0.0;
+        MDX_TRY(pairs_to_host(ctx, U, U->red_blocks, &sum, nullptr));
+        MDX_LAUNCH(ctx, MDX_T_OTHER, "unet delta zero mean", k_add_const, nblocks(n), 256, 0, n, U->delta,
+                   -sum / (double)n);
+    }
     MDX_TRY(mdx_apply_guess(ctx, U->delta, dg));
     MDX_CUDA(ctx, cudaEventRecord(U->ev[1], ctx->stream));
     double r = 0.0, linf = 0.0;
