@@ -3,15 +3,60 @@
 ! procedure names and argument lists (src/modules/gpu_runtime.f90,
 ! step.f90, boundary.f90, pressure_solver.f90).  Each body hands the call to
 ! libmobyb200.so through mdx_bindings.  init.f90, config.f90, ibm.f90 (host
-! geometry), io.f90 and field_hdf5.c stay unchanged; io.f90's `!$omp target
-! update` lines become calls to mdx_update_host / mdx_update_device
-! (INTEGRATION.md).  Not compiled in this repository (no Fortran compiler).
+! geometry) and field_hdf5.c stay unchanged; io.f90's `!$omp target update`
+! lines become calls to mdx_update_host / mdx_update_device.  Not compiled in
+! this repository (no Fortran compiler); tests/test_gpu_shim_replay.py replays
+! the call sequence of every body below through the same C entry points.
 
 module mdx_state
     use, intrinsic :: iso_c_binding
     implicit none
     type(C_PTR), save :: ctx = C_NULL_PTR
+    ! host addresses of the IBM coefficient arrays last uploaded, and whether
+    ! they must be sent again (no upload yet, or marked changed)
+    type(C_PTR), save :: ibm_sent(3) = C_NULL_PTR
+    logical, save :: ibm_stale = .true.
 end module mdx_state
+
+! The reference computes the IBM coefficients on the host (set_ibm_coeff,
+! main.f90:57-60) and maps them with enter_ibm_data (ibm.f90:57-68), which
+! stays unchanged and holds only OpenMP directives.  The shim therefore sends
+! ibm%coef_u/v/w to the device itself: before the first predictor or
+! projection, again when the arrays are reallocated (new addresses), and
+! again after ibm_coefficients_changed() -- the call for a program that
+! rewrites the coefficients in place (main.f90 never does).
+module mdx_ibm_sync
+    use, intrinsic :: iso_c_binding
+    use :: ibmm, only: ibm_type
+    use :: mdx_bindings
+    use :: mdx_state
+    implicit none
+    private
+    public :: sync_ibm, ibm_coefficients_changed
+contains
+    subroutine sync_ibm(ibm)
+        type(ibm_type), intent(in), target :: ibm
+        type(C_PTR) :: p(3)
+        if (.not. (allocated(ibm%coef_u) .and. allocated(ibm%coef_v) .and. allocated(ibm%coef_w))) then
+            print *, "ERROR: IBM coefficients not allocated (init_ibm and set_ibm_coeff come first)."
+            error stop 1
+        end if
+        p(1) = c_loc(ibm%coef_u)
+        p(2) = c_loc(ibm%coef_v)
+        p(3) = c_loc(ibm%coef_w)
+        if (.not. ibm_stale) then
+            if (c_associated(p(1), ibm_sent(1)) .and. c_associated(p(2), ibm_sent(2)) .and. &
+                c_associated(p(3), ibm_sent(3))) return
+        end if
+        call mdx_check(mdx_enter_ibm_data(ctx, p(1), p(2), p(3)), ctx, "enter_ibm_data")
+        ibm_sent = p
+        ibm_stale = .false.
+    end subroutine sync_ibm
+
+    subroutine ibm_coefficients_changed()
+        ibm_stale = .true.
+    end subroutine ibm_coefficients_changed
+end module mdx_ibm_sync
 
 module gpu_runtime
     use, intrinsic :: iso_c_binding
@@ -22,9 +67,10 @@ module gpu_runtime
 contains
     subroutine init_openmp_offload()
         integer(C_INT) :: n, rc
+        n = 0
         rc = mdx_device_count(n)
-        if (n <= 0) then
-            print *, "ERROR: no CUDA device available for mobydiff_b200."
+        if (rc /= MDX_OK .or. n <= 0) then
+            print *, "ERROR: no CUDA device available for mobydiff_b200 (mdx_device_count status", rc, ")."
             error stop 1
         end if
         print *, "CUDA devices available:", n
@@ -53,6 +99,8 @@ contains
         call mdx_check(mdx_exit_field_data(ctx), ctx, "exit_field_data")
         call mdx_check(mdx_destroy(ctx), ctx, "mdx_destroy")
         ctx = C_NULL_PTR
+        ibm_sent = C_NULL_PTR
+        ibm_stale = .true.
     end subroutine exit_field_data
 end module gpu_runtime
 
@@ -118,6 +166,7 @@ module step
     use :: init, only: grid_type, field_type
     use :: ibmm, only: ibm_type
     use :: boundary, only: boundary_type, sync_bc
+    use :: mdx_ibm_sync, only: sync_ibm
     use :: mdx_bindings
     use :: mdx_state
     implicit none
@@ -129,9 +178,10 @@ contains
         type(field_type), intent(inout) :: f
         type(grid_type),  intent(in)    :: g
         real(C_DOUBLE),   intent(in)    :: dt_alpha, dt_beta, dt_gamma
-        type(ibm_type),   intent(in)    :: ibm
+        type(ibm_type),   intent(in), target :: ibm
         type(boundary_type), intent(in) :: bc
         call sync_bc(bc)
+        call sync_ibm(ibm)
         call mdx_check(mdx_momentum(ctx, dt_alpha, dt_beta, dt_gamma), ctx, "momentum")
     end subroutine momentum
 
@@ -148,6 +198,7 @@ module pressure_solver
     use :: pressure_workspace, only: pressure_solver_type
     use :: ibmm, only: ibm_type
     use :: boundary, only: boundary_type, sync_bc
+    use :: mdx_ibm_sync, only: sync_ibm
     use :: mdx_bindings
     use :: mdx_state
     implicit none
@@ -174,9 +225,10 @@ contains
         type(field_type), intent(inout) :: f
         type(grid_type), intent(in) :: g
         real(C_DOUBLE), intent(in) :: dt_gamma
-        type(ibm_type), intent(in) :: ibm
+        type(ibm_type), intent(in), target :: ibm
         type(boundary_type), intent(in) :: bc
         call sync_bc(bc)
+        call sync_ibm(ibm)
         call mdx_check(mdx_pressure_projection(ctx, dt_gamma, C_NULL_PTR), ctx, "pressure_projection")
     end subroutine pressure_projection
 
