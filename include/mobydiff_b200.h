@@ -97,7 +97,12 @@ typedef struct {
                           launch per colour; 2 fused red+black pass, 32x8 tiles;
                           3 fused pass, 32x16 tiles; 4 one launch per colour on
                           colour-split copies of u, v, w, p made once per projection
-                          (2-4: periodic x and z, IBM factors 1 or z-invariant) */
+                          (2-4: periodic x and z, IBM factors 1 or z-invariant).
+                          FP32 sweeps of the mixed precision: 1 one launch per colour;
+                          2 or 3 the fused red+black pass (one launch per iteration) in
+                          the fastest of four tile shapes; 0 or 4 the fastest of all five,
+                          each timed on one block of the first iterations (all give the
+                          same bits) */
     int sor_kz;        /* z planes per block of the fused pass (0: default 16) */
     int check_mode;    /* red-black, tol > 0: 0 (default) residual checks at multiples of check_every,
                           up to 8 blocks apart while the residual falls at a steady rate that

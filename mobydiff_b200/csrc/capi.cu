@@ -318,6 +318,8 @@ int mdx_set_bc(mdx_ctx_t* ctx, const mdx_bc_t* bc) {
     for (int t = 0; t < 24; ++t) { ctx->bcd.type[t] = bc->bc_type[t]; ctx->bcd.value[t] = bc->bc_value[t]; }
     ctx->sor_tuned = 0;
     for (int t = 0; t < 8; ++t) ctx->sor_tune_ms[t] = 0.0;
+    ctx->rb32_tuned = 0;
+    for (int t = 0; t < 8; ++t) ctx->rb32_tune_ms[t] = 0.0;
     return MDX_OK;
 }
 
@@ -523,6 +525,8 @@ int mdx_init_pressure_solver(mdx_ctx_t* ctx, const mdx_solver_opts_t* opts) {
     ctx->opts = o;
     ctx->sor_tuned = 0;
     for (int t = 0; t < 8; ++t) ctx->sor_tune_ms[t] = 0.0;
+    ctx->rb32_tuned = 0;
+    for (int t = 0; t < 8; ++t) ctx->rb32_tune_ms[t] = 0.0;
     MDX_TRY(mdx_reduce_init(ctx));
     if (o.solver == MDX_SOLVER_REDBLACK) {
         // src/modules/pressure/pressure_redblack.f90:16-18

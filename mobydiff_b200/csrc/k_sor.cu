@@ -489,10 +489,7 @@ static int sor_iteration(mdx_ctx_t* ctx, const mdx_sor_params& p) {
 //                      (tol > 0 only: the copies cost two passes over u, v,
 //                      w, p per projection)
 // All but the first need periodic x and z and mu = 1 or z-invariant.
-enum {
-    MDX_SORV_AUTO = 0, MDX_SORV_SWEEPS = 1, MDX_SORV_FUSED8 = 2, MDX_SORV_FUSED16 = 3, MDX_SORV_SPLIT = 4,
-    MDX_SORV_NUM = 5
-};
+// (the enum is in mdx_internal.cuh)
 
 static int split_alloc(mdx_ctx_t* ctx) {
     const size_t bytes = sizeof(double) * (size_t)split_elems(ctx->d);

@@ -126,6 +126,261 @@ k_sor_sweep32(mdx_dims d, mixed_params P, int parity, int reverse, float* __rest
     sweep32_cell<PY>(d, P, i, j, k, du, dv, dw, dp, r, mu32, fac32);
 }
 
+// ---------------------------------------------------------------------------
+// Fused red+black pass: one launch per red-black iteration of the FP32
+// correction sweeps, with the result of the two colour sweeps bit for bit.
+//
+// A CTA owns TI x TJ columns (x, y) of cells over a chunk of TK z planes and
+// marches the chunk plane by plane.  Each thread holds a pair of x-adjacent
+// cells (even, odd) of one row, so in every plane one of its cells is red
+// (first colour: i + j + k odd) and the other black, and the cell that is red
+// in plane q is black in plane q - 1.  Step q:
+//   A  publish this plane's pre-sweep face u(even) in shared memory; barrier;
+//   B  red cell of plane q: phi_R from pre-sweep faces;
+//   C  black cell of plane q - 1: its faces after the red sweep (pre-sweep
+//      value plus the red neighbour's contribution), then phi_B; barrier;
+//   D  plane q - 1's own faces and dp: the red contribution, then the black
+//      one, in the two sweeps' order.
+// Plane data arrive by cp.async three planes ahead into a five-plane ring.
+// Halo columns (2 on the low side, 1 on the high side, in x and y) and halo
+// planes recompute red and black cells of the neighbouring tiles.  Faces are
+// read from x* (the pre-sweep state, never written here, so that halo reads
+// never see a neighbour's results) and written to y*; dp is only read and
+// written by its own CTA, in place.  Wall faces v(1), v(ny+1) (y not
+// periodic) are never written; the caller keeps them 0 in both buffers.
+// tests/rb32_model.py restates this kernel step by step.
+// ---------------------------------------------------------------------------
+template <int TI, int TJ>
+struct rb32_geom {
+    static constexpr int PW = TI / 2 + 2;   // pair columns (x halo 2 low, 1 high, rounded to pairs)
+    static constexpr int RW = TJ + 3;       // rows (y halo 2 low, 1 high)
+    static constexpr int CW = 2 * PW;
+    static constexpr int NT = PW * RW;
+    // plane data staged by cp.async: SLOTS planes, FIELDS values per thread
+    // (u, v, v(j+1), r, dp and w(q+1) of both cells), field-major so that a
+    // warp's accesses to one field are consecutive words
+    static constexpr int SLOTS = 5, FIELDS = 12;
+    static constexpr int slot_floats = FIELDS * NT;
+};
+enum { RB_U0 = 0, RB_U1, RB_V0, RB_V1, RB_VN0, RB_VN1, RB_R0, RB_R1, RB_DP0, RB_DP1, RB_W0, RB_W1 };
+
+__device__ __forceinline__ int rb32_cx(int i, int nx) {   // unwrapped x cell -> 1..nx (0 <-> nx)
+    int m = i % nx;
+    if (m < 0) m += nx;
+    return m == 0 ? nx : m;
+}
+__device__ __forceinline__ int rb32_c1(int k, int n) {    // unwrapped 1-based -> 1..n
+    int m = (k - 1) % n;
+    if (m < 0) m += n;
+    return m + 1;
+}
+// 4-byte cp.async; with on == false the word is zero-filled and nothing is read
+__device__ __forceinline__ void rb32_cp4(unsigned dst, const float* src, bool on) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(dst), "l"(src), "r"(on ? 4 : 0) : "memory");
+}
+
+template <int PY, int TI, int TJ, int TK>
+__global__ void __launch_bounds__(rb32_geom<TI, TJ>::NT)
+k_rb32_fused(mdx_dims d, mixed_params P, const float* __restrict__ xu, const float* __restrict__ xv,
+             const float* __restrict__ xw, float* __restrict__ yu, float* __restrict__ yv, float* __restrict__ yw,
+             float* __restrict__ dp, const float* __restrict__ r, const float* __restrict__ mu32,
+             const float* __restrict__ fac32) {
+    using G = rb32_geom<TI, TJ>;
+    constexpr int S = G::SLOTS, NT = G::NT, SF = G::slot_floats;
+    extern __shared__ __align__(16) float rb32_ring[];   // [SLOTS][FIELDS][NT]
+    __shared__ float U_s[2][G::RW][G::PW + 1];   // pre-sweep u(even cell), plane ring
+    __shared__ float PH[2][G::RW][G::CW + 2];    // phi of both colours, plane ring; column 2 tx + c + 1
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * G::PW + tx;
+    const int nx = d.nx, ny = d.ny, nz = d.nz;
+    const int i0 = blockIdx.x * TI, j0 = 1 + blockIdx.y * TJ, k0 = 1 + blockIdx.z * TK;
+    const int ie = i0 - 2 + 2 * tx;               // unwrapped even cell of the pair
+    const int j = j0 - 2 + ty;
+    const bool ex = PY || (j >= 1 && j <= ny);    // the row's cells exist
+    const bool ex_dn = PY || j - 1 >= 1, ex_up = PY || j + 1 <= ny;
+    const bool own_row = ex && ty >= 2 && ty < TJ + 2 && j <= ny;
+    const int jc = PY ? rb32_c1(j, ny) : (ex ? j : 1);    // rows that load nothing point at row 1
+    const int jn = PY ? rb32_c1(j + 1, ny) : (ex ? j + 1 : 1);
+    const int ic0 = rb32_cx(ie, nx), ic1 = rb32_cx(ie + 1, nx), ic2 = rb32_cx(ie + 2, nx);
+    // 32-bit colour-split offsets: cell (ic, row, kc) at half (ic+row+kc)&1
+    const int H = d.hs * d.nyp * d.nzp, PL = d.nyp * d.hs;
+    const int b0 = jc * d.hs + (ic0 >> 1), b1 = jc * d.hs + (ic1 >> 1);
+    const int bn0 = jn * d.hs + (ic0 >> 1), bn1 = jn * d.hs + (ic1 >> 1);
+    const int par0 = (ic0 + jc) & 1, par1 = (ic1 + jc) & 1, parn0 = (ic0 + jn) & 1, parn1 = (ic1 + jn) & 1;
+    const int np = split_plane_elems(d);
+    const unsigned ring0 = (unsigned)__cvta_generic_to_shared(rb32_ring) + 4u * tid;
+    const float* rt = rb32_ring + tid;
+
+    // per-column factors (z-invariant)
+    float fac[2] = {0.f, 0.f}, mu_u[3] = {0.f, 0.f, 0.f}, mu_v[2] = {0.f, 0.f}, mu_vn[2] = {0.f, 0.f},
+          mu_w[2] = {0.f, 0.f};
+    if (ex) {
+        const int q0 = pidx2(d, ic0, jc), q1 = pidx2(d, ic1, jc);
+        fac[0] = __ldg(fac32 + q0);
+        fac[1] = __ldg(fac32 + q1);
+        mu_u[0] = __ldg(mu32 + q0);
+        mu_u[1] = __ldg(mu32 + q1);
+        mu_u[2] = __ldg(mu32 + pidx2(d, ic2, jc));
+        mu_v[0] = __ldg(mu32 + np + q0);
+        mu_v[1] = __ldg(mu32 + np + q1);
+        mu_w[0] = __ldg(mu32 + 2 * np + q0);
+        mu_w[1] = __ldg(mu32 + 2 * np + q1);
+        mu_vn[0] = __ldg(mu32 + np + pidx2(d, ic0, jn));
+        mu_vn[1] = __ldg(mu32 + np + pidx2(d, ic1, jn));
+    }
+    // stage plane kc (its slot at byte offset sb): u, v, v(j+1), r, dp of both
+    // cells and w of plane kn = kc + 1 (periodic)
+    auto issue = [&](unsigned sb, int kc, int kn) {
+        const int hc = (kc & 1) ? H : 0, hn = (kn & 1) ? H : 0, hh = H - hc;   // hh: the other half at kc
+        const int a0 = b0 + kc * PL + (par0 ? hh : hc), a1 = b1 + kc * PL + (par1 ? hh : hc);
+        const int an0 = bn0 + kc * PL + (parn0 ? hh : hc), an1 = bn1 + kc * PL + (parn1 ? hh : hc);
+        const int w0 = b0 + kn * PL + (par0 ? H - hn : hn), w1 = b1 + kn * PL + (par1 ? H - hn : hn);
+        const bool vn_on = ex;   // v(j+1): the top wall face for j = ny (0 in the array)
+        rb32_cp4(sb + 4u * (RB_U0 * NT), xu + a0, ex);
+        rb32_cp4(sb + 4u * (RB_U1 * NT), xu + a1, ex);
+        rb32_cp4(sb + 4u * (RB_V0 * NT), xv + a0, ex);
+        rb32_cp4(sb + 4u * (RB_V1 * NT), xv + a1, ex);
+        rb32_cp4(sb + 4u * (RB_VN0 * NT), xv + an0, vn_on);
+        rb32_cp4(sb + 4u * (RB_VN1 * NT), xv + an1, vn_on);
+        rb32_cp4(sb + 4u * (RB_R0 * NT), r + a0, ex);
+        rb32_cp4(sb + 4u * (RB_R1 * NT), r + a1, ex);
+        rb32_cp4(sb + 4u * (RB_DP0 * NT), dp + a0, own_row);
+        rb32_cp4(sb + 4u * (RB_DP1 * NT), dp + a1, own_row);
+        rb32_cp4(sb + 4u * (RB_W0 * NT), xw + w0, ex);
+        rb32_cp4(sb + 4u * (RB_W1 * NT), xw + w1, ex);
+    };
+    auto knext = [&](int k) { return k == nz ? 1 : k + 1; };
+
+    float w[2] = {0.f, 0.f}, wp[2] = {0.f, 0.f};            // w(q), w(q-1)
+    float ph[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};     // phi per column at planes q, q-1, q-2
+    int kq = rb32_c1(k0 - 2, nz);                            // plane q
+    if (ex) {
+        const int hc = (kq & 1) ? H : 0;
+        w[0] = __ldg(xw + b0 + kq * PL + (par0 ? H - hc : hc));
+        w[1] = __ldg(xw + b1 + kq * PL + (par1 ? H - hc : hc));
+    }
+    // slots: plane q in slot sq; the prologue stages planes k0-2 .. k0
+    int sq = 0;
+    {
+        int k = kq;
+        for (int t = 0; t < 3; ++t) {
+            issue(ring0 + 4u * (t * SF), k, knext(k));
+            asm volatile("cp.async.commit_group;\n" ::);
+            k = knext(k);
+        }
+    }
+    int k_issue = knext(knext(knext(kq)));                  // plane q + 3
+    int kd = kq == 1 ? nz : kq - 1;                          // plane q - 1
+    const float idx = P.idx, idy = P.idy, idz = P.idz;
+    for (int q = k0 - 2; q <= k0 + TK; ++q) {
+        const int h = q & 1, hp = (q - 1) & 1;
+        const int sp = sq == 0 ? S - 1 : sq - 1;             // slot of plane q - 1
+        const int si = sq + 3 >= S ? sq + 3 - S : sq + 3;    // slot of plane q + 3 (plane q - 2's)
+        const float* cs = rt + sq * SF;
+        const float* ps = rt + sp * SF;
+        // stage plane q + 3; plane q is then complete
+        if (q + 3 <= k0 + TK) issue(ring0 + 4u * (si * SF), k_issue, knext(k_issue));
+        asm volatile("cp.async.commit_group;\n" ::);
+        asm volatile("cp.async.wait_group 3;\n" ::: "memory");
+        // A
+        U_s[h][ty][tx] = cs[RB_U0 * NT];
+        __syncthreads();
+        const int c = ((j + q) & 1) ? 0 : 1;   // the red cell of plane q (the black cell of plane q - 1)
+        // the column-c values by selection (register arrays are indexed by constants only)
+        const bool c1 = c == 1;
+        const float fac_c = c1 ? fac[1] : fac[0], mu_w_c = c1 ? mu_w[1] : mu_w[0];
+        const float w_c = c1 ? w[1] : w[0], wp_c = c1 ? wp[1] : wp[0];
+        // B: red cell of plane q
+        if (ex && 2 * tx + c <= TI + 2 && ty <= TJ + 2) {
+            const float ui = cs[(RB_U0 + c) * NT];
+            const float uip = c1 ? U_s[h][ty][tx + 1] : cs[RB_U1 * NT];
+            const float vj = cs[(RB_V0 + c) * NT], vjp = cs[(RB_VN0 + c) * NT];
+            const float phi = __fmul_rn(sweep32_div(P, cs[(RB_R0 + c) * NT], ui, uip, vj, vjp, w_c, cs[(RB_W0 + c) * NT]),
+                                        fac_c);
+            if (c1) ph[1][0] = phi;
+            else ph[0][0] = phi;
+            PH[h][ty][2 * tx + c + 1] = phi;
+        }
+        // C reads no value B writes (its neighbours' plane q - 1 values date
+        // from the last step; the red phi of plane q is its own), so no
+        // barrier between them
+        // C: black cell of plane q - 1, faces after the red sweep
+        if (q >= k0 && ex && 2 * tx + c >= 1 && 2 * tx + c <= TI + 1 && ty >= 1 && ty <= TJ + 1) {
+            const float p_left = c1 ? ph[0][1] : PH[hp][ty][2 * tx];
+            const float p_right = c1 ? PH[hp][ty][2 * tx + 3] : ph[1][1];
+            const float mu_ui = c1 ? mu_u[1] : mu_u[0], mu_uip = c1 ? mu_u[2] : mu_u[1];
+            const float up_i = ps[(RB_U0 + c) * NT];
+            const float up_ip = c1 ? U_s[hp][ty][tx + 1] : ps[RB_U1 * NT];
+            const float ui = __fmaf_rn(__fmul_rn(p_left, idx), mu_ui, up_i);
+            const float uip = __fmaf_rn(-__fmul_rn(p_right, idx), mu_uip, up_ip);
+            float vj = ps[(RB_V0 + c) * NT];
+            if (ex_dn) vj = __fmaf_rn(__fmul_rn(PH[hp][ty - 1][2 * tx + c + 1], idy), c1 ? mu_v[1] : mu_v[0], vj);
+            float vjp = ps[(RB_VN0 + c) * NT];
+            if (ex_up) vjp = __fmaf_rn(-__fmul_rn(PH[hp][ty + 1][2 * tx + c + 1], idy), c1 ? mu_vn[1] : mu_vn[0], vjp);
+            const float ph2 = c1 ? ph[1][2] : ph[0][2], ph0 = c1 ? ph[1][0] : ph[0][0];
+            const float wk = __fmaf_rn(__fmul_rn(ph2, idz), mu_w_c, wp_c);
+            const float wkp = __fmaf_rn(-__fmul_rn(ph0, idz), mu_w_c, w_c);
+            const float phi = __fmul_rn(sweep32_div(P, ps[(RB_R0 + c) * NT], ui, uip, vj, vjp, wk, wkp), fac_c);
+            if (c1) ph[1][1] = phi;
+            else ph[0][1] = phi;
+            PH[hp][ty][2 * tx + c + 1] = phi;
+        }
+        __syncthreads();
+        // D: own faces and dp of plane q - 1
+        if (q >= k0 + 1 && q - 1 < k0 + TK && q - 1 <= nz && own_row) {
+            const int hd = (kd & 1) ? H : 0;
+#pragma unroll
+            for (int cc = 0; cc < 2; ++cc) {
+                const int pos = 2 * tx + cc;
+                if (pos < 2 || pos >= TI + 2 || ie + cc >= nx) continue;
+                const bool red = ((cc + j + q - 1) & 1) == 1;
+                const float phi = ph[cc][1];
+                const float px = __fmul_rn(phi, idx), py = __fmul_rn(phi, idy), pz = __fmul_rn(phi, idz);
+                const float pxl = __fmul_rn(cc == 1 ? ph[0][1] : PH[hp][ty][2 * tx], idx);
+                const float mu = mu_u[cc];
+                const float u0 = ps[(RB_U0 + cc) * NT];
+                const float u2 = red ? __fmaf_rn(pxl, mu, __fmaf_rn(-px, mu, u0)) : __fmaf_rn(-px, mu, __fmaf_rn(pxl, mu, u0));
+                const bool v_lo = PY || j > 1;
+                const float pyd = ex_dn ? __fmul_rn(PH[hp][ty - 1][2 * tx + cc + 1], idy) : 0.f;
+                const float mv = mu_v[cc];
+                float v1 = ps[(RB_V0 + cc) * NT];
+                if (red) {
+                    if (v_lo) v1 = __fmaf_rn(-py, mv, v1);
+                    if (ex_dn) v1 = __fmaf_rn(pyd, mv, v1);
+                } else {
+                    if (ex_dn) v1 = __fmaf_rn(pyd, mv, v1);
+                    if (v_lo) v1 = __fmaf_rn(-py, mv, v1);
+                }
+                const float pzb = __fmul_rn(ph[cc][2], idz);
+                const float mw = mu_w[cc];
+                const float w2 = red ? __fmaf_rn(pzb, mw, __fmaf_rn(-pz, mw, wp[cc]))
+                                     : __fmaf_rn(-pz, mw, __fmaf_rn(pzb, mw, wp[cc]));
+                const int par = cc == 0 ? par0 : par1;
+                const int a = (cc == 0 ? b0 : b1) + kd * PL + (par ? H - hd : hd);
+                yu[a] = u2;
+                yv[a] = v1;
+                yw[a] = w2;
+                dp[a] = __fmaf_rn(phi, P.idt, ps[(RB_DP0 + cc) * NT]);
+            }
+        }
+        // the next plane
+        wp[0] = w[0];
+        wp[1] = w[1];
+        w[0] = cs[RB_W0 * NT];
+        w[1] = cs[RB_W1 * NT];
+#pragma unroll
+        for (int cc = 0; cc < 2; ++cc) {
+            ph[cc][2] = ph[cc][1];
+            ph[cc][1] = ph[cc][0];
+            ph[cc][0] = 0.f;
+        }
+        sq = sq + 1 == S ? 0 : sq + 1;
+        kd = kq;
+        kq = knext(kq);
+        k_issue = knext(k_issue);
+    }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
 // u += du, v += dv, w += dw, p += dp over the padded arrays; corrections reset.
 __global__ void k_mixed_apply(mdx_dims d, double* __restrict__ u, double* __restrict__ v, double* __restrict__ w,
                               double* __restrict__ p, float* __restrict__ du, float* __restrict__ dv,
@@ -145,22 +400,58 @@ bool mixed_supported(const mdx_ctx_t* ctx) {
            T[bci(2, 0, 0)] == 1 && V[bci(2, 0, 0)] == 0.0 && T[bci(2, 1, 0)] == 1 && V[bci(2, 1, 0)] == 0.0;
 }
 
-// One allocation for the five colour-split FP32 arrays and the tables, each
-// part starting on a 256-byte boundary.
+// One allocation for the eight colour-split FP32 arrays (du, dv, dw, dp, r
+// and the fused pass's second du, dv, dw) and the tables, each part starting
+// on a 256-byte boundary, all zero (the wall faces v(1), v(ny+1) stay 0 in
+// both face buffers).
 int mixed_alloc(mdx_ctx_t* ctx) {
-    if (ctx->mx_du) return MDX_OK;
+    if (ctx->mx_base) return MDX_OK;
     const size_t n = (size_t)split_elems(ctx->d), np = (size_t)split_plane_elems(ctx->d);
     auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
     const size_t arr = up(sizeof(float) * n), mu = up(sizeof(float) * 3 * np), fac = up(sizeof(float) * np);
-    const size_t total = 5 * arr + mu + fac;
+    const size_t total = 8 * arr + mu + fac;
     char* base = nullptr;
     MDX_CUDA(ctx, cudaMalloc(&base, total));
     MDX_CUDA(ctx, cudaMemsetAsync(base, 0, total, ctx->stream));
-    float** arrs[5] = {&ctx->mx_du, &ctx->mx_dv, &ctx->mx_dw, &ctx->mx_dp, &ctx->mx_r};
-    for (int a = 0; a < 5; ++a) *arrs[a] = reinterpret_cast<float*>(base + a * arr);
-    ctx->mx_mu = reinterpret_cast<float*>(base + 5 * arr);
-    ctx->mx_fac = reinterpret_cast<float*>(base + 5 * arr + mu);
+    float** arrs[8] = {&ctx->mx_du, &ctx->mx_dv, &ctx->mx_dw, &ctx->mx_dp, &ctx->mx_r,
+                       &ctx->mx_du2, &ctx->mx_dv2, &ctx->mx_dw2};
+    for (int a = 0; a < 8; ++a) *arrs[a] = reinterpret_cast<float*>(base + a * arr);
+    ctx->mx_mu = reinterpret_cast<float*>(base + 8 * arr);
+    ctx->mx_fac = reinterpret_cast<float*>(base + 8 * arr + mu);
+    ctx->mx_base = base;
     ctx->mx_bytes = total;
+    return MDX_OK;
+}
+
+// Tile shapes (TI x TJ columns, TK planes) of the fused pass, tried by the
+// autotuner in this order; all give the same bits.
+#define RB32_SHAPES 4
+template <int PY>
+static int rb32_launch(mdx_ctx_t* ctx, int shape, const mixed_params& P) {
+    const mdx_dims& d = ctx->d;
+    auto go = [&](auto kfn, int TI, int TJ, int TK) -> int {
+        const int NT = (TI / 2 + 2) * (TJ + 3);
+        const size_t smem = sizeof(float) * 5 * 12 * NT;   // SLOTS x FIELDS x threads
+        const unsigned bit = 1u << (shape + 4 * PY);
+        if (!(ctx->rb32_attr & bit)) {
+            MDX_CUDA(ctx, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            ctx->rb32_attr |= bit;
+        }
+        dim3 block(TI / 2 + 2, TJ + 3);
+        dim3 grid((d.nx + TI - 1) / TI, (d.ny + TJ - 1) / TJ, (d.nz + TK - 1) / TK);
+        MDX_LAUNCH(ctx, MDX_T_SOR_SWEEP, "sor rb32 fused", kfn, grid, block, smem, d, P, ctx->mx_du, ctx->mx_dv,
+                   ctx->mx_dw, ctx->mx_du2, ctx->mx_dv2, ctx->mx_dw2, ctx->mx_dp, ctx->mx_r, ctx->mx_mu, ctx->mx_fac);
+        return MDX_OK;
+    };
+    switch (shape) {
+        case 0: MDX_TRY(go(k_rb32_fused<PY, 64, 8, 16>, 64, 8, 16)); break;
+        case 1: MDX_TRY(go(k_rb32_fused<PY, 64, 16, 16>, 64, 16, 16)); break;
+        case 2: MDX_TRY(go(k_rb32_fused<PY, 32, 8, 16>, 32, 8, 16)); break;
+        default: MDX_TRY(go(k_rb32_fused<PY, 64, 8, 32>, 64, 8, 32)); break;
+    }
+    std::swap(ctx->mx_du, ctx->mx_du2);
+    std::swap(ctx->mx_dv, ctx->mx_dv2);
+    std::swap(ctx->mx_dw, ctx->mx_dw2);
     return MDX_OK;
 }
 
@@ -168,9 +459,11 @@ int mixed_alloc(mdx_ctx_t* ctx) {
 }  // namespace
 
 void mdx_mixed_free(mdx_ctx_t* ctx) {
-    cudaFree(ctx->mx_du);   // the base of the one allocation
-    float** arrs[7] = {&ctx->mx_du, &ctx->mx_dv, &ctx->mx_dw, &ctx->mx_dp, &ctx->mx_r, &ctx->mx_mu, &ctx->mx_fac};
+    if (ctx->mx_base) cudaFree(ctx->mx_base);
+    float** arrs[10] = {&ctx->mx_du, &ctx->mx_dv, &ctx->mx_dw, &ctx->mx_dp, &ctx->mx_r, &ctx->mx_mu, &ctx->mx_fac,
+                        &ctx->mx_du2, &ctx->mx_dv2, &ctx->mx_dw2};
     for (auto a : arrs) *a = nullptr;
+    ctx->mx_base = nullptr;
     ctx->mx_bytes = 0;
 }
 
@@ -221,19 +514,65 @@ int mdx_k_projection_redblack_mixed(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t
         *l2 = std::sqrt(s2);
         return MDX_OK;
     };
-    auto sweeps = [&](int iters) -> int {
+    // Inner sweeps: the colour sweeps (one launch per colour) when asked
+    // for; otherwise the autotuner's choice among the fused red+black pass's
+    // tile shapes and the colour sweeps, each timed on one block of
+    // iterations of the first projections (all give the same bits).
+    const bool tune_all = o.sor_variant != MDX_SORV_SWEEPS;
+    const bool fused_only = o.sor_variant == MDX_SORV_FUSED8 || o.sor_variant == MDX_SORV_FUSED16;
+    const int ncand = fused_only ? RB32_SHAPES : RB32_SHAPES + 1;
+    if (tune_all && !ctx->tune_ev[0]) {
+        MDX_CUDA(ctx, cudaEventCreate(&ctx->tune_ev[0]));
+        MDX_CUDA(ctx, cudaEventCreate(&ctx->tune_ev[1]));
+    }
+    bool used_fused = false;
+    auto colour_sweeps = [&](int iters) -> int {
         const int na = d.nx / 2;
         dim3 block(32, 4, 2);
         dim3 grid((na + 31) / 32, (d.ny + 3) / 4, (d.nz + 1) / 2);
-        mdx_event_pair run{};
-        mdx_sweep_run_begin(ctx, &run);
         for (int it = 0; it < iters; ++it)
             for (int parity = 0; parity < 2; ++parity) {
                 auto kfn = py ? k_sor_sweep32<1> : k_sor_sweep32<0>;
                 MDX_LAUNCH(ctx, MDX_T_SOR_SWEEP, "sor sweep fp32", kfn, grid, block, 0, d, P, parity, parity,
                            ctx->mx_du, ctx->mx_dv, ctx->mx_dw, ctx->mx_dp, ctx->mx_r, ctx->mx_mu, ctx->mx_fac);
             }
+        return MDX_OK;
+    };
+    auto sweeps = [&](int iters) -> int {
+        mdx_event_pair run{};
+        int cand = RB32_SHAPES;   // the colour sweeps
+        bool tuning = false;
+        if (tune_all) {
+            cand = ctx->rb32_tuned - 1;
+            tuning = cand < 0;
+            if (tuning) {
+                cand = 0;
+                while (cand < ncand - 1 && ctx->rb32_tune_ms[cand] > 0.0) ++cand;
+                MDX_CUDA(ctx, cudaEventRecord(ctx->tune_ev[0], ctx->stream));
+            }
+        }
+        mdx_sweep_run_begin(ctx, &run);
+        if (cand < RB32_SHAPES) {
+            for (int it = 0; it < iters; ++it) MDX_TRY(py ? rb32_launch<1>(ctx, cand, P) : rb32_launch<0>(ctx, cand, P));
+            used_fused = true;
+        } else {
+            MDX_TRY(colour_sweeps(iters));
+            used_fused = false;
+        }
         mdx_sweep_run_end(ctx, &run);
+        if (tuning) {
+            MDX_CUDA(ctx, cudaEventRecord(ctx->tune_ev[1], ctx->stream));
+            MDX_CUDA(ctx, cudaEventSynchronize(ctx->tune_ev[1]));
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, ctx->tune_ev[0], ctx->tune_ev[1]) == cudaSuccess && iters > 0)
+                ctx->rb32_tune_ms[cand] = ms > 0.f ? ms / iters : 1e-9;
+            if (cand == ncand - 1 && ctx->rb32_tune_ms[cand] > 0.0) {
+                int best = 0;
+                for (int t = 1; t < ncand; ++t)
+                    if (ctx->rb32_tune_ms[t] < ctx->rb32_tune_ms[best]) best = t;
+                ctx->rb32_tuned = best + 1;
+            }
+        }
         return MDX_OK;
     };
 
@@ -284,7 +623,9 @@ int mdx_k_projection_redblack_mixed(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t
         s.residual = r / r0;
     }
     s.iterations = it;
-    s.variant = 100 + outer;   // mixed path: 100 + outer FP64 corrections
+    // mixed path: 100 + outer FP64 corrections with the colour sweeps, 300 +
+    // outer with the fused red+black pass
+    s.variant = (used_fused ? 300 : 100) + outer;
     ctx->last = s;
     if (st) *st = s;
     return MDX_OK;

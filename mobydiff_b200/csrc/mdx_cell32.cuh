@@ -9,6 +9,17 @@ struct mixed_params {
     float idx, idy, idz, idt;
 };
 
+// The FP32 arithmetic of the correction sweeps is written with explicit
+// roundings (__fmul_rn, __fsub_rn, __fmaf_rn), so that every kernel that
+// updates a cell -- the colour sweeps, the fused red+black pass, the ensemble
+// -- rounds the same operations whatever its compile flags, and they agree
+// bit for bit.
+// Cell divergence plus residual: r~ + (u_ip-u_i)/dx + (v_jp-v_j)/dy + (w_kp-w_k)/dz.
+__device__ __forceinline__ float sweep32_div(const mixed_params& P, float r, float ui, float uip, float vj, float vjp,
+                                             float wk, float wkp) {
+    return __fmaf_rn(__fsub_rn(wkp, wk), P.idz, __fmaf_rn(__fsub_rn(vjp, vj), P.idy, __fmaf_rn(__fsub_rn(uip, ui), P.idx, r)));
+}
+
 // The update of one cell from its six faces, its correction dp and its
 // residual r~ (pressure_redblack.f90:117-241 with homogeneous boundary
 // values): phi = fac * (r~ + div), dp += phi/dt_gamma, faces -+ phi/h mu.
@@ -18,15 +29,15 @@ __device__ __forceinline__ void sweep32_update(const mixed_params& P, float r, f
                                                float mu_u_ip, float mu_v_j, float mu_v_jp, float mu_w, float fac,
                                                bool v_lo, bool v_hi) {
     const float ui = u_i, uip = u_ip, vj = v_j, vjp = v_jp, wk = w_k, wkp = w_kp;
-    const float div = r + (uip - ui) * P.idx + (vjp - vj) * P.idy + (wkp - wk) * P.idz;
-    const float phi = div * fac;
-    dp += phi * P.idt;
-    u_i = ui - phi * P.idx * mu_u_i;
-    u_ip = uip + phi * P.idx * mu_u_ip;
-    if (v_lo) v_j = vj - phi * P.idy * mu_v_j;
-    if (v_hi) v_jp = vjp + phi * P.idy * mu_v_jp;
-    w_k = wk - phi * P.idz * mu_w;
-    w_kp = wkp + phi * P.idz * mu_w;
+    const float phi = __fmul_rn(sweep32_div(P, r, ui, uip, vj, vjp, wk, wkp), fac);
+    dp = __fmaf_rn(phi, P.idt, dp);
+    const float px = __fmul_rn(phi, P.idx), py = __fmul_rn(phi, P.idy), pz = __fmul_rn(phi, P.idz);
+    u_i = __fmaf_rn(-px, mu_u_i, ui);
+    u_ip = __fmaf_rn(px, mu_u_ip, uip);
+    if (v_lo) v_j = __fmaf_rn(-py, mu_v_j, vj);
+    if (v_hi) v_jp = __fmaf_rn(py, mu_v_jp, vjp);
+    w_k = __fmaf_rn(-pz, mu_w, wk);
+    w_kp = __fmaf_rn(pz, mu_w, wkp);
 }
 
 // One FP32 colour-sweep update of cell (i, j, k) of the correction problem

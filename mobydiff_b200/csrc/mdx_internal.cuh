@@ -59,6 +59,12 @@ __host__ __device__ __forceinline__ int pidx2(const mdx_dims& d, int i, int j) {
 __host__ __device__ inline int split_plane_elems(const mdx_dims& d) { return 2 * d.hs * d.nyp; }
 
 
+// Red-black kernel variants (opts.sor_variant; k_sor.cu, k_sor_mixed.cu).
+enum {
+    MDX_SORV_AUTO = 0, MDX_SORV_SWEEPS = 1, MDX_SORV_FUSED8 = 2, MDX_SORV_FUSED16 = 3, MDX_SORV_SPLIT = 4,
+    MDX_SORV_NUM = 5
+};
+
 // Scalars of one time step, passed by value to kernels.
 struct mdx_step_params {
     double dx, dy, dz;
@@ -108,7 +114,15 @@ struct mdx_ctx {
     // carved from one allocation (mx_du is its base) of mx_bytes
     float *mx_du = nullptr, *mx_dv = nullptr, *mx_dw = nullptr, *mx_dp = nullptr, *mx_r = nullptr;
     float *mx_mu = nullptr, *mx_fac = nullptr;
+    // the fused red+black pass reads faces from mx_du/dv/dw and writes the
+    // second buffers, then the pointers swap
+    float *mx_du2 = nullptr, *mx_dv2 = nullptr, *mx_dw2 = nullptr;
+    void* mx_base = nullptr;
     size_t mx_bytes = 0;
+    int rb32_tuned = 0;                      // FP32 inner sweeps: candidate + 1 chosen by the autotuner (0: not yet;
+                                             // candidates: the fused pass's tile shapes, then the colour sweeps)
+    unsigned rb32_attr = 0;                  // fused FP32 pass: shared-memory attribute set, bit per kernel
+    double rb32_tune_ms[8] = {0.0};          // time per iteration per candidate
     // warm starts: increments of the last projection of each RK substage
     int guess_mode = 0;                      // MDX_GUESS_*
     bool record_increments = false;

@@ -1,7 +1,8 @@
 """CPU model of the FP32 red-black correction sweeps of the mixed-precision
 projection: the two colour sweeps as the kernels k_sor_sweep32 run them, and
 the fused red+black pass k_rb32_fused (k_sor_mixed.cu) step by step, with its
-tiles, halo threads, shared-memory rings and register history.  Arrays are in
+tiles, halo threads, plane loads (the kernel stages them with cp.async in a
+ring of five planes), shared-memory rings and register history.  Arrays are in
 natural padded order [k][j][i] (the CUDA code's colour-split storage is an
 index permutation).  Both use the same FP32 operations (one rounding per
 multiply, add and fused multiply-add), so the fused pass must reproduce the
@@ -81,7 +82,7 @@ def fused(g, P, xu, xv, xw, dp, r, mu_u, mu_v, mu_w, fac, TI, TJ, TK):
     yv[:, 0, :] = xv[:, 0, :]          # wall rows are never written (they stay 0)
     yv[:, ny + 1, :] = xv[:, ny + 1, :]
     dp = dp.copy()
-    PW, RW, CW = TI // 2 + 2, TJ + 4, 2 * (TI // 2 + 2)
+    PW, RW, CW = TI // 2 + 2, TJ + 3, 2 * (TI // 2 + 2)
 
     def cx(i):
         m = i % nx
@@ -102,7 +103,6 @@ def fused(g, P, xu, xv, xw, dp, r, mu_u, mu_v, mu_w, fac, TI, TJ, TK):
                 i0, j0, k0 = bx * TI, 1 + by * TJ, 1 + bz * TK
                 thr = [(tx, ty) for ty in range(RW) for tx in range(PW)]
                 U = np.zeros((2, RW, PW + 1), F)
-                V = np.zeros((2, RW + 1, CW), F)
                 PH = np.zeros((2, RW, CW + 2), F)
                 st = {}
                 for tx, ty in thr:
@@ -122,15 +122,16 @@ def fused(g, P, xu, xv, xw, dp, r, mu_u, mu_v, mu_w, fac, TI, TJ, TK):
                     st[(tx, ty)] = s
 
                 def load(s, q):
-                    """Plane q: u, v, r, dp of the two cells and w(q+1)."""
+                    """Plane q: u, v, v(j+1), r, dp of the two cells and w(q+1)."""
                     j, ex = s["j"], s["ex"]
                     kc, kn = cz(q), cz(q + 1)
+                    jn = cy(j + 1) if PY else j + 1
                     out = {}
                     for c in (0, 1):
                         ic = s["ic"][c]
-                        vrow = ex or (not PY and j == ny + 1)
                         out[("u", c)] = xu[kc, s["jc"], ic] if ex else F(0)
-                        out[("v", c)] = xv[kc, s["jc"] if PY else j, ic] if vrow else F(0)
+                        out[("v", c)] = xv[kc, s["jc"], ic] if ex else F(0)
+                        out[("vn", c)] = xv[kc, jn, ic] if ex else F(0)
                         out[("r", c)] = r[kc, s["jc"], ic] if ex else F(0)
                         out[("dp", c)] = dp[kc, s["jc"], ic] if ex else F(0)
                         out[("w1", c)] = xw[kn, s["jc"], ic] if ex else F(0)
@@ -142,11 +143,9 @@ def fused(g, P, xu, xv, xw, dp, r, mu_u, mu_v, mu_w, fac, TI, TJ, TK):
                     s["cur"] = load(s, k0 - 2)
                     s["prev"] = None
                 for q in range(k0 - 2, k0 + TK + 1):
-                    # A: publish this plane's u(even) and v
+                    # A: publish this plane's u(even)
                     for (tx, ty), s in st.items():
                         U[q & 1, ty, tx] = s["cur"][("u", 0)]
-                        V[q & 1, ty, 2 * tx] = s["cur"][("v", 0)]
-                        V[q & 1, ty, 2 * tx + 1] = s["cur"][("v", 1)]
                     # B: red cell of plane q
                     for (tx, ty), s in st.items():
                         j = s["j"]
@@ -156,7 +155,7 @@ def fused(g, P, xu, xv, xw, dp, r, mu_u, mu_v, mu_w, fac, TI, TJ, TK):
                         cur = s["cur"]
                         ui = cur[("u", c)]
                         uip = cur[("u", 1)] if c == 0 else U[q & 1, ty, tx + 1]
-                        vj, vjp = cur[("v", c)], V[q & 1, ty + 1, 2 * tx + c]
+                        vj, vjp = cur[("v", c)], cur[("vn", c)]
                         wk, wkp = s["w"][c], cur[("w1", c)]
                         phi = mul(div_of(P, cur[("r", c)], ui, uip, vj, vjp, wk, wkp), s["fac"][c])
                         s["p"][c][0] = phi
@@ -180,7 +179,7 @@ def fused(g, P, xu, xv, xw, dp, r, mu_u, mu_v, mu_w, fac, TI, TJ, TK):
                             vj = pv[("v", c)]
                             if exists(j - 1):
                                 vj = fma(mul(PH[h, ty - 1, 2 * tx + c + 1], P["idy"]), s["mu_v"][c], vj)
-                            vjp = V[h, ty + 1, 2 * tx + c]
+                            vjp = pv[("vn", c)]
                             if exists(j + 1):
                                 vjp = fma(-mul(PH[h, ty + 1, 2 * tx + c + 1], P["idy"]), s["mu_vn"][c], vjp)
                             wk = fma(mul(s["p"][c][2], P["idz"]), s["mu_w"][c], s["wp"][c])
