@@ -1140,12 +1140,14 @@ int mdx_k_projection_fft_mixed(mdx_ctx_t* ctx, double dg) {
 // runtime (the reference hands cuFFT such arrays through use_device_addr).
 //
 // The array is MDX_NOALLOC_SCRATCH_BYTES per device and lives as long as the
-// library is loaded.  Its device address is looked up once per device, on
-// that device's first call (cudaGetSymbolAddress), so the first call on a
-// device should come before any stream capture.  All calls share the array
-// and it keeps the last call's contents; every call rewrites all of it that
-// it reads, so nothing needs clearing.  Calls that overlap on the GPU (two
-// streams, or two host threads) race on the array.
+// library is loaded.  Its device address is looked up (cudaGetSymbolAddress)
+// on a device's first call, and again on every later call made outside a
+// stream capture, so the first call on a device should come before any
+// stream capture.  All calls share the array and it keeps the last call's
+// contents; every call rewrites all of it that it reads (tables, twiddles
+// and wavenumbers are rebuilt on the device each call), so nothing needs
+// clearing.  Calls that overlap on the GPU (two streams, or two host
+// threads) race on the array.
 // ---------------------------------------------------------------------------
 #include <mutex>
 
@@ -1193,6 +1195,31 @@ k_fftx_r2c(mdx_dims d, int R, const double* __restrict__ rhs, double2* __restric
 
 static size_t noalloc_align(size_t b) { return (b + 255) & ~(size_t)255; }
 
+// The allocation-free solve's trigonometric tables: twiddles
+// W_n^t = exp(-2 pi i t / n) of the x (n = nx) and z (n = nz) transforms,
+// and the modified wavenumbers 4/h^2 sin^2(pi k / n) with k = ikx - 1 for
+// x and the signed kz for z (pressure_fft.f90:53,61).
+__global__ void k_noalloc_trig(int nx, int nz, int nxh, double dx, double dz, double2* __restrict__ twx,
+                               double2* __restrict__ twz, double* __restrict__ kxp, double* __restrict__ kzp) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    double s, c;
+    if (t < nx) {
+        sincospi(2.0 * (double)t / (double)nx, &s, &c);
+        twx[t] = make_double2(c, -s);
+    }
+    if (t < nz) {
+        sincospi(2.0 * (double)t / (double)nz, &s, &c);
+        twz[t] = make_double2(c, -s);
+        const int kz = (t + 1 <= nz / 2 + 1) ? t : t - nz;
+        const double q = sinpi((double)kz / (double)nz);
+        kzp[t] = (4.0 / (dz * dz)) * (q * q);
+    }
+    if (t < nxh) {
+        const double q = sinpi((double)t / (double)nx);
+        kxp[t] = (4.0 / (dx * dx)) * (q * q);
+    }
+}
+
 extern "C" int mdx_solve_pressure_fft_noalloc(const double* rhs, double* phi, int nx, int ny, int nz, double dx,
                                               double dy, double dz, void* stream) {
     if (!rhs || !phi) return mdx_fail(nullptr, MDX_ERR_ARG, "noalloc solve: null rhs or phi");
@@ -1231,15 +1258,30 @@ extern "C" int mdx_solve_pressure_fft_noalloc(const double* rhs, double* phi, in
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return mdx_fail(nullptr, MDX_ERR_NO_DEVICE, "noalloc solve: %s", cudaGetErrorString(e));
     if (dev < 0 || dev >= MDX_NOALLOC_MAX_DEVICES) return mdx_fail(nullptr, MDX_ERR_ARG, "noalloc solve: device %d", dev);
+    cudaStream_t st = (cudaStream_t)stream;
+    // The array's device address belongs to the context current now.  Outside
+    // a stream capture it is looked up on every call, so that a context made
+    // current since the last call (a device reset, or a runtime that brings
+    // its own context) gets its own address; during a capture the lookup is
+    // not made (it may load the module, which a capture forbids) and the
+    // address from the last call on this device outside a capture is used.
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cap) != cudaSuccess) {
+        (void)cudaGetLastError();
+        cap = cudaStreamCaptureStatusActive;
+    }
     unsigned char* base = nullptr;
     {
         std::lock_guard<std::mutex> lk(g_noalloc_mu);
-        if (!g_noalloc_addr[dev]) {
+        if (cap == cudaStreamCaptureStatusNone) {
             void* p = nullptr;
             e = cudaGetSymbolAddress(&p, mdx_noalloc_scratch);
             if (e != cudaSuccess)
                 return mdx_fail(nullptr, MDX_ERR_CUDA, "noalloc solve: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
             g_noalloc_addr[dev] = p;
+        } else if (!g_noalloc_addr[dev]) {
+            return mdx_fail(nullptr, MDX_ERR_STATE,
+                            "noalloc solve: first call on device %d made during a stream capture; call once before", dev);
         }
         base = (unsigned char*)g_noalloc_addr[dev];
     }
@@ -1250,43 +1292,12 @@ extern "C" int mdx_solve_pressure_fft_noalloc(const double* rhs, double* phi, in
     double2* twz = (double2*)(base + b_spec + 2 * b_tab + b_twx);
     double* kxp = (double*)(base + b_spec + 2 * b_tab + b_twx + b_twz);
     double* kzp = (double*)(base + b_spec + 2 * b_tab + b_twx + b_twz + b_kx);
-    cudaStream_t st = (cudaStream_t)stream;
 
-    // Twiddles (long-double cosl/sinl) and modified wavenumbers (libm sin,
-    // pressure_fft.f90:53,61) on the host, staged through fixed static host
-    // arrays (under the lock) and copied into the scratch; a copy from
-    // pageable memory has read the host array when cudaMemcpyAsync returns.
+    // Twiddles and modified wavenumbers (pressure_fft.f90:53,61) are built on
+    // the device in the scratch, so the call copies nothing from the host.
     {
-        static double2 host_tw[8192];
-        static double host_k[4097];
-        std::lock_guard<std::mutex> lk(g_noalloc_mu);
-        const long double two_pi = 6.283185307179586476925286766559005768L;
-        for (int t = 0; t < nx; ++t) {
-            const long double a = two_pi * (long double)t / (long double)nx;
-            host_tw[t] = make_double2((double)cosl(a), (double)(-sinl(a)));
-        }
-        e = cudaMemcpyAsync(twx, host_tw, sizeof(double2) * nx, cudaMemcpyHostToDevice, st);
-        if (e != cudaSuccess) return mdx_fail(nullptr, MDX_ERR_CUDA, "noalloc solve: copy: %s", cudaGetErrorString(e));
-        for (int t = 0; t < nz; ++t) {
-            const long double a = two_pi * (long double)t / (long double)nz;
-            host_tw[t] = make_double2((double)cosl(a), (double)(-sinl(a)));
-        }
-        e = cudaMemcpyAsync(twz, host_tw, sizeof(double2) * nz, cudaMemcpyHostToDevice, st);
-        if (e != cudaSuccess) return mdx_fail(nullptr, MDX_ERR_CUDA, "noalloc solve: copy: %s", cudaGetErrorString(e));
-        const double pi = 3.141592653589793;
-        for (int ikx = 1; ikx <= d.nxh; ++ikx) {
-            const double s = std::sin(pi * (double)(ikx - 1) / (double)nx);
-            host_k[ikx - 1] = (4.0 / (dx * dx)) * (s * s);
-        }
-        e = cudaMemcpyAsync(kxp, host_k, sizeof(double) * d.nxh, cudaMemcpyHostToDevice, st);
-        if (e != cudaSuccess) return mdx_fail(nullptr, MDX_ERR_CUDA, "noalloc solve: copy: %s", cudaGetErrorString(e));
-        for (int ikz = 1; ikz <= nz; ++ikz) {
-            const int kz = (ikz <= nz / 2 + 1) ? ikz - 1 : ikz - nz - 1;
-            const double s = std::sin(pi * (double)kz / (double)nz);
-            host_k[ikz - 1] = (4.0 / (dz * dz)) * (s * s);
-        }
-        e = cudaMemcpyAsync(kzp, host_k, sizeof(double) * nz, cudaMemcpyHostToDevice, st);
-        if (e != cudaSuccess) return mdx_fail(nullptr, MDX_ERR_CUDA, "noalloc solve: copy: %s", cudaGetErrorString(e));
+        const int nmax = std::max(nx, nz);
+        k_noalloc_trig<<<(nmax + 255) / 256, 256, 0, st>>>(nx, nz, d.nxh, dx, dz, twx, twz, kxp, kzp);
     }
 
     const double dyi2 = 1.0 / (dy * dy);

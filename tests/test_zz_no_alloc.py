@@ -11,7 +11,10 @@ This test calls it through the C ABI twice in a row, on two different grids
 and right-hand sides, and checks each result against the pressure correction
 of the regular entry point (mdx_pressure_projection on a context) for the
 same right-hand side, within the 1e-12 relative tolerance of the FFT-path
-tests.  It lives in a file of its own that pytest collects last.
+tests.  A second test solves in place (phi and rhs the same array) and then a
+grid of another size on a fresh non-default stream, so each call must rebuild
+every part of the shared scratch it reads.  It lives in a file of its own that
+pytest collects last.
 """
 import ctypes as C
 
@@ -59,6 +62,33 @@ def test_noalloc_solve_matches_regular_entry_point():
         phi = d_phi.cpu().numpy()
         assert np.all(np.isfinite(phi))
         assert rel_l2(phi, phi_ref) <= 1e-12
+
+
+def _fn():
+    fn = M.lib().mdx_solve_pressure_fft_noalloc
+    fn.restype = C.c_int
+    fn.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                   C.c_void_p]
+    return fn
+
+
+@pytest.mark.gpu
+def test_noalloc_in_place_then_other_grid_on_new_stream():
+    import torch
+
+    fn = _fn()
+    torch.cuda.set_device(0)
+    cases = (((40, 12, 30), 43, 0.5e-3, None), ((24, 18, 40), 44, 0.3e-3, torch.cuda.Stream()))
+    for shape, seed, dg, stream in cases:
+        g, rhs, phi_ref = _regular_phi(shape, seed, dg)
+        d = torch.from_numpy(rhs).to("cuda")
+        sp = (stream or torch.cuda.current_stream()).cuda_stream
+        if stream is not None:
+            stream.wait_stream(torch.cuda.current_stream())
+        rc = fn(d.data_ptr(), d.data_ptr(), g.nx, g.ny, g.nz, g.dx, g.dy, g.dz, sp)   # phi = rhs, in place
+        assert rc == M.MDX_OK, M.lib().mdx_last_error(None).decode()
+        torch.cuda.synchronize()
+        assert rel_l2(d.cpu().numpy(), phi_ref) <= 1e-12, shape
 
 
 def test_noalloc_rejects_grids_beyond_its_scratch():
