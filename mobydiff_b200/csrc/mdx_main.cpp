@@ -53,6 +53,17 @@ static int write_field(mdx_ctx_t* ctx, const mdx_grid_t& g, int step, const char
     return MDX_OK;
 }
 
+// One value under the Fortran edit descriptor ES20.12 (io.f90:237-257):
+// 12 digits after the point, exponent E+dd, and for a three-digit exponent
+// the form +ddd without the letter E; right-justified in 20 characters.
+static void put_es20_12(FILE* fp, double x) {
+    char b[64];
+    std::snprintf(b, sizeof(b), "%.12E", x);
+    char* e = std::strchr(b, 'E');
+    if (e && std::strlen(e + 2) > 2) std::memmove(e, e + 1, std::strlen(e + 1) + 1);   // E+123 -> +123
+    std::fprintf(fp, "%20s", b);
+}
+
 static int write_vtk(mdx_ctx_t* ctx, const mdx_grid_t& g, int step, const char* prefix) {
     char name[512];
     std::snprintf(name, sizeof(name), "%s_%d.vtk", prefix, step);
@@ -65,11 +76,19 @@ static int write_vtk(mdx_ctx_t* ctx, const mdx_grid_t& g, int step, const char* 
     if (!fp) return MDX_ERR_IO;
     std::fprintf(fp, "# vtk DataFile Version 3.0\n3D velocity field\nASCII\nDATASET STRUCTURED_POINTS\n");
     std::fprintf(fp, "DIMENSIONS %d %d %d\n", g.nx + 1, g.ny + 1, g.nz + 1);
-    std::fprintf(fp, "ORIGIN %20.12E%20.12E%20.12E\n", 0.0, 0.0, 0.0);
-    std::fprintf(fp, "SPACING %20.12E%20.12E%20.12E\n", g.dx, g.dy, g.dz);
-    std::fprintf(fp, "FIELD FieldData 1\nTIME 1 1 double\n%20.12E\n", g.t_current);
-    std::fprintf(fp, "CELL_DATA %zu\nVECTORS U double\n", n);
-    for (size_t t = 0; t < n; ++t) std::fprintf(fp, "%20.12E%20.12E%20.12E\n", uc[t], vc[t], wc[t]);
+    std::fprintf(fp, "ORIGIN ");
+    for (double x : {0.0, 0.0, 0.0}) put_es20_12(fp, x);
+    std::fprintf(fp, "\nSPACING ");
+    for (double x : {g.dx, g.dy, g.dz}) put_es20_12(fp, x);
+    std::fprintf(fp, "\nFIELD FieldData 1\nTIME 1 1 double\n");
+    put_es20_12(fp, g.t_current);
+    std::fprintf(fp, "\nCELL_DATA %zu\nVECTORS U double\n", n);
+    for (size_t t = 0; t < n; ++t) {
+        put_es20_12(fp, uc[t]);
+        put_es20_12(fp, vc[t]);
+        put_es20_12(fp, wc[t]);
+        std::fputc('\n', fp);
+    }
     std::fclose(fp);
     return MDX_OK;
 }
