@@ -61,10 +61,12 @@ CONFIGS = {
                tol=1e-8, method="learned-eval", check_every=10, train_runs=8, record_steps=8, heldout_runs=4,
                heldout_steps=10),
     "c4": dict(workload="ensemble of 64 wavy-wall IBM channels, nx,nz in 32..128 and ny in 32..96 (multiples of 16), "
-                         "Re U(1000,5000), A U(0,0.1), red-black SOR omega=1.7 to residual 1e-8 from the extrapolated "
-                         "increment, FP32 sweeps in FP64 defect correction; one persistent launch per RK3 substage, "
-                         "CUDA graph, autotuned launch shape",
-               solver="redblack", sor=1.7, tol=1e-8, check_every=10, members=64, method="ensemble", mixed=True),
+                         "Re U(1000,5000), A U(0,0.1), red-black SOR omega=1.7 to residual 1e-8, FP32 sweeps in FP64 "
+                         "defect correction, learned warm start (network trained on stratified member-like runs); "
+                         "two persistent launches per RK3 substage with the network between, CUDA graph, autotuned "
+                         "launch shape",
+               solver="redblack", sor=1.7, tol=1e-8, check_every=10, members=64, method="ensemble", mixed=True,
+               learned=True, train_runs=6, record_steps=6),
     "c0": dict(workload="periodic channel 64^3, FP64 FFT+Thomas", nx=64, ny=64, nz=64, lx=2 * math.pi, ly=2.0,
                lz=math.pi, re=2000.0, dt=1e-3, solver="fft", ibm="none", amp=0.0, method="plain"),
     "c2": dict(workload="channel 512x256x256 (Lx 4pi, Lz 2pi, Re 5000): FP32 FFT + Thomas inside FP64 defect "
@@ -157,6 +159,14 @@ SOR_VARIANT = 0   # --sor-variant: red-black kernel variant (0: the autotuner's 
 FFT_KERNEL = 0    # --fft-kernel: 0 warp-shuffle transforms where the lengths allow, 1 Stockham
 SOR_NAMES = {1: "one launch per colour sweep", 2: "fused red+black pass 32x8", 3: "fused red+black pass 32x16",
              4: "one launch per colour sweep on colour-split copies"}
+
+
+# FP32 correction sweeps of the mixed path, by the hundreds digit of the
+# solve's variant
+SOR32_NAMES = {1: "k_sor_sweep32: one launch per colour, one cell per thread",
+               3: "k_rb32_fused: one launch per red+black iteration",
+               5: "k_sor_sweep32v: one launch per colour, 2 or 4 cells per thread"}
+SOR32_TRAFFIC = {1: "sor_sweep32", 3: "rb32_fused", 5: "sor_sweep32v"}
 
 
 def _sor64_traffic_key(variant):
@@ -632,6 +642,25 @@ def ensemble_members(M, n, seed=SEED):
     return out
 
 
+def _train_ensemble_net(M, cfg, device, iters):
+    """The learned warm start for the ensemble: snapshots of wavy-channel runs
+    on one member-like grid (64x48x64, the members' lengths), Re and A each
+    stratified over the members' ranges (1000..5000, 0..0.1), then Adam on
+    the device; the network is fully convolutional, so it applies to every
+    member's grid."""
+    from mobydiff_b200 import learned
+    rng = np.random.default_rng(SEED + 4)
+    nt = cfg["train_runs"]
+    perm = rng.permutation(nt)
+    runs = [(SEED + 300 + q, float(0.1 * (q + rng.uniform()) / nt), float(1000.0 + 4000.0 * (perm[q] + rng.uniform()) / nt))
+            for q in range(nt)]
+    s, g = learned.wavy_solver(64, 48, 64, runs[0][2], runs[0][1], cfg["tol"], check_every=cfg["check_every"],
+                               precision=M.PREC_MIXED, device=device)
+    net = learned.record_and_train(s, g, runs, warm_steps=3, record_steps=cfg["record_steps"], iters=iters)
+    s.close()
+    return net
+
+
 def partition_members(sizes, world):
     """Ensemble members to ranks by cell count: largest first, each to the
     rank with the fewest cells so far (ties: lowest rank).  Deterministic,
@@ -665,8 +694,16 @@ def run_ensemble(args, cfg):
     opts = M.make_solver_opts(M.SOLVER_REDBLACK, sor=cfg["sor"], tol=cfg["tol"], check_every=cfg["check_every"],
                               max_iter=400000, precision=prec)
     W, K = args.warmup, args.steps
+    net, train_wall = None, 0.0
+    if cfg.get("learned"):
+        t0 = time.time()
+        net = _train_ensemble_net(M, cfg, device, args.train_iters * 2)
+        train_wall = time.time() - t0
+    mode = M.GUESS_LEARNED if net else M.GUESS_EXTRAPOLATED
     E = M.Ensemble(mems, opts, device)
-    E.set_guess(M.GUESS_EXTRAPOLATED)
+    if net:
+        E.unet_load(net.params, net.out_scale, channels=net.channels)
+    E.set_guess(mode)
     E.ic()
     cache = os.path.join(os.path.expanduser("~"), ".cache", "mobydiff_b200", "ensemble_tune.json")
     os.makedirs(os.path.dirname(cache), exist_ok=True)
@@ -678,9 +715,11 @@ def run_ensemble(args, cfg):
         pg.barrier()
     clocks = ClockSampler(device)
     clocks.start()
+    l0 = E.info()["launches"]
     iters = E.step(K)   # device time between events around the K graph replays
     clk = clocks.stop()
     info = E.info()
+    launches_timed = info["launches"] - l0
     it_m = [E.member_stats(q)[1] - it0[q] for q in range(len(mems))]
     ms = info["last_step_ms"] * K
     ms_all = ms
@@ -697,6 +736,13 @@ def run_ensemble(args, cfg):
     roofline = {"kernel": "k_ens_substage (whole substage)", "bound": "hbm", "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
                 "algorithmic_bytes": alg / K, "avg_launch_ms": ms / (3 * K), "launches": 3 * K}
+    learned_info = None
+    if net:
+        kept, undone = E.unet_stats()
+        learned_info = {"corrections_kept": kept, "corrections_undone": undone, "snapshots": net.snapshots,
+                        "loss_first": net.loss_first, "loss_last": net.loss_last, "train_ms": net.train_ms,
+                        "setup_wall_s": train_wall, "train_runs": [list(r) for r in net.runs],
+                        "launches_per_step": launches_timed / max(K, 1)}
     # e2e: the timed steps replayed from the same u, v, w, p, copied from host
     # memory every step through the C ABI (the warm-start history has moved on)
     e2e_line = None
@@ -717,6 +763,24 @@ def run_ensemble(args, cfg):
         e2e_line = {"value": cells_total * K / e2e_s / 1e6, "unit": UNIT, "h2d_bytes_per_step": nbytes,
                     "d2h_bytes_per_step": nbytes, "timer": "host wall clock around the C-ABI calls",
                     "same_steps_as_value": False, "iterations": e2e_iters}
+    # the same members and steps from the extrapolated increment alone
+    no_net = None
+    if net:
+        E.close()
+        X = M.Ensemble(mems, opts, device)
+        X.set_guess(M.GUESS_EXTRAPOLATED)
+        X.ic()
+        X.step(W)
+        X.tune(cache)
+        if pg:
+            pg.barrier()
+        x_iters = X.step(K)
+        x_ms = X.info()["last_step_ms"] * K
+        x_all = max_over_ranks(x_ms, pg) if pg else x_ms
+        no_net = {"value": cells_total * K / (x_all / 1e3) / 1e6, "unit": UNIT, "ms_per_step": x_all / K,
+                  "poisson_iters_per_member_substage": x_iters / (3 * K * len(mems)),
+                  "note": "same members, steps and launch-shape tuning, extrapolated increment only"}
+        E = X
     # the same members one after another through single contexts
     seq = None
     if not args.quick and ws == 1:
@@ -756,8 +820,9 @@ def run_ensemble(args, cfg):
                                            "step_ms": tuned[3] if tuned[3] >= 0 else "from cache"},
                              "launches_per_step": 3},
                 "sequential_single_contexts": seq,
+                "learned": learned_info, "extrapolated_no_network": no_net,
                 "roofline": roofline, "cpu_baseline": None, "clocks": clk, "e2e": e2e_line,
-                "gpu_launches": 3 * K}
+                "gpu_launches": launches_timed}
         print(json.dumps(line), flush=True)
     E.close()
     if pg:
@@ -926,8 +991,10 @@ def run_learned_eval(args, cfg):
     st_.close()
     train_wall = time.time() - t0
 
+    # "learned": the correction as predicted, kept when it lowers ||div u||;
+    # "learned_energy": scaled by its energy-optimal step, kept when that is > 0
     modes = [("zero", M.GUESS_ZERO), ("previous", M.GUESS_PREVIOUS), ("extrapolated", M.GUESS_EXTRAPOLATED),
-             ("learned", M.GUESS_LEARNED)]
+             ("learned", M.GUESS_LEARNED), ("learned_energy", M.GUESS_LEARNED)]
     per_run, totals = [], {m: [0, 0.0] for m, _ in modes}
     for seed, amp, re in held:
         row = {"seed": seed, "re": re, "amp": amp}
@@ -935,7 +1002,7 @@ def run_learned_eval(args, cfg):
         for name, mode in modes:
             s, g = solver(re, amp)
             if mode == M.GUESS_LEARNED:
-                learned.load_into(s, net)
+                learned.load_into(s, net, step_rule=1 if name == "learned_energy" else 0)
             s.set_pressure_guess(mode, record=True)
             s.channel_ic(seed, 0.1, 0.01, y0, amp, lam)
             s.step(3)
@@ -971,6 +1038,8 @@ def run_learned_eval(args, cfg):
                                      summary["learned"]["iters_per_substage"],
             "reduction_vs_extrapolated": summary["extrapolated"]["iters_per_substage"] /
                                          summary["learned"]["iters_per_substage"],
+            "energy_step_reduction_vs_extrapolated": summary["extrapolated"]["iters_per_substage"] /
+                                                     summary["learned_energy"]["iters_per_substage"],
             "heldout_runs": per_run,
             "learned": {"snapshots": net.snapshots, "loss_first": net.loss_first, "loss_last": net.loss_last,
                         "train_ms": net.train_ms, "record_s": net.record_seconds, "setup_wall_s": train_wall},
@@ -1079,8 +1148,12 @@ def run_learned_mixed(args, cfg):
     s.warm_checkpoint(restore=True)
     s.update_device(*[h.numpy() for h in host])
     _, r_ms, _, _, tim = _timed_steps(s, stream, K, pg, timing=2)
-    # 4 floats per cell per colour sweep
-    roofline = _roofline(tim, "sor_run", _sor_alg_per_launch(1, fp32=True), cells, r_ms, traffic_key="sor_sweep32")
+    # 4 floats per cell per colour sweep; the FP32 sweep kernel the autotuner
+    # kept is the hundreds digit of the solve's variant
+    kind = s.last_solve_stats().variant // 100
+    roofline = _roofline(tim, "sor_run", _sor_alg_per_launch(2 if kind == 3 else 1, fp32=True), cells, r_ms,
+                         traffic_key=SOR32_TRAFFIC.get(kind, "sor_sweep32"))
+    roofline["sor_kernel"] = SOR32_NAMES.get(kind, "?")
     step_hbm = _step_hbm(cells, ms_all / K, iters / K, 32.0)
 
     # ---- the same steps without the network: extrapolated increment only ----

@@ -98,11 +98,12 @@ typedef struct {
                           3 fused pass, 32x16 tiles; 4 one launch per colour on
                           colour-split copies of u, v, w, p made once per projection
                           (2-4: periodic x and z, IBM factors 1 or z-invariant).
-                          FP32 sweeps of the mixed precision: 1 one launch per colour;
-                          2 or 3 the fused red+black pass (one launch per iteration) in
-                          the fastest of four tile shapes; 0 or 4 the fastest of all five,
-                          each timed on one block of the first iterations (all give the
-                          same bits) */
+                          FP32 sweeps of the mixed precision: 1 one launch per colour,
+                          one cell per thread; 2 or 3 the fused red+black pass (one
+                          launch per iteration) in the fastest of four tile shapes; 4 one
+                          launch per colour with 2 or 4 cells per thread, the faster;
+                          0 the fastest of all seven, each timed on one block of the
+                          first iterations (all give the same bits) */
     int sor_kz;        /* z planes per block of the fused pass (0: default 16) */
     int check_mode;    /* red-black, tol > 0: 0 (default) residual checks at multiples of check_every,
                           up to 8 blocks apart while the residual falls at a steady rate that
@@ -129,7 +130,9 @@ typedef struct {
     double residual0;   /* ||div u*||2                                       */
     double atol;        /* absolute floor used (red-black)                   */
     int variant;        /* red-black kernel variant of the last iterations;
-                           100 + n: mixed precision with n FP64 corrections;
+                           100 + n: mixed precision with n FP64 corrections
+                           (300 + n with the fused FP32 pass, 500 + n with the
+                           FP32 sweeps of 2 or 4 cells per thread);
                            200 + n: FFT path in mixed precision, n FP64 passes
                            (iterations = n as well) */
     int guessed;        /* 1 when a warm-start guess was applied             */
@@ -377,7 +380,9 @@ int mdx_ensemble_create(int device, int n, const mdx_member_t* members, const md
                         mdx_ensemble_t** out);
 int mdx_ensemble_destroy(mdx_ensemble_t* ens);
 const char* mdx_ensemble_last_error(const mdx_ensemble_t* ens);
-/* MDX_GUESS_ZERO, MDX_GUESS_PREVIOUS or MDX_GUESS_EXTRAPOLATED. */
+/* MDX_GUESS_ZERO, MDX_GUESS_PREVIOUS, MDX_GUESS_EXTRAPOLATED, or
+ * MDX_GUESS_LEARNED once a network is loaded (mdx_ensemble_unet_load) and
+ * tol > 0. */
 int mdx_ensemble_set_guess(mdx_ensemble_t* ens, int mode);
 /* Seeded channel initial condition of every member, projected at t = 0
  * (dt_gamma = 1), then p = 0 (mdx_channel_ic with y0 = (Ly-2)/2, the
@@ -429,7 +434,12 @@ typedef struct {
     int conv_kernel;        /* 0 (default): forward convolutions and data gradients on levels whose
                                nx is a multiple of 128 run on tcgen05 (tensor-memory accumulators),
                                the rest on mma.sync; 1: mma.sync everywhere                  */
-    int reserved_i[7];
+    int step_rule;          /* 0 (default): apply the correction as predicted, keep it when it lowers
+                               ||div u||; 1: apply alpha x the correction with alpha the step that
+                               minimises the energy norm of the pressure error along it,
+                               alpha = -<delta, d0> / <delta, d1 - d0> (d0, d1 the divergence before
+                               and after the correction), kept when alpha > 0               */
+    int reserved_i[6];
     double reserved_d[8];
 } mdx_unet_opts_t;
 
@@ -444,10 +454,29 @@ typedef struct {
     double infer_ms;        /* device time of the last correction               */
     double train_ms;        /* device time of the last mdx_unet_train call      */
     long long tc_convs;     /* convolution launches on tcgen05 since creation   */
-    double reserved_d[5];
+    double last_step;       /* step_rule 1: the last step length alpha           */
+    double reserved_d[4];
 } mdx_unet_stats_t;
 
 void mdx_default_unet_opts(mdx_unet_opts_t* opts);
+
+/* Learned warm start in the ensemble (no counterpart in the reference): the
+ * trained parameters and output scale of a network with options `opts`
+ * (from a context: mdx_unet_get_params / mdx_unet_get_out_scale; the net is
+ * fully convolutional, so one trained on any grid applies to every member;
+ * member sizes must be multiples of 8).  With MDX_GUESS_LEARNED each
+ * substage runs as two cooperative launches with the network between them:
+ * the first applies the members' extrapolated increments, the network then
+ * runs for every member in turn on its own grid (one network sized for the
+ * member with the most cells; scales and the zero-mean projection on the
+ * device, no host read, so the step stays one CUDA graph), and the second
+ * applies each correction, keeps it where it lowers ||div u|| (else back to
+ * the extrapolated increment) and sweeps to the tolerance. */
+int mdx_ensemble_unet_load(mdx_ensemble_t* ens, const mdx_unet_opts_t* opts, const float* params, long long n,
+                           double out_scale);
+/* Learned corrections kept and undone over all members since creation
+ * (synchronises). */
+int mdx_ensemble_unet_stats(mdx_ensemble_t* ens, long long* corrections, long long* rejected);
 int mdx_unet_create(mdx_ctx_t* ctx, const mdx_unet_opts_t* opts);
 int mdx_unet_destroy(mdx_ctx_t* ctx);
 /* Record a snapshot in every converged projection that had an extrapolated
@@ -486,6 +515,23 @@ int mdx_center_vel(mdx_ctx_t* ctx, double* uc, double* vc, double* wc);
  * replayed from a CUDA graph.  total_iters (may be NULL) returns the summed
  * red-black iterations. */
 int mdx_step(mdx_ctx_t* ctx, int nsteps, long long* total_iters);
+
+/* `nsteps` RK3 steps with the reference's adaptive dt, src/main.f90:66-97:
+ * t += dt, the three substages, then cfl = get_cfl and, when cflmax > 0
+ * and cfl > 0, dt = min(cflmax/cfl, dtmax).  cflmax <= 0: mdx_step (fixed
+ * dt, no CFL).  On the FP64 FFT path every step is one CUDA graph in which
+ * the kernels read dt from device memory and the CFL reduction and the dt
+ * update run on the device; dt, t_current and cfl come back to the host
+ * once, after the last step.  On the other paths the CFL is read after
+ * every step.  g.dt, g.t_current, g.cfl, g.cflmax and g.dtmax are updated
+ * (mdx_get_time).  total_iters as mdx_step (0 on the FFT path). */
+int mdx_step_adaptive(mdx_ctx_t* ctx, int nsteps, double cflmax, double dtmax, long long* total_iters);
+
+/* The context's dt, t_current and the last CFL number (each may be NULL). */
+int mdx_get_time(mdx_ctx_t* ctx, double* dt, double* t_current, double* cfl);
+
+/* Set the dt mdx_step and mdx_step_adaptive start from (> 0, finite). */
+int mdx_set_dt(mdx_ctx_t* ctx, double dt);
 
 /* Seeded channel initial condition + projection at t=0 (new; the reference
  * zero-initialises, src/modules/init.f90:67-70): u = max(0,1-(y-yc(x))^2) +

@@ -96,7 +96,8 @@ class SolveStatsT(C.Structure):
 
 class UnetOptsT(C.Structure):
     _fields_ = [("channels0", C.c_int), ("channels", C.c_int), ("extra_bottleneck", C.c_int), ("capacity", C.c_int),
-                ("slope", C.c_double), ("seed", C.c_uint64), ("conv_kernel", C.c_int), ("reserved_i", C.c_int * 7),
+                ("slope", C.c_double), ("seed", C.c_uint64), ("conv_kernel", C.c_int), ("step_rule", C.c_int),
+                ("reserved_i", C.c_int * 6),
                 ("reserved_d", C.c_double * 8)]
 
 
@@ -104,7 +105,7 @@ class UnetStatsT(C.Structure):
     _fields_ = [("corrections", C.c_longlong), ("rejected", C.c_longlong), ("snapshots", C.c_longlong),
                 ("stored", C.c_int), ("trained", C.c_int), ("out_scale", C.c_double), ("last_gain", C.c_double),
                 ("infer_ms", C.c_double), ("train_ms", C.c_double), ("tc_convs", C.c_longlong),
-                ("reserved_d", C.c_double * 5)]
+                ("last_step", C.c_double), ("reserved_d", C.c_double * 4)]
 
 
 class MemberT(C.Structure):
@@ -184,6 +185,9 @@ def lib():
         "mdx_get_cfl": (i, [vp, P(d)]),
         "mdx_center_vel": (i, [vp, vp, vp, vp]),
         "mdx_step": (i, [vp, i, P(C.c_longlong)]),
+        "mdx_step_adaptive": (i, [vp, i, d, d, P(C.c_longlong)]),
+        "mdx_get_time": (i, [vp, P(d), P(d), P(d)]),
+        "mdx_set_dt": (i, [vp, d]),
         "mdx_channel_ic": (i, [vp, C.c_uint64, d, d, d, d, d, P(SolveStatsT)]),
         "mdx_divergence_norms": (i, [vp, P(d), P(d)]),
         "mdx_set_timing": (i, [vp, i]),
@@ -207,6 +211,8 @@ def lib():
         "mdx_ensemble_tune": (i, [vp, C.c_char_p, P(i), P(i), P(i), P(d)]),
         "mdx_ensemble_use_graph": (i, [vp, i]),
         "mdx_ensemble_info": (i, [vp, P(i), P(i), P(i), P(i), P(d), P(C.c_longlong)]),
+        "mdx_ensemble_unet_load": (i, [vp, P(UnetOptsT), P(C.c_float), C.c_longlong, d]),
+        "mdx_ensemble_unet_stats": (i, [vp, P(C.c_longlong), P(C.c_longlong)]),
         "mdx_default_unet_opts": (None, [P(UnetOptsT)]),
         "mdx_unet_create": (i, [vp, P(UnetOptsT)]),
         "mdx_unet_destroy": (i, [vp]),
@@ -511,6 +517,22 @@ class Solver:
         self._c(lib().mdx_step(self.h, int(nsteps), C.byref(it)))
         return it.value
 
+    def step_adaptive(self, nsteps: int, cflmax: float, dtmax: float) -> int:
+        """nsteps RK3 steps with the adaptive dt of src/main.f90:92-97
+        (dt = min(cflmax/cfl, dtmax) after every step); see time()."""
+        it = C.c_longlong(0)
+        self._c(lib().mdx_step_adaptive(self.h, int(nsteps), float(cflmax), float(dtmax), C.byref(it)))
+        return it.value
+
+    def time(self):
+        """(dt, t_current, cfl) of the context."""
+        a, b, c = C.c_double(0.0), C.c_double(0.0), C.c_double(0.0)
+        self._c(lib().mdx_get_time(self.h, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
+
+    def set_dt(self, dt: float) -> None:
+        self._c(lib().mdx_set_dt(self.h, float(dt)))
+
     def channel_ic(self, seed, amp_u=0.1, amp_vw=0.01, y0=0.0, wave_amp=0.0, wave_lambda=1.0) -> SolveStatsT:
         st = SolveStatsT()
         self._c(lib().mdx_channel_ic(self.h, seed, amp_u, amp_vw, y0, wave_amp, wave_lambda, C.byref(st)))
@@ -552,7 +574,7 @@ class Solver:
 
     # ---- learned warm start ----------------------------------------------
     def unet_create(self, channels: int = 32, extra_bottleneck: int = 0, capacity: int = 64, slope: float = 0.1,
-                    seed: int = 20261203, tcgen05: bool = True) -> None:
+                    seed: int = 20261203, tcgen05: bool = True, step_rule: int = 0) -> None:
         o = UnetOptsT()
         lib().mdx_default_unet_opts(C.byref(o))
         o.channels = channels
@@ -561,6 +583,7 @@ class Solver:
         o.slope = slope
         o.seed = seed
         o.conv_kernel = 0 if tcgen05 else 1
+        o.step_rule = step_rule
         self._c(lib().mdx_unet_create(self.h, C.byref(o)))
 
     def unet_destroy(self) -> None:
@@ -682,6 +705,27 @@ class Ensemble:
         it = C.c_longlong(0)
         self._c(lib().mdx_ensemble_step(self.h, int(nsteps), C.byref(it)))
         return it.value
+
+    def unet_load(self, params, out_scale: float, channels: int = 32, extra_bottleneck: int = 0,
+                  slope: float = 0.1, tcgen05: bool = True) -> None:
+        """A trained network (mobydiff_b200.learned.TrainedNet's parameters
+        and output scale) for the learned warm start of every member."""
+        o = UnetOptsT()
+        lib().mdx_default_unet_opts(C.byref(o))
+        o.channels = channels
+        o.extra_bottleneck = extra_bottleneck
+        o.capacity = 0
+        o.slope = slope
+        o.conv_kernel = 0 if tcgen05 else 1
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        self._c(lib().mdx_ensemble_unet_load(self.h, C.byref(o), p.ctypes.data_as(C.POINTER(C.c_float)), p.size,
+                                             float(out_scale)))
+
+    def unet_stats(self):
+        """(learned corrections kept, undone) over all members."""
+        a, b = C.c_longlong(0), C.c_longlong(0)
+        self._c(lib().mdx_ensemble_unet_stats(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
     def member_stats(self, m: int):
         st = SolveStatsT()

@@ -134,6 +134,8 @@ static size_t field_elems(const mdx_ctx_t* ctx, int f) {
 static void release_graph(mdx_ctx_t* ctx) {
     if (ctx->step_graph) cudaGraphExecDestroy(ctx->step_graph);
     ctx->step_graph = nullptr;
+    if (ctx->adapt_graph) cudaGraphExecDestroy(ctx->adapt_graph);
+    ctx->adapt_graph = nullptr;
 }
 
 extern "C" {
@@ -279,6 +281,7 @@ int mdx_destroy(mdx_ctx_t* ctx) {
     cudaFree(ctx->red_part);
     cudaFree(ctx->red_out);
     cudaFreeHost(ctx->red_host);
+    cudaFree(ctx->dt_dev);
     for (int t = 0; t < 2; ++t)
         if (ctx->tune_ev[t]) cudaEventDestroy(ctx->tune_ev[t]);
     for (auto& p : ctx->ev_pending) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
@@ -320,6 +323,13 @@ int mdx_set_bc(mdx_ctx_t* ctx, const mdx_bc_t* bc) {
     for (int t = 0; t < 8; ++t) ctx->sor_tune_ms[t] = 0.0;
     ctx->rb32_tuned = 0;
     for (int t = 0; t < 8; ++t) ctx->rb32_tune_ms[t] = 0.0;
+    // FFT solver: walls in x or z change the solve grid (and need Neumann
+    // pressure there); rebuild its workspace for the new conditions
+    if (ctx->solver && ctx->opts.solver == MDX_SOLVER_FFT &&
+        (ctx->fft_ext_x || ctx->fft_ext_z || !bc->is_periodic[0] || !bc->is_periodic[2])) {
+        mdx_fft_free(ctx);
+        MDX_TRY(mdx_fft_init(ctx));
+    }
     return MDX_OK;
 }
 
@@ -602,11 +612,20 @@ int mdx_divergence_norms(mdx_ctx_t* ctx, double* l2, double* linf) {
 }
 
 // One RK3 substage sequence, src/main.f90:69-89.
-static int rk_step_eager(mdx_ctx_t* ctx, double dt, long long* iters) {
+// One RK3 step with dt; with dtp (the FP64 FFT path only) the kernels read
+// dt from the device instead.
+static int rk_step_eager(mdx_ctx_t* ctx, double dt, long long* iters, const double* dtp = nullptr) {
     double a[3], b[3], c[3];
     mdx_rk_coeffs(a, b, c);
     for (int s = 0; s < 3; ++s) {
         const double da = dt * a[s], db = dt * b[s], dg = dt * c[s];
+        if (dtp) {
+            MDX_TRY(mdx_k_momentum(ctx, mdx_dscal(dtp, a[s]), mdx_dscal(dtp, b[s]), mdx_dscal(dtp, c[s])));
+            MDX_TRY(mdx_k_apply_bc(ctx));
+            MDX_TRY(mdx_k_projection_fft(ctx, mdx_dscal(dtp, c[s])));
+            MDX_TRY(mdx_k_apply_bc(ctx));
+            continue;
+        }
         MDX_TRY(mdx_k_momentum(ctx, da, db, dg));
         if (ctx->opts.solver == MDX_SOLVER_FFT) {
             MDX_TRY(mdx_k_apply_bc(ctx));
@@ -649,6 +668,90 @@ static int capture_fft_step(mdx_ctx_t* ctx, double dt) {
     cudaGraphDestroy(graph);
     if (e != cudaSuccess) { ctx->step_graph = nullptr; return mdx_fail(ctx, MDX_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e)); }
     ctx->graph_dt = dt;
+    return MDX_OK;
+}
+
+// One adaptive-dt step as a CUDA graph: the RK3 substages reading dt from
+// ctx->dt_dev, then get_cfl's reduction and the dt update on the device.
+static int capture_adaptive_step(mdx_ctx_t* ctx, double cflmax, double dtmax) {
+    release_graph(ctx);
+    cudaGraph_t graph = nullptr;
+    MDX_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    ctx->capturing = true;
+    const long long before = ctx->launches;
+    int rc = rk_step_eager(ctx, 0.0, nullptr, ctx->dt_dev);
+    if (rc == MDX_OK) rc = mdx_k_dt_update(ctx, ctx->dt_dev, cflmax, dtmax);
+    ctx->adapt_launches = ctx->launches - before;
+    ctx->launches = before;
+    ctx->capturing = false;
+    cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+    if (rc != MDX_OK) { if (graph) cudaGraphDestroy(graph); return rc; }
+    if (e != cudaSuccess) return mdx_fail(ctx, MDX_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&ctx->adapt_graph, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) { ctx->adapt_graph = nullptr; return mdx_fail(ctx, MDX_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e)); }
+    ctx->adapt_cflmax = cflmax;
+    ctx->adapt_dtmax = dtmax;
+    return MDX_OK;
+}
+
+int mdx_step_adaptive(mdx_ctx_t* ctx, int nsteps, double cflmax, double dtmax, long long* total_iters) {
+    MDX_TRY(need_solver(ctx));
+    if (nsteps < 0) return mdx_fail(ctx, MDX_ERR_ARG, "nsteps < 0");
+    if (!std::isfinite(cflmax) || !std::isfinite(dtmax) || (cflmax > 0.0 && !(dtmax > 0.0)))
+        return mdx_fail(ctx, MDX_ERR_ARG, "cflmax and dtmax must be finite, dtmax > 0 when cflmax > 0");
+    ctx->g.cflmax = cflmax;
+    ctx->g.dtmax = dtmax;
+    if (!(cflmax > 0.0)) return mdx_step(ctx, nsteps, total_iters);   // fixed dt, no CFL (main.f90:92-97)
+    long long iters = 0;
+    const bool use_graph = ctx->opts.solver == MDX_SOLVER_FFT && ctx->opts.precision == MDX_PREC_FP64 && !ctx->timing;
+    if (!use_graph) {
+        for (int n = 0; n < nsteps; ++n) {
+            const double dt = ctx->g.dt;
+            ctx->g.t_current = ctx->g.t_current + dt;
+            MDX_TRY(rk_step_eager(ctx, dt, &iters));
+            double cfl = 0.0;
+            MDX_TRY(mdx_k_cfl(ctx, &cfl));
+            ctx->g.cfl = cfl;
+            if (cfl > 0.0) ctx->g.dt = std::fmin(cflmax / cfl, dtmax);
+        }
+        if (total_iters) *total_iters = iters;
+        return MDX_OK;
+    }
+    if (!ctx->dt_dev) MDX_CUDA(ctx, cudaMalloc(&ctx->dt_dev, 4 * sizeof(double)));
+    if (!ctx->adapt_graph || ctx->adapt_cflmax != cflmax || ctx->adapt_dtmax != dtmax)
+        MDX_TRY(capture_adaptive_step(ctx, cflmax, dtmax));
+    double* hs = ctx->red_host;   // pinned, 3 doubles: {dt, t, cfl} in and out
+    MDX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    hs[0] = ctx->g.dt;
+    hs[1] = ctx->g.t_current;
+    hs[2] = ctx->g.cfl;
+    MDX_CUDA(ctx, cudaMemcpyAsync(ctx->dt_dev, hs, 3 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    for (int n = 0; n < nsteps; ++n) {
+        MDX_CUDA(ctx, cudaGraphLaunch(ctx->adapt_graph, ctx->stream));
+        ctx->launches += ctx->adapt_launches;
+    }
+    MDX_CUDA(ctx, cudaMemcpyAsync(hs, ctx->dt_dev, 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    MDX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    ctx->g.dt = hs[0];
+    ctx->g.t_current = hs[1];
+    ctx->g.cfl = hs[2];
+    if (total_iters) *total_iters = 0;
+    return MDX_OK;
+}
+
+int mdx_get_time(mdx_ctx_t* ctx, double* dt, double* t_current, double* cfl) {
+    if (!ctx) return mdx_fail(nullptr, MDX_ERR_ARG, "null context");
+    if (dt) *dt = ctx->g.dt;
+    if (t_current) *t_current = ctx->g.t_current;
+    if (cfl) *cfl = ctx->g.cfl;
+    return MDX_OK;
+}
+
+int mdx_set_dt(mdx_ctx_t* ctx, double dt) {
+    if (!ctx) return mdx_fail(nullptr, MDX_ERR_ARG, "null context");
+    if (!(dt > 0.0) || !std::isfinite(dt)) return mdx_fail(ctx, MDX_ERR_ARG, "dt must be positive and finite");
+    ctx->g.dt = dt;
     return MDX_OK;
 }
 

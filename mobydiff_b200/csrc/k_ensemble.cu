@@ -73,6 +73,9 @@ struct ens_member {                  // per member, read-only in the kernel
     double* h[3][2];                 // increment history per substage
     // mixed precision: FP32 corrections and residual (colour-split), FP32 factor planes
     float *du, *dv, *dw, *dp, *r32, *mu32, *fac32;
+    // learned warm start: the last two increments of this substage (network
+    // inputs) and the network's correction
+    double *hl1, *hl2, *delta;
 };
 
 struct ens_state {                   // per member, updated in the kernel
@@ -87,6 +90,10 @@ struct ens_state {                   // per member, updated in the kernel
     // sweeps, 2 done; outer FP64 corrections; inner stop state
     int phase, outer, stale;
     double e_best, inner_target;
+    // learned warm start: this projection's correction (0 none, 1 kept, 2
+    // undone, 3 being tried) and the counts over the run
+    int lr_last;
+    long long lr_corr, lr_rej;
 };
 
 struct ens_list {
@@ -111,6 +118,10 @@ struct ens_args {
     double tol, atol;
     int mixed;                       // FP32 sweeps in FP64 defect correction
     double inner_sor;                // their over-relaxation
+    // 0: the whole substage; 1: up to the warm start, then the network's
+    // inputs; 2: from the learned correction on (the network ran between)
+    int split;
+    const int* learn_ok;             // per member: the network wrote a correction
 };
 
 __device__ __forceinline__ double nanmax(double a, double b) { return (a != a || b != b) ? (a + b) : fmax(a, b); }
@@ -483,14 +494,13 @@ __device__ void cell_tiles(const ens_args& A, F f) {
 }
 
 // Apply member M's increment guess at cell t (k_apply_guess of k_warm.cu).
-__device__ __forceinline__ void guess_cell(const ens_member& M, double dg, unsigned t) {
+__device__ __forceinline__ void guess_cell(const ens_member& M, double dg, unsigned t, const double* gs) {
     const mdx_dims& d = M.d;
     int i, j, k;
     cell_ijk(M, t, i, j, k);
     const int im = i == 1 ? d.nx : i - 1;
     const int km = k == 1 ? d.nz : k - 1;
     const long long c = pidx(d, i, j, k);
-    const double* gs = M.guess;
     const double phi = gs[t] * dg;
     const double phx = gs[qidx(d, im, j, k)] * dg;
     const double phz = gs[qidx(d, i, j, km)] * dg;
@@ -521,6 +531,7 @@ __global__ void __launch_bounds__(MAX_THREADS, MINB) k_ens_substage(ens_args A) 
     const bool warm = A.momentum && A.guess_mode != MDX_GUESS_ZERO;
     const bool meas = A.tol > 0.0;
 
+    if (A.split != 2) {
     // ---- predictor (or u* = u for the t=0 projection) ----
     if (A.momentum) {
         for (int ti = blockIdx.x; ti < A.cell.n; ti += gridDim.x) {
@@ -591,6 +602,7 @@ __global__ void __launch_bounds__(MAX_THREADS, MINB) k_ens_substage(ens_args A) 
             const int h = S.hist_valid;
             S.has_guess = warm && (h & (1 << s));
             S.extrap = A.guess_mode != MDX_GUESS_PREVIOUS && (h & (8 << s));
+            S.lr_last = 0;
         }
     grid.sync();
 
@@ -643,7 +655,7 @@ __global__ void __launch_bounds__(MAX_THREADS, MINB) k_ens_substage(ens_args A) 
         });
         grid.sync();
         cell_tiles(A, [&](int m, const ens_member& M, unsigned t) {
-            if (A.st[m].has_guess) guess_cell(M, dg_of(A, M), t);
+            if (A.st[m].has_guess) guess_cell(M, dg_of(A, M), t, M.guess);
         });
         grid.sync();
         if (meas) {
@@ -682,6 +694,72 @@ __global__ void __launch_bounds__(MAX_THREADS, MINB) k_ens_substage(ens_args A) 
         } else if (blockIdx.x == 0) {
             for (int m = threadIdx.x; m < A.nmem; m += blockDim.x) A.st[m].guessed = A.st[m].has_guess;
         }
+    }
+    if (A.split == 1) {   // the network's inputs: the last two increments of members that kept the extrapolated guess
+        if (warm && meas)
+            cell_tiles(A, [&](int m, const ens_member& M, unsigned t) {
+                const ens_state& S = A.st[m];
+                if (!(S.guessed && S.extrap)) return;
+                const int cur = (S.flip >> s) & 1;
+                M.hl1[t] = M.h[s][cur][t];
+                M.hl2[t] = M.h[s][cur ^ 1][t];
+            });
+        return;
+    }
+    }   // split != 2
+
+    // ---- the learned correction (the network ran between parts 1 and 2):
+    // applied like a guess on top of the extrapolated one, kept when it
+    // lowers ||div u||, else undone back to the extrapolated guess ----
+    if (A.split == 2 && warm && meas) {
+        if (blockIdx.x == 0)
+            for (int m = threadIdx.x; m < A.nmem; m += blockDim.x) {
+                ens_state& S = A.st[m];
+                S.lr_last = (A.learn_ok[m] && S.guessed && S.extrap && S.status == MDX_NOT_CONVERGED) ? 3 : 0;
+            }
+        grid.sync();
+        cell_tiles(A, [&](int m, const ens_member& M, unsigned t) {
+            if (A.st[m].lr_last == 3) guess_cell(M, dg_of(A, M), t, M.delta);
+        });
+        grid.sync();
+        residual_tiles(A, [&](int m) { return A.st[m].lr_last == 3; });
+        grid.sync();
+        for (int m = blockIdx.x; m < A.nmem; m += gridDim.x) {
+            if (A.st[m].lr_last != 3) continue;
+            double s2, um;
+            member_sums(A, m, s2, um);
+            if (threadIdx.x == 0) {
+                ens_state& S = A.st[m];
+                const double rl = sqrt(s2);
+                if (rl < S.rg) {
+                    S.lr_last = 1;
+                    S.lr_corr++;
+                    S.rg = rl;
+                    S.r = rl;
+                    if (rl <= S.target) {
+                        S.status = MDX_OK;
+                        S.active = 0;
+                    }
+                } else {
+                    S.lr_last = 2;
+                    S.lr_rej++;
+                }
+            }
+            __syncthreads();
+        }
+        grid.sync();
+        pad_tiles(A, [&](int m, const ens_member& M, long long t) {
+            if (A.st[m].lr_last != 2) return;
+            M.un[t] = M.us[t];
+            M.vn[t] = M.vs[t];
+            M.wn[t] = M.ws[t];
+            M.pn[t] = M.p0[t];
+        });
+        grid.sync();
+        cell_tiles(A, [&](int m, const ens_member& M, unsigned t) {
+            if (A.st[m].lr_last == 2) guess_cell(M, dg_of(A, M), t, M.guess);
+        });
+        grid.sync();
     }
 
     // ---- red-black iterations ----
@@ -941,7 +1019,14 @@ struct mdx_ensemble {
     std::vector<std::pair<void*, size_t>> state_arrays;   // the state a snapshot copies
     std::vector<char*> shadow;
     long long launches = 0;
+    long long graph_launches = 3;
     double last_step_ms = 0.0;
+    // learned warm start: one network context sized for the member with the
+    // most cells (its activations fit every member), its per-member scales
+    // and the flags its passes write
+    mdx_ctx_t* net = nullptr;
+    double* net_scal = nullptr;      // 4 per member
+    int* learn_ok = nullptr;         // per member
 };
 
 namespace {
@@ -1018,18 +1103,50 @@ ens_args make_args(mdx_ensemble_t* E, int s, int momentum) {
     A.atol = E->opts.atol;
     A.mixed = E->opts.precision == MDX_PREC_MIXED && E->opts.tol > 0.0;
     A.inner_sor = E->opts.inner_sor;
+    A.split = 0;
+    A.learn_ok = E->learn_ok;
     return A;
 }
 
-int launch_substage(mdx_ensemble_t* E, int s, int momentum, int variant, int threads, int grid) {
+int launch_substage(mdx_ensemble_t* E, int s, int momentum, int variant, int threads, int grid, int split = 0) {
     ens_args A = make_args(E, s, momentum);
+    A.split = split;
     void* args[] = {&A};
     ENS_CUDA(E, cudaLaunchCooperativeKernel(kernel_of(variant), dim3(grid), dim3(threads), args, 0, E->stream));
     E->launches++;
     return MDX_OK;
 }
 
+bool learned_on(const mdx_ensemble_t* E) { return E->guess_mode == MDX_GUESS_LEARNED && E->net && E->opts.tol > 0.0; }
+
+// The network for every member, one after another on the ensemble's stream:
+// each pass reads the member's velocity after its extrapolated guess and its
+// last two increments (copied by part 1), and writes its correction and a
+// flag; part 2 uses them for the members that kept the extrapolated guess.
+int net_pass(mdx_ensemble_t* E, int s) {
+    double a[3], b[3], c[3];
+    rk_coeffs(a, b, c);
+    const long long l0 = E->net->launches;
+    for (int m = 0; m < E->n; ++m) {
+        const ens_member& M = E->hm[m];
+        const int rc = mdx_unet_member_delta(E->net, M.d, M.p.dx, M.p.dy, M.p.dz, M.dt * c[s], M.un, M.vn, M.wn, M.hl1,
+                                             M.hl2, M.ibm ? M.mu : nullptr, M.delta, E->net_scal + 4 * m,
+                                             E->learn_ok + m);
+        if (rc != MDX_OK) return efail(E, rc, "member %d network pass: %s", m, mdx_last_error(E->net));
+    }
+    E->launches += E->net->launches - l0;
+    return MDX_OK;
+}
+
 int step_eager(mdx_ensemble_t* E, int variant, int threads, int grid) {
+    if (learned_on(E)) {
+        for (int s = 0; s < 3; ++s) {
+            MDX_TRY(launch_substage(E, s, 1, variant, threads, grid, 1));
+            MDX_TRY(net_pass(E, s));
+            MDX_TRY(launch_substage(E, s, 1, variant, threads, grid, 2));
+        }
+        return MDX_OK;
+    }
     for (int s = 0; s < 3; ++s) MDX_TRY(launch_substage(E, s, 1, variant, threads, grid));
     return MDX_OK;
 }
@@ -1158,6 +1275,7 @@ int mdx_ensemble_destroy(mdx_ensemble_t* E) {
     cudaSetDevice(E->device);
     if (E->stream) cudaStreamSynchronize(E->stream);
     free_graph(E);
+    if (E->net) mdx_destroy(E->net);
     for (void* p : E->allocs) cudaFree(p);
     for (char* p : E->shadow) cudaFree(p);
     for (int q = 0; q < 7; ++q) cudaFree(E->dtiles[q]);
@@ -1345,8 +1463,13 @@ int mdx_ensemble_create(int device, int n, const mdx_member_t* members, const md
 
 int mdx_ensemble_set_guess(mdx_ensemble_t* E, int mode) {
     if (!E) return MDX_ERR_ARG;
-    if (mode != MDX_GUESS_ZERO && mode != MDX_GUESS_PREVIOUS && mode != MDX_GUESS_EXTRAPOLATED)
-        return efail(E, MDX_ERR_ARG, "ensemble guess mode %d: zero, previous or extrapolated", mode);
+    if (mode != MDX_GUESS_ZERO && mode != MDX_GUESS_PREVIOUS && mode != MDX_GUESS_EXTRAPOLATED &&
+        mode != MDX_GUESS_LEARNED)
+        return efail(E, MDX_ERR_ARG, "ensemble guess mode %d: zero, previous, extrapolated or learned", mode);
+    if (mode == MDX_GUESS_LEARNED && !E->net)
+        return efail(E, MDX_ERR_STATE, "learned guess: load a network first (mdx_ensemble_unet_load)");
+    if (mode == MDX_GUESS_LEARNED && !(E->opts.tol > 0.0))
+        return efail(E, MDX_ERR_ARG, "learned guess: needs a residual tolerance (tol > 0)");
     E->guess_mode = mode;
     free_graph(E);
     return MDX_OK;
@@ -1403,6 +1526,81 @@ int mdx_ensemble_ic(mdx_ensemble_t* E) {
     return MDX_OK;
 }
 
+int mdx_ensemble_unet_load(mdx_ensemble_t* E, const mdx_unet_opts_t* opts, const float* params, long long n,
+                           double out_scale) {
+    if (!E || !params) return MDX_ERR_ARG;
+    ENS_CUDA(E, cudaSetDevice(E->device));
+    ENS_CUDA(E, cudaStreamSynchronize(E->stream));
+    free_graph(E);
+    // the member with the most cells gives the network's grid (sizes are
+    // multiples of 16, so it has the most cells at every level too)
+    int big = 0;
+    for (int m = 1; m < E->n; ++m)
+        if (E->hm[m].d.nint > E->hm[big].d.nint) big = m;
+    for (int m = 0; m < E->n; ++m) {
+        const mdx_dims& d = E->hm[m].d;
+        if (d.nx % 8 || d.ny % 8 || d.nz % 8)
+            return efail(E, MDX_ERR_ARG, "learned guess: member %d sizes must be multiples of 8", m);
+    }
+    if (!E->net) {
+        const mdx_member_t& q = E->members[big];
+        mdx_grid_t g;
+        mdx_default_grid(&g);
+        g.nx = q.nx;
+        g.ny = q.ny;
+        g.nz = q.nz;
+        g.lx = q.lx;
+        g.ly = q.ly;
+        g.lz = q.lz;
+        g.dx = q.lx / q.nx;
+        g.dy = q.ly / q.ny;
+        g.dz = q.lz / q.nz;
+        g.re = q.re;
+        g.dt = q.dt;
+        mdx_bc_t bc;
+        mdx_default_bc(&bc);
+        bc.is_periodic[1] = E->hm[big].bc.per[1];
+        mdx_ctx_t* net = nullptr;
+        int rc = mdx_create(E->device, &g, &bc, &net);
+        if (rc != MDX_OK) return efail(E, rc, "learned guess: network context: %s", mdx_last_error(nullptr));
+        E->net = net;
+        rc = mdx_enter_field_data(net, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                                  nullptr);
+        if (rc == MDX_OK) rc = mdx_set_stream(net, (void*)E->stream);
+        if (rc == MDX_OK) rc = mdx_unet_create(net, opts);
+        if (rc != MDX_OK) return efail(E, rc, "learned guess: network: %s", mdx_last_error(net));
+        MDX_TRY(ealloc(E, &E->net_scal, 4 * (size_t)E->n));
+        MDX_TRY(ealloc(E, &E->learn_ok, (size_t)E->n));
+        for (int m = 0; m < E->n; ++m) {
+            ens_member& M = E->hm[m];
+            const size_t ni = (size_t)M.d.nint;
+            MDX_TRY(ealloc(E, &M.hl1, ni));
+            MDX_TRY(ealloc(E, &M.hl2, ni));
+            MDX_TRY(ealloc(E, &M.delta, ni));
+        }
+        ENS_CUDA(E, cudaMemcpy(E->dm, E->hm.data(), sizeof(ens_member) * E->n, cudaMemcpyHostToDevice));
+    }
+    int rc = mdx_unet_set_params(E->net, params, n);
+    if (rc == MDX_OK) rc = mdx_unet_set_out_scale(E->net, out_scale);
+    if (rc != MDX_OK) return efail(E, rc, "learned guess: parameters: %s", mdx_last_error(E->net));
+    ENS_CUDA(E, cudaStreamSynchronize(E->stream));
+    return MDX_OK;
+}
+
+int mdx_ensemble_unet_stats(mdx_ensemble_t* E, long long* corrections, long long* rejected) {
+    if (!E) return MDX_ERR_ARG;
+    std::vector<ens_state> h;
+    MDX_TRY(read_stats(E, h));
+    long long c = 0, r = 0;
+    for (const auto& S : h) {
+        c += S.lr_corr;
+        r += S.lr_rej;
+    }
+    if (corrections) *corrections = c;
+    if (rejected) *rejected = r;
+    return MDX_OK;
+}
+
 int mdx_ensemble_config(mdx_ensemble_t* E, int threads, int blocks_per_sm, int low_regs) {
     if (!E) return MDX_ERR_ARG;
     const int variant = low_regs ? 1 : 0;
@@ -1439,6 +1637,7 @@ int mdx_ensemble_step(mdx_ensemble_t* E, int nsteps, long long* total_iters) {
             ENS_CUDA(E, cudaStreamBeginCapture(E->stream, cudaStreamCaptureModeThreadLocal));
             const long long l0 = E->launches;
             int rc = step_eager(E, E->variant, E->threads, E->grid);
+            E->graph_launches = E->launches - l0;   // kernels one replay runs
             E->launches = l0;
             cudaError_t e = cudaStreamEndCapture(E->stream, &g);
             if (rc != MDX_OK || e != cudaSuccess || !g || cudaGraphInstantiate(&E->graph, g, 0) != cudaSuccess) {
@@ -1450,7 +1649,7 @@ int mdx_ensemble_step(mdx_ensemble_t* E, int nsteps, long long* total_iters) {
         }
         if (E->graph) {
             ENS_CUDA(E, cudaGraphLaunch(E->graph, E->stream));
-            E->launches += 3;
+            E->launches += E->graph_launches;
         } else {
             MDX_TRY(step_eager(E, E->variant, E->threads, E->grid));
         }

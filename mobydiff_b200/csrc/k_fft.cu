@@ -171,9 +171,10 @@ __device__ C2* smem_fft(C2* A, C2* B, int n, int nlines, int ls, const mdx_fft_p
 // ---------------------------------------------------------------------------
 template <typename C2>
 __global__ void __launch_bounds__(256)
-k_div_fftx(mdx_dims d, int R, double dx, double dy, double dz, double dt_gamma, const double* __restrict__ us,
+k_div_fftx(mdx_dims d, int R, double dx, double dy, double dz, mdx_dscal dgs, const double* __restrict__ us,
            const double* __restrict__ vs, const double* __restrict__ ws, C2* __restrict__ spec,
            mdx_fft_plan pl, const C2* __restrict__ twx) {
+    const double dt_gamma = dgs.get();
     typedef typename cx<C2>::R RT;
     extern __shared__ __align__(16) unsigned char sm_raw[];
     C2* sm = reinterpret_cast<C2*>(sm_raw);
@@ -540,9 +541,10 @@ template <typename C2> __device__ __forceinline__ void cp_async_elem(C2* dst, co
 // build_fft_rhs + forward real FFT along x, one warp per (k, j) row; M = nx/2 = 32 P.
 template <int P, typename C2>
 __global__ void __launch_bounds__(256, P >= 16 ? 2 : 4)
-k_div_fftx_w(mdx_dims d, double dx, double dy, double dz, double dt_gamma, const double* __restrict__ us,
+k_div_fftx_w(mdx_dims d, double dx, double dy, double dz, mdx_dscal dgs, const double* __restrict__ us,
              const double* __restrict__ vs, const double* __restrict__ ws, C2* __restrict__ spec,
              const C2* __restrict__ twx) {
+    const double dt_gamma = dgs.get();
     typedef typename cx<C2>::R RT;
     constexpr int M = 32 * P;
     extern __shared__ __align__(16) unsigned char sm_raw[];
@@ -678,10 +680,11 @@ k_ifftx_w(mdx_dims d, typename cx<C2>::R scale, const C2* __restrict__ spec, typ
 // ---------------------------------------------------------------------------
 template <bool IBM>
 __global__ void __launch_bounds__(256)
-k_correct(mdx_dims d, double dx, double dy, double dz, double dt_gamma, const double* __restrict__ phi,
+k_correct(mdx_dims d, double dx, double dy, double dz, mdx_dscal dgs, const double* __restrict__ phi,
           const double* __restrict__ us, const double* __restrict__ vs, const double* __restrict__ ws,
           double* __restrict__ un, double* __restrict__ vn, double* __restrict__ wn, double* __restrict__ pn,
           const double* __restrict__ cu, const double* __restrict__ cv, const double* __restrict__ cw) {
+    const double dt_gamma = dgs.get();
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     const int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
@@ -702,6 +705,136 @@ k_correct(mdx_dims d, double dx, double dy, double dz, double dt_gamma, const do
     }
     un[c] = u;
     wn[c] = w;
+    pn[c] = pn[c] + r;
+    if (j >= 2) {
+        double v = (__ldg(vs + c) - dt_gamma * (r - __ldg(phi + ridx(d, i, k, j - 1))) / dy);
+        if (IBM) v = v / (1.0 + dt_gamma * __ldg(cv + c));
+        vn[c] = v;
+    }
+}
+
+// Forward real FFT along x of each row of rhs(nx, nz, ny): rows r =
+// (k-1) + nz*(j-1) of nx reals -> nx/2+1 complex in plane_hat order.
+__global__ void __launch_bounds__(256)
+k_fftx_r2c(mdx_dims d, int R, const double* __restrict__ rhs, double2* __restrict__ spec, mdx_fft_plan pl,
+           const double2* __restrict__ twx) {
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    double2* sm = reinterpret_cast<double2*>(sm_raw);
+    const int M = d.nx / 2;
+    double2* A = sm;
+    double2* B = sm + R * M;
+    const int nrows = d.nz * d.ny;
+    const int row0 = blockIdx.x * R;
+    for (int t = threadIdx.x; t < R * M; t += blockDim.x) {
+        const int rl = t / M, n = t - rl * M;
+        const int row = row0 + rl;
+        A[rl * M + n] = (row < nrows) ? make_double2(__ldg(rhs + (long long)row * d.nx + 2 * n),
+                                                     __ldg(rhs + (long long)row * d.nx + 2 * n + 1))
+                                      : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    double2* Z = smem_fft<false>(A, B, M, R, M, pl, twx, 2);
+    const int nxh = M + 1;
+    for (int t = threadIdx.x; t < R * nxh; t += blockDim.x) {
+        const int rl = t / nxh, kx = t - rl * nxh;
+        const int row = row0 + rl;
+        if (row >= nrows) continue;
+        const double2 zk = Z[rl * M + (kx == M ? 0 : kx)];
+        const double2 zc = cconj(Z[rl * M + (kx == 0 ? 0 : M - kx)]);
+        const double2 e = make_double2(0.5 * (zk.x + zc.x), 0.5 * (zk.y + zc.y));
+        const double2 o = cmul_mi(make_double2(0.5 * (zk.x - zc.x), 0.5 * (zk.y - zc.y)));
+        spec[(long long)row * nxh + kx] = cadd(e, cmul(__ldg(twx + kx), o));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Walls in x or z on the FFT path.  With a wall (pressure Neumann) in x, the
+// red-black method keeps the wall faces u(1), u(nx+1) at their boundary
+// values and makes every cell divergence-free: the correction solves the
+// pressure equation with a Neumann condition at both x faces.  That problem
+// of length nx is the periodic one of length 2 nx on the even extension
+// (mirror the right-hand side about each wall): the extension's solution is
+// even, its ghost cells equal the cells they mirror, and the modified
+// wavenumbers 4/dx^2 sin^2(pi k / 2nx) of length 2 nx are the cosine
+// transform's eigenvalues.  So the periodic transforms solve it exactly on
+// the extended grid dfft; the correction then leaves the wall faces alone.
+// ---------------------------------------------------------------------------
+
+// rhs(i,k,j) = div(u*)/dt_gamma on the physical grid, the faces as the
+// boundary routine left them (build_fft_rhs's expression,
+// pressure_solver.f90:77-115).
+__global__ void k_div_rhs(mdx_dims d, double dx, double dy, double dz, mdx_dscal dgs, const double* __restrict__ us,
+                          const double* __restrict__ vs, const double* __restrict__ ws, double* __restrict__ rhs) {
+    const double dt_gamma = dgs.get();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
+    if (i > d.nx || j > d.ny || k > d.nz) return;
+    const long long c = pidx(d, i, j, k);
+    rhs[ridx(d, i, k, j)] = ((__ldg(us + c + 1) - __ldg(us + c)) / dx + (__ldg(vs + c + d.nxp) - __ldg(vs + c)) / dy +
+                             (__ldg(ws + c + (long long)d.nxp * d.nyp) - __ldg(ws + c)) / dz) / dt_gamma;
+}
+
+// The extension: cell I of the solve grid is cell I (I <= n) or its mirror
+// 2n + 1 - I of the physical grid in a direction with walls.
+__global__ void k_extend(mdx_dims d, mdx_dims e, const double* __restrict__ rhs, double* __restrict__ ext) {
+    const long long n = (long long)e.nx * e.nz * e.ny;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int I = (int)(t % e.nx) + 1;
+        const long long r = t / e.nx;
+        const int K = (int)(r % e.nz) + 1;
+        const int j = (int)(r / e.nz) + 1;
+        const int i = I <= d.nx ? I : 2 * d.nx + 1 - I;
+        const int k = K <= d.nz ? K : 2 * d.nz + 1 - K;
+        ext[t] = __ldg(rhs + ridx(d, i, k, j));
+    }
+}
+
+// phi of the physical cells: the first nx x nz block of each plane.
+__global__ void k_restrict(mdx_dims d, mdx_dims e, const double* __restrict__ ext, double* __restrict__ phi) {
+    const long long n = d.nint;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % d.nx) + 1;
+        const long long r = t / d.nx;
+        const int k = (int)(r % d.nz) + 1;
+        const int j = (int)(r / d.nz) + 1;
+        phi[t] = __ldg(ext + ridx(e, i, k, j));
+    }
+}
+
+// apply_fft_pressure_correction (pressure_solver.f90:117-173) with walls in
+// x (WX) or z (WZ): a wall face u(1) / w(1) keeps its boundary value (no
+// correction), as the red-black sweeps leave it; other faces as k_correct.
+template <bool IBM, bool WX, bool WZ>
+__global__ void __launch_bounds__(256)
+k_correct_walls(mdx_dims d, double dx, double dy, double dz, mdx_dscal dgs, const double* __restrict__ phi,
+                const double* __restrict__ us, const double* __restrict__ vs, const double* __restrict__ ws,
+                double* __restrict__ un, double* __restrict__ vn, double* __restrict__ wn, double* __restrict__ pn,
+                const double* __restrict__ cu, const double* __restrict__ cv, const double* __restrict__ cw) {
+    const double dt_gamma = dgs.get();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
+    if (i > d.nx || j > d.ny || k > d.nz) return;
+    int im = i - 1, km = k - 1;
+    if (im < 1) im = d.nx;
+    if (km < 1) km = d.nz;
+    const long long c = pidx(d, i, j, k);
+    const double r = __ldg(phi + ridx(d, i, k, j));
+    if (WX && i == 1) {
+        un[c] = __ldg(us + c);
+    } else {
+        double u = (__ldg(us + c) - dt_gamma * (r - __ldg(phi + ridx(d, im, k, j))) / dx);
+        if (IBM) u = u / (1.0 + dt_gamma * __ldg(cu + c));
+        un[c] = u;
+    }
+    if (WZ && k == 1) {
+        wn[c] = __ldg(ws + c);
+    } else {
+        double w = (__ldg(ws + c) - dt_gamma * (r - __ldg(phi + ridx(d, i, km, j))) / dz);
+        if (IBM) w = w / (1.0 + dt_gamma * __ldg(cw + c));
+        wn[c] = w;
+    }
     pn[c] = pn[c] + r;
     if (j >= 2) {
         double v = (__ldg(vs + c) - dt_gamma * (r - __ldg(phi + ridx(d, i, k, j - 1))) / dy);
@@ -764,7 +897,7 @@ template <typename C2> static int fft_warp_attrs(mdx_ctx_t* ctx) {
 // The three transform passes of a projection, warp-shuffle where the length
 // allows and opts.fft_kernel is 0, shared-memory Stockham otherwise.
 template <typename C2>
-static int launch_div_fftx(mdx_ctx_t* ctx, const char* what, double dg, C2* spec, const C2* twx) {
+static int launch_div_fftx(mdx_ctx_t* ctx, const char* what, mdx_dscal dg, C2* spec, const C2* twx) {
     const mdx_dims& d = ctx->d;
     const mdx_grid_t& g = ctx->g;
     double** f = ctx->f;
@@ -823,55 +956,96 @@ static int launch_ifftx(mdx_ctx_t* ctx, const char* what, typename cx<C2>::R sca
     return MDX_OK;
 }
 
+// Walls in x or z: the pressure boundary condition must be Neumann (type 1,
+// value 0) on both faces of that direction, and y must have walls with
+// Neumann pressure (the Thomas solve).  Returns MDX_OK and sets the flags.
+static int fft_wall_setup(mdx_ctx_t* ctx) {
+    const mdx_bc_t& b = ctx->bc;
+    ctx->fft_ext_x = b.is_periodic[0] ? 0 : 1;
+    ctx->fft_ext_z = b.is_periodic[2] ? 0 : 1;
+    if (!ctx->fft_ext_x && !ctx->fft_ext_z) return MDX_OK;
+    auto neumann_p = [&](int dir) {
+        return b.bc_type[bci(dir, 0, 0)] == 1 && b.bc_value[bci(dir, 0, 0)] == 0.0 && b.bc_type[bci(dir, 1, 0)] == 1 &&
+               b.bc_value[bci(dir, 1, 0)] == 0.0;
+    };
+    for (int dir : {1, 3})
+        if (!b.is_periodic[dir - 1] && !neumann_p(dir))
+            return mdx_fail(ctx, MDX_ERR_ARG,
+                            "FFT solver: a non-periodic %c direction needs Neumann pressure (type 1, value 0) on both "
+                            "faces (the red-black solver takes other pressure conditions)", dir == 1 ? 'x' : 'z');
+    if (b.is_periodic[1] || !neumann_p(2))
+        return mdx_fail(ctx, MDX_ERR_ARG, "FFT solver with walls in x or z: y needs walls with Neumann pressure");
+    if (ctx->opts.precision == MDX_PREC_MIXED)
+        return mdx_fail(ctx, MDX_ERR_ARG, "FFT solver: mixed precision needs periodic x and z");
+    return MDX_OK;
+}
+
 int mdx_fft_init(mdx_ctx_t* ctx) {
     const mdx_dims& d = ctx->d;
     if (d.nx % 2 != 0)
         return mdx_fail(ctx, MDX_ERR_ARG, "FFT solver: nx must be even (nx=%d)", d.nx);
+    MDX_TRY(fft_wall_setup(ctx));
+    // the solve grid: twice the length in a direction with walls
+    mdx_dims e = d;
+    e.nx = ctx->fft_ext_x ? 2 * d.nx : d.nx;
+    e.nz = ctx->fft_ext_z ? 2 * d.nz : d.nz;
+    e.nxp = e.nx + 2;
+    e.nzp = e.nz + 2;
+    e.nxh = e.nx / 2 + 1;
+    e.npad = (long long)e.nxp * e.nyp * e.nzp;
+    e.nint = (long long)e.nx * e.ny * e.nz;
+    e.nspec = (long long)e.nxh * e.nz * e.ny;
+    e.hs = split_stride(e.nx);
+    ctx->dfft = e;
+    const mdx_dims& D = e;
     bool ok1 = false, ok2 = false;
-    mdx_fft_make_plan(d.nx / 2, &ctx->plan_xh, &ok1);
-    mdx_fft_make_plan(d.nz, &ctx->plan_z, &ok2);
+    mdx_fft_make_plan(D.nx / 2, &ctx->plan_xh, &ok1);
+    mdx_fft_make_plan(D.nz, &ctx->plan_z, &ok2);
     if (!ok1 || !ok2)
-        return mdx_fail(ctx, MDX_ERR_ARG, "FFT solver: nx/2=%d and nz=%d must factor into 2,3,5,7", d.nx / 2, d.nz);
-    if (d.nx / 2 > 4096 || d.nz > 4096)
-        return mdx_fail(ctx, MDX_ERR_ARG, "FFT solver: nx/2 and nz must be <= 4096");
+        return mdx_fail(ctx, MDX_ERR_ARG, "FFT solver: nx/2=%d and nz=%d (solve grid) must factor into 2,3,5,7",
+                        D.nx / 2, D.nz);
+    if (D.nx / 2 > 4096 || D.nz > 4096)
+        return mdx_fail(ctx, MDX_ERR_ARG, "FFT solver: nx/2 and nz of the solve grid must be <= 4096");
     std::vector<double2> tx, tz;
-    mdx_fft_twiddles(d.nx, tx);
-    mdx_fft_twiddles(d.nz, tz);
-    MDX_CUDA(ctx, cudaMalloc(&ctx->tw_x, sizeof(double2) * d.nx));
-    MDX_CUDA(ctx, cudaMalloc(&ctx->tw_z, sizeof(double2) * d.nz));
-    MDX_CUDA(ctx, cudaMemcpy(ctx->tw_x, tx.data(), sizeof(double2) * d.nx, cudaMemcpyHostToDevice));
-    MDX_CUDA(ctx, cudaMemcpy(ctx->tw_z, tz.data(), sizeof(double2) * d.nz, cudaMemcpyHostToDevice));
-    MDX_CUDA(ctx, cudaMalloc(&ctx->spec, sizeof(double2) * d.nspec));
+    mdx_fft_twiddles(D.nx, tx);
+    mdx_fft_twiddles(D.nz, tz);
+    MDX_CUDA(ctx, cudaMalloc(&ctx->tw_x, sizeof(double2) * D.nx));
+    MDX_CUDA(ctx, cudaMalloc(&ctx->tw_z, sizeof(double2) * D.nz));
+    MDX_CUDA(ctx, cudaMemcpy(ctx->tw_x, tx.data(), sizeof(double2) * D.nx, cudaMemcpyHostToDevice));
+    MDX_CUDA(ctx, cudaMemcpy(ctx->tw_z, tz.data(), sizeof(double2) * D.nz, cudaMemcpyHostToDevice));
+    MDX_CUDA(ctx, cudaMalloc(&ctx->spec, sizeof(double2) * D.nspec));
     if (!ctx->f[MDX_PHI]) {
         MDX_CUDA(ctx, cudaMalloc(&ctx->f[MDX_PHI], sizeof(double) * d.nint));
         MDX_CUDA(ctx, cudaMemset(ctx->f[MDX_PHI], 0, sizeof(double) * d.nint));
     }
+    if (ctx->fft_ext_x || ctx->fft_ext_z) MDX_CUDA(ctx, cudaMalloc(&ctx->phi_ext, sizeof(double) * D.nint));
 
-    // Modified wavenumbers on the host with libm sin, pressure_fft.f90:53,61.
+    // Modified wavenumbers on the host with libm sin, pressure_fft.f90:53,61
+    // (of the solve grid's lengths).
     const double pi = 3.141592653589793;
-    const int nzh = d.nz / 2 + 1;
-    std::vector<double> kxp(d.nxh), kzp(d.nz);
-    for (int ikx = 1; ikx <= d.nxh; ++ikx) {
+    const int nzh = D.nz / 2 + 1;
+    std::vector<double> kxp(D.nxh), kzp(D.nz);
+    for (int ikx = 1; ikx <= D.nxh; ++ikx) {
         const int kx = ikx - 1;
-        const double s = std::sin(pi * (double)kx / (double)d.nx);
+        const double s = std::sin(pi * (double)kx / (double)D.nx);
         kxp[ikx - 1] = (4.0 / (ctx->g.dx * ctx->g.dx)) * (s * s);
     }
-    for (int ikz = 1; ikz <= d.nz; ++ikz) {
-        const int kz = (ikz <= d.nz / 2 + 1) ? ikz - 1 : ikz - d.nz - 1;
-        const double s = std::sin(pi * (double)kz / (double)d.nz);
+    for (int ikz = 1; ikz <= D.nz; ++ikz) {
+        const int kz = (ikz <= D.nz / 2 + 1) ? ikz - 1 : ikz - D.nz - 1;
+        const double s = std::sin(pi * (double)kz / (double)D.nz);
         kzp[ikz - 1] = (4.0 / (ctx->g.dz * ctx->g.dz)) * (s * s);
     }
     double *dkx = nullptr, *dkz = nullptr;
-    MDX_CUDA(ctx, cudaMalloc(&dkx, sizeof(double) * d.nxh));
-    MDX_CUDA(ctx, cudaMalloc(&dkz, sizeof(double) * d.nz));
-    MDX_CUDA(ctx, cudaMemcpy(dkx, kxp.data(), sizeof(double) * d.nxh, cudaMemcpyHostToDevice));
-    MDX_CUDA(ctx, cudaMemcpy(dkz, kzp.data(), sizeof(double) * d.nz, cudaMemcpyHostToDevice));
-    const long long tsize = (long long)d.ny * d.nxh * nzh;
+    MDX_CUDA(ctx, cudaMalloc(&dkx, sizeof(double) * D.nxh));
+    MDX_CUDA(ctx, cudaMalloc(&dkz, sizeof(double) * D.nz));
+    MDX_CUDA(ctx, cudaMemcpy(dkx, kxp.data(), sizeof(double) * D.nxh, cudaMemcpyHostToDevice));
+    MDX_CUDA(ctx, cudaMemcpy(dkz, kzp.data(), sizeof(double) * D.nz, cudaMemcpyHostToDevice));
+    const long long tsize = (long long)D.ny * D.nxh * nzh;
     MDX_CUDA(ctx, cudaMalloc(&ctx->thomas_dinv, sizeof(double) * tsize));
     MDX_CUDA(ctx, cudaMalloc(&ctx->thomas_cp, sizeof(double) * tsize));
     const double dyi2 = 1.0 / (ctx->g.dy * ctx->g.dy);
-    const int nm = d.nxh * nzh;
-    k_thomas_tables<<<(nm + 127) / 128, 128, 0, ctx->stream>>>(d.nxh, nzh, d.ny, dyi2, dkx, dkz, ctx->thomas_dinv,
+    const int nm = D.nxh * nzh;
+    k_thomas_tables<<<(nm + 127) / 128, 128, 0, ctx->stream>>>(D.nxh, nzh, D.ny, dyi2, dkx, dkz, ctx->thomas_dinv,
                                                               ctx->thomas_cp);
     int rc = mdx_check_launch(ctx, "thomas tables");
     MDX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
@@ -879,14 +1053,15 @@ int mdx_fft_init(mdx_ctx_t* ctx) {
     cudaFree(dkz);
     if (rc != MDX_OK) return rc;
 
-    const int M = d.nx / 2;
+    const int M = D.nx / 2;
     const size_t smx = sizeof(double2) * 2 * rows_per_block(M) * M;
-    const size_t smz = sizeof(double2) * 2 * ztile(d.nz) * (d.nz + 1);
+    const size_t smz = sizeof(double2) * 2 * ztile(D.nz) * (D.nz + 1);
     MDX_CUDA(ctx, cudaFuncSetAttribute(k_div_fftx<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx));
+    MDX_CUDA(ctx, cudaFuncSetAttribute(k_fftx_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx));
     MDX_CUDA(ctx, cudaFuncSetAttribute(k_ifftx<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx));
     MDX_CUDA(ctx, cudaFuncSetAttribute(k_fftz<false, double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz));
     MDX_CUDA(ctx, cudaFuncSetAttribute(k_fftz<true, double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz));
-    MDX_TRY(fft_warp_attrs<double2>(ctx));
+    if (!ctx->fft_ext_x && !ctx->fft_ext_z) MDX_TRY(fft_warp_attrs<double2>(ctx));
     return MDX_OK;
 }
 
@@ -904,11 +1079,67 @@ void mdx_fft_free(mdx_ctx_t* ctx) {
     cudaFree(ctx->tw_z); ctx->tw_z = nullptr;
     cudaFree(ctx->thomas_dinv); ctx->thomas_dinv = nullptr;
     cudaFree(ctx->thomas_cp); ctx->thomas_cp = nullptr;
+    cudaFree(ctx->phi_ext); ctx->phi_ext = nullptr;
+    ctx->fft_ext_x = ctx->fft_ext_z = 0;
+}
+
+// The projection with walls in x or z: divergence on the physical grid,
+// its even extension, the Stockham transforms, Thomas and the inverse on the
+// solve grid, the physical block of phi, the correction.
+static int projection_fft_walls(mdx_ctx_t* ctx, mdx_dscal dg) {
+    const mdx_dims& d = ctx->d;
+    const mdx_dims& e = ctx->dfft;
+    const mdx_grid_t& g = ctx->g;
+    double** f = ctx->f;
+    dim3 block(32, 4, 2);
+    dim3 grid((d.nx + 31) / 32, (d.ny + 3) / 4, (d.nz + 1) / 2);
+    MDX_LAUNCH(ctx, MDX_T_FFT_FWD, "div rhs", k_div_rhs, grid, block, 0, d, g.dx, g.dy, g.dz, dg, f[MDX_US], f[MDX_VS],
+               f[MDX_WS], f[MDX_PHI]);
+    const int nb = (int)std::min<long long>((e.nint + 255) / 256, 8192);
+    MDX_LAUNCH(ctx, MDX_T_FFT_FWD, "extend rhs", k_extend, nb, 256, 0, d, e, f[MDX_PHI], ctx->phi_ext);
+    const int M = e.nx / 2, R = rows_per_block(M), nrows = e.nz * e.ny;
+    const size_t smx = sizeof(double2) * 2 * R * M;
+    MDX_LAUNCH(ctx, MDX_T_FFT_FWD, "fft x (extended)", k_fftx_r2c, (nrows + R - 1) / R, 256, smx, e, R, ctx->phi_ext,
+               ctx->spec, ctx->plan_xh, ctx->tw_x);
+    const int TX = ztile(e.nz);
+    const size_t smz = sizeof(double2) * 2 * TX * (e.nz + 1);
+    const int zblocks = ((e.nxh + TX - 1) / TX) * e.ny;
+    MDX_LAUNCH(ctx, MDX_T_FFT_FWD, "fft z (extended)", (k_fftz<false, double2>), zblocks, 256, smz, e, TX, ctx->spec,
+               ctx->plan_z, ctx->tw_z);
+    const int nm = e.nxh * e.nz;
+    MDX_LAUNCH(ctx, MDX_T_THOMAS, "thomas (extended)", (k_thomas<double2, false>), (nm + 127) / 128, 128, 0, e,
+               1.0 / (g.dy * g.dy), ctx->spec, ctx->thomas_dinv, ctx->thomas_cp);
+    MDX_LAUNCH(ctx, MDX_T_FFT_INV, "ifft z (extended)", (k_fftz<true, double2>), zblocks, 256, smz, e, TX, ctx->spec,
+               ctx->plan_z, ctx->tw_z);
+    MDX_LAUNCH(ctx, MDX_T_FFT_INV, "ifft x (extended)", k_ifftx<double2>, (nrows + R - 1) / R, 256, smx, e, R,
+               1.0 / (double)((long long)e.nx * e.nz), ctx->spec, ctx->phi_ext, ctx->plan_xh, ctx->tw_x);
+    const int nbd = (int)std::min<long long>((d.nint + 255) / 256, 8192);
+    MDX_LAUNCH(ctx, MDX_T_FFT_INV, "restrict phi", k_restrict, nbd, 256, 0, d, e, ctx->phi_ext, f[MDX_PHI]);
+    auto go = [&](auto kern) -> int {
+        MDX_LAUNCH(ctx, MDX_T_CORRECT, "correction (walls)", kern, grid, block, 0, d, g.dx, g.dy, g.dz, dg, f[MDX_PHI],
+                   f[MDX_US], f[MDX_VS], f[MDX_WS], f[MDX_UN], f[MDX_VN], f[MDX_WN], f[MDX_PN], f[MDX_COEF_U],
+                   f[MDX_COEF_V], f[MDX_COEF_W]);
+        return MDX_OK;
+    };
+    const bool ibm = !ctx->ibm_zero, wx = ctx->fft_ext_x, wz = ctx->fft_ext_z;
+    if (ibm) {
+        if (wx && wz) return go(k_correct_walls<true, true, true>);
+        if (wx) return go(k_correct_walls<true, true, false>);
+        return go(k_correct_walls<true, false, true>);
+    }
+    if (wx && wz) return go(k_correct_walls<false, true, true>);
+    if (wx) return go(k_correct_walls<false, true, false>);
+    return go(k_correct_walls<false, false, true>);
 }
 
 // pressure_projection of the FFT builds, pressure_solver.f90:58-61.
-int mdx_k_projection_fft(mdx_ctx_t* ctx, double dg) {
-    if (ctx->opts.precision == MDX_PREC_MIXED) return mdx_k_projection_fft_mixed(ctx, dg);
+int mdx_k_projection_fft(mdx_ctx_t* ctx, mdx_dscal dg) {
+    if (!ctx->spec) return mdx_fail(ctx, MDX_ERR_STATE, "FFT solver workspace missing (its set-up failed)");
+    if (ctx->fft_ext_x || ctx->fft_ext_z) return projection_fft_walls(ctx, dg);
+    if (ctx->opts.precision == MDX_PREC_MIXED) {
+        if (dg.p) return mdx_fail(ctx, MDX_ERR_STATE, "device-resident dt needs the FP64 FFT path");
+        return mdx_k_projection_fft_mixed(ctx, dg.v);
+    }
     const mdx_dims& d = ctx->d;
     const mdx_grid_t& g = ctx->g;
     double** f = ctx->f;
@@ -1158,40 +1389,6 @@ static __device__ __align__(256) unsigned char mdx_noalloc_scratch[MDX_NOALLOC_S
 
 static std::mutex g_noalloc_mu;
 static void* g_noalloc_addr[MDX_NOALLOC_MAX_DEVICES] = {nullptr};
-
-// Forward real FFT along x of each row of rhs(nx, nz, ny): rows r =
-// (k-1) + nz*(j-1) of nx reals -> nx/2+1 complex in plane_hat order.
-__global__ void __launch_bounds__(256)
-k_fftx_r2c(mdx_dims d, int R, const double* __restrict__ rhs, double2* __restrict__ spec, mdx_fft_plan pl,
-           const double2* __restrict__ twx) {
-    extern __shared__ __align__(16) unsigned char sm_raw[];
-    double2* sm = reinterpret_cast<double2*>(sm_raw);
-    const int M = d.nx / 2;
-    double2* A = sm;
-    double2* B = sm + R * M;
-    const int nrows = d.nz * d.ny;
-    const int row0 = blockIdx.x * R;
-    for (int t = threadIdx.x; t < R * M; t += blockDim.x) {
-        const int rl = t / M, n = t - rl * M;
-        const int row = row0 + rl;
-        A[rl * M + n] = (row < nrows) ? make_double2(__ldg(rhs + (long long)row * d.nx + 2 * n),
-                                                     __ldg(rhs + (long long)row * d.nx + 2 * n + 1))
-                                      : make_double2(0.0, 0.0);
-    }
-    __syncthreads();
-    double2* Z = smem_fft<false>(A, B, M, R, M, pl, twx, 2);
-    const int nxh = M + 1;
-    for (int t = threadIdx.x; t < R * nxh; t += blockDim.x) {
-        const int rl = t / nxh, kx = t - rl * nxh;
-        const int row = row0 + rl;
-        if (row >= nrows) continue;
-        const double2 zk = Z[rl * M + (kx == M ? 0 : kx)];
-        const double2 zc = cconj(Z[rl * M + (kx == 0 ? 0 : M - kx)]);
-        const double2 e = make_double2(0.5 * (zk.x + zc.x), 0.5 * (zk.y + zc.y));
-        const double2 o = cmul_mi(make_double2(0.5 * (zk.x - zc.x), 0.5 * (zk.y - zc.y)));
-        spec[(long long)row * nxh + kx] = cadd(e, cmul(__ldg(twx + kx), o));
-    }
-}
 
 static size_t noalloc_align(size_t b) { return (b + 255) & ~(size_t)255; }
 

@@ -126,6 +126,129 @@ k_sor_sweep32(mdx_dims d, mixed_params P, int parity, int reverse, float* __rest
     sweep32_cell<PY>(d, P, i, j, k, du, dv, dw, dp, r, mu32, fac32);
 }
 
+// V consecutive FP32 values at p (16-byte aligned for V = 4, 8-byte for V = 2).
+template <int V>
+__device__ __forceinline__ void ld_vec(float (&a)[V], const float* p) {
+    if constexpr (V == 4) {
+        const float4 q = *reinterpret_cast<const float4*>(p);
+        a[0] = q.x; a[1] = q.y; a[2] = q.z; a[3] = q.w;
+    } else {
+        const float2 q = *reinterpret_cast<const float2*>(p);
+        a[0] = q.x; a[1] = q.y;
+    }
+}
+template <int V>
+__device__ __forceinline__ void ld_vec_ro(float (&a)[V], const float* __restrict__ p) {
+    if constexpr (V == 4) {
+        const float4 q = __ldg(reinterpret_cast<const float4*>(p));
+        a[0] = q.x; a[1] = q.y; a[2] = q.z; a[3] = q.w;
+    } else {
+        const float2 q = __ldg(reinterpret_cast<const float2*>(p));
+        a[0] = q.x; a[1] = q.y;
+    }
+}
+template <int V>
+__device__ __forceinline__ void st_vec(float* p, const float (&a)[V]) {
+    if constexpr (V == 4) *reinterpret_cast<float4*>(p) = make_float4(a[0], a[1], a[2], a[3]);
+    else *reinterpret_cast<float2*>(p) = make_float2(a[0], a[1]);
+}
+
+// One FP32 colour sweep with V consecutive cells of the swept colour per
+// thread (V = 2 or 4), on the colour-split arrays.  Window w of a row is the
+// positions V w .. V w + V - 1 (rows start on 16-byte boundaries).  A thread
+// owns its window in the swept colour's half of row (j, k) and in the other
+// half's rows (j + 1, k) and (j, k + 1) -- the lower faces of its y and z
+// neighbours -- and moves each with one vector load and store, writing back
+// unchanged the positions that hold no swept cell (the row's ends and its
+// padding).  The x neighbours' faces u(i+1) sit one position to the right
+// in rows whose swept cells have odd i (the window plus one scalar), and at
+// the window's own positions in the others, except the periodic wrap of
+// cell nx to position 0; they are written with scalar stores, one per cell.
+// The arithmetic is sweep32_update, so the result is k_sor_sweep32's bit for
+// bit.  Needs nx and nz even, and ny even when y is periodic (every neighbour
+// has the other colour).
+template <int PY, int V>
+__global__ void __launch_bounds__(256)
+k_sor_sweep32v(mdx_dims d, mixed_params P, int parity, int reverse, int nwin, float* __restrict__ du,
+               float* __restrict__ dv, float* __restrict__ dw, float* __restrict__ dp, const float* __restrict__ r,
+               const float* __restrict__ mu32, const float* __restrict__ fac32) {
+    const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long per_plane = (long long)nwin * d.ny;
+    if (g >= per_plane * d.nz) return;
+    const int kk = (int)(g / per_plane);
+    const int rem = (int)(g - (long long)kk * per_plane);
+    const int j = rem / nwin + 1;
+    const int p0 = V * (rem - (j - 1) * nwin);
+    const int k = reverse ? d.nz - kk : kk + 1;
+    const int cs = 1 - parity;            // colour (i + j + k) & 1 of the swept cells
+    const int eo = (cs + j + k) & 1;      // i & 1 of the swept cells of this row
+    const int half = d.nx / 2;            // position of the last cell of a row
+    const int jp = (PY && j == d.ny) ? 1 : j + 1;
+    const int kp = (k == d.nz) ? 1 : k + 1;
+    const long long H = (long long)d.hs * d.nyp * d.nzp;
+    const long long own = cs * H + ((long long)k * d.nyp + j) * d.hs + p0;
+    const long long oth = (1 - cs) * H + ((long long)k * d.nyp + j) * d.hs;
+    const long long ojp = (1 - cs) * H + ((long long)k * d.nyp + jp) * d.hs + p0;
+    const long long okp = (1 - cs) * H + ((long long)kp * d.nyp + j) * d.hs + p0;
+    const int PH = d.hs * d.nyp, np = 2 * PH;
+    const int hp = (eo + j) & 1;          // (i + j) & 1: the factor planes' half of the swept cells
+    const int mown = hp * PH + j * d.hs + p0;
+    const int mox = (1 - hp) * PH + j * d.hs;
+    const int mjp = (1 - hp) * PH + jp * d.hs + p0;
+
+    float u0[V], ux[V], v0[V], vy[V], w0[V], wz[V], q[V], rr[V];
+    float mu_u[V], mu_ux[V], mu_v[V], mu_vy[V], mu_w[V], fc[V];
+    ld_vec<V>(u0, du + own);
+    ld_vec<V>(v0, dv + own);
+    ld_vec<V>(w0, dw + own);
+    ld_vec<V>(q, dp + own);
+    ld_vec<V>(ux, du + oth + p0);
+    ld_vec<V>(vy, dv + ojp);
+    ld_vec<V>(wz, dw + okp);
+    ld_vec_ro<V>(rr, r + own);
+    ld_vec_ro<V>(mu_u, mu32 + mown);
+    ld_vec_ro<V>(mu_v, mu32 + np + mown);
+    ld_vec_ro<V>(mu_w, mu32 + 2 * np + mown);
+    ld_vec_ro<V>(fc, fac32 + mown);
+    ld_vec_ro<V>(mu_ux, mu32 + mox + p0);
+    ld_vec_ro<V>(mu_vy, mu32 + np + mjp);
+    // the x-neighbour face one past the window (odd i), or the wrap target
+    // position 0 of cell nx (even i)
+    const int xe = eo ? p0 + V : 0;
+    const bool need_xe = eo ? (p0 + V < d.hs) : (half >= p0 && half < p0 + V);
+    float uxe = 0.f, muxe = 0.f;
+    if (need_xe) {
+        uxe = du[oth + xe];
+        muxe = __ldg(mu32 + mox + xe);
+    }
+    const bool v_lo = PY || j > 1, v_hi = PY || j < d.ny;   // wall faces v(1), v(ny+1) stay 0
+#pragma unroll
+    for (int e = 0; e < V; ++e) {
+        const int p = p0 + e;
+        const bool valid = eo ? (p < half) : (p >= 1 && p <= half);
+        const bool wrap = !eo && p == half;
+        float uip, muip;
+        if (e + 1 < V) {
+            uip = eo ? ux[e + 1 < V ? e + 1 : e] : (wrap ? uxe : ux[e]);
+            muip = eo ? mu_ux[e + 1 < V ? e + 1 : e] : (wrap ? muxe : mu_ux[e]);
+        } else {
+            uip = (eo || wrap) ? uxe : ux[e];
+            muip = (eo || wrap) ? muxe : mu_ux[e];
+        }
+        if (valid) {
+            sweep32_update(P, rr[e], u0[e], uip, v0[e], vy[e], w0[e], wz[e], q[e], mu_u[e], muip, mu_v[e],
+                           mu_vy[e], mu_w[e], fc[e], v_lo, v_hi);
+            du[oth + (eo ? p + 1 : (wrap ? 0 : p))] = uip;
+        }
+    }
+    st_vec<V>(du + own, u0);
+    st_vec<V>(dv + own, v0);
+    st_vec<V>(dw + own, w0);
+    st_vec<V>(dp + own, q);
+    st_vec<V>(dv + ojp, vy);
+    st_vec<V>(dw + okp, wz);
+}
+
 // ---------------------------------------------------------------------------
 // Fused red+black pass: one launch per red-black iteration of the FP32
 // correction sweeps, with the result of the two colour sweeps bit for bit.
@@ -515,17 +638,27 @@ int mdx_k_projection_redblack_mixed(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t
         return MDX_OK;
     };
     // Inner sweeps: the colour sweeps (one launch per colour) when asked
-    // for; otherwise the autotuner's choice among the fused red+black pass's
-    // tile shapes and the colour sweeps, each timed on one block of
-    // iterations of the first projections (all give the same bits).
-    const bool tune_all = o.sor_variant != MDX_SORV_SWEEPS;
-    const bool fused_only = o.sor_variant == MDX_SORV_FUSED8 || o.sor_variant == MDX_SORV_FUSED16;
-    const int ncand = fused_only ? RB32_SHAPES : RB32_SHAPES + 1;
-    if (tune_all && !ctx->tune_ev[0]) {
+    // for; otherwise the autotuner's choice among its candidates (the fused
+    // red+black pass's tile shapes, the colour sweeps, the vector colour
+    // sweeps), each timed on one block of iterations of the first
+    // projections (all give the same bits).
+    enum { CAND_SWEEPS = RB32_SHAPES, CAND_VEC2, CAND_VEC4, CAND_NUM };
+    int cands[CAND_NUM], ncand = 0;
+    if (o.sor_variant == MDX_SORV_SWEEPS) {
+        cands[ncand++] = CAND_SWEEPS;
+    } else if (o.sor_variant == MDX_SORV_FUSED8 || o.sor_variant == MDX_SORV_FUSED16) {
+        for (int c = 0; c < RB32_SHAPES; ++c) cands[ncand++] = c;
+    } else if (o.sor_variant == MDX_SORV_SPLIT) {
+        cands[ncand++] = CAND_VEC2;
+        cands[ncand++] = CAND_VEC4;
+    } else {
+        for (int c = 0; c < CAND_NUM; ++c) cands[ncand++] = c;
+    }
+    if (ncand > 1 && !ctx->tune_ev[0]) {
         MDX_CUDA(ctx, cudaEventCreate(&ctx->tune_ev[0]));
         MDX_CUDA(ctx, cudaEventCreate(&ctx->tune_ev[1]));
     }
-    bool used_fused = false;
+    int used_kind = 1;   // 1 colour sweeps, 3 fused pass, 5 vector colour sweeps
     auto colour_sweeps = [&](int iters) -> int {
         const int na = d.nx / 2;
         dim3 block(32, 4, 2);
@@ -538,26 +671,42 @@ int mdx_k_projection_redblack_mixed(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t
             }
         return MDX_OK;
     };
+    auto vector_sweeps = [&](int iters, int V) -> int {
+        const int nwin = (d.nx / 2 + V) / V;   // windows covering positions 0 .. nx/2
+        const long long nthr = (long long)nwin * d.ny * d.nz;
+        const int nb = (int)((nthr + 255) / 256);
+        auto kfn = V == 4 ? (py ? k_sor_sweep32v<1, 4> : k_sor_sweep32v<0, 4>)
+                          : (py ? k_sor_sweep32v<1, 2> : k_sor_sweep32v<0, 2>);
+        for (int it = 0; it < iters; ++it)
+            for (int parity = 0; parity < 2; ++parity)
+                MDX_LAUNCH(ctx, MDX_T_SOR_SWEEP, "sor sweep fp32 vec", kfn, nb, 256, 0, d, P, parity, parity, nwin,
+                           ctx->mx_du, ctx->mx_dv, ctx->mx_dw, ctx->mx_dp, ctx->mx_r, ctx->mx_mu, ctx->mx_fac);
+        return MDX_OK;
+    };
     auto sweeps = [&](int iters) -> int {
         mdx_event_pair run{};
-        int cand = RB32_SHAPES;   // the colour sweeps
+        int cand = cands[0];
         bool tuning = false;
-        if (tune_all) {
+        int slot = 0;
+        if (ncand > 1) {
             cand = ctx->rb32_tuned - 1;
             tuning = cand < 0;
             if (tuning) {
-                cand = 0;
-                while (cand < ncand - 1 && ctx->rb32_tune_ms[cand] > 0.0) ++cand;
+                while (slot < ncand - 1 && ctx->rb32_tune_ms[cands[slot]] > 0.0) ++slot;
+                cand = cands[slot];
                 MDX_CUDA(ctx, cudaEventRecord(ctx->tune_ev[0], ctx->stream));
             }
         }
         mdx_sweep_run_begin(ctx, &run);
         if (cand < RB32_SHAPES) {
             for (int it = 0; it < iters; ++it) MDX_TRY(py ? rb32_launch<1>(ctx, cand, P) : rb32_launch<0>(ctx, cand, P));
-            used_fused = true;
-        } else {
+            used_kind = 3;
+        } else if (cand == CAND_SWEEPS) {
             MDX_TRY(colour_sweeps(iters));
-            used_fused = false;
+            used_kind = 1;
+        } else {
+            MDX_TRY(vector_sweeps(iters, cand == CAND_VEC4 ? 4 : 2));
+            used_kind = 5;
         }
         mdx_sweep_run_end(ctx, &run);
         if (tuning) {
@@ -566,10 +715,10 @@ int mdx_k_projection_redblack_mixed(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t
             float ms = 0.f;
             if (cudaEventElapsedTime(&ms, ctx->tune_ev[0], ctx->tune_ev[1]) == cudaSuccess && iters > 0)
                 ctx->rb32_tune_ms[cand] = ms > 0.f ? ms / iters : 1e-9;
-            if (cand == ncand - 1 && ctx->rb32_tune_ms[cand] > 0.0) {
-                int best = 0;
+            if (slot == ncand - 1 && ctx->rb32_tune_ms[cand] > 0.0) {
+                int best = cands[0];
                 for (int t = 1; t < ncand; ++t)
-                    if (ctx->rb32_tune_ms[t] < ctx->rb32_tune_ms[best]) best = t;
+                    if (ctx->rb32_tune_ms[cands[t]] < ctx->rb32_tune_ms[best]) best = cands[t];
                 ctx->rb32_tuned = best + 1;
             }
         }
@@ -624,8 +773,9 @@ int mdx_k_projection_redblack_mixed(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t
     }
     s.iterations = it;
     // mixed path: 100 + outer FP64 corrections with the colour sweeps, 300 +
-    // outer with the fused red+black pass
-    s.variant = (used_fused ? 300 : 100) + outer;
+    // outer with the fused red+black pass, 500 + outer with the vector
+    // colour sweeps
+    s.variant = 100 * used_kind + outer;
     ctx->last = s;
     if (st) *st = s;
     return MDX_OK;

@@ -20,9 +20,11 @@
 // ---------------------------------------------------------------------------
 constexpr int MOM_KZ = 8;
 
-template <bool IBM>
+// DTD: the three step scalars come from the device's dt (adaptive-dt graph);
+// otherwise their values are kernel parameters.
+template <bool IBM, bool DTD>
 __global__ void __launch_bounds__(256, 4)
-k_momentum(mdx_dims d, mdx_step_params p, double dt_alpha, double dt_beta, double dt_gamma,
+k_momentum(mdx_dims d, mdx_step_params p, mdx_dscal da, mdx_dscal db, mdx_dscal dg,
            const double* __restrict__ un, const double* __restrict__ vn, const double* __restrict__ wn,
            const double* __restrict__ pn, double* __restrict__ us, double* __restrict__ vs,
            double* __restrict__ ws, double* __restrict__ ou, double* __restrict__ ov, double* __restrict__ ow,
@@ -31,6 +33,8 @@ k_momentum(mdx_dims d, mdx_step_params p, double dt_alpha, double dt_beta, doubl
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     const int k0 = blockIdx.z * MOM_KZ + 1;
     if (i > d.nx || j > d.ny) return;
+    const double dt_alpha = DTD ? da.get() : da.v, dt_beta = DTD ? db.get() : db.v,
+                 dt_gamma = DTD ? dg.get() : dg.v;
     const int k1 = min(k0 + MOM_KZ - 1, d.nz);
     const long long SX = 1, SY = d.nxp, SZ = (long long)d.nxp * d.nyp;
     long long c = pidx(d, i, j, k0);
@@ -84,20 +88,18 @@ mdx_step_params mdx_make_params(const mdx_ctx_t* ctx) {
     return p;
 }
 
-int mdx_k_momentum(mdx_ctx_t* ctx, double da, double db, double dg) {
+int mdx_k_momentum(mdx_ctx_t* ctx, mdx_dscal da, mdx_dscal db, mdx_dscal dg) {
     const mdx_dims& d = ctx->d;
     dim3 block(32, 8, 1);
     dim3 grid((d.nx + 31) / 32, (d.ny + 7) / 8, (d.nz + MOM_KZ - 1) / MOM_KZ);
     mdx_step_params p = mdx_make_params(ctx);
     double** f = ctx->f;
-    if (ctx->ibm_zero)
-        MDX_LAUNCH(ctx, MDX_T_MOMENTUM, "momentum", k_momentum<false>, grid, block, 0, d, p, da, db, dg,
-                   f[MDX_UN], f[MDX_VN], f[MDX_WN], f[MDX_PN], f[MDX_US], f[MDX_VS], f[MDX_WS], f[MDX_OLDRHSU],
-                   f[MDX_OLDRHSV], f[MDX_OLDRHSW], f[MDX_COEF_U], f[MDX_COEF_V], f[MDX_COEF_W]);
-    else
-        MDX_LAUNCH(ctx, MDX_T_MOMENTUM, "momentum", k_momentum<true>, grid, block, 0, d, p, da, db, dg,
-                   f[MDX_UN], f[MDX_VN], f[MDX_WN], f[MDX_PN], f[MDX_US], f[MDX_VS], f[MDX_WS], f[MDX_OLDRHSU],
-                   f[MDX_OLDRHSV], f[MDX_OLDRHSW], f[MDX_COEF_U], f[MDX_COEF_V], f[MDX_COEF_W]);
+    const bool dev = da.p || db.p || dg.p;
+    auto kfn = ctx->ibm_zero ? (dev ? k_momentum<false, true> : k_momentum<false, false>)
+                             : (dev ? k_momentum<true, true> : k_momentum<true, false>);
+    MDX_LAUNCH(ctx, MDX_T_MOMENTUM, "momentum", kfn, grid, block, 0, d, p, da, db, dg, f[MDX_UN], f[MDX_VN],
+               f[MDX_WN], f[MDX_PN], f[MDX_US], f[MDX_VS], f[MDX_WS], f[MDX_OLDRHSU], f[MDX_OLDRHSV], f[MDX_OLDRHSW],
+               f[MDX_COEF_U], f[MDX_COEF_V], f[MDX_COEF_W]);
     return MDX_OK;
 }
 
@@ -178,9 +180,30 @@ __global__ void k_bc_periodic_z(mdx_dims d, mdx_six f) {   // boundary.f90:137-1
     }
 }
 
+__global__ void k_bcrb_y(mdx_dims d, mdx_bc_dev bc, double dy, mdx_four f);
+__global__ void k_bcrb_x(mdx_dims d, mdx_bc_dev bc, double dx, mdx_four f);
+__global__ void k_bcrb_z(mdx_dims d, mdx_bc_dev bc, double dz, mdx_four f);
+
 int mdx_k_apply_bc(mdx_ctx_t* ctx) {
     const mdx_dims& d = ctx->d;
     double** a = ctx->f;
+    if (ctx->fft_ext_x || ctx->fft_ext_z) {
+        // walls in x or z on the FFT path: the general boundary routine
+        // (apply_bc_redblack's face rules, which for walls in y with zero
+        // velocity give apply_bc's values) on u, v, w, p and on u*, v*, w*,
+        // whose wall faces the right-hand side reads
+        dim3 b(32, 8);
+        for (const mdx_four& f : {mdx_four{a[MDX_UN], a[MDX_VN], a[MDX_WN], a[MDX_PN]},
+                                  mdx_four{a[MDX_US], a[MDX_VS], a[MDX_WS], a[MDX_PN]}}) {
+            MDX_LAUNCH(ctx, MDX_T_BC, "apply_bc y (walls)", k_bcrb_y, dim3((d.nx + 31) / 32, (d.nz + 7) / 8), b, 0, d,
+                       ctx->bcd, ctx->g.dy, f);
+            MDX_LAUNCH(ctx, MDX_T_BC, "apply_bc x (walls)", k_bcrb_x, dim3((d.ny + 31) / 32, (d.nz + 7) / 8), b, 0, d,
+                       ctx->bcd, ctx->g.dx, f);
+            MDX_LAUNCH(ctx, MDX_T_BC, "apply_bc z (walls)", k_bcrb_z, dim3((d.nx + 31) / 32, (d.ny + 7) / 8), b, 0, d,
+                       ctx->bcd, ctx->g.dz, f);
+        }
+        return MDX_OK;
+    }
     mdx_six f{a[MDX_UN], a[MDX_VN], a[MDX_WN], a[MDX_US], a[MDX_VS], a[MDX_WS], a[MDX_PN]};
     dim3 b(32, 8);
     MDX_LAUNCH(ctx, MDX_T_BC, "apply_bc y", k_bc_walls_y, dim3((d.nxp + 31) / 32, (d.nzp + 7) / 8), b, 0, d, f);
@@ -384,7 +407,20 @@ int mdx_k_div_norms(mdx_ctx_t* ctx, const double* u, const double* v, const doub
 
 // get_cfl, src/modules/step.f90:210-258: max over the padded arrays of
 // |u/dx|, |v/dy|, |w/dz| (max is exact, so the result is order-independent).
-int mdx_k_cfl(mdx_ctx_t* ctx, double* cfl) {
+// After a step of the adaptive-dt path (src/main.f90:67,92-97), on the
+// device: t += dt (the step's dt), cfl = get_cfl's maximum (red[1]), and
+// when cflmax > 0 and cfl > 0, dt = min(cflmax/cfl, dtmax).  s = {dt, t, cfl}.
+__global__ void k_dt_update(const double* __restrict__ red, double* __restrict__ s, double cflmax, double dtmax) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const double dt = s[0];
+    s[1] = s[1] + dt;
+    const double cfl = red[1];
+    s[2] = cfl;
+    if (cflmax > 0.0 && cfl > 0.0) s[0] = fmin(cflmax / cfl, dtmax);
+}
+
+// get_cfl's reduction into red_out[1], left on the device.
+static int cfl_launch(mdx_ctx_t* ctx) {
     MDX_TRY(mdx_reduce_init(ctx));
     const mdx_dims& d = ctx->d;
     MDX_LAUNCH(ctx, MDX_T_OTHER, "cfl partials", k_cfl_partials, ctx->red_blocks, MDX_RED_THREADS, 0, d.npad,
@@ -392,6 +428,17 @@ int mdx_k_cfl(mdx_ctx_t* ctx, double* cfl) {
                ctx->red_part);
     MDX_LAUNCH(ctx, MDX_T_OTHER, "reduce final", k_reduce_final, 1, MDX_RED_THREADS, 0, ctx->red_blocks,
                ctx->red_part, ctx->red_out);
+    return MDX_OK;
+}
+
+int mdx_k_dt_update(mdx_ctx_t* ctx, double* s, double cflmax, double dtmax) {
+    MDX_TRY(cfl_launch(ctx));
+    MDX_LAUNCH(ctx, MDX_T_OTHER, "dt update", k_dt_update, 1, 32, 0, ctx->red_out, s, cflmax, dtmax);
+    return MDX_OK;
+}
+
+int mdx_k_cfl(mdx_ctx_t* ctx, double* cfl) {
+    MDX_TRY(cfl_launch(ctx));
     MDX_CUDA(ctx, cudaMemcpyAsync(ctx->red_host, ctx->red_out, 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     MDX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     *cfl = ctx->red_host[1];

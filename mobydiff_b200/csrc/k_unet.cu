@@ -485,7 +485,8 @@ __device__ __forceinline__ float head_dot(const bf16* a, const float* w, float b
 // Inference head: delta[v] (FP64) = (sum_c A[v][c] w[c] + b) * scale.
 template <int C0>
 __global__ void k_head_infer(long long n, const bf16* __restrict__ A, const float* __restrict__ wb, double scale,
-                             double* __restrict__ delta) {
+                             double* __restrict__ delta, const double* __restrict__ scal = nullptr) {
+    if (scal) scale = scal[2];   // the device-computed output scale (k_net_scales)
     __shared__ float w[C0 + 1];
     if (threadIdx.x <= C0) w[threadIdx.x] = wb[threadIdx.x];
     __syncthreads();
@@ -609,6 +610,55 @@ __global__ void __launch_bounds__(256) k_sum_field(long long n, const double* __
     }
 }
 
+// Along a correction delta applied once: per-block pairs of sum(delta d0)
+// and sum(delta (d1 - d0)), d0 = raw (the divergence before, FP32), d1 the
+// divergence of (u, v, w) now (the red-black neighbour rule).  With A =
+// -div(mu grad), applying delta changes the divergence by dt_gamma A delta =
+// d1 - d0, so -sum(delta d0) / sum(delta (d1 - d0)) is the step along delta
+// that minimises the energy norm of the pressure error.
+__global__ void __launch_bounds__(256) k_energy_dots(mdx_dims d, int pery, double idx, double idy, double idz,
+                                                     const double* __restrict__ u, const double* __restrict__ v,
+                                                     const double* __restrict__ w, const float* __restrict__ raw,
+                                                     const double* __restrict__ delta, double* __restrict__ part) {
+    double s0 = 0.0, s1 = 0.0;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < d.nint; t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % d.nx) + 1;
+        const long long r = t / d.nx;
+        const int j = (int)(r % d.ny) + 1;
+        const int k = (int)(r / d.ny) + 1;
+        const int ip = i + 1 > d.nx ? 1 : i + 1;
+        const int jp = (pery && j + 1 > d.ny) ? 1 : j + 1;
+        const int kp = k + 1 > d.nz ? 1 : k + 1;
+        const long long c = pidx(d, i, j, k);
+        const double d1 = (__ldg(u + pidx(d, ip, j, k)) - __ldg(u + c)) * idx +
+                          (__ldg(v + pidx(d, i, jp, k)) - __ldg(v + c)) * idy +
+                          (__ldg(w + pidx(d, i, j, kp)) - __ldg(w + c)) * idz;
+        const double d0 = (double)raw[t], dl = __ldg(delta + t);
+        s0 += dl * d0;
+        s1 += dl * (d1 - d0);
+    }
+    __shared__ double sh[2][8];
+    for (int o = 16; o > 0; o >>= 1) {
+        s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        sh[0][threadIdx.x >> 5] = s0;
+        sh[1][threadIdx.x >> 5] = s1;
+    }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+        double q = 0.0;
+        for (int i = 0; i < 8; ++i) q += sh[threadIdx.x][i];
+        part[2 * blockIdx.x + threadIdx.x] = q;
+    }
+}
+
+__global__ void k_scale(long long n, double* __restrict__ a, double c) {
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+        a[t] *= c;
+}
+
 __global__ void k_add_const(long long n, double* __restrict__ a, double c) {
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
         a[t] += c;
@@ -640,9 +690,16 @@ __global__ void k_sum_pairs(int nb, const double* __restrict__ part, double* __r
 
 // Normalised inputs: in[0] = raw*ir, in[1] = dp1*ip, in[2] = dp2*ip, in[3] =
 // IBM factor of the cell (mean of its three lower faces; 1 without IBM).
-__global__ void k_norm_in(mdx_dims d, int mu_mode, const float* __restrict__ raw, const double* __restrict__ dp1,
-                          const double* __restrict__ dp2, const double* __restrict__ mu, double ir, double ip,
-                          float* __restrict__ in) {
+// DEV: the two scales come from the device (scal[0], scal[1]), written by
+// k_net_scales, so that the pass needs no host read.
+template <bool DEV>
+__global__ void k_norm_in_t(mdx_dims d, int mu_mode, const float* __restrict__ raw, const double* __restrict__ dp1,
+                            const double* __restrict__ dp2, const double* __restrict__ mu, double ir, double ip,
+                            const double* __restrict__ scal, float* __restrict__ in) {
+    if (DEV) {
+        ir = scal[0];
+        ip = scal[1];
+    }
     const long long n = d.nint;
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
         in[t] = (float)(raw[t] * ir);
@@ -670,6 +727,30 @@ __global__ void k_norm_in(mdx_dims d, int mu_mode, const float* __restrict__ raw
         }
         in[3 * n + t] = m;
     }
+}
+
+// Input and output scales of one pass from the sums of div^2 and dp1^2 over
+// n cells (sums[0..1]): scal = {1/rms(div), 1/rms(dp1) (1 when 0), the
+// output scale out_scale rms(div) h^2 / dt_gamma}; *ok = 0 when the
+// divergence is zero or not finite (no correction).
+__global__ void k_net_scales(long long n, const double* __restrict__ sums, double out_scale, double h2, double dg,
+                             double* __restrict__ scal, int* __restrict__ ok) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    const double sr = sqrt(sums[0] / (double)n);
+    double sp = sqrt(sums[1] / (double)n);
+    const bool good = sr > 0.0 && isfinite(sr);
+    if (!(sp > 0.0) || !isfinite(sp)) sp = 1.0;
+    scal[0] = good ? 1.0 / sr : 0.0;
+    scal[1] = 1.0 / sp;
+    scal[2] = good ? out_scale * sr * h2 / dg : 0.0;
+    *ok = good ? 1 : 0;
+}
+
+// a[t] -= sums[0] / n (the mean from k_sum_pairs)
+__global__ void k_sub_mean(long long n, double* __restrict__ a, const double* __restrict__ sums) {
+    const double m = sums[0] / (double)n;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+        a[t] -= m;
 }
 
 // Snapshot target: (dp - g) * scale.
@@ -1159,13 +1240,13 @@ int mdx_unet_correct(mdx_ctx_t* ctx, double dg, double* rg) {
         U->pending = U->next;
         U->pending_scale = dg / (sr * h2);
     }
-    MDX_LAUNCH(ctx, MDX_T_OTHER, "unet inputs", k_norm_in, nblocks(n), 256, 0, d, ctx->mu_mode, U->raw, ctx->dp_hist[s],
-               ctx->dp_hist2[s], ctx->mu, 1.0 / sr, 1.0 / sp, dst);
+    MDX_LAUNCH(ctx, MDX_T_OTHER, "unet inputs", k_norm_in_t<false>, nblocks(n), 256, 0, d, ctx->mu_mode, U->raw,
+               ctx->dp_hist[s], ctx->dp_hist2[s], ctx->mu, 1.0 / sr, 1.0 / sp, (const double*)nullptr, dst);
     if (!learn) return MDX_OK;
     MDX_LAUNCH(ctx, MDX_T_OTHER, "unet pack", k_pack_in, nblocks(n), 256, 0, n, dst, U->x0);
     MDX_TRY(forward(ctx, U));
     MDX_LAUNCH(ctx, MDX_T_OTHER, "unet head", k_head_infer<16>, nblocks(n), 256, 0, n, U->act.back(),
-               U->param + U->head_off, U->out_scale * sr * h2 / dg, U->delta);
+               U->param + U->head_off, U->out_scale * sr * h2 / dg, U->delta, (const double*)nullptr);
     // A constant pressure increment moves no face (the red-black operator's
     // null space with periodic or Neumann pressure), so the solve never
     // removes one; a correction with a non-zero mean would shift p by a
@@ -1179,13 +1260,32 @@ int mdx_unet_correct(mdx_ctx_t* ctx, double dg, double* rg) {
                    -sum / (double)n);
     }
     MDX_TRY(mdx_apply_guess(ctx, U->delta, dg));
+    bool keep_by_energy = false;
+    if (U->o.step_rule == 1) {
+        // the energy-optimal step alpha along delta: apply (alpha - 1) delta
+        // more; kept when alpha > 0 (the error's energy norm then falls)
+        MDX_LAUNCH(ctx, MDX_T_OTHER, "unet energy dots", k_energy_dots, U->red_blocks, 256, 0, d, U->pery,
+                   1.0 / ctx->g.dx, 1.0 / ctx->g.dy, 1.0 / ctx->g.dz, ctx->f[MDX_UN], ctx->f[MDX_VN], ctx->f[MDX_WN],
+                   U->raw, U->delta, U->red_part);
+        double a = 0.0, b = 0.0;
+        MDX_TRY(pairs_to_host(ctx, U, U->red_blocks, &a, &b));
+        const double alpha = (b != 0.0) ? -a / b : 0.0;
+        U->st.last_step = alpha;
+        if (std::isfinite(alpha) && alpha > 0.0) {
+            keep_by_energy = true;
+            if (alpha != 1.0) {
+                MDX_LAUNCH(ctx, MDX_T_OTHER, "unet step scale", k_scale, nblocks(n), 256, 0, n, U->delta, alpha - 1.0);
+                MDX_TRY(mdx_apply_guess(ctx, U->delta, dg));
+            }
+        }
+    }
     MDX_CUDA(ctx, cudaEventRecord(U->ev[1], ctx->stream));
     double r = 0.0, linf = 0.0;
     MDX_TRY(mdx_k_div_norms(ctx, ctx->f[MDX_UN], ctx->f[MDX_VN], ctx->f[MDX_WN], &r, &linf));
     MDX_TRY(check_tc(ctx, U));
     float ms = 0.f;
     if (cudaEventElapsedTime(&ms, U->ev[0], U->ev[1]) == cudaSuccess) U->st.infer_ms = ms;
-    if (r < *rg) {
+    if (U->o.step_rule == 1 ? keep_by_energy : r < *rg) {
         U->st.corrections++;
         U->st.last_gain = r > 0.0 ? *rg / r : 0.0;
         *rg = r;
@@ -1196,6 +1296,49 @@ int mdx_unet_correct(mdx_ctx_t* ctx, double dg, double* rg) {
         MDX_TRY(mdx_apply_guess(ctx, ctx->guess, dg));
     }
     return MDX_OK;
+}
+
+// The learned correction for a grid other than the context's -- an ensemble
+// member -- with no host read, so that a CUDA graph can hold it: the
+// network (sized for the largest member) runs on the member's level sizes
+// (the activations are dense [z][y][x][c], so a grid with no more cells at
+// every level fits), the scales come from device reductions, and *ok
+// (device) says whether delta holds a correction.  Inputs are the member's
+// u, v, w after its extrapolated guess, its last two increments of this
+// substage and its IBM factor planes (or null).
+int mdx_unet_member_delta(mdx_ctx_t* nc, const mdx_dims& dm, double dx, double dy, double dz, double dg,
+                          const double* un, const double* vn, const double* wn, const double* dp1, const double* dp2,
+                          const double* mu_planes, double* delta, double* scal, int* ok) {
+    mdx_unet* U = static_cast<mdx_unet*>(nc->unet);
+    if (!U || !U->trained) return mdx_fail(nc, MDX_ERR_STATE, "ensemble network: no trained parameters");
+    if (dm.nx % 8 || dm.ny % 8 || dm.nz % 8) return mdx_fail(nc, MDX_ERR_ARG, "ensemble network: member sizes not multiples of 8");
+    if (dm.nint > U->L[0].n) return mdx_fail(nc, MDX_ERR_ARG, "ensemble network: member larger than the network's grid");
+    lvl saved[4];
+    for (int l = 0; l < 4; ++l) {
+        saved[l] = U->L[l];
+        U->L[l] = lvl{dm.nx >> l, dm.ny >> l, dm.nz >> l, (long long)(dm.nx >> l) * (dm.ny >> l) * (dm.nz >> l)};
+    }
+    const long long n = dm.nint;
+    const double h2 = 1.0 / (1.0 / (dx * dx) + 1.0 / (dy * dy) + 1.0 / (dz * dz));
+    auto run = [&]() -> int {
+        MDX_LAUNCH(nc, MDX_T_OTHER, "unet div field", k_div_field, U->red_blocks, 256, 0, dm, U->pery, 1.0 / dx, 1.0 / dy,
+                   1.0 / dz, un, vn, wn, dp1, U->raw, U->red_part);
+        MDX_LAUNCH(nc, MDX_T_OTHER, "unet sum pairs", k_sum_pairs, 1, 256, 0, U->red_blocks, U->red_part, U->red_out);
+        MDX_LAUNCH(nc, MDX_T_OTHER, "unet scales", k_net_scales, 1, 32, 0, n, U->red_out, U->out_scale, h2, dg, scal, ok);
+        MDX_LAUNCH(nc, MDX_T_OTHER, "unet inputs", k_norm_in_t<true>, nblocks(n), 256, 0, dm, mu_planes ? 1 : 0, U->raw,
+                   dp1, dp2, mu_planes, 0.0, 0.0, (const double*)scal, U->in);
+        MDX_LAUNCH(nc, MDX_T_OTHER, "unet pack", k_pack_in, nblocks(n), 256, 0, n, U->in, U->x0);
+        MDX_TRY(forward(nc, U));
+        MDX_LAUNCH(nc, MDX_T_OTHER, "unet head", k_head_infer<16>, nblocks(n), 256, 0, n, U->act.back(),
+                   U->param + U->head_off, 0.0, delta, (const double*)scal);
+        MDX_LAUNCH(nc, MDX_T_OTHER, "unet delta mean", k_sum_field, U->red_blocks, 256, 0, n, delta, U->red_part);
+        MDX_LAUNCH(nc, MDX_T_OTHER, "unet sum pairs", k_sum_pairs, 1, 256, 0, U->red_blocks, U->red_part, U->red_out);
+        MDX_LAUNCH(nc, MDX_T_OTHER, "unet delta zero mean", k_sub_mean, nblocks(n), 256, 0, n, delta, U->red_out);
+        return MDX_OK;
+    };
+    const int rc = run();
+    for (int l = 0; l < 4; ++l) U->L[l] = saved[l];
+    return rc;
 }
 
 // After the projection (dp_hist[s] = its increment): the pending snapshot's
@@ -1238,7 +1381,8 @@ int mdx_unet_create(mdx_ctx_t* ctx, const mdx_unet_opts_t* opts) {
     else mdx_default_unet_opts(&o);
     if (o.channels0 != 16 || (o.channels != 16 && o.channels != 32))
         return mdx_fail(ctx, MDX_ERR_ARG, "unet channels must be 16 and 16|32");
-    if (o.extra_bottleneck < 0 || o.extra_bottleneck > MAX_EXTRA || o.capacity < 0 || !(o.slope > 0.0) || o.slope > 1.0)
+    if (o.extra_bottleneck < 0 || o.extra_bottleneck > MAX_EXTRA || o.capacity < 0 || !(o.slope > 0.0) || o.slope > 1.0 ||
+        o.step_rule < 0 || o.step_rule > 1)
         return mdx_fail(ctx, MDX_ERR_ARG, "unet options out of range");
     const mdx_dims& d = ctx->d;
     if (d.nx % 8 || d.ny % 8 || d.nz % 8) return mdx_fail(ctx, MDX_ERR_ARG, "unet needs nx, ny, nz multiples of 8");

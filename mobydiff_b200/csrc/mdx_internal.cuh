@@ -24,10 +24,12 @@ struct mdx_dims {
     long long npad;      // (nx+2)(ny+2)(nz+2)
     long long nint;      // nx*ny*nz
     long long nspec;     // nxh*nz*ny
-    int hs;              // row length of the colour-split layout, (nx+2)/2
+    int hs;              // row length of the colour-split layout, (nx+2)/2 rounded up to a multiple of 4
 };
 
-__host__ __device__ inline int split_stride(int nx) { return (nx + 2) / 2; }
+// Rows of the colour-split layout start on 16-byte boundaries (FP32), so
+// that a colour sweep can move four consecutive cells with one vector access.
+__host__ __device__ inline int split_stride(int nx) { return ((nx + 2) / 2 + 3) & ~3; }
 
 __host__ __device__ inline long long pidx(const mdx_dims& d, int i, int j, int k) {
     return (long long)i + (long long)d.nxp * ((long long)j + (long long)d.nyp * (long long)k);
@@ -41,11 +43,12 @@ __host__ __device__ inline long long ridx(const mdx_dims& d, int i, int k, int j
 
 // Colour-split layout (the mixed path's FP32 arrays, the FP64 sweeps' working
 // copies, the ensemble's FP32 arrays): element (i, j, k) of the padded grid
-// lives in half (i + j + k) & 1 at (k (ny+2) + j) hs + i/2, hs = (nx+2)/2,
+// lives in half (i + j + k) & 1 at (k (ny+2) + j) hs + i/2, hs >= (nx+2)/2,
 // so the cells of one colour in a row -- and the faces they own or share --
 // are consecutive: every access of a colour sweep is unit-stride.  A face
 // belongs to the cell on its high side (u(i) to cell i).  nx is even, so
-// (nx+2)/2 is whole.
+// (nx+2)/2 is whole; positions (nx+2)/2 .. hs-1 of a row are padding that
+// holds no element.
 __host__ __device__ __forceinline__ long long cidx(const mdx_dims& d, int i, int j, int k) {
     return ((i + j + k) & 1) * ((long long)d.hs * d.nyp * d.nzp) + ((long long)k * d.nyp + j) * d.hs + (i >> 1);
 }
@@ -63,6 +66,21 @@ __host__ __device__ inline int split_plane_elems(const mdx_dims& d) { return 2 *
 enum {
     MDX_SORV_AUTO = 0, MDX_SORV_SWEEPS = 1, MDX_SORV_FUSED8 = 2, MDX_SORV_FUSED16 = 3, MDX_SORV_SPLIT = 4,
     MDX_SORV_NUM = 5
+};
+
+// A step scalar (dt times an RK coefficient) handed to a kernel either by
+// value or, on the adaptive-dt path, as the address of the device's dt and
+// the coefficient, so that a CUDA graph replays the step with the dt the
+// device computed after the step before.  get() is the one FP64 multiply
+// dt * coefficient that the host does otherwise.
+struct mdx_dscal {
+    double v = 0.0;
+    const double* p = nullptr;
+    double m = 0.0;
+    mdx_dscal() = default;
+    __host__ __device__ mdx_dscal(double x) : v(x) {}
+    __host__ __device__ mdx_dscal(const double* dt, double coef) : p(dt), m(coef) {}
+    __device__ __forceinline__ double get() const { return p ? *p * m : v; }
 };
 
 // Scalars of one time step, passed by value to kernels.
@@ -120,7 +138,8 @@ struct mdx_ctx {
     void* mx_base = nullptr;
     size_t mx_bytes = 0;
     int rb32_tuned = 0;                      // FP32 inner sweeps: candidate + 1 chosen by the autotuner (0: not yet;
-                                             // candidates: the fused pass's tile shapes, then the colour sweeps)
+                                             // candidates: the fused pass's 4 tile shapes, the colour sweeps, the
+                                             // vector colour sweeps with 2 and 4 cells per thread)
     unsigned rb32_attr = 0;                  // fused FP32 pass: shared-memory attribute set, bit per kernel
     double rb32_tune_ms[8] = {0.0};          // time per iteration per candidate
     // warm starts: increments of the last projection of each RK substage
@@ -151,6 +170,13 @@ struct mdx_ctx {
     double2* tw_z = nullptr;                 // exp(-2 pi i t/nz), t < nz
     mdx_fft_plan plan_xh{};                  // complex length nx/2 (packed real transform)
     mdx_fft_plan plan_z{};                   // complex length nz
+    // FFT path with walls in x or z (pressure Neumann there): the pressure
+    // equation is solved on the even extension of the grid in those
+    // directions, periodic of twice the length; the workspace above is then
+    // sized for dfft instead of d
+    int fft_ext_x = 0, fft_ext_z = 0;
+    mdx_dims dfft{};                         // the solve grid (d itself without walls in x and z)
+    double* phi_ext = nullptr;               // right-hand side, then phi, on dfft in rhs(i,k,j) order
     // mixed-precision FFT path: FP32 spectrum, correction, twiddles, Thomas
     // tables; FP64 zero-wavenumber right-hand side and solution per y
     float2 *spec32 = nullptr, *tw_x32 = nullptr, *tw_z32 = nullptr;
@@ -169,6 +195,13 @@ struct mdx_ctx {
     cudaGraphExec_t step_graph = nullptr;
     double graph_dt = 0.0;
     long long graph_launches = 0;
+    // adaptive-dt FFT step: {dt, t_current, cfl} on the device, read by the
+    // step's kernels and updated by its last kernel; the graph of one step
+    // and the cflmax / dtmax it was captured with
+    double* dt_dev = nullptr;
+    cudaGraphExec_t adapt_graph = nullptr;
+    double adapt_cflmax = 0.0, adapt_dtmax = 0.0;
+    long long adapt_launches = 0;
 
     // timing: 0 off, 1 sampled launches + sweep runs, 2 sweep runs only
     int timing = 0;
@@ -249,12 +282,12 @@ int mdx_check_launch(mdx_ctx_t* ctx, const char* what);
 
 // ---- per-module entry points (internal) --------------------------------------
 mdx_step_params mdx_make_params(const mdx_ctx_t* ctx);
-int mdx_k_momentum(mdx_ctx_t* ctx, double da, double db, double dg);
+int mdx_k_momentum(mdx_ctx_t* ctx, mdx_dscal da, mdx_dscal db, mdx_dscal dg);
 int mdx_k_apply_bc(mdx_ctx_t* ctx);
 int mdx_k_apply_bc_redblack(mdx_ctx_t* ctx);
 int mdx_fft_init(mdx_ctx_t* ctx);
 void mdx_fft_free(mdx_ctx_t* ctx);
-int mdx_k_projection_fft(mdx_ctx_t* ctx, double dg);
+int mdx_k_projection_fft(mdx_ctx_t* ctx, mdx_dscal dg);
 int mdx_k_projection_fft_mixed(mdx_ctx_t* ctx, double dg);
 int mdx_k_projection_redblack(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t* st);
 int mdx_k_div_norms(mdx_ctx_t* ctx, const double* u, const double* v, const double* w, double* l2, double* linf,
@@ -283,9 +316,15 @@ int mdx_guess_apply(mdx_ctx_t* ctx, double dg, double r0, bool* guessed, double*
 // learned correction of an applied extrapolated guess and snapshot capture (k_unet.cu)
 int mdx_unet_correct(mdx_ctx_t* ctx, double dg, double* rg);
 int mdx_unet_finish(mdx_ctx_t* ctx, bool converged);
+// The learned correction for another grid (an ensemble member), no host read
+// (k_unet.cu): delta and its flag *ok on the device.
+int mdx_unet_member_delta(mdx_ctx_t* nc, const mdx_dims& dm, double dx, double dy, double dz, double dg,
+                          const double* un, const double* vn, const double* wn, const double* dp1, const double* dp2,
+                          const double* mu_planes, double* delta, double* scal, int* ok);
 void mdx_unet_free(mdx_ctx_t* ctx);
 int mdx_k_div_norms_async(mdx_ctx_t* ctx, const double* u, const double* v, const double* w);
 int mdx_k_cfl(mdx_ctx_t* ctx, double* cfl);
+int mdx_k_dt_update(mdx_ctx_t* ctx, double* s, double cflmax, double dtmax);
 int mdx_k_center_vel(mdx_ctx_t* ctx, double* uc, double* vc, double* wc);
 int mdx_k_channel_ic(mdx_ctx_t* ctx, uint64_t seed, double amp_u, double amp_vw, const double* yc_host);
 int mdx_k_fill(mdx_ctx_t* ctx, double* p, long long n, double v);

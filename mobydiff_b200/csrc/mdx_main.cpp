@@ -153,36 +153,31 @@ int main(int argc, char** argv) {
         CHECK(ctx, mdx_channel_ic(ctx, run.seed, 0.1, 0.01, ic_y0, wave, lam, &st));
     }
 
-    double ra[3] = {64.0 / 120.0, 50.0 / 120.0, 90.0 / 120.0};   // step.f90:21-23
-    double rb[3] = {0.0, -34.0 / 120.0, -50.0 / 120.0};
-    double rg[3] = {64.0 / 120.0, 16.0 / 120.0, 40.0 / 120.0};
-
     std::printf(" main loop starting...\n");
     std::fflush(stdout);
     auto t0 = std::chrono::steady_clock::now();
     long long total_iters = 0;
-    for (int i = 1; i <= g.nsteps; ++i) {
-        g.t_current = g.t_current + g.dt;
-        for (int s = 0; s < 3; ++s) {
-            const double da = g.dt * ra[s], db = g.dt * rb[s], dg = g.dt * rg[s];
-            CHECK(ctx, mdx_momentum(ctx, da, db, dg));
-            if (opts.solver == MDX_SOLVER_FFT) CHECK(ctx, mdx_apply_bc(ctx));
-            mdx_solve_stats_t st;
-            CHECK(ctx, mdx_pressure_projection(ctx, dg, opts.solver == MDX_SOLVER_REDBLACK ? &st : nullptr));
-            if (opts.solver == MDX_SOLVER_REDBLACK) {
-                total_iters += st.iterations;
-                CHECK(ctx, mdx_apply_bc_redblack(ctx));
-            } else {
-                CHECK(ctx, mdx_apply_bc(ctx));
-            }
-        }
-        const bool need_cfl = (g.cflmax > 0.0) || output_is_due(i, run.output_interval);   // main.f90:92-97
-        if (need_cfl) CHECK(ctx, mdx_get_cfl(ctx, &g.cfl));
-        if (g.cflmax > 0.0 && g.cfl > 0.0) g.dt = std::fmin(g.cflmax / g.cfl, g.dtmax);
+    // src/main.f90:66-106.  The steps up to the next output run in one
+    // mdx_step_adaptive call: t += dt, the three substages, then with
+    // cflmax > 0 the CFL and dt = min(cflmax/cfl, dtmax) after every step
+    // (on the FFT path inside the step's CUDA graph, on the device).
+    auto next_due = [](int i, int interval) { return interval > 0 ? ((i + interval - 1) / interval) * interval : 0; };
+    for (int i = 1; i <= g.nsteps;) {
+        int last = g.nsteps;
+        if (run.output_interval > 0) last = std::min(last, next_due(i, run.output_interval));
+        if (run.field_interval > 0) last = std::min(last, next_due(i, run.field_interval));
+        long long it = 0;
+        CHECK(ctx, mdx_step_adaptive(ctx, last - i + 1, g.cflmax, g.dtmax, &it));
+        total_iters += it;
+        CHECK(ctx, mdx_get_time(ctx, &g.dt, &g.t_current, &g.cfl));
+        i = last;
+        // main.f90:92-93: the CFL is also computed when output is due
+        if (!(g.cflmax > 0.0) && output_is_due(i, run.output_interval)) CHECK(ctx, mdx_get_cfl(ctx, &g.cfl));
         if (run.output_interval > 0 && output_is_due(i, run.output_interval))
             CHECK(ctx, write_vtk(ctx, g, i, run.output_prefix));
         if (run.field_interval > 0 && output_is_due(i, run.field_interval))   // io.f90:95-137
             CHECK(ctx, write_field(ctx, g, i, run.field_prefix));
+        ++i;
     }
     double dummy = 0.0;
     CHECK(ctx, mdx_divergence_norms(ctx, &dummy, &dummy));   // drains the stream

@@ -95,8 +95,10 @@ def record_and_train(s: Solver, g, runs, warm_steps: int = 3, record_steps: int 
                       snapshots=int(st.snapshots), record_seconds=rec, train_ms=tm + st.train_ms, runs=list(runs))
 
 
-def load_into(s: Solver, net: TrainedNet) -> None:
-    """Give solver `s` (same grid) the trained network, without snapshot storage."""
-    s.unet_create(channels=net.channels, extra_bottleneck=net.extra_bottleneck, capacity=0, slope=net.slope)
+def load_into(s: Solver, net: TrainedNet, step_rule: int = 0) -> None:
+    """Give solver `s` (same grid) the trained network, without snapshot
+    storage; step_rule 1 scales each correction by its energy-optimal step."""
+    s.unet_create(channels=net.channels, extra_bottleneck=net.extra_bottleneck, capacity=0, slope=net.slope,
+                  step_rule=step_rule)
     s.unet_set_params(net.params)
     s.unet_out_scale(net.out_scale)

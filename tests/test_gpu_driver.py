@@ -109,3 +109,57 @@ seed = 5
                 for a, b, c in zip(uc.ravel(), vc.ravel(), wc.ravel())]
         assert lines[12:12 + len(body)] == body
         assert lines[12 + len(body):] == [""]
+
+
+@pytest.mark.gpu
+def test_driver_adaptive_dt(tmp_path):
+    """cflmax > 0 in input.ini: the driver's steps take dt = min(cflmax/cfl,
+    dtmax) after every step (src/main.f90:92-97), computed on the device; the
+    field file's dt and t_current and its state match the oracle's adaptive
+    loop."""
+    ini = tmp_path / "input.ini"
+    ini.write_text("""
+[grid]
+nx = 32
+ny = 16
+nz = 16
+lx = 6.283185307179586
+ly = 2.0
+lz = 3.141592653589793
+[flow]
+re = 2000.0
+forcing_x = 1e-3
+[time]
+dt = 1e-3
+nsteps = 5
+cflmax = 0.02
+dtmax = 5e-3
+[boundary]
+periodic_y = no
+y_min_p_type = neumann
+y_max_p_type = neumann
+[output]
+h5_interval = 5
+field_prefix = chk
+[b200]
+ic = channel
+seed = 5
+""")
+    r = subprocess.run([MAIN, str(ini)], cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    h = M.h5_read_header(str(tmp_path / "chk_5.h5"))
+    g, bc = channel_case(32, 16, 16, re=2000.0, dt=1e-3)
+    g.forcing = (1e-3, 0.0, 0.0)
+    f = O.Fields(g)
+    O.set_ibm_coeff(g, O.ibm_reference(g), f)
+    oracle_channel_ic(g, bc, f, 5)
+    dt, t = 1e-3, 0.0
+    for _ in range(5):
+        t += dt
+        O.run(g, bc, f, dt, 1, solver=0)
+        dt = min(0.02 / O.get_cfl(g, f), 5e-3)
+    assert dt != 1e-3
+    assert abs(h["t_current"] - t) <= 1e-12 * t and abs(h["dt"] - dt) <= 1e-10 * dt
+    fields = M.h5_read_field(str(tmp_path / "chk_5.h5"), 32, 16, 16)
+    for n, a in zip(("un", "vn", "wn", "pn"), fields):
+        assert rel_l2(a, getattr(f, n)) <= 1e-10, n

@@ -159,3 +159,80 @@ def test_mixed_precision_members_match_single_channels():
                     assert (num / den) ** 0.5 <= 1e-6, q          # the velocity vector
                     for n in ("un", "vn", "wn"):                  # each component, v and w of small norm
                         assert rel_l2(E.get(q, n), other(n)) <= 1e-5, (q, n)
+
+
+def test_sixteen_uneven_members_bitwise_and_mixed():
+    """16 members of uneven sizes drawn like the 64-member configuration (nx,
+    nz in 32..128, ny in 32..96, multiples of 16; Re in 1000..5000; A in
+    0..0.1): with a fixed iteration count every member equals its single
+    context bit for bit; with FP32 sweeps in FP64 defect correction to 1e-8
+    every member's velocity is within 1e-6 of its single context."""
+    import bench
+    mems = bench.ensemble_members(M, 16, seed=20261207)
+    sizes = {(m.nx, m.ny, m.nz) for m in mems}
+    assert len(sizes) >= 10
+    opts = M.make_solver_opts(M.SOLVER_REDBLACK, sor=1.7, n_iter=20, tol=0.0)
+    with M.Ensemble(mems, opts) as E:
+        E.set_guess(M.GUESS_EXTRAPOLATED)
+        E.ic()
+        E.step(2)
+        for q, m in enumerate(mems):
+            with _single(m, opts, M.GUESS_EXTRAPOLATED) as s:
+                s.step(2)
+                for n in ("un", "vn", "wn", "pn"):
+                    assert np.array_equal(E.get(q, n), s.get(n)), (q, n)
+    opts = M.make_solver_opts(M.SOLVER_REDBLACK, sor=1.7, tol=1e-8, check_every=10, max_iter=200000,
+                              precision=M.PREC_MIXED, adaptive_checks=False)
+    with M.Ensemble(mems, opts) as E:
+        E.set_guess(M.GUESS_EXTRAPOLATED)
+        E.ic()
+        E.step(2)
+        for q, m in enumerate(mems):
+            with _single(m, opts, M.GUESS_EXTRAPOLATED) as s:
+                s.step(2)
+                st, _ = E.member_stats(q)
+                assert st.status == 0, q
+                for n in ("un", "vn", "wn"):
+                    assert rel_l2(E.get(q, n), s.get(n)) <= 1e-6, (q, n)
+
+
+def test_learned_warm_start_in_the_ensemble():
+    """The learned warm start inside the ensemble: a network trained on one
+    context's snapshots (fully convolutional, so it applies to every member's
+    grid) is loaded into a 4-member ensemble of uneven sizes; with FP32 sweeps
+    in FP64 defect correction to 1e-8 the members converge, the network's
+    corrections are applied (kept or undone by the divergence test) and every
+    member's velocity agrees with the same ensemble started from the
+    extrapolated increment alone within 1e-6; the step stays one CUDA graph."""
+    from mobydiff_b200 import learned
+    s, g = learned.wavy_solver(32, 32, 32, 3000.0, 0.05, 1e-8, check_every=10, precision=M.PREC_MIXED)
+    with s:
+        net = learned.record_and_train(s, g, [(31, 0.03, 2000.0), (32, 0.07, 4000.0)], warm_steps=3, record_steps=3,
+                                       iters=200, channels=32)
+    mems = [M.make_member(nx=32, ny=32, nz=32, re=2500.0, amp=0.05, seed=41),
+            M.make_member(nx=64, ny=48, nz=32, re=3500.0, amp=0.08, seed=42),
+            M.make_member(nx=48, ny=32, nz=64, re=1500.0, amp=0.02, seed=43),
+            M.make_member(nx=32, ny=64, nz=48, re=4500.0, amp=0.0, seed=44)]
+    opts = M.make_solver_opts(M.SOLVER_REDBLACK, sor=1.7, tol=1e-8, check_every=10, max_iter=200000,
+                              precision=M.PREC_MIXED, adaptive_checks=False)
+    out = {}
+    for mode in (M.GUESS_EXTRAPOLATED, M.GUESS_LEARNED):
+        with M.Ensemble(mems, opts) as E:
+            if mode == M.GUESS_LEARNED:
+                E.unet_load(net.params, net.out_scale, channels=net.channels)
+            E.set_guess(mode)
+            E.ic()
+            its = E.step(6)
+            for q in range(len(mems)):
+                st, _ = E.member_stats(q)
+                assert st.status == 0, (mode, q)
+            out[mode] = (its, [E.get(q, "un") for q in range(len(mems))], [E.get(q, "vn") for q in range(len(mems))],
+                         E.unet_stats() if mode == M.GUESS_LEARNED else None, E.info())
+    its_l, u_l, v_l, (kept, undone), info = out[M.GUESS_LEARNED]
+    its_x, u_x, v_x, _, _ = out[M.GUESS_EXTRAPOLATED]
+    print("iterations extrapolated", its_x, "learned", its_l, "corrections kept", kept, "undone", undone,
+          "graph", info["graph"])
+    assert kept + undone > 0
+    for q in range(len(mems)):
+        assert rel_l2(u_l[q], u_x[q]) <= 1e-6, q
+    assert info["graph"]

@@ -99,11 +99,13 @@ def test_mixed_falls_back_to_fp64_for_other_boundaries():
 @pytest.mark.parametrize("shape,periodic_y", [((64, 32, 32), False), ((40, 12, 10), False), ((32, 16, 16), True),
                                               ((96, 20, 18), False)])
 @pytest.mark.parametrize("tol", [1e-8, 0.0])
-def test_fused_fp32_pass_equals_colour_sweeps(shape, periodic_y, tol):
+def test_fused_and_vector_fp32_sweeps_equal_colour_sweeps(shape, periodic_y, tol):
     """The fused red+black FP32 pass (one launch per iteration, every tile
-    shape the autotuner tries) against one launch per colour: the same FP32
-    corrections bit for bit, so the same iterations and the same FP64 state
-    after the projection; tol 0 runs 25 fixed iterations per inner pass."""
+    shape the autotuner tries) and the vector colour sweeps (2 and 4 cells
+    per thread, then the faster) against one launch per colour with one cell
+    per thread: the same FP32 corrections bit for bit, so the same
+    iterations and the same FP64 state after the projection; tol 0 runs 25
+    fixed iterations per inner pass."""
     nx, ny, nz = shape
     if periodic_y:
         g = O.Grid(nx, ny, nz, lx=2.0, ly=1.0, lz=1.0, re=800.0, dt=1e-3, forcing=(0.1, 0.0, 0.0))
@@ -113,18 +115,23 @@ def test_fused_fp32_pass_equals_colour_sweeps(shape, periodic_y, tol):
         g, bc, f = _wavy_case(nx, ny, nz)
         a, b, c = O.rk_coeffs()
         O.momentum(g, bc, f, g.dt * a[0], g.dt * b[0], g.dt * c[0])
-    out = []
-    for variant in (1, 2):    # colour sweeps; fused pass only (all four tile shapes, then the tuned one)
+    out = {}
+    # 1: colour sweeps; 2: fused pass only (4 tile shapes, then the tuned
+    # one); 4: vector colour sweeps only (2 and 4 cells, then the tuned one)
+    for variant in (1, 2, 4):
         with to_device(M, g, bc, f) as s:
             s.init_pressure_solver(M.make_solver_opts(M.SOLVER_REDBLACK, sor=1.7, tol=tol or 1e-30, check_every=5,
                                                       max_iter=25 if tol == 0.0 else 100000,
                                                       precision=M.PREC_MIXED, sor_variant=variant,
                                                       adaptive_checks=False))
-            sts = [s.pressure_projection(0.4e-3, check=False) for _ in range(5)]   # all 4 tile shapes + tuned
-            out.append(([st.iterations for st in sts], [st.variant for st in sts],
-                        {n: s.get(n) for n in ("un", "vn", "wn", "pn")}))
-    (it1, v1, f1), (it0, v0, f0) = out
-    assert all(v // 100 == 1 for v in v1) and all(v // 100 == 3 for v in v0), (v1, v0)
-    assert it1 == it0
-    for n in f1:
-        assert np.array_equal(f1[n], f0[n]), (n, float(np.max(np.abs(f1[n] - f0[n]))))
+            sts = [s.pressure_projection(0.4e-3, check=False) for _ in range(5)]
+            out[variant] = ([st.iterations for st in sts], [st.variant for st in sts],
+                            {n: s.get(n) for n in ("un", "vn", "wn", "pn")})
+    it1, v1, f1 = out[1]
+    assert all(v // 100 == 1 for v in v1), v1
+    for variant, kind in ((2, 3), (4, 5)):
+        it0, v0, f0 = out[variant]
+        assert all(v // 100 == kind for v in v0), (variant, v0)
+        assert it1 == it0, variant
+        for n in f1:
+            assert np.array_equal(f1[n], f0[n]), (variant, n, float(np.max(np.abs(f1[n] - f0[n]))))
