@@ -155,6 +155,7 @@ def _dist():
     return ws, rank, local
 
 
+C3_GATE_PERIOD = 16   # the learned_gated guess re-tries the other choice every 16th projection of a substage
 SOR_VARIANT = 0   # --sor-variant: red-black kernel variant (0: the autotuner's choice)
 FFT_KERNEL = 0    # --fft-kernel: 0 warp-shuffle transforms where the lengths allow, 1 Stockham
 SOR_NAMES = {1: "one launch per colour sweep", 2: "fused red+black pass 32x8", 3: "fused red+black pass 32x16",
@@ -702,7 +703,7 @@ def run_ensemble(args, cfg):
     mode = M.GUESS_LEARNED if net else M.GUESS_EXTRAPOLATED
     E = M.Ensemble(mems, opts, device)
     if net:
-        E.unet_load(net.params, net.out_scale, channels=net.channels)
+        E.unet_load(net.params, net.out_scale, channels=net.channels, gate_period=C3_GATE_PERIOD)
     E.set_guess(mode)
     E.ic()
     cache = os.path.join(os.path.expanduser("~"), ".cache", "mobydiff_b200", "ensemble_tune.json")
@@ -738,8 +739,9 @@ def run_ensemble(args, cfg):
                 "algorithmic_bytes": alg / K, "avg_launch_ms": ms / (3 * K), "launches": 3 * K}
     learned_info = None
     if net:
-        kept, undone = E.unet_stats()
-        learned_info = {"corrections_kept": kept, "corrections_undone": undone, "snapshots": net.snapshots,
+        kept, undone, gated = E.unet_stats()
+        learned_info = {"corrections_kept": kept, "corrections_undone": undone, "gate_period": C3_GATE_PERIOD,
+                        "left_to_extrapolation_by_gate": gated, "snapshots": net.snapshots,
                         "loss_first": net.loss_first, "loss_last": net.loss_last, "train_ms": net.train_ms,
                         "setup_wall_s": train_wall, "train_runs": [list(r) for r in net.runs],
                         "launches_per_step": launches_timed / max(K, 1)}
@@ -992,9 +994,12 @@ def run_learned_eval(args, cfg):
     train_wall = time.time() - t0
 
     # "learned": the correction as predicted, kept when it lowers ||div u||;
+    # "learned_gated": the same, applied per RK substage only while it takes
+    # fewer iterations than the extrapolated guess alone (gate period 16);
     # "learned_energy": scaled by its energy-optimal step, kept when that is > 0
-    modes = [("zero", M.GUESS_ZERO), ("previous", M.GUESS_PREVIOUS), ("extrapolated", M.GUESS_EXTRAPOLATED),
-             ("learned", M.GUESS_LEARNED), ("learned_energy", M.GUESS_LEARNED)]
+    all_modes = {"zero": M.GUESS_ZERO, "previous": M.GUESS_PREVIOUS, "extrapolated": M.GUESS_EXTRAPOLATED,
+                 "learned": M.GUESS_LEARNED, "learned_gated": M.GUESS_LEARNED, "learned_energy": M.GUESS_LEARNED}
+    modes = [(m, all_modes[m]) for m in args.c3_guesses.split(",")]
     per_run, totals = [], {m: [0, 0.0] for m, _ in modes}
     for seed, amp, re in held:
         row = {"seed": seed, "re": re, "amp": amp}
@@ -1002,7 +1007,8 @@ def run_learned_eval(args, cfg):
         for name, mode in modes:
             s, g = solver(re, amp)
             if mode == M.GUESS_LEARNED:
-                learned.load_into(s, net, step_rule=1 if name == "learned_energy" else 0)
+                learned.load_into(s, net, step_rule=1 if name == "learned_energy" else 0,
+                                  gate_period=C3_GATE_PERIOD if name == "learned_gated" else 0)
             s.set_pressure_guess(mode, record=True)
             s.channel_ic(seed, 0.1, 0.01, y0, amp, lam)
             s.step(3)
@@ -1013,33 +1019,39 @@ def run_learned_eval(args, cfg):
             row[name] = {"iters_per_substage": it / (3 * steps), "mcell_steps_s": cells * steps / dt / 1e6}
             totals[name][0] += it
             totals[name][1] += dt
+            if name == "learned_gated":
+                row[name]["gated_off"] = s.unet_stats().gated
             final[name] = [s.get(n) for n in ("un", "vn", "wn")]
             s.close()
-        num = sum(float(np.sum((a - b) ** 2)) for a, b in zip(final["learned"], final["zero"]))
-        den = sum(float(np.sum(b ** 2)) for b in final["zero"])
-        row["velocity_rel_l2_learned_vs_zero"] = math.sqrt(num / den)
+        ref_name = "zero" if "zero" in final else "extrapolated"
+        for name in final:
+            if name.startswith("learned"):
+                num = sum(float(np.sum((a - b) ** 2)) for a, b in zip(final[name], final[ref_name]))
+                den = sum(float(np.sum(b ** 2)) for b in final[ref_name])
+                row[f"velocity_rel_l2_{name}_vs_{ref_name}"] = math.sqrt(num / den)
         per_run.append(row)
     nsub = 3 * steps * len(held)
     summary = {m: {"iters_per_substage": totals[m][0] / nsub,
                    "mcell_steps_s": cells * steps * len(held) / totals[m][1] / 1e6} for m, _ in modes}
+    head = "learned_gated" if "learned_gated" in summary else "learned"
+    ratios = {f"reduction_vs_{b}": summary[b]["iters_per_substage"] / summary[head]["iters_per_substage"]
+              for b in ("zero", "previous", "extrapolated") if b in summary}
+    for m in ("learned", "learned_energy"):
+        if m in summary and m != head and "extrapolated" in summary:
+            ratios[f"{m}_reduction_vs_extrapolated"] = (summary["extrapolated"]["iters_per_substage"] /
+                                                        summary[m]["iters_per_substage"])
     if rank == 0:
         print(json.dumps({
             "metric": "red-black iterations per substage to residual 1e-8 on held-out runs, learned warm start vs "
                       "zero / previous / extrapolated guesses, 1 B200",
-            "value": summary["learned"]["iters_per_substage"], "unit": "iterations per substage",
+            "value": summary[head]["iters_per_substage"], "unit": "iterations per substage", "value_guess": head,
             "higher_is_better": False, "n_gpus": 1, "steps": steps, "warmup": 3, "dtype": "f64+f32",
             "data": "synthetic: seeded Poiseuille+noise ICs; training and held-out runs at seeded Re and A",
             "config": {"workload": cfg["workload"], "grid": [cfg["nx"], cfg["ny"], cfg["nz"]], "tol": cfg["tol"],
                        "train_runs": [{"seed": a, "amp": b, "re": c} for a, b, c in train],
                        "record_steps_per_run": cfg["record_steps"], "heldout_steps": steps * len(held)},
-            "by_guess": summary,
-            "reduction_vs_zero": summary["zero"]["iters_per_substage"] / summary["learned"]["iters_per_substage"],
-            "reduction_vs_previous": summary["previous"]["iters_per_substage"] /
-                                     summary["learned"]["iters_per_substage"],
-            "reduction_vs_extrapolated": summary["extrapolated"]["iters_per_substage"] /
-                                         summary["learned"]["iters_per_substage"],
-            "energy_step_reduction_vs_extrapolated": summary["extrapolated"]["iters_per_substage"] /
-                                                     summary["learned_energy"]["iters_per_substage"],
+            "by_guess": summary, **ratios,
+            "gate_period": C3_GATE_PERIOD,
             "heldout_runs": per_run,
             "learned": {"snapshots": net.snapshots, "loss_first": net.loss_first, "loss_last": net.loss_last,
                         "train_ms": net.train_ms, "record_s": net.record_seconds, "setup_wall_s": train_wall},
@@ -1253,6 +1265,9 @@ def main():
                     help="FFT path transforms: 0 warp-shuffle where nx/2 and nz allow, 1 shared-memory Stockham")
     ap.add_argument("--c3-steps", type=int, default=0,
                     help="config c3: measured steps per held-out run (0: the config's 10)")
+    ap.add_argument("--c3-guesses", default="zero,previous,extrapolated,learned,learned_gated",
+                    help="config c3: the guesses compared (comma list of zero, previous, extrapolated, learned, "
+                         "learned_gated, learned_energy)")
     ap.add_argument("--train-iters", type=int, default=1200, help="Adam steps of the learned warm start")
     args = ap.parse_args()
     global SOR_VARIANT, FFT_KERNEL

@@ -439,7 +439,12 @@ typedef struct {
                                minimises the energy norm of the pressure error along it,
                                alpha = -<delta, d0> / <delta, d1 - d0> (d0, d1 the divergence before
                                and after the correction), kept when alpha > 0               */
-    int reserved_i[6];
+    int gate_period;        /* 0 (default): correct every projection that has a two-step history;
+                               P > 0: per RK substage, apply the correction or not by the red-black
+                               iterations each choice took (exponential averages, weight 1/2):
+                               the first projection without it, the next with it, then the
+                               cheaper one, with the other re-tried every P-th projection  */
+    int reserved_i[5];
     double reserved_d[8];
 } mdx_unet_opts_t;
 
@@ -455,7 +460,8 @@ typedef struct {
     double train_ms;        /* device time of the last mdx_unet_train call      */
     long long tc_convs;     /* convolution launches on tcgen05 since creation   */
     double last_step;       /* step_rule 1: the last step length alpha           */
-    double reserved_d[4];
+    long long gated;        /* projections the gate left to the extrapolated guess */
+    double reserved_d[3];
 } mdx_unet_stats_t;
 
 void mdx_default_unet_opts(mdx_unet_opts_t* opts);
@@ -474,9 +480,11 @@ void mdx_default_unet_opts(mdx_unet_opts_t* opts);
  * the extrapolated increment) and sweeps to the tolerance. */
 int mdx_ensemble_unet_load(mdx_ensemble_t* ens, const mdx_unet_opts_t* opts, const float* params, long long n,
                            double out_scale);
-/* Learned corrections kept and undone over all members since creation
- * (synchronises). */
-int mdx_ensemble_unet_stats(mdx_ensemble_t* ens, long long* corrections, long long* rejected);
+/* Learned corrections kept and undone, and projections the gate left to
+ * the extrapolated guess (opts->gate_period > 0 at mdx_ensemble_unet_load:
+ * per member and RK substage, as for a context), over all members since
+ * creation (synchronises; each pointer may be NULL). */
+int mdx_ensemble_unet_stats(mdx_ensemble_t* ens, long long* corrections, long long* rejected, long long* gated);
 int mdx_unet_create(mdx_ctx_t* ctx, const mdx_unet_opts_t* opts);
 int mdx_unet_destroy(mdx_ctx_t* ctx);
 /* Record a snapshot in every converged projection that had an extrapolated
@@ -495,11 +503,12 @@ int mdx_unet_get_params(mdx_ctx_t* ctx, float* host, long long n);
 int mdx_unet_set_params(mdx_ctx_t* ctx, const float* host, long long n);   /* marks the net trained */
 int mdx_unet_get_out_scale(mdx_ctx_t* ctx, double* scale);
 int mdx_unet_set_out_scale(mdx_ctx_t* ctx, double scale);
-/* One forward and backward pass on host inputs in4 [4][ncells] and target
- * [ncells] (cells x fastest): loss = mean((out - target)^2), its gradient
+/* One forward and backward pass on host inputs in [5][ncells] (the
+ * normalised divergence, the last two increments, the IBM factor and the
+ * viscous-number channel) and target [ncells] (cells x fastest): loss = mean((out - target)^2), its gradient
  * with respect to every parameter (param_count floats) and the output
  * [ncells].  No update; used to check the kernels against a CPU network. */
-int mdx_unet_loss_grad(mdx_ctx_t* ctx, const float* in4, const float* target, double* loss, float* grad, float* out);
+int mdx_unet_loss_grad(mdx_ctx_t* ctx, const float* in, const float* target, double* loss, float* grad, float* out);
 int mdx_unet_stats(mdx_ctx_t* ctx, mdx_unet_stats_t* stats);
 
 /* get_cfl, src/modules/step.f90:210-258 (synchronises). */

@@ -97,7 +97,7 @@ class SolveStatsT(C.Structure):
 class UnetOptsT(C.Structure):
     _fields_ = [("channels0", C.c_int), ("channels", C.c_int), ("extra_bottleneck", C.c_int), ("capacity", C.c_int),
                 ("slope", C.c_double), ("seed", C.c_uint64), ("conv_kernel", C.c_int), ("step_rule", C.c_int),
-                ("reserved_i", C.c_int * 6),
+                ("gate_period", C.c_int), ("reserved_i", C.c_int * 5),
                 ("reserved_d", C.c_double * 8)]
 
 
@@ -105,7 +105,8 @@ class UnetStatsT(C.Structure):
     _fields_ = [("corrections", C.c_longlong), ("rejected", C.c_longlong), ("snapshots", C.c_longlong),
                 ("stored", C.c_int), ("trained", C.c_int), ("out_scale", C.c_double), ("last_gain", C.c_double),
                 ("infer_ms", C.c_double), ("train_ms", C.c_double), ("tc_convs", C.c_longlong),
-                ("last_step", C.c_double), ("reserved_d", C.c_double * 4)]
+                ("last_step", C.c_double), ("gated", C.c_longlong),
+                ("reserved_d", C.c_double * 3)]
 
 
 class MemberT(C.Structure):
@@ -212,7 +213,7 @@ def lib():
         "mdx_ensemble_use_graph": (i, [vp, i]),
         "mdx_ensemble_info": (i, [vp, P(i), P(i), P(i), P(i), P(d), P(C.c_longlong)]),
         "mdx_ensemble_unet_load": (i, [vp, P(UnetOptsT), P(C.c_float), C.c_longlong, d]),
-        "mdx_ensemble_unet_stats": (i, [vp, P(C.c_longlong), P(C.c_longlong)]),
+        "mdx_ensemble_unet_stats": (i, [vp, P(C.c_longlong), P(C.c_longlong), P(C.c_longlong)]),
         "mdx_default_unet_opts": (None, [P(UnetOptsT)]),
         "mdx_unet_create": (i, [vp, P(UnetOptsT)]),
         "mdx_unet_destroy": (i, [vp]),
@@ -574,7 +575,7 @@ class Solver:
 
     # ---- learned warm start ----------------------------------------------
     def unet_create(self, channels: int = 32, extra_bottleneck: int = 0, capacity: int = 64, slope: float = 0.1,
-                    seed: int = 20261203, tcgen05: bool = True, step_rule: int = 0) -> None:
+                    seed: int = 20261203, tcgen05: bool = True, step_rule: int = 0, gate_period: int = 0) -> None:
         o = UnetOptsT()
         lib().mdx_default_unet_opts(C.byref(o))
         o.channels = channels
@@ -584,6 +585,7 @@ class Solver:
         o.seed = seed
         o.conv_kernel = 0 if tcgen05 else 1
         o.step_rule = step_rule
+        o.gate_period = gate_period
         self._c(lib().mdx_unet_create(self.h, C.byref(o)))
 
     def unet_destroy(self) -> None:
@@ -618,7 +620,7 @@ class Solver:
         return v.value
 
     def unet_loss_grad(self, in4, target):
-        """One forward/backward pass on host inputs [4][n] and target [n]:
+        """One forward/backward pass on host inputs [5][n] and target [n]:
         (loss, gradient [param_count], output [n])."""
         in4 = np.ascontiguousarray(in4, dtype=np.float32)
         target = np.ascontiguousarray(target, dtype=np.float32)
@@ -707,9 +709,11 @@ class Ensemble:
         return it.value
 
     def unet_load(self, params, out_scale: float, channels: int = 32, extra_bottleneck: int = 0,
-                  slope: float = 0.1, tcgen05: bool = True) -> None:
+                  slope: float = 0.1, tcgen05: bool = True, gate_period: int = 0) -> None:
         """A trained network (mobydiff_b200.learned.TrainedNet's parameters
-        and output scale) for the learned warm start of every member."""
+        and output scale) for the learned warm start of every member;
+        gate_period > 0 applies its correction per member and substage only
+        while it takes fewer iterations than the extrapolated guess alone."""
         o = UnetOptsT()
         lib().mdx_default_unet_opts(C.byref(o))
         o.channels = channels
@@ -717,15 +721,17 @@ class Ensemble:
         o.capacity = 0
         o.slope = slope
         o.conv_kernel = 0 if tcgen05 else 1
+        o.gate_period = gate_period
         p = np.ascontiguousarray(params, dtype=np.float32)
         self._c(lib().mdx_ensemble_unet_load(self.h, C.byref(o), p.ctypes.data_as(C.POINTER(C.c_float)), p.size,
                                              float(out_scale)))
 
     def unet_stats(self):
-        """(learned corrections kept, undone) over all members."""
-        a, b = C.c_longlong(0), C.c_longlong(0)
-        self._c(lib().mdx_ensemble_unet_stats(self.h, C.byref(a), C.byref(b)))
-        return a.value, b.value
+        """(learned corrections kept, undone, left to the extrapolated guess
+        by the gate) over all members."""
+        a, b, c = C.c_longlong(0), C.c_longlong(0), C.c_longlong(0)
+        self._c(lib().mdx_ensemble_unet_stats(self.h, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
 
     def member_stats(self, m: int):
         st = SolveStatsT()

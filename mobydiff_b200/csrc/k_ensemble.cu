@@ -94,6 +94,15 @@ struct ens_state {                   // per member, updated in the kernel
     // undone, 3 being tried) and the counts over the run
     int lr_last;
     long long lr_corr, lr_rej;
+    // the gate (gate_period > 0): per substage, averages of the iterations
+    // with the correction (1) and without (0), their counts, projections
+    // since the other choice was tried, this projection's choice (-1 none),
+    // and the projections left to the extrapolated guess
+    double g_ema[3][2];
+    int g_n[3][2];
+    int g_since[3];
+    int g_arm;
+    long long lr_gated;
 };
 
 struct ens_list {
@@ -122,7 +131,23 @@ struct ens_args {
     // inputs; 2: from the learned correction on (the network ran between)
     int split;
     const int* learn_ok;             // per member: the network wrote a correction
+    int gate_period;                 // > 0: apply it per substage only while it takes fewer iterations
 };
+
+// The gate's choice for an eligible projection of substage s: 0 the
+// extrapolated guess alone, 1 with the learned correction (the rule of
+// mdx_unet_correct: a baseline without it first, then with it, then the
+// cheaper one, the other re-tried every period-th projection).
+__device__ int gate_choose(ens_state& S, int s, int period) {
+    if (S.g_n[s][0] == 0) return 0;
+    if (S.g_n[s][1] == 0) return 1;
+    const int pref = S.g_ema[s][1] <= S.g_ema[s][0] ? 1 : 0;
+    if (++S.g_since[s] >= period) {
+        S.g_since[s] = 0;
+        return 1 - pref;
+    }
+    return pref;
+}
 
 __device__ __forceinline__ double nanmax(double a, double b) { return (a != a || b != b) ? (a + b) : fmax(a, b); }
 
@@ -603,6 +628,7 @@ __global__ void __launch_bounds__(MAX_THREADS, MINB) k_ens_substage(ens_args A) 
             S.has_guess = warm && (h & (1 << s));
             S.extrap = A.guess_mode != MDX_GUESS_PREVIOUS && (h & (8 << s));
             S.lr_last = 0;
+            S.g_arm = -1;
         }
     grid.sync();
 
@@ -715,7 +741,14 @@ __global__ void __launch_bounds__(MAX_THREADS, MINB) k_ens_substage(ens_args A) 
         if (blockIdx.x == 0)
             for (int m = threadIdx.x; m < A.nmem; m += blockDim.x) {
                 ens_state& S = A.st[m];
-                S.lr_last = (A.learn_ok[m] && S.guessed && S.extrap && S.status == MDX_NOT_CONVERGED) ? 3 : 0;
+                const bool elig = A.learn_ok[m] && S.guessed && S.extrap && S.status == MDX_NOT_CONVERGED;
+                int arm = elig ? 1 : 0;
+                if (elig && A.gate_period > 0) {
+                    arm = gate_choose(S, s, A.gate_period);
+                    S.g_arm = arm;
+                    if (arm == 0) S.lr_gated++;
+                }
+                S.lr_last = arm == 1 ? 3 : 0;
             }
         grid.sync();
         cell_tiles(A, [&](int m, const ens_member& M, unsigned t) {
@@ -907,6 +940,14 @@ __global__ void __launch_bounds__(MAX_THREADS, MINB) k_ens_substage(ens_args A) 
             const int iters = meas ? S.it : A.n_iter;   // mixed: FP32 iterations
             S.last_iters = iters;
             S.iters_total += iters;
+            if (S.g_arm >= 0) {   // the gate's sample
+                if (S.status == MDX_OK) {
+                    double& e = S.g_ema[s][S.g_arm];
+                    e = S.g_n[s][S.g_arm] > 0 ? 0.5 * e + 0.5 * (double)iters : (double)iters;
+                    S.g_n[s][S.g_arm]++;
+                }
+                S.g_arm = -1;
+            }
             S.last_residual = meas ? (S.r0 > 0.0 ? S.r / S.r0 : 0.0) : 0.0;
             if (warm) {
                 S.flip ^= 1 << s;
@@ -1027,6 +1068,7 @@ struct mdx_ensemble {
     mdx_ctx_t* net = nullptr;
     double* net_scal = nullptr;      // 4 per member
     int* learn_ok = nullptr;         // per member
+    int gate_period = 0;             // of the loaded network's options
 };
 
 namespace {
@@ -1105,6 +1147,7 @@ ens_args make_args(mdx_ensemble_t* E, int s, int momentum) {
     A.inner_sor = E->opts.inner_sor;
     A.split = 0;
     A.learn_ok = E->learn_ok;
+    A.gate_period = E->gate_period;
     return A;
 }
 
@@ -1129,7 +1172,7 @@ int net_pass(mdx_ensemble_t* E, int s) {
     const long long l0 = E->net->launches;
     for (int m = 0; m < E->n; ++m) {
         const ens_member& M = E->hm[m];
-        const int rc = mdx_unet_member_delta(E->net, M.d, M.p.dx, M.p.dy, M.p.dz, M.dt * c[s], M.un, M.vn, M.wn, M.hl1,
+        const int rc = mdx_unet_member_delta(E->net, M.d, M.p.dx, M.p.dy, M.p.dz, M.p.ire, M.dt * c[s], M.un, M.vn, M.wn, M.hl1,
                                              M.hl2, M.ibm ? M.mu : nullptr, M.delta, E->net_scal + 4 * m,
                                              E->learn_ok + m);
         if (rc != MDX_OK) return efail(E, rc, "member %d network pass: %s", m, mdx_last_error(E->net));
@@ -1580,6 +1623,8 @@ int mdx_ensemble_unet_load(mdx_ensemble_t* E, const mdx_unet_opts_t* opts, const
         }
         ENS_CUDA(E, cudaMemcpy(E->dm, E->hm.data(), sizeof(ens_member) * E->n, cudaMemcpyHostToDevice));
     }
+    if (opts && opts->gate_period < 0) return efail(E, MDX_ERR_ARG, "learned guess: gate_period < 0");
+    E->gate_period = opts ? opts->gate_period : 0;
     int rc = mdx_unet_set_params(E->net, params, n);
     if (rc == MDX_OK) rc = mdx_unet_set_out_scale(E->net, out_scale);
     if (rc != MDX_OK) return efail(E, rc, "learned guess: parameters: %s", mdx_last_error(E->net));
@@ -1587,17 +1632,19 @@ int mdx_ensemble_unet_load(mdx_ensemble_t* E, const mdx_unet_opts_t* opts, const
     return MDX_OK;
 }
 
-int mdx_ensemble_unet_stats(mdx_ensemble_t* E, long long* corrections, long long* rejected) {
+int mdx_ensemble_unet_stats(mdx_ensemble_t* E, long long* corrections, long long* rejected, long long* gated) {
     if (!E) return MDX_ERR_ARG;
     std::vector<ens_state> h;
     MDX_TRY(read_stats(E, h));
-    long long c = 0, r = 0;
+    long long c = 0, r = 0, q = 0;
     for (const auto& S : h) {
         c += S.lr_corr;
         r += S.lr_rej;
+        q += S.lr_gated;
     }
     if (corrections) *corrections = c;
     if (rejected) *rejected = r;
+    if (gated) *gated = q;
     return MDX_OK;
 }
 

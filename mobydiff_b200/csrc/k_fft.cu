@@ -1115,6 +1115,14 @@ static int projection_fft_walls(mdx_ctx_t* ctx, mdx_dscal dg) {
                1.0 / (double)((long long)e.nx * e.nz), ctx->spec, ctx->phi_ext, ctx->plan_xh, ctx->tw_x);
     const int nbd = (int)std::min<long long>((d.nint + 255) / 256, 8192);
     MDX_LAUNCH(ctx, MDX_T_FFT_INV, "restrict phi", k_restrict, nbd, 256, 0, d, e, ctx->phi_ext, f[MDX_PHI]);
+    // u <- u* on the whole padded arrays first, as the red-black projection
+    // starts (pressure_redblack.f90:63-84): the edges and corners of the
+    // ghost layers, which the face rules of apply_bc_redblack do not set and
+    // the predictor's diagonal neighbours read, then hold u*'s values there
+    const size_t bytes = sizeof(double) * (size_t)d.npad;
+    MDX_CUDA(ctx, cudaMemcpyAsync(f[MDX_UN], f[MDX_US], bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    MDX_CUDA(ctx, cudaMemcpyAsync(f[MDX_VN], f[MDX_VS], bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    MDX_CUDA(ctx, cudaMemcpyAsync(f[MDX_WN], f[MDX_WS], bytes, cudaMemcpyDeviceToDevice, ctx->stream));
     auto go = [&](auto kern) -> int {
         MDX_LAUNCH(ctx, MDX_T_CORRECT, "correction (walls)", kern, grid, block, 0, d, g.dx, g.dy, g.dz, dg, f[MDX_PHI],
                    f[MDX_US], f[MDX_VS], f[MDX_WS], f[MDX_UN], f[MDX_VN], f[MDX_WN], f[MDX_PN], f[MDX_COEF_U],

@@ -647,7 +647,7 @@ int mdx_k_projection_redblack(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t* st) 
         if (handled) {
             ctx->last.guessed = guessed ? 1 : 0;
             if (st) st->guessed = ctx->last.guessed;
-            if (warm) MDX_TRY(mdx_warm_end(ctx, ctx->last.status == MDX_OK));
+            if (warm) MDX_TRY(mdx_warm_end(ctx, ctx->last.status == MDX_OK, ctx->last.iterations));
             return MDX_OK;
         }
     }
@@ -739,7 +739,7 @@ int mdx_k_projection_redblack(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t* st) 
             s.residual = r / r0;
         }
     }
-    if (warm) MDX_TRY(mdx_warm_end(ctx, o.tol > 0.0 && s.status == MDX_OK));
+    if (warm) MDX_TRY(mdx_warm_end(ctx, o.tol > 0.0 && s.status == MDX_OK, s.iterations));
     ctx->last = s;
     if (st) *st = s;
     return MDX_OK;

@@ -53,7 +53,7 @@ constexpr int TX = 16, TY = 4, TZ = 4;   // output tile of the convolutions
 constexpr int HX = TX + 2, HY = TY + 2, HZ = TZ + 2;
 constexpr int HV = HX * HY * HZ;         // cells of the input halo
 constexpr int TV = TX * TY * TZ;         // cells of the tile (256)
-constexpr int NIN = 4;                   // input channels used
+constexpr int NIN = 5;                   // input channels used
 constexpr int C_IN = 16;                 // input channels stored (zero padded)
 constexpr int MAX_EXTRA = 8;
 
@@ -455,7 +455,7 @@ __global__ void k_act_bwd_down(lvl Lc, lvl Lf, int C, const float* __restrict__ 
     }
 }
 
-// Input of the network: in[c][v] (c < 4) -> X[v][16] BF16.
+// Input of the network: in[c][v] (c < NIN) -> X[v][16] BF16.
 __global__ void k_pack_in(long long n, const float* __restrict__ in, bf16* __restrict__ X) {
     for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x) {
         float s[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
@@ -689,13 +689,14 @@ __global__ void k_sum_pairs(int nb, const double* __restrict__ part, double* __r
 }
 
 // Normalised inputs: in[0] = raw*ir, in[1] = dp1*ip, in[2] = dp2*ip, in[3] =
-// IBM factor of the cell (mean of its three lower faces; 1 without IBM).
-// DEV: the two scales come from the device (scal[0], scal[1]), written by
-// k_net_scales, so that the pass needs no host read.
+// IBM factor of the cell (mean of its three lower faces; 1 without IBM),
+// in[4] = vis, the same for every cell (net_vis_input: the flow's viscous
+// number).  DEV: the two scales come from the device (scal[0], scal[1]),
+// written by k_net_scales, so that the pass needs no host read.
 template <bool DEV>
 __global__ void k_norm_in_t(mdx_dims d, int mu_mode, const float* __restrict__ raw, const double* __restrict__ dp1,
                             const double* __restrict__ dp2, const double* __restrict__ mu, double ir, double ip,
-                            const double* __restrict__ scal, float* __restrict__ in) {
+                            float vis, const double* __restrict__ scal, float* __restrict__ in) {
     if (DEV) {
         ir = scal[0];
         ip = scal[1];
@@ -726,7 +727,18 @@ __global__ void k_norm_in_t(mdx_dims d, int mu_mode, const float* __restrict__ r
             m = (float)((a + b + c) * (1.0 / 3.0));
         }
         in[3 * n + t] = m;
+        in[4 * n + t] = vis;
     }
+}
+
+// The network's constant input: the viscous number dt_gamma / (Re h^2) of
+// the substage, as log10 + 3 (about -0.8 .. 0.6 over Re 1000..5000 on the
+// 256x128x128 channel at dt 1e-3).  The pressure increment's shape depends
+// on how far viscous diffusion reaches in a substage; the other inputs are
+// normalised and carry no scale.
+float net_vis_input(double dg, double ire, double h2) {
+    const double v = std::fabs(dg) * ire / h2;
+    return v > 0.0 && std::isfinite(v) ? (float)(std::log10(v) + 3.0) : 0.f;
 }
 
 // Input and output scales of one pass from the sums of div^2 and dp1^2 over
@@ -849,14 +861,14 @@ struct mdx_unet {
     float* head_part = nullptr;
     int head_blocks = 0;
     float* out = nullptr;       // FP32 head output (training)
-    float* in = nullptr;        // [4][n] normalised inputs (inference)
+    float* in = nullptr;        // [NIN][n] normalised inputs (inference)
     float* raw = nullptr;       // raw divergence
     double* delta = nullptr;    // learned correction
     double* red_part = nullptr;
     double* red_out = nullptr;
     double* red_host = nullptr;
     int red_blocks = 0;
-    // snapshots: slot s holds in[4][n] then target[n]
+    // snapshots: slot s holds in[NIN][n] then target[n]
     float* snap = nullptr;
     int stored = 0, next = 0;
     long long total_snaps = 0;
@@ -866,6 +878,14 @@ struct mdx_unet {
     double out_scale = 1.0;
     uint64_t order_state = 0;
     mdx_unet_stats_t st{};
+    // gate (o.gate_period > 0): per RK substage, exponential averages of the
+    // iterations of projections with the correction (on) and with the
+    // extrapolated guess alone (off), their sample counts, projections since
+    // the other arm was last tried, and this projection's arm (-1: none)
+    double gate_ema[3][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+    int gate_n[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+    int gate_since[3] = {0, 0, 0};
+    int gate_arm = -1;
     cudaEvent_t ev[2] = {nullptr, nullptr};
     int* tc_err = nullptr;      // set by a tcgen05 convolution whose bounded wait gave up
 };
@@ -1214,7 +1234,9 @@ void mdx_unet_free(mdx_ctx_t* ctx) {
 
 // With the extrapolated increment applied (*rg = ||div u||): record a
 // snapshot's inputs, and in learned mode apply the network's correction,
-// undoing it when it does not lower ||div u||.
+// undoing it when it does not lower ||div u||.  With a gate period the
+// correction is applied or not per RK substage by the iterations each
+// choice took (mdx_unet_finish records them).
 int mdx_unet_correct(mdx_ctx_t* ctx, double dg, double* rg) {
     mdx_unet* U = static_cast<mdx_unet*>(ctx->unet);
     const bool learn = ctx->guess_mode == MDX_GUESS_LEARNED && U->trained;
@@ -1223,7 +1245,30 @@ int mdx_unet_correct(mdx_ctx_t* ctx, double dg, double* rg) {
     const mdx_dims& d = ctx->d;
     const long long n = d.nint;
     const int s = (int)(ctx->proj_count % 3);
-    if (learn) MDX_CUDA(ctx, cudaEventRecord(U->ev[0], ctx->stream));
+    // the gate: off -> the extrapolated guess alone for this projection
+    bool apply = learn;
+    U->gate_arm = -1;
+    if (learn && U->o.gate_period > 0) {
+        const int* cnt = U->gate_n[s];
+        int arm;
+        if (cnt[0] == 0) arm = 0;        // a baseline without the correction first
+        else if (cnt[1] == 0) arm = 1;
+        else {
+            const int pref = U->gate_ema[s][1] <= U->gate_ema[s][0] ? 1 : 0;
+            arm = pref;
+            if (++U->gate_since[s] >= U->o.gate_period) {   // re-try the other arm
+                arm = 1 - pref;
+                U->gate_since[s] = 0;
+            }
+        }
+        U->gate_arm = arm;
+        if (arm == 0) {
+            apply = false;
+            U->st.gated++;
+        }
+    }
+    if (!apply && !rec) return MDX_OK;
+    if (apply) MDX_CUDA(ctx, cudaEventRecord(U->ev[0], ctx->stream));
     MDX_LAUNCH(ctx, MDX_T_OTHER, "unet div field", k_div_field, U->red_blocks, 256, 0, d, U->pery, 1.0 / ctx->g.dx,
                1.0 / ctx->g.dy, 1.0 / ctx->g.dz, ctx->f[MDX_UN], ctx->f[MDX_VN], ctx->f[MDX_WN], ctx->dp_hist[s], U->raw,
                U->red_part);
@@ -1241,8 +1286,9 @@ int mdx_unet_correct(mdx_ctx_t* ctx, double dg, double* rg) {
         U->pending_scale = dg / (sr * h2);
     }
     MDX_LAUNCH(ctx, MDX_T_OTHER, "unet inputs", k_norm_in_t<false>, nblocks(n), 256, 0, d, ctx->mu_mode, U->raw,
-               ctx->dp_hist[s], ctx->dp_hist2[s], ctx->mu, 1.0 / sr, 1.0 / sp, (const double*)nullptr, dst);
-    if (!learn) return MDX_OK;
+               ctx->dp_hist[s], ctx->dp_hist2[s], ctx->mu, 1.0 / sr, 1.0 / sp, net_vis_input(dg, 1.0 / ctx->g.re, h2),
+               (const double*)nullptr, dst);
+    if (!apply) return MDX_OK;
     MDX_LAUNCH(ctx, MDX_T_OTHER, "unet pack", k_pack_in, nblocks(n), 256, 0, n, dst, U->x0);
     MDX_TRY(forward(ctx, U));
     MDX_LAUNCH(ctx, MDX_T_OTHER, "unet head", k_head_infer<16>, nblocks(n), 256, 0, n, U->act.back(),
@@ -1306,7 +1352,7 @@ int mdx_unet_correct(mdx_ctx_t* ctx, double dg, double* rg) {
 // (device) says whether delta holds a correction.  Inputs are the member's
 // u, v, w after its extrapolated guess, its last two increments of this
 // substage and its IBM factor planes (or null).
-int mdx_unet_member_delta(mdx_ctx_t* nc, const mdx_dims& dm, double dx, double dy, double dz, double dg,
+int mdx_unet_member_delta(mdx_ctx_t* nc, const mdx_dims& dm, double dx, double dy, double dz, double ire, double dg,
                           const double* un, const double* vn, const double* wn, const double* dp1, const double* dp2,
                           const double* mu_planes, double* delta, double* scal, int* ok) {
     mdx_unet* U = static_cast<mdx_unet*>(nc->unet);
@@ -1326,7 +1372,7 @@ int mdx_unet_member_delta(mdx_ctx_t* nc, const mdx_dims& dm, double dx, double d
         MDX_LAUNCH(nc, MDX_T_OTHER, "unet sum pairs", k_sum_pairs, 1, 256, 0, U->red_blocks, U->red_part, U->red_out);
         MDX_LAUNCH(nc, MDX_T_OTHER, "unet scales", k_net_scales, 1, 32, 0, n, U->red_out, U->out_scale, h2, dg, scal, ok);
         MDX_LAUNCH(nc, MDX_T_OTHER, "unet inputs", k_norm_in_t<true>, nblocks(n), 256, 0, dm, mu_planes ? 1 : 0, U->raw,
-                   dp1, dp2, mu_planes, 0.0, 0.0, (const double*)scal, U->in);
+                   dp1, dp2, mu_planes, 0.0, 0.0, net_vis_input(dg, ire, h2), (const double*)scal, U->in);
         MDX_LAUNCH(nc, MDX_T_OTHER, "unet pack", k_pack_in, nblocks(n), 256, 0, n, U->in, U->x0);
         MDX_TRY(forward(nc, U));
         MDX_LAUNCH(nc, MDX_T_OTHER, "unet head", k_head_infer<16>, nblocks(n), 256, 0, n, U->act.back(),
@@ -1343,8 +1389,17 @@ int mdx_unet_member_delta(mdx_ctx_t* nc, const mdx_dims& dm, double dx, double d
 
 // After the projection (dp_hist[s] = its increment): the pending snapshot's
 // target, or drop it when the projection did not converge.
-int mdx_unet_finish(mdx_ctx_t* ctx, bool converged) {
+int mdx_unet_finish(mdx_ctx_t* ctx, bool converged, int iterations) {
     mdx_unet* U = static_cast<mdx_unet*>(ctx->unet);
+    if (U->gate_arm >= 0) {   // the gate's sample: this projection's iterations
+        const int s = (int)(ctx->proj_count % 3), a = U->gate_arm;
+        if (converged) {
+            double& e = U->gate_ema[s][a];
+            e = U->gate_n[s][a] > 0 ? 0.5 * e + 0.5 * (double)iterations : (double)iterations;
+            U->gate_n[s][a]++;
+        }
+        U->gate_arm = -1;
+    }
     if (U->pending < 0) return MDX_OK;
     const int slot = U->pending;
     U->pending = -1;
@@ -1382,7 +1437,7 @@ int mdx_unet_create(mdx_ctx_t* ctx, const mdx_unet_opts_t* opts) {
     if (o.channels0 != 16 || (o.channels != 16 && o.channels != 32))
         return mdx_fail(ctx, MDX_ERR_ARG, "unet channels must be 16 and 16|32");
     if (o.extra_bottleneck < 0 || o.extra_bottleneck > MAX_EXTRA || o.capacity < 0 || !(o.slope > 0.0) || o.slope > 1.0 ||
-        o.step_rule < 0 || o.step_rule > 1)
+        o.step_rule < 0 || o.step_rule > 1 || o.gate_period < 0)
         return mdx_fail(ctx, MDX_ERR_ARG, "unet options out of range");
     const mdx_dims& d = ctx->d;
     if (d.nx % 8 || d.ny % 8 || d.nz % 8) return mdx_fail(ctx, MDX_ERR_ARG, "unet needs nx, ny, nz multiples of 8");

@@ -132,7 +132,7 @@ int mdx_warm_begin(mdx_ctx_t* ctx) {
     return MDX_OK;
 }
 
-int mdx_warm_end(mdx_ctx_t* ctx, bool converged) {
+int mdx_warm_end(mdx_ctx_t* ctx, bool converged, int iterations) {
     const int s = (int)(ctx->proj_count % 3);
     const mdx_dims& d = ctx->d;
     const int nb = (int)std::min<long long>((d.nint + 255) / 256, 8192);
@@ -142,7 +142,7 @@ int mdx_warm_end(mdx_ctx_t* ctx, bool converged) {
     MDX_LAUNCH(ctx, MDX_T_OTHER, "record increment", k_record_increment, nb, 256, 0, d, ctx->f[MDX_PN], ctx->p_before,
                ctx->dp_hist[s]);
     ctx->hist_valid |= 1 << s;
-    if (ctx->unet) MDX_TRY(mdx_unet_finish(ctx, converged));
+    if (ctx->unet) MDX_TRY(mdx_unet_finish(ctx, converged, iterations));
     ctx->proj_count++;
     return MDX_OK;
 }

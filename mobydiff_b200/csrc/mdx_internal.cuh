@@ -306,7 +306,7 @@ bool mdx_guess_supported(const mdx_ctx_t* ctx);
 int mdx_warm_alloc(mdx_ctx_t* ctx);
 void mdx_warm_free(mdx_ctx_t* ctx);
 int mdx_warm_begin(mdx_ctx_t* ctx);
-int mdx_warm_end(mdx_ctx_t* ctx, bool converged);
+int mdx_warm_end(mdx_ctx_t* ctx, bool converged, int iterations);
 int mdx_apply_guess(mdx_ctx_t* ctx, const double* gs, double dg);
 int mdx_undo_guess(mdx_ctx_t* ctx);
 int mdx_make_guess(mdx_ctx_t* ctx, bool* made);
@@ -315,10 +315,10 @@ int mdx_make_guess(mdx_ctx_t* ctx, bool* made);
 int mdx_guess_apply(mdx_ctx_t* ctx, double dg, double r0, bool* guessed, double* rg);
 // learned correction of an applied extrapolated guess and snapshot capture (k_unet.cu)
 int mdx_unet_correct(mdx_ctx_t* ctx, double dg, double* rg);
-int mdx_unet_finish(mdx_ctx_t* ctx, bool converged);
+int mdx_unet_finish(mdx_ctx_t* ctx, bool converged, int iterations);
 // The learned correction for another grid (an ensemble member), no host read
 // (k_unet.cu): delta and its flag *ok on the device.
-int mdx_unet_member_delta(mdx_ctx_t* nc, const mdx_dims& dm, double dx, double dy, double dz, double dg,
+int mdx_unet_member_delta(mdx_ctx_t* nc, const mdx_dims& dm, double dx, double dy, double dz, double ire, double dg,
                           const double* un, const double* vn, const double* wn, const double* dp1, const double* dp2,
                           const double* mu_planes, double* delta, double* scal, int* ok);
 void mdx_unet_free(mdx_ctx_t* ctx);

@@ -95,10 +95,12 @@ def record_and_train(s: Solver, g, runs, warm_steps: int = 3, record_steps: int 
                       snapshots=int(st.snapshots), record_seconds=rec, train_ms=tm + st.train_ms, runs=list(runs))
 
 
-def load_into(s: Solver, net: TrainedNet, step_rule: int = 0) -> None:
+def load_into(s: Solver, net: TrainedNet, step_rule: int = 0, gate_period: int = 0) -> None:
     """Give solver `s` (same grid) the trained network, without snapshot
-    storage; step_rule 1 scales each correction by its energy-optimal step."""
+    storage; step_rule 1 scales each correction by its energy-optimal step;
+    gate_period > 0 applies the correction per RK substage only while it
+    takes fewer iterations than the extrapolated guess alone."""
     s.unet_create(channels=net.channels, extra_bottleneck=net.extra_bottleneck, capacity=0, slope=net.slope,
-                  step_rule=step_rule)
+                  step_rule=step_rule, gate_period=gate_period)
     s.unet_set_params(net.params)
     s.unet_out_scale(net.out_scale)

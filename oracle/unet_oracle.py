@@ -30,7 +30,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-NIN = 4
+NIN = 5
 C_IN = 16
 
 
@@ -138,7 +138,7 @@ def loss_grad(net: Net, params: np.ndarray, in4: np.ndarray, target: np.ndarray,
               masks=None, return_masks: bool = False):
     """Forward and backward of the network on one field.
 
-    in4: [4][n] cell inputs (x fastest), target: [n], shape = (nx, ny, nz).
+    in4: [NIN][n] cell inputs (x fastest), target: [n], shape = (nx, ny, nz).
     Returns (loss, grad (flat like params), out [n]).  loss = mean((out-t)^2).
     ``masks`` (one boolean array per convolution, as returned with
     ``return_masks``) fixes which pre-activations count as positive, so that

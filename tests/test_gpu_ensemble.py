@@ -216,23 +216,33 @@ def test_learned_warm_start_in_the_ensemble():
     opts = M.make_solver_opts(M.SOLVER_REDBLACK, sor=1.7, tol=1e-8, check_every=10, max_iter=200000,
                               precision=M.PREC_MIXED, adaptive_checks=False)
     out = {}
-    for mode in (M.GUESS_EXTRAPOLATED, M.GUESS_LEARNED):
+    for mode in (M.GUESS_EXTRAPOLATED, M.GUESS_LEARNED, "gated"):
         with M.Ensemble(mems, opts) as E:
             if mode == M.GUESS_LEARNED:
                 E.unet_load(net.params, net.out_scale, channels=net.channels)
+            if mode == "gated":   # the correction per member and substage only while it saves iterations
+                E.unet_load(net.params, net.out_scale, channels=net.channels, gate_period=4)
+                mode = M.GUESS_LEARNED
+                key = "gated"
+            else:
+                key = mode
             E.set_guess(mode)
             E.ic()
             its = E.step(6)
             for q in range(len(mems)):
                 st, _ = E.member_stats(q)
                 assert st.status == 0, (mode, q)
-            out[mode] = (its, [E.get(q, "un") for q in range(len(mems))], [E.get(q, "vn") for q in range(len(mems))],
-                         E.unet_stats() if mode == M.GUESS_LEARNED else None, E.info())
-    its_l, u_l, v_l, (kept, undone), info = out[M.GUESS_LEARNED]
+            out[key] = (its, [E.get(q, "un") for q in range(len(mems))], [E.get(q, "vn") for q in range(len(mems))],
+                        E.unet_stats() if mode == M.GUESS_LEARNED else None, E.info())
+    its_l, u_l, v_l, (kept, undone, gated), info = out[M.GUESS_LEARNED]
     its_x, u_x, v_x, _, _ = out[M.GUESS_EXTRAPOLATED]
+    its_g, u_g, _, (kept_g, undone_g, gated_g), _ = out["gated"]
     print("iterations extrapolated", its_x, "learned", its_l, "corrections kept", kept, "undone", undone,
-          "graph", info["graph"])
-    assert kept + undone > 0
+          "graph", info["graph"], "gated: iterations", its_g, "kept", kept_g, "undone", undone_g, "left", gated_g)
+    assert kept + undone > 0 and gated == 0
+    assert gated_g > 0 and kept_g + undone_g > 0
+    for q in range(len(mems)):
+        assert rel_l2(u_g[q], u_x[q]) <= 1e-6, q
     for q in range(len(mems)):
         assert rel_l2(u_l[q], u_x[q]) <= 1e-6, q
     assert info["graph"]

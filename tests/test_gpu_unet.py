@@ -42,7 +42,7 @@ def test_unet_loss_and_gradients_match_cpu_network(c1, pery, extra):
         s.unet_set_params(p)
         assert np.array_equal(s.unet_params(), p)
         rng = np.random.default_rng(5)
-        in4 = rng.standard_normal((4, n)).astype(np.float32)
+        in4 = rng.standard_normal((5, n)).astype(np.float32)
         t = rng.standard_normal(n).astype(np.float32)
         lg, gg, og = s.unet_loss_grad(in4, t)
         lc, gc, oc = UO.loss_grad(net, p.astype(np.float64), in4, t, (nx, ny, nz), bf16=True)
@@ -66,7 +66,7 @@ def test_tcgen05_convolutions_match_mma_and_cpu_network(pery):
     n = nx * ny * nz
     slope = 0.1
     rng = np.random.default_rng(9)
-    in4 = rng.standard_normal((4, n)).astype(np.float32)
+    in4 = rng.standard_normal((5, n)).astype(np.float32)
     t = rng.standard_normal(n).astype(np.float32)
     net = UO.Net(c0=16, c1=32, extra=0, slope=slope, pery=pery)
     p = UO.init_params(net, 21).astype(np.float32)
@@ -146,6 +146,22 @@ def test_snapshots_train_and_learned_guess_gain():
         assert l2 <= max(1e-8 * ls.residual0, ls.atol) * 1.0000001
         for n in ("un", "vn", "wn"):
             assert rel_l2(sl.get(n), se.get(n)) <= 1e-6, n
+    # the gate: per substage the first eligible projection runs without the
+    # correction, the next with it, then the one that took fewer iterations,
+    # the other re-tried every 4th projection; every eligible projection is
+    # either corrected, undone or left to the extrapolated guess
+    sg = _wavy(202, 3000.0, M.GUESS_LEARNED)
+    with sg:
+        sg.unet_create(channels=32, capacity=0, slope=0.1, gate_period=4)
+        sg.unet_set_params(params)
+        sg.unet_out_scale(scale)
+        sg.step(3)
+        sg.step(8)
+        st = sg.unet_stats()
+        print("gate: corrections", st.corrections, "rejected", st.rejected, "left to extrapolation", st.gated)
+        assert st.gated >= 3
+        assert st.corrections + st.rejected + st.gated == 24
+        assert sg.last_solve_stats().status == 0
 
 
 def test_unet_argument_checks():

@@ -14,7 +14,7 @@ def test_oracle_gradient_matches_finite_differences(pery, extra):
     n = 16 * 8 * 8
     rng = np.random.default_rng(7)
     p = U.init_params(net, 3)
-    in4 = rng.standard_normal((4, n))
+    in4 = rng.standard_normal((5, n))
     t = rng.standard_normal(n)
     loss, g, out, masks = U.loss_grad(net, p, in4, t, shape, bf16=False, return_masks=True)
     assert out.shape == (n,) and g.shape == p.shape
