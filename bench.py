@@ -1033,10 +1033,10 @@ def run_learned_eval(args, cfg):
     nsub = 3 * steps * len(held)
     summary = {m: {"iters_per_substage": totals[m][0] / nsub,
                    "mcell_steps_s": cells * steps * len(held) / totals[m][1] / 1e6} for m, _ in modes}
-    head = "learned_gated" if "learned_gated" in summary else "learned"
+    head = "learned" if "learned" in summary else "learned_gated"
     ratios = {f"reduction_vs_{b}": summary[b]["iters_per_substage"] / summary[head]["iters_per_substage"]
               for b in ("zero", "previous", "extrapolated") if b in summary}
-    for m in ("learned", "learned_energy"):
+    for m in ("learned_gated", "learned_energy"):
         if m in summary and m != head and "extrapolated" in summary:
             ratios[f"{m}_reduction_vs_extrapolated"] = (summary["extrapolated"]["iters_per_substage"] /
                                                         summary[m]["iters_per_substage"])

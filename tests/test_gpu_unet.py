@@ -108,8 +108,9 @@ def _wavy(seed, re, mode, nx=64, ny=32, nz=32, amp=0.05, tol=1e-8):
 def test_snapshots_train_and_learned_guess_gain():
     """Snapshots recorded by one wavy-channel run (Re 2500) train the net;
     on a held-out run (Re 3000, another seed) the learned correction lowers
-    the divergence the extrapolated guess leaves, the sweeps still run to
-    the same tolerance, and the result agrees with the run without it."""
+    the divergence the extrapolated guess leaves and the iterations below
+    those of the extrapolated guess, the sweeps still run to the same
+    tolerance, and the result agrees with the run without it."""
     tr = _wavy(101, 2500.0, M.GUESS_EXTRAPOLATED)
     with tr:
         tr.unet_create(channels=32, capacity=48, slope=0.1)
@@ -139,7 +140,7 @@ def test_snapshots_train_and_learned_guess_gain():
               "inference ms", st.infer_ms)
         assert st.corrections == 12 and st.rejected == 0
         assert st.last_gain >= 2.0          # ||div|| after extrapolation / after the correction
-        assert il <= 1.1 * ie
+        assert il < ie                      # strictly fewer iterations on the held-out Re
         ls = sl.last_solve_stats()
         assert ls.status == 0 and ls.guessed == 1
         l2, _ = sl.divergence_norms()
