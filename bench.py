@@ -159,7 +159,8 @@ C3_GATE_PERIOD = 16   # the learned_gated guess re-tries the other choice every 
 SOR_VARIANT = 0   # --sor-variant: red-black kernel variant (0: the autotuner's choice)
 FFT_KERNEL = 0    # --fft-kernel: 0 warp-shuffle transforms where the lengths allow, 1 Stockham
 SOR_NAMES = {1: "one launch per colour sweep", 2: "fused red+black pass 32x8", 3: "fused red+black pass 32x16",
-             4: "one launch per colour sweep on colour-split copies"}
+             4: "one launch per colour sweep on colour-split copies",
+             5: "one launch per colour sweep on colour-split copies, 2 cells per thread"}
 
 
 # FP32 correction sweeps of the mixed path, by the hundreds digit of the
@@ -172,7 +173,7 @@ SOR32_TRAFFIC = {1: "sor_sweep32", 3: "rb32_fused", 5: "sor_sweep32v"}
 
 def _sor64_traffic_key(variant):
     """traffic.json entry of the FP64 sweep kernel a solve ran."""
-    return "sor_sweep_split" if variant == 4 else "sor_sweep"
+    return {4: "sor_sweep_split", 5: "sor_sweep_splitv"}.get(variant, "sor_sweep")
 
 
 def _setup(cfg, M, device, profile=False, tol=None, precision=None, seed=None):
@@ -1259,7 +1260,7 @@ def main():
     ap.add_argument("--profile-mixed", action="store_true",
                     help="profiling run for ncu: the full-size t=0 projection with FP32 sweeps to residual 1e-8")
     ap.add_argument("--quick", action="store_true", help="skip the plain FP64 leg at residual 1e-10")
-    ap.add_argument("--sor-variant", type=int, default=0, choices=[0, 1, 2, 3, 4],
+    ap.add_argument("--sor-variant", type=int, default=0, choices=[0, 1, 2, 3, 4, 5],
                     help="red-black kernel variant (0: autotuned; all give the same bits)")
     ap.add_argument("--fft-kernel", type=int, default=0, choices=[0, 1],
                     help="FFT path transforms: 0 warp-shuffle where nx/2 and nz allow, 1 shared-memory Stockham")

@@ -96,12 +96,13 @@ typedef struct {
                           block of its own iterations and keeps the fastest; 1 one
                           launch per colour; 2 fused red+black pass, 32x8 tiles;
                           3 fused pass, 32x16 tiles; 4 one launch per colour on
-                          colour-split copies of u, v, w, p made once per projection
-                          (2-4: periodic x and z, IBM factors 1 or z-invariant).
+                          colour-split copies of u, v, w, p made once per projection;
+                          5 the same with two cells per thread and 16-byte accesses
+                          (2-5: periodic x and z, IBM factors 1 or z-invariant).
                           FP32 sweeps of the mixed precision: 1 one launch per colour,
                           one cell per thread; 2 or 3 the fused red+black pass (one
-                          launch per iteration) in the fastest of four tile shapes; 4 one
-                          launch per colour with 2 or 4 cells per thread, the faster;
+                          launch per iteration) in the fastest of four tile shapes; 4 or
+                          5 one launch per colour with 2 or 4 cells per thread, the faster;
                           0 the fastest of all seven, each timed on one block of the
                           first iterations (all give the same bits) */
     int sor_kz;        /* z planes per block of the fused pass (0: default 16) */

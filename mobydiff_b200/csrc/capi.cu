@@ -247,6 +247,8 @@ int mdx_destroy_pressure_solver(mdx_ctx_t* ctx) {
         cudaFree(ctx->split_f[t]);
         ctx->split_f[t] = nullptr;
     }
+    cudaFree(ctx->split_tab);
+    ctx->split_tab = nullptr;
     ctx->split_norms = false;
     mdx_mixed_free(ctx);
     mdx_warm_free(ctx);

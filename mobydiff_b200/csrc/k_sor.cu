@@ -420,6 +420,147 @@ k_sor_sweep_split(mdx_dims d, mdx_bc_dev bc, mdx_sor_params p, int parity, int r
     pn[c] = pc;
 }
 
+// The IBM factors (1 without IBM) and -omega/denom of every (i, j) column in
+// colour-split planes (pidx2) for k_sor_sweep_splitv: [mu_u | mu_v | mu_w |
+// fac], each split_plane_elems long.  fac is sor_factor of the column -- the
+// FP64 expression the other kernels evaluate per cell; with z-invariant
+// factors it is the same for every cell of the column, so the same bits.
+template <int MU>
+__global__ void k_split_tables(mdx_dims d, int py, mdx_sor_params p, const double* __restrict__ mu,
+                               double* __restrict__ tab) {
+    const long long np = (long long)d.nxp * d.nyp;
+    const int ps = split_plane_elems(d);
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < np; t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % d.nxp), j = (int)(t / d.nxp);
+        double mu_u = 1.0, mu_v = 1.0, mu_w = 1.0;
+        if (MU == MU_PLANE) {
+            mu_u = __ldg(mu + t);
+            mu_v = __ldg(mu + np + t);
+            mu_w = __ldg(mu + 2 * np + t);
+        }
+        const int o = pidx2(d, i, j);
+        tab[o] = mu_u;
+        tab[ps + o] = mu_v;
+        tab[2 * ps + o] = mu_w;
+        double f = 0.0;
+        if (i >= 1 && i <= d.nx && j >= 1 && j <= d.ny) {
+            const int ip = i == d.nx ? 1 : i + 1;
+            const int jp = (py && j == d.ny) ? 1 : j + 1;
+            double mu_uip = 1.0, mu_vjp = 1.0;
+            if (MU == MU_PLANE) {
+                mu_uip = __ldg(mu + ip + (long long)d.nxp * j);
+                mu_vjp = __ldg(mu + np + i + (long long)d.nxp * jp);
+            }
+            f = sor_factor(mu_u, mu_uip, mu_v, mu_vjp, mu_w, mu_w, p);
+        }
+        tab[3 * ps + o] = f;
+    }
+}
+
+__device__ __forceinline__ void ld2(double (&a)[2], const double* q) {
+    const double2 v = *reinterpret_cast<const double2*>(q);
+    a[0] = v.x;
+    a[1] = v.y;
+}
+__device__ __forceinline__ void ld2_ro(double (&a)[2], const double* __restrict__ q) {
+    const double2 v = __ldg(reinterpret_cast<const double2*>(q));
+    a[0] = v.x;
+    a[1] = v.y;
+}
+__device__ __forceinline__ void st2(double* q, const double (&a)[2]) {
+    *reinterpret_cast<double2*>(q) = make_double2(a[0], a[1]);
+}
+
+// One FP64 colour sweep on the colour-split copies with two consecutive cells
+// of the swept colour per thread, moved with 16-byte accesses: the layout
+// and ownership of k_sor_sweep32v (k_sor_mixed.cu) -- a thread owns window w
+// (positions 2w, 2w + 1) of its row in the swept colour's half and of the
+// other half's rows (j + 1, k) and (j, k + 1); the x neighbours' faces u(i+1)
+// are the window shifted by one in rows whose swept cells have odd i (window
+// plus one scalar), the window itself in the others except the wrap of cell
+// nx to position 0, and are stored one scalar per cell; positions without a
+// swept cell are written back unchanged.  The factors come from
+// k_split_tables.  The per-cell arithmetic is sor_cell_fac, as in
+// k_sor_sweep_split, so the same bits.  Periodic x and z.
+template <int PY>
+__global__ void __launch_bounds__(128)
+k_sor_sweep_splitv(mdx_dims d, mdx_bc_dev bc, mdx_sor_params p, int parity, int reverse, int nwin,
+                   double* __restrict__ un, double* __restrict__ vn, double* __restrict__ wn,
+                   double* __restrict__ pn, const double* __restrict__ tab) {
+    const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long per_plane = (long long)nwin * d.ny;
+    if (g >= per_plane * d.nz) return;
+    const int kk = (int)(g / per_plane);
+    const int rem = (int)(g - (long long)kk * per_plane);
+    const int j = rem / nwin + 1;
+    const int p0 = 2 * (rem - (j - 1) * nwin);
+    const int k = reverse ? d.nz - kk : kk + 1;
+    const int cs = 1 - parity;            // colour (i + j + k) & 1 of the swept cells
+    const int eo = (cs + j + k) & 1;      // i & 1 of the swept cells of this row
+    const int half = d.nx / 2;
+    const int jp = (PY && j == d.ny) ? 1 : j + 1;
+    const int kp = (k == d.nz) ? 1 : k + 1;
+    const long long H = (long long)d.hs * d.nyp * d.nzp;
+    const long long own = cs * H + ((long long)k * d.nyp + j) * d.hs + p0;
+    const long long oth = (1 - cs) * H + ((long long)k * d.nyp + j) * d.hs;
+    const long long ojp = (1 - cs) * H + ((long long)k * d.nyp + jp) * d.hs + p0;
+    const long long okp = (1 - cs) * H + ((long long)kp * d.nyp + j) * d.hs + p0;
+    const int PH = d.hs * d.nyp, ps = 2 * PH;
+    const int hp = (eo + j) & 1;
+    const int mown = hp * PH + j * d.hs + p0;
+    const int mox = (1 - hp) * PH + j * d.hs;
+    const int mjp = (1 - hp) * PH + jp * d.hs + p0;
+
+    double u0[2], ux[2], v0[2], vy[2], w0[2], wz[2], q[2];
+    double mu_u[2], mu_ux[2], mu_v[2], mu_vy[2], mu_w[2], fc[2];
+    ld2(u0, un + own);
+    ld2(v0, vn + own);
+    ld2(w0, wn + own);
+    ld2(q, pn + own);
+    ld2(ux, un + oth + p0);
+    ld2(vy, vn + ojp);
+    ld2(wz, wn + okp);
+    ld2_ro(mu_u, tab + mown);
+    ld2_ro(mu_v, tab + ps + mown);
+    ld2_ro(mu_w, tab + 2 * ps + mown);
+    ld2_ro(fc, tab + 3 * ps + mown);
+    ld2_ro(mu_ux, tab + mox + p0);
+    ld2_ro(mu_vy, tab + ps + mjp);
+    const int xe = eo ? p0 + 2 : 0;
+    const bool need_xe = eo ? (p0 + 2 < d.hs) : (half >= p0 && half < p0 + 2);
+    double uxe = 0.0, muxe = 0.0;
+    if (need_xe) {
+        uxe = un[oth + xe];
+        muxe = __ldg(tab + mox + xe);
+    }
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+        const int pe = p0 + e;
+        const bool valid = eo ? (pe < half) : (pe >= 1 && pe <= half);
+        const bool wrap = !eo && pe == half;
+        double u_ip, mu_ip;
+        if (e == 0) {
+            u_ip = eo ? ux[1] : (wrap ? uxe : ux[0]);
+            mu_ip = eo ? mu_ux[1] : (wrap ? muxe : mu_ux[0]);
+        } else {
+            u_ip = (eo || wrap) ? uxe : ux[1];
+            mu_ip = (eo || wrap) ? muxe : mu_ux[1];
+        }
+        if (valid) {
+            const int i = 2 * pe + eo;
+            sor_cell_fac<1, PY, 1>(u0[e], u_ip, v0[e], vy[e], w0[e], wz[e], q[e], mu_u[e], mu_ip, mu_v[e], mu_vy[e],
+                                   mu_w[e], mu_w[e], fc[e], p, bc, i, j, k, d.nx, d.ny, d.nz);
+            un[oth + (eo ? pe + 1 : (wrap ? 0 : pe))] = u_ip;
+        }
+    }
+    st2(un + own, u0);
+    st2(vn + own, v0);
+    st2(wn + own, w0);
+    st2(pn + own, q);
+    st2(vn + ojp, vy);
+    st2(wn + okp, wz);
+}
+
 // Every padded element of u, v, w, p between the reference layout and the
 // colour-split copies (TO_SPLIT) or back.
 template <bool TO_SPLIT>
@@ -488,6 +629,8 @@ static int sor_iteration(mdx_ctx_t* ctx, const mdx_sor_params& p) {
 //   MDX_SORV_SPLIT     one launch per colour sweep on colour-split copies
 //                      (tol > 0 only: the copies cost two passes over u, v,
 //                      w, p per projection)
+//   MDX_SORV_SPLITV    the same with two cells per thread and 16-byte
+//                      accesses, the column factors from tables
 // All but the first need periodic x and z and mu = 1 or z-invariant.
 // (the enum is in mdx_internal.cuh)
 
@@ -495,6 +638,34 @@ static int split_alloc(mdx_ctx_t* ctx) {
     const size_t bytes = sizeof(double) * (size_t)split_elems(ctx->d);
     for (int t = 0; t < 4; ++t)
         if (!ctx->split_f[t]) MDX_CUDA(ctx, cudaMalloc(&ctx->split_f[t], bytes));
+    if (!ctx->split_tab) {
+        const size_t tb = sizeof(double) * 4 * (size_t)split_plane_elems(ctx->d);
+        MDX_CUDA(ctx, cudaMalloc(&ctx->split_tab, tb));
+        MDX_CUDA(ctx, cudaMemsetAsync(ctx->split_tab, 0, tb, ctx->stream));
+    }
+    return MDX_OK;
+}
+
+// The column factors of this projection for k_sor_sweep_splitv.
+static int split_tables(mdx_ctx_t* ctx, const mdx_sor_params& p) {
+    const mdx_dims& d = ctx->d;
+    const int py = ctx->bc.is_periodic[1] ? 1 : 0;
+    const int nb = (int)std::min<long long>(((long long)d.nxp * d.nyp + 255) / 256, 1024);
+    auto kfn = ctx->mu_mode == MU_PLANE ? k_split_tables<MU_PLANE> : k_split_tables<MU_ONE>;
+    MDX_LAUNCH(ctx, MDX_T_OTHER, "split tables", kfn, nb, 256, 0, d, py, p, ctx->mu, ctx->split_tab);
+    return MDX_OK;
+}
+
+static int sor_splitv_iteration(mdx_ctx_t* ctx, const mdx_sor_params& p) {
+    const mdx_dims& d = ctx->d;
+    double** s = ctx->split_f;
+    const int nwin = (d.nx / 2 + 2) / 2;   // windows of two positions covering 0 .. nx/2
+    const long long nthr = (long long)nwin * d.ny * d.nz;
+    const int nb = (int)((nthr + 127) / 128);   // 128-thread blocks: 5 per SM at 92 registers
+    auto kfn = ctx->bc.is_periodic[1] ? k_sor_sweep_splitv<1> : k_sor_sweep_splitv<0>;
+    for (int parity = 0; parity < 2; ++parity)
+        MDX_LAUNCH(ctx, MDX_T_SOR_SWEEP, "sor sweep split vec", kfn, nb, 128, 0, d, ctx->bcd, p, parity, parity, nwin,
+                   s[0], s[1], s[2], s[3], ctx->split_tab);
     return MDX_OK;
 }
 
@@ -587,6 +758,7 @@ static int sor_fused_iteration(mdx_ctx_t* ctx, const mdx_sor_params& p) {
 
 static int sor_iterate(mdx_ctx_t* ctx, const mdx_sor_params& p, int variant) {
     if (variant == MDX_SORV_SPLIT) return sor_split_iteration(ctx, p);
+    if (variant == MDX_SORV_SPLITV) return sor_splitv_iteration(ctx, p);
     if (variant == MDX_SORV_FUSED8) return sor_fused_iteration<8, 256>(ctx, p);
     if (variant == MDX_SORV_FUSED16) return sor_fused_iteration<16, 512>(ctx, p);
     return sor_iteration(ctx, p);
@@ -658,13 +830,15 @@ int mdx_k_projection_redblack(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t* st) 
     if (want < MDX_SORV_AUTO || want >= MDX_SORV_NUM) want = MDX_SORV_AUTO;
     if (want != MDX_SORV_SWEEPS && !fok) want = MDX_SORV_SWEEPS;
     if (want == MDX_SORV_AUTO || want == MDX_SORV_FUSED8 || want == MDX_SORV_FUSED16) MDX_TRY(fused_prepare(ctx));
-    if (want == MDX_SORV_AUTO || want == MDX_SORV_SPLIT) MDX_TRY(split_alloc(ctx));
+    const bool splitv = want == MDX_SORV_AUTO || want == MDX_SORV_SPLITV;
+    if (want == MDX_SORV_AUTO || want == MDX_SORV_SPLIT || splitv) MDX_TRY(split_alloc(ctx));
     const mdx_sor_params p = sor_params(ctx, dg);
+    if (splitv) MDX_TRY(split_tables(ctx, p));
     // where u, v, w, p live while the sweeps run: the colour-split copies for
     // MDX_SORV_SPLIT blocks, the reference arrays for the others
     bool in_split = false;
     auto layout_for = [&](int v) -> int {
-        if ((v == MDX_SORV_SPLIT) != in_split) {
+        if ((v == MDX_SORV_SPLIT || v == MDX_SORV_SPLITV) != in_split) {
             in_split = !in_split;
             MDX_TRY(split_copy(ctx, in_split));
         }

@@ -648,7 +648,7 @@ int mdx_k_projection_redblack_mixed(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t
         cands[ncand++] = CAND_SWEEPS;
     } else if (o.sor_variant == MDX_SORV_FUSED8 || o.sor_variant == MDX_SORV_FUSED16) {
         for (int c = 0; c < RB32_SHAPES; ++c) cands[ncand++] = c;
-    } else if (o.sor_variant == MDX_SORV_SPLIT) {
+    } else if (o.sor_variant == MDX_SORV_SPLIT || o.sor_variant == MDX_SORV_SPLITV) {
         cands[ncand++] = CAND_VEC2;
         cands[ncand++] = CAND_VEC4;
     } else {

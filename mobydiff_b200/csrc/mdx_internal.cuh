@@ -65,7 +65,7 @@ __host__ __device__ inline int split_plane_elems(const mdx_dims& d) { return 2 *
 // Red-black kernel variants (opts.sor_variant; k_sor.cu, k_sor_mixed.cu).
 enum {
     MDX_SORV_AUTO = 0, MDX_SORV_SWEEPS = 1, MDX_SORV_FUSED8 = 2, MDX_SORV_FUSED16 = 3, MDX_SORV_SPLIT = 4,
-    MDX_SORV_NUM = 5
+    MDX_SORV_SPLITV = 5, MDX_SORV_NUM = 6
 };
 
 // A step scalar (dt times an RK coefficient) handed to a kernel either by
@@ -126,6 +126,7 @@ struct mdx_ctx {
     bool coef_zinv = false;                  // coefficients equal on every z plane
     double* sor_alt[4] = {nullptr};          // second u,v,w,p state of the fused red-black pass
     double* split_f[4] = {nullptr};          // colour-split copies of u,v,w,p (split sweeps)
+    double* split_tab = nullptr;             // their column factors: mu_u, mu_v, mu_w, fac planes (pidx2)
     bool split_norms = false;                // divergence norms read colour-split arrays
     bool fused_attr = false;
     // mixed-precision red-black: FP32 corrections, FP32 residual, IBM tables,

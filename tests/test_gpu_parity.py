@@ -69,12 +69,13 @@ def test_apply_bc_redblack_bitwise(bcname):
 
 @pytest.mark.parametrize("bcname", list(BC_CASES))
 @pytest.mark.parametrize("ibm", ["none", "random", "zinv"])
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5])
 def test_redblack_fixed_iterations_bitwise(bcname, ibm, variant):
     """pressure_projection_redblack with the reference's fixed nIter: bit-exact with
     every kernel variant -- one launch per colour sweep (1), the fused red+black passes
-    (2, 3), the sweeps on colour-split copies (4), the autotuner's choice (0); 2-4 run
-    when x and z are periodic and the IBM factors are 1 or z-invariant."""
+    (2, 3), the sweeps on colour-split copies (4) and with two cells per thread (5), the
+    autotuner's choice (0); 2-5 run when x and z are periodic and the IBM factors are 1
+    or z-invariant."""
     g = O.Grid(16, 10, 12, lx=1.3, ly=0.7, lz=2.0, re=500.0)
     bc = BC_CASES[bcname]()
     f = random_fields(g, 7, ibm)
@@ -88,7 +89,7 @@ def test_redblack_fixed_iterations_bitwise(bcname, ibm, variant):
 
 @pytest.mark.parametrize("shape,kz", [((36, 10, 6), 4), ((64, 24, 20), 16), ((40, 12, 10), 3), ((96, 48, 34), 8)])
 @pytest.mark.parametrize("bcname", ["periodic", "channel"])
-@pytest.mark.parametrize("variant", [2, 3, 4])
+@pytest.mark.parametrize("variant", [2, 3, 4, 5])
 def test_redblack_fused_partial_tiles_bitwise(shape, kz, bcname, variant):
     """Fused passes on grids that are not multiples of their 32x8 / 32x16 tiles or z
     chunk, and the colour-split sweeps on the same odd sizes."""
@@ -104,7 +105,7 @@ def test_redblack_fused_partial_tiles_bitwise(shape, kz, bcname, variant):
     assert all(v == 0.0 for v in diff.values()), diff
 
 
-@pytest.mark.parametrize("variant", [0, 1, 4])
+@pytest.mark.parametrize("variant", [0, 1, 4, 5])
 def test_redblack_residual_driven_matches_oracle(variant):
     g, bc = channel_case(32, 16, 16, re=3000.0)
     f = O.Fields(g)
