@@ -925,6 +925,35 @@ def run_profile_mixed(args, cfg):
     return 0
 
 
+def run_profile_ensemble(args, cfg):
+    """The first N members of the C4 ensemble (extrapolated start, FP32 sweeps
+    in FP64 defect correction, residual 1e-8), 3 warm-up steps and 2 more, no
+    autotuning (for an ncu capture of one substage launch); prints each
+    member's iterations over the last 2 steps."""
+    import torch
+    import mobydiff_b200 as M
+    _, rank, local = _dist()
+    torch.cuda.set_device(local)
+    n = args.profile_ensemble
+    mems = ensemble_members(M, n)
+    opts = M.make_solver_opts(M.SOLVER_REDBLACK, sor=cfg["sor"], tol=cfg["tol"], check_every=cfg["check_every"],
+                              max_iter=400000, precision=M.PREC_MIXED)
+    E = M.Ensemble(mems, opts, local)
+    E.set_guess(M.GUESS_EXTRAPOLATED)
+    E.ic()
+    E.step(3)
+    it0 = [E.member_stats(q)[1] for q in range(n)]
+    E.step(2)
+    its = [E.member_stats(q)[1] - it0[q] for q in range(n)]
+    info = E.info()
+    E.close()
+    if rank == 0:
+        print(json.dumps({"profile_run": f"first {n} members of the C4 ensemble, 3 + 2 steps",
+                          "cells": sum(m.nx * m.ny * m.nz for m in mems), "iters_per_member_2_steps": its,
+                          "threads": info.get("threads"), "grid": info.get("grid")}), flush=True)
+    return 0
+
+
 def run_profile_unet(args, cfg):
     """One forward + backward pass of the learned warm start's network on
     random inputs of the workload's grid (for an ncu capture of a few
@@ -1257,6 +1286,8 @@ def main():
                     help="profiling run for ncu: full-size state, fixed 20 red-black iterations per projection")
     ap.add_argument("--profile-unet", action="store_true",
                     help="one network forward + backward on the workload's grid (for an ncu capture)")
+    ap.add_argument("--profile-ensemble", type=int, default=0, metavar="N",
+                    help="profiling run for ncu: the first N members of the C4 ensemble, 3 + 2 steps")
     ap.add_argument("--profile-mixed", action="store_true",
                     help="profiling run for ncu: the full-size t=0 projection with FP32 sweeps to residual 1e-8")
     ap.add_argument("--quick", action="store_true", help="skip the plain FP64 leg at residual 1e-10")
@@ -1279,6 +1310,8 @@ def main():
         return run_reference(args, cfg)
     if args.profile_mixed:
         return run_profile_mixed(args, cfg)
+    if args.profile_ensemble:
+        return run_profile_ensemble(args, cfg)
     if args.profile_unet:
         return run_profile_unet(args, cfg)
     if cfg["method"] == "ensemble":
