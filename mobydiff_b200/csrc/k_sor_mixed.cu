@@ -168,7 +168,7 @@ __device__ __forceinline__ void st_vec(float* p, const float (&a)[V]) {
 // bit.  Needs nx and nz even, and ny even when y is periodic (every neighbour
 // has the other colour).
 template <int PY, int V>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, V == 4 ? 3 : 1)
 k_sor_sweep32v(mdx_dims d, mixed_params P, int parity, int reverse, int nwin, float* __restrict__ du,
                float* __restrict__ dv, float* __restrict__ dw, float* __restrict__ dp, const float* __restrict__ r,
                const float* __restrict__ mu32, const float* __restrict__ fac32) {
@@ -196,6 +196,10 @@ k_sor_sweep32v(mdx_dims d, mixed_params P, int parity, int reverse, int nwin, fl
     const int mox = (1 - hp) * PH + j * d.hs;
     const int mjp = (1 - hp) * PH + jp * d.hs + p0;
 
+    // V = 4 reads the z-invariant factor planes (L1-resident) per cell when
+    // it uses them instead of holding them as vectors: 80 registers, three
+    // blocks per SM instead of two
+    constexpr bool SMU = V == 4;
     float u0[V], ux[V], v0[V], vy[V], w0[V], wz[V], q[V], rr[V];
     float mu_u[V], mu_ux[V], mu_v[V], mu_vy[V], mu_w[V], fc[V];
     ld_vec<V>(u0, du + own);
@@ -206,12 +210,14 @@ k_sor_sweep32v(mdx_dims d, mixed_params P, int parity, int reverse, int nwin, fl
     ld_vec<V>(vy, dv + ojp);
     ld_vec<V>(wz, dw + okp);
     ld_vec_ro<V>(rr, r + own);
-    ld_vec_ro<V>(mu_u, mu32 + mown);
-    ld_vec_ro<V>(mu_v, mu32 + np + mown);
-    ld_vec_ro<V>(mu_w, mu32 + 2 * np + mown);
-    ld_vec_ro<V>(fc, fac32 + mown);
-    ld_vec_ro<V>(mu_ux, mu32 + mox + p0);
-    ld_vec_ro<V>(mu_vy, mu32 + np + mjp);
+    if constexpr (!SMU) {
+        ld_vec_ro<V>(mu_u, mu32 + mown);
+        ld_vec_ro<V>(mu_v, mu32 + np + mown);
+        ld_vec_ro<V>(mu_w, mu32 + 2 * np + mown);
+        ld_vec_ro<V>(fc, fac32 + mown);
+        ld_vec_ro<V>(mu_ux, mu32 + mox + p0);
+        ld_vec_ro<V>(mu_vy, mu32 + np + mjp);
+    }
     // the x-neighbour face one past the window (odd i), or the wrap target
     // position 0 of cell nx (even i)
     const int xe = eo ? p0 + V : 0;
@@ -219,7 +225,7 @@ k_sor_sweep32v(mdx_dims d, mixed_params P, int parity, int reverse, int nwin, fl
     float uxe = 0.f, muxe = 0.f;
     if (need_xe) {
         uxe = du[oth + xe];
-        muxe = __ldg(mu32 + mox + xe);
+        if constexpr (!SMU) muxe = __ldg(mu32 + mox + xe);
     }
     const bool v_lo = PY || j > 1, v_hi = PY || j < d.ny;   // wall faces v(1), v(ny+1) stay 0
 #pragma unroll
@@ -227,18 +233,24 @@ k_sor_sweep32v(mdx_dims d, mixed_params P, int parity, int reverse, int nwin, fl
         const int p = p0 + e;
         const bool valid = eo ? (p < half) : (p >= 1 && p <= half);
         const bool wrap = !eo && p == half;
-        float uip, muip;
+        const int pip = eo ? p + 1 : (wrap ? 0 : p);   // position of the x neighbour's face
+        float uip, muip = 0.f;
         if (e + 1 < V) {
             uip = eo ? ux[e + 1 < V ? e + 1 : e] : (wrap ? uxe : ux[e]);
-            muip = eo ? mu_ux[e + 1 < V ? e + 1 : e] : (wrap ? muxe : mu_ux[e]);
+            if constexpr (!SMU) muip = eo ? mu_ux[e + 1 < V ? e + 1 : e] : (wrap ? muxe : mu_ux[e]);
         } else {
             uip = (eo || wrap) ? uxe : ux[e];
-            muip = (eo || wrap) ? muxe : mu_ux[e];
+            if constexpr (!SMU) muip = (eo || wrap) ? muxe : mu_ux[e];
         }
         if (valid) {
-            sweep32_update(P, rr[e], u0[e], uip, v0[e], vy[e], w0[e], wz[e], q[e], mu_u[e], muip, mu_v[e],
-                           mu_vy[e], mu_w[e], fc[e], v_lo, v_hi);
-            du[oth + (eo ? p + 1 : (wrap ? 0 : p))] = uip;
+            if constexpr (SMU)
+                sweep32_update(P, rr[e], u0[e], uip, v0[e], vy[e], w0[e], wz[e], q[e], __ldg(mu32 + mown + e),
+                               __ldg(mu32 + mox + pip), __ldg(mu32 + np + mown + e), __ldg(mu32 + np + mjp + e),
+                               __ldg(mu32 + 2 * np + mown + e), __ldg(fac32 + mown + e), v_lo, v_hi);
+            else
+                sweep32_update(P, rr[e], u0[e], uip, v0[e], vy[e], w0[e], wz[e], q[e], mu_u[e], muip, mu_v[e],
+                               mu_vy[e], mu_w[e], fc[e], v_lo, v_hi);
+            du[oth + pip] = uip;
         }
     }
     st_vec<V>(du + own, u0);
