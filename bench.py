@@ -969,7 +969,7 @@ def run_profile_unet(args, cfg):
     s.unet_create(channels=32, capacity=0, slope=0.1)
     n = cfg["nx"] * cfg["ny"] * cfg["nz"]
     rng = np.random.default_rng(SEED)
-    loss, _, _ = s.unet_loss_grad(rng.standard_normal((4, n)).astype(np.float32),
+    loss, _, _ = s.unet_loss_grad(rng.standard_normal((M.UNET_INPUTS, n)).astype(np.float32),
                                   rng.standard_normal(n).astype(np.float32))
     st = s.unet_stats()
     if rank == 0:

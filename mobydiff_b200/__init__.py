@@ -51,6 +51,7 @@ PREC_MIXED = 1
 GUESS_ZERO = 0
 GUESS_PREVIOUS = 1
 GUESS_LEARNED = 2
+UNET_INPUTS = 5            # input channels of the warm-start network (mdx_unet_loss_grad)
 GUESS_EXTRAPOLATED = 3
 
 FIELDS = ["un", "us", "vn", "vs", "wn", "ws", "pn", "oldrhsu", "oldrhsv", "oldrhsw",
@@ -620,10 +621,14 @@ class Solver:
         return v.value
 
     def unet_loss_grad(self, in4, target):
-        """One forward/backward pass on host inputs [5][n] and target [n]:
-        (loss, gradient [param_count], output [n])."""
+        """One forward/backward pass on host inputs [UNET_INPUTS][n] and
+        target [n]: (loss, gradient [param_count], output [n])."""
         in4 = np.ascontiguousarray(in4, dtype=np.float32)
         target = np.ascontiguousarray(target, dtype=np.float32)
+        n = int(np.prod(self.interior))
+        if target.size != n or in4.size != UNET_INPUTS * n:
+            raise ValueError(f"unet_loss_grad: inputs must be [{UNET_INPUTS}][{n}] and the target [{n}], "
+                             f"got {in4.shape} and {target.shape}")
         grad = np.empty(self.unet_param_count(), dtype=np.float32)
         out = np.empty(target.size, dtype=np.float32)
         loss = C.c_double(0.0)
