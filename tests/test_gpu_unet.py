@@ -110,7 +110,7 @@ def test_snapshots_train_and_learned_guess_gain():
     on a held-out run (Re 3000, another seed) the learned correction lowers
     the divergence the extrapolated guess leaves, the sweeps still run to
     the same tolerance, and the result agrees with the run without it (the
-    iteration count is judged in the next test, with a training set that
+    iteration count is checked in the next test, with a training set that
     spans the held-out Re)."""
     tr = _wavy(101, 2500.0, M.GUESS_EXTRAPOLATED)
     with tr:
