@@ -44,6 +44,9 @@ namespace cg = cooperative_groups;
 namespace {
 
 constexpr int ETILE = 256;           // elements per work tile
+// cells of one colour per sweep tile: a tile's set-up (the member's views,
+// factors and 1/dt_gamma) is spread over several cells per thread
+constexpr int HTILE = 1024;
 constexpr int MAX_THREADS = 512;
 
 // n / d for 32-bit n by one multiply-high with c = ceil(2^64 / d) (Lemire,
@@ -438,7 +441,7 @@ __device__ __forceinline__ void sweep32_tile(const ens_args& A, int parity, int 
     float *du = M.du, *dv = M.dv, *dw = M.dw, *dp = M.dp;
     const float *r = M.r32, *mu32 = M.mu32, *fac32 = M.fac32;
     const unsigned nh = (unsigned)((d.nx / 2) * d.ny * d.nz);
-    for (int e = threadIdx.x; e < ETILE; e += blockDim.x) {
+    for (int e = threadIdx.x; e < HTILE; e += blockDim.x) {
         const unsigned t = (unsigned)T.y + e;
         if (t >= nh) break;
         const unsigned q = fq(t, fh);
@@ -472,7 +475,7 @@ __device__ __forceinline__ void sweep_tile(const ens_args& A, int parity, int ti
     const sweep_view v = make_view(M);
     const unsigned nh = (unsigned)((v.d.nx / 2) * v.d.ny * v.d.nz);
     const mdx_sor_params p = proj_params(M, dg_of(A, M));
-    for (int e = threadIdx.x; e < ETILE; e += blockDim.x) {
+    for (int e = threadIdx.x; e < HTILE; e += blockDim.x) {
         const unsigned t = (unsigned)T.y + e;
         if (t >= nh) break;
         sweep_cell(v, M.bc, p, parity, t);
@@ -1472,8 +1475,10 @@ int mdx_ensemble_create(int device, int n, const mdx_member_t* members, const md
                                   (long long)d.nx * d.nz, (long long)d.ny * d.nz, (long long)d.nx * d.ny};
         E->cell_begin[m] = (int)E->tiles[0].size();
         E->half_begin[m] = (int)E->tiles[1].size();
-        for (int q = 0; q < 7; ++q)
-            for (long long s0 = 0; s0 < cnt[q]; s0 += ETILE) E->tiles[q].push_back(make_int2(m, (int)s0));
+        for (int q = 0; q < 7; ++q) {
+            const int step = q == 1 ? HTILE : ETILE;   // list 1: the sweep tiles
+            for (long long s0 = 0; s0 < cnt[q]; s0 += step) E->tiles[q].push_back(make_int2(m, (int)s0));
+        }
     }
     E->cell_begin[n] = (int)E->tiles[0].size();
     E->half_begin[n] = (int)E->tiles[1].size();
