@@ -44,9 +44,11 @@ namespace cg = cooperative_groups;
 namespace {
 
 constexpr int ETILE = 256;           // elements per work tile
-// cells of one colour per sweep tile: a tile's set-up (the member's views,
-// factors and 1/dt_gamma) is spread over several cells per thread
-constexpr int HTILE = 1024;
+// cells of one colour per sweep tile.  1024 (the tile set-up spread over
+// more cells per thread) measured 3 % slower on the 64-member C4 ensemble:
+// late in a substage only the slowest members are swept, and four times
+// fewer tiles then keep fewer blocks busy.
+constexpr int HTILE = 256;
 constexpr int MAX_THREADS = 512;
 
 // n / d for 32-bit n by one multiply-high with c = ceil(2^64 / d) (Lemire,
