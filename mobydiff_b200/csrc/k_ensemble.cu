@@ -44,10 +44,11 @@ namespace cg = cooperative_groups;
 namespace {
 
 constexpr int ETILE = 256;           // elements per work tile
-// cells of one colour per sweep tile.  1024 (the tile set-up spread over
-// more cells per thread) measured 3 % slower on the 64-member C4 ensemble:
-// late in a substage only the slowest members are swept, and four times
-// fewer tiles then keep fewer blocks busy.
+// cells of one colour per sweep tile.  Measured on the 64-member C4
+// ensemble: 1024 (the tile set-up spread over more cells per thread) 3 %
+// slower -- late in a substage only the slowest members are swept, and
+// fewer tiles keep fewer blocks busy -- and 128 (more tiles, set-up per
+// cell) 13 % slower.
 constexpr int HTILE = 256;
 constexpr int MAX_THREADS = 512;
 
