@@ -109,6 +109,9 @@ struct ens_state {                   // per member, updated in the kernel
     int g_since[3];
     int g_arm;
     long long lr_gated;
+    // the FP32 sweeps' scalars of this substage (1/dx, 1/dy, 1/dz, 1/dt_gamma),
+    // set once at the substage start instead of per tile
+    float p32[4];
 };
 
 struct ens_list {
@@ -410,7 +413,8 @@ __device__ void corr_residual_tile(const ens_args& A, int ti) {
     const int2 T = A.cell.t[ti];
     const ens_member& M = A.mem[T.x];
     const mdx_dims d = M.d;
-    const mixed_params P = mixed_of(M, dg_of(A, M));
+    const float* p32 = A.st[T.x].p32;
+    const mixed_params P{p32[0], p32[1], p32[2], p32[3]};
     const fdiv32 fx = M.fx, fy = M.fy;
     double s = 0.0, m = 0.0, z = 0.0;
     for (int e = threadIdx.x; e < ETILE; e += blockDim.x) {
@@ -439,7 +443,8 @@ __device__ __forceinline__ void sweep32_tile(const ens_args& A, int parity, int 
     const int2 T = A.half.t[ti];
     const ens_member& M = A.mem[T.x];
     const mdx_dims d = M.d;
-    const mixed_params P = mixed_of(M, dg_of(A, M));
+    const float* p32 = A.st[T.x].p32;
+    const mixed_params P{p32[0], p32[1], p32[2], p32[3]};
     const fdiv32 fy = M.fy, fh = M.fh;
     float *du = M.du, *dv = M.dv, *dw = M.dw, *dp = M.dp;
     const float *r = M.r32, *mu32 = M.mu32, *fac32 = M.fac32;
@@ -635,6 +640,11 @@ __global__ void __launch_bounds__(MAX_THREADS, MINB) k_ens_substage(ens_args A) 
             S.extrap = A.guess_mode != MDX_GUESS_PREVIOUS && (h & (8 << s));
             S.lr_last = 0;
             S.g_arm = -1;
+            const mixed_params P = mixed_of(A.mem[m], dg_of(A, A.mem[m]));
+            S.p32[0] = P.idx;
+            S.p32[1] = P.idy;
+            S.p32[2] = P.idz;
+            S.p32[3] = P.idt;
         }
     grid.sync();
 
