@@ -998,7 +998,7 @@ def run_learned_eval(args, cfg):
     train = [(SEED + 100 + q, float(0.1 * (q + rng.uniform()) / nt),
               float(1000.0 + 4000.0 * (perm[q] + rng.uniform()) / nt)) for q in range(nt)]   # (seed, A, Re)
     held = [(SEED + 200 + q, float(rng.uniform(0.0, 0.1)), float(rng.uniform(1000.0, 5000.0)))
-            for q in range(cfg["heldout_runs"])]
+            for q in range(args.c3_heldout or cfg["heldout_runs"])]
     steps = args.c3_steps or cfg["heldout_steps"]
     cells = cfg["nx"] * cfg["ny"] * cfg["nz"]
     y0 = (cfg["ly"] - 2.0) / 2.0
@@ -1297,6 +1297,8 @@ def main():
                     help="FFT path transforms: 0 warp-shuffle where nx/2 and nz allow, 1 shared-memory Stockham")
     ap.add_argument("--c3-steps", type=int, default=0,
                     help="config c3: measured steps per held-out run (0: the config's 10)")
+    ap.add_argument("--c3-heldout", type=int, default=0,
+                    help="config c3: held-out runs (0: the config's 4; the first 4 draws are the same either way)")
     ap.add_argument("--c3-guesses", default="zero,previous,extrapolated,learned,learned_gated",
                     help="config c3: the guesses compared (comma list of zero, previous, extrapolated, learned, "
                          "learned_gated, learned_energy)")
