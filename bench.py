@@ -704,7 +704,7 @@ def run_ensemble(args, cfg):
     mode = M.GUESS_LEARNED if net else M.GUESS_EXTRAPOLATED
     E = M.Ensemble(mems, opts, device)
     if net:
-        E.unet_load(net.params, net.out_scale, channels=net.channels, gate_period=C3_GATE_PERIOD)
+        E.unet_load(net.params, net.out_scale, channels=net.channels, gate_period=args.c4_gate)
     E.set_guess(mode)
     E.ic()
     cache = os.path.join(os.path.expanduser("~"), ".cache", "mobydiff_b200", "ensemble_tune.json")
@@ -741,7 +741,7 @@ def run_ensemble(args, cfg):
     learned_info = None
     if net:
         kept, undone, gated = E.unet_stats()
-        learned_info = {"corrections_kept": kept, "corrections_undone": undone, "gate_period": C3_GATE_PERIOD,
+        learned_info = {"corrections_kept": kept, "corrections_undone": undone, "gate_period": args.c4_gate,
                         "left_to_extrapolation_by_gate": gated, "snapshots": net.snapshots,
                         "loss_first": net.loss_first, "loss_last": net.loss_last, "train_ms": net.train_ms,
                         "setup_wall_s": train_wall, "train_runs": [list(r) for r in net.runs],
@@ -1297,6 +1297,8 @@ def main():
                     help="FFT path transforms: 0 warp-shuffle where nx/2 and nz allow, 1 shared-memory Stockham")
     ap.add_argument("--c3-steps", type=int, default=0,
                     help="config c3: measured steps per held-out run (0: the config's 10)")
+    ap.add_argument("--c4-gate", type=int, default=C3_GATE_PERIOD,
+                    help="config c4: gate period of the learned correction per member (0: no gate)")
     ap.add_argument("--c3-heldout", type=int, default=0,
                     help="config c3: held-out runs (0: the config's 4; the first 4 draws are the same either way)")
     ap.add_argument("--c3-guesses", default="zero,previous,extrapolated,learned,learned_gated",
