@@ -1297,8 +1297,8 @@ def main():
                     help="FFT path transforms: 0 warp-shuffle where nx/2 and nz allow, 1 shared-memory Stockham")
     ap.add_argument("--c3-steps", type=int, default=0,
                     help="config c3: measured steps per held-out run (0: the config's 10)")
-    ap.add_argument("--c4-gate", type=int, default=C3_GATE_PERIOD,
-                    help="config c4: gate period of the learned correction per member (0: no gate)")
+    ap.add_argument("--c4-gate", type=int, default=0,
+                    help="config c4: gate period of the learned correction per member (0, the default: no gate)")
     ap.add_argument("--c3-heldout", type=int, default=0,
                     help="config c3: held-out runs (0: the config's 4; the first 4 draws are the same either way)")
     ap.add_argument("--c3-guesses", default="zero,previous,extrapolated,learned,learned_gated",
