@@ -157,7 +157,7 @@ def _dist():
 
 C3_GATE_PERIOD = 16   # the learned_gated guess re-tries the other choice every 16th projection of a substage
 SOR_VARIANT = 0   # --sor-variant: red-black kernel variant (0: the autotuner's choice)
-FFT_KERNEL = 0    # --fft-kernel: 0 warp-shuffle transforms where the lengths allow, 1 Stockham, 2 warp with a separate divergence pass
+FFT_KERNEL = 0    # --fft-kernel: 0 warp-shuffle transforms where the lengths allow, 1 Stockham
 SOR_NAMES = {1: "one launch per colour sweep", 2: "fused red+black pass 32x8", 3: "fused red+black pass 32x16",
              4: "one launch per colour sweep on colour-split copies",
              5: "one launch per colour sweep on colour-split copies, 2 cells per thread"}
@@ -1293,9 +1293,8 @@ def main():
     ap.add_argument("--quick", action="store_true", help="skip the plain FP64 leg at residual 1e-10")
     ap.add_argument("--sor-variant", type=int, default=0, choices=[0, 1, 2, 3, 4, 5],
                     help="red-black kernel variant (0: autotuned; all give the same bits)")
-    ap.add_argument("--fft-kernel", type=int, default=0, choices=[0, 1, 2],
-                    help="FFT path transforms: 0 warp-shuffle where nx/2 and nz allow, 1 shared-memory Stockham, "
-                         "2 as 0 with the divergence as a pass of its own")
+    ap.add_argument("--fft-kernel", type=int, default=0, choices=[0, 1],
+                    help="FFT path transforms: 0 warp-shuffle where nx/2 and nz allow, 1 shared-memory Stockham")
     ap.add_argument("--c3-steps", type=int, default=0,
                     help="config c3: measured steps per held-out run (0: the config's 10)")
     ap.add_argument("--c4-gate", type=int, default=0,

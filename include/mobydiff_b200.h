@@ -113,8 +113,7 @@ typedef struct {
                           meets the target) */
     int fft_kernel;    /* FFT path: 0 (default) warp-shuffle transforms where nx/2 and nz are
                           32, 64, 128, 256 or 512 (shared-memory Stockham otherwise); 1 always
-                          the shared-memory Stockham transforms; 2 as 0 with the divergence
-                          (FP64 path) as a pass of its own before the x transform (same bits) */
+                          the shared-memory Stockham transforms */
     int reserved_i[3];
     double atol;       /* red-black: absolute floor of ||div u||2, also accepted as converged.
                           < 0 (default): the FP64 round-off level of the divergence,

@@ -193,8 +193,7 @@ struct Reader {
         } else if (key == "fft_kernel") {
             if (v == "warp" || v == "0") o->fft_kernel = 0;
             else if (v == "stockham" || v == "1") o->fft_kernel = 1;
-            else if (v == "warp_split" || v == "2") o->fft_kernel = 2;
-            else warn("b200 fft_kernel must be warp, stockham or warp_split", line);
+            else warn("b200 fft_kernel must be warp or stockham", line);
         } else if (key == "max_iter") {
             rd_int(value, &o->max_iter, line);
         } else if (key == "check_every") {

@@ -586,46 +586,6 @@ k_div_fftx_w(mdx_dims d, double dx, double dy, double dz, mdx_dscal dgs, const d
     }
 }
 
-// The forward real FFT of k_div_fftx_w on rows of a right-hand side already
-// in rhs(nx, nz, ny) order (k_div_rhs wrote it): the divergence and the
-// transform as two passes, each a plain stream (two consecutive values per
-// lane and row, 16-byte loads).  Same values into the same transform, so the
-// same bits as k_div_fftx_w.
-template <int P, typename C2>
-__global__ void __launch_bounds__(256, P >= 16 ? 2 : 4)
-k_fftx_w_rhs(mdx_dims d, const double* __restrict__ rhs, C2* __restrict__ spec, const C2* __restrict__ twx) {
-    typedef typename cx<C2>::R RT;
-    constexpr int M = 32 * P;
-    extern __shared__ __align__(16) unsigned char sm_raw[];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    C2* buf = reinterpret_cast<C2*>(sm_raw) + warp * M;
-    const int row = blockIdx.x * 8 + warp;
-    if (row >= d.nz * d.ny) return;
-    const double2* src = reinterpret_cast<const double2*>(rhs + (long long)row * d.nx);
-    C2 v[P];
-#pragma unroll
-    for (int m = 0; m < P; ++m) {
-        const double2 x = __ldg(src + lane + 32 * m);
-        v[m] = cx<C2>::mk((RT)x.x, (RT)x.y);
-    }
-    warp_fft<false, P>(v, lane, twx, 2);
-#pragma unroll
-    for (int p = 0; p < P; ++p) buf[wline<P, C2>(wout<P>(lane, p))] = v[p];
-    __syncwarp();
-    C2* X = spec + (long long)row * d.nxh;
-    const RT h = (RT)0.5;
-#pragma unroll
-    for (int m = 0; m <= P; ++m) {
-        const int kx = lane + 32 * m;
-        if (m == P && lane != 0) break;
-        const C2 zk = buf[wline<P, C2>(kx & (M - 1))];
-        const C2 zc = cconj(buf[wline<P, C2>((M - kx) & (M - 1))]);
-        const C2 e = cx<C2>::mk(h * (zk.x + zc.x), h * (zk.y + zc.y));
-        const C2 o = cmul_mi(cx<C2>::mk(h * (zk.x - zc.x), h * (zk.y - zc.y)));
-        X[kx] = cadd(e, cmul_f(__ldg(twx + kx), o));
-    }
-}
-
 // Complex FFT along z of spec(kx, :, j), nz = 32 P: a block stages TX = G
 // consecutive kx columns of one j (one 128-byte row segment per kz: 8 FP64
 // or 16 FP32 complex values) through shared memory; one warp per column.
@@ -910,8 +870,8 @@ template <typename F> static int with_p(int p, F&& f) {
     }
     return MDX_ERR_ARG;
 }
-static int fft_px(const mdx_ctx_t* ctx) { return ctx->opts.fft_kernel != 1 ? warp_p(ctx->d.nx / 2) : 0; }
-static int fft_pz(const mdx_ctx_t* ctx) { return ctx->opts.fft_kernel != 1 ? warp_p(ctx->d.nz) : 0; }
+static int fft_px(const mdx_ctx_t* ctx) { return ctx->opts.fft_kernel == 0 ? warp_p(ctx->d.nx / 2) : 0; }
+static int fft_pz(const mdx_ctx_t* ctx) { return ctx->opts.fft_kernel == 0 ? warp_p(ctx->d.nz) : 0; }
 
 template <typename C2> static int fft_warp_attrs(mdx_ctx_t* ctx) {
     const int px = warp_p(ctx->d.nx / 2), pz = warp_p(ctx->d.nz);
@@ -942,23 +902,7 @@ static int launch_div_fftx(mdx_ctx_t* ctx, const char* what, mdx_dscal dg, C2* s
     const mdx_grid_t& g = ctx->g;
     double** f = ctx->f;
     const int nrows = d.nz * d.ny;
-    // fft_kernel 2 (FP64): the divergence into rhs (the phi array, which the
-    // inverse transform overwrites later), then the warp transform of its rows
-    const bool split = ctx->opts.fft_kernel == 2 && std::is_same<C2, double2>::value;
-    if (const int px = fft_px(ctx)) {
-        if (split) {
-            dim3 block(32, 4, 2);
-            dim3 grid((d.nx + 31) / 32, (d.ny + 3) / 4, (d.nz + 1) / 2);
-            MDX_LAUNCH(ctx, MDX_T_FFT_FWD, "div rhs", k_div_rhs, grid, block, 0, d, g.dx, g.dy, g.dz, dg, f[MDX_US],
-                       f[MDX_VS], f[MDX_WS], f[MDX_PHI]);
-            return with_p(px, [&](auto pc) -> int {
-                constexpr int P = decltype(pc)::value;
-                auto kern = k_fftx_w_rhs<P, C2>;
-                MDX_LAUNCH(ctx, MDX_T_FFT_FWD, what, kern, (nrows + 7) / 8, 256, 8 * 32 * P * sizeof(C2), d,
-                           (const double*)f[MDX_PHI], spec, twx);
-                return MDX_OK;
-            });
-        }
+    if (const int px = fft_px(ctx))
         return with_p(px, [&](auto pc) -> int {
             constexpr int P = decltype(pc)::value;
             auto kern = k_div_fftx_w<P, C2>;
@@ -966,7 +910,6 @@ static int launch_div_fftx(mdx_ctx_t* ctx, const char* what, mdx_dscal dg, C2* s
                        g.dz, dg, f[MDX_US], f[MDX_VS], f[MDX_WS], spec, twx);
             return MDX_OK;
         });
-    }
     const int M = d.nx / 2, R = rows_per_block(M);
     auto kern = k_div_fftx<C2>;
     MDX_LAUNCH(ctx, MDX_T_FFT_FWD, what, kern, (nrows + R - 1) / R, 256, sizeof(C2) * 2 * R * M, d, R, g.dx, g.dy,

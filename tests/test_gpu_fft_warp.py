@@ -30,9 +30,6 @@ def test_warp_transforms_match_oracle_and_stockham(shape):
     f = random_fields(g, 31, scale=0.5)
     warp = _project(g, bc, f, 0)
     stock = _project(g, bc, f, 1)
-    split = _project(g, bc, f, 2)   # the divergence as its own pass, then the same warp transforms
-    for n in warp:
-        assert np.array_equal(split[n], warp[n]), n
     O.apply_bc(g, f)
     phi_o = O.pressure_projection_fft(g, f, 0.4e-3)
     assert rel_l2(warp["phi"], phi_o) < 1e-12
