@@ -1297,6 +1297,8 @@ def main():
                     help="FFT path transforms: 0 warp-shuffle where nx/2 and nz allow, 1 shared-memory Stockham")
     ap.add_argument("--c3-steps", type=int, default=0,
                     help="config c3: measured steps per held-out run (0: the config's 10)")
+    ap.add_argument("--check-every", type=int, default=0,
+                    help="red-black: iterations between residual checks (0: the config's)")
     ap.add_argument("--c4-gate", type=int, default=0,
                     help="config c4: gate period of the learned correction per member (0, the default: no gate)")
     ap.add_argument("--c3-heldout", type=int, default=0,
@@ -1310,6 +1312,8 @@ def main():
     SOR_VARIANT = args.sor_variant
     FFT_KERNEL = args.fft_kernel
     cfg = CONFIGS[args.config]
+    if args.check_every > 0:
+        cfg = dict(cfg, check_every=args.check_every)
     if args.impl == "reference":
         return run_reference(args, cfg)
     if args.profile_mixed:
