@@ -65,7 +65,7 @@ CONFIGS = {
                          "defect correction, learned warm start (network trained on stratified member-like runs); "
                          "two persistent launches per RK3 substage with the network between, CUDA graph, autotuned "
                          "launch shape",
-               solver="redblack", sor=1.7, tol=1e-8, check_every=10, members=64, method="ensemble", mixed=True,
+               solver="redblack", sor=1.7, tol=1e-8, check_every=25, members=64, method="ensemble", mixed=True,
                learned=True, train_runs=6, record_steps=6),
     "c0": dict(workload="periodic channel 64^3, FP64 FFT+Thomas", nx=64, ny=64, nz=64, lx=2 * math.pi, ly=2.0,
                lz=math.pi, re=2000.0, dt=1e-3, solver="fft", ibm="none", amp=0.0, method="plain"),
