@@ -160,6 +160,7 @@ def _dist():
 C3_GATE_PERIOD = 16   # the learned_gated guess re-tries the other choice every 16th projection of a substage
 SOR_VARIANT = 0   # --sor-variant: red-black kernel variant (0: the autotuner's choice)
 FFT_KERNEL = 0    # --fft-kernel: 0 warp-shuffle transforms where the lengths allow, 1 Stockham
+INNER_FORM = 0    # --inner-form: FP32 correction sweeps of the mixed path, 0 potential form, 1 face form
 SOR_NAMES = {1: "one launch per colour sweep", 2: "fused red+black pass 32x8", 3: "fused red+black pass 32x16",
              4: "one launch per colour sweep on colour-split copies",
              5: "one launch per colour sweep on colour-split copies, 2 cells per thread"}
@@ -169,8 +170,15 @@ SOR_NAMES = {1: "one launch per colour sweep", 2: "fused red+black pass 32x8", 3
 # solve's variant
 SOR32_NAMES = {1: "k_sor_sweep32: one launch per colour, one cell per thread",
                3: "k_rb32_fused: one launch per red+black iteration",
-               5: "k_sor_sweep32v: one launch per colour, 2 or 4 cells per thread"}
-SOR32_TRAFFIC = {1: "sor_sweep32", 3: "rb32_fused", 5: "sor_sweep32v"}
+               5: "k_sor_sweep32v: one launch per colour, 2 or 4 cells per thread",
+               7: "k_pot_sweep: potential form, one launch per colour, 2 or 4 cells per thread marching z"}
+SOR32_TRAFFIC = {1: "sor_sweep32", 3: "rb32_fused", 5: "sor_sweep32v", 7: "pot_sweep"}
+# algorithmic bytes per cell of one FP32 colour sweep launch (a fused
+# red+black launch does both colours): the face form reads and writes 4
+# floats per cell of one colour (16 B per cell of the grid); the potential
+# form reads phi of both colours and r~ of the swept one and writes phi of
+# the swept one (8 B per cell of the grid)
+SOR32_ALG = {1: 16.0, 3: 32.0, 5: 16.0, 7: 8.0}
 
 
 def _sor64_traffic_key(variant):
@@ -196,7 +204,7 @@ def _setup(cfg, M, device, profile=False, tol=None, precision=None, seed=None):
         opts = M.make_solver_opts(M.SOLVER_REDBLACK, sor=cfg["sor"], tol=cfg["tol"] if tol is None else tol,
                                   check_every=cfg["check_every"], max_iter=400000,
                                   precision=M.PREC_FP64 if precision is None else precision,
-                                  sor_variant=SOR_VARIANT)
+                                  sor_variant=SOR_VARIANT, inner_form=INNER_FORM)
     else:
         opts = M.make_solver_opts(M.SOLVER_FFT, tol=cfg.get("tol", 0.0) if precision == M.PREC_MIXED else 0.0,
                                   precision=M.PREC_FP64 if precision is None else precision, fft_kernel=FFT_KERNEL)
@@ -468,7 +476,8 @@ def _sor_alg_per_launch(variant, fp32=False):
 def _step_hbm(cells, ms_per_step, iters_per_step, per_iter):
     """The whole red-black step against its algorithmic bytes: 104 B per cell
     per substage for the predictor and projection set-up (13 doubles) and
-    `per_iter` B per cell per red+black iteration (64 FP64, 32 FP32)."""
+    `per_iter` B per cell per red+black iteration (64 FP64, 32 FP32 face
+    form, 16 FP32 potential form)."""
     peak, peak_kind = _peaks()
     b = cells * (3 * 104.0 + per_iter * iters_per_step)
     gbs = b / (ms_per_step / 1e3) / 1e9
@@ -1015,7 +1024,7 @@ def run_learned_eval(args, cfg):
             s.enter_ibm_geometry(M.ibm_wavy(amp, lam, y0))
         s.init_pressure_solver(M.make_solver_opts(M.SOLVER_REDBLACK, sor=cfg["sor"], tol=cfg["tol"],
                                                   check_every=cfg["check_every"], max_iter=400000,
-                                                  precision=M.PREC_MIXED))
+                                                  precision=M.PREC_MIXED, inner_form=INNER_FORM))
         return s, g
 
     t0 = time.time()
@@ -1197,10 +1206,13 @@ def run_learned_mixed(args, cfg):
     # 4 floats per cell per colour sweep; the FP32 sweep kernel the autotuner
     # kept is the hundreds digit of the solve's variant
     kind = s.last_solve_stats().variant // 100
-    roofline = _roofline(tim, "sor_run", _sor_alg_per_launch(2 if kind == 3 else 1, fp32=True), cells, r_ms,
+    roofline = _roofline(tim, "sor_run", SOR32_ALG.get(kind, 16.0), cells, r_ms,
                          traffic_key=SOR32_TRAFFIC.get(kind, "sor_sweep32"))
     roofline["sor_kernel"] = SOR32_NAMES.get(kind, "?")
-    step_hbm = _step_hbm(cells, ms_all / K, iters / K, 32.0)
+    if kind == 7:
+        roofline["note"] = ("phi and r~ (37 MB) stay resident in the 126 MB L2 across sweeps, so the sweeps "
+                            "run from L2 and can pass the HBM copy rate")
+    step_hbm = _step_hbm(cells, ms_all / K, iters / K, 16.0 if kind == 7 else 32.0)
 
     # ---- the same steps without the network: extrapolated increment only ----
     s.warm_checkpoint(restore=True)
@@ -1220,7 +1232,8 @@ def run_learned_mixed(args, cfg):
         st2, _ = _setup(cfg, M, device, tol=tol, precision=M.PREC_MIXED)
         st2.init_pressure_solver(M.make_solver_opts(M.SOLVER_REDBLACK, sor=cfg["sor"], tol=tol,
                                                     check_every=cfg["check_every"], max_iter=400000,
-                                                    precision=M.PREC_MIXED, inner_sor=om))
+                                                    precision=M.PREC_MIXED, inner_sor=om,
+                                                    inner_form=INNER_FORM))
         st2.channel_ic(SEED, 0.1, 0.01, (cfg["ly"] - 2.0) / 2.0, cfg["amp"], cfg["lx"] / 2.0)
         learned.load_into(st2, net)
         st2.set_pressure_guess(M.GUESS_LEARNED, record=True)
@@ -1298,8 +1311,11 @@ def main():
     ap.add_argument("--profile-mixed", action="store_true",
                     help="profiling run for ncu: the full-size t=0 projection with FP32 sweeps to residual 1e-8")
     ap.add_argument("--quick", action="store_true", help="skip the plain FP64 leg at residual 1e-10")
-    ap.add_argument("--sor-variant", type=int, default=0, choices=[0, 1, 2, 3, 4, 5],
-                    help="red-black kernel variant (0: autotuned; all give the same bits)")
+    ap.add_argument("--sor-variant", type=int, default=0, choices=list(range(9)),
+                    help="red-black kernel variant (0: autotuned; all give the same bits); FP64 sweeps and the "
+                         "face form 1-5, the potential form's sweep shapes 1-8")
+    ap.add_argument("--inner-form", type=int, default=0, choices=[0, 1],
+                    help="mixed red-black: FP32 correction sweeps in the potential form (0) or the face form (1)")
     ap.add_argument("--fft-kernel", type=int, default=0, choices=[0, 1],
                     help="FFT path transforms: 0 warp-shuffle where nx/2 and nz allow, 1 shared-memory Stockham")
     ap.add_argument("--c3-steps", type=int, default=0,
@@ -1317,8 +1333,9 @@ def main():
     ap.add_argument("--train-runs", type=int, default=2, choices=[2, 4],
                     help="headline: training runs of the learned warm start (2: A 0.03, 0.07; 4: A 0.02..0.08)")
     args = ap.parse_args()
-    global SOR_VARIANT, FFT_KERNEL
+    global SOR_VARIANT, FFT_KERNEL, INNER_FORM
     SOR_VARIANT = args.sor_variant
+    INNER_FORM = args.inner_form
     FFT_KERNEL = args.fft_kernel
     cfg = CONFIGS[args.config]
     if args.check_every > 0:

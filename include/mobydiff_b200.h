@@ -114,7 +114,15 @@ typedef struct {
     int fft_kernel;    /* FFT path: 0 (default) warp-shuffle transforms where nx/2 and nz are
                           32, 64, 128, 256 or 512 (shared-memory Stockham otherwise); 1 always
                           the shared-memory Stockham transforms */
-    int reserved_i[3];
+    int inner_form;    /* mixed-precision red-black: what the FP32 correction sweeps carry.
+                          0 (default): the potential form -- the accumulated phi of each
+                          cell alone, swept with the 7-point stencil that the face updates
+                          of pressure_redblack.f90:117-241 amount to (the same iteration in
+                          exact arithmetic; 8 B per cell per colour sweep instead of 30),
+                          where nx is a multiple of 4, the face form otherwise; 1: the face
+                          form (corrections du, dv, dw, dp updated face by face, kernels
+                          chosen by sor_variant) */
+    int reserved_i[2];
     double atol;       /* red-black: absolute floor of ||div u||2, also accepted as converged.
                           < 0 (default): the FP64 round-off level of the divergence,
                           eps*sqrt(nx*ny*nz)*max|u*|*(1/dx+1/dy+1/dz); 0: none */
@@ -133,7 +141,8 @@ typedef struct {
     int variant;        /* red-black kernel variant of the last iterations;
                            100 + n: mixed precision with n FP64 corrections
                            (300 + n with the fused FP32 pass, 500 + n with the
-                           FP32 sweeps of 2 or 4 cells per thread);
+                           FP32 sweeps of 2 or 4 cells per thread, 700 + n with
+                           the potential form, opts.inner_form);
                            200 + n: FFT path in mixed precision, n FP64 passes
                            (iterations = n as well) */
     int guessed;        /* 1 when a warm-start guess was applied             */

@@ -86,7 +86,7 @@ class SolverOptsT(C.Structure):
     _fields_ = [("solver", C.c_int), ("n_iter", C.c_int), ("sor", C.c_double), ("tol", C.c_double),
                 ("max_iter", C.c_int), ("check_every", C.c_int), ("precision", C.c_int),
                 ("sor_variant", C.c_int), ("sor_kz", C.c_int), ("check_mode", C.c_int),
-                ("fft_kernel", C.c_int), ("reserved_i", C.c_int * 3),
+                ("fft_kernel", C.c_int), ("inner_form", C.c_int), ("reserved_i", C.c_int * 2),
                 ("atol", C.c_double), ("inner_sor", C.c_double), ("reserved_d", C.c_double * 6)]
 
 
@@ -290,7 +290,7 @@ def channel_bc() -> BcT:
 
 def make_solver_opts(solver=SOLVER_FFT, n_iter=3, sor=1.5, tol=0.0, max_iter=100000, check_every=10,
                      precision=PREC_FP64, atol=-1.0, sor_variant=0, sor_kz=0, inner_sor=0.0,
-                     adaptive_checks=True, fft_kernel=0) -> SolverOptsT:
+                     adaptive_checks=True, fft_kernel=0, inner_form=0) -> SolverOptsT:
     o = SolverOptsT()
     lib().mdx_default_solver_opts(C.byref(o))
     o.solver, o.n_iter, o.sor, o.tol = int(solver), int(n_iter), float(sor), float(tol)
@@ -300,6 +300,7 @@ def make_solver_opts(solver=SOLVER_FFT, n_iter=3, sor=1.5, tol=0.0, max_iter=100
     o.inner_sor = float(inner_sor)
     o.check_mode = 0 if adaptive_checks else 1
     o.fft_kernel = int(fft_kernel)
+    o.inner_form = int(inner_form)
     return o
 
 

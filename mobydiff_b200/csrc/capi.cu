@@ -325,6 +325,8 @@ int mdx_set_bc(mdx_ctx_t* ctx, const mdx_bc_t* bc) {
     for (int t = 0; t < 8; ++t) ctx->sor_tune_ms[t] = 0.0;
     ctx->rb32_tuned = 0;
     for (int t = 0; t < 8; ++t) ctx->rb32_tune_ms[t] = 0.0;
+    ctx->pt_tuned = 0;
+    for (int t = 0; t < 8; ++t) ctx->pt_tune_ms[t] = 0.0;
     // FFT solver: walls in x or z change the solve grid (and need Neumann
     // pressure there); rebuild its workspace for the new conditions
     if (ctx->solver && ctx->opts.solver == MDX_SOLVER_FFT &&
@@ -531,6 +533,8 @@ int mdx_init_pressure_solver(mdx_ctx_t* ctx, const mdx_solver_opts_t* opts) {
         return mdx_fail(ctx, MDX_ERR_ARG, "unknown solver %d", o.solver);
     if (o.precision != MDX_PREC_FP64 && o.precision != MDX_PREC_MIXED)
         return mdx_fail(ctx, MDX_ERR_ARG, "unknown precision %d", o.precision);
+    if (o.inner_form != 0 && o.inner_form != 1)
+        return mdx_fail(ctx, MDX_ERR_ARG, "inner_form must be 0 (potential) or 1 (faces), got %d", o.inner_form);
     if (o.check_every < 1) o.check_every = 1;
     if (o.max_iter < 1) o.max_iter = 1;
     if (o.n_iter < 0) return mdx_fail(ctx, MDX_ERR_ARG, "n_iter must be >= 0");
@@ -539,6 +543,8 @@ int mdx_init_pressure_solver(mdx_ctx_t* ctx, const mdx_solver_opts_t* opts) {
     for (int t = 0; t < 8; ++t) ctx->sor_tune_ms[t] = 0.0;
     ctx->rb32_tuned = 0;
     for (int t = 0; t < 8; ++t) ctx->rb32_tune_ms[t] = 0.0;
+    ctx->pt_tuned = 0;
+    for (int t = 0; t < 8; ++t) ctx->pt_tune_ms[t] = 0.0;
     MDX_TRY(mdx_reduce_init(ctx));
     if (o.solver == MDX_SOLVER_REDBLACK) {
         // src/modules/pressure/pressure_redblack.f90:16-18

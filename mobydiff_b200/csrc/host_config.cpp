@@ -194,6 +194,10 @@ struct Reader {
             if (v == "warp" || v == "0") o->fft_kernel = 0;
             else if (v == "stockham" || v == "1") o->fft_kernel = 1;
             else warn("b200 fft_kernel must be warp or stockham", line);
+        } else if (key == "inner_form") {
+            if (v == "potential" || v == "0") o->inner_form = 0;
+            else if (v == "faces" || v == "1") o->inner_form = 1;
+            else warn("b200 inner_form must be potential or faces", line);
         } else if (key == "max_iter") {
             rd_int(value, &o->max_iter, line);
         } else if (key == "check_every") {

@@ -8,6 +8,10 @@
 //      start) with the cell divergence r~ + div(du): the same update as
 //      pressure_redblack.f90:117-241 with homogeneous boundary values;
 //   3. adds the corrections to the FP64 state (u += du, p += dp).
+// By default (opts.inner_form 0) step 2 carries the corrections in their
+// potential form -- the accumulated phi of each cell, from which every face
+// correction follows -- and step 3 forms the face corrections from it in
+// FP64 (k_pot_* below).
 // It stops when the FP64 residual meets max(tol*||div u*||, atol), the
 // target of the FP64 path.  A sweep moves 36 B per cell instead of 64 B;
 // the slowest mode sets the iteration count, so the total number of sweeps
@@ -524,6 +528,335 @@ __global__ void k_mixed_apply(mdx_dims d, double* __restrict__ u, double* __rest
         mixed_apply_elem(d, t, u, v, w, p, du, dv, dw, dp);
 }
 
+// ---------------------------------------------------------------------------
+// Potential form of the FP32 correction sweeps (opts.inner_form 0).
+//
+// Starting from zero corrections, the face updates of
+// pressure_redblack.f90:117-241 leave every face at h^-1 mu (Phi(low cell) -
+// Phi(high cell)), Phi being the sum of the phi a cell has taken, and dp at
+// Phi/dt_gamma.  The divergence the next update of cell c needs is then
+//   e(c) = r~(c) + sum over the faces f of c of a_f (Phi(c) - Phi(across f)),
+//   a_f = h^-2 mu_f, 0 for a wall face (which never moves),
+// and the update is Phi(c) += fac(c) e(c): the same red-black iteration in
+// exact arithmetic, carried by one array instead of four.  A colour sweep
+// reads Phi of the other colour and Phi and r~ of its own and writes Phi of
+// its own: 8 B per cell instead of 30.
+//
+// Layout (pot_geom): cell (i, j, k), i in 0..nx+1, in half (i + j + k) & 1 at
+// (k (ny+2) + j) hq + 3 + (i + 1) / 2.  A row of one half holds its nx/2
+// interior cells at positions 4 .. nx/2 + 3 (16-byte aligned), the copy of
+// cell nx at position 3 (rows of even cells) or of cell 1 at nx/2 + 4 (rows
+// of odd cells); planes 0 and nz+1, and rows 0 and ny+1 when y is periodic,
+// hold copies of planes nz and 1 (rows ny and 1).  A sweep writes the copies
+// of the cells it updates, so no neighbour read tests for a wrap.  Corners
+// are never read.  tests/pot32_model.py restates the sweep thread by thread.
+// ---------------------------------------------------------------------------
+struct pot_geom {
+    int nx, ny, nz;
+    int hq;   // row length of one half (positions)
+    int rz;   // one plane of one half: hq (ny+2)
+    int H;    // one half, a multiple of 64 elements
+};
+
+__host__ __device__ __forceinline__ int pot_row(const pot_geom& L, int h, int j, int k) {
+    return h * L.H + (k * (L.ny + 2) + j) * L.hq;
+}
+__host__ __device__ __forceinline__ int pot_idx(const pot_geom& L, int i, int j, int k) {
+    return pot_row(L, (i + j + k) & 1, j, k) + 3 + (i + 1) / 2;
+}
+
+pot_geom pot_make(const mdx_dims& d) {
+    pot_geom L;
+    L.nx = d.nx;
+    L.ny = d.ny;
+    L.nz = d.nz;
+    L.hq = ((d.nx / 2 + 5) + 3) & ~3;
+    L.rz = L.hq * (d.ny + 2);
+    L.H = (int)((((long long)L.rz * (d.nz + 2)) + 63) & ~63LL);
+    return L;
+}
+
+// The cell update of the potential form, shared by the sweep and the
+// residual: e = r~ + sum a (c - neighbour), FP32 roundings explicit.
+__device__ __forceinline__ float pot_e(float r, float c, float xl, float xr, float ym, float yp, float zm, float zp,
+                                       float axl, float axr, float ayl, float ayr, float az) {
+    float e = __fmaf_rn(axl, __fsub_rn(c, xl), r);
+    e = __fmaf_rn(axr, __fsub_rn(c, xr), e);
+    e = __fmaf_rn(ayl, __fsub_rn(c, ym), e);
+    e = __fmaf_rn(ayr, __fsub_rn(c, yp), e);
+    return __fmaf_rn(az, __fadd_rn(__fsub_rn(c, zm), __fsub_rn(c, zp)), e);
+}
+
+// Column table: per (i, j) {a_x of the low x face, a_y of the low y face (0
+// at a wall), a_z, fac = -omega/denom}; column nx+1 repeats column 1's a_x,
+// row ny+1 holds the top faces' a_y (0 at walls, row 1's when y is
+// periodic).  a_f and fac are formed in FP64 (the denominator of
+// pressure_redblack.f90:124-126) and rounded once.
+__global__ void k_pot_tables(pot_geom L, int py, double idx2, double idy2, double idz2, double sor,
+                             const double* __restrict__ mu, int plane_mu, float4* __restrict__ tab) {
+    const int nxp = L.nx + 2, nyp = L.ny + 2;
+    const long long np = (long long)nxp * nyp;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < np; t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % nxp), j = (int)(t / nxp);
+        auto MU = [&](int c, int ii, int jj) { return plane_mu ? mu[c * np + ii + (long long)nxp * jj] : 1.0; };
+        float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (j >= 1 && j <= L.ny && i >= 1 && i <= L.nx) {
+            const int ip = i == L.nx ? 1 : i + 1;
+            const int jp = (py && j == L.ny) ? 1 : j + 1;
+            const double mu_u = MU(0, i, j), mu_v = MU(1, i, j), mu_w = MU(2, i, j);
+            const double denom = (mu_u + MU(0, ip, j)) * idx2 + (mu_w + mu_w) * idz2 + (mu_v + MU(1, i, jp)) * idy2;
+            o.x = (float)(idx2 * mu_u);
+            o.y = (py || j > 1) ? (float)(idy2 * mu_v) : 0.f;
+            o.z = (float)(idz2 * mu_w);
+            o.w = (float)(-sor / denom);
+        } else if (j >= 1 && j <= L.ny && i == L.nx + 1) {
+            o.x = (float)(idx2 * MU(0, 1, j));
+        } else if (j == L.ny + 1 && i >= 1 && i <= L.nx) {
+            o.y = py ? (float)(idy2 * MU(1, i, 1)) : 0.f;
+        }
+        tab[t] = o;
+    }
+}
+
+// FP64 divergence of (u, v, w) per cell, stored as FP32 r~ in the potential
+// layout; partial sums of r^2, max|r| and max(|u|,|v|,|w|) (the expression of
+// k_mixed_residual, so the same norms).
+template <int PY>
+__global__ void __launch_bounds__(MDX_RED_THREADS)
+k_pot_residual(mdx_dims d, pot_geom L, double idx, double idy, double idz, const double* __restrict__ u,
+               const double* __restrict__ v, const double* __restrict__ w, float* __restrict__ r,
+               double* __restrict__ part) {
+    double s = 0.0, m = 0.0, um = 0.0;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < d.nint; t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % d.nx) + 1;
+        const long long rr = t / d.nx;
+        const int j = (int)(rr % d.ny) + 1;
+        const int k = (int)(rr / d.ny) + 1;
+        const int ip = i == d.nx ? 1 : i + 1;
+        const int jp = (PY && j == d.ny) ? 1 : j + 1;
+        const int kp = k == d.nz ? 1 : k + 1;
+        const long long c = pidx(d, i, j, k);
+        const double dv = (__ldg(u + pidx(d, ip, j, k)) - __ldg(u + c)) * idx +
+                          (__ldg(v + pidx(d, i, jp, k)) - __ldg(v + c)) * idy +
+                          (__ldg(w + pidx(d, i, j, kp)) - __ldg(w + c)) * idz;
+        r[pot_idx(L, i, j, k)] = (float)dv;
+        s += dv * dv;
+        m = nanmax2(m, fabs(dv));
+        um = nanmax2(um, nanmax2(fabs(__ldg(u + c)), nanmax2(fabs(__ldg(v + c)), fabs(__ldg(w + c)))));
+    }
+    block_reduce3(s, m, um);
+    if (threadIdx.x == 0) {
+        part[3 * blockIdx.x] = s;
+        part[3 * blockIdx.x + 1] = m;
+        part[3 * blockIdx.x + 2] = um;
+    }
+}
+
+// Residual of the correction problem, e(c) of every cell, as partial sums.
+__global__ void __launch_bounds__(MDX_RED_THREADS)
+k_pot_corr_residual(mdx_dims d, pot_geom L, const float* __restrict__ phi, const float* __restrict__ r,
+                    const float4* __restrict__ tab, double* __restrict__ part) {
+    double s = 0.0, m = 0.0, z = 0.0;
+    const int ncol = d.nx + 2;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < d.nint; t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % d.nx) + 1;
+        const long long rr = t / d.nx;
+        const int j = (int)(rr % d.ny) + 1;
+        const int k = (int)(rr / d.ny) + 1;
+        const int c = pot_idx(L, i, j, k);
+        const float4 T = __ldg(tab + j * ncol + i);
+        const float axr = __ldg(&tab[j * ncol + i + 1].x), ayr = __ldg(&tab[(j + 1) * ncol + i].y);
+        const float e = pot_e(__ldg(r + c), __ldg(phi + c), __ldg(phi + pot_idx(L, i - 1, j, k)),
+                              __ldg(phi + pot_idx(L, i + 1, j, k)), __ldg(phi + pot_idx(L, i, j - 1, k)),
+                              __ldg(phi + pot_idx(L, i, j + 1, k)), __ldg(phi + pot_idx(L, i, j, k - 1)),
+                              __ldg(phi + pot_idx(L, i, j, k + 1)), T.x, axr, T.y, ayr, T.z);
+        s += (double)e * (double)e;
+        m = nanmax2(m, fabs((double)e));
+    }
+    block_reduce3(s, m, z);
+    if (threadIdx.x == 0) {
+        part[3 * blockIdx.x] = s;
+        part[3 * blockIdx.x + 1] = m;
+        part[3 * blockIdx.x + 2] = 0.0;
+    }
+}
+
+// One colour sweep of the potential form (cells of colour cs = (i+j+k)&1).
+// A thread owns positions q0 .. q0+V-1 of row j (the 2V cells 2 q0 + 1 ..
+// 2 q0 + 2V, both colours) and marches planes k0 .. k0+KZ-1, holding the
+// other colour's values of planes k-1, k, k+1 in registers and the 2V
+// columns' coefficients for the whole march.  In plane k its V swept cells
+// have odd i when (cs + j + k) is odd; their x neighbours are the other
+// colour's values at the same positions and one position to the left (odd)
+// or right (even), that one value a scalar load.  Needs nx/2 a multiple of
+// V, nz even (and ny even when y is periodic): every neighbour then has the
+// other colour, so a thread reads nothing that another thread writes.
+template <int PY, int V, int KZ, bool PF>
+__global__ void __launch_bounds__(256)
+k_pot_sweep(pot_geom L, int cs, float* __restrict__ phi, const float* __restrict__ r, const float4* __restrict__ tab) {
+    const int half = L.nx / 2;
+    const int q0 = V * (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    const int j = 1 + (int)(blockIdx.y * blockDim.y + threadIdx.y);
+    if (q0 >= half || j > L.ny) return;
+    const int k0 = 1 + (int)blockIdx.z * KZ;
+    const int k1 = min(k0 + KZ - 1, L.nz);
+    const int ncol = L.nx + 2;
+    // coefficients: column m = 0 .. 2V-1 is cell 2 q0 + 1 + m, odd cells at
+    // even m (set 0), even cells at odd m (set 1)
+    float axl[2][V], axr[2][V], ayl[2][V], ayr[2][V], az[2][V], fc[2][V];
+    const float4* t0 = tab + j * ncol + 2 * q0 + 1;
+    const float4* t1 = tab + (j + 1) * ncol + 2 * q0 + 1;
+#pragma unroll
+    for (int m = 0; m < 2 * V; ++m) {
+        const float4 c = __ldg(t0 + m);
+        const int s = m & 1, e = m >> 1;
+        axl[s][e] = c.x;
+        ayl[s][e] = c.y;
+        az[s][e] = c.z;
+        fc[s][e] = c.w;
+        ayr[s][e] = __ldg(&t1[m].y);
+        if (m > 0) axr[(m - 1) & 1][(m - 1) >> 1] = c.x;
+    }
+    axr[1][V - 1] = __ldg(&t0[2 * V].x);
+
+    const int oh = 1 - cs;
+    const int ob = pot_row(L, oh, j, 0) + 4 + q0;   // other colour, row j, plane 0, position q0
+    const int sb = pot_row(L, cs, j, 0) + 4 + q0;   // swept colour
+    // Every value a thread reads is either the other colour's (not written
+    // by this sweep) or its own cell's before it writes it, so all reads
+    // take the read-only path; with PF the loads of plane k+1 are issued
+    // before plane k is computed (one plane in flight while the other is
+    // used).
+    struct plane_in { float zp[V], s[V], rr[V], ym[V], yp[V], xs; };
+    auto load = [&](plane_in& P, int k) {
+        const int ok = ob + k * L.rz, sk = sb + k * L.rz;
+        ld_vec_ro<V>(P.zp, phi + ok + L.rz);
+        ld_vec_ro<V>(P.s, phi + sk);
+        ld_vec_ro<V>(P.rr, r + sk);
+        ld_vec_ro<V>(P.ym, phi + ok - L.hq);
+        ld_vec_ro<V>(P.yp, phi + ok + L.hq);
+        P.xs = __ldg(phi + ok + (((cs + j + k) & 1) ? -1 : V));
+    };
+    float zm[V], z0[V];
+    ld_vec_ro<V>(zm, phi + ob + (k0 - 1) * L.rz);
+    ld_vec_ro<V>(z0, phi + ob + k0 * L.rz);
+    plane_in cur, nxt;
+    if (PF) load(cur, k0);
+    for (int k = k0; k <= k1; ++k) {
+        if (!PF) load(cur, k);
+        else if (k < k1) load(nxt, k + 1);
+        const int sk = sb + k * L.rz;
+        const bool odd = ((cs + j + k) & 1) != 0;
+        float out[V];
+#pragma unroll
+        for (int e = 0; e < V; ++e) {
+            const float xl = odd ? (e == 0 ? cur.xs : z0[e > 0 ? e - 1 : 0]) : z0[e];
+            const float xr = odd ? z0[e] : (e == V - 1 ? cur.xs : z0[e + 1 < V ? e + 1 : e]);
+            const float c = cur.s[e];
+            const float E = pot_e(cur.rr[e], c, xl, xr, cur.ym[e], cur.yp[e], zm[e], cur.zp[e],
+                                  odd ? axl[0][e] : axl[1][e], odd ? axr[0][e] : axr[1][e],
+                                  odd ? ayl[0][e] : ayl[1][e], odd ? ayr[0][e] : ayr[1][e],
+                                  odd ? az[0][e] : az[1][e]);
+            out[e] = __fmaf_rn(odd ? fc[0][e] : fc[1][e], E, c);
+        }
+        st_vec<V>(phi + sk, out);
+        // copies of the updated cells
+        if (odd && q0 == 0) phi[sk + half] = out[0];                  // cell nx+1 = cell 1
+        if (!odd && q0 + V == half) phi[sk - q0 - 1] = out[V - 1];    // cell 0 = cell nx
+        if (k == L.nz) st_vec<V>(phi + sb, out);                      // plane 0
+        if (k == 1) st_vec<V>(phi + sb + (L.nz + 1) * L.rz, out);     // plane nz+1
+        if (PY && j == L.ny) st_vec<V>(phi + sk - L.ny * L.hq, out);  // row 0
+        if (PY && j == 1) st_vec<V>(phi + sk + L.ny * L.hq, out);     // row ny+1
+#pragma unroll
+        for (int e = 0; e < V; ++e) {
+            zm[e] = z0[e];
+            z0[e] = cur.zp[e];
+        }
+        if (PF) cur = nxt;
+    }
+}
+
+// u, v, w, p += the corrections Phi stands for, in FP64: the low faces of
+// every interior cell (u(i) += mu_u (Phi(i-1) - Phi(i))/dx, v likewise
+// except a wall face v(1), w likewise) and p += Phi/dt_gamma.  Each thread
+// writes its own cell's entries only.
+template <int PY>
+__global__ void k_pot_apply(mdx_dims d, pot_geom L, double idx, double idy, double idz, double idt,
+                            const double* __restrict__ mu, int plane_mu, double* __restrict__ u,
+                            double* __restrict__ v, double* __restrict__ w, double* __restrict__ p,
+                            const float* __restrict__ phi) {
+    const long long np = (long long)d.nxp * d.nyp;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < d.nint; t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % d.nx) + 1;
+        const long long rr = t / d.nx;
+        const int j = (int)(rr % d.ny) + 1;
+        const int k = (int)(rr / d.ny) + 1;
+        const long long q = i + (long long)d.nxp * j;
+        const double mu_u = plane_mu ? __ldg(mu + q) : 1.0;
+        const double mu_v = plane_mu ? __ldg(mu + np + q) : 1.0;
+        const double mu_w = plane_mu ? __ldg(mu + 2 * np + q) : 1.0;
+        const double c = (double)__ldg(phi + pot_idx(L, i, j, k));
+        const long long a = pidx(d, i, j, k);
+        u[a] += idx * mu_u * ((double)__ldg(phi + pot_idx(L, i - 1, j, k)) - c);
+        if (PY || j > 1) v[a] += idy * mu_v * ((double)__ldg(phi + pot_idx(L, i, j - 1, k)) - c);
+        w[a] += idz * mu_w * ((double)__ldg(phi + pot_idx(L, i, j, k - 1)) - c);
+        p[a] += c * idt;
+    }
+}
+
+bool pot_supported(const mdx_ctx_t* ctx) {
+    const mdx_dims& d = ctx->d;
+    if (d.nx % 4 != 0 || d.nz % 2 != 0) return false;
+    if (ctx->bc.is_periodic[1] && d.ny % 2 != 0) return false;
+    const pot_geom L = pot_make(d);
+    return 2LL * L.H + 64 < (1LL << 31) && (long long)(d.nx + 2) * (d.ny + 2) < (1LL << 31);
+}
+
+// One allocation for Phi and r~ (zeroed: the copies and the rows a wall
+// reads stay 0 until written) and the column table.
+int pot_alloc(mdx_ctx_t* ctx) {
+    if (ctx->pt_base) return MDX_OK;
+    const pot_geom L = pot_make(ctx->d);
+    auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    const size_t arr = up(sizeof(float) * 2 * (size_t)L.H);
+    const size_t tab = up(sizeof(float4) * (size_t)(ctx->d.nx + 2) * (ctx->d.ny + 2));
+    const size_t total = 2 * arr + tab;
+    char* base = nullptr;
+    MDX_CUDA(ctx, cudaMalloc(&base, total));
+    MDX_CUDA(ctx, cudaMemsetAsync(base, 0, total, ctx->stream));
+    ctx->pt_phi = reinterpret_cast<float*>(base);
+    ctx->pt_r = reinterpret_cast<float*>(base + arr);
+    ctx->pt_tab = reinterpret_cast<float4*>(base + 2 * arr);
+    ctx->pt_base = base;
+    ctx->pt_bytes = total;
+    return MDX_OK;
+}
+
+// Shapes of the potential-form sweep the autotuner tries (all give the same
+// bits): positions per thread V, planes per march KZ, next-plane prefetch.
+#define POT_SHAPES 8
+static const int pot_shape_v[POT_SHAPES] = {2, 2, 4, 4, 2, 4, 2, 4};
+static const int pot_shape_kz[POT_SHAPES] = {8, 16, 8, 16, 4, 4, 8, 16};
+template <int PY>
+static int pot_launch(mdx_ctx_t* ctx, int shape, const pot_geom& L, int cs) {
+    const int V = pot_shape_v[shape], KZ = pot_shape_kz[shape];
+    dim3 block(32, 8);
+    dim3 grid((L.nx / 2 / V + 31) / 32, (L.ny + 7) / 8, (L.nz + KZ - 1) / KZ);
+    void (*kfn)(pot_geom, int, float*, const float*, const float4*) = nullptr;
+    switch (shape) {
+        case 0: kfn = k_pot_sweep<PY, 2, 8, true>; break;
+        case 1: kfn = k_pot_sweep<PY, 2, 16, true>; break;
+        case 2: kfn = k_pot_sweep<PY, 4, 8, true>; break;
+        case 3: kfn = k_pot_sweep<PY, 4, 16, true>; break;
+        case 4: kfn = k_pot_sweep<PY, 2, 4, true>; break;
+        case 5: kfn = k_pot_sweep<PY, 4, 4, true>; break;
+        case 6: kfn = k_pot_sweep<PY, 2, 8, false>; break;
+        default: kfn = k_pot_sweep<PY, 4, 16, false>; break;
+    }
+    MDX_LAUNCH(ctx, MDX_T_SOR_SWEEP, "pot sweep", kfn, grid, block, 0, L, cs, ctx->pt_phi, ctx->pt_r, ctx->pt_tab);
+    return MDX_OK;
+}
+
 bool mixed_supported(const mdx_ctx_t* ctx) {
     const mdx_bc_t& b = ctx->bc;
     if (!b.is_periodic[0] || !b.is_periodic[2]) return false;
@@ -600,6 +933,11 @@ void mdx_mixed_free(mdx_ctx_t* ctx) {
     for (auto a : arrs) *a = nullptr;
     ctx->mx_base = nullptr;
     ctx->mx_bytes = 0;
+    if (ctx->pt_base) cudaFree(ctx->pt_base);
+    ctx->pt_base = nullptr;
+    ctx->pt_phi = ctx->pt_r = nullptr;
+    ctx->pt_tab = nullptr;
+    ctx->pt_bytes = 0;
 }
 
 // Called after u <- u*, the FP64 IBM factors of this projection and any
@@ -610,8 +948,12 @@ int mdx_k_projection_redblack_mixed(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t
     *handled = false;
     if (!mixed_supported(ctx) || ctx->opts.tol <= 0.0) return MDX_OK;
     *handled = true;
-    MDX_TRY(mixed_alloc(ctx));
+    // the potential form where the grid allows it, unless the face form is asked for
+    const bool pot = ctx->opts.inner_form == 0 && pot_supported(ctx);
+    if (pot) MDX_TRY(pot_alloc(ctx));
+    else MDX_TRY(mixed_alloc(ctx));
     const mdx_dims& d = ctx->d;
+    const pot_geom L = pot_make(d);
     const mdx_grid_t& g = ctx->g;
     const mdx_solver_opts_t& o = ctx->opts;
     const int py = ctx->bc.is_periodic[1] ? 1 : 0;
@@ -619,13 +961,24 @@ int mdx_k_projection_redblack_mixed(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t
     const double idx = 1.0 / g.dx, idy = 1.0 / g.dy, idz = 1.0 / g.dz;
     mixed_params P{(float)idx, (float)idy, (float)idz, (float)(1.0 / dg)};
     const int nbt = (int)std::min<long long>(((long long)d.nxp * d.nyp + 255) / 256, 1024);
-    MDX_LAUNCH(ctx, MDX_T_OTHER, "mixed tables", k_mixed_tables, nbt, 256, 0, d, py, idx * idx, idy * idy, idz * idz,
-               o.inner_sor > 0.0 ? o.inner_sor : o.sor, ctx->mu, ctx->mu_mode == MU_PLANE ? 1 : 0, ctx->mx_mu,
-               ctx->mx_fac);
+    const double inner_omega = o.inner_sor > 0.0 ? o.inner_sor : o.sor;
+    const int plane_mu = ctx->mu_mode == MU_PLANE ? 1 : 0;
+    if (pot)
+        MDX_LAUNCH(ctx, MDX_T_OTHER, "pot tables", k_pot_tables, nbt, 256, 0, L, py, idx * idx, idy * idy, idz * idz,
+                   inner_omega, ctx->mu, plane_mu, ctx->pt_tab);
+    else
+        MDX_LAUNCH(ctx, MDX_T_OTHER, "mixed tables", k_mixed_tables, nbt, 256, 0, d, py, idx * idx, idy * idy,
+                   idz * idz, inner_omega, ctx->mu, plane_mu, ctx->mx_mu, ctx->mx_fac);
     MDX_TRY(mdx_reduce_init(ctx));
 
     auto residual = [&](double* l2, double* umax) -> int {
-        if (py)
+        if (pot && py)
+            MDX_LAUNCH(ctx, MDX_T_RESIDUAL, "pot residual", k_pot_residual<1>, ctx->red_blocks, MDX_RED_THREADS, 0, d,
+                       L, idx, idy, idz, f[MDX_UN], f[MDX_VN], f[MDX_WN], ctx->pt_r, ctx->red_part);
+        else if (pot)
+            MDX_LAUNCH(ctx, MDX_T_RESIDUAL, "pot residual", k_pot_residual<0>, ctx->red_blocks, MDX_RED_THREADS, 0, d,
+                       L, idx, idy, idz, f[MDX_UN], f[MDX_VN], f[MDX_WN], ctx->pt_r, ctx->red_part);
+        else if (py)
             MDX_LAUNCH(ctx, MDX_T_RESIDUAL, "mixed residual", k_mixed_residual<1>, ctx->red_blocks, MDX_RED_THREADS,
                        0, d, idx, idy, idz, f[MDX_UN], f[MDX_VN], f[MDX_WN], ctx->mx_r, ctx->red_part);
         else
@@ -638,7 +991,10 @@ int mdx_k_projection_redblack_mixed(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t
         return MDX_OK;
     };
     auto corr_residual = [&](double* l2) -> int {
-        if (py)
+        if (pot)
+            MDX_LAUNCH(ctx, MDX_T_RESIDUAL, "pot corr residual", k_pot_corr_residual, ctx->red_blocks,
+                       MDX_RED_THREADS, 0, d, L, ctx->pt_phi, ctx->pt_r, ctx->pt_tab, ctx->red_part);
+        else if (py)
             MDX_LAUNCH(ctx, MDX_T_RESIDUAL, "mixed corr residual", k_mixed_corr_residual<1>, ctx->red_blocks,
                        MDX_RED_THREADS, 0, d, P, ctx->mx_du, ctx->mx_dv, ctx->mx_dw, ctx->mx_r, ctx->red_part);
         else
@@ -695,7 +1051,55 @@ int mdx_k_projection_redblack_mixed(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t
                            ctx->mx_du, ctx->mx_dv, ctx->mx_dw, ctx->mx_dp, ctx->mx_r, ctx->mx_mu, ctx->mx_fac);
         return MDX_OK;
     };
+    // the potential form's sweeps: the autotuner's choice among its shapes,
+    // each timed on one block of iterations of the first projections (all
+    // give the same bits)
+    int pcands[POT_SHAPES], npc = 0;
+    const bool v4_ok = (d.nx / 2) % 4 == 0;
+    if (o.sor_variant >= 1 && o.sor_variant <= POT_SHAPES && (pot_shape_v[o.sor_variant - 1] == 2 || v4_ok))
+        pcands[npc++] = o.sor_variant - 1;   // one shape asked for
+    else
+        for (int c = 0; c < POT_SHAPES; ++c)
+            if (pot_shape_v[c] == 2 || v4_ok) pcands[npc++] = c;
+    if (pot && npc > 1 && !ctx->tune_ev[0]) {
+        MDX_CUDA(ctx, cudaEventCreate(&ctx->tune_ev[0]));
+        MDX_CUDA(ctx, cudaEventCreate(&ctx->tune_ev[1]));
+    }
+    auto pot_sweeps = [&](int iters) -> int {
+        mdx_event_pair run{};
+        int cand = ctx->pt_tuned - 1;
+        const bool tuning = cand < 0;
+        int slot = 0;
+        if (tuning) {
+            while (slot < npc - 1 && ctx->pt_tune_ms[pcands[slot]] > 0.0) ++slot;
+            cand = pcands[slot];
+            if (npc > 1) MDX_CUDA(ctx, cudaEventRecord(ctx->tune_ev[0], ctx->stream));
+        }
+        mdx_sweep_run_begin(ctx, &run);
+        for (int it = 0; it < iters; ++it)
+            for (int cs = 1; cs >= 0; --cs)   // first colour i+j+k odd, as the face form
+                MDX_TRY(py ? pot_launch<1>(ctx, cand, L, cs) : pot_launch<0>(ctx, cand, L, cs));
+        mdx_sweep_run_end(ctx, &run);
+        used_kind = 7;
+        if (tuning && npc == 1) {
+            ctx->pt_tuned = cand + 1;
+        } else if (tuning) {
+            MDX_CUDA(ctx, cudaEventRecord(ctx->tune_ev[1], ctx->stream));
+            MDX_CUDA(ctx, cudaEventSynchronize(ctx->tune_ev[1]));
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, ctx->tune_ev[0], ctx->tune_ev[1]) == cudaSuccess && iters > 0)
+                ctx->pt_tune_ms[cand] = ms > 0.f ? ms / iters : 1e-9;
+            if (slot == npc - 1 && ctx->pt_tune_ms[cand] > 0.0) {
+                int best = pcands[0];
+                for (int t = 1; t < npc; ++t)
+                    if (ctx->pt_tune_ms[pcands[t]] < ctx->pt_tune_ms[best]) best = pcands[t];
+                ctx->pt_tuned = best + 1;
+            }
+        }
+        return MDX_OK;
+    };
     auto sweeps = [&](int iters) -> int {
+        if (pot) return pot_sweeps(iters);
         mdx_event_pair run{};
         int cand = cands[0];
         bool tuning = false;
@@ -773,10 +1177,18 @@ int mdx_k_projection_redblack_mixed(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t
                 else if ((stale += m) >= 20 * cs.every) break;
                 block = cs.next(it, e, inner_target);
             }
-            const long long n = d.npad;
-            MDX_LAUNCH(ctx, MDX_T_OTHER, "mixed apply", k_mixed_apply, (int)std::min<long long>((n + 255) / 256, 8192),
-                       256, 0, d, f[MDX_UN], f[MDX_VN], f[MDX_WN], f[MDX_PN], ctx->mx_du, ctx->mx_dv, ctx->mx_dw,
-                       ctx->mx_dp);
+            if (pot) {
+                const int nb = (int)std::min<long long>((d.nint + 255) / 256, 8192);
+                auto kfn = py ? k_pot_apply<1> : k_pot_apply<0>;
+                MDX_LAUNCH(ctx, MDX_T_OTHER, "pot apply", kfn, nb, 256, 0, d, L, idx, idy, idz, 1.0 / dg, ctx->mu,
+                           plane_mu, f[MDX_UN], f[MDX_VN], f[MDX_WN], f[MDX_PN], ctx->pt_phi);
+                MDX_CUDA(ctx, cudaMemsetAsync(ctx->pt_phi, 0, sizeof(float) * 2 * (size_t)L.H, ctx->stream));
+            } else {
+                const long long n = d.npad;
+                MDX_LAUNCH(ctx, MDX_T_OTHER, "mixed apply", k_mixed_apply,
+                           (int)std::min<long long>((n + 255) / 256, 8192), 256, 0, d, f[MDX_UN], f[MDX_VN],
+                           f[MDX_WN], f[MDX_PN], ctx->mx_du, ctx->mx_dv, ctx->mx_dw, ctx->mx_dp);
+            }
             MDX_TRY(residual(&r, nullptr));
             if (!std::isfinite(r)) { s.status = MDX_ERR_NONFINITE; break; }
             if (r <= target) { s.status = MDX_OK; break; }
@@ -786,7 +1198,7 @@ int mdx_k_projection_redblack_mixed(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t
     s.iterations = it;
     // mixed path: 100 + outer FP64 corrections with the colour sweeps, 300 +
     // outer with the fused red+black pass, 500 + outer with the vector
-    // colour sweeps
+    // colour sweeps, 700 + outer with the potential form
     s.variant = 100 * used_kind + outer;
     ctx->last = s;
     if (st) *st = s;

@@ -143,6 +143,15 @@ struct mdx_ctx {
                                              // vector colour sweeps with 2 and 4 cells per thread)
     unsigned rb32_attr = 0;                  // fused FP32 pass: shared-memory attribute set, bit per kernel
     double rb32_tune_ms[8] = {0.0};          // time per iteration per candidate
+    // potential form of the FP32 sweeps (opts.inner_form 0): phi and r~ in
+    // their own colour-split layout (k_sor_mixed.cu pot_geom) and one float4
+    // table per (i, j) column, carved from one allocation of pt_bytes
+    float *pt_phi = nullptr, *pt_r = nullptr;
+    float4* pt_tab = nullptr;
+    void* pt_base = nullptr;
+    size_t pt_bytes = 0;
+    int pt_tuned = 0;                        // candidate + 1 chosen by the autotuner (0: not yet)
+    double pt_tune_ms[8] = {0.0};            // time per iteration per candidate
     // warm starts: increments of the last projection of each RK substage
     int guess_mode = 0;                      // MDX_GUESS_*
     bool record_increments = false;

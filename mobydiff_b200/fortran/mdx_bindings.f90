@@ -31,7 +31,8 @@ module mdx_bindings
         integer(C_INT) :: sor_variant, sor_kz
         integer(C_INT) :: check_mode
         integer(C_INT) :: fft_kernel
-        integer(C_INT) :: reserved_i(3)
+        integer(C_INT) :: inner_form
+        integer(C_INT) :: reserved_i(2)
         real(C_DOUBLE) :: atol
         real(C_DOUBLE) :: inner_sor
         real(C_DOUBLE) :: reserved_d(6)

@@ -137,8 +137,9 @@ def test_mixed_precision_members_match_single_channels():
     each member lands within the solve tolerance of the single-context mixed
     path and of the FP64 ensemble (the FP32 arithmetic is not bit-equal: the
     ensemble file is built without FMA contraction)."""
+    # the ensemble's FP32 sweeps are the face form: the single contexts run it too
     mix = M.make_solver_opts(M.SOLVER_REDBLACK, sor=1.7, tol=1e-8, check_every=10, max_iter=200000,
-                             precision=M.PREC_MIXED)
+                             precision=M.PREC_MIXED, inner_form=1)
     f64 = M.make_solver_opts(M.SOLVER_REDBLACK, sor=1.7, tol=1e-8, check_every=10, max_iter=200000)
     mems = _members()
     with M.Ensemble(mems, mix) as E, M.Ensemble(mems, f64) as F:
@@ -181,8 +182,9 @@ def test_sixteen_uneven_members_bitwise_and_mixed():
                 s.step(2)
                 for n in ("un", "vn", "wn", "pn"):
                     assert np.array_equal(E.get(q, n), s.get(n)), (q, n)
+    # the ensemble's FP32 sweeps are the face form: the single contexts run it too
     opts = M.make_solver_opts(M.SOLVER_REDBLACK, sor=1.7, tol=1e-8, check_every=10, max_iter=200000,
-                              precision=M.PREC_MIXED, adaptive_checks=False)
+                              precision=M.PREC_MIXED, adaptive_checks=False, inner_form=1)
     with M.Ensemble(mems, opts) as E:
         E.set_guess(M.GUESS_EXTRAPOLATED)
         E.ic()

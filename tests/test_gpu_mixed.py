@@ -41,7 +41,7 @@ def test_mixed_projection_matches_fp64(tol):
         stp = sp.pressure_projection(g.dt * c[0])
         stm = sm.pressure_projection(g.dt * c[0])
         assert stp.status == 0 and stm.status == 0
-        assert stm.variant > 100                      # the mixed path ran
+        assert stm.variant // 100 == 7                # the mixed path ran, in the potential form
         assert stm.residual <= tol * 1.0000001 or stm.residual * stm.residual0 <= stm.atol
         # FP32 sweeps: about as many iterations as FP64
         assert stm.iterations <= 1.5 * stp.iterations + 200
@@ -100,8 +100,8 @@ def test_mixed_falls_back_to_fp64_for_other_boundaries():
                                               ((96, 20, 18), False)])
 @pytest.mark.parametrize("tol", [1e-8, 0.0])
 def test_fused_and_vector_fp32_sweeps_equal_colour_sweeps(shape, periodic_y, tol):
-    """The fused red+black FP32 pass (one launch per iteration, every tile
-    shape the autotuner tries) and the vector colour sweeps (2 and 4 cells
+    """Face form of the FP32 correction sweeps: the fused red+black FP32
+    pass (one launch per iteration, every tile shape the autotuner tries) and the vector colour sweeps (2 and 4 cells
     per thread, then the faster) against one launch per colour with one cell
     per thread: the same FP32 corrections bit for bit, so the same
     iterations and the same FP64 state after the projection; tol 0 runs 25
@@ -123,7 +123,7 @@ def test_fused_and_vector_fp32_sweeps_equal_colour_sweeps(shape, periodic_y, tol
             s.init_pressure_solver(M.make_solver_opts(M.SOLVER_REDBLACK, sor=1.7, tol=tol or 1e-30, check_every=5,
                                                       max_iter=25 if tol == 0.0 else 100000,
                                                       precision=M.PREC_MIXED, sor_variant=variant,
-                                                      adaptive_checks=False))
+                                                      adaptive_checks=False, inner_form=1))
             sts = [s.pressure_projection(0.4e-3, check=False) for _ in range(5)]
             out[variant] = ([st.iterations for st in sts], [st.variant for st in sts],
                             {n: s.get(n) for n in ("un", "vn", "wn", "pn")})
@@ -135,3 +135,71 @@ def test_fused_and_vector_fp32_sweeps_equal_colour_sweeps(shape, periodic_y, tol
         assert it1 == it0, variant
         for n in f1:
             assert np.array_equal(f1[n], f0[n]), (variant, n, float(np.max(np.abs(f1[n] - f0[n]))))
+
+
+def _sweep_case(shape, periodic_y):
+    nx, ny, nz = shape
+    if periodic_y:
+        g = O.Grid(nx, ny, nz, lx=2.0, ly=1.0, lz=1.0, re=800.0, dt=1e-3, forcing=(0.1, 0.0, 0.0))
+        bc = O.BC((True, True, True))
+        f = random_fields(g, 31, "zinv", scale=0.3)
+    else:
+        g, bc, f = _wavy_case(nx, ny, nz)
+        a, b, c = O.rk_coeffs()
+        O.momentum(g, bc, f, g.dt * a[0], g.dt * b[0], g.dt * c[0])
+    return g, bc, f
+
+
+POT_V = [2, 2, 4, 4, 2, 4, 2, 4]   # cells per thread of the potential form's sweep shapes (sor_variant 1-8)
+
+
+@pytest.mark.parametrize("shape,periodic_y", [((64, 32, 32), False), ((40, 12, 10), False), ((32, 16, 16), True),
+                                              ((96, 20, 18), False)])
+def test_potential_form_shapes_agree_and_match_face_form(shape, periodic_y):
+    """The potential form of the FP32 correction sweeps (the accumulated phi
+    of each cell swept with the 7-point stencil the face updates amount to):
+    each shape of its sweep kernel (2 or 4 cells per thread, marches of 4, 8
+    or 16 planes, with or without the next plane's prefetch; sor_variant
+    1-8) gives the same bits; against the face form
+    the projections meet the same FP64 tolerance with velocity within 1e-6
+    and about as many red-black iterations."""
+    g, bc, f = _sweep_case(shape, periodic_y)
+    nx = shape[0]
+    out = {}
+    for form, variant in [(1, 1)] + [(0, v) for v in range(1, 9)]:
+        if form == 0 and POT_V[variant - 1] == 4 and (nx // 2) % 4:
+            continue
+        with to_device(M, g, bc, f) as s:
+            s.init_pressure_solver(M.make_solver_opts(M.SOLVER_REDBLACK, sor=1.7, tol=1e-8, check_every=5,
+                                                      max_iter=100000, precision=M.PREC_MIXED, sor_variant=variant,
+                                                      adaptive_checks=False, inner_form=form))
+            sts = [s.pressure_projection(0.4e-3, check=False) for _ in range(3)]
+            assert all(st.status == 0 for st in sts)
+            l2, _ = s.divergence_norms()
+            assert l2 <= max(1e-8 * sts[-1].residual0, sts[-1].atol) * 1.0000001
+            out[(form, variant)] = ([st.iterations for st in sts], [st.variant for st in sts],
+                                    {n: s.get(n) for n in ("un", "vn", "wn", "pn")})
+    it_f, v_f, f_f = out[(1, 1)]
+    it_p, v_p, f_p = out[(0, 1)]
+    assert all(v // 100 == 1 for v in v_f), v_f
+    assert all(v // 100 == 7 for v in v_p), v_p
+    for key, (it, v, fl) in out.items():
+        if key[0] == 0 and key != (0, 1):
+            assert it == it_p, key
+            for n in fl:
+                assert np.array_equal(fl[n], f_p[n]), (key, n)
+    print("iterations face", it_f, "potential", it_p)
+    assert sum(it_p) <= 1.3 * sum(it_f) + 50
+    num = sum(float(np.sum((f_p[n] - f_f[n]) ** 2)) for n in ("un", "vn", "wn"))
+    den = sum(float(np.sum(f_f[n] ** 2)) for n in ("un", "vn", "wn"))
+    assert (num / den) ** 0.5 <= 1e-6
+
+
+def test_potential_form_needs_nx_multiple_of_4():
+    """nx = 42 (nx/2 odd): the mixed path runs the face form."""
+    g, bc, f = _sweep_case((42, 12, 10), False)
+    with to_device(M, g, bc, f) as s:
+        s.init_pressure_solver(M.make_solver_opts(M.SOLVER_REDBLACK, sor=1.7, tol=1e-8, check_every=5,
+                                                  precision=M.PREC_MIXED))
+        st = s.pressure_projection(0.4e-3, check=False)
+        assert st.status == 0 and st.variant > 100 and st.variant // 100 != 7

@@ -66,6 +66,7 @@ def test_sections_keys_aliases(tmp_path, capfd):
         inner_omega = 1.95
         residual_checks = fixed
         fft_kernel = stockham
+        inner_form = faces
     """)
     g, b, o, r = M.read_runtime_config(path)
     assert (g.nx, g.ny, g.nz) == (96, 48, 40)
@@ -82,7 +83,7 @@ def test_sections_keys_aliases(tmp_path, capfd):
     assert r.output_interval == 0 and r.output_prefix == b"run 1" and r.field_interval == 5
     assert r.ic == 1 and r.seed == 42 and r.ibm == 1 and r.ibm_amp == 0.05
     assert r.guess == M.GUESS_EXTRAPOLATED and o.inner_sor == 1.95 and o.check_mode == 1
-    assert o.fft_kernel == 1
+    assert o.fft_kernel == 1 and o.inner_form == 1
     out = capfd.readouterr().out
     assert "unknown boundary key" in out      # bottom_min_p_type: "bottom" is not a direction
 
