@@ -171,8 +171,10 @@ SOR_NAMES = {1: "one launch per colour sweep", 2: "fused red+black pass 32x8", 3
 SOR32_NAMES = {1: "k_sor_sweep32: one launch per colour, one cell per thread",
                3: "k_rb32_fused: one launch per red+black iteration",
                5: "k_sor_sweep32v: one launch per colour, 2 or 4 cells per thread",
-               7: "k_pot_sweep: potential form, one launch per colour, 2 or 4 cells per thread marching z"}
-SOR32_TRAFFIC = {1: "sor_sweep32", 3: "rb32_fused", 5: "sor_sweep32v", 7: "pot_sweep"}
+               7: "potential form: the autotuner's pick among k_pot_sweep (2 or 4 cells per thread), k_pot_sweep_w "
+                  "(one warp per row), k_pot_sweep_a (planes staged by cp.async) and k_pot_run_w (one warp per row, "
+                  "a block of iterations per cooperative launch; the pick on 256x128x128)"}
+SOR32_TRAFFIC = {1: "sor_sweep32", 3: "rb32_fused", 5: "sor_sweep32v", 7: "pot_run_w"}
 # algorithmic bytes per cell of one FP32 colour sweep launch (a fused
 # red+black launch does both colours): the face form reads and writes 4
 # floats per cell of one colour (16 B per cell of the grid); the potential
@@ -1311,9 +1313,9 @@ def main():
     ap.add_argument("--profile-mixed", action="store_true",
                     help="profiling run for ncu: the full-size t=0 projection with FP32 sweeps to residual 1e-8")
     ap.add_argument("--quick", action="store_true", help="skip the plain FP64 leg at residual 1e-10")
-    ap.add_argument("--sor-variant", type=int, default=0, choices=list(range(9)),
+    ap.add_argument("--sor-variant", type=int, default=0, choices=list(range(16)),
                     help="red-black kernel variant (0: autotuned; all give the same bits); FP64 sweeps and the "
-                         "face form 1-5, the potential form's sweep shapes 1-8")
+                         "face form 1-5, the potential form's sweep shapes 1-15")
     ap.add_argument("--inner-form", type=int, default=0, choices=[0, 1],
                     help="mixed red-black: FP32 correction sweeps in the potential form (0) or the face form (1)")
     ap.add_argument("--fft-kernel", type=int, default=0, choices=[0, 1],

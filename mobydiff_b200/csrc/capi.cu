@@ -99,10 +99,10 @@ void mdx_sweep_run_begin(mdx_ctx_t* ctx, mdx_event_pair* p) {
     cudaEventRecord(p->a, ctx->stream);
 }
 
-void mdx_sweep_run_end(mdx_ctx_t* ctx, mdx_event_pair* p) {
+void mdx_sweep_run_end(mdx_ctx_t* ctx, mdx_event_pair* p, long long sweeps) {
     if (!p->a) return;
     cudaEventRecord(p->b, ctx->stream);
-    p->n = ctx->launches - p->n;
+    p->n = sweeps >= 0 ? sweeps : ctx->launches - p->n;
     ctx->ev_pending.push_back(*p);
 }
 
@@ -326,7 +326,7 @@ int mdx_set_bc(mdx_ctx_t* ctx, const mdx_bc_t* bc) {
     ctx->rb32_tuned = 0;
     for (int t = 0; t < 8; ++t) ctx->rb32_tune_ms[t] = 0.0;
     ctx->pt_tuned = 0;
-    for (int t = 0; t < 8; ++t) ctx->pt_tune_ms[t] = 0.0;
+    for (int t = 0; t < 16; ++t) ctx->pt_tune_ms[t] = 0.0;
     // FFT solver: walls in x or z change the solve grid (and need Neumann
     // pressure there); rebuild its workspace for the new conditions
     if (ctx->solver && ctx->opts.solver == MDX_SOLVER_FFT &&
@@ -544,7 +544,7 @@ int mdx_init_pressure_solver(mdx_ctx_t* ctx, const mdx_solver_opts_t* opts) {
     ctx->rb32_tuned = 0;
     for (int t = 0; t < 8; ++t) ctx->rb32_tune_ms[t] = 0.0;
     ctx->pt_tuned = 0;
-    for (int t = 0; t < 8; ++t) ctx->pt_tune_ms[t] = 0.0;
+    for (int t = 0; t < 16; ++t) ctx->pt_tune_ms[t] = 0.0;
     MDX_TRY(mdx_reduce_init(ctx));
     if (o.solver == MDX_SOLVER_REDBLACK) {
         // src/modules/pressure/pressure_redblack.f90:16-18

@@ -23,6 +23,9 @@
 // z-invariant.  Other boundary sets run the FP64 path.
 #include "mdx_cell32.cuh"
 
+#include <cooperative_groups.h>
+namespace cg = cooperative_groups;
+
 #include <algorithm>
 #include <cmath>
 
@@ -591,9 +594,14 @@ __device__ __forceinline__ float pot_e(float r, float c, float xl, float xr, flo
 // at a wall), a_z, fac = -omega/denom}; column nx+1 repeats column 1's a_x,
 // row ny+1 holds the top faces' a_y (0 at walls, row 1's when y is
 // periodic).  a_f and fac are formed in FP64 (the denominator of
-// pressure_redblack.f90:124-126) and rounded once.
+// pressure_redblack.f90:124-126) and rounded once.  tabu repeats the a_y of
+// every column's top face, row j holding cy(i, j+1) at (i-1), rows ncu
+// (nx rounded up to 4) apart, so that a row's top faces are one aligned
+// vector load.
+__host__ __device__ inline int pot_ncu(int nx) { return (nx + 3) & ~3; }
 __global__ void k_pot_tables(pot_geom L, int py, double idx2, double idy2, double idz2, double sor,
-                             const double* __restrict__ mu, int plane_mu, float4* __restrict__ tab) {
+                             const double* __restrict__ mu, int plane_mu, float4* __restrict__ tab,
+                             float* __restrict__ tabu) {
     const int nxp = L.nx + 2, nyp = L.ny + 2;
     const long long np = (long long)nxp * nyp;
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < np; t += (long long)gridDim.x * blockDim.x) {
@@ -615,6 +623,7 @@ __global__ void k_pot_tables(pot_geom L, int py, double idx2, double idy2, doubl
             o.y = py ? (float)(idy2 * MU(1, i, 1)) : 0.f;
         }
         tab[t] = o;
+        if (j >= 1 && i >= 1 && i <= L.nx) tabu[(j - 1) * pot_ncu(L.nx) + (i - 1)] = o.y;
     }
 }
 
@@ -776,6 +785,301 @@ k_pot_sweep(pot_geom L, int cs, float* __restrict__ phi, const float* __restrict
     }
 }
 
+// The same colour sweep with one warp per row (nx/2 = 32 V positions, so a
+// lane owns V positions and a warp the whole row) and 8 rows per block
+// (ny a multiple of 8).  The x neighbours come from the neighbouring lanes by
+// shuffle, wrapping at the row's ends (x periodic); the other colour's rows
+// j-1 and j+1 from a shared-memory exchange between the block's warps
+// (warps 0 and 7 also load the rows just outside the block); the
+// coefficients from aligned vector loads, the top faces' a_y from tabu.  The
+// arithmetic is pot_e's, so the result is k_pot_sweep's bit for bit.
+// V floats at p (8- or 16-byte aligned), cached in L2 only: in the
+// persistent kernel Phi changes between its sweeps, so it bypasses L1.
+template <int V>
+__device__ __forceinline__ void ld_vec_cg(float (&a)[V], const float* p) {
+    if constexpr (V == 4) {
+        const float4 q = __ldcg(reinterpret_cast<const float4*>(p));
+        a[0] = q.x; a[1] = q.y; a[2] = q.z; a[3] = q.w;
+    } else {
+        const float2 q = __ldcg(reinterpret_cast<const float2*>(p));
+        a[0] = q.x; a[1] = q.y;
+    }
+}
+
+// The column coefficients a lane of the warp-per-row sweeps holds: its 2V
+// columns 2 q0 + 1 .. 2 q0 + 2V, odd cells at even m (set 0), even cells at
+// odd m (set 1); the top faces' a_y from tabu, the next lane's first a_x by
+// shuffle (lane 31: column nx+1 = column 1).
+template <int V>
+struct pot_coef {
+    float axl[2][V], axr[2][V], ayl[2][V], ayr[2][V], az[2][V], fc[2][V];
+    __device__ __forceinline__ void load(const pot_geom& L, int j, int q0, int lane, const float4* __restrict__ tab,
+                                         const float* __restrict__ tabu) {
+        const float4* t0 = tab + j * (L.nx + 2) + 2 * q0 + 1;
+        const float* tu = tabu + j * pot_ncu(L.nx) + 2 * q0;
+        float up[2 * V];
+#pragma unroll
+        for (int m = 0; m < 2 * V; m += 4) {
+            const float4 u4 = __ldg(reinterpret_cast<const float4*>(tu + m));
+            up[m] = u4.x;
+            up[m + 1] = u4.y;
+            up[m + 2] = u4.z;
+            up[m + 3] = u4.w;
+        }
+#pragma unroll
+        for (int m = 0; m < 2 * V; ++m) {
+            const float4 c = __ldg(t0 + m);
+            const int s = m & 1, e = m >> 1;
+            axl[s][e] = c.x;
+            ayl[s][e] = c.y;
+            az[s][e] = c.z;
+            fc[s][e] = c.w;
+            ayr[s][e] = up[m];
+            if (m > 0) axr[(m - 1) & 1][(m - 1) >> 1] = c.x;
+        }
+        axr[1][V - 1] = __shfl_sync(0xffffffffu, axl[0][0], (lane + 1) & 31);
+    }
+};
+
+// One colour sweep of rows j0 .. j0+7 (warp w: row j0 + w), planes k0 .. k1,
+// by one block of the warp-per-row kernels.  COH: Phi is read through L2
+// only (it changed since the kernel started), else through the read-only
+// path.
+template <int PY, int V, bool COH>
+__device__ __forceinline__ void pot_rows_sweep(const pot_geom& L, int cs, int j0, int k0, int k1,
+                                               float* __restrict__ phi, const float* __restrict__ r,
+                                               const pot_coef<V>& C, float (*ybuf)[10][32 * V]) {
+    constexpr int NW = 8, RL = 32 * V;
+    const int lane = threadIdx.x, w = threadIdx.y;
+    const int j = j0 + w, q0 = V * lane;
+    const int oh = 1 - cs;
+    const int ob = pot_row(L, oh, j, 0) + 4 + q0;   // other colour, row j, plane 0, position q0
+    const int sb = pot_row(L, cs, j, 0) + 4 + q0;   // swept colour
+    const bool hlo = w == 0, hhi = w == NW - 1;
+    const int hb = pot_row(L, oh, hlo ? j0 - 1 : j0 + NW, 0) + 4 + q0;   // the row outside the block
+    auto ldp = [&](float (&a)[V], const float* p) {
+        if constexpr (COH) ld_vec_cg<V>(a, p);
+        else ld_vec_ro<V>(a, p);
+    };
+    struct plane_in { float zp[V], s[V], rr[V], h[V]; };
+    auto load = [&](plane_in& P, int k) {
+        ldp(P.zp, phi + ob + (k + 1) * L.rz);
+        ldp(P.s, phi + sb + k * L.rz);
+        ld_vec_ro<V>(P.rr, r + sb + k * L.rz);
+        if (hlo || hhi) ldp(P.h, phi + hb + k * L.rz);
+    };
+    float zm[V], z0[V];
+    ldp(zm, phi + ob + (k0 - 1) * L.rz);
+    ldp(z0, phi + ob + k0 * L.rz);
+    plane_in cur, nxt;
+    load(cur, k0);
+    for (int k = k0; k <= k1; ++k) {
+        if (k < k1) load(nxt, k + 1);
+        // the other colour's rows j0-1 .. j0+NW of plane k; the buffers
+        // alternate with k, so one barrier per plane keeps writes of plane
+        // k+1 apart from reads of plane k
+        float(*yb)[RL] = ybuf[k & 1];
+        st_vec<V>(&yb[w + 1][q0], z0);
+        if (hlo) st_vec<V>(&yb[0][q0], cur.h);
+        if (hhi) st_vec<V>(&yb[NW + 1][q0], cur.h);
+        __syncthreads();
+        float ym[V], yp[V];
+        ld_vec<V>(ym, &yb[w][q0]);
+        ld_vec<V>(yp, &yb[w + 2][q0]);
+        const bool odd = ((cs + j + k) & 1) != 0;
+        const float xlw = __shfl_sync(0xffffffffu, z0[V - 1], (lane + 31) & 31);   // position q0 - 1
+        const float xrw = __shfl_sync(0xffffffffu, z0[0], (lane + 1) & 31);        // position q0 + V
+        const int sk = sb + k * L.rz;
+        float out[V];
+#pragma unroll
+        for (int e = 0; e < V; ++e) {
+            const float xl = odd ? (e == 0 ? xlw : z0[e > 0 ? e - 1 : 0]) : z0[e];
+            const float xr = odd ? z0[e] : (e == V - 1 ? xrw : z0[e + 1 < V ? e + 1 : e]);
+            const float c = cur.s[e];
+            const float E = pot_e(cur.rr[e], c, xl, xr, ym[e], yp[e], zm[e], cur.zp[e],
+                                  odd ? C.axl[0][e] : C.axl[1][e], odd ? C.axr[0][e] : C.axr[1][e],
+                                  odd ? C.ayl[0][e] : C.ayl[1][e], odd ? C.ayr[0][e] : C.ayr[1][e],
+                                  odd ? C.az[0][e] : C.az[1][e]);
+            out[e] = __fmaf_rn(odd ? C.fc[0][e] : C.fc[1][e], E, c);
+        }
+        st_vec<V>(phi + sk, out);
+        // copies of the updated cells, for the residual and the FP64 update
+        if (odd && lane == 0) phi[sk + RL] = out[0];                  // cell nx+1 = cell 1
+        if (!odd && lane == 31) phi[sk - q0 - 1] = out[V - 1];        // cell 0 = cell nx
+        if (k == L.nz) st_vec<V>(phi + sb, out);                      // plane 0
+        if (k == 1) st_vec<V>(phi + sb + (L.nz + 1) * L.rz, out);     // plane nz+1
+        if (PY && j == L.ny) st_vec<V>(phi + sk - L.ny * L.hq, out);  // row 0
+        if (PY && j == 1) st_vec<V>(phi + sk + L.ny * L.hq, out);     // row ny+1
+#pragma unroll
+        for (int e = 0; e < V; ++e) {
+            zm[e] = z0[e];
+            z0[e] = cur.zp[e];
+        }
+        cur = nxt;
+    }
+}
+
+template <int PY, int V, int KZ>
+__global__ void __launch_bounds__(256)
+k_pot_sweep_w(pot_geom L, int cs, float* __restrict__ phi, const float* __restrict__ r,
+              const float4* __restrict__ tab, const float* __restrict__ tabu) {
+    __shared__ __align__(16) float ybuf[2][10][32 * V];
+    const int j0 = 1 + (int)blockIdx.x * 8;
+    const int k0 = 1 + (int)blockIdx.y * KZ;
+    pot_coef<V> C;
+    C.load(L, j0 + (int)threadIdx.y, V * (int)threadIdx.x, threadIdx.x, tab, tabu);
+    pot_rows_sweep<PY, V, false>(L, cs, j0, k0, min(k0 + KZ - 1, L.nz), phi, r, C, ybuf);
+}
+
+// The warp-per-row sweeps of `iters` red-black iterations in one cooperative
+// launch: every block keeps its rows' coefficients in registers for all of
+// them, and a grid-wide barrier separates the colour sweeps (every block is
+// resident: the host launches this only when the grid fits the device).
+template <int PY, int V, int KZ>
+__global__ void __launch_bounds__(256)
+k_pot_run_w(pot_geom L, int iters, float* __restrict__ phi, const float* __restrict__ r,
+            const float4* __restrict__ tab, const float* __restrict__ tabu) {
+    __shared__ __align__(16) float ybuf[2][10][32 * V];
+    cg::grid_group grid = cg::this_grid();
+    const int j0 = 1 + (int)blockIdx.x * 8;
+    const int k0 = 1 + (int)blockIdx.y * KZ;
+    const int k1 = min(k0 + KZ - 1, L.nz);
+    pot_coef<V> C;
+    C.load(L, j0 + (int)threadIdx.y, V * (int)threadIdx.x, threadIdx.x, tab, tabu);
+    for (int it = 0; it < iters; ++it)
+        for (int cs = 1; cs >= 0; --cs) {
+            pot_rows_sweep<PY, V, true>(L, cs, j0, k0, k1, phi, r, C, ybuf);
+            grid.sync();
+        }
+}
+
+// The warp-per-row sweep with its planes staged in shared memory: a ring of
+// POT_SLOTS plane slots, each holding the other colour's rows j0-1 ..
+// j0+8, the swept colour's rows j0 .. j0+7 and their r~ rows, filled by
+// cp.async two planes ahead of the plane being swept.  Every neighbour value
+// is then a shared-memory read (the row ends wrap, x periodic); the
+// arithmetic is pot_e's, so the result is k_pot_sweep's bit for bit.
+#define POT_SLOTS 5
+__device__ __forceinline__ void pot_cp16(unsigned dst, const float* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void pot_cp8(unsigned dst, const float* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src) : "memory");
+}
+template <int PY, int V, int KZ>
+__global__ void __launch_bounds__(256)
+k_pot_sweep_a(pot_geom L, int cs, float* __restrict__ phi, const float* __restrict__ r,
+              const float4* __restrict__ tab, const float* __restrict__ tabu) {
+    constexpr int NW = 8, RL = 32 * V;
+    constexpr int ROWS = 3 * NW + 2;              // other rows j0-1..j0+NW, swept rows, r~ rows
+    constexpr int SLOT = ROWS * RL;               // floats per slot
+    extern __shared__ __align__(16) float pring[];   // [POT_SLOTS][ROWS][RL]
+    const int lane = threadIdx.x, w = threadIdx.y;
+    const int j0 = 1 + (int)blockIdx.x * NW;
+    const int j = j0 + w;
+    const int k0 = 1 + (int)blockIdx.y * KZ;
+    const int k1 = min(k0 + KZ - 1, L.nz);
+    const int q0 = V * lane;
+    const int ncol = L.nx + 2;
+    const int oh = 1 - cs;
+    // staging: warp w copies the other colour's row j (and warps 0 / NW-1
+    // the rows j0-1 / j0+NW), the swept row j and its r~ row, V floats a lane
+    const unsigned sbase = (unsigned)__cvta_generic_to_shared(pring) + 4u * q0;
+    const int go = pot_row(L, oh, j, 0) + 4 + q0;
+    const int gs = pot_row(L, cs, j, 0) + 4 + q0;
+    const bool hlo = w == 0, hhi = w == NW - 1;
+    const int gh = pot_row(L, oh, hlo ? j0 - 1 : j0 + NW, 0) + 4 + q0;
+    const int hrow = hlo ? 0 : NW + 1;
+    auto issue = [&](int kk) {   // plane kk into its slot
+        const unsigned sl = sbase + 4u * (unsigned)(((kk % POT_SLOTS) + POT_SLOTS) % POT_SLOTS) * SLOT;
+        const int pk = kk * L.rz;
+        if constexpr (V == 4) {
+            pot_cp16(sl + 4u * (w + 1) * RL, phi + go + pk);
+            pot_cp16(sl + 4u * (NW + 2 + w) * RL, phi + gs + pk);
+            pot_cp16(sl + 4u * (2 * NW + 2 + w) * RL, r + gs + pk);
+            if (hlo || hhi) pot_cp16(sl + 4u * hrow * RL, phi + gh + pk);
+        } else {
+            pot_cp8(sl + 4u * (w + 1) * RL, phi + go + pk);
+            pot_cp8(sl + 4u * (NW + 2 + w) * RL, phi + gs + pk);
+            pot_cp8(sl + 4u * (2 * NW + 2 + w) * RL, r + gs + pk);
+            if (hlo || hhi) pot_cp8(sl + 4u * hrow * RL, phi + gh + pk);
+        }
+    };
+    // planes k0-1 .. k0+2 in flight while the coefficients load
+    for (int kk = k0 - 1; kk <= k0 + 2; ++kk) {
+        if (kk <= k1 + 1) issue(kk);
+        asm volatile("cp.async.commit_group;\n" ::);
+    }
+    float axl[2][V], axr[2][V], ayl[2][V], ayr[2][V], az[2][V], fc[2][V];
+    {
+        const float4* t0 = tab + j * ncol + 2 * q0 + 1;
+        const float* tu = tabu + j * pot_ncu(L.nx) + 2 * q0;
+        float up[2 * V];
+#pragma unroll
+        for (int m = 0; m < 2 * V; m += 4) {
+            const float4 u4 = __ldg(reinterpret_cast<const float4*>(tu + m));
+            up[m] = u4.x;
+            up[m + 1] = u4.y;
+            up[m + 2] = u4.z;
+            up[m + 3] = u4.w;
+        }
+#pragma unroll
+        for (int m = 0; m < 2 * V; ++m) {
+            const float4 c = __ldg(t0 + m);
+            const int s = m & 1, e = m >> 1;
+            axl[s][e] = c.x;
+            ayl[s][e] = c.y;
+            az[s][e] = c.z;
+            fc[s][e] = c.w;
+            ayr[s][e] = up[m];
+            if (m > 0) axr[(m - 1) & 1][(m - 1) >> 1] = c.x;
+        }
+        axr[1][V - 1] = __shfl_sync(0xffffffffu, axl[0][0], (lane + 1) & 31);
+    }
+    const int sb = gs;   // the swept row j, plane 0, position q0
+    for (int k = k0; k <= k1; ++k) {
+        // planes up to k+1 complete (only plane k+2's group may be pending)
+        asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+        __syncthreads();
+        // the slot of plane k+3 held plane k-2, which no warp reads any more
+        if (k + 3 <= k1 + 1) issue(k + 3);
+        asm volatile("cp.async.commit_group;\n" ::);
+        const float* Sm = pring + ((k - 1 + POT_SLOTS) % POT_SLOTS) * SLOT;
+        const float* S0 = pring + (k % POT_SLOTS) * SLOT;
+        const float* Sp = pring + ((k + 1) % POT_SLOTS) * SLOT;
+        float zm[V], z0[V], zp[V], ym[V], yp[V], sv[V], rr[V];
+        ld_vec<V>(zm, Sm + (w + 1) * RL + q0);
+        ld_vec<V>(z0, S0 + (w + 1) * RL + q0);
+        ld_vec<V>(zp, Sp + (w + 1) * RL + q0);
+        ld_vec<V>(ym, S0 + w * RL + q0);
+        ld_vec<V>(yp, S0 + (w + 2) * RL + q0);
+        ld_vec<V>(sv, S0 + (NW + 2 + w) * RL + q0);
+        ld_vec<V>(rr, S0 + (2 * NW + 2 + w) * RL + q0);
+        const bool odd = ((cs + j + k) & 1) != 0;
+        const float xs = odd ? S0[(w + 1) * RL + ((q0 + RL - 1) & (RL - 1))] : S0[(w + 1) * RL + ((q0 + V) & (RL - 1))];
+        const int sk = sb + k * L.rz;
+        float out[V];
+#pragma unroll
+        for (int e = 0; e < V; ++e) {
+            const float xl = odd ? (e == 0 ? xs : z0[e > 0 ? e - 1 : 0]) : z0[e];
+            const float xr = odd ? z0[e] : (e == V - 1 ? xs : z0[e + 1 < V ? e + 1 : e]);
+            const float c = sv[e];
+            const float E = pot_e(rr[e], c, xl, xr, ym[e], yp[e], zm[e], zp[e], odd ? axl[0][e] : axl[1][e],
+                                  odd ? axr[0][e] : axr[1][e], odd ? ayl[0][e] : ayl[1][e],
+                                  odd ? ayr[0][e] : ayr[1][e], odd ? az[0][e] : az[1][e]);
+            out[e] = __fmaf_rn(odd ? fc[0][e] : fc[1][e], E, c);
+        }
+        st_vec<V>(phi + sk, out);
+        if (odd && lane == 0) phi[sk + RL] = out[0];                  // cell nx+1 = cell 1
+        if (!odd && lane == 31) phi[sk - q0 - 1] = out[V - 1];        // cell 0 = cell nx
+        if (k == L.nz) st_vec<V>(phi + sb, out);                      // plane 0
+        if (k == 1) st_vec<V>(phi + sb + (L.nz + 1) * L.rz, out);     // plane nz+1
+        if (PY && j == L.ny) st_vec<V>(phi + sk - L.ny * L.hq, out);  // row 0
+        if (PY && j == 1) st_vec<V>(phi + sk + L.ny * L.hq, out);     // row ny+1
+    }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
 // u, v, w, p += the corrections Phi stands for, in FP64: the low faces of
 // every interior cell (u(i) += mu_u (Phi(i-1) - Phi(i))/dx, v likewise
 // except a wall face v(1), w likewise) and p += Phi/dt_gamma.  Each thread
@@ -820,26 +1124,105 @@ int pot_alloc(mdx_ctx_t* ctx) {
     auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
     const size_t arr = up(sizeof(float) * 2 * (size_t)L.H);
     const size_t tab = up(sizeof(float4) * (size_t)(ctx->d.nx + 2) * (ctx->d.ny + 2));
-    const size_t total = 2 * arr + tab;
+    const size_t tabu = up(sizeof(float) * (size_t)pot_ncu(ctx->d.nx) * (ctx->d.ny + 2));
+    const size_t total = 2 * arr + tab + tabu;
     char* base = nullptr;
     MDX_CUDA(ctx, cudaMalloc(&base, total));
     MDX_CUDA(ctx, cudaMemsetAsync(base, 0, total, ctx->stream));
     ctx->pt_phi = reinterpret_cast<float*>(base);
     ctx->pt_r = reinterpret_cast<float*>(base + arr);
     ctx->pt_tab = reinterpret_cast<float4*>(base + 2 * arr);
+    ctx->pt_tabu = reinterpret_cast<float*>(base + 2 * arr + tab);
     ctx->pt_base = base;
     ctx->pt_bytes = total;
     return MDX_OK;
 }
 
 // Shapes of the potential-form sweep the autotuner tries (all give the same
-// bits): positions per thread V, planes per march KZ, next-plane prefetch.
-#define POT_SHAPES 8
-static const int pot_shape_v[POT_SHAPES] = {2, 2, 4, 4, 2, 4, 2, 4};
-static const int pot_shape_kz[POT_SHAPES] = {8, 16, 8, 16, 4, 4, 8, 16};
+// bits): positions per thread V, planes per march KZ, next-plane prefetch;
+// shapes 8 and 9 are the warp-per-row kernel (V = nx/64), 10-12 the
+// warp-per-row kernel with its planes staged by cp.async, 13-14 the
+// warp-per-row sweeps of a whole block of iterations in one cooperative
+// launch (when its grid fits the device).
+#define POT_SHAPES 15
+static const int pot_shape_v[POT_SHAPES] = {2, 2, 4, 4, 2, 4, 2, 4, 0, 0, -1, -1, -1, -2, -2};
+static const int pot_shape_kz[POT_SHAPES] = {8, 16, 8, 16, 4, 4, 8, 16, 8, 16, 8, 16, 4, 8, 16};
+template <int PY>
+static void (*pot_run_kernel(const pot_geom& L, int KZ))(pot_geom, int, float*, const float*, const float4*,
+                                                        const float*) {
+    const bool v4 = L.nx / 2 == 128;
+    if (KZ == 8) return v4 ? k_pot_run_w<PY, 4, 8> : k_pot_run_w<PY, 2, 8>;
+    return v4 ? k_pot_run_w<PY, 4, 16> : k_pot_run_w<PY, 2, 16>;
+}
+static bool pot_shape_ok(const mdx_ctx_t* ctx, int shape) {
+    const mdx_dims& d = ctx->d;
+    const int half = d.nx / 2;
+    if (pot_shape_v[shape] > 0) return half % pot_shape_v[shape] == 0;
+    if (!((half == 64 || half == 128) && d.ny % 8 == 0)) return false;
+    if (pot_shape_v[shape] == -2) {   // the cooperative grid must be resident at once
+        const pot_geom L = pot_make(d);
+        const int KZ = pot_shape_kz[shape];
+        int occ = 0, sms = 0;
+        const bool py = ctx->bc.is_periodic[1] != 0;
+        auto fn = py ? pot_run_kernel<1>(L, KZ) : pot_run_kernel<0>(L, KZ);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 256, 0) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        return (long long)occ * sms >= (long long)(d.ny / 8) * ((d.nz + KZ - 1) / KZ);
+    }
+    return true;
+}
+// `iters` red-black iterations of shape 13 or 14: one cooperative launch
+template <int PY>
+static int pot_run(mdx_ctx_t* ctx, int shape, const pot_geom& L, int iters) {
+    const int KZ = pot_shape_kz[shape];
+    auto fn = pot_run_kernel<PY>(L, KZ);
+    dim3 grid(L.ny / 8, (L.nz + KZ - 1) / KZ);
+    pot_geom Lc = L;
+    int it = iters;
+    float* phi = ctx->pt_phi;
+    const float* r = ctx->pt_r;
+    const float4* tab = ctx->pt_tab;
+    const float* tabu = ctx->pt_tabu;
+    void* args[] = {&Lc, &it, &phi, &r, &tab, &tabu};
+    mdx_event_pair p{};
+    mdx_timer_begin(ctx, MDX_T_SOR_SWEEP, &p);
+    MDX_CUDA(ctx, cudaLaunchCooperativeKernel((const void*)fn, grid, dim3(32, 8), args, 0, ctx->stream));
+    mdx_timer_end(ctx, &p);
+    return mdx_check_launch(ctx, "pot run (cooperative)");
+}
 template <int PY>
 static int pot_launch(mdx_ctx_t* ctx, int shape, const pot_geom& L, int cs) {
     const int V = pot_shape_v[shape], KZ = pot_shape_kz[shape];
+    if (V < 0) {
+        void (*afn)(pot_geom, int, float*, const float*, const float4*, const float*) = nullptr;
+        const bool v4 = L.nx / 2 == 128;
+        if (KZ == 8) afn = v4 ? k_pot_sweep_a<PY, 4, 8> : k_pot_sweep_a<PY, 2, 8>;
+        else if (KZ == 16) afn = v4 ? k_pot_sweep_a<PY, 4, 16> : k_pot_sweep_a<PY, 2, 16>;
+        else afn = v4 ? k_pot_sweep_a<PY, 4, 4> : k_pot_sweep_a<PY, 2, 4>;
+        const int smem = (int)(sizeof(float) * POT_SLOTS * (3 * 8 + 2) * (L.nx / 2));
+        const unsigned bit = 1u << ((v4 ? 0 : 3) + (KZ == 8 ? 0 : KZ == 16 ? 1 : 2) + 6 * PY);
+        if (!(ctx->pt_attr & bit)) {
+            MDX_CUDA(ctx, cudaFuncSetAttribute(afn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+            ctx->pt_attr |= bit;
+        }
+        dim3 agrid(L.ny / 8, (L.nz + KZ - 1) / KZ);
+        MDX_LAUNCH(ctx, MDX_T_SOR_SWEEP, "pot sweep staged", afn, agrid, dim3(32, 8), smem, L, cs, ctx->pt_phi,
+                   ctx->pt_r, ctx->pt_tab, ctx->pt_tabu);
+        return MDX_OK;
+    }
+    if (V == 0) {
+        void (*wfn)(pot_geom, int, float*, const float*, const float4*, const float*) = nullptr;
+        const bool v4 = L.nx / 2 == 128;
+        if (KZ == 8) wfn = v4 ? k_pot_sweep_w<PY, 4, 8> : k_pot_sweep_w<PY, 2, 8>;
+        else wfn = v4 ? k_pot_sweep_w<PY, 4, 16> : k_pot_sweep_w<PY, 2, 16>;
+        dim3 wgrid(L.ny / 8, (L.nz + KZ - 1) / KZ);
+        MDX_LAUNCH(ctx, MDX_T_SOR_SWEEP, "pot sweep rows", wfn, wgrid, dim3(32, 8), 0, L, cs, ctx->pt_phi, ctx->pt_r,
+                   ctx->pt_tab, ctx->pt_tabu);
+        return MDX_OK;
+    }
     dim3 block(32, 8);
     dim3 grid((L.nx / 2 / V + 31) / 32, (L.ny + 7) / 8, (L.nz + KZ - 1) / KZ);
     void (*kfn)(pot_geom, int, float*, const float*, const float4*) = nullptr;
@@ -937,6 +1320,7 @@ void mdx_mixed_free(mdx_ctx_t* ctx) {
     ctx->pt_base = nullptr;
     ctx->pt_phi = ctx->pt_r = nullptr;
     ctx->pt_tab = nullptr;
+    ctx->pt_tabu = nullptr;
     ctx->pt_bytes = 0;
 }
 
@@ -965,7 +1349,7 @@ int mdx_k_projection_redblack_mixed(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t
     const int plane_mu = ctx->mu_mode == MU_PLANE ? 1 : 0;
     if (pot)
         MDX_LAUNCH(ctx, MDX_T_OTHER, "pot tables", k_pot_tables, nbt, 256, 0, L, py, idx * idx, idy * idy, idz * idz,
-                   inner_omega, ctx->mu, plane_mu, ctx->pt_tab);
+                   inner_omega, ctx->mu, plane_mu, ctx->pt_tab, ctx->pt_tabu);
     else
         MDX_LAUNCH(ctx, MDX_T_OTHER, "mixed tables", k_mixed_tables, nbt, 256, 0, d, py, idx * idx, idy * idy,
                    idz * idz, inner_omega, ctx->mu, plane_mu, ctx->mx_mu, ctx->mx_fac);
@@ -1055,12 +1439,11 @@ int mdx_k_projection_redblack_mixed(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t
     // each timed on one block of iterations of the first projections (all
     // give the same bits)
     int pcands[POT_SHAPES], npc = 0;
-    const bool v4_ok = (d.nx / 2) % 4 == 0;
-    if (o.sor_variant >= 1 && o.sor_variant <= POT_SHAPES && (pot_shape_v[o.sor_variant - 1] == 2 || v4_ok))
+    if (pot && o.sor_variant >= 1 && o.sor_variant <= POT_SHAPES && pot_shape_ok(ctx, o.sor_variant - 1))
         pcands[npc++] = o.sor_variant - 1;   // one shape asked for
-    else
+    else if (pot)
         for (int c = 0; c < POT_SHAPES; ++c)
-            if (pot_shape_v[c] == 2 || v4_ok) pcands[npc++] = c;
+            if (pot_shape_ok(ctx, c)) pcands[npc++] = c;
     if (pot && npc > 1 && !ctx->tune_ev[0]) {
         MDX_CUDA(ctx, cudaEventCreate(&ctx->tune_ev[0]));
         MDX_CUDA(ctx, cudaEventCreate(&ctx->tune_ev[1]));
@@ -1076,10 +1459,13 @@ int mdx_k_projection_redblack_mixed(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t
             if (npc > 1) MDX_CUDA(ctx, cudaEventRecord(ctx->tune_ev[0], ctx->stream));
         }
         mdx_sweep_run_begin(ctx, &run);
-        for (int it = 0; it < iters; ++it)
-            for (int cs = 1; cs >= 0; --cs)   // first colour i+j+k odd, as the face form
-                MDX_TRY(py ? pot_launch<1>(ctx, cand, L, cs) : pot_launch<0>(ctx, cand, L, cs));
-        mdx_sweep_run_end(ctx, &run);
+        if (pot_shape_v[cand] == -2 && iters > 0)
+            MDX_TRY(py ? pot_run<1>(ctx, cand, L, iters) : pot_run<0>(ctx, cand, L, iters));
+        else
+            for (int it = 0; it < iters; ++it)
+                for (int cs = 1; cs >= 0; --cs)   // first colour i+j+k odd, as the face form
+                    MDX_TRY(py ? pot_launch<1>(ctx, cand, L, cs) : pot_launch<0>(ctx, cand, L, cs));
+        mdx_sweep_run_end(ctx, &run, 2LL * iters);
         used_kind = 7;
         if (tuning && npc == 1) {
             ctx->pt_tuned = cand + 1;

@@ -148,10 +148,12 @@ struct mdx_ctx {
     // table per (i, j) column, carved from one allocation of pt_bytes
     float *pt_phi = nullptr, *pt_r = nullptr;
     float4* pt_tab = nullptr;
+    float* pt_tabu = nullptr;                // the columns' top-face a_y, one row per y row
     void* pt_base = nullptr;
     size_t pt_bytes = 0;
     int pt_tuned = 0;                        // candidate + 1 chosen by the autotuner (0: not yet)
-    double pt_tune_ms[8] = {0.0};            // time per iteration per candidate
+    unsigned pt_attr = 0;                    // staged sweeps: shared-memory attribute set, bit per kernel
+    double pt_tune_ms[16] = {0.0};            // time per iteration per candidate
     // warm starts: increments of the last projection of each RK substage
     int guess_mode = 0;                      // MDX_GUESS_*
     bool record_increments = false;
@@ -277,7 +279,9 @@ void mdx_timer_end(mdx_ctx_t* ctx, mdx_event_pair* p);
 // whole (MDX_T_SOR_BLOCK) whenever timing is on; `end` counts the launches
 // issued since `begin`.
 void mdx_sweep_run_begin(mdx_ctx_t* ctx, mdx_event_pair* p);
-void mdx_sweep_run_end(mdx_ctx_t* ctx, mdx_event_pair* p);
+// sweeps >= 0: the colour sweeps the run made, when one launch makes several
+// (the cooperative potential-form runs); otherwise the launches are counted
+void mdx_sweep_run_end(mdx_ctx_t* ctx, mdx_event_pair* p, long long sweeps = -1);
 int mdx_check_launch(mdx_ctx_t* ctx, const char* what);
 
 // Launch wrapper: times the launch when timing is on and checks the launch.

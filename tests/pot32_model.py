@@ -240,3 +240,107 @@ def sweep(L, py, cs, phi, r, tab, V, TX, TY, KZ, log=None):
                                 vst(t, L.row(cs, ny + 1, k) + 4 + q0, out)
                             zm, z0 = z0, zp
     return new
+
+
+def tabu_of(L, tab):
+    """k_pot_tables' tabu: row j holds the a_y of column i's top face,
+    cy(i, j+1), at (i - 1); rows ncu = nx rounded up to 4 apart."""
+    nx, ny = L.nx, L.ny
+    ncu = (nx + 3) & ~3
+    tu = np.zeros((ny + 2) * ncu)
+    for j in range(1, ny + 2):
+        for i in range(1, nx + 1):
+            tu[(j - 1) * ncu + (i - 1)] = tab[j, i, 1]
+    return tu, ncu
+
+
+def sweep_rows(L, py, cs, phi, r, tab, KZ):
+    """One colour sweep as k_pot_sweep_w runs it: one warp per row (nx/2 =
+    32 V positions), 8 rows per block, x neighbours by shuffle with the
+    row's wrap, rows j-1 and j+1 through the block's shared buffer (warps 0
+    and 7 load the rows just outside the block), coefficients from the
+    column table and tabu, the next lane's first a_x by shuffle."""
+    nx, ny, nz = L.nx, L.ny, L.nz
+    half = nx // 2
+    assert half % 32 == 0 and ny % 8 == 0
+    V = half // 32
+    NW = 8
+    old = phi.copy()
+    new = phi.copy()
+    tabf = tab.reshape(-1, 4)
+    ncol = nx + 2
+    tu, ncu = tabu_of(L, tab)
+    oh = 1 - cs
+    for by in range(ny // NW):
+        for bz in range((nz + KZ - 1) // KZ):
+            j0 = 1 + by * NW
+            k0 = 1 + bz * KZ
+            k1 = min(k0 + KZ - 1, nz)
+            # per lane coefficient sets, like the kernel's registers
+            co = {}
+            for w in range(NW):
+                j = j0 + w
+                for lane in range(32):
+                    q0 = V * lane
+                    cr = [tabf[j * ncol + 2 * q0 + 1 + m] for m in range(2 * V)]
+                    up = [tu[j * ncu + 2 * q0 + m] for m in range(2 * V)]
+                    axl = [[0.0] * V for _ in range(2)]
+                    axr = [[0.0] * V for _ in range(2)]
+                    ayl = [[0.0] * V for _ in range(2)]
+                    ayr = [[0.0] * V for _ in range(2)]
+                    az = [[0.0] * V for _ in range(2)]
+                    fc = [[0.0] * V for _ in range(2)]
+                    for m in range(2 * V):
+                        s_, e = m & 1, m >> 1
+                        axl[s_][e], ayl[s_][e], az[s_][e], fc[s_][e] = cr[m]
+                        ayr[s_][e] = up[m]
+                        if m > 0:
+                            axr[(m - 1) & 1][(m - 1) >> 1] = cr[m][0]
+                    co[(w, lane)] = [axl, axr, ayl, ayr, az, fc]
+                for lane in range(32):   # the shuffle of the next lane's first a_x
+                    co[(w, lane)][1][1][V - 1] = co[(w, (lane + 1) % 32)][0][0][0]
+            for k in range(k0, k1 + 1):
+                rows = {}
+                for w in range(-1, NW + 1):
+                    rows[w] = [old[L.row(oh, j0 + w, k) + 4 + q] for q in range(half)]
+                for w in range(NW):
+                    j = j0 + w
+                    z0 = rows[w]
+                    zm = [old[L.row(oh, j, k - 1) + 4 + q] for q in range(half)]
+                    zp = [old[L.row(oh, j, k + 1) + 4 + q] for q in range(half)]
+                    odd = (cs + j + k) & 1
+                    for lane in range(32):
+                        axl, axr, ayl, ayr, az, fc = co[(w, lane)]
+                        st = 0 if odd else 1
+                        q0 = V * lane
+                        out = []
+                        for e in range(V):
+                            q = q0 + e
+                            xl = z0[(q - 1) % half] if odd else z0[q]
+                            xr = z0[q] if odd else z0[(q + 1) % half]
+                            c = old[L.row(cs, j, k) + 4 + q]
+                            rr = r[L.row(cs, j, k) + 4 + q]
+                            E = (rr + axl[st][e] * (c - xl) + axr[st][e] * (c - xr)
+                                 + ayl[st][e] * (c - rows[w - 1][q]) + ayr[st][e] * (c - rows[w + 1][q])
+                                 + az[st][e] * ((c - zm[q]) + (c - zp[q])))
+                            out.append(c + fc[st][e] * E)
+                        sk = L.row(cs, j, k) + 4 + q0
+                        for e in range(V):
+                            new[sk + e] = out[e]
+                        if odd and lane == 0:
+                            new[sk + half] = out[0]
+                        if not odd and lane == 31:
+                            new[sk - q0 - 1] = out[V - 1]
+                        if k == nz:
+                            for e in range(V):
+                                new[L.row(cs, j, 0) + 4 + q0 + e] = out[e]
+                        if k == 1:
+                            for e in range(V):
+                                new[L.row(cs, j, nz + 1) + 4 + q0 + e] = out[e]
+                        if py and j == ny:
+                            for e in range(V):
+                                new[L.row(cs, 0, k) + 4 + q0 + e] = out[e]
+                        if py and j == 1:
+                            for e in range(V):
+                                new[L.row(cs, ny + 1, k) + 4 + q0 + e] = out[e]
+    return new

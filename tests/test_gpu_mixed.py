@@ -150,24 +150,34 @@ def _sweep_case(shape, periodic_y):
     return g, bc, f
 
 
-POT_V = [2, 2, 4, 4, 2, 4, 2, 4]   # cells per thread of the potential form's sweep shapes (sor_variant 1-8)
+# positions per thread of the potential form's sweep shapes (sor_variant 1-15; 0: one warp per row, -1: one
+# warp per row with the planes staged in shared memory, -2: one warp per row, a whole block of iterations in
+# one cooperative launch)
+POT_V = [2, 2, 4, 4, 2, 4, 2, 4, 0, 0, -1, -1, -1, -2, -2]
+
+
+def _pot_shape_ok(shape, variant):
+    nx, ny, _ = shape
+    v = POT_V[variant - 1]
+    return (nx in (128, 256) and ny % 8 == 0) if v <= 0 else (nx // 2) % v == 0
 
 
 @pytest.mark.parametrize("shape,periodic_y", [((64, 32, 32), False), ((40, 12, 10), False), ((32, 16, 16), True),
-                                              ((96, 20, 18), False)])
+                                              ((96, 20, 18), False), ((128, 24, 20), False), ((128, 16, 12), True)])
 def test_potential_form_shapes_agree_and_match_face_form(shape, periodic_y):
     """The potential form of the FP32 correction sweeps (the accumulated phi
     of each cell swept with the 7-point stencil the face updates amount to):
     each shape of its sweep kernel (2 or 4 cells per thread, marches of 4, 8
-    or 16 planes, with or without the next plane's prefetch; sor_variant
-    1-8) gives the same bits; against the face form
+    or 16 planes, with or without the next plane's prefetch, one warp per
+    row, planes staged in shared memory, whole blocks of iterations in one
+    cooperative launch; sor_variant 1-15) gives the same bits; against the face form
     the projections meet the same FP64 tolerance with velocity within 1e-6
     and about as many red-black iterations."""
     g, bc, f = _sweep_case(shape, periodic_y)
     nx = shape[0]
     out = {}
-    for form, variant in [(1, 1)] + [(0, v) for v in range(1, 9)]:
-        if form == 0 and POT_V[variant - 1] == 4 and (nx // 2) % 4:
+    for form, variant in [(1, 1)] + [(0, v) for v in range(1, 16)]:
+        if form == 0 and not _pot_shape_ok(shape, variant):
             continue
         with to_device(M, g, bc, f) as s:
             s.init_pressure_solver(M.make_solver_opts(M.SOLVER_REDBLACK, sor=1.7, tol=1e-8, check_every=5,

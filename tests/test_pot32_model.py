@@ -95,3 +95,40 @@ def test_potential_sweeps_equal_face_sweeps(nx, ny, nz, py, TX, TY, KZ, V):
             for i in range(1, nx + 1):
                 assert phi[L.idx(i, 0, k)] == phi[L.idx(i, ny, k)]
                 assert phi[L.idx(i, ny + 1, k)] == phi[L.idx(i, 1, k)]
+
+
+@pytest.mark.parametrize("nx,ny,nz,py,KZ", [(128, 8, 4, 0, 8), (128, 16, 6, 1, 4), (256, 8, 4, 0, 16)])
+def test_row_warp_sweeps_equal_thread_sweeps(nx, ny, nz, py, KZ):
+    """k_pot_sweep_w (one warp per row, shuffles and a shared-memory row
+    exchange) against the thread-by-thread sweep: the same values, copies
+    included, after a red and a black sweep from a random Phi."""
+    (idx, idy, idz, idt), r, mu_u, mu_v, mu_w, fac = _case(nx, ny, nz, py, nx + ny + nz)
+    L = PM.PotLayout(nx, ny, nz)
+    tab = PM.tables(nx, ny, nz, py, idx * idx, idy * idy, idz * idz, mu_u, mu_v, mu_w, fac)
+    rl = PM.to_layout(L, r, 0.0)
+    rng = np.random.default_rng(7)
+    phi = np.zeros(L.n)
+    for k in range(1, nz + 1):
+        for j in range(1, ny + 1):
+            for i in range(1, nx + 1):
+                phi[L.idx(i, j, k)] = rng.uniform(-1, 1)
+    # the copies a sweep's predecessor leaves
+    for k in range(1, nz + 1):
+        for j in range(1, ny + 1):
+            phi[L.idx(0, j, k)] = phi[L.idx(nx, j, k)]
+            phi[L.idx(nx + 1, j, k)] = phi[L.idx(1, j, k)]
+    for j in range(0 if py else 1, ny + 2 if py else ny + 1):
+        jj = (j - 1) % ny + 1
+        for i in range(0, nx + 2):
+            phi[L.idx(i, j, 0)] = phi[L.idx(i, jj, nz)]
+            phi[L.idx(i, j, nz + 1)] = phi[L.idx(i, jj, 1)]
+    if py:
+        for k in range(0, nz + 2):
+            for i in range(0, nx + 2):
+                phi[L.idx(i, 0, k)] = phi[L.idx(i, ny, k)]
+                phi[L.idx(i, ny + 1, k)] = phi[L.idx(i, 1, k)]
+    a = b = phi
+    for cs in (1, 0):
+        a = PM.sweep(L, py, cs, a, rl, tab, 2, 64, 8, KZ)
+        b = PM.sweep_rows(L, py, cs, b, rl, tab, KZ)
+        assert np.array_equal(a, b), cs
