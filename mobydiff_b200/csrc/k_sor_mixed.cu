@@ -934,16 +934,17 @@ k_pot_sweep_w(pot_geom L, int cs, float* __restrict__ phi, const float* __restri
 // The warp-per-row sweeps of `iters` red-black iterations in one cooperative
 // launch: every block keeps its rows' coefficients in registers for all of
 // them, and a grid-wide barrier separates the colour sweeps (every block is
-// resident: the host launches this only when the grid fits the device).
-template <int PY, int V, int KZ>
+// resident: the host launches this only when the grid fits the device).  z
+// is cut into gridDim.y chunks of nz/gridDim.y planes, rounded.
+template <int PY, int V>
 __global__ void __launch_bounds__(256)
 k_pot_run_w(pot_geom L, int iters, float* __restrict__ phi, const float* __restrict__ r,
             const float4* __restrict__ tab, const float* __restrict__ tabu) {
     __shared__ __align__(16) float ybuf[2][10][32 * V];
     cg::grid_group grid = cg::this_grid();
     const int j0 = 1 + (int)blockIdx.x * 8;
-    const int k0 = 1 + (int)blockIdx.y * KZ;
-    const int k1 = min(k0 + KZ - 1, L.nz);
+    const int k0 = 1 + (int)(((long long)blockIdx.y * L.nz) / gridDim.y);
+    const int k1 = (int)(((long long)(blockIdx.y + 1) * L.nz) / gridDim.y);
     pot_coef<V> C;
     C.load(L, j0 + (int)threadIdx.y, V * (int)threadIdx.x, threadIdx.x, tab, tabu);
     for (int it = 0; it < iters; ++it)
@@ -1143,43 +1144,48 @@ int pot_alloc(mdx_ctx_t* ctx) {
 // shapes 8 and 9 are the warp-per-row kernel (V = nx/64), 10-12 the
 // warp-per-row kernel with its planes staged by cp.async, 13-14 the
 // warp-per-row sweeps of a whole block of iterations in one cooperative
-// launch (when its grid fits the device).
+// launch (when its grid fits the device; 13: z in as many chunks as fill the
+// resident blocks, 14: chunks of 16 planes).
 #define POT_SHAPES 15
 static const int pot_shape_v[POT_SHAPES] = {2, 2, 4, 4, 2, 4, 2, 4, 0, 0, -1, -1, -1, -2, -2};
 static const int pot_shape_kz[POT_SHAPES] = {8, 16, 8, 16, 4, 4, 8, 16, 8, 16, 8, 16, 4, 8, 16};
 template <int PY>
-static void (*pot_run_kernel(const pot_geom& L, int KZ))(pot_geom, int, float*, const float*, const float4*,
-                                                        const float*) {
-    const bool v4 = L.nx / 2 == 128;
-    if (KZ == 8) return v4 ? k_pot_run_w<PY, 4, 8> : k_pot_run_w<PY, 2, 8>;
-    return v4 ? k_pot_run_w<PY, 4, 16> : k_pot_run_w<PY, 2, 16>;
+static void (*pot_run_kernel(const pot_geom& L))(pot_geom, int, float*, const float*, const float4*, const float*) {
+    return L.nx / 2 == 128 ? k_pot_run_w<PY, 4> : k_pot_run_w<PY, 2>;
+}
+// z chunks of the cooperative run: shape 13 as many as fill the device's
+// resident blocks (at most nz), shape 14 chunks of 16 planes; 0 when the
+// grid does not fit
+static int pot_run_chunks(const mdx_ctx_t* ctx, int shape) {
+    const mdx_dims& d = ctx->d;
+    const pot_geom L = pot_make(d);
+    int occ = 0, sms = 0;
+    const bool py = ctx->bc.is_periodic[1] != 0;
+    auto fn = py ? pot_run_kernel<1>(L) : pot_run_kernel<0>(L);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 256, 0) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    const long long slots = (long long)occ * sms, rb = d.ny / 8;
+    const int nch = shape == 13 ? (int)std::min<long long>(d.nz, slots / rb) : (d.nz + 15) / 16;
+    return (nch >= 1 && rb * nch <= slots) ? nch : 0;
 }
 static bool pot_shape_ok(const mdx_ctx_t* ctx, int shape) {
     const mdx_dims& d = ctx->d;
     const int half = d.nx / 2;
     if (pot_shape_v[shape] > 0) return half % pot_shape_v[shape] == 0;
     if (!((half == 64 || half == 128) && d.ny % 8 == 0)) return false;
-    if (pot_shape_v[shape] == -2) {   // the cooperative grid must be resident at once
-        const pot_geom L = pot_make(d);
-        const int KZ = pot_shape_kz[shape];
-        int occ = 0, sms = 0;
-        const bool py = ctx->bc.is_periodic[1] != 0;
-        auto fn = py ? pot_run_kernel<1>(L, KZ) : pot_run_kernel<0>(L, KZ);
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 256, 0) != cudaSuccess ||
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device) != cudaSuccess) {
-            cudaGetLastError();
-            return false;
-        }
-        return (long long)occ * sms >= (long long)(d.ny / 8) * ((d.nz + KZ - 1) / KZ);
-    }
+    if (pot_shape_v[shape] == -2) return pot_run_chunks(ctx, shape) > 0;   // the grid must be resident at once
     return true;
 }
 // `iters` red-black iterations of shape 13 or 14: one cooperative launch
 template <int PY>
 static int pot_run(mdx_ctx_t* ctx, int shape, const pot_geom& L, int iters) {
-    const int KZ = pot_shape_kz[shape];
-    auto fn = pot_run_kernel<PY>(L, KZ);
-    dim3 grid(L.ny / 8, (L.nz + KZ - 1) / KZ);
+    auto fn = pot_run_kernel<PY>(L);
+    const int nch = pot_run_chunks(ctx, shape);
+    if (nch <= 0) return mdx_fail(ctx, MDX_ERR_CUDA, "pot run: the cooperative grid does not fit the device");
+    dim3 grid(L.ny / 8, nch);
     pot_geom Lc = L;
     int it = iters;
     float* phi = ctx->pt_phi;
