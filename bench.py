@@ -1316,8 +1316,9 @@ def main():
     ap.add_argument("--sor-variant", type=int, default=0, choices=list(range(16)),
                     help="red-black kernel variant (0: autotuned; all give the same bits); FP64 sweeps and the "
                          "face form 1-5, the potential form's sweep shapes 1-15")
-    ap.add_argument("--inner-form", type=int, default=0, choices=[0, 1],
-                    help="mixed red-black: FP32 correction sweeps in the potential form (0) or the face form (1)")
+    ap.add_argument("--inner-form", type=int, default=0, choices=[0, 1, 2],
+                    help="mixed red-black: FP32 correction sweeps in the potential form (0; the ensemble keeps the "
+                         "face form), the face form (1), or the potential form in the ensemble too (2)")
     ap.add_argument("--fft-kernel", type=int, default=0, choices=[0, 1],
                     help="FFT path transforms: 0 warp-shuffle where nx/2 and nz allow, 1 shared-memory Stockham")
     ap.add_argument("--c3-steps", type=int, default=0,

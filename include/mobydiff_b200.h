@@ -104,7 +104,10 @@ typedef struct {
                           launch per iteration) in the fastest of four tile shapes; 4 or
                           5 one launch per colour with 2 or 4 cells per thread, the faster;
                           0 the fastest of all seven, each timed on one block of the
-                          first iterations (all give the same bits) */
+                          first iterations (all give the same bits).  In the potential
+                          form (inner_form 0 or 2): 1-15 pin one shape of its sweep
+                          kernels, 0 the fastest of those the grid allows (all give the
+                          same bits) */
     int sor_kz;        /* z planes per block of the fused pass (0: default 16) */
     int check_mode;    /* red-black, tol > 0: 0 (default) residual checks at multiples of check_every,
                           up to 8 blocks apart while the residual falls at a steady rate that
@@ -119,9 +122,10 @@ typedef struct {
                           cell alone, swept with the 7-point stencil that the face updates
                           of pressure_redblack.f90:117-241 amount to (the same iteration in
                           exact arithmetic; 8 B per cell per colour sweep instead of 30),
-                          where nx is a multiple of 4, the face form otherwise; 1: the face
-                          form (corrections du, dv, dw, dp updated face by face, kernels
-                          chosen by sor_variant) */
+                          where nx is a multiple of 4, the face form otherwise; the ensemble
+                          keeps the face form; 1: the face form (corrections du, dv, dw, dp
+                          updated face by face, kernels chosen by sor_variant); 2: the
+                          potential form in the ensemble's persistent kernel as well */
     int reserved_i[2];
     double atol;       /* red-black: absolute floor of ||div u||2, also accepted as converged.
                           < 0 (default): the FP64 round-off level of the divergence,

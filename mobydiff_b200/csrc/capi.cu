@@ -533,8 +533,8 @@ int mdx_init_pressure_solver(mdx_ctx_t* ctx, const mdx_solver_opts_t* opts) {
         return mdx_fail(ctx, MDX_ERR_ARG, "unknown solver %d", o.solver);
     if (o.precision != MDX_PREC_FP64 && o.precision != MDX_PREC_MIXED)
         return mdx_fail(ctx, MDX_ERR_ARG, "unknown precision %d", o.precision);
-    if (o.inner_form != 0 && o.inner_form != 1)
-        return mdx_fail(ctx, MDX_ERR_ARG, "inner_form must be 0 (potential) or 1 (faces), got %d", o.inner_form);
+    if (o.inner_form < 0 || o.inner_form > 2)
+        return mdx_fail(ctx, MDX_ERR_ARG, "inner_form must be 0, 1 or 2, got %d", o.inner_form);
     if (o.check_every < 1) o.check_every = 1;
     if (o.max_iter < 1) o.max_iter = 1;
     if (o.n_iter < 0) return mdx_fail(ctx, MDX_ERR_ARG, "n_iter must be >= 0");

@@ -197,7 +197,8 @@ struct Reader {
         } else if (key == "inner_form") {
             if (v == "potential" || v == "0") o->inner_form = 0;
             else if (v == "faces" || v == "1") o->inner_form = 1;
-            else warn("b200 inner_form must be potential or faces", line);
+            else if (v == "potential_all" || v == "2") o->inner_form = 2;
+            else warn("b200 inner_form must be potential, faces or potential_all", line);
         } else if (key == "max_iter") {
             rd_int(value, &o->max_iter, line);
         } else if (key == "check_every") {

@@ -135,6 +135,7 @@ struct ens_args {
     int n_iter, max_iter, check_every;
     double tol, atol;
     int mixed;                       // FP32 sweeps in FP64 defect correction
+    int pot;                         // ... carrying each cell's phi (the potential form, Phi in dp; inner_form 2)
     double inner_sor;                // their over-relaxation
     // 0: the whole substage; 1: up to the warm start, then the network's
     // inputs; 2: from the learned correction on (the network ran between)
@@ -394,6 +395,7 @@ __device__ void mixed_residual_tile(const ens_args& A, int ti) {
         const int j = (int)(q - kq * fy.d) + 1;
         const int k = (int)kq + 1;
         const double dv = mixed_residual_cell<0>(d, idx, idy, idz, i, j, k, un, vn, wn, r);
+        if (A.pot) M.dp[cidx(d, i, j, k)] = 0.f;   // Phi starts from 0 (its corrections were applied)
         const long long c = pidx(d, i, j, k);
         s += dv * dv;
         m = nanmax(m, fabs(dv));
@@ -425,7 +427,8 @@ __device__ void corr_residual_tile(const ens_args& A, int ti) {
         const unsigned kq = fq(q, fy);
         const int j = (int)(q - kq * fy.d) + 1;
         const int k = (int)kq + 1;
-        const float ev = corr_residual_cell<0>(d, P, i, j, k, M.du, M.dv, M.dw, M.r32);
+        const float ev = A.pot ? pot_split_e<0>(d, P, i, j, k, M.dp[cidx(d, i, j, k)], M.dp, M.r32, M.mu32)
+                               : corr_residual_cell<0>(d, P, i, j, k, M.du, M.dv, M.dw, M.r32);
         s += (double)ev * (double)ev;
         m = nanmax(m, fabs((double)ev));
     }
@@ -459,7 +462,8 @@ __device__ __forceinline__ void sweep32_tile(const ens_args& A, int parity, int 
         const int kk = (int)kq + 1;
         const int k = parity ? d.nz + 1 - kk : kk;
         const int i = 1 + ((j + k + parity) & 1) + 2 * (ni - 1);
-        sweep32_cell<0>(d, P, i, j, k, du, dv, dw, dp, r, mu32, fac32);
+        if (A.pot) pot_split_cell<0>(d, P, i, j, k, dp, r, mu32, fac32);
+        else sweep32_cell<0>(d, P, i, j, k, du, dv, dw, dp, r, mu32, fac32);
     }
 }
 
@@ -835,10 +839,22 @@ __global__ void __launch_bounds__(MAX_THREADS, MINB) k_ens_substage(ens_args A) 
         grid.sync();
         const int max_rounds = A.max_iter / max(A.check_every, 1) + 64;
         for (int round = 0; round < max_rounds; ++round) {
-            pad_tiles(A, [&](int m, const ens_member& M, long long t) {
-                const ens_state& S = A.st[m];
-                if (S.phase == 0 && S.outer > 0) mixed_apply_elem(M.d, t, M.un, M.vn, M.wn, M.pn, M.du, M.dv, M.dw, M.dp);
-            });
+            if (A.pot)
+                cell_tiles(A, [&](int m, const ens_member& M, unsigned t) {
+                    const ens_state& S = A.st[m];
+                    if (S.phase == 0 && S.outer > 0) {
+                        int i, j, k;
+                        cell_ijk(M, t, i, j, k);
+                        pot_split_apply<0>(M.d, i, j, k, M.idx, M.idy, M.idz, 1.0 / dg_of(A, M), M.ibm ? M.mu : nullptr,
+                                           M.dp, M.un, M.vn, M.wn, M.pn);
+                    }
+                });
+            else
+                pad_tiles(A, [&](int m, const ens_member& M, long long t) {
+                    const ens_state& S = A.st[m];
+                    if (S.phase == 0 && S.outer > 0)
+                        mixed_apply_elem(M.d, t, M.un, M.vn, M.wn, M.pn, M.du, M.dv, M.dw, M.dp);
+                });
             grid.sync();
             for (int ti = blockIdx.x; ti < A.cell.n; ti += gridDim.x)
                 if (A.st[A.cell.t[ti].x].phase == 0) mixed_residual_tile(A, ti);
@@ -1160,6 +1176,7 @@ ens_args make_args(mdx_ensemble_t* E, int s, int momentum) {
     A.tol = E->opts.tol;
     A.atol = E->opts.atol;
     A.mixed = E->opts.precision == MDX_PREC_MIXED && E->opts.tol > 0.0;
+    A.pot = A.mixed && E->opts.inner_form == 2;
     A.inner_sor = E->opts.inner_sor;
     A.split = 0;
     A.learn_ok = E->learn_ok;
@@ -1749,7 +1766,9 @@ int mdx_ensemble_member_stats(mdx_ensemble_t* E, int m, mdx_solve_stats_t* st, l
         st->residual = S.last_residual;
         st->residual0 = S.r0;
         st->atol = S.atol;
-        st->variant = E->opts.precision == MDX_PREC_MIXED && E->opts.tol > 0.0 ? 100 + S.outer : 1;
+        st->variant = E->opts.precision == MDX_PREC_MIXED && E->opts.tol > 0.0
+                          ? (E->opts.inner_form == 2 ? 700 : 100) + S.outer
+                          : 1;
         st->guessed = S.guessed;
     }
     if (iters_total) *iters_total = S.iters_total;

@@ -579,17 +579,6 @@ pot_geom pot_make(const mdx_dims& d) {
     return L;
 }
 
-// The cell update of the potential form, shared by the sweep and the
-// residual: e = r~ + sum a (c - neighbour), FP32 roundings explicit.
-__device__ __forceinline__ float pot_e(float r, float c, float xl, float xr, float ym, float yp, float zm, float zp,
-                                       float axl, float axr, float ayl, float ayr, float az) {
-    float e = __fmaf_rn(axl, __fsub_rn(c, xl), r);
-    e = __fmaf_rn(axr, __fsub_rn(c, xr), e);
-    e = __fmaf_rn(ayl, __fsub_rn(c, ym), e);
-    e = __fmaf_rn(ayr, __fsub_rn(c, yp), e);
-    return __fmaf_rn(az, __fadd_rn(__fsub_rn(c, zm), __fsub_rn(c, zp)), e);
-}
-
 // Column table: per (i, j) {a_x of the low x face, a_y of the low y face (0
 // at a wall), a_z, fac = -omega/denom}; column nx+1 repeats column 1's a_x,
 // row ny+1 holds the top faces' a_y (0 at walls, row 1's when y is
@@ -1339,7 +1328,7 @@ int mdx_k_projection_redblack_mixed(mdx_ctx_t* ctx, double dg, mdx_solve_stats_t
     if (!mixed_supported(ctx) || ctx->opts.tol <= 0.0) return MDX_OK;
     *handled = true;
     // the potential form where the grid allows it, unless the face form is asked for
-    const bool pot = ctx->opts.inner_form == 0 && pot_supported(ctx);
+    const bool pot = ctx->opts.inner_form != 1 && pot_supported(ctx);
     if (pot) MDX_TRY(pot_alloc(ctx));
     else MDX_TRY(mixed_alloc(ctx));
     const mdx_dims& d = ctx->d;

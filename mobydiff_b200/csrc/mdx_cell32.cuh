@@ -156,3 +156,69 @@ __device__ __forceinline__ void mixed_tables_elem(const mdx_dims& d, int py, dou
     }
     fac32[o] = (float)f;
 }
+
+// ---- potential form ----------------------------------------------------------
+// Starting from zero corrections, the face updates of sweep32_update leave
+// every face at h^-1 mu (Phi(low cell) - Phi(high cell)), Phi the sum of the
+// phi a cell has taken, so the divergence the next update needs is a
+// 7-point stencil of Phi: e = r~ + sum over the faces of a_f (Phi(c) -
+// Phi(across)), a_f = h^-2 mu_f (0 for a wall face), and the update is
+// Phi += fac e.  The cell arithmetic, FP32 roundings explicit, shared by the
+// single-channel kernels (k_sor_mixed.cu) and the ensemble.
+__device__ __forceinline__ float pot_e(float r, float c, float xl, float xr, float ym, float yp, float zm, float zp,
+                                       float axl, float axr, float ayl, float ayr, float az) {
+    float e = __fmaf_rn(axl, __fsub_rn(c, xl), r);
+    e = __fmaf_rn(axr, __fsub_rn(c, xr), e);
+    e = __fmaf_rn(ayl, __fsub_rn(c, ym), e);
+    e = __fmaf_rn(ayr, __fsub_rn(c, yp), e);
+    return __fmaf_rn(az, __fadd_rn(__fsub_rn(c, zm), __fsub_rn(c, zp)), e);
+}
+
+// e of cell (i, j, k) with Phi and r~ in the face form's colour-split layout
+// (cidx) and the FP32 factor planes mu32: x and z periodic, y periodic when
+// PY, else walls (rows 0 and ny+1 hold 0, their faces' a_y is 0).  Phi and r~
+// change inside a persistent kernel, so they are read with coherent loads.
+template <int PY>
+__device__ __forceinline__ float pot_split_e(const mdx_dims& d, const mixed_params& P, int i, int j, int k, float c,
+                                             const float* phi, const float* r, const float* mu32) {
+    const int ip = i == d.nx ? 1 : i + 1, im = i == 1 ? d.nx : i - 1;
+    const int kp = k == d.nz ? 1 : k + 1, km = k == 1 ? d.nz : k - 1;
+    const int jp = (PY && j == d.ny) ? 1 : j + 1, jm = (PY && j == 1) ? d.ny : j - 1;
+    const int np = split_plane_elems(d);
+    const float ix2 = __fmul_rn(P.idx, P.idx), iy2 = __fmul_rn(P.idy, P.idy), iz2 = __fmul_rn(P.idz, P.idz);
+    const float axl = __fmul_rn(ix2, mu32[pidx2(d, i, j)]);
+    const float axr = __fmul_rn(ix2, mu32[pidx2(d, ip, j)]);
+    const float ayl = (PY || j > 1) ? __fmul_rn(iy2, mu32[np + pidx2(d, i, j)]) : 0.f;
+    const float ayr = (PY || j < d.ny) ? __fmul_rn(iy2, mu32[np + pidx2(d, i, jp)]) : 0.f;
+    const float az = __fmul_rn(iz2, mu32[2 * np + pidx2(d, i, j)]);
+    return pot_e(r[cidx(d, i, j, k)], c, phi[cidx(d, im, j, k)], phi[cidx(d, ip, j, k)], phi[cidx(d, i, jm, k)],
+                 phi[cidx(d, i, jp, k)], phi[cidx(d, i, j, km)], phi[cidx(d, i, j, kp)], axl, axr, ayl, ayr, az);
+}
+
+// One potential-form update of cell (i, j, k), fac from the factor plane.
+template <int PY>
+__device__ __forceinline__ void pot_split_cell(const mdx_dims& d, const mixed_params& P, int i, int j, int k,
+                                               float* phi, const float* r, const float* mu32, const float* fac32) {
+    const long long c = cidx(d, i, j, k);
+    const float v = phi[c];
+    phi[c] = __fmaf_rn(fac32[pidx2(d, i, j)], pot_split_e<PY>(d, P, i, j, k, v, phi, r, mu32), v);
+}
+
+// u, v, w, p of cell (i, j, k) += the corrections Phi stands for, in FP64:
+// its low faces (a wall face v(1) stays) and p += Phi/dt_gamma; mu = the
+// FP64 factor planes (u, v, w, each (nx+2)(ny+2)) or null for none.
+template <int PY>
+__device__ __forceinline__ void pot_split_apply(const mdx_dims& d, int i, int j, int k, double idx, double idy,
+                                                double idz, double idt, const double* mu, const float* phi,
+                                                double* u, double* v, double* w, double* p) {
+    const int im = i == 1 ? d.nx : i - 1, km = k == 1 ? d.nz : k - 1;
+    const int jm = (PY && j == 1) ? d.ny : j - 1;
+    const long long np = (long long)d.nxp * d.nyp, q = i + (long long)d.nxp * j;
+    const double mu_u = mu ? mu[q] : 1.0, mu_v = mu ? mu[np + q] : 1.0, mu_w = mu ? mu[2 * np + q] : 1.0;
+    const double c = (double)phi[cidx(d, i, j, k)];
+    const long long a = pidx(d, i, j, k);
+    u[a] += idx * mu_u * ((double)phi[cidx(d, im, j, k)] - c);
+    if (PY || j > 1) v[a] += idy * mu_v * ((double)phi[cidx(d, i, jm, k)] - c);
+    w[a] += idz * mu_w * ((double)phi[cidx(d, i, j, km)] - c);
+    p[a] += c * idt;
+}

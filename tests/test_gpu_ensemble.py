@@ -162,6 +162,39 @@ def test_mixed_precision_members_match_single_channels():
                         assert rel_l2(E.get(q, n), other(n)) <= 1e-5, (q, n)
 
 
+def test_potential_form_members_match_single_channels():
+    """The potential form of the FP32 sweeps inside the persistent kernel
+    (each cell's phi in place of the face corrections): every member meets
+    the tolerance and lands within the solve tolerance of the single-context
+    potential form and of the face-form ensemble (velocity vector 1e-6, each
+    component 1e-5)."""
+    # inner_form 2: the potential form in the ensemble's kernel too (its default is the face form)
+    pot = M.make_solver_opts(M.SOLVER_REDBLACK, sor=1.7, tol=1e-8, check_every=10, max_iter=200000,
+                             precision=M.PREC_MIXED, inner_form=2)
+    face = M.make_solver_opts(M.SOLVER_REDBLACK, sor=1.7, tol=1e-8, check_every=10, max_iter=200000,
+                              precision=M.PREC_MIXED, inner_form=1)
+    mems = _members()
+    with M.Ensemble(mems, pot) as E, M.Ensemble(mems, face) as F:
+        for X in (E, F):
+            X.set_guess(M.GUESS_EXTRAPOLATED)
+            X.ic()
+        ie, i_f = E.step(4), F.step(4)
+        print("iterations: potential", ie, "face", i_f)
+        assert ie <= 1.3 * i_f + 100
+        for q, m in enumerate(mems):
+            st, _ = E.member_stats(q)
+            assert st.status == 0 and st.variant // 100 == 7, (q, st.variant)
+            assert st.residual <= 1e-8 * 1.0000001 or st.residual * st.residual0 <= st.atol * 1.0000001
+            with _single(m, pot, M.GUESS_EXTRAPOLATED) as s:
+                s.step(4)
+                for other in (s.get, lambda n: F.get(q, n)):
+                    num = sum(float(np.sum((E.get(q, n) - other(n)) ** 2)) for n in ("un", "vn", "wn"))
+                    den = sum(float(np.sum(other(n) ** 2)) for n in ("un", "vn", "wn"))
+                    assert (num / den) ** 0.5 <= 1e-6, q
+                    for n in ("un", "vn", "wn"):
+                        assert rel_l2(E.get(q, n), other(n)) <= 1e-5, (q, n)
+
+
 def test_sixteen_uneven_members_bitwise_and_mixed():
     """16 members of uneven sizes drawn like the 64-member configuration (nx,
     nz in 32..128, ny in 32..96, multiples of 16; Re in 1000..5000; A in

@@ -143,3 +143,13 @@ def test_ibm_coefficients_match_oracle(geom):
     assert np.array_equal(cv, f.coef_v)
     assert np.array_equal(cw, f.coef_w)
     assert (cu > 0).any() and (cu < 1e30 / 3000.0).any()
+
+
+def test_inner_form_values(tmp_path):
+    for text, want in (("potential", 0), ("faces", 1), ("potential_all", 2), ("2", 2)):
+        path = _ini(tmp_path, f"""
+            [b200]
+            inner_form = {text}
+        """)
+        _, _, o, _ = M.read_runtime_config(path)
+        assert o.inner_form == want, text
