@@ -770,7 +770,7 @@ k_pot_sweep(pot_geom L, int cs, float* __restrict__ phi, const float* __restrict
             zm[e] = z0[e];
             z0[e] = cur.zp[e];
         }
-        if (PF) cur = nxt;
+        if (PF && k < k1) cur = nxt;   // the last plane loads no successor
     }
 }
 
@@ -904,7 +904,7 @@ __device__ __forceinline__ void pot_rows_sweep(const pot_geom& L, int cs, int j0
             zm[e] = z0[e];
             z0[e] = cur.zp[e];
         }
-        cur = nxt;
+        if (k < k1) cur = nxt;   // the last plane loads no successor
     }
 }
 
