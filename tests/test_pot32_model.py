@@ -132,3 +132,17 @@ def test_row_warp_sweeps_equal_thread_sweeps(nx, ny, nz, py, KZ):
         a = PM.sweep(L, py, cs, a, rl, tab, 2, 64, 8, KZ)
         b = PM.sweep_rows(L, py, cs, b, rl, tab, KZ)
         assert np.array_equal(a, b), cs
+
+
+@pytest.mark.parametrize("nz", [2, 7, 16, 128, 130])
+def test_cooperative_run_chunks_cover_every_plane_once(nz):
+    """k_pot_run_w cuts z into gridDim.y chunks [1 + b nz / n, (b + 1) nz / n]
+    (integer division); for every chunk count up to nz the chunks are
+    non-empty and cover planes 1..nz exactly once, in order."""
+    for n in range(1, nz + 1):
+        planes = []
+        for b in range(n):
+            k0, k1 = 1 + (b * nz) // n, ((b + 1) * nz) // n
+            assert k1 >= k0, (n, b)
+            planes.extend(range(k0, k1 + 1))
+        assert planes == list(range(1, nz + 1)), n
